@@ -1,0 +1,233 @@
+"""Generate golden input/output vectors by running the reference's own source.
+
+Run in an environment that has the reference checkout (it is not needed anywhere
+else)::
+
+    python tests/golden/make_golden.py /root/reference
+
+JAX is not installed here, so ``numpy_jax_shim`` is installed as ``jax`` first; the
+reference modules (``src/microcosmos/{utils,forces,simulate}.py``,
+``solver/{fluid,pbd,config}.py``, ``structs/*.py``, ``graph.py``) are then imported
+from the checkout unmodified and executed on numpy float32.  Each case writes one
+``.npz`` with its inputs, its parameters and the reference outputs.
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+sys.path.insert(0, REPO)
+
+import numpy_jax_shim  # noqa: E402
+
+
+def load_reference(ref_root):
+    numpy_jax_shim.install()
+    sys.path.insert(0, os.path.join(ref_root, "src"))
+    import microcosmos.simulate as simulate_mod
+    import microcosmos.forces as forces_mod
+    import microcosmos.utils as utils_mod
+    import microcosmos.solver.fluid as fluid_mod
+    import microcosmos.solver.pbd as pbd_mod
+    import microcosmos.solver.config as config_mod
+    import microcosmos.graph as graph_mod
+    from microcosmos.structs.nodes import Nodes
+    from microcosmos.structs.edges import Edges
+    from microcosmos.structs.fields import Fields
+    for cls in (Nodes, Edges, Fields):
+        if not hasattr(cls, "__replace__"):
+            cls.__replace__ = lambda self, **kw: dataclasses.replace(self, **kw)
+    return dict(simulate=simulate_mod, forces=forces_mod, utils=utils_mod, fluid=fluid_mod,
+                pbd=pbd_mod, config=config_mod, graph=graph_mod, Nodes=Nodes, Edges=Edges,
+                Fields=Fields)
+
+
+def A(x):
+    return np.asarray(x).view(np.ndarray).copy()
+
+
+def baseline_config(cfg_mod, **over):
+    """PBD_SCHEME with the benchmark overrides (viscosity 0.1 -> tau+=0.8, Lambda=1/4,
+    4-point IB kernel, steric on, stretch/bend/"twist"=shear 1.0/0.1/0.1)."""
+    base = dict(viscosity=0.1, lambda_trt=0.25, ibm_kernel_size=4, enable_steric=True,
+                stiffness_stretch=1.0, stiffness_shear=0.1)
+    base.update(over)
+    return dataclasses.replace(cfg_mod.PBD_SCHEME, **base)
+
+
+CFG_KEYS = ["cycles_per_step", "stiffness_stretch", "stiffness_shear", "damping", "enable_fluid",
+            "viscosity", "max_fluid_velocity", "ibm_iterations", "synthetic_node_width",
+            "ibm_kernel_size", "ibm_relaxation", "node_mass", "lambda_trt", "enable_force_clamp",
+            "enable_steric", "steric_strength", "steric_sigma", "steric_neighbor_skip",
+            "steric_scatter_value"]
+
+
+def cfg_arrays(cfg):
+    return {"cfg_" + k: np.asarray(getattr(cfg, k)) for k in CFG_KEYS}
+
+
+def state_arrays(prefix, nodes, edges, fields):
+    out = {}
+    if nodes is not None:
+        out[prefix + "position"] = A(nodes.position)
+        out[prefix + "velocity"] = A(nodes.velocity)
+    if edges is not None:
+        out[prefix + "theta"] = A(edges.theta)
+        out[prefix + "pairs"] = A(edges.pairs)
+        out[prefix + "rest_lengths"] = A(edges.rest_lengths)
+        out[prefix + "bending_pairs"] = A(edges.bending_pairs)
+        out[prefix + "bending_rest_angles"] = A(edges.bending_rest_angles)
+        out[prefix + "bending_stiffness"] = A(edges.bending_stiffness)
+    if fields is not None:
+        out[prefix + "steric"] = A(fields.steric)
+        out[prefix + "fluid_velocity"] = A(fields.fluid_velocity)
+        if fields.f_grid is not None:
+            out[prefix + "f_grid"] = A(fields.f_grid)
+    return out
+
+
+def to_ref(R, sc):
+    jnp = sys.modules["jax"].numpy
+    nodes = R["Nodes"](position=jnp.array(sc.position), velocity=jnp.array(sc.velocity),
+                       color_bend=jnp.zeros(sc.N), debug_vector=jnp.zeros((sc.N, 2)))
+    edges = R["Edges"](pairs=jnp.array(sc.pairs), theta=jnp.array(sc.theta),
+                       rest_lengths=jnp.array(sc.rest_lengths),
+                       bending_pairs=jnp.array(sc.bending_pairs),
+                       bending_rest_angles=jnp.array(sc.bending_rest_angles),
+                       bending_stiffness=jnp.array(sc.bending_stiffness))
+    fields = R["Fields"](grid_shape=(sc.H, sc.W), steric=jnp.array(sc.steric),
+                         fluid_velocity=jnp.array(sc.fluid_velocity), f_grid=jnp.array(sc.f_grid))
+    return nodes, edges, fields
+
+
+def save(name, **arrs):
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **arrs)
+    print("wrote", path, sum(v.nbytes for v in arrs.values()), "bytes")
+
+
+def main(ref_root):
+    R = load_reference(ref_root)
+    from microcosmos_b200 import scenarios as S
+    U = R["utils"]
+    jnp = sys.modules["jax"].numpy
+    rng = np.random.default_rng(1234)
+
+    # ---- utils: displacement, periodic_boundary, gaussian_filter (utils.py:18-49)
+    for (H, W) in [(16, 16), (12, 20)]:
+        x = rng.uniform(-30, 50, size=(64, 2)).astype(np.float32)
+        y = rng.uniform(-30, 50, size=(64, 2)).astype(np.float32)
+        data = rng.uniform(0, 1, size=(H, W)).astype(np.float32)
+        save(f"utils_{H}x{W}", H=np.int32(H), W=np.int32(W), x=x, y=y, data=data,
+             sigma=np.float32(1.5),
+             displacement=A(U.displacement((H, W), jnp.array(x), jnp.array(y))),
+             periodic_boundary=A(U.periodic_boundary((H, W), jnp.array(x))),
+             gaussian_filter=A(U.gaussian_filter(jnp.array(data), sigma=1.5)))
+
+    cfg_mod = R["config"]
+
+    # ---- steric: deposit + filter + corrected force (forces.py:41-118)
+    for (H, W, F, n, seed) in [(20, 28, 3, 9, 5), (32, 32, 2, 14, 6)]:
+        sc = S.make_scenario(H, W, F, n, seed=seed, amp=0.2)
+        nodes, edges, fields = to_ref(R, sc)
+        pred = jnp.array(sc.position + rng.normal(0, 0.3, size=sc.position.shape).astype(np.float32)
+                         + np.float32(W) * (rng.uniform(size=sc.position.shape) < 0.1))
+        nodes = nodes.__replace__(position=pred)
+        fields2, f_st = R["forces"].compute_field_steric_force_corrected(
+            nodes, fields, sigma=1.5, neighbor_skip=5, scatter_value=1.0)
+        save(f"steric_{H}x{W}", H=np.int32(H), W=np.int32(W), position=A(pred), sigma=np.float32(1.5),
+             neighbor_skip=np.int32(5), scatter_value=np.float32(1.0),
+             steric=A(fields2.steric), force=A(f_st))
+
+    # ---- PBD: one iteration and a 20-iteration fori_loop (solver/pbd.py:14-91)
+    for (H, W, F, n, seed) in [(20, 28, 3, 9, 7), (64, 64, 2, 24, 8)]:
+        sc = S.make_scenario(H, W, F, n, seed=seed, amp=0.3)
+        nodes, edges, fields = to_ref(R, sc)
+        pos = jnp.array(sc.position + rng.normal(0, 0.2, size=sc.position.shape).astype(np.float32))
+        th = jnp.array(sc.theta + rng.normal(0, 0.3, size=sc.theta.shape).astype(np.float32))
+        nodes = nodes.__replace__(position=pos)
+        edges = edges.__replace__(theta=th)
+        cfg = baseline_config(cfg_mod)
+        n1, e1 = R["pbd"].pbd_rod_constraint(0, (nodes, edges), cfg, (H, W))
+        carry = (nodes, edges)
+        for i in range(cfg.cycles_per_step):
+            carry = R["pbd"].pbd_rod_constraint(i, carry, cfg, (H, W))
+        n20, e20 = carry
+        save(f"pbd_{H}x{W}", H=np.int32(H), W=np.int32(W), **cfg_arrays(cfg),
+             **state_arrays("in_", nodes, edges, None),
+             pos_1=A(n1.position), theta_1=A(e1.theta), pos_20=A(n20.position), theta_20=A(e20.theta))
+
+    # ---- IB + LBM: immersed_boundary_interaction (solver/fluid.py:202-386)
+    for (H, W, F, n, ks, seed, ustd) in [(24, 24, 2, 10, 4, 9, 1e-3), (24, 24, 2, 10, 2, 10, 1e-3),
+                                         (20, 28, 2, 8, 4, 11, 1e-3), (16, 16, 1, 10, 4, 12, 0.15)]:
+        sc = S.make_scenario(H, W, F, n, seed=seed, u0_std=ustd)
+        nodes, edges, fields = to_ref(R, sc)
+        vel = jnp.array(rng.normal(0, 5.0, size=sc.position.shape).astype(np.float32))
+        nodes = nodes.__replace__(velocity=vel)
+        cfg = baseline_config(cfg_mod, ibm_kernel_size=ks)
+        dt = 0.01
+        n2, f2, fnew = R["fluid"].immersed_boundary_interaction(nodes, edges, fields, fields.f_grid, dt, cfg)
+        save(f"ib_{H}x{W}_k{ks}" + ("_clamp" if ustd > 0.01 else ""), H=np.int32(H), W=np.int32(W),
+             dt=np.float32(dt), **cfg_arrays(cfg), **state_arrays("in_", nodes, edges, fields),
+             velocity_out=A(n2.velocity), fluid_velocity_out=A(f2.fluid_velocity), f_grid_out=A(fnew))
+
+    # ---- full step / simulate (simulate.py:15-100)
+    for (H, W, F, n, seed, steps, name) in [(24, 32, 2, 10, 13, 6, "sim_24x32"),
+                                            (32, 32, 3, 12, 14, 6, "sim_32x32")]:
+        sc = S.make_scenario(H, W, F, n, seed=seed, amp=0.2, period=20.0)
+        nodes, edges, fields = to_ref(R, sc)
+        cfg = baseline_config(cfg_mod)
+        dt = 0.01
+        # a) simulate() with fixed rest angles: reference-shaped timeseries
+        nts, fts = R["simulate"].simulate(nodes, edges, fields, dt, steps, cfg)
+        # b) step() loop with the caller-side curvature actuation
+        nd, ed, fd = nodes, edges, fields
+        traj = []
+        for t in range(steps):
+            ed = ed.__replace__(bending_rest_angles=jnp.array(S.actuation_rest_angles(sc, t)))
+            nd, ed, fd = R["simulate"].step(nd, ed, fd, dt, cfg)
+            traj.append(A(nd.position))
+        save(name, H=np.int32(H), W=np.int32(W), dt=np.float32(dt), steps=np.int32(steps),
+             **cfg_arrays(cfg), **state_arrays("in_", nodes, edges, fields),
+             act_c=sc.act_c, act_amp=sc.act_amp, act_omega=sc.act_omega, act_phase=sc.act_phase,
+             ts_position=A(nts.position), ts_velocity=A(nts.velocity), ts_steric=A(fts.steric),
+             ts_fluid_velocity=A(fts.fluid_velocity),
+             act_position=np.stack(traj), act_velocity=A(nd.velocity), act_theta=A(ed.theta),
+             act_f_grid=A(fd.f_grid), act_steric=A(fd.steric), act_fluid_velocity=A(fd.fluid_velocity))
+
+    # ---- the reference test scenario: closed loop of 10 nodes (tests/conftest.py:9-59),
+    #      PBD_SCHEME defaults (2-point kernel, steric off), one step on a 32x32 grid
+    G = R["graph"]
+    num = 10
+    pairs, dep = G.make_edges(num, graph="loop", num_instances=1)
+    bp, _ = G.compute_bending_pairs(pairs, dep, num)
+    radius = 3.0 / (2.0 * np.sin(np.pi / num))
+    ang = np.linspace(0, 2 * np.pi, num, endpoint=False)
+    pos = (np.array([16.0, 16.0]) + radius * np.stack([np.cos(ang), np.sin(ang)], 1)).astype(np.float32)
+    d = U.displacement((32, 32), jnp.array(pos)[A(pairs)[:, 1]], jnp.array(pos)[A(pairs)[:, 0]])
+    th = np.arctan2(A(d)[:, 1], A(d)[:, 0]).astype(np.float32)
+    sc = S.make_scenario(32, 32, 1, num, seed=15)
+    sc.position = pos
+    sc.velocity = rng.normal(0, 1.0, size=pos.shape).astype(np.float32)
+    sc.pairs = A(pairs)
+    sc.theta = th
+    sc.rest_lengths = np.full(num, 3.0, np.float32)
+    sc.bending_pairs = A(bp)
+    sc.bending_rest_angles = np.full(bp.shape[0], 2 * np.pi / num, np.float32)
+    sc.bending_stiffness = np.full(bp.shape[0], 0.5, np.float32)
+    nodes, edges, fields = to_ref(R, sc)
+    cfg = cfg_mod.PBD_SCHEME
+    nd, ed, fd = R["simulate"].step(nodes, edges, fields, 0.01, cfg)
+    nd2, ed2, fd2 = R["simulate"].step(nd, ed, fd, 0.01, cfg)
+    save("loop_32x32", H=np.int32(32), W=np.int32(32), dt=np.float32(0.01), **cfg_arrays(cfg),
+         **state_arrays("in_", nodes, edges, fields), **state_arrays("out_", nd2, ed2, fd2))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
