@@ -1,0 +1,164 @@
+/*
+ * microcosmos_b200 — C ABI of the B200 (sm_100a) physics hot path of microcosmos.
+ *
+ * One rollout = the reference's `simulate(nodes, edges, fields, dt, num_steps,
+ * solver_config)` (src/microcosmos/simulate.py:15-35) with the PBD constraint plugin
+ * (src/microcosmos/solver/pbd.py:14-91), the IB + D2Q9 TRT lattice-Boltzmann fluid
+ * (src/microcosmos/solver/fluid.py:202-386) and the FFT steric field
+ * (src/microcosmos/forces.py:41-118).  A batch is a set of rollouts of any sizes that
+ * step together; the single-instance path is a batch of one.
+ *
+ * Conventions
+ *   - All array arguments of mc_state / mc_actuation / mc_record are DEVICE pointers
+ *     (float32 or int32, C-contiguous, the reference's layouts: positions (N,2) as
+ *     (x, y), f_grid (9,H,W), fluid_velocity (2,H,W), steric (H,W)).  Topology
+ *     (pairs, bending_pairs) is passed as HOST arrays at plan creation.
+ *   - The library never allocates device memory: the caller provides one workspace of
+ *     mc_plan_workspace_bytes() bytes (256-byte aligned).  Host memory for the plan
+ *     object itself is allocated by mc_plan_create and released by mc_plan_destroy.
+ *   - Work is stream-ordered on the caller's stream; calls return after enqueueing.
+ *     A plan is not thread-safe; distinct plans are independent.
+ *   - Errors are returned as mc_status; nothing aborts, traps or exits.
+ *     Numerical faults (non-finite node state) are recorded per rollout on the device
+ *     and read back with mc_plan_read_flags().
+ */
+#ifndef MICROCOSMOS_B200_H
+#define MICROCOSMOS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum mc_status {
+  MC_OK = 0,
+  MC_ERR_INVALID = 1,      /* bad argument: shape, index out of range, null pointer */
+  MC_ERR_CUDA = 2,         /* a CUDA runtime call failed (mc_last_error() has the text) */
+  MC_ERR_WORKSPACE = 3,    /* workspace missing, too small or misaligned */
+  MC_ERR_UNSUPPORTED = 4,  /* configuration outside what the kernels implement */
+  MC_ERR_NOT_BOUND = 5     /* plan used before mc_plan_bind() */
+} mc_status;
+
+/* Per-rollout flag bits reported by mc_plan_read_flags(). */
+#define MC_FLAG_NONFINITE 1u /* a node position/velocity became NaN/Inf */
+
+/* Scalar fields of ConstraintSolverConfig used by the PBD scheme
+ * (src/microcosmos/solver/config.py:9-72).  The callable `bending_constraint` is fixed
+ * to pbd_rod_constraint; `cycles_per_constraint` is never read by the reference. */
+typedef struct mc_config {
+  int32_t cycles_per_step;
+  float stiffness_stretch;
+  float stiffness_shear;
+  float damping;
+  int32_t enable_fluid;
+  float viscosity;
+  float max_fluid_velocity;
+  int32_t ibm_iterations;
+  float synthetic_node_width; /* must be 0 (the reference default) */
+  int32_t ibm_kernel_size;    /* 1..8 */
+  float ibm_relaxation;
+  float node_mass;
+  float lambda_trt;
+  int32_t enable_force_clamp;
+  int32_t enable_steric;
+  float steric_strength;
+  float steric_sigma;
+  int32_t steric_neighbor_skip;
+  float steric_scatter_value;
+} mc_config;
+
+/* Sizes of one rollout.  H, W: grid_shape (the fluid grid equals the domain grid). */
+typedef struct mc_dims {
+  int32_t H, W;
+  int32_t N; /* nodes */
+  int32_t E; /* edges (pairs) */
+  int32_t B; /* bending pairs */
+} mc_dims;
+
+/* Device state of one rollout (Nodes / Edges / Fields of src/microcosmos/structs/*.py).
+ * Read at the start of a rollout call and written back at its end. */
+typedef struct mc_state {
+  float* position;            /* (N,2) in/out */
+  float* velocity;            /* (N,2) in/out */
+  float* theta;               /* (E,)  in/out */
+  const float* rest_lengths;  /* (E,)  in */
+  float* bending_rest_angles; /* (B,)  in/out (overwritten by the actuation, if any) */
+  const float* bending_stiffness; /* (B,) in */
+  float* steric;              /* (H,W) in/out */
+  float* fluid_velocity;      /* (2,H,W) in/out (u* of the last step) */
+  float* f_grid;              /* (9,H,W) in/out */
+} mc_state;
+
+/* Optional caller-side curvature actuation, evaluated on the device before every step:
+ *   rest[b](t) = c[b] + amp[b] * sin(omega[b] * t + phase[b]),  t = t0 + step index.
+ * Replaces the reference's control_fn that rewrites edges.bending_rest_angles before
+ * each step (experiments/swim_sweep/swimmers/worm.py:60-74). All arrays (B,), device. */
+typedef struct mc_actuation {
+  const float* c;
+  const float* amp;
+  const float* omega;
+  const float* phase;
+  int32_t t0;
+} mc_actuation;
+
+/* Optional per-step recording, the reference's scan outputs (simulate.py:21-34).
+ * Entry k (0-based) is written after step (k+1)*every - 1.  Any pointer may be NULL. */
+typedef struct mc_record {
+  float* position;       /* (T,N,2) */
+  float* velocity;       /* (T,N,2) */
+  float* steric;         /* (T,H,W) */
+  float* fluid_velocity; /* (T,2,H,W) */
+  int32_t every;         /* >= 1 */
+} mc_record;
+
+typedef struct mc_plan mc_plan;
+
+/* Build a plan for `n` rollouts.  dims/cfg/dt/pairs/bending_pairs are arrays of length
+ * n; pairs[r] is (E_r,2) and bending_pairs[r] is (B_r,2) int32 HOST memory.  The
+ * topology is validated (indices in range) and turned into gather lists that keep the
+ * reference's scatter-add order.  Replaces the jit-static arguments of
+ * simulate()/step() (src/microcosmos/simulate.py:15,37). */
+mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, const float* dt,
+                         const int32_t* const* pairs, const int32_t* const* bending_pairs,
+                         mc_plan** out);
+void mc_plan_destroy(mc_plan* plan);
+
+/* Bytes of device workspace the plan needs (all rollouts). */
+size_t mc_plan_workspace_bytes(const mc_plan* plan);
+
+/* Attach a caller-allocated device workspace and upload the plan's tables on `stream`. */
+mc_status mc_plan_bind(mc_plan* plan, void* workspace, size_t bytes, void* stream);
+
+/* Run `num_steps` steps of every rollout of the plan: the device-side equivalent of
+ * simulate() (src/microcosmos/simulate.py:15-35) / repeated step() (:37-100).
+ * states[r], act[r] (NULL = none), rec[r] (NULL = none) per rollout; act and rec may
+ * themselves be NULL.  use_graph != 0 captures the per-step launch sequence in a CUDA
+ * graph on first use and replays it. */
+mc_status mc_rollout(mc_plan* plan, const mc_state* states, int32_t num_steps,
+                     const mc_actuation* const* act, const mc_record* const* rec,
+                     int32_t use_graph, void* stream);
+
+/* One step: mc_rollout with num_steps = 1 (src/microcosmos/simulate.py:37-100). */
+mc_status mc_step(mc_plan* plan, const mc_state* states, void* stream);
+
+/* Copy the per-rollout MC_FLAG_* words to host `flags` (n entries); synchronises
+ * `stream`.  clear != 0 resets them afterwards. */
+mc_status mc_plan_read_flags(mc_plan* plan, uint32_t* flags, int32_t clear, void* stream);
+
+/* Number of kernel launches the last mc_rollout() enqueued (graph replays count the
+ * kernels inside the graph). */
+int64_t mc_plan_last_launch_count(const mc_plan* plan);
+
+/* Text of the last error of this thread ("" if none). */
+const char* mc_last_error(void);
+
+/* Library version string. */
+const char* mc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MICROCOSMOS_B200_H */

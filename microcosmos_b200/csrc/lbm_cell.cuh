@@ -1,0 +1,120 @@
+// Per-cell D2Q9 TRT + Guo arithmetic shared by the dense pass and the IB pre-pass.
+// Operation order follows src/microcosmos/solver/fluid.py (compiled with -fmad=false so
+// every product and sum is rounded as in the reference's float32 elementwise ops).
+#pragma once
+#include "mc_internal.cuh"
+
+namespace mc {
+
+// D2Q9 velocities and weights (src/microcosmos/solver/fluid.py:15-23)
+__device__ __constant__ static const int kEx[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+__device__ __constant__ static const int kEy[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+
+// jnp.maximum / jnp.minimum propagate NaN from the array operand; fmaxf/fminf do not.
+__device__ __forceinline__ float max_prop(float v, float c) { return (v < c) ? c : v; }
+__device__ __forceinline__ float min_prop(float c, float v) { return (v > c) ? c : v; }
+
+// min(1, vmax / (sqrt(x^2 + y^2 + EPSIL) + EPSIL))  (fluid.py:272-273, 300-301, 327-328)
+__device__ __forceinline__ float clamp_factor(float x, float y, float vmax) {
+  float mag = sqrtf((x * x + y * y) + MC_EPSIL);
+  return min_prop(1.0f, vmax / (mag + MC_EPSIL));
+}
+
+// f = max(f, EPSIL); rho = max(sum f, 0.1); u = sum e f / rho; velocity clamp
+// (fluid.py:136-142, 268-274).  Returns rho and the clamped velocity.
+__device__ __forceinline__ void macroscopic(float f[9], float vmax, float& rho, float& vx, float& vy) {
+#pragma unroll
+  for (int i = 0; i < 9; ++i) f[i] = max_prop(f[i], MC_EPSIL);
+  float r = f[0];
+#pragma unroll
+  for (int i = 1; i < 9; ++i) r = r + f[i];
+  r = max_prop(r, 0.1f);
+  float ux = ((((f[1] - f[3]) + f[5]) - f[6]) - f[7]) + f[8];
+  float uy = ((((f[2] - f[4]) + f[5]) + f[6]) - f[7]) - f[8];
+  ux = ux / r;
+  uy = uy / r;
+  float c1 = clamp_factor(ux, uy, vmax);
+  rho = r;
+  vx = ux * c1;
+  vy = uy * c1;
+}
+
+// Force of a cell that no IB point touches: the post-accumulation clamp applied to the
+// unchanged velocity (fluid.py:327-339).
+__device__ __forceinline__ void free_cell_force(float rho, float vx, float vy, float vmax, int force_clamp,
+                                                float& Fx, float& Fy) {
+  float c2 = clamp_factor(vx, vy, vmax);
+  Fx = (vx * c2 - vx) * rho;
+  Fy = (vy * c2 - vy) * rho;
+  if (force_clamp) {
+    float c3 = clamp_factor(Fx, Fy, vmax);
+    Fx = Fx * c3;
+    Fy = Fy * c3;
+  }
+}
+
+// TRT collision at u* = u + F/(2 rho) with the TRT-aware Guo source and the EPSIL floor
+// (fluid.py:145-199, 342-350).  f holds the clamped populations.  cp = 1 - wp/2 and
+// cm = 1 - wm/2 are computed on the host in float32.
+__device__ __forceinline__ void collide(const float f[9], float rho, float vx, float vy, float Fx, float Fy,
+                                        float wp, float wm, float cp, float cm, float out[9],
+                                        float& usx_o, float& usy_o) {
+  const float half = 0.5f;
+  float usx = vx + (half * Fx) / rho;
+  float usy = vy + (half * Fy) / rho;
+  float usq = usx * usx + usy * usy;
+  float eu[9];
+  eu[0] = 0.0f;
+  eu[1] = usx;
+  eu[2] = usy;
+  eu[3] = -usx;
+  eu[4] = -usy;
+  eu[5] = usx + usy;
+  eu[6] = -usx + usy;
+  eu[7] = -usx - usy;
+  eu[8] = usx - usy;
+  const float w[9] = {4.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f,
+                      1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f};
+  float feq[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i)
+    feq[i] = (rho * w[i]) * (((1.0f + 3.0f * eu[i]) + 4.5f * (eu[i] * eu[i])) - 1.5f * usq);
+  const int opp[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+  if (Fx == 0.0f && Fy == 0.0f) {
+    // zero force: the Guo source is exactly zero and u* = u
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      int o = opp[i];
+      float post = (f[i] - wp * (half * (f[i] + f[o]) - half * (feq[i] + feq[o])))
+                   - wm * (half * (f[i] - f[o]) - half * (feq[i] - feq[o]));
+      out[i] = max_prop(post, MC_EPSIL);
+    }
+  } else {
+    float eF[9];
+    eF[0] = 0.0f;
+    eF[1] = Fx;
+    eF[2] = Fy;
+    eF[3] = -Fx;
+    eF[4] = -Fy;
+    eF[5] = Fx + Fy;
+    eF[6] = -Fx + Fy;
+    eF[7] = -Fx - Fy;
+    eF[8] = Fx - Fy;
+    float udF = usx * Fx + usy * Fy;
+    float raw[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) raw[i] = w[i] * (3.0f * (eF[i] - udF) + (9.0f * eu[i]) * eF[i]);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      int o = opp[i];
+      float post = (f[i] - wp * (half * (f[i] + f[o]) - half * (feq[i] + feq[o])))
+                   - wm * (half * (f[i] - f[o]) - half * (feq[i] - feq[o]));
+      float src = cp * (half * (raw[i] + raw[o])) + cm * (half * (raw[i] - raw[o]));
+      out[i] = max_prop(post + src, MC_EPSIL);
+    }
+  }
+  usx_o = usx;
+  usy_o = usy;
+}
+
+}  // namespace mc

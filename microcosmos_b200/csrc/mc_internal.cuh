@@ -1,0 +1,191 @@
+// Internal declarations shared by the kernels and the host runtime.
+//
+// Every kernel takes the plan's rollout descriptor table (RDesc[n], device memory)
+// and a per-kernel CTA offset table cta_off[n+1]: CTA b works for rollout
+// r = max{r : cta_off[r] <= b} on its local block b - cta_off[r].  A single
+// rollout is the batch of one, so the plain and batched paths share every kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define MC_EPSIL 1.1920928955078125e-07f  // float32 eps (src/microcosmos/utils.py:9)
+#define MC_PI_F 3.14159265358979323846f
+#define MC_2PI_F 6.28318530717958647692f
+
+namespace mc {
+
+constexpr int kBinTile = 16;       // binning tile edge for the deterministic reductions
+constexpr int kLbmTileX = 128;     // dense LBM CTA tile: 32 lanes x 4 cells
+constexpr int kLbmTileY = 8;       //                    8 rows
+constexpr int kSortCap = 4096;     // keys sorted in shared memory per pass
+constexpr int kFftMaxN = 4096;     // largest FFT length (shared memory)
+constexpr int kFftMaxFactors = 16;
+constexpr int kFftColsPerCta = 4;  // complex columns per column-pass CTA (8 real columns)
+
+// Per-rollout descriptor.  All pointers are device pointers.
+struct RDesc {
+  // sizes
+  int H, W, N, E, B, K;  // K = ibm_kernel_size
+  int ncomp;             // rod components
+  int M;                 // IB contributions = N*K*K
+  int ntile_x, ntile_y;  // binning tiles (kBinTile)
+  int lbm_tx, lbm_ty;    // LBM tiles
+  int lbm_tw;            // LBM tile width in cells (32 * cells per lane)
+  int max_comp_nodes, max_comp_edges, max_comp_pairs;
+  // configuration
+  float dt, damping, k_stretch, k_shear, vmax, relax, node_mass, wp, wm;
+  float st_strength, st_sigma, st_scatter;
+  float st_2s2, st_norm, st_coef;  // 2 sigma^2, 2 pi sigma^2, scatter / sigma^2 (float32 of the double values)
+  int st_skip, ib_iters, cycles, enable_fluid, enable_steric, force_clamp;
+  float scale_x, scale_y;   // fluid grid / domain grid, reference axis order
+  float sdt_x, sdt_y;       // scale * dt (float32)
+  // FFT plans (steric filter)
+  int fftW_nf, fftH_nf;
+  int fftW_f[kFftMaxFactors], fftH_f[kFftMaxFactors];
+  const float2* twW;  // W roots exp(-2 pi i k / W)
+  const float2* twH;
+  const float* gW;    // separable spectral Gaussian / W
+  const float* gH;    // ... / H
+  // state (caller buffers)
+  float* pos;
+  float* vel;
+  float* theta;
+  const float* rest_len;
+  float* rest_ang;
+  const float* kb;
+  float* steric;
+  float* fluid_vel;
+  float* f_grid;
+  // actuation
+  const float* act_c;
+  const float* act_amp;
+  const float* act_omega;
+  const float* act_phase;
+  int act_t0;
+  // recording
+  float* rec_pos;
+  float* rec_vel;
+  float* rec_steric;
+  float* rec_fluid;
+  int rec_every;
+  // topology (workspace)
+  const int* pairs;    // (E,2)
+  const int* bpairs;   // (B,2)
+  const int* comp_n;   // (ncomp+1) node offsets
+  const int* comp_e;   // (ncomp+1) edge offsets
+  const int* comp_b;   // (ncomp+1) pair offsets
+  const int* ep_off;   // (E+1) edge -> bending pairs, (pair<<1)|neg
+  const int* ep_idx;
+  const int* ne_off;   // (N+1) node -> edges, (edge<<1)|neg
+  const int* ne_idx;
+  const float* edeg;   // (E,) max(bending degree, 1)
+  const float* ndeg;   // (N,) max(node degree, 1)
+  // workspace
+  float* h[2];         // pull-scheme post-collision populations (9,H,W)
+  float* fov;          // (2,H,W) force overlay, NaN = no IB force at the cell
+  int* lbm_flag;       // (lbm_ty*lbm_tx) tile has overlay entries
+  float* dep;          // (H,W) CIC deposit (kept zero between steps)
+  float* tmp;          // (H,W) FFT row-pass output
+  float* prev;         // (N,2)
+  float* pred;         // (N,2)
+  float* nvl;          // (N,2) node velocity in lattice units
+  float* delta;        // (N,2) IB per-iteration correction
+  // IB contributions (M = N*K*K), then per-slot arrays indexed by sorted position
+  int* ib_cell;
+  float* ib_w;
+  int* ib_binned;
+  int* ib_sorted;
+  int* ib_slot;     // contribution -> slot (sorted position of its cell's first entry)
+  int* s_cell;      // slot -> cell (heads only)
+  int* s_len;       // slot -> run length (0 for non-heads)
+  float* s_rho;
+  float* s_vx;
+  float* s_vy;
+  float* s_inv;
+  float* s_ucx;
+  float* s_ucy;
+  float* s_fx;
+  float* s_fy;
+  int* ib_tcount;   // (ntiles) contributions per binning tile
+  int* ib_tfill;
+  int* ib_toff;     // (ntiles+1)
+  // CIC deposit contributions (4N)
+  int* c_cell;
+  float* c_w;
+  int* c_binned;
+  int* c_sorted;
+  int* c_tcount;
+  int* c_tfill;
+  int* c_toff;
+  unsigned* flags;  // MC_FLAG_* for this rollout
+};
+
+struct Batch {
+  const RDesc* d;  // device descriptor table
+  int n;
+};
+
+__device__ __forceinline__ int find_rollout(const int* __restrict__ off, int n, int b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(off + mid) <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Floored float modulo, the semantics of jnp.mod / numpy.mod for floats.
+__device__ __forceinline__ float fmod_floor(float x, float y) {
+  float r = fmodf(x, y);
+  if (r != 0.0f && ((r < 0.0f) != (y < 0.0f))) r += y;
+  return r;
+}
+
+__device__ __forceinline__ int imod_floor(int x, int m) {
+  int r = x % m;
+  return r < 0 ? r + m : r;
+}
+
+// utils.displacement for one (x, y) pair, size (H, W) flipped to (W, H)
+// (src/microcosmos/utils.py:18-23): mod(a - b + L/2, L) - L/2.
+__device__ __forceinline__ float2 min_image(float ax, float ay, float bx, float by, float W, float H) {
+  float hx = W / 2.0f, hy = H / 2.0f;
+  return make_float2(fmod_floor((ax - bx) + hx, W) - hx, fmod_floor((ay - by) + hy, H) - hy);
+}
+
+__device__ __forceinline__ float nan_f() { return __int_as_float(0x7fffffff); }
+__device__ __forceinline__ bool is_sentinel(float v) { return __float_as_int(v) == 0x7fffffff; }
+
+// ------------------------------------------------------------------ launch helpers
+// (host) kernels launched by the runtime; each takes the descriptor table, the CTA
+// offset table for its kind, and the number of rollouts.
+struct Launch {
+  const RDesc* d;
+  const int* off;
+  int n;
+  int grid;
+  cudaStream_t s;
+};
+
+void launch_predict(const Launch& L);
+void launch_bin_scan(const Launch& L, int which);
+void launch_bin_scatter(const Launch& L, int which);
+void launch_bin_sort(const Launch& L, int which, int parity);
+void launch_fft_rows(const Launch& L, size_t smem);
+void launch_fft_cols(const Launch& L, size_t smem);
+void launch_node(const Launch& L, const int* tdev, size_t smem, int bs);
+void launch_ib_interp(const Launch& L, int it);
+void launch_ib_spread(const Launch& L, int it);
+void launch_ib_finalize(const Launch& L);
+void launch_lbm(const Launch& L, int parity, int write_u, int vec);
+void launch_reaction(const Launch& L, const int* tdev);
+void launch_record_fields(const Launch& L, const int* tdev);
+void launch_unstream(const Launch& L);
+void launch_stream_out(const Launch& L, int parity);
+void launch_clear_ws(const Launch& L);
+void launch_tick(int* tdev, cudaStream_t s);
+cudaError_t fft_set_smem(size_t rows, size_t cols);
+cudaError_t node_set_smem(size_t bytes);
+
+}  // namespace mc

@@ -1,0 +1,264 @@
+// Node-side kernels of one step (src/microcosmos/simulate.py:37-84):
+//   k_predict: damping, inertial prediction, steric cloud-in-cell contributions;
+//   k_node:    per rod component (one CTA, state in shared memory): steric force
+//              (forces.py:41-81), curvature actuation, cycles_per_step Jacobi iterations
+//              of pbd_rod_constraint (solver/pbd.py:14-91), velocity from positions, and
+//              the IB stencil of every node (solver/fluid.py:40-87).
+#include "lbm_cell.cuh"
+
+namespace mc {
+
+__device__ __forceinline__ int bin_tile(const RDesc& d, int cy, int cx) {
+  return (cy / kBinTile) * d.ntile_x + cx / kBinTile;
+}
+
+__global__ void __launch_bounds__(256) k_predict(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int node = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
+  if (node >= d.N) return;
+  const float px = d.pos[2 * node], py = d.pos[2 * node + 1];
+  const float vx = d.vel[2 * node] * d.damping, vy = d.vel[2 * node + 1] * d.damping;
+  d.prev[2 * node] = px;
+  d.prev[2 * node + 1] = py;
+  d.vel[2 * node] = vx;
+  d.vel[2 * node + 1] = vy;
+  const float qx = px + vx * d.dt, qy = py + vy * d.dt;
+  d.pred[2 * node] = qx;
+  d.pred[2 * node + 1] = qy;
+  if (!d.enable_steric) return;
+  // update_steric_potential (forces.py:84-115): CIC weights of the wrapped prediction
+  const float W = (float)d.W, H = (float)d.H;
+  const float x = fmod_floor(qx, W), y = fmod_floor(qy, H);
+  const float fx = floorf(x), fy = floorf(y);
+  const int x0 = imod_floor((int)fx, d.W), y0 = imod_floor((int)fy, d.H);
+  const int x1 = (x0 + 1) % d.W, y1 = (y0 + 1) % d.H;
+  const float dx = x - fx, dy = y - fy;
+  const float s = d.st_scatter;
+  const float w[4] = {((1.0f - dx) * (1.0f - dy)) * s, (dx * (1.0f - dy)) * s, ((1.0f - dx) * dy) * s, (dx * dy) * s};
+  const int cy[4] = {y0, y0, y1, y1};
+  const int cx[4] = {x0, x1, x0, x1};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int k = c * d.N + node;
+    d.c_cell[k] = cy[c] * d.W + cx[c];
+    d.c_w[k] = w[c];
+    atomicAdd(d.c_tcount + bin_tile(d, cy[c], cx[c]), 1);
+  }
+}
+
+// map_coordinates(V, [yy, xx], order=1, mode="wrap") (forces.py:30-34)
+__device__ __forceinline__ float sample_wrap(const float* __restrict__ V, int H, int W, float yy, float xx) {
+  const float ly = floorf(yy), lx = floorf(xx);
+  const float ty = yy - ly, tx = xx - lx;
+  const float wy0 = 1.0f - ty, wx0 = 1.0f - tx;
+  const int iy = (int)ly, ix = (int)lx;
+  const int iy0 = imod_floor(iy, H), iy1 = imod_floor(iy + 1, H);
+  const int ix0 = imod_floor(ix, W), ix1 = imod_floor(ix + 1, W);
+  float acc = (wy0 * wx0) * V[(size_t)iy0 * W + ix0];
+  acc = acc + (wy0 * tx) * V[(size_t)iy0 * W + ix1];
+  acc = acc + (ty * wx0) * V[(size_t)iy1 * W + ix0];
+  acc = acc + (ty * tx) * V[(size_t)iy1 * W + ix1];
+  return acc;
+}
+
+// compute_field_steric_force_corrected for node gi (forces.py:41-81): -grad V by central
+// differences of bilinear samples, minus the analytic Gaussian of global neighbours
+// gi-n..gi+n (the 0 <= j < N mask only, as in the reference).
+__device__ float2 steric_force(const RDesc& d, int gi) {
+  const float W = (float)d.W, H = (float)d.H;
+  const float px = fmod_floor(d.pred[2 * gi], W), py = fmod_floor(d.pred[2 * gi + 1], H);
+  const float* V = d.steric;
+  const float gx = (sample_wrap(V, d.H, d.W, py, px + 0.5f) - sample_wrap(V, d.H, d.W, py, px - 0.5f)) / 1.0f;
+  const float gy = (sample_wrap(V, d.H, d.W, py + 0.5f, px) - sample_wrap(V, d.H, d.W, py - 0.5f, px)) / 1.0f;
+  float fx = -gx, fy = -gy;
+  const int nsk = d.st_skip;
+  if (nsk > 0) {
+    float ax = 0.0f, ay = 0.0f;
+    for (int o = -nsk; o <= nsk; ++o) {
+      const int j = gi + o;
+      const float valid = (j >= 0 && j < d.N) ? 1.0f : 0.0f;
+      const int js = j < 0 ? 0 : (j >= d.N ? d.N - 1 : j);
+      const float qx = fmod_floor(d.pred[2 * js], W), qy = fmod_floor(d.pred[2 * js + 1], H);
+      const float2 rr = min_image(px, py, qx, qy, W, H);
+      const float d2 = rr.x * rr.x + rr.y * rr.y;
+      const float K = expf(-d2 / d.st_2s2) / d.st_norm;
+      const float kv = K * valid;
+      ax = ax + kv * rr.x;
+      ay = ay + kv * rr.y;
+    }
+    fx = fx - d.st_coef * ax;
+    fy = fy - d.st_coef * ay;
+  }
+  return make_float2(fx, fy);
+}
+
+__global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
+                       const int* __restrict__ tdev) {
+  extern __shared__ float sm[];
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int comp = blockIdx.x - off[r];
+  const int n0 = d.comp_n[comp], nn = d.comp_n[comp + 1] - n0;
+  const int e0 = d.comp_e[comp], ne = d.comp_e[comp + 1] - e0;
+  const int b0 = d.comp_b[comp], nb = d.comp_b[comp + 1] - b0;
+  float* px = sm;
+  float* py = px + d.max_comp_nodes;
+  float* th = py + d.max_comp_nodes;
+  float* l0 = th + d.max_comp_edges;
+  float* fx = l0 + d.max_comp_edges;
+  float* fy = fx + d.max_comp_edges;
+  float* corr = fy + d.max_comp_edges;
+  float* ra = corr + d.max_comp_pairs;
+  float* kb = ra + d.max_comp_pairs;
+  const int tid = threadIdx.x, bd = blockDim.x;
+  const int t = *tdev;
+
+  // actuation (caller-side control of bending_rest_angles) and per-pair constants
+  for (int b = tid; b < nb; b += bd) {
+    const int gb = b0 + b;
+    float a;
+    if (d.act_amp) {
+      const float arg = d.act_omega[gb] * (float)(d.act_t0 + t) + d.act_phase[gb];
+      a = d.act_c[gb] + d.act_amp[gb] * sinf(arg);
+      d.rest_ang[gb] = a;
+    } else {
+      a = d.rest_ang[gb];
+    }
+    ra[b] = a;
+    kb[b] = d.kb[gb];
+  }
+  for (int e = tid; e < ne; e += bd) {
+    th[e] = d.theta[e0 + e];
+    l0[e] = d.rest_len[e0 + e];
+  }
+  // steric displacement of the prediction (simulate.py:55-63)
+  for (int i = tid; i < nn; i += bd) {
+    const int gi = n0 + i;
+    float qx = d.pred[2 * gi], qy = d.pred[2 * gi + 1];
+    if (d.enable_steric) {
+      const float2 f = steric_force(d, gi);
+      qx = qx + (f.x * d.st_strength) * d.dt;
+      qy = qy + (f.y * d.st_strength) * d.dt;
+    }
+    px[i] = qx;
+    py[i] = qy;
+  }
+  __syncthreads();
+
+  const float W = (float)d.W, H = (float)d.H;
+  for (int it = 0; it < d.cycles; ++it) {
+    // theta pass over bending pairs (pbd.py:23-49)
+    for (int b = tid; b < nb; b += bd) {
+      const int ein = d.bpairs[2 * (b0 + b)] - e0, eout = d.bpairs[2 * (b0 + b) + 1] - e0;
+      float diff = th[eout] - th[ein];
+      diff = fmod_floor(diff + MC_PI_F, MC_2PI_F) - MC_PI_F;
+      corr[b] = ((diff - ra[b]) * kb[b]) * 0.5f;
+    }
+    __syncthreads();
+    for (int e = tid; e < ne; e += bd) {
+      const int ge = e0 + e;
+      float acc = 0.0f;
+      for (int j = d.ep_off[ge]; j < d.ep_off[ge + 1]; ++j) {
+        const int code = d.ep_idx[j];
+        const float c = corr[(code >> 1) - b0];
+        acc = (code & 1) ? acc + (-c) : acc + c;
+      }
+      th[e] = th[e] + (acc / d.edeg[ge]) * 1.8f;
+    }
+    __syncthreads();
+    // position pass over edges (pbd.py:51-89)
+    for (int e = tid; e < ne; e += bd) {
+      const int s = d.pairs[2 * (e0 + e)] - n0, g = d.pairs[2 * (e0 + e) + 1] - n0;
+      const float dirx = cosf(th[e]), diry = sinf(th[e]);
+      const float L0 = l0[e];
+      const float tx = dirx * L0, ty = diry * L0;
+      const float2 cur = min_image(px[g], py[g], px[s], py[s], W, H);
+      const float L = sqrtf(cur.x * cur.x + cur.y * cur.y);
+      const float Lc = max_prop(L, 1e-8f);
+      const float stx = (cur.x / Lc) * (L - L0), sty = (cur.y / Lc) * (L - L0);
+      const float shx = (cur.x - tx) - stx, shy = (cur.y - ty) - sty;
+      fx[e] = ((stx + shx * d.k_shear) * d.k_stretch) * 0.5f;
+      fy[e] = ((sty + shy * d.k_shear) * d.k_stretch) * 0.5f;
+    }
+    __syncthreads();
+    for (int i = tid; i < nn; i += bd) {
+      const int gi = n0 + i;
+      float ax = 0.0f, ay = 0.0f;
+      for (int j = d.ne_off[gi]; j < d.ne_off[gi + 1]; ++j) {
+        const int code = d.ne_idx[j];
+        const int e = (code >> 1) - e0;
+        if (code & 1) {
+          ax = ax + (-fx[e]);
+          ay = ay + (-fy[e]);
+        } else {
+          ax = ax + fx[e];
+          ay = ay + fy[e];
+        }
+      }
+      const float dg = d.ndeg[gi];
+      px[i] = px[i] + ax / dg;
+      py[i] = py[i] + ay / dg;
+    }
+    __syncthreads();
+  }
+
+  for (int e = tid; e < ne; e += bd) d.theta[e0 + e] = th[e];
+  const int K = d.K, K2 = K * K;
+  for (int i = tid; i < nn; i += bd) {
+    const int gi = n0 + i;
+    const float x = px[i], y = py[i];
+    const float vx = (x - d.prev[2 * gi]) / d.dt, vy = (y - d.prev[2 * gi + 1]) / d.dt;
+    d.pos[2 * gi] = x;
+    d.pos[2 * gi + 1] = y;
+    d.vel[2 * gi] = vx;
+    d.vel[2 * gi + 1] = vy;
+    if (d.enable_steric) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) d.dep[d.c_cell[c * d.N + gi]] = 0.0f;
+    }
+    if (d.enable_fluid) {
+      // IB point in lattice units (fluid.py:236-239) and its K x K stencil (fluid.py:40-79)
+      const float gx = x * d.scale_x, gy = y * d.scale_y;
+      d.nvl[2 * gi] = (vx * d.scale_x) * d.dt;
+      d.nvl[2 * gi + 1] = (vy * d.scale_y) * d.dt;
+      const int half = (K - 1) / 2;
+      const float hw = (float)K / 2.0f;
+      const float sx = floorf(gx) - (float)half, sy = floorf(gy) - (float)half;
+      float wx[8], wy[8];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        if (a < K) {
+          const float rx = fabsf((sx + (float)a) - gx) / hw;
+          const float ry = fabsf((sy + (float)a) - gy) / hw;
+          wx[a] = rx <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * rx) / 2.0f)) : 0.0f;
+          wy[a] = ry <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * ry) / 2.0f)) : 0.0f;
+        }
+      }
+      float sum = 0.0f;
+      for (int a = 0; a < K; ++a)
+        for (int b = 0; b < K; ++b) sum = sum + wx[a] * wy[b];
+      const float den = sum + MC_EPSIL;
+      for (int a = 0; a < K; ++a) {
+        const int cx = imod_floor((int)(sx + (float)a), d.W);
+        for (int b = 0; b < K; ++b) {
+          const int cy = imod_floor((int)(sy + (float)b), d.H);
+          const int k = gi * K2 + a * K + b;
+          d.ib_cell[k] = cy * d.W + cx;
+          d.ib_w[k] = (wx[a] * wy[b]) / den;
+          atomicAdd(d.ib_tcount + bin_tile(d, cy, cx), 1);
+        }
+      }
+    }
+  }
+}
+
+void launch_predict(const Launch& L) { k_predict<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
+void launch_node(const Launch& L, const int* tdev, size_t smem, int bs) {
+  k_node<<<L.grid, bs, smem, L.s>>>(L.d, L.off, L.n, tdev);
+}
+cudaError_t node_set_smem(size_t bytes) {
+  return cudaFuncSetAttribute(k_node, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace mc

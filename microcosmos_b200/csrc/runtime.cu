@@ -1,0 +1,767 @@
+// Host runtime behind the C ABI (include/microcosmos_b200.h): plan construction
+// (topology gather lists, FFT tables, workspace layout, CTA offset tables), workspace
+// binding, and the per-step launch sequence with optional CUDA-graph replay.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/microcosmos_b200.h"
+#include "mc_internal.cuh"
+
+using mc::RDesc;
+
+namespace {
+
+thread_local std::string g_err;
+
+mc_status fail(mc_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+
+mc_status cuda_fail(cudaError_t e, const char* where) {
+  g_err = std::string(where) + ": " + cudaGetErrorString(e);
+  return MC_ERR_CUDA;
+}
+
+#define MC_CUDA(call)                                  \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+enum Kind { K_NODES = 0, K_COMP, K_IB, K_CIC, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_COUNT };
+
+struct Region {
+  size_t off = 0;
+  size_t bytes = 0;
+};
+
+struct HostRollout {
+  mc_dims dims{};
+  mc_config cfg{};
+  float dt = 0.f;
+  std::vector<int> pairs, bpairs;
+  std::vector<int> comp_n, comp_e, comp_b, ep_off, ep_idx, ne_off, ne_idx;
+  std::vector<float> edeg, ndeg;
+  int ncomp = 0, max_cn = 0, max_ce = 0, max_cb = 0;
+  std::vector<int> fW, fH;
+  std::vector<float2> twW, twH;
+  std::vector<float> gW, gH;
+  int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4;
+  // workspace regions (offsets relative to the workspace base)
+  Region r_h0, r_h1, r_fov, r_lflag, r_dep, r_tmp, r_prev, r_pred, r_nvl, r_delta;
+  Region r_ibcell, r_ibw, r_ibbin, r_ibsort, r_ibslot, r_scell, r_slen, r_srho, r_svx, r_svy, r_sinv, r_sucx,
+      r_sucy, r_sfx, r_sfy, r_ibtc, r_ibtf, r_ibto;
+  Region r_ccell, r_cw, r_cbin, r_csort, r_ctc, r_ctf, r_cto;
+  Region r_pairs, r_bpairs, r_compn, r_compe, r_compb, r_epo, r_epi, r_neo, r_nei, r_edeg, r_ndeg;
+  Region r_twW, r_twH, r_gW, r_gH, r_flags;
+};
+
+}  // namespace
+
+struct mc_plan {
+  int n = 0;
+  std::vector<HostRollout> R;
+  size_t ws_bytes = 0;
+  Region r_desc, r_tdev;
+  Region r_off[K_COUNT];
+  std::vector<int> off[K_COUNT];
+  int grid[K_COUNT] = {};
+  char* ws = nullptr;
+  bool bound = false;
+  int any_fluid = 0, any_steric = 0, max_iters = 0;
+  size_t node_smem = 0, fftr_smem = 0, fftc_smem = 0;
+  int node_bs = 32;
+  std::vector<RDesc> desc;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // 0: no field recording, 1: steric, 2: steric + fluid
+  int64_t graph_kernels = 0;
+  int64_t last_launches = 0;
+  int64_t step_kernels = 0;
+};
+
+namespace {
+
+bool factorize(int N, std::vector<int>& f) {
+  f.clear();
+  while (N % 4 == 0) { f.push_back(4); N /= 4; }
+  const int ps[] = {2, 3, 5, 7, 11, 13};
+  for (int p : ps)
+    while (N % p == 0) { f.push_back(p); N /= p; }
+  return N == 1 && (int)f.size() <= mc::kFftMaxFactors;
+}
+
+void fft_tables(int N, double sigma, std::vector<float2>& tw, std::vector<float>& g) {
+  tw.resize(N);
+  g.resize(N);
+  for (int k = 0; k < N; ++k) {
+    const double a = -2.0 * M_PI * (double)k / (double)N;
+    tw[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+    // numpy.fft.fftfreq abscissa
+    const double f = (k < (N + 1) / 2 ? (double)k : (double)(k - N)) / (double)N;
+    g[k] = (float)(std::exp(-2.0 * M_PI * M_PI * sigma * sigma * f * f) / (double)N);
+  }
+}
+
+// Topology: rod components and the gather lists that reproduce the reference's in-order
+// scatter-adds (pbd.py:26-47, 54-87).
+mc_status build_topology(HostRollout& h) {
+  const int N = h.dims.N, E = h.dims.E, B = h.dims.B;
+  for (int e = 0; e < E; ++e)
+    for (int j = 0; j < 2; ++j)
+      if (h.pairs[2 * e + j] < 0 || h.pairs[2 * e + j] >= N)
+        return fail(MC_ERR_INVALID, "edge " + std::to_string(e) + " references a node outside [0, N)");
+  for (int b = 0; b < B; ++b)
+    for (int j = 0; j < 2; ++j)
+      if (h.bpairs[2 * b + j] < 0 || h.bpairs[2 * b + j] >= E)
+        return fail(MC_ERR_INVALID, "bending pair " + std::to_string(b) + " references an edge outside [0, E)");
+  // edge -> bending pairs: all pairs where it is e_in (ascending), then all where it is e_out
+  std::vector<std::vector<int>> ein(E), eout(E);
+  for (int b = 0; b < B; ++b) {
+    ein[h.bpairs[2 * b]].push_back(b);
+    eout[h.bpairs[2 * b + 1]].push_back(b);
+  }
+  h.ep_off.assign(E + 1, 0);
+  h.ep_idx.clear();
+  h.edeg.assign(E, 1.f);
+  for (int e = 0; e < E; ++e) {
+    h.ep_off[e] = (int)h.ep_idx.size();
+    for (int b : ein[e]) h.ep_idx.push_back(b << 1);
+    for (int b : eout[e]) h.ep_idx.push_back((b << 1) | 1);
+    h.edeg[e] = (float)std::max<size_t>(ein[e].size() + eout[e].size(), 1);
+  }
+  h.ep_off[E] = (int)h.ep_idx.size();
+  // node -> edges: edges where it is src (ascending), then edges where it is tgt
+  std::vector<std::vector<int>> nsrc(N), ntgt(N);
+  for (int e = 0; e < E; ++e) {
+    nsrc[h.pairs[2 * e]].push_back(e);
+    ntgt[h.pairs[2 * e + 1]].push_back(e);
+  }
+  h.ne_off.assign(N + 1, 0);
+  h.ne_idx.clear();
+  h.ndeg.assign(N, 1.f);
+  for (int v = 0; v < N; ++v) {
+    h.ne_off[v] = (int)h.ne_idx.size();
+    for (int e : nsrc[v]) h.ne_idx.push_back(e << 1);
+    for (int e : ntgt[v]) h.ne_idx.push_back((e << 1) | 1);
+    h.ndeg[v] = (float)std::max<size_t>(nsrc[v].size() + ntgt[v].size(), 1);
+  }
+  h.ne_off[N] = (int)h.ne_idx.size();
+  // connected components (union-find over edges)
+  std::vector<int> par(N);
+  for (int i = 0; i < N; ++i) par[i] = i;
+  auto find = [&](int x) {
+    while (par[x] != x) { par[x] = par[par[x]]; x = par[x]; }
+    return x;
+  };
+  for (int e = 0; e < E; ++e) {
+    int a = find(h.pairs[2 * e]), b = find(h.pairs[2 * e + 1]);
+    if (a != b) par[std::max(a, b)] = std::min(a, b);
+  }
+  // components must be contiguous node ranges whose edges and pairs are contiguous
+  // ranges in the same order; otherwise the whole graph is one component
+  std::vector<int> cid(N);
+  std::vector<int> root_to_c(N, -1);
+  bool ok = true;
+  int nc = 0, last_root = -1;
+  for (int i = 0; i < N; ++i) {
+    int rt = find(i);
+    if (rt != last_root) {
+      if (root_to_c[rt] != -1) ok = false;
+      root_to_c[rt] = nc++;
+      last_root = rt;
+    }
+    cid[i] = root_to_c[rt];
+  }
+  std::vector<int> ce(nc + 1, 0), cb(nc + 1, 0), cn(nc + 1, 0);
+  if (ok) {
+    for (int i = 0; i < N; ++i) cn[cid[i] + 1]++;
+    int prev = 0;
+    for (int e = 0; e < E && ok; ++e) {
+      int c = cid[h.pairs[2 * e]];
+      if (c < prev) ok = false;
+      prev = c;
+      ce[c + 1]++;
+    }
+    prev = 0;
+    for (int b = 0; b < B && ok; ++b) {
+      int c = cid[h.pairs[2 * h.bpairs[2 * b]]];
+      int c2 = cid[h.pairs[2 * h.bpairs[2 * b + 1]]];
+      if (c != c2 || c < prev) ok = false;
+      prev = c;
+      cb[c + 1]++;
+    }
+  }
+  if (ok && nc > 0) {
+    for (int c = 0; c < nc; ++c) {
+      cn[c + 1] += cn[c];
+      ce[c + 1] += ce[c];
+      cb[c + 1] += cb[c];
+    }
+    h.comp_n = cn;
+    h.comp_e = ce;
+    h.comp_b = cb;
+    h.ncomp = nc;
+  } else {
+    h.comp_n = {0, N};
+    h.comp_e = {0, E};
+    h.comp_b = {0, B};
+    h.ncomp = 1;
+  }
+  h.max_cn = h.max_ce = h.max_cb = 1;
+  for (int c = 0; c < h.ncomp; ++c) {
+    h.max_cn = std::max(h.max_cn, h.comp_n[c + 1] - h.comp_n[c]);
+    h.max_ce = std::max(h.max_ce, h.comp_e[c + 1] - h.comp_e[c]);
+    h.max_cb = std::max(h.max_cb, h.comp_b[c + 1] - h.comp_b[c]);
+  }
+  return MC_OK;
+}
+
+struct Layout {
+  size_t cur = 0;
+  Region take(size_t bytes) {
+    Region r;
+    r.off = cur;
+    r.bytes = bytes;
+    cur = align_up(cur + std::max<size_t>(bytes, 1), 256);
+    return r;
+  }
+};
+
+int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+template <typename T>
+T* at(char* base, const Region& r) {
+  return reinterpret_cast<T*>(base + r.off);
+}
+
+void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, const mc_record* rec) {
+  HostRollout& h = p->R[i];
+  RDesc d;
+  std::memset(&d, 0, sizeof(d));
+  char* b = p->ws;
+  d.H = h.dims.H;
+  d.W = h.dims.W;
+  d.N = h.dims.N;
+  d.E = h.dims.E;
+  d.B = h.dims.B;
+  d.K = h.cfg.ibm_kernel_size;
+  d.ncomp = h.ncomp;
+  d.M = h.M;
+  d.ntile_x = h.ntx;
+  d.ntile_y = h.nty;
+  d.lbm_tx = h.lbm_tx;
+  d.lbm_ty = h.lbm_ty;
+  d.lbm_tw = 32 * h.vec;
+  const mc_config& c = h.cfg;
+  d.dt = h.dt;
+  d.damping = c.damping;
+  d.k_stretch = c.stiffness_stretch;
+  d.k_shear = c.stiffness_shear;
+  // mean_scale = 1 (fluid grid == domain grid) but scale keeps the reference's axis order
+  const double sx = (double)h.dims.W / (double)h.dims.H, sy = (double)h.dims.H / (double)h.dims.W;
+  d.scale_x = (float)sx;
+  d.scale_y = (float)sy;
+  d.vmax = (float)((double)c.max_fluid_velocity * (0.5 * (sx + sy)));
+  d.sdt_x = d.scale_x * h.dt;
+  d.sdt_y = d.scale_y * h.dt;
+  d.relax = c.ibm_relaxation;
+  d.node_mass = c.node_mass;
+  {
+    // omega+ = clip(1/(3 nu + 0.5), 0, 1.9); omega- from Lambda (fluid.py:155-161, 342-344)
+    double wpd = 1.0 / (3.0 * (double)c.viscosity + 0.5);
+    wpd = std::min(std::max(wpd, 0.0), 1.9);
+    const float eps = 1.1920928955078125e-07f;
+    float wp = (float)wpd;
+    float offs = 1.0f / std::max(wp, eps) - 0.5f;
+    float wm = 1.0f / (c.lambda_trt / std::max(offs, eps) + 0.5f);
+    d.wp = wp;
+    d.wm = wm;
+  }
+  d.st_strength = c.steric_strength;
+  d.st_sigma = c.steric_sigma;
+  d.st_scatter = c.steric_scatter_value;
+  const double sg = (double)c.steric_sigma;
+  d.st_2s2 = (float)(2.0 * sg * sg);
+  d.st_norm = (float)(2.0 * M_PI * sg * sg);
+  d.st_coef = (float)((double)c.steric_scatter_value / (sg * sg));
+  d.st_skip = c.steric_neighbor_skip;
+  d.ib_iters = c.ibm_iterations;
+  d.cycles = c.cycles_per_step;
+  d.enable_fluid = c.enable_fluid ? 1 : 0;
+  d.enable_steric = c.enable_steric ? 1 : 0;
+  d.force_clamp = c.enable_force_clamp ? 1 : 0;
+  d.fftW_nf = (int)h.fW.size();
+  d.fftH_nf = (int)h.fH.size();
+  for (size_t k = 0; k < h.fW.size(); ++k) d.fftW_f[k] = h.fW[k];
+  for (size_t k = 0; k < h.fH.size(); ++k) d.fftH_f[k] = h.fH[k];
+  d.twW = at<float2>(b, h.r_twW);
+  d.twH = at<float2>(b, h.r_twH);
+  d.gW = at<float>(b, h.r_gW);
+  d.gH = at<float>(b, h.r_gH);
+  if (st) {
+    d.pos = st->position;
+    d.vel = st->velocity;
+    d.theta = st->theta;
+    d.rest_len = st->rest_lengths;
+    d.rest_ang = st->bending_rest_angles;
+    d.kb = st->bending_stiffness;
+    d.steric = st->steric;
+    d.fluid_vel = st->fluid_velocity;
+    d.f_grid = st->f_grid;
+  }
+  if (act) {
+    d.act_c = act->c;
+    d.act_amp = act->amp;
+    d.act_omega = act->omega;
+    d.act_phase = act->phase;
+    d.act_t0 = act->t0;
+  }
+  if (rec) {
+    d.rec_pos = rec->position;
+    d.rec_vel = rec->velocity;
+    d.rec_steric = rec->steric;
+    d.rec_fluid = rec->fluid_velocity;
+    d.rec_every = rec->every;
+  }
+  d.max_comp_nodes = 0;
+  int mcn = 1, mce = 1, mcb = 1;
+  for (auto& o : p->R) {
+    mcn = std::max(mcn, o.max_cn);
+    mce = std::max(mce, o.max_ce);
+    mcb = std::max(mcb, o.max_cb);
+  }
+  d.max_comp_nodes = mcn;
+  d.max_comp_edges = mce;
+  d.max_comp_pairs = mcb;
+  d.pairs = at<int>(b, h.r_pairs);
+  d.bpairs = at<int>(b, h.r_bpairs);
+  d.comp_n = at<int>(b, h.r_compn);
+  d.comp_e = at<int>(b, h.r_compe);
+  d.comp_b = at<int>(b, h.r_compb);
+  d.ep_off = at<int>(b, h.r_epo);
+  d.ep_idx = at<int>(b, h.r_epi);
+  d.ne_off = at<int>(b, h.r_neo);
+  d.ne_idx = at<int>(b, h.r_nei);
+  d.edeg = at<float>(b, h.r_edeg);
+  d.ndeg = at<float>(b, h.r_ndeg);
+  d.h[0] = at<float>(b, h.r_h0);
+  d.h[1] = at<float>(b, h.r_h1);
+  d.fov = at<float>(b, h.r_fov);
+  d.lbm_flag = at<int>(b, h.r_lflag);
+  d.dep = at<float>(b, h.r_dep);
+  d.tmp = at<float>(b, h.r_tmp);
+  d.prev = at<float>(b, h.r_prev);
+  d.pred = at<float>(b, h.r_pred);
+  d.nvl = at<float>(b, h.r_nvl);
+  d.delta = at<float>(b, h.r_delta);
+  d.ib_cell = at<int>(b, h.r_ibcell);
+  d.ib_w = at<float>(b, h.r_ibw);
+  d.ib_binned = at<int>(b, h.r_ibbin);
+  d.ib_sorted = at<int>(b, h.r_ibsort);
+  d.ib_slot = at<int>(b, h.r_ibslot);
+  d.s_cell = at<int>(b, h.r_scell);
+  d.s_len = at<int>(b, h.r_slen);
+  d.s_rho = at<float>(b, h.r_srho);
+  d.s_vx = at<float>(b, h.r_svx);
+  d.s_vy = at<float>(b, h.r_svy);
+  d.s_inv = at<float>(b, h.r_sinv);
+  d.s_ucx = at<float>(b, h.r_sucx);
+  d.s_ucy = at<float>(b, h.r_sucy);
+  d.s_fx = at<float>(b, h.r_sfx);
+  d.s_fy = at<float>(b, h.r_sfy);
+  d.ib_tcount = at<int>(b, h.r_ibtc);
+  d.ib_tfill = at<int>(b, h.r_ibtf);
+  d.ib_toff = at<int>(b, h.r_ibto);
+  d.c_cell = at<int>(b, h.r_ccell);
+  d.c_w = at<float>(b, h.r_cw);
+  d.c_binned = at<int>(b, h.r_cbin);
+  d.c_sorted = at<int>(b, h.r_csort);
+  d.c_tcount = at<int>(b, h.r_ctc);
+  d.c_tfill = at<int>(b, h.r_ctf);
+  d.c_toff = at<int>(b, h.r_cto);
+  d.flags = at<unsigned>(b, h.r_flags);
+  p->desc[i] = d;
+}
+
+mc::Launch L(mc_plan* p, Kind k, cudaStream_t s) {
+  mc::Launch l;
+  l.d = at<RDesc>(p->ws, p->r_desc);
+  l.off = at<int>(p->ws, p->r_off[k]);
+  l.n = p->n;
+  l.grid = p->grid[k];
+  l.s = s;
+  return l;
+}
+
+// The launch sequence of one step (src/microcosmos/simulate.py:37-100).
+int64_t enqueue_step(mc_plan* p, int parity, int write_u, int rec_fields, cudaStream_t s) {
+  int* tdev = at<int>(p->ws, p->r_tdev);
+  int64_t k = 0;
+  if (p->grid[K_NODES]) { mc::launch_predict(L(p, K_NODES, s)); ++k; }
+  if (p->any_steric) {
+    mc::launch_bin_scan(L(p, K_CIC, s), 1);
+    mc::launch_bin_scatter(L(p, K_CIC, s), 1);
+    mc::launch_bin_sort(L(p, K_TILES, s), 1, parity);
+    mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem);
+    mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem);
+    k += 5;
+  }
+  if (p->grid[K_COMP]) { mc::launch_node(L(p, K_COMP, s), tdev, p->node_smem, p->node_bs); ++k; }
+  if (p->any_fluid) {
+    mc::launch_bin_scan(L(p, K_IB, s), 0);
+    mc::launch_bin_scatter(L(p, K_IB, s), 0);
+    mc::launch_bin_sort(L(p, K_TILES, s), 0, parity);
+    k += 3;
+    for (int it = 0; it < p->max_iters; ++it) {
+      mc::launch_ib_interp(L(p, K_NODES, s), it);
+      mc::launch_ib_spread(L(p, K_IB, s), it);
+      k += 2;
+    }
+    mc::launch_ib_finalize(L(p, K_IB, s));
+    mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->R[0].vec);
+    k += 2;
+  }
+  if (p->grid[K_NODES]) { mc::launch_reaction(L(p, K_NODES, s), tdev); ++k; }
+  if (rec_fields) { mc::launch_record_fields(L(p, K_CELLS, s), tdev); ++k; }
+  mc::launch_tick(tdev, s);
+  ++k;
+  return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mc_last_error(void) { return g_err.c_str(); }
+const char* mc_version(void) { return "microcosmos_b200 0.1.0 (sm_100a)"; }
+
+mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, const float* dt,
+                         const int32_t* const* pairs, const int32_t* const* bending_pairs, mc_plan** out) {
+  g_err.clear();
+  if (!out || n <= 0 || !dims || !cfg || !dt || !pairs || !bending_pairs) return fail(MC_ERR_INVALID, "null argument");
+  *out = nullptr;
+  mc_plan* p = new mc_plan();
+  p->n = n;
+  p->R.resize(n);
+  Layout lay;
+  p->r_desc = lay.take(sizeof(RDesc) * n);
+  p->r_tdev = lay.take(sizeof(int));
+  for (int k = 0; k < K_COUNT; ++k) p->r_off[k] = lay.take(sizeof(int) * (n + 1));
+  int vec_all = -1;
+  for (int i = 0; i < n; ++i) {
+    HostRollout& h = p->R[i];
+    h.dims = dims[i];
+    h.cfg = cfg[i];
+    h.dt = dt[i];
+    const mc_dims& D = h.dims;
+    const mc_config& c = h.cfg;
+    if (D.H < 4 || D.W < 4 || D.N < 0 || D.E < 0 || D.B < 0) {
+      delete p;
+      return fail(MC_ERR_INVALID, "rollout " + std::to_string(i) + ": grid must be at least 4x4 and counts >= 0");
+    }
+    if ((D.E > 0 && !pairs[i]) || (D.B > 0 && !bending_pairs[i])) {
+      delete p;
+      return fail(MC_ERR_INVALID, "null topology array");
+    }
+    if (c.synthetic_node_width != 0.0f) {
+      delete p;
+      return fail(MC_ERR_UNSUPPORTED, "synthetic_node_width > 0 is not implemented");
+    }
+    if (c.ibm_kernel_size < 1 || c.ibm_kernel_size > 8) {
+      delete p;
+      return fail(MC_ERR_UNSUPPORTED, "ibm_kernel_size must be in [1, 8]");
+    }
+    if (!(dt[i] > 0.0f)) {
+      delete p;
+      return fail(MC_ERR_INVALID, "dt must be > 0");
+    }
+    const long long M = c.enable_fluid ? (long long)D.N * c.ibm_kernel_size * c.ibm_kernel_size : 0;
+    if (M >= (1LL << 24) || 4LL * D.N >= (1LL << 24)) {
+      delete p;
+      return fail(MC_ERR_UNSUPPORTED, "too many IB contributions for 24-bit sort keys (N*K*K < 2^24)");
+    }
+    h.M = (int)M;
+    h.pairs.assign(pairs[i] ? pairs[i] : nullptr, pairs[i] ? pairs[i] + 2 * (size_t)D.E : nullptr);
+    h.bpairs.assign(bending_pairs[i] ? bending_pairs[i] : nullptr,
+                    bending_pairs[i] ? bending_pairs[i] + 2 * (size_t)D.B : nullptr);
+    mc_status st = build_topology(h);
+    if (st != MC_OK) {
+      delete p;
+      return st;
+    }
+    if (c.enable_steric) {
+      if (!factorize(D.W, h.fW) || !factorize(D.H, h.fH) || D.W > mc::kFftMaxN || D.H > 2048) {
+        delete p;
+        return fail(MC_ERR_UNSUPPORTED, "steric FFT needs H, W with prime factors <= 13, W <= 4096, H <= 2048");
+      }
+      fft_tables(D.W, c.steric_sigma, h.twW, h.gW);
+      fft_tables(D.H, c.steric_sigma, h.twH, h.gH);
+    }
+    h.vec = (D.W % 4 == 0) ? 4 : 1;
+    if (vec_all == -1) vec_all = h.vec;
+    if (vec_all != h.vec) vec_all = 1;
+    h.ntx = div_up(D.W, mc::kBinTile);
+    h.nty = div_up(D.H, mc::kBinTile);
+    const size_t HW = (size_t)D.H * D.W;
+    const size_t N = D.N, E = D.E, B = D.B, nt = (size_t)h.ntx * h.nty;
+    h.r_h0 = lay.take(9 * HW * 4);
+    h.r_h1 = lay.take(9 * HW * 4);
+    h.r_fov = lay.take(2 * HW * 4);
+    h.r_dep = lay.take(HW * 4);
+    h.r_tmp = lay.take(HW * 4);
+    h.r_prev = lay.take(2 * N * 4);
+    h.r_pred = lay.take(2 * N * 4);
+    h.r_nvl = lay.take(2 * N * 4);
+    h.r_delta = lay.take(2 * N * 4);
+    const size_t Mz = (size_t)M;
+    h.r_ibcell = lay.take(Mz * 4);
+    h.r_ibw = lay.take(Mz * 4);
+    h.r_ibbin = lay.take(Mz * 4);
+    h.r_ibsort = lay.take(Mz * 4);
+    h.r_ibslot = lay.take(Mz * 4);
+    h.r_scell = lay.take(Mz * 4);
+    h.r_slen = lay.take(Mz * 4);
+    h.r_srho = lay.take(Mz * 4);
+    h.r_svx = lay.take(Mz * 4);
+    h.r_svy = lay.take(Mz * 4);
+    h.r_sinv = lay.take(Mz * 4);
+    h.r_sucx = lay.take(Mz * 4);
+    h.r_sucy = lay.take(Mz * 4);
+    h.r_sfx = lay.take(Mz * 4);
+    h.r_sfy = lay.take(Mz * 4);
+    h.r_ibtc = lay.take(nt * 4);
+    h.r_ibtf = lay.take(nt * 4);
+    h.r_ibto = lay.take((nt + 1) * 4);
+    h.r_ccell = lay.take(4 * N * 4);
+    h.r_cw = lay.take(4 * N * 4);
+    h.r_cbin = lay.take(4 * N * 4);
+    h.r_csort = lay.take(4 * N * 4);
+    h.r_ctc = lay.take(nt * 4);
+    h.r_ctf = lay.take(nt * 4);
+    h.r_cto = lay.take((nt + 1) * 4);
+    h.r_pairs = lay.take(2 * E * 4);
+    h.r_bpairs = lay.take(2 * B * 4);
+    h.r_compn = lay.take((h.ncomp + 1) * 4);
+    h.r_compe = lay.take((h.ncomp + 1) * 4);
+    h.r_compb = lay.take((h.ncomp + 1) * 4);
+    h.r_epo = lay.take((E + 1) * 4);
+    h.r_epi = lay.take(h.ep_idx.size() * 4);
+    h.r_neo = lay.take((N + 1) * 4);
+    h.r_nei = lay.take(h.ne_idx.size() * 4);
+    h.r_edeg = lay.take(E * 4);
+    h.r_ndeg = lay.take(N * 4);
+    h.r_twW = lay.take(h.twW.size() * 8);
+    h.r_twH = lay.take(h.twH.size() * 8);
+    h.r_gW = lay.take(h.gW.size() * 4);
+    h.r_gH = lay.take(h.gH.size() * 4);
+    h.r_flags = lay.take(4);
+    if (c.enable_fluid) p->any_fluid = 1;
+    if (c.enable_steric) p->any_steric = 1;
+    p->max_iters = std::max(p->max_iters, c.enable_fluid ? c.ibm_iterations : 0);
+  }
+  for (int i = 0; i < n; ++i) {
+    HostRollout& h = p->R[i];
+    h.vec = vec_all;
+    h.lbm_tx = div_up(h.dims.W, 32 * h.vec);
+    h.lbm_ty = div_up(h.dims.H, mc::kLbmTileY);
+    h.r_lflag = lay.take((size_t)h.lbm_tx * h.lbm_ty * 4);
+  }
+  p->ws_bytes = lay.cur;
+  // CTA offset tables
+  for (int k = 0; k < K_COUNT; ++k) p->off[k].assign(n + 1, 0);
+  int mcn = 1, mce = 1, mcb = 1;
+  for (int i = 0; i < n; ++i) {
+    HostRollout& h = p->R[i];
+    const mc_config& c = h.cfg;
+    const long long HW = (long long)h.dims.H * h.dims.W;
+    int cnt[K_COUNT];
+    cnt[K_NODES] = div_up(h.dims.N, 256);
+    cnt[K_COMP] = h.dims.N > 0 ? h.ncomp : 0;
+    cnt[K_IB] = div_up(h.M, 256);
+    cnt[K_CIC] = c.enable_steric ? div_up(4LL * h.dims.N, 256) : 0;
+    cnt[K_TILES] = h.ntx * h.nty;
+    cnt[K_LBM] = c.enable_fluid ? h.lbm_tx * h.lbm_ty : 0;
+    cnt[K_CELLS] = std::min(div_up(HW, 256), 1024);
+    cnt[K_FFTR] = c.enable_steric ? div_up(h.dims.H, 2) : 0;
+    cnt[K_FFTC] = c.enable_steric ? div_up(h.dims.W, 2 * mc::kFftColsPerCta) : 0;
+    for (int k = 0; k < K_COUNT; ++k) p->off[k][i + 1] = p->off[k][i] + cnt[k];
+    mcn = std::max(mcn, h.max_cn);
+    mce = std::max(mce, h.max_ce);
+    mcb = std::max(mcb, h.max_cb);
+    p->fftr_smem = std::max(p->fftr_smem, c.enable_steric ? (size_t)2 * h.dims.W * sizeof(float2) : 0);
+    p->fftc_smem = std::max(p->fftc_smem,
+                            c.enable_steric ? (size_t)2 * mc::kFftColsPerCta * h.dims.H * sizeof(float2) : 0);
+  }
+  for (int k = 0; k < K_COUNT; ++k) p->grid[k] = p->off[k][n];
+  p->node_smem = (size_t)(2 * mcn + 4 * mce + 3 * mcb) * sizeof(float);
+  if (p->node_smem > 200 * 1024) {
+    delete p;
+    return fail(MC_ERR_UNSUPPORTED, "rod component too large for shared memory (> ~6000 nodes)");
+  }
+  int work = std::max(mcn, std::max(mce, mcb));
+  p->node_bs = std::min(256, std::max(32, (work + 31) / 32 * 32));
+  p->desc.resize(n);
+  *out = p;
+  return MC_OK;
+}
+
+void mc_plan_destroy(mc_plan* p) {
+  if (!p) return;
+  for (auto& g : p->graph)
+    if (g) cudaGraphExecDestroy(g);
+  if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+  delete p;
+}
+
+size_t mc_plan_workspace_bytes(const mc_plan* p) { return p ? p->ws_bytes : 0; }
+
+mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (!workspace || bytes < p->ws_bytes) return fail(MC_ERR_WORKSPACE, "workspace missing or smaller than mc_plan_workspace_bytes()");
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return fail(MC_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  p->ws = (char*)workspace;
+  auto up = [&](const Region& r, const void* src, size_t n) -> cudaError_t {
+    if (n == 0) return cudaSuccess;
+    return cudaMemcpyAsync(p->ws + r.off, src, n, cudaMemcpyHostToDevice, s);
+  };
+  for (int i = 0; i < p->n; ++i) {
+    HostRollout& h = p->R[i];
+    MC_CUDA(up(h.r_pairs, h.pairs.data(), h.pairs.size() * 4));
+    MC_CUDA(up(h.r_bpairs, h.bpairs.data(), h.bpairs.size() * 4));
+    MC_CUDA(up(h.r_compn, h.comp_n.data(), h.comp_n.size() * 4));
+    MC_CUDA(up(h.r_compe, h.comp_e.data(), h.comp_e.size() * 4));
+    MC_CUDA(up(h.r_compb, h.comp_b.data(), h.comp_b.size() * 4));
+    MC_CUDA(up(h.r_epo, h.ep_off.data(), h.ep_off.size() * 4));
+    MC_CUDA(up(h.r_epi, h.ep_idx.data(), h.ep_idx.size() * 4));
+    MC_CUDA(up(h.r_neo, h.ne_off.data(), h.ne_off.size() * 4));
+    MC_CUDA(up(h.r_nei, h.ne_idx.data(), h.ne_idx.size() * 4));
+    MC_CUDA(up(h.r_edeg, h.edeg.data(), h.edeg.size() * 4));
+    MC_CUDA(up(h.r_ndeg, h.ndeg.data(), h.ndeg.size() * 4));
+    MC_CUDA(up(h.r_twW, h.twW.data(), h.twW.size() * 8));
+    MC_CUDA(up(h.r_twH, h.twH.data(), h.twH.size() * 8));
+    MC_CUDA(up(h.r_gW, h.gW.data(), h.gW.size() * 4));
+    MC_CUDA(up(h.r_gH, h.gH.data(), h.gH.size() * 4));
+    fill_desc(p, i, nullptr, nullptr, nullptr);
+  }
+  for (int k = 0; k < K_COUNT; ++k) MC_CUDA(up(p->r_off[k], p->off[k].data(), p->off[k].size() * 4));
+  MC_CUDA(up(p->r_desc, p->desc.data(), p->desc.size() * sizeof(RDesc)));
+  // zero the binning counters of every tile before the first clear kernel runs
+  MC_CUDA(mc::node_set_smem(std::max<size_t>(p->node_smem, 1)));
+  if (p->any_steric) MC_CUDA(mc::fft_set_smem(p->fftr_smem, p->fftc_smem));
+  mc::launch_clear_ws(L(p, K_CELLS, s));
+  MC_CUDA(cudaGetLastError());
+  for (auto& g : p->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  if (!p->cap_stream) MC_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+  p->bound = true;
+  return MC_OK;
+}
+
+mc_status mc_rollout(mc_plan* p, const mc_state* states, int32_t num_steps, const mc_actuation* const* act,
+                     const mc_record* const* rec, int32_t use_graph, void* stream) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (!p->bound) return fail(MC_ERR_NOT_BOUND, "mc_plan_bind() was not called");
+  if (!states || num_steps < 0) return fail(MC_ERR_INVALID, "null states or negative num_steps");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rec_fields = 0, rec_fluid = 0;
+  for (int i = 0; i < p->n; ++i) {
+    const mc_state& st = states[i];
+    const HostRollout& h = p->R[i];
+    if (!st.position || !st.velocity || (h.dims.E && (!st.theta || !st.rest_lengths)) ||
+        (h.dims.B && (!st.bending_rest_angles || !st.bending_stiffness)) ||
+        (h.cfg.enable_fluid && (!st.f_grid || !st.fluid_velocity)) || (h.cfg.enable_steric && !st.steric))
+      return fail(MC_ERR_INVALID, "rollout " + std::to_string(i) + ": null state array");
+    if (h.cfg.enable_fluid && (reinterpret_cast<uintptr_t>(st.fluid_velocity) % 16 != 0))
+      return fail(MC_ERR_INVALID, "fluid_velocity must be 16-byte aligned");
+    const mc_actuation* a = act ? act[i] : nullptr;
+    if (a && (!a->c || !a->amp || !a->omega || !a->phase)) return fail(MC_ERR_INVALID, "incomplete actuation");
+    const mc_record* r = rec ? rec[i] : nullptr;
+    if (r) {
+      if (r->every < 1) return fail(MC_ERR_INVALID, "record.every must be >= 1");
+      if (r->steric || r->fluid_velocity) rec_fields = 1;
+      if (r->fluid_velocity) rec_fluid = 1;
+    }
+    fill_desc(p, i, &st, a, r);
+  }
+  MC_CUDA(cudaMemcpyAsync(p->ws + p->r_desc.off, p->desc.data(), p->desc.size() * sizeof(RDesc),
+                          cudaMemcpyHostToDevice, s));
+  int* tdev = at<int>(p->ws, p->r_tdev);
+  MC_CUDA(cudaMemsetAsync(tdev, 0, sizeof(int), s));
+  int64_t launches = 0;
+  if (p->any_fluid) {
+    mc::launch_unstream(L(p, K_CELLS, s));
+    ++launches;
+  }
+  int step = 0;
+  while (step < num_steps) {
+    const bool pair_ok = use_graph && (step % 2 == 0) && (step + 2 <= num_steps - 1);
+    if (pair_ok) {
+      cudaGraphExec_t& g = p->graph[rec_fields ? (rec_fluid ? 2 : 1) : 0];
+      if (!g) {
+        cudaGraph_t graph;
+        MC_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
+        int64_t k0 = enqueue_step(p, 0, rec_fluid, rec_fields, p->cap_stream);
+        int64_t k1 = enqueue_step(p, 1, rec_fluid, rec_fields, p->cap_stream);
+        cudaError_t e = cudaStreamEndCapture(p->cap_stream, &graph);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&g, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+          g = nullptr;
+          return cuda_fail(e, "cudaGraphInstantiate");
+        }
+        p->graph_kernels = k0 + k1;
+      }
+      MC_CUDA(cudaGraphLaunch(g, s));
+      launches += p->graph_kernels;
+      step += 2;
+      continue;
+    }
+    const bool final = (step == num_steps - 1);
+    launches += enqueue_step(p, step & 1, (final || rec_fluid) ? 1 : 0, rec_fields, s);
+    ++step;
+  }
+  if (p->any_fluid) {
+    mc::launch_stream_out(L(p, K_CELLS, s), num_steps & 1);
+    ++launches;
+  }
+  MC_CUDA(cudaGetLastError());
+  p->last_launches = launches;
+  return MC_OK;
+}
+
+mc_status mc_step(mc_plan* p, const mc_state* states, void* stream) {
+  return mc_rollout(p, states, 1, nullptr, nullptr, 0, stream);
+}
+
+mc_status mc_plan_read_flags(mc_plan* p, uint32_t* flags, int32_t clear, void* stream) {
+  g_err.clear();
+  if (!p || !flags) return fail(MC_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(MC_ERR_NOT_BOUND, "mc_plan_bind() was not called");
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int i = 0; i < p->n; ++i)
+    MC_CUDA(cudaMemcpyAsync(flags + i, p->ws + p->R[i].r_flags.off, 4, cudaMemcpyDeviceToHost, s));
+  MC_CUDA(cudaStreamSynchronize(s));
+  if (clear)
+    for (int i = 0; i < p->n; ++i) MC_CUDA(cudaMemsetAsync(p->ws + p->R[i].r_flags.off, 0, 4, s));
+  return MC_OK;
+}
+
+int64_t mc_plan_last_launch_count(const mc_plan* p) { return p ? p->last_launches : 0; }
+
+}  // extern "C"

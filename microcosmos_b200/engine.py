@@ -1,0 +1,269 @@
+"""Host-side engine over the C ABI: plans, device workspaces and device-resident
+rollout state.
+
+A ``Plan`` holds one or more rollouts (any grid and filament sizes) that step
+together; the single-instance path is a plan of one.  The C library allocates nothing
+on the device: the workspace is a torch tensor owned by the ``Plan``.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+
+import numpy as np
+import torch
+
+from . import _lib
+from .config import ConstraintSolverConfig, pbd_rod_constraint
+
+_F32 = torch.float32
+
+
+def _require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("microcosmos_b200 needs a CUDA device; there is no CPU fallback")
+
+
+def mc_config(cfg: ConstraintSolverConfig) -> _lib.McConfig:
+    if cfg.bending_constraint is not pbd_rod_constraint or cfg.solver_type != "pbd":
+        raise NotImplementedError("only the PBD rod constraint plugin (pbd_rod_constraint) is implemented")
+    c = _lib.McConfig()
+    c.cycles_per_step = int(cfg.cycles_per_step)
+    c.stiffness_stretch = float(cfg.stiffness_stretch)
+    c.stiffness_shear = float(cfg.stiffness_shear)
+    c.damping = float(cfg.damping)
+    c.enable_fluid = int(bool(cfg.enable_fluid))
+    c.viscosity = float(cfg.viscosity)
+    c.max_fluid_velocity = float(cfg.max_fluid_velocity)
+    c.ibm_iterations = int(cfg.ibm_iterations)
+    c.synthetic_node_width = float(cfg.synthetic_node_width)
+    c.ibm_kernel_size = int(cfg.ibm_kernel_size)
+    c.ibm_relaxation = float(cfg.ibm_relaxation)
+    c.node_mass = float(cfg.node_mass)
+    c.lambda_trt = float(cfg.lambda_trt)
+    c.enable_force_clamp = int(bool(cfg.enable_force_clamp))
+    c.enable_steric = int(bool(cfg.enable_steric))
+    c.steric_strength = float(cfg.steric_strength)
+    c.steric_sigma = float(cfg.steric_sigma)
+    c.steric_neighbor_skip = int(cfg.steric_neighbor_skip)
+    c.steric_scatter_value = float(cfg.steric_scatter_value)
+    return c
+
+
+def _dev(x, dtype=_F32, device="cuda"):
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype, device=device)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+@dataclasses.dataclass
+class DeviceState:
+    """Device-resident Nodes/Edges/Fields of one rollout (float32, contiguous)."""
+    H: int
+    W: int
+    position: torch.Tensor
+    velocity: torch.Tensor
+    theta: torch.Tensor
+    rest_lengths: torch.Tensor
+    bending_rest_angles: torch.Tensor
+    bending_stiffness: torch.Tensor
+    steric: torch.Tensor
+    fluid_velocity: torch.Tensor
+    f_grid: torch.Tensor
+    pairs: np.ndarray          # host int32 topology
+    bending_pairs: np.ndarray
+
+    @property
+    def N(self):
+        return self.position.shape[0]
+
+    @classmethod
+    def from_arrays(cls, H, W, position, velocity, pairs, theta, rest_lengths, bending_pairs,
+                    bending_rest_angles, bending_stiffness, f_grid, steric=None, fluid_velocity=None,
+                    device="cuda"):
+        pairs_h = np.ascontiguousarray(
+            pairs.detach().cpu().numpy() if isinstance(pairs, torch.Tensor) else pairs, dtype=np.int32).reshape(-1, 2)
+        bp_h = np.ascontiguousarray(
+            bending_pairs.detach().cpu().numpy() if isinstance(bending_pairs, torch.Tensor) else bending_pairs,
+            dtype=np.int32).reshape(-1, 2)
+        return cls(
+            H=int(H), W=int(W),
+            position=_dev(position, device=device).reshape(-1, 2).clone(),
+            velocity=_dev(velocity, device=device).reshape(-1, 2).clone(),
+            theta=_dev(theta, device=device).reshape(-1).clone(),
+            rest_lengths=_dev(rest_lengths, device=device).reshape(-1).clone(),
+            bending_rest_angles=_dev(bending_rest_angles, device=device).reshape(-1).clone(),
+            bending_stiffness=_dev(bending_stiffness, device=device).reshape(-1).clone(),
+            steric=(_dev(steric, device=device).clone() if steric is not None
+                    else torch.zeros((H, W), dtype=_F32, device=device)),
+            fluid_velocity=(_dev(fluid_velocity, device=device).clone() if fluid_velocity is not None
+                            else torch.zeros((2, H, W), dtype=_F32, device=device)),
+            f_grid=_dev(f_grid, device=device).reshape(9, H, W).clone(),
+            pairs=pairs_h, bending_pairs=bp_h)
+
+    @classmethod
+    def from_scenario(cls, sc, device="cuda"):
+        return cls.from_arrays(sc.H, sc.W, sc.position, sc.velocity, sc.pairs, sc.theta, sc.rest_lengths,
+                               sc.bending_pairs, sc.bending_rest_angles, sc.bending_stiffness, sc.f_grid,
+                               sc.steric, sc.fluid_velocity, device=device)
+
+    def struct(self) -> _lib.McState:
+        s = _lib.McState()
+        s.position = self.position.data_ptr()
+        s.velocity = self.velocity.data_ptr()
+        s.theta = self.theta.data_ptr()
+        s.rest_lengths = self.rest_lengths.data_ptr()
+        s.bending_rest_angles = self.bending_rest_angles.data_ptr()
+        s.bending_stiffness = self.bending_stiffness.data_ptr()
+        s.steric = self.steric.data_ptr()
+        s.fluid_velocity = self.fluid_velocity.data_ptr()
+        s.f_grid = self.f_grid.data_ptr()
+        return s
+
+    def host(self):
+        """Copy to numpy (synchronises)."""
+        return {k: getattr(self, k).detach().cpu().numpy() for k in
+                ("position", "velocity", "theta", "bending_rest_angles", "steric", "fluid_velocity", "f_grid")}
+
+
+@dataclasses.dataclass
+class Actuation:
+    """rest[b](t) = c[b] + amp[b] sin(omega[b] t + phase[b]) on the device."""
+    c: torch.Tensor
+    amp: torch.Tensor
+    omega: torch.Tensor
+    phase: torch.Tensor
+    t0: int = 0
+
+    @classmethod
+    def from_scenario(cls, sc, device="cuda", t0=0):
+        if sc.act_amp is None:
+            return None
+        return cls(_dev(sc.act_c, device=device), _dev(sc.act_amp, device=device),
+                   _dev(sc.act_omega, device=device), _dev(sc.act_phase, device=device), t0)
+
+    def struct(self):
+        a = _lib.McActuation()
+        a.c, a.amp, a.omega, a.phase = (self.c.data_ptr(), self.amp.data_ptr(), self.omega.data_ptr(),
+                                        self.phase.data_ptr())
+        a.t0 = int(self.t0)
+        return a
+
+
+@dataclasses.dataclass
+class Record:
+    position: torch.Tensor | None = None
+    velocity: torch.Tensor | None = None
+    steric: torch.Tensor | None = None
+    fluid_velocity: torch.Tensor | None = None
+    every: int = 1
+
+    @classmethod
+    def allocate(cls, state: DeviceState, num_steps: int, every: int = 1, fields=True, device="cuda"):
+        T = num_steps // every
+        N, H, W = state.N, state.H, state.W
+        return cls(position=torch.empty((T, N, 2), dtype=_F32, device=device),
+                   velocity=torch.empty((T, N, 2), dtype=_F32, device=device),
+                   steric=torch.empty((T, H, W), dtype=_F32, device=device) if fields else None,
+                   fluid_velocity=torch.empty((T, 2, H, W), dtype=_F32, device=device) if fields else None,
+                   every=every)
+
+    def struct(self):
+        r = _lib.McRecord()
+        r.position = self.position.data_ptr() if self.position is not None else None
+        r.velocity = self.velocity.data_ptr() if self.velocity is not None else None
+        r.steric = self.steric.data_ptr() if self.steric is not None else None
+        r.fluid_velocity = self.fluid_velocity.data_ptr() if self.fluid_velocity is not None else None
+        r.every = int(self.every)
+        return r
+
+
+class Plan:
+    """A bound plan for a list of rollouts (dims + config + dt + topology each)."""
+
+    def __init__(self, specs, device="cuda"):
+        """specs: list of (H, W, N, pairs(E,2) int32, bending_pairs(B,2) int32, cfg, dt)."""
+        _require_cuda()
+        lib = _lib.load()
+        n = len(specs)
+        dims = (_lib.McDims * n)()
+        cfgs = (_lib.McConfig * n)()
+        dts = (ctypes.c_float * n)()
+        self._keep = []
+        pp = (_lib.c_int_p * n)()
+        bp = (_lib.c_int_p * n)()
+        for i, (H, W, N, pairs, bpairs, cfg, dt) in enumerate(specs):
+            pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+            bpairs = np.ascontiguousarray(bpairs, dtype=np.int32).reshape(-1, 2)
+            self._keep += [pairs, bpairs]
+            dims[i] = _lib.McDims(int(H), int(W), int(N), pairs.shape[0], bpairs.shape[0])
+            cfgs[i] = mc_config(cfg)
+            dts[i] = float(dt)
+            pp[i] = pairs.ctypes.data_as(_lib.c_int_p)
+            bp[i] = bpairs.ctypes.data_as(_lib.c_int_p)
+        h = ctypes.c_void_p()
+        _lib.check(lib.mc_plan_create(n, dims, cfgs, dts, pp, bp, ctypes.byref(h)))
+        self._h = h
+        self.n = n
+        self.specs = specs
+        nbytes = lib.mc_plan_workspace_bytes(h)
+        self.workspace = torch.empty(nbytes + 256, dtype=torch.uint8, device=device)
+        base = self.workspace.data_ptr()
+        self._ws_ptr = (base + 255) // 256 * 256
+        self.workspace_bytes = nbytes
+        stream = torch.cuda.current_stream().cuda_stream
+        _lib.check(lib.mc_plan_bind(h, ctypes.c_void_p(self._ws_ptr), nbytes, ctypes.c_void_p(stream)))
+
+    @classmethod
+    def for_states(cls, states, cfgs, dts, device="cuda"):
+        specs = [(s.H, s.W, s.N, s.pairs, s.bending_pairs, c, d) for s, c, d in zip(states, cfgs, dts)]
+        return cls(specs, device=device)
+
+    def rollout(self, states, num_steps, actuations=None, records=None, use_graph=True, stream=None):
+        lib = _lib.load()
+        n = self.n
+        if len(states) != n:
+            raise ValueError(f"plan has {n} rollouts, got {len(states)} states")
+        st = (_lib.McState * n)()
+        for i, s in enumerate(states):
+            st[i] = s.struct()
+        act_arr = None
+        if actuations is not None and any(a is not None for a in actuations):
+            structs = [a.struct() if a is not None else None for a in actuations]
+            self._act_structs = structs
+            act_arr = (ctypes.POINTER(_lib.McActuation) * n)(
+                *[ctypes.pointer(s) if s is not None else ctypes.POINTER(_lib.McActuation)() for s in structs])
+        rec_arr = None
+        if records is not None and any(r is not None for r in records):
+            structs = [r.struct() if r is not None else None for r in records]
+            self._rec_structs = structs
+            rec_arr = (ctypes.POINTER(_lib.McRecord) * n)(
+                *[ctypes.pointer(s) if s is not None else ctypes.POINTER(_lib.McRecord)() for s in structs])
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        _lib.check(lib.mc_rollout(self._h, st, int(num_steps), act_arr, rec_arr, int(bool(use_graph)),
+                                  ctypes.c_void_p(s)))
+
+    def read_flags(self, clear=False):
+        lib = _lib.load()
+        out = (ctypes.c_uint32 * self.n)()
+        s = torch.cuda.current_stream().cuda_stream
+        _lib.check(lib.mc_plan_read_flags(self._h, out, int(bool(clear)), ctypes.c_void_p(s)))
+        return list(out)
+
+    def last_launch_count(self):
+        return int(_lib.load().mc_plan_last_launch_count(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().mc_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,116 @@
+"""C ABI checks that need no GPU: the in-tree library loads, exports every function that
+include/microcosmos_b200.h declares, and validates plans on the host (mc_plan_create
+touches no device)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from microcosmos_b200 import _lib, baseline_config, scenarios
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(REPO, "include", "microcosmos_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(mc_[a-z_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from microcosmos_b200 import build
+    build.build()
+    return _lib.load()
+
+
+def test_exports_every_declared_symbol(lib):
+    names = header_functions()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(_lib.SIGNATURES) == set(names)
+
+
+def test_version(lib):
+    assert b"sm_100a" in lib.mc_version()
+
+
+def _create(specs):
+    lib = _lib.load()
+    from microcosmos_b200.engine import mc_config
+    n = len(specs)
+    dims = (_lib.McDims * n)()
+    cfgs = (_lib.McConfig * n)()
+    dts = (ctypes.c_float * n)()
+    pp = (_lib.c_int_p * n)()
+    bp = (_lib.c_int_p * n)()
+    keep = []
+    for i, (H, W, N, pairs, bpairs, cfg, dt) in enumerate(specs):
+        pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1, 2)
+        bpairs = np.ascontiguousarray(bpairs, np.int32).reshape(-1, 2)
+        keep += [pairs, bpairs]
+        dims[i] = _lib.McDims(H, W, N, pairs.shape[0], bpairs.shape[0])
+        cfgs[i] = mc_config(cfg)
+        dts[i] = dt
+        pp[i] = pairs.ctypes.data_as(_lib.c_int_p)
+        bp[i] = bpairs.ctypes.data_as(_lib.c_int_p)
+    h = ctypes.c_void_p()
+    st = lib.mc_plan_create(n, dims, cfgs, dts, pp, bp, ctypes.byref(h))
+    return st, h
+
+
+def test_plan_create_and_workspace_size(lib):
+    sc = scenarios.make_scenario(64, 64, 3, 20, seed=0)
+    st, h = _create([(64, 64, sc.N, sc.pairs, sc.bending_pairs, baseline_config(), 0.01)])
+    assert st == _lib.MC_OK, lib.mc_last_error()
+    nbytes = lib.mc_plan_workspace_bytes(h)
+    # two population buffers dominate: 2 * 9 * 64 * 64 * 4 bytes
+    assert nbytes > 2 * 9 * 64 * 64 * 4
+    lib.mc_plan_destroy(h)
+
+
+def test_plan_rejects_bad_topology(lib):
+    sc = scenarios.make_scenario(32, 32, 1, 10, seed=0)
+    bad = sc.pairs.copy()
+    bad[3, 1] = sc.N + 5
+    st, _ = _create([(32, 32, sc.N, bad, sc.bending_pairs, baseline_config(), 0.01)])
+    assert st == _lib.MC_ERR_INVALID
+    assert b"outside" in lib.mc_last_error()
+    badb = sc.bending_pairs.copy()
+    badb[0, 0] = -1
+    st, _ = _create([(32, 32, sc.N, sc.pairs, badb, baseline_config(), 0.01)])
+    assert st == _lib.MC_ERR_INVALID
+
+
+def test_plan_rejects_unsupported_config(lib):
+    sc = scenarios.make_scenario(32, 32, 1, 10, seed=0)
+    import dataclasses
+    st, _ = _create([(32, 32, sc.N, sc.pairs, sc.bending_pairs,
+                      dataclasses.replace(baseline_config(), synthetic_node_width=1.0), 0.01)])
+    assert st == _lib.MC_ERR_UNSUPPORTED
+    # steric FFT sizes need prime factors <= 13
+    st, _ = _create([(34, 34, sc.N, sc.pairs, sc.bending_pairs, baseline_config(), 0.01)])
+    assert st == _lib.MC_ERR_UNSUPPORTED
+    st, _ = _create([(34, 34, sc.N, sc.pairs, sc.bending_pairs,
+                      dataclasses.replace(baseline_config(), enable_steric=False), 0.01)])
+    assert st == _lib.MC_OK
+    st, _ = _create([(32, 32, sc.N, sc.pairs, sc.bending_pairs, baseline_config(), 0.0)])
+    assert st == _lib.MC_ERR_INVALID
+
+
+def test_stable_cosserat_plugin_is_rejected():
+    from microcosmos_b200 import COSSERAT_SCHEME
+    from microcosmos_b200.engine import mc_config
+    with pytest.raises(NotImplementedError):
+        mc_config(COSSERAT_SCHEME)
+
+
+def test_batch_plan_of_uneven_rollouts(lib):
+    scs = [scenarios.make_scenario(s, s, f, n, seed=i) for i, (s, f, n) in
+           enumerate([(128, 3, 16), (192, 1, 100), (64, 5, 30)])]
+    st, h = _create([(s.H, s.W, s.N, s.pairs, s.bending_pairs, baseline_config(), 0.01) for s in scs])
+    assert st == _lib.MC_OK, lib.mc_last_error()
+    lib.mc_plan_destroy(h)
