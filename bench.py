@@ -1,0 +1,352 @@
+"""Benchmark: lattice MLUPS of the microcosmos per-step physics hot path on B200.
+
+Workload (default): the plain method at scale — one 1024x1024 periodic D2Q9 TRT fp32
+lattice, 256 filaments x 64 nodes (Poisson-disk centres, min sep 8), steric FFT on the
+same grid, 4-point IB, 20 PBD iterations, curvature actuation amp ~U(0.1,0.3),
+period ~U(100,400), dt = 0.01.  A "step" is one simulate.step of that instance.
+
+  value      MLUPS = cells x steps / device time, state resident in HBM, L2 flushed
+             (256 MiB write) between timed steps, each step timed with CUDA events
+  e2e        MLUPS through the reference-facing run() API with pinned host inputs and
+             host outputs (H2D of the state, the rollout, D2H of the final state)
+  roofline   the dense stream+collide kernel: 72 B/cell algorithmic traffic per launch
+             / its CUDA-event duration (L2 flushed before every step)
+  cpu_baseline  the numpy restatement (oracle) on a bounded sample of the same workload
+
+--impl reference times the reference's CPU path (its numpy restatement, since JAX is not
+installed) on the same workload, metric and unit.
+
+Multi-GPU: rollouts do not exchange data, so N GPUs run N independent replicas
+("scaling": "weak"); value = total cells x steps / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "lattice MLUPS & rollouts/s batched vs plain on 1 B200; p50/p99 latency"
+BYTES_PER_CELL = 72  # 9 fp32 populations read + 9 written per cell per step
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="scale", choices=["scale", "small"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=100)
+    return ap.parse_args()
+
+
+def workload(name, seed):
+    from microcosmos_b200 import scenarios
+    if name == "scale":
+        return scenarios.config_scale(seed=seed), {
+            "workload": "plain method at scale: 1024x1024 periodic D2Q9 TRT fp32, 256 filaments x 64 nodes "
+                        "(Poisson-disk, min sep 8), steric FFT 1024^2, 4-pt IB, 20 PBD iterations, dt 0.01",
+            "grid": [1024, 1024], "filaments": 256, "nodes_per_filament": 64}
+    return scenarios.config_small(seed=seed), {
+        "workload": "plain method small: 128x128 periodic D2Q9 TRT fp32, 4 filaments x 32 nodes, dt 0.01",
+        "grid": [128, 128], "filaments": 4, "nodes_per_filament": 32}
+
+
+def measured_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(kernel, H, W):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, scaled to H*W."""
+    p = os.path.join(HERE, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    e = d.get(kernel)
+    if not e:
+        return None
+    return float(e["dram_bytes_per_launch"]) * (H * W) / float(e["cells"])
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(sc, cfg_steps_budget_s=15.0):
+    """Oracle (numpy restatement, single process) on a bounded sample of the workload."""
+    from oracle import ref_numpy as O
+    s = O.state_from_scenario(sc)
+    act = (sc.act_c, sc.act_amp, sc.act_omega, sc.act_phase)
+    cfg = O.Config()
+    t0 = time.perf_counter()
+    s, _ = O.simulate(s, cfg, 0.01, 1, act=act, t0=0)
+    t1 = time.perf_counter() - t0
+    n = int(max(1, min(50, cfg_steps_budget_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    s, _ = O.simulate(s, cfg, 0.01, n, act=act, t0=1)
+    dt = time.perf_counter() - t0
+    cells = sc.H * sc.W
+    return {"value": cells * n / dt / 1e6, "unit": "MLUPS", "cores": 1, "kind": "port",
+            "sample": f"{n} steps of the {sc.H}x{sc.W} workload after 1 warm-up step (numpy restatement, not JAX; "
+                      f"{dt:.1f} s)", "seconds_per_step": dt / n}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    sc, cfgj = workload(args.config, 0)
+    from oracle import ref_numpy as O
+    s = O.state_from_scenario(sc)
+    act = (sc.act_c, sc.act_amp, sc.act_omega, sc.act_phase)
+    cfg = O.Config()
+    # warm-up then a bounded number of timed steps (the reference CPU path is ~1 s/step at 1024^2)
+    w = max(1, min(args.warmup, 2))
+    s, _ = O.simulate(s, cfg, 0.01, w, act=act)
+    t0 = time.perf_counter()
+    k = 1
+    s, _ = O.simulate(s, cfg, 0.01, 1, act=act, t0=w)
+    per = time.perf_counter() - t0
+    k_more = int(max(0, min(args.steps - 1, 60.0 / max(per, 1e-6) - 1)))
+    if k_more:
+        s, _ = O.simulate(s, cfg, 0.01, k_more, act=act, t0=w + 1)
+        k += k_more
+    dt = time.perf_counter() - t0
+    v = sc.H * sc.W * k / dt / 1e6
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus, "steps": k,
+        "warmup": w, "ms_per_step": dt / k * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy.random)", "config": cfgj,
+        "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": 1, "kind": "port",
+                         "sample": f"{k} steps of the {sc.H}x{sc.W} workload (numpy restatement of the reference "
+                                   f"step; JAX is not installed, so the reference itself cannot run)"},
+        "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from microcosmos_b200 import baseline_config
+    from microcosmos_b200.engine import Actuation, DeviceState, Plan
+    from microcosmos_b200.simulate import run as api_run
+    from microcosmos_b200.structs import Edges, Fields, Nodes
+
+    sc, cfgj = workload(args.config, rank)
+    cfg = baseline_config()
+    H, W = sc.H, sc.W
+    cells = H * W
+    st = DeviceState.from_scenario(sc)
+    act = Actuation.from_scenario(sc)
+    plan = Plan.for_states([st], [cfg], [0.01])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    # ---------------- device-resident timed region
+    plan.begin([st], actuations=[act])
+    plan.advance(args.warmup, use_graph=True)
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    # last_launch_count accumulates over the begin/advance calls of one rollout
+    launches0 = plan.last_launch_count()
+    for i in range(K):
+        flush.zero_()
+        ev[i][0].record(stream)
+        plan.advance(1, use_graph=True, last=(i == K - 1))
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if ws > 1:
+        dist.barrier()
+    launches = plan.last_launch_count() - launches0
+    plan.end()
+    torch.cuda.synchronize()
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_ms = float(t.item())
+    flags = plan.read_flags()
+
+    # ---------------- per-kernel event pass (roofline), L2 flushed before each step
+    st2 = DeviceState.from_scenario(sc)
+    plan.profile(True)
+    plan.begin([st2], actuations=[act])
+    plan.advance(2, use_graph=False)
+    plan.profile_reset()
+    P = args.profile_steps
+    for i in range(P):
+        flush.zero_()
+        plan.advance(1, use_graph=False, last=(i == P - 1))
+    plan.end()
+    torch.cuda.synchronize()
+    prof = plan.profile_read()
+    plan.profile(False)
+    step_kernel_ms = sum(ms for ms, n in prof.values())
+    per_step = {k: {"ms_per_launch": ms / n, "launches_per_step": n / P, "share": ms / step_kernel_ms}
+                for k, (ms, n) in prof.items() if n}
+    lbm_ms, lbm_n = prof["lbm"]
+    lbm_s = lbm_ms / lbm_n / 1e3
+    achieved = BYTES_PER_CELL * cells / lbm_s / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = committed_traffic("lbm", H, W)
+
+    # ---------------- end to end through the reference-facing API (host buffers)
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    hn = Nodes(position=pinned(sc.position), velocity=pinned(sc.velocity), color_bend=pinned(np.zeros(sc.N, np.float32)),
+               debug_vector=pinned(np.zeros((sc.N, 2), np.float32)))
+    he = Edges(pairs=sc.pairs, theta=pinned(sc.theta), rest_lengths=pinned(sc.rest_lengths),
+               bending_pairs=sc.bending_pairs, bending_rest_angles=pinned(sc.bending_rest_angles),
+               bending_stiffness=pinned(sc.bending_stiffness))
+    hf = Fields(grid_shape=(H, W), steric=pinned(sc.steric), fluid_velocity=pinned(sc.fluid_velocity),
+                f_grid=pinned(sc.f_grid))
+    actn = (sc.act_c, sc.act_amp, sc.act_omega, sc.act_phase)
+    outs = {k: torch.empty(s, dtype=torch.float32).pin_memory() for k, s in
+            (("position", (sc.N, 2)), ("velocity", (sc.N, 2)), ("theta", (sc.E,)), ("f_grid", (9, H, W)),
+             ("steric", (H, W)), ("fluid_velocity", (2, H, W)))}
+    api_run(hn, he, hf, 0.01, 4, cfg, actuation=actn)  # plan/graph warm-up
+    torch.cuda.synchronize()
+    Ke = K
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    n_, e_, f_ = api_run(hn, he, hf, 0.01, Ke, cfg, actuation=actn)
+    outs["position"].copy_(n_.position)
+    outs["velocity"].copy_(n_.velocity)
+    outs["theta"].copy_(e_.theta)
+    outs["f_grid"].copy_(f_.f_grid)
+    outs["steric"].copy_(f_.steric)
+    outs["fluid_velocity"].copy_(f_.fluid_velocity)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    te = e0.elapsed_time(e1)
+    h2d = sum(int(np.asarray(a).nbytes) for a in (sc.position, sc.velocity, sc.theta, sc.rest_lengths,
+                                                   sc.bending_rest_angles, sc.bending_stiffness, sc.f_grid,
+                                                   sc.steric, sc.fluid_velocity))
+    d2h = sum(int(v.numel() * 4) for v in outs.values())
+    te_t = torch.tensor([te], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(te_t, op=dist.ReduceOp.MAX)
+    te = float(te_t.item())
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(sc)
+
+    if rank == 0:
+        value = cells * K * ws / (t_ms / 1e3) / 1e6
+        out = {
+            "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": ws, "steps": K, "warmup": args.warmup,
+            "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded numpy.random, BASELINE config shapes)",
+            "config": dict(cfgj, l2="flushed (256 MiB write) before every timed step; each step timed alone with "
+                                    "CUDA events", parallelism=f"replicas x{ws}", dt=0.01,
+                           timed="device-resident: one graph-launched simulate.step per event pair"),
+            "e2e": {"value": cells * Ke * ws / (te / 1e3) / 1e6, "unit": "MLUPS",
+                    "h2d_bytes_per_step": h2d / Ke, "d2h_bytes_per_step": d2h / Ke, "steps_per_call": Ke,
+                    "h2d_bytes_per_call": h2d, "d2h_bytes_per_call": d2h,
+                    "api": "microcosmos_b200.simulate.run (pinned host inputs -> host outputs)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_lbm<4> (fused pull stream + TRT/Guo collide)",
+                         "algorithmic_bytes_per_launch": BYTES_PER_CELL * cells,
+                         "ms_per_launch": lbm_s * 1e3},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": int(launches),
+            "kernels": per_step,
+            "flags": flags,
+            "step_kernel_ms": step_kernel_ms / P,
+        }
+        print(json.dumps(out))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

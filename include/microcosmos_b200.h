@@ -140,6 +140,16 @@ mc_status mc_rollout(mc_plan* plan, const mc_state* states, int32_t num_steps,
                      const mc_actuation* const* act, const mc_record* const* rec,
                      int32_t use_graph, void* stream);
 
+/* The three phases of mc_rollout, for callers that interleave their own work between
+ * steps (timing, L2 flushes, host control).  begin: bind states/actuation/recording and
+ * convert fields.f_grid to the internal layout; advance: run num_steps more steps
+ * (last != 0: the final one of them writes fields.fluid_velocity); end: write
+ * fields.f_grid back.  mc_rollout(...) == begin + advance(num_steps, last=1) + end. */
+mc_status mc_rollout_begin(mc_plan* plan, const mc_state* states, const mc_actuation* const* act,
+                           const mc_record* const* rec, void* stream);
+mc_status mc_rollout_advance(mc_plan* plan, int32_t num_steps, int32_t use_graph, int32_t last, void* stream);
+mc_status mc_rollout_end(mc_plan* plan, void* stream);
+
 /* One step: mc_rollout with num_steps = 1 (src/microcosmos/simulate.py:37-100). */
 mc_status mc_step(mc_plan* plan, const mc_state* states, void* stream);
 
@@ -150,6 +160,15 @@ mc_status mc_plan_read_flags(mc_plan* plan, uint32_t* flags, int32_t clear, void
 /* Number of kernel launches the last mc_rollout() enqueued (graph replays count the
  * kernels inside the graph). */
 int64_t mc_plan_last_launch_count(const mc_plan* plan);
+
+/* Per-kernel CUDA-event timing.  While enabled, steps are launched directly (no graph)
+ * and each kernel launch is bracketed by two events; mc_plan_profile_read() returns the
+ * accumulated milliseconds and launch count of one kernel (names from
+ * mc_profile_kernel_names(), comma-separated) and synchronises on pending events. */
+mc_status mc_plan_profile(mc_plan* plan, int32_t enable);
+mc_status mc_plan_profile_read(mc_plan* plan, const char* kernel, double* total_ms, int64_t* launches);
+mc_status mc_plan_profile_reset(mc_plan* plan);
+const char* mc_profile_kernel_names(void);
 
 /* Text of the last error of this thread ("" if none). */
 const char* mc_last_error(void);

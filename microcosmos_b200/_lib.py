@@ -83,7 +83,18 @@ SIGNATURES = {
     "mc_rollout": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(McState), ctypes.c_int32,
                                   ctypes.POINTER(ctypes.POINTER(McActuation)),
                                   ctypes.POINTER(ctypes.POINTER(McRecord)), ctypes.c_int32, ctypes.c_void_p]),
+    "mc_rollout_begin": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(McState),
+                                        ctypes.POINTER(ctypes.POINTER(McActuation)),
+                                        ctypes.POINTER(ctypes.POINTER(McRecord)), ctypes.c_void_p]),
+    "mc_rollout_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_void_p]),
+    "mc_rollout_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "mc_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(McState), ctypes.c_void_p]),
+    "mc_plan_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "mc_plan_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_int64)]),
+    "mc_plan_profile_reset": (ctypes.c_int, [ctypes.c_void_p]),
+    "mc_profile_kernel_names": (ctypes.c_char_p, []),
     "mc_plan_read_flags": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int32,
                                           ctypes.c_void_p]),
     "mc_plan_last_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),

@@ -82,10 +82,24 @@ struct mc_plan {
   int node_bs = 32;
   std::vector<RDesc> desc;
   cudaStream_t cap_stream = nullptr;
-  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // 0: no field recording, 1: steric, 2: steric + fluid
-  int64_t graph_kernels = 0;
+  // CUDA graphs, keyed by [steps-1][parity][recording variant][write_u]
+  cudaGraphExec_t graph[2][2][3][2] = {};
+  int64_t graph_kernels[2][2][3][2] = {};
   int64_t last_launches = 0;
-  int64_t step_kernels = 0;
+  // rollout in progress (mc_rollout_begin .. mc_rollout_end)
+  bool active = false;
+  int step = 0;
+  int rec_fields = 0, rec_fluid = 0;
+  // per-kernel CUDA-event profiling (direct launches only)
+  bool profiling = false;
+  struct Ev {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Ev> ev_pending;
+  std::vector<cudaEvent_t> ev_pool;
+  double prof_ms[32] = {};
+  int64_t prof_n[32] = {};
 };
 
 namespace {
@@ -402,39 +416,136 @@ mc::Launch L(mc_plan* p, Kind k, cudaStream_t s) {
   return l;
 }
 
+const char* const kProfNames[] = {"predict", "cic_scan", "cic_scatter", "cic_sort", "fft_rows", "fft_cols",
+                                   "node", "ib_scan", "ib_scatter", "ib_sort", "ib_interp", "ib_spread",
+                                   "ib_finalize", "lbm", "reaction", "record_fields", "tick"};
+constexpr int kNumProf = sizeof(kProfNames) / sizeof(kProfNames[0]);
+
+cudaEvent_t take_event(mc_plan* p) {
+  if (!p->ev_pool.empty()) {
+    cudaEvent_t e = p->ev_pool.back();
+    p->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  return e;
+}
+
+// Runs `launch` bracketed by two events when profiling (direct launches only).
+template <typename F>
+void timed(mc_plan* p, int kind, cudaStream_t s, bool capture, F&& launch) {
+  if (!p->profiling || capture) {
+    launch();
+    return;
+  }
+  cudaEvent_t a = take_event(p), b = take_event(p);
+  if (!a || !b) {
+    launch();
+    return;
+  }
+  cudaEventRecord(a, s);
+  launch();
+  cudaEventRecord(b, s);
+  p->ev_pending.push_back({kind, a, b});
+}
+
 // The launch sequence of one step (src/microcosmos/simulate.py:37-100).
-int64_t enqueue_step(mc_plan* p, int parity, int write_u, int rec_fields, cudaStream_t s) {
+int64_t enqueue_step(mc_plan* p, int parity, int write_u, int rec_fields, cudaStream_t s, bool capture) {
   int* tdev = at<int>(p->ws, p->r_tdev);
   int64_t k = 0;
-  if (p->grid[K_NODES]) { mc::launch_predict(L(p, K_NODES, s)); ++k; }
+  if (p->grid[K_NODES]) {
+    timed(p, 0, s, capture, [&] { mc::launch_predict(L(p, K_NODES, s)); });
+    ++k;
+  }
   if (p->any_steric) {
-    mc::launch_bin_scan(L(p, K_CIC, s), 1);
-    mc::launch_bin_scatter(L(p, K_CIC, s), 1);
-    mc::launch_bin_sort(L(p, K_TILES, s), 1, parity);
-    mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem);
-    mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem);
+    timed(p, 1, s, capture, [&] { mc::launch_bin_scan(L(p, K_CIC, s), 1); });
+    timed(p, 2, s, capture, [&] { mc::launch_bin_scatter(L(p, K_CIC, s), 1); });
+    timed(p, 3, s, capture, [&] { mc::launch_bin_sort(L(p, K_TILES, s), 1, parity); });
+    timed(p, 4, s, capture, [&] { mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem); });
+    timed(p, 5, s, capture, [&] { mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem); });
     k += 5;
   }
-  if (p->grid[K_COMP]) { mc::launch_node(L(p, K_COMP, s), tdev, p->node_smem, p->node_bs); ++k; }
+  if (p->grid[K_COMP]) {
+    timed(p, 6, s, capture, [&] { mc::launch_node(L(p, K_COMP, s), tdev, p->node_smem, p->node_bs); });
+    ++k;
+  }
   if (p->any_fluid) {
-    mc::launch_bin_scan(L(p, K_IB, s), 0);
-    mc::launch_bin_scatter(L(p, K_IB, s), 0);
-    mc::launch_bin_sort(L(p, K_TILES, s), 0, parity);
+    timed(p, 7, s, capture, [&] { mc::launch_bin_scan(L(p, K_IB, s), 0); });
+    timed(p, 8, s, capture, [&] { mc::launch_bin_scatter(L(p, K_IB, s), 0); });
+    timed(p, 9, s, capture, [&] { mc::launch_bin_sort(L(p, K_TILES, s), 0, parity); });
     k += 3;
     for (int it = 0; it < p->max_iters; ++it) {
-      mc::launch_ib_interp(L(p, K_NODES, s), it);
-      mc::launch_ib_spread(L(p, K_IB, s), it);
+      timed(p, 10, s, capture, [&] { mc::launch_ib_interp(L(p, K_NODES, s), it); });
+      timed(p, 11, s, capture, [&] { mc::launch_ib_spread(L(p, K_IB, s), it); });
       k += 2;
     }
-    mc::launch_ib_finalize(L(p, K_IB, s));
-    mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->R[0].vec);
+    timed(p, 12, s, capture, [&] { mc::launch_ib_finalize(L(p, K_IB, s)); });
+    timed(p, 13, s, capture, [&] { mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->R[0].vec); });
     k += 2;
   }
-  if (p->grid[K_NODES]) { mc::launch_reaction(L(p, K_NODES, s), tdev); ++k; }
-  if (rec_fields) { mc::launch_record_fields(L(p, K_CELLS, s), tdev); ++k; }
-  mc::launch_tick(tdev, s);
+  if (p->grid[K_NODES]) {
+    timed(p, 14, s, capture, [&] { mc::launch_reaction(L(p, K_NODES, s), tdev); });
+    ++k;
+  }
+  if (rec_fields) {
+    timed(p, 15, s, capture, [&] { mc::launch_record_fields(L(p, K_CELLS, s), tdev); });
+    ++k;
+  }
+  timed(p, 16, s, capture, [&] { mc::launch_tick(tdev, s); });
   ++k;
   return k;
+}
+
+mc_status run_steps(mc_plan* p, int num, int use_graph, int last, cudaStream_t s, int64_t& launches) {
+  const int recv = p->rec_fields ? (p->rec_fluid ? 2 : 1) : 0;
+  int remaining = num;
+  while (remaining > 0) {
+    const int parity = p->step & 1;
+    const bool is_last = last && remaining == 1;
+    const int write_u = (is_last || p->rec_fluid) ? 1 : 0;
+    if (use_graph && !p->profiling) {
+      const int ns = (parity == 0 && remaining >= 3) ? 2 : 1;
+      const int wu = ns == 2 ? p->rec_fluid : write_u;
+      cudaGraphExec_t& g = p->graph[ns - 1][parity][recv][wu];
+      if (!g) {
+        cudaGraph_t graph;
+        MC_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
+        int64_t kk = 0;
+        for (int j = 0; j < ns; ++j)
+          kk += enqueue_step(p, (parity + j) & 1, wu, p->rec_fields, p->cap_stream, true);
+        cudaError_t e = cudaStreamEndCapture(p->cap_stream, &graph);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&g, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+          g = nullptr;
+          return cuda_fail(e, "cudaGraphInstantiate");
+        }
+        p->graph_kernels[ns - 1][parity][recv][wu] = kk;
+      }
+      MC_CUDA(cudaGraphLaunch(g, s));
+      launches += p->graph_kernels[ns - 1][parity][recv][wu];
+      p->step += ns;
+      remaining -= ns;
+      continue;
+    }
+    launches += enqueue_step(p, parity, write_u, p->rec_fields, s, false);
+    p->step += 1;
+    remaining -= 1;
+  }
+  return MC_OK;
+}
+
+void destroy_graphs(mc_plan* p) {
+  for (auto& a : p->graph)
+    for (auto& b : a)
+      for (auto& c : b)
+        for (auto& g : c)
+          if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+          }
 }
 
 }  // namespace
@@ -616,8 +727,12 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
 
 void mc_plan_destroy(mc_plan* p) {
   if (!p) return;
-  for (auto& g : p->graph)
-    if (g) cudaGraphExecDestroy(g);
+  destroy_graphs(p);
+  for (auto& e : p->ev_pending) {
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+  for (auto e : p->ev_pool) cudaEventDestroy(e);
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
   delete p;
 }
@@ -661,22 +776,18 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
   if (p->any_steric) MC_CUDA(mc::fft_set_smem(p->fftr_smem, p->fftc_smem));
   mc::launch_clear_ws(L(p, K_CELLS, s));
   MC_CUDA(cudaGetLastError());
-  for (auto& g : p->graph)
-    if (g) {
-      cudaGraphExecDestroy(g);
-      g = nullptr;
-    }
+  destroy_graphs(p);
   if (!p->cap_stream) MC_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
   p->bound = true;
   return MC_OK;
 }
 
-mc_status mc_rollout(mc_plan* p, const mc_state* states, int32_t num_steps, const mc_actuation* const* act,
-                     const mc_record* const* rec, int32_t use_graph, void* stream) {
+mc_status mc_rollout_begin(mc_plan* p, const mc_state* states, const mc_actuation* const* act,
+                           const mc_record* const* rec, void* stream) {
   g_err.clear();
   if (!p) return fail(MC_ERR_INVALID, "null plan");
   if (!p->bound) return fail(MC_ERR_NOT_BOUND, "mc_plan_bind() was not called");
-  if (!states || num_steps < 0) return fail(MC_ERR_INVALID, "null states or negative num_steps");
+  if (!states) return fail(MC_ERR_INVALID, "null states");
   cudaStream_t s = (cudaStream_t)stream;
   int rec_fields = 0, rec_fluid = 0;
   for (int i = 0; i < p->n; ++i) {
@@ -700,49 +811,104 @@ mc_status mc_rollout(mc_plan* p, const mc_state* states, int32_t num_steps, cons
   }
   MC_CUDA(cudaMemcpyAsync(p->ws + p->r_desc.off, p->desc.data(), p->desc.size() * sizeof(RDesc),
                           cudaMemcpyHostToDevice, s));
-  int* tdev = at<int>(p->ws, p->r_tdev);
-  MC_CUDA(cudaMemsetAsync(tdev, 0, sizeof(int), s));
-  int64_t launches = 0;
+  MC_CUDA(cudaMemsetAsync(at<int>(p->ws, p->r_tdev), 0, sizeof(int), s));
+  p->rec_fields = rec_fields;
+  p->rec_fluid = rec_fluid;
+  p->step = 0;
+  p->active = true;
+  p->last_launches = 0;
   if (p->any_fluid) {
     mc::launch_unstream(L(p, K_CELLS, s));
-    ++launches;
-  }
-  int step = 0;
-  while (step < num_steps) {
-    const bool pair_ok = use_graph && (step % 2 == 0) && (step + 2 <= num_steps - 1);
-    if (pair_ok) {
-      cudaGraphExec_t& g = p->graph[rec_fields ? (rec_fluid ? 2 : 1) : 0];
-      if (!g) {
-        cudaGraph_t graph;
-        MC_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
-        int64_t k0 = enqueue_step(p, 0, rec_fluid, rec_fields, p->cap_stream);
-        int64_t k1 = enqueue_step(p, 1, rec_fluid, rec_fields, p->cap_stream);
-        cudaError_t e = cudaStreamEndCapture(p->cap_stream, &graph);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-        e = cudaGraphInstantiate(&g, graph, 0);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) {
-          g = nullptr;
-          return cuda_fail(e, "cudaGraphInstantiate");
-        }
-        p->graph_kernels = k0 + k1;
-      }
-      MC_CUDA(cudaGraphLaunch(g, s));
-      launches += p->graph_kernels;
-      step += 2;
-      continue;
-    }
-    const bool final = (step == num_steps - 1);
-    launches += enqueue_step(p, step & 1, (final || rec_fluid) ? 1 : 0, rec_fields, s);
-    ++step;
-  }
-  if (p->any_fluid) {
-    mc::launch_stream_out(L(p, K_CELLS, s), num_steps & 1);
-    ++launches;
+    p->last_launches += 1;
   }
   MC_CUDA(cudaGetLastError());
-  p->last_launches = launches;
   return MC_OK;
+}
+
+mc_status mc_rollout_advance(mc_plan* p, int32_t num_steps, int32_t use_graph, int32_t last, void* stream) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (!p->active) return fail(MC_ERR_INVALID, "mc_rollout_begin() was not called");
+  if (num_steps < 0) return fail(MC_ERR_INVALID, "negative num_steps");
+  int64_t launches = 0;
+  mc_status st = run_steps(p, num_steps, use_graph, last, (cudaStream_t)stream, launches);
+  p->last_launches += launches;
+  if (st != MC_OK) return st;
+  MC_CUDA(cudaGetLastError());
+  return MC_OK;
+}
+
+mc_status mc_rollout_end(mc_plan* p, void* stream) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (!p->active) return fail(MC_ERR_INVALID, "mc_rollout_begin() was not called");
+  if (p->any_fluid) {
+    mc::launch_stream_out(L(p, K_CELLS, (cudaStream_t)stream), p->step & 1);
+    p->last_launches += 1;
+  }
+  p->active = false;
+  MC_CUDA(cudaGetLastError());
+  return MC_OK;
+}
+
+mc_status mc_rollout(mc_plan* p, const mc_state* states, int32_t num_steps, const mc_actuation* const* act,
+                     const mc_record* const* rec, int32_t use_graph, void* stream) {
+  if (num_steps < 0) return fail(MC_ERR_INVALID, "negative num_steps");
+  mc_status st = mc_rollout_begin(p, states, act, rec, stream);
+  if (st != MC_OK) return st;
+  st = mc_rollout_advance(p, num_steps, use_graph, 1, stream);
+  if (st != MC_OK) {
+    p->active = false;
+    return st;
+  }
+  return mc_rollout_end(p, stream);
+}
+
+mc_status mc_plan_profile(mc_plan* p, int32_t enable) {
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  p->profiling = enable != 0;
+  return MC_OK;
+}
+
+mc_status mc_plan_profile_read(mc_plan* p, const char* kernel, double* total_ms, int64_t* launches) {
+  g_err.clear();
+  if (!p || !kernel || !total_ms || !launches) return fail(MC_ERR_INVALID, "null argument");
+  for (auto& e : p->ev_pending) {
+    float ms = 0.f;
+    MC_CUDA(cudaEventSynchronize(e.b));
+    MC_CUDA(cudaEventElapsedTime(&ms, e.a, e.b));
+    p->prof_ms[e.kind] += ms;
+    p->prof_n[e.kind] += 1;
+    p->ev_pool.push_back(e.a);
+    p->ev_pool.push_back(e.b);
+  }
+  p->ev_pending.clear();
+  for (int k = 0; k < kNumProf; ++k)
+    if (std::strcmp(kProfNames[k], kernel) == 0) {
+      *total_ms = p->prof_ms[k];
+      *launches = p->prof_n[k];
+      return MC_OK;
+    }
+  return fail(MC_ERR_INVALID, std::string("unknown kernel name ") + kernel);
+}
+
+mc_status mc_plan_profile_reset(mc_plan* p) {
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  for (int k = 0; k < 32; ++k) {
+    p->prof_ms[k] = 0.0;
+    p->prof_n[k] = 0;
+  }
+  return MC_OK;
+}
+
+const char* mc_profile_kernel_names(void) {
+  static std::string names;
+  if (names.empty())
+    for (int k = 0; k < kNumProf; ++k) {
+      if (k) names += ",";
+      names += kProfNames[k];
+    }
+  return names.c_str();
 }
 
 mc_status mc_step(mc_plan* p, const mc_state* states, void* stream) {

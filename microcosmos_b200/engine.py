@@ -223,8 +223,7 @@ class Plan:
         specs = [(s.H, s.W, s.N, s.pairs, s.bending_pairs, c, d) for s, c, d in zip(states, cfgs, dts)]
         return cls(specs, device=device)
 
-    def rollout(self, states, num_steps, actuations=None, records=None, use_graph=True, stream=None):
-        lib = _lib.load()
+    def _arrays(self, states, actuations, records):
         n = self.n
         if len(states) != n:
             raise ValueError(f"plan has {n} rollouts, got {len(states)} states")
@@ -243,9 +242,46 @@ class Plan:
             self._rec_structs = structs
             rec_arr = (ctypes.POINTER(_lib.McRecord) * n)(
                 *[ctypes.pointer(s) if s is not None else ctypes.POINTER(_lib.McRecord)() for s in structs])
-        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
-        _lib.check(lib.mc_rollout(self._h, st, int(num_steps), act_arr, rec_arr, int(bool(use_graph)),
-                                  ctypes.c_void_p(s)))
+        self._st = st
+        return st, act_arr, rec_arr
+
+    @staticmethod
+    def _stream(stream):
+        return ctypes.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+
+    def rollout(self, states, num_steps, actuations=None, records=None, use_graph=True, stream=None):
+        """Run num_steps steps of every rollout (mc_rollout)."""
+        st, act_arr, rec_arr = self._arrays(states, actuations, records)
+        _lib.check(_lib.load().mc_rollout(self._h, st, int(num_steps), act_arr, rec_arr, int(bool(use_graph)),
+                                          self._stream(stream)))
+
+    def begin(self, states, actuations=None, records=None, stream=None):
+        st, act_arr, rec_arr = self._arrays(states, actuations, records)
+        _lib.check(_lib.load().mc_rollout_begin(self._h, st, act_arr, rec_arr, self._stream(stream)))
+
+    def advance(self, num_steps, use_graph=True, last=False, stream=None):
+        _lib.check(_lib.load().mc_rollout_advance(self._h, int(num_steps), int(bool(use_graph)), int(bool(last)),
+                                                  self._stream(stream)))
+
+    def end(self, stream=None):
+        _lib.check(_lib.load().mc_rollout_end(self._h, self._stream(stream)))
+
+    def profile(self, enable=True):
+        _lib.check(_lib.load().mc_plan_profile(self._h, int(bool(enable))))
+
+    def profile_reset(self):
+        _lib.check(_lib.load().mc_plan_profile_reset(self._h))
+
+    def profile_read(self):
+        """{kernel: (total_ms, launches)} of the per-kernel event timing."""
+        lib = _lib.load()
+        out = {}
+        for name in lib.mc_profile_kernel_names().decode().split(","):
+            ms = ctypes.c_double()
+            cnt = ctypes.c_int64()
+            _lib.check(lib.mc_plan_profile_read(self._h, name.encode(), ctypes.byref(ms), ctypes.byref(cnt)))
+            out[name] = (ms.value, cnt.value)
+        return out
 
     def read_flags(self, clear=False):
         lib = _lib.load()
