@@ -236,17 +236,26 @@ __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off,
         }
       }
       float sum = 0.0f;
-      for (int a = 0; a < K; ++a)
-        for (int b = 0; b < K; ++b) sum = sum + wx[a] * wy[b];
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b)
+          if (a < K && b < K) sum = sum + wx[a] * wy[b];
       const float den = sum + MC_EPSIL;
-      for (int a = 0; a < K; ++a) {
-        const int cx = imod_floor((int)(sx + (float)a), d.W);
-        for (int b = 0; b < K; ++b) {
-          const int cy = imod_floor((int)(sy + (float)b), d.H);
-          const int k = gi * K2 + a * K + b;
-          d.ib_cell[k] = cy * d.W + cx;
-          d.ib_w[k] = (wx[a] * wy[b]) / den;
-          atomicAdd(d.ib_tcount + bin_tile(d, cy, cx), 1);
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        if (a < K) {
+          const int cx = imod_floor((int)(sx + (float)a), d.W);
+#pragma unroll
+          for (int b = 0; b < 8; ++b) {
+            if (b < K) {
+              const int cy = imod_floor((int)(sy + (float)b), d.H);
+              const int k = gi * K2 + a * K + b;
+              d.ib_cell[k] = cy * d.W + cx;
+              d.ib_w[k] = (wx[a] * wy[b]) / den;
+              atomicAdd(d.ib_tcount + bin_tile(d, cy, cx), 1);
+            }
+          }
         }
       }
     }

@@ -17,18 +17,19 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 
 // One Stockham stage of radix R over `nt` transforms of length N laid out [t][N].
 // Output index of butterfly j: (j / Ns) * Ns * R + j % Ns + q * Ns.
+// Radix 2 and 4 keep their operands in registers; the odd radices (non-power-of-two
+// lengths only) use a generic R-point DFT.
 template <int R>
-__device__ void stockham_stage_r(const float2* __restrict__ in, float2* __restrict__ out, int N, int Ns,
-                                 const float2* __restrict__ tw, int nt) {
+__device__ __forceinline__ void stockham_pow2(const float2* __restrict__ in, float2* __restrict__ out, int N,
+                                              int Ns, const float2* __restrict__ tw, int nt) {
   const int S = N / R;
   const int twstep = N / (Ns * R);
-  const int rstep = N / R;
   for (int idx = threadIdx.x; idx < nt * S; idx += blockDim.x) {
     const int t = idx / S, j = idx - t * S;
     const float2* x = in + t * N;
     float2* y = out + t * N;
-    const int k = j % Ns;
-    const int dst = (j / Ns) * Ns * R + k;
+    const int k = j & (Ns - 1);
+    const int dst = (j - k) * R + k;
     float2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -39,7 +40,7 @@ __device__ void stockham_stage_r(const float2* __restrict__ in, float2* __restri
     if (R == 2) {
       y[dst] = make_float2(v[0].x + v[1].x, v[0].y + v[1].y);
       y[dst + Ns] = make_float2(v[0].x - v[1].x, v[0].y - v[1].y);
-    } else if (R == 4) {
+    } else {
       float2 a0 = make_float2(v[0].x + v[2 % R].x, v[0].y + v[2 % R].y);
       float2 a1 = make_float2(v[0].x - v[2 % R].x, v[0].y - v[2 % R].y);
       float2 b0 = make_float2(v[1].x + v[3 % R].x, v[1].y + v[3 % R].y);
@@ -50,34 +51,50 @@ __device__ void stockham_stage_r(const float2* __restrict__ in, float2* __restri
       y[dst + Ns] = make_float2(a1.x + b1m.x, a1.y + b1m.y);
       y[dst + 2 * Ns] = make_float2(a0.x - b0.x, a0.y - b0.y);
       y[dst + 3 * Ns] = make_float2(a1.x - b1m.x, a1.y - b1m.y);
-    } else {
-#pragma unroll
-      for (int q = 0; q < R; ++q) {
-        float2 acc = v[0];
-#pragma unroll
-        for (int r = 1; r < R; ++r) {
-          float2 w = __ldg(tw + ((r * q) % R) * rstep);
-          float2 p = cmul(v[r], w);
-          acc.x = acc.x + p.x;
-          acc.y = acc.y + p.y;
-        }
-        y[dst + q * Ns] = acc;
-      }
     }
   }
 }
 
-__device__ void stockham_stage(const float2* in, float2* out, int N, int R, int Ns, const float2* tw, int nt) {
-  switch (R) {
-    case 4: stockham_stage_r<4>(in, out, N, Ns, tw, nt); break;
-    case 2: stockham_stage_r<2>(in, out, N, Ns, tw, nt); break;
-    case 3: stockham_stage_r<3>(in, out, N, Ns, tw, nt); break;
-    case 5: stockham_stage_r<5>(in, out, N, Ns, tw, nt); break;
-    case 7: stockham_stage_r<7>(in, out, N, Ns, tw, nt); break;
-    case 11: stockham_stage_r<11>(in, out, N, Ns, tw, nt); break;
-    case 13: stockham_stage_r<13>(in, out, N, Ns, tw, nt); break;
-    default: break;
+__device__ __noinline__ void stockham_generic(const float2* __restrict__ in, float2* __restrict__ out, int N,
+                                              int R, int Ns, const float2* __restrict__ tw, int nt) {
+  const int S = N / R;
+  const int twstep = N / (Ns * R);
+  const int rstep = N / R;
+  for (int idx = threadIdx.x; idx < nt * S; idx += blockDim.x) {
+    const int t = idx / S, j = idx - t * S;
+    const float2* x = in + t * N;
+    float2* y = out + t * N;
+    const int k = j % Ns;
+    const int dst = (j / Ns) * Ns * R + k;
+    float2 v[13];
+#pragma unroll 1
+    for (int r = 0; r < R; ++r) {
+      float2 a = x[j + r * S];
+      if (r > 0 && k > 0) a = cmul(a, __ldg(tw + r * k * twstep));
+      v[r] = a;
+    }
+#pragma unroll 1
+    for (int q = 0; q < R; ++q) {
+      float2 acc = v[0];
+#pragma unroll 1
+      for (int r = 1; r < R; ++r) {
+        float2 p = cmul(v[r], __ldg(tw + ((r * q) % R) * rstep));
+        acc.x = acc.x + p.x;
+        acc.y = acc.y + p.y;
+      }
+      y[dst + q * Ns] = acc;
+    }
   }
+}
+
+__device__ __forceinline__ void stockham_stage(const float2* in, float2* out, int N, int R, int Ns,
+                                               const float2* tw, int nt) {
+  if (R == 4)
+    stockham_pow2<4>(in, out, N, Ns, tw, nt);
+  else if (R == 2)
+    stockham_pow2<2>(in, out, N, Ns, tw, nt);
+  else
+    stockham_generic(in, out, N, R, Ns, tw, nt);
 }
 
 // Forward FFT of nt transforms in `a` (scratch `b`); returns the buffer holding the result.
