@@ -4,12 +4,11 @@
 //
 // Scatter-adds are never done with float atomics.  Each contribution k (IB: k = n*K*K + s,
 // CIC: k = corner*N + n — the order in which the reference's scatters apply them) is
-// binned into a 16x16-cell tile (integer atomics: counts only), the tile's contributions
-// are sorted by (cell, k) in shared memory, and every run of equal cells is summed
-// sequentially in k order.  The result is bit-reproducible and equals the reference's
-// in-order scatter-add.  The IB iterations then work on the compact set of touched cells
-// ("slots", indexed by the sorted position of each cell's first contribution) instead
-// of full (H, W) grids.
+// appended to the bin of its 16x16-cell tile (an integer atomic picks the slot; a full
+// bin spills to an overflow list).  One CTA per tile then counting-sorts the bin by cell,
+// orders each cell's run by k and sums it sequentially — the reference's in-order
+// scatter-add, bit-reproducibly.  The IB iterations work on the compact list of touched
+// cells ("heads") instead of full (H, W) grids.
 #include "lbm_cell.cuh"
 
 namespace mc {
@@ -17,22 +16,22 @@ namespace mc {
 struct BinView {
   const int* cell;
   const float* w;
-  int* binned;
-  int* sorted;
+  int* store;
   int* tcount;
-  int* tfill;
-  int* toff;
+  int* ovf;
+  int* ctl;
+  int cap;
   int count;
 };
 
 __device__ __forceinline__ BinView bin_view(const RDesc& d, int which) {
   BinView v;
   if (which == 0) {
-    v.cell = d.ib_cell; v.w = d.ib_w; v.binned = d.ib_binned; v.sorted = d.ib_sorted;
-    v.tcount = d.ib_tcount; v.tfill = d.ib_tfill; v.toff = d.ib_toff; v.count = d.M;
+    v.cell = d.ib_cell; v.w = d.ib_w; v.store = d.ib_store; v.tcount = d.ib_tcount; v.ovf = d.ib_ovf;
+    v.ctl = d.ib_ctl; v.cap = d.ib_cap; v.count = d.M;
   } else {
-    v.cell = d.c_cell; v.w = d.c_w; v.binned = d.c_binned; v.sorted = d.c_sorted;
-    v.tcount = d.c_tcount; v.tfill = d.c_tfill; v.toff = d.c_toff; v.count = d.enable_steric ? 4 * d.N : 0;
+    v.cell = d.c_cell; v.w = d.c_w; v.store = d.c_store; v.tcount = d.c_tcount; v.ovf = d.c_ovf;
+    v.ctl = d.c_ctl; v.cap = d.c_cap; v.count = d.enable_steric ? 4 * d.N : 0;
   }
   return v;
 }
@@ -44,67 +43,6 @@ __device__ __forceinline__ int tile_of(const RDesc& d, int cell) {
 __device__ __forceinline__ unsigned local_of(const RDesc& d, int cell) {
   const int cy = cell / d.W, cx = cell - cy * d.W;
   return (unsigned)((cy % kBinTile) * kBinTile + (cx % kBinTile));
-}
-
-// Exclusive scan of the tile counts of every rollout (one CTA per rollout).
-__global__ void __launch_bounds__(1024) k_bin_scan(const RDesc* __restrict__ D, int n, int which) {
-  const int r = blockIdx.x;
-  if (r >= n) return;
-  const RDesc& d = D[r];
-  BinView v = bin_view(d, which);
-  if (v.count == 0 || v.tcount == nullptr) return;
-  const int nt = d.ntile_x * d.ntile_y;
-  __shared__ int wsum[32];
-  __shared__ int carry_s;
-  if (threadIdx.x == 0) carry_s = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int base = 0; base < nt; base += blockDim.x) {
-    const int i = base + threadIdx.x;
-    const int x = (i < nt) ? v.tcount[i] : 0;
-    int incl = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    if (lane == 31) wsum[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-      int s = (lane < (int)(blockDim.x >> 5)) ? wsum[lane] : 0;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, s, o);
-        if (lane >= o) s += y;
-      }
-      wsum[lane] = s;
-    }
-    __syncthreads();
-    const int carry = carry_s;
-    const int pre = (wid > 0 ? wsum[wid - 1] : 0) + incl - x;
-    if (i < nt) {
-      v.toff[i] = carry + pre;
-      v.tfill[i] = 0;
-    }
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry_s = carry + wsum[(blockDim.x >> 5) - 1];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) v.toff[nt] = carry_s;
-}
-
-// Place every contribution into its tile's segment (order inside a tile is arbitrary;
-// the per-tile sort restores the reference order).
-__global__ void __launch_bounds__(256) k_bin_scatter(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
-                                                     int which) {
-  const int r = find_rollout(off, n, blockIdx.x);
-  const RDesc& d = D[r];
-  BinView v = bin_view(d, which);
-  const int k = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
-  if (k >= v.count) return;
-  const int t = tile_of(d, v.cell[k]);
-  const int p = v.toff[t] + atomicAdd(v.tfill + t, 1);
-  v.binned[p] = k;
 }
 
 __device__ void bitonic_sort_smem(unsigned* s, int P) {
@@ -135,143 +73,197 @@ __device__ __forceinline__ int lower_bound_u(const unsigned* a, int len, unsigne
   return lo;
 }
 
-// Per tile: sort contributions by (cell, k), then reduce each run of equal cells.
-// which == 0 (IB): per touched cell, kernel coverage -> 1/max(cov, 1), the macroscopic
-//   state pulled from h[parity] (density, clamped velocity), u_corrected = velocity, and
-//   contribution -> slot links.   (fluid.py:268-290)
-// which == 1 (CIC): deposit grid value = sum of the run's weights.   (forces.py:98-115)
-__global__ void __launch_bounds__(256) k_bin_sort(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
-                                                  int which, int parity) {
-  __shared__ unsigned skeys[kSortCap];
-  const int r = find_rollout(off, n, blockIdx.x);
-  const RDesc& d = D[r];
-  BinView v = bin_view(d, which);
-  const int t = blockIdx.x - off[r];
-  if (v.count == 0) return;
-  const int s = v.toff[t];
-  const int m = v.toff[t + 1] - s;
-  if (m == 0) {
-    if (threadIdx.x == 0) v.tcount[t] = 0;
+// Work for one touched cell: its contributions are run[0..len) in increasing k.
+// which == 0 (IB): coverage -> 1/max(cov, 1), the macroscopic state pulled from h[parity]
+//   (density, clamped velocity), u_corrected = velocity, contribution -> head links
+//   (fluid.py:268-290).   which == 1 (CIC): deposit value = in-order sum (forces.py:98-115).
+__device__ __forceinline__ void head_work(const RDesc& d, const BinView& v, int which, int parity, const int* run,
+                                          int len, int run_pos) {
+  const int k0 = run[0];
+  const int cell = v.cell[k0];
+  float acc = v.w[k0];
+  for (int j = 1; j < len; ++j) acc = acc + v.w[run[j]];
+  if (which == 1) {
+    d.dep[cell] = acc;
     return;
   }
-  unsigned* kp;
-  if (m <= kSortCap) {
-    int P = 1;
-    while (P < m) P <<= 1;
-    for (int i = threadIdx.x; i < P; i += blockDim.x) {
-      unsigned key = 0xffffffffu;
-      if (i < m) {
-        const int k = v.binned[s + i];
-        key = (local_of(d, v.cell[k]) << 24) | (unsigned)k;
-      }
-      skeys[i] = key;
+  const int slot = atomicAdd(v.ctl + 2, 1);
+  d.h_cell[slot] = cell;
+  d.h_start[slot] = run_pos;
+  d.h_len[slot] = len;
+  d.s_inv[slot] = 1.0f / max_prop(acc, 1.0f);
+  for (int j = 0; j < len; ++j) d.ib_slot[run[j]] = slot;
+  const int y = cell / d.W, x = cell - y * d.W;
+  const size_t HW = (size_t)d.H * d.W;
+  const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+  const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+  float f[9];
+  const float* hp = d.h[parity];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    const int ys = imod_floor(y - ey[q], d.H), xs = imod_floor(x - ex[q], d.W);
+    f[q] = hp[q * HW + (size_t)ys * d.W + xs];
+  }
+  float rho, vx, vy;
+  macroscopic(f, d.vmax, d.vmax_q4, rho, vx, vy);
+  d.s_rho[slot] = rho;
+  d.s_vx[slot] = vx;
+  d.s_vy[slot] = vy;
+  d.s_ucx[slot] = vx;
+  d.s_ucy[slot] = vy;
+}
+
+// One CTA (256 threads) per bin tile: sort the tile's contributions by (cell, k) and
+// reduce every cell's run.
+__global__ void __launch_bounds__(256) k_bin_tiles(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
+                                                   int which, int parity) {
+  __shared__ unsigned skeys[kSortCap];
+  __shared__ int cnt[kBinTile * kBinTile];
+  __shared__ int cpos[kBinTile * kBinTile];
+  __shared__ int s_spill;
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const BinView v = bin_view(d, which);
+  if (v.count == 0) return;
+  const int t = blockIdx.x - off[r];
+  const int total = v.tcount[t];
+  if (total == 0) return;
+  const int tid = threadIdx.x;
+  const int ntiles = d.ntile_x * d.ntile_y;
+  int* bin = v.store + (size_t)t * v.cap;
+
+  if (total <= v.cap) {
+    // counting sort by local cell; positions inside a cell come from shared atomics
+    // (arbitrary order), so each cell's run is then ordered by k
+    for (int c = tid; c < kBinTile * kBinTile; c += blockDim.x) cnt[c] = 0;
+    __syncthreads();
+    for (int i = tid; i < total; i += blockDim.x) {
+      const int k = bin[i];
+      const unsigned lc = local_of(d, v.cell[k]);
+      const int pos = atomicAdd(cnt + lc, 1);
+      skeys[i] = (lc << 24) | (unsigned)pos;  // (cell, rank inside the cell)
+      skeys[kSortCap / 2 + i] = (unsigned)k;
     }
     __syncthreads();
-    bitonic_sort_smem(skeys, P);
-    kp = skeys;
-  } else {
-    // chunks of kSortCap sorted in shared memory, then pairwise merges by rank
-    unsigned* bufA = reinterpret_cast<unsigned*>(v.sorted) + s;
-    unsigned* bufB = reinterpret_cast<unsigned*>(v.binned) + s;
-    for (int c0 = 0; c0 < m; c0 += kSortCap) {
-      const int len = min(kSortCap, m - c0);
-      int P = 1;
-      while (P < len) P <<= 1;
-      for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        unsigned key = 0xffffffffu;
-        if (i < len) {
-          const int k = v.binned[s + c0 + i];
-          key = (local_of(d, v.cell[k]) << 24) | (unsigned)k;
+    // exclusive scan of the 256 cell counts (one warp, 8 per lane)
+    if (tid < 32) {
+      int loc[8];
+      int sum = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        loc[q] = cnt[tid * 8 + q];
+        sum += loc[q];
+      }
+      int incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (tid >= o) incl += y;
+      }
+      int run = incl - sum;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        cpos[tid * 8 + q] = run;
+        run += loc[q];
+      }
+    }
+    __syncthreads();
+    // scatter into cell order (a bin holds at most cap <= kSortCap / 2 entries)
+    for (int i = tid; i < total; i += blockDim.x) {
+      const unsigned key = skeys[i];
+      const int lc = (int)(key >> 24), pos = (int)(key & 0xffffffu);
+      bin[cpos[lc] + pos] = (int)skeys[kSortCap / 2 + i];
+    }
+    __syncthreads();
+    // one thread per cell: order its run by k (runs are short), then reduce it
+    for (int c = tid; c < kBinTile * kBinTile; c += blockDim.x) {
+      const int len = cnt[c];
+      if (len == 0) continue;
+      int* run = bin + cpos[c];
+      for (int a = 1; a < len; ++a) {
+        const int key = run[a];
+        int b = a - 1;
+        while (b >= 0 && run[b] > key) {
+          run[b + 1] = run[b];
+          --b;
         }
-        skeys[i] = key;
+        run[b + 1] = key;
       }
-      __syncthreads();
-      bitonic_sort_smem(skeys, P);
-      for (int i = threadIdx.x; i < len; i += blockDim.x) bufA[c0 + i] = skeys[i];
-      __syncthreads();
+      head_work(d, v, which, parity, run, len, t * v.cap + cpos[c]);
     }
-    unsigned* src = bufA;
-    unsigned* dst = bufB;
-    for (int wdt = kSortCap; wdt < m; wdt <<= 1) {
-      for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        const int ps = (i / (2 * wdt)) * (2 * wdt);
-        const int a_len = min(wdt, m - ps);
-        const int b0 = ps + a_len;
-        const int b_len = max(0, min(wdt, m - b0));
-        const unsigned key = src[i];
-        int pos;
-        if (i < b0)
-          pos = (i - ps) + lower_bound_u(src + b0, b_len, key);
-        else
-          pos = (i - b0) + lower_bound_u(src + ps, a_len, key);
-        dst[ps + pos] = key;
-      }
-      __syncthreads();
-      unsigned* tmp = src;
-      src = dst;
-      dst = tmp;
-    }
-    if (src != bufA) {
-      for (int i = threadIdx.x; i < m; i += blockDim.x) bufA[i] = src[i];
-      __syncthreads();
-    }
-    kp = bufA;
+    __syncthreads();
+    if (tid == 0) v.tcount[t] = 0;
+    return;
   }
 
-  const float vmax = d.vmax;
-  const size_t HW = (size_t)d.H * d.W;
-  for (int i = threadIdx.x; i < m; i += blockDim.x) {
-    const unsigned key = kp[i];
-    const unsigned lc = key >> 24;
-    const bool head = (i == 0) || ((kp[i - 1] >> 24) != lc);
-    int len = 0;
-    if (head) {
-      len = 1;
-      while (i + len < m && (kp[i + len] >> 24) == lc) ++len;
-    }
-    if (which == 1) {
-      if (head) {
-        const int k0 = (int)(key & 0xffffffu);
-        float acc = v.w[k0];
-        for (int j = 1; j < len; ++j) acc = acc + v.w[(int)(kp[i + j] & 0xffffffu)];
-        d.dep[v.cell[k0]] = acc;
-      }
-    } else {
-      int h0 = i;
-      while (h0 > 0 && (kp[h0 - 1] >> 24) == lc) --h0;
-      const int k = (int)(key & 0xffffffu);
-      d.ib_slot[k] = s + h0;
-      d.s_len[s + i] = len;
-      if (head) {
-        const int cell = v.cell[k];
-        float cov = v.w[k];
-        for (int j = 1; j < len; ++j) cov = cov + v.w[(int)(kp[i + j] & 0xffffffu)];
-        const int p = s + i;
-        d.s_cell[p] = cell;
-        d.s_inv[p] = 1.0f / max_prop(cov, 1.0f);
-        const int y = cell / d.W, x = cell - y * d.W;
-        const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
-        const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
-        float f[9];
-        const float* hp = d.h[parity];
-#pragma unroll
-        for (int q = 0; q < 9; ++q) {
-          const int ys = imod_floor(y - ey[q], d.H), xs = imod_floor(x - ex[q], d.W);
-          f[q] = hp[q * HW + (size_t)ys * d.W + xs];
-        }
-        float rho, vx, vy;
-        macroscopic(f, vmax, rho, vx, vy);
-        d.s_rho[p] = rho;
-        d.s_vx[p] = vx;
-        d.s_vy[p] = vy;
-        d.s_ucx[p] = vx;
-        d.s_ucy[p] = vy;
-      }
+  // Spilled tile: gather its bin and its overflow entries into a private arena region,
+  // sort by (cell, k) with shared-memory chunk sorts and rank merges, then reduce.
+  if (tid == 0) s_spill = atomicAdd(v.ctl + 1, 2 * total);
+  __syncthreads();
+  const int base = ntiles * v.cap + s_spill;
+  unsigned* bufA = reinterpret_cast<unsigned*>(v.store) + base;
+  unsigned* bufB = bufA + total;
+  for (int i = tid; i < v.cap; i += blockDim.x) {
+    const int k = bin[i];
+    bufB[i] = (local_of(d, v.cell[k]) << 24) | (unsigned)k;
+  }
+  if (tid == 0) {
+    // the overflow list is unordered: collect this tile's entries sequentially
+    int m = v.cap;
+    const int no = v.ctl[0];
+    for (int i = 0; i < no && m < total; ++i) {
+      const int k = v.ovf[i];
+      if (tile_of(d, v.cell[k]) == t) bufB[m++] = (local_of(d, v.cell[k]) << 24) | (unsigned)k;
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < m; i += blockDim.x) v.sorted[s + i] = (int)(kp[i] & 0xffffffu);
-  if (threadIdx.x == 0) v.tcount[t] = 0;
+  const int m = total;
+  for (int c0 = 0; c0 < m; c0 += kSortCap) {
+    const int len = min(kSortCap, m - c0);
+    int P = 1;
+    while (P < len) P <<= 1;
+    for (int i = tid; i < P; i += blockDim.x) skeys[i] = i < len ? bufB[c0 + i] : 0xffffffffu;
+    __syncthreads();
+    bitonic_sort_smem(skeys, P);
+    for (int i = tid; i < len; i += blockDim.x) bufA[c0 + i] = skeys[i];
+    __syncthreads();
+  }
+  unsigned* src = bufA;
+  unsigned* dst = bufB;
+  for (int wdt = kSortCap; wdt < m; wdt <<= 1) {
+    for (int i = tid; i < m; i += blockDim.x) {
+      const int ps = (i / (2 * wdt)) * (2 * wdt);
+      const int a_len = min(wdt, m - ps);
+      const int b0 = ps + a_len;
+      const int b_len = max(0, min(wdt, m - b0));
+      const unsigned key = src[i];
+      int pos;
+      if (i < b0)
+        pos = (i - ps) + lower_bound_u(src + b0, b_len, key);
+      else
+        pos = (i - b0) + lower_bound_u(src + ps, a_len, key);
+      dst[ps + pos] = key;
+    }
+    __syncthreads();
+    unsigned* tmp = src;
+    src = dst;
+    dst = tmp;
+  }
+  // runs are located on the sorted keys; their k values go to the other buffer
+  const unsigned* keys = src;
+  int* kv = reinterpret_cast<int*>(dst);
+  for (int i = tid; i < m; i += blockDim.x) kv[i] = (int)(keys[i] & 0xffffffu);
+  __syncthreads();
+  const int kv_pos = base + (int)(reinterpret_cast<unsigned*>(kv) - bufA);
+  for (int i = tid; i < m; i += blockDim.x) {
+    const unsigned lc = keys[i] >> 24;
+    if (i > 0 && (keys[i - 1] >> 24) == lc) continue;
+    int len = 1;
+    while (i + len < m && (keys[i + len] >> 24) == lc) ++len;
+    head_work(d, v, which, parity, kv + i, len, kv_pos + i);
+  }
+  __syncthreads();
+  if (tid == 0) v.tcount[t] = 0;
 }
 
 // Multi-direct forcing, interpolation half (fluid.py:292-302): per IB point, u at the point
@@ -306,13 +298,13 @@ __global__ void __launch_bounds__(256) k_ib_spread(const RDesc* __restrict__ D, 
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
-  if (p >= d.M || it >= d.ib_iters) return;
-  const int len = d.s_len[p];
-  if (len == 0) return;
+  if (it >= d.ib_iters || p >= d.ib_ctl[2]) return;
+  const int len = d.h_len[p];
+  const int* run = d.ib_store + d.h_start[p];
   const int K2 = d.K * d.K;
   float dx = 0.0f, dy = 0.0f;
   for (int j = 0; j < len; ++j) {
-    const int k = d.ib_sorted[p + j];
+    const int k = run[j];
     const int node = k / K2;
     const float w = d.ib_w[k];
     dx = dx + d.delta[2 * node] * w;
@@ -329,8 +321,7 @@ __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
-  if (p >= d.M) return;
-  if (d.s_len[p] == 0) return;
+  if (p >= d.ib_ctl[2]) return;
   float ucx = d.s_ucx[p], ucy = d.s_ucy[p];
   const float c2 = clamp_factor(ucx, ucy, d.vmax);
   ucx = ucx * c2;
@@ -345,7 +336,7 @@ __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D
   }
   d.s_fx[p] = Fx;
   d.s_fy[p] = Fy;
-  const int cell = d.s_cell[p];
+  const int cell = d.h_cell[p];
   const size_t HW = (size_t)d.H * d.W;
   d.fov[cell] = Fx;
   d.fov[HW + cell] = Fy;
@@ -360,6 +351,11 @@ __global__ void __launch_bounds__(256) k_reaction(const RDesc* __restrict__ D, c
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int node = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
+  if (node == 0) {
+    // this step's deposit has been reduced: reset the CIC bin controls
+    d.c_ctl[0] = 0;
+    d.c_ctl[1] = 0;
+  }
   if (node >= d.N) return;
   float vx = d.vel[2 * node], vy = d.vel[2 * node + 1];
   if (d.enable_fluid) {
@@ -420,10 +416,8 @@ __global__ void k_record_fields(const RDesc* __restrict__ D, const int* __restri
 
 __global__ void k_tick(int* tdev) { *tdev += 1; }
 
-void launch_bin_scan(const Launch& L, int which) { k_bin_scan<<<L.n, 1024, 0, L.s>>>(L.d, L.n, which); }
-void launch_bin_scatter(const Launch& L, int which) { k_bin_scatter<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, which); }
-void launch_bin_sort(const Launch& L, int which, int parity) {
-  k_bin_sort<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, which, parity);
+void launch_bin_tiles(const Launch& L, int which, int parity) {
+  k_bin_tiles<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, which, parity);
 }
 void launch_ib_interp(const Launch& L, int it) { k_ib_interp<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
 void launch_ib_spread(const Launch& L, int it) { k_ib_spread<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }

@@ -95,12 +95,12 @@ __global__ void __launch_bounds__(256) k_lbm(const RDesc* __restrict__ D, const 
 #pragma unroll
       for (int i = 0; i < 9; ++i) f[i] = fin[i][c];
       float rho, vx, vy, Fx, Fy;
-      macroscopic(f, d.vmax, rho, vx, vy);
+      macroscopic(f, d.vmax, d.vmax_q4, rho, vx, vy);
       if (ov[c]) {
         Fx = ovx[c];
         Fy = ovy[c];
       } else {
-        free_cell_force(rho, vx, vy, d.vmax, d.force_clamp, Fx, Fy);
+        free_cell_force(rho, vx, vy, d.vmax, d.vmax_q4, d.force_clamp, Fx, Fy);
       }
       float o[9];
       collide(f, rho, vx, vy, Fx, Fy, d.wp, d.wm, cp, cm, o, usx[c], usy[c]);
@@ -186,14 +186,13 @@ __global__ void k_clear_ws(const RDesc* __restrict__ D, const int* __restrict__ 
   const int nt = d.ntile_x * d.ntile_y;
   for (size_t i = t0; i < (size_t)nt; i += stride) {
     d.ib_tcount[i] = 0;
-    d.ib_tfill[i] = 0;
-    if (d.c_tcount) {
-      d.c_tcount[i] = 0;
-      d.c_tfill[i] = 0;
-    }
+    d.c_tcount[i] = 0;
   }
   for (size_t i = t0; i < (size_t)d.lbm_tx * d.lbm_ty; i += stride) d.lbm_flag[i] = 0;
-  for (size_t i = t0; i < (size_t)d.M; i += stride) d.s_len[i] = 0;
+  if (t0 < 4) {
+    d.ib_ctl[t0] = 0;
+    d.c_ctl[t0] = 0;
+  }
   if (t0 == 0) *d.flags = 0u;
 }
 

@@ -20,9 +20,18 @@ __device__ __forceinline__ float clamp_factor(float x, float y, float vmax) {
   return min_prop(1.0f, vmax / (mag + MC_EPSIL));
 }
 
+// The same factor with an exact shortcut: when x^2 + y^2 + EPSIL <= vmax^2 / 4 the magnitude
+// is at most vmax / 2, so vmax / (mag + EPSIL) > 1 and the factor is exactly 1.
+// q4 = vmax^2 / 4 (computed on the host, rounded down).  NaN inputs take the full path.
+__device__ __forceinline__ float clamp_factor_fast(float x, float y, float vmax, float q4) {
+  const float m2 = (x * x + y * y) + MC_EPSIL;
+  if (m2 <= q4) return 1.0f;
+  return min_prop(1.0f, vmax / (sqrtf(m2) + MC_EPSIL));
+}
+
 // f = max(f, EPSIL); rho = max(sum f, 0.1); u = sum e f / rho; velocity clamp
 // (fluid.py:136-142, 268-274).  Returns rho and the clamped velocity.
-__device__ __forceinline__ void macroscopic(float f[9], float vmax, float& rho, float& vx, float& vy) {
+__device__ __forceinline__ void macroscopic(float f[9], float vmax, float q4, float& rho, float& vx, float& vy) {
 #pragma unroll
   for (int i = 0; i < 9; ++i) f[i] = max_prop(f[i], MC_EPSIL);
   float r = f[0];
@@ -33,7 +42,7 @@ __device__ __forceinline__ void macroscopic(float f[9], float vmax, float& rho, 
   float uy = ((((f[2] - f[4]) + f[5]) + f[6]) - f[7]) - f[8];
   ux = ux / r;
   uy = uy / r;
-  float c1 = clamp_factor(ux, uy, vmax);
+  float c1 = clamp_factor_fast(ux, uy, vmax, q4);
   rho = r;
   vx = ux * c1;
   vy = uy * c1;
@@ -41,9 +50,14 @@ __device__ __forceinline__ void macroscopic(float f[9], float vmax, float& rho, 
 
 // Force of a cell that no IB point touches: the post-accumulation clamp applied to the
 // unchanged velocity (fluid.py:327-339).
-__device__ __forceinline__ void free_cell_force(float rho, float vx, float vy, float vmax, int force_clamp,
+__device__ __forceinline__ void free_cell_force(float rho, float vx, float vy, float vmax, float q4, int force_clamp,
                                                 float& Fx, float& Fy) {
-  float c2 = clamp_factor(vx, vy, vmax);
+  float c2 = clamp_factor_fast(vx, vy, vmax, q4);
+  if (c2 == 1.0f) {  // (v * 1 - v) * rho == 0 exactly
+    Fx = 0.0f;
+    Fy = 0.0f;
+    return;
+  }
   Fx = (vx * c2 - vx) * rho;
   Fy = (vy * c2 - vy) * rho;
   if (force_clamp) {
@@ -79,16 +93,30 @@ __device__ __forceinline__ void collide(const float f[9], float rho, float vx, f
 #pragma unroll
   for (int i = 0; i < 9; ++i)
     feq[i] = (rho * w[i]) * (((1.0f + 3.0f * eu[i]) + 4.5f * (eu[i] * eu[i])) - 1.5f * usq);
-  const int opp[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+  // Opposite directions (i, o): f_i + f_o and feq_i + feq_o are commutative sums, and
+  // 0.5 (f_o - f_i) - 0.5 (feq_o - feq_i) is exactly the negation of the i term, so each
+  // pair's symmetric and antisymmetric parts are computed once:
+  //   out_i = (f_i - wp*sym) - wm*anti,   out_o = (f_o - wp*sym) - wm*(-anti)
+  const int pi[4] = {1, 2, 5, 6};
+  const int po[4] = {3, 4, 7, 8};
+  {
+    // rest direction: f_o = f_i, the antisymmetric part is 0 - 0
+    const float sym = half * (f[0] + f[0]) - half * (feq[0] + feq[0]);
+    const float anti = half * (f[0] - f[0]) - half * (feq[0] - feq[0]);
+    out[0] = (f[0] - wp * sym) - wm * anti;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int i = pi[q], o = po[q];
+    const float sym = half * (f[i] + f[o]) - half * (feq[i] + feq[o]);
+    const float anti = half * (f[i] - f[o]) - half * (feq[i] - feq[o]);
+    out[i] = (f[i] - wp * sym) - wm * anti;
+    out[o] = (f[o] - wp * sym) - wm * (-anti);
+  }
   if (Fx == 0.0f && Fy == 0.0f) {
     // zero force: the Guo source is exactly zero and u* = u
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
-      int o = opp[i];
-      float post = (f[i] - wp * (half * (f[i] + f[o]) - half * (feq[i] + feq[o])))
-                   - wm * (half * (f[i] - f[o]) - half * (feq[i] - feq[o]));
-      out[i] = max_prop(post, MC_EPSIL);
-    }
+    for (int i = 0; i < 9; ++i) out[i] = max_prop(out[i], MC_EPSIL);
   } else {
     float eF[9];
     eF[0] = 0.0f;
@@ -104,13 +132,12 @@ __device__ __forceinline__ void collide(const float f[9], float rho, float vx, f
     float raw[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) raw[i] = w[i] * (3.0f * (eF[i] - udF) + (9.0f * eu[i]) * eF[i]);
+    const int opp[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
       int o = opp[i];
-      float post = (f[i] - wp * (half * (f[i] + f[o]) - half * (feq[i] + feq[o])))
-                   - wm * (half * (f[i] - f[o]) - half * (feq[i] - feq[o]));
       float src = cp * (half * (raw[i] + raw[o])) + cm * (half * (raw[i] - raw[o]));
-      out[i] = max_prop(post + src, MC_EPSIL);
+      out[i] = max_prop(out[i] + src, MC_EPSIL);
     }
   }
   usx_o = usx;

@@ -18,10 +18,12 @@ namespace mc {
 constexpr int kBinTile = 16;       // binning tile edge for the deterministic reductions
 constexpr int kLbmTileX = 128;     // dense LBM CTA tile: 32 lanes x 4 cells
 constexpr int kLbmTileY = 8;       //                    8 rows
-constexpr int kSortCap = 4096;     // keys sorted in shared memory per pass
+constexpr int kSortCap = 4096;     // keys sorted in shared memory per pass (>= every bin capacity)
+constexpr int kIbCap = 1024;       // IB contributions per 16x16 bin tile before spilling
+constexpr int kCicCap = 512;       // CIC contributions per bin tile before spilling
 constexpr int kFftMaxN = 4096;     // largest FFT length (shared memory)
 constexpr int kFftMaxFactors = 16;
-constexpr int kFftColsPerCta = 4;  // complex columns per column-pass CTA (8 real columns)
+constexpr int kFftColsPerCta = 2;  // complex columns per column-pass CTA (4 real columns)
 
 // Per-rollout descriptor.  All pointers are device pointers.
 struct RDesc {
@@ -35,6 +37,7 @@ struct RDesc {
   int max_comp_nodes, max_comp_edges, max_comp_pairs;
   // configuration
   float dt, damping, k_stretch, k_shear, vmax, relax, node_mass, wp, wm;
+  float vmax_q4;  // (vmax / 2)^2 rounded down: below it every velocity clamp factor is exactly 1
   float st_strength, st_sigma, st_scatter;
   float st_2s2, st_norm, st_coef;  // 2 sigma^2, 2 pi sigma^2, scatter / sigma^2 (float32 of the double values)
   int st_skip, ib_iters, cycles, enable_fluid, enable_steric, force_clamp;
@@ -91,14 +94,22 @@ struct RDesc {
   float* pred;         // (N,2)
   float* nvl;          // (N,2) node velocity in lattice units
   float* delta;        // (N,2) IB per-iteration correction
-  // IB contributions (M = N*K*K), then per-slot arrays indexed by sorted position
-  int* ib_cell;
-  float* ib_w;
-  int* ib_binned;
-  int* ib_sorted;
-  int* ib_slot;     // contribution -> slot (sorted position of its cell's first entry)
-  int* s_cell;      // slot -> cell (heads only)
-  int* s_len;       // slot -> run length (0 for non-heads)
+  // Deterministic scatter-add bins.  Contribution k goes to bin tile t at
+  // store[t * cap + atomic position]; a tile that fills up spills into the overflow list.
+  // store[ntiles * cap ...] is an arena for sorting tiles with more than cap entries.
+  // ctl[0] = overflow count, ctl[1] = arena use, ctl[2] = touched-cell (head) count.
+  int ib_cap;
+  int* ib_cell;     // (M) cell of contribution k = n*K*K + s
+  float* ib_w;      // (M) normalised stencil weight
+  int* ib_store;    // (ntiles * ib_cap + 2 * M)
+  int* ib_tcount;   // (ntiles)
+  int* ib_ovf;      // (M)
+  int* ib_ctl;      // (4)
+  int* ib_slot;     // (M) contribution -> head slot of its cell
+  // per touched cell ("head"), slots in [0, ctl[2])
+  int* h_cell;
+  int* h_start;     // position of the cell's sorted run in ib_store
+  int* h_len;
   float* s_rho;
   float* s_vx;
   float* s_vy;
@@ -107,17 +118,18 @@ struct RDesc {
   float* s_ucy;
   float* s_fx;
   float* s_fy;
-  int* ib_tcount;   // (ntiles) contributions per binning tile
-  int* ib_tfill;
-  int* ib_toff;     // (ntiles+1)
-  // CIC deposit contributions (4N)
+  // CIC deposit contributions k = corner*N + n (4N)
+  int c_cap;
   int* c_cell;
   float* c_w;
-  int* c_binned;
-  int* c_sorted;
+  int* c_store;     // (ntiles * c_cap + 8 * N)
   int* c_tcount;
-  int* c_tfill;
-  int* c_toff;
+  int* c_ovf;       // (4N)
+  int* c_ctl;       // (4)
+  // rod components: chains (warp kernel) and general graphs (CTA kernel)
+  int nchain, ngeneric;
+  const int* chain_comp;    // (nchain) component index
+  const int* generic_comp;  // (ngeneric)
   unsigned* flags;  // MC_FLAG_* for this rollout
 };
 
@@ -169,12 +181,11 @@ struct Launch {
 };
 
 void launch_predict(const Launch& L);
-void launch_bin_scan(const Launch& L, int which);
-void launch_bin_scatter(const Launch& L, int which);
-void launch_bin_sort(const Launch& L, int which, int parity);
+void launch_bin_tiles(const Launch& L, int which, int parity);
 void launch_fft_rows(const Launch& L, size_t smem);
 void launch_fft_cols(const Launch& L, size_t smem);
 void launch_node(const Launch& L, const int* tdev, size_t smem, int bs);
+void launch_chain(const Launch& L, const int* tdev, int slots);
 void launch_ib_interp(const Launch& L, int it);
 void launch_ib_spread(const Launch& L, int it);
 void launch_ib_finalize(const Launch& L);

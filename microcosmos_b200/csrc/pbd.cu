@@ -1,9 +1,12 @@
 // Node-side kernels of one step (src/microcosmos/simulate.py:37-84):
 //   k_predict: damping, inertial prediction, steric cloud-in-cell contributions;
-//   k_node:    per rod component (one CTA, state in shared memory): steric force
-//              (forces.py:41-81), curvature actuation, cycles_per_step Jacobi iterations
-//              of pbd_rod_constraint (solver/pbd.py:14-91), velocity from positions, and
-//              the IB stencil of every node (solver/fluid.py:40-87).
+//   k_chain:   one warp per chain rod (the topology make_edges(.., "line", F) builds),
+//              node/edge state in registers, neighbours exchanged with shuffles;
+//   k_node:    one CTA per rod of any other topology (trees, loops), state in shared
+//              memory, scatter-adds as gather lists in the reference's order.
+// Both rod kernels compute the steric force (forces.py:41-81), the curvature actuation,
+// cycles_per_step Jacobi iterations of pbd_rod_constraint (solver/pbd.py:14-91), the
+// velocity from positions, and every node's IB stencil (solver/fluid.py:40-87).
 #include "lbm_cell.cuh"
 
 namespace mc {
@@ -12,10 +15,27 @@ __device__ __forceinline__ int bin_tile(const RDesc& d, int cy, int cx) {
   return (cy / kBinTile) * d.ntile_x + cx / kBinTile;
 }
 
+// Append contribution k of cell (cy, cx) to its tile's bin (or the overflow list).
+__device__ __forceinline__ void bin_push(int* store, int* tcount, int* ovf, int* ctl, int cap, int tile, int k) {
+  const int pos = atomicAdd(tcount + tile, 1);
+  if (pos < cap) {
+    store[(size_t)tile * cap + pos] = k;
+  } else {
+    const int o = atomicAdd(ctl, 1);
+    ovf[o] = k;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_predict(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int node = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
+  if (node == 0) {
+    // the previous step's IB work is complete: reset this step's IB bin controls
+    d.ib_ctl[0] = 0;
+    d.ib_ctl[1] = 0;
+    d.ib_ctl[2] = 0;
+  }
   if (node >= d.N) return;
   const float px = d.pos[2 * node], py = d.pos[2 * node + 1];
   const float vx = d.vel[2 * node] * d.damping, vy = d.vel[2 * node + 1] * d.damping;
@@ -43,7 +63,7 @@ __global__ void __launch_bounds__(256) k_predict(const RDesc* __restrict__ D, co
     const int k = c * d.N + node;
     d.c_cell[k] = cy[c] * d.W + cx[c];
     d.c_w[k] = w[c];
-    atomicAdd(d.c_tcount + bin_tile(d, cy[c], cx[c]), 1);
+    bin_push(d.c_store, d.c_tcount, d.c_ovf, d.c_ctl, d.c_cap, bin_tile(d, cy[c], cx[c]), k);
   }
 }
 
@@ -93,12 +113,220 @@ __device__ float2 steric_force(const RDesc& d, int gi) {
   return make_float2(fx, fy);
 }
 
+// Predicted position of node gi after the steric displacement (simulate.py:55-63).
+__device__ __forceinline__ float2 node_start(const RDesc& d, int gi) {
+  float qx = d.pred[2 * gi], qy = d.pred[2 * gi + 1];
+  if (d.enable_steric) {
+    const float2 f = steric_force(d, gi);
+    qx = qx + (f.x * d.st_strength) * d.dt;
+    qy = qy + (f.y * d.st_strength) * d.dt;
+  }
+  return make_float2(qx, qy);
+}
+
+// Rest angle of pair gb at step t (the caller-side curvature actuation, if any).
+__device__ __forceinline__ float rest_angle(const RDesc& d, int gb, int t) {
+  if (!d.act_amp) return d.rest_ang[gb];
+  const float arg = d.act_omega[gb] * (float)(d.act_t0 + t) + d.act_phase[gb];
+  const float a = d.act_c[gb] + d.act_amp[gb] * sinf(arg);
+  d.rest_ang[gb] = a;
+  return a;
+}
+
+// One theta correction (pbd.py:35-40) and one edge force (pbd.py:60-81).
+__device__ __forceinline__ float bend_corr(float th_in, float th_out, float rest, float kb) {
+  float diff = th_out - th_in;
+  diff = fmod_floor(diff + MC_PI_F, MC_2PI_F) - MC_PI_F;
+  return ((diff - rest) * kb) * 0.5f;
+}
+
+__device__ __forceinline__ float2 edge_force(const RDesc& d, float th, float L0, float xs, float ys, float xt,
+                                             float yt) {
+  float sn, cs;
+  sincosf(th, &sn, &cs);
+  const float tx = cs * L0, ty = sn * L0;
+  const float2 cur = min_image(xt, yt, xs, ys, (float)d.W, (float)d.H);
+  const float L = sqrtf(cur.x * cur.x + cur.y * cur.y);
+  const float Lc = max_prop(L, 1e-8f);
+  const float stx = (cur.x / Lc) * (L - L0), sty = (cur.y / Lc) * (L - L0);
+  const float shx = (cur.x - tx) - stx, shy = (cur.y - ty) - sty;
+  return make_float2(((stx + shx * d.k_shear) * d.k_stretch) * 0.5f, ((sty + shy * d.k_shear) * d.k_stretch) * 0.5f);
+}
+
+// After the iterations: velocity (simulate.py:83-84), the IB point in lattice units
+// (fluid.py:236-239), its K x K stencil (fluid.py:40-79) appended to the IB bins, and the
+// clearing of the node's CIC deposit cells (the deposit grid stays zero between steps).
+__device__ __forceinline__ void node_finish(const RDesc& d, int gi, float x, float y) {
+  const float vx = (x - d.prev[2 * gi]) / d.dt, vy = (y - d.prev[2 * gi + 1]) / d.dt;
+  d.pos[2 * gi] = x;
+  d.pos[2 * gi + 1] = y;
+  d.vel[2 * gi] = vx;
+  d.vel[2 * gi + 1] = vy;
+  if (d.enable_steric) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) d.dep[d.c_cell[c * d.N + gi]] = 0.0f;
+  }
+  if (!d.enable_fluid) return;
+  const int K = d.K, K2 = K * K;
+  const float gx = x * d.scale_x, gy = y * d.scale_y;
+  d.nvl[2 * gi] = (vx * d.scale_x) * d.dt;
+  d.nvl[2 * gi + 1] = (vy * d.scale_y) * d.dt;
+  const int half = (K - 1) / 2;
+  const float hw = (float)K / 2.0f;
+  const float sx = floorf(gx) - (float)half, sy = floorf(gy) - (float)half;
+  float wx[8], wy[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    if (a < K) {
+      const float rx = fabsf((sx + (float)a) - gx) / hw;
+      const float ry = fabsf((sy + (float)a) - gy) / hw;
+      wx[a] = rx <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * rx) / 2.0f)) : 0.0f;
+      wy[a] = ry <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * ry) / 2.0f)) : 0.0f;
+    }
+  }
+  float sum = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+      if (a < K && b < K) sum = sum + wx[a] * wy[b];
+  const float den = sum + MC_EPSIL;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    if (a < K) {
+      const int cx = imod_floor((int)(sx + (float)a), d.W);
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        if (b < K) {
+          const int cy = imod_floor((int)(sy + (float)b), d.H);
+          const int k = gi * K2 + a * K + b;
+          d.ib_cell[k] = cy * d.W + cx;
+          d.ib_w[k] = (wx[a] * wy[b]) / den;
+          bin_push(d.ib_store, d.ib_tcount, d.ib_ovf, d.ib_ctl, d.ib_cap, bin_tile(d, cy, cx), k);
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- chains: warp per rod
+// Lane l owns nodes/edges/pairs j = l*P + q (q < P).  In a chain, edge j = (node j, node
+// j+1) and pair j = (edge j, edge j+1); the scatter-adds reduce to
+//   theta_j += ((0 + c_j) + (-c_{j-1})) / deg_j * 1.8,   x_j += ((0 + f_j) + (-f_{j-1})) / deg_j
+// with the terms that exist, in the reference's order (e_in / src updates first).
+template <int P>
+__device__ __forceinline__ void shift_next(const float (&v)[P], float (&nx)[P]) {
+  const float first_next = __shfl_down_sync(0xffffffffu, v[0], 1);
+#pragma unroll
+  for (int q = 0; q < P - 1; ++q) nx[q] = v[q + 1];
+  nx[P - 1] = first_next;
+}
+template <int P>
+__device__ __forceinline__ void shift_prev(const float (&v)[P], float (&pv)[P]) {
+  const float last_prev = __shfl_up_sync(0xffffffffu, v[P - 1], 1);
+#pragma unroll
+  for (int q = P - 1; q > 0; --q) pv[q] = v[q - 1];
+  pv[0] = last_prev;
+}
+
+template <int P>
+__global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
+                                               const int* __restrict__ tdev) {
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ci = (blockIdx.x - off[r]) * 4 + warp;
+  if (ci >= d.nchain) return;  // the whole warp leaves together
+  const int comp = d.chain_comp[ci];
+  const int n0 = d.comp_n[comp], nn = d.comp_n[comp + 1] - n0;
+  const int e0 = d.comp_e[comp], ne = nn - 1;
+  const int b0 = d.comp_b[comp], nb = nn > 2 ? nn - 2 : 0;
+  const int t = *tdev;
+  float x[P], y[P], th[P], l0[P], ra[P], kb[P], edg[P], ndg[P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    const int j = lane * P + q;
+    x[q] = y[q] = th[q] = l0[q] = ra[q] = kb[q] = 0.0f;
+    if (j < nn) {
+      const float2 s = node_start(d, n0 + j);
+      x[q] = s.x;
+      y[q] = s.y;
+    }
+    if (j < ne) {
+      th[q] = d.theta[e0 + j];
+      l0[q] = d.rest_len[e0 + j];
+    }
+    if (j < nb) {
+      ra[q] = rest_angle(d, b0 + j, t);
+      kb[q] = d.kb[b0 + j];
+    }
+    edg[q] = fmaxf((float)((j < nb) + (j >= 1 && j - 1 < nb)), 1.0f);
+    ndg[q] = fmaxf((float)((j < ne) + (j >= 1 && j - 1 < ne)), 1.0f);
+  }
+  const int cycles = d.cycles;
+  for (int it = 0; it < cycles; ++it) {
+    float nx[P], pv[P], c[P];
+    shift_next<P>(th, nx);
+#pragma unroll
+    for (int q = 0; q < P; ++q) c[q] = (lane * P + q < nb) ? bend_corr(th[q], nx[q], ra[q], kb[q]) : 0.0f;
+    shift_prev<P>(c, pv);
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      const int j = lane * P + q;
+      if (j < ne) {
+        float acc = 0.0f;
+        if (j < nb) acc = acc + c[q];
+        if (j >= 1 && j - 1 < nb) acc = acc + (-pv[q]);
+        th[q] = th[q] + (acc / edg[q]) * 1.8f;
+      }
+    }
+    float xn[P], yn[P], fx[P], fy[P], fxp[P], fyp[P];
+    shift_next<P>(x, xn);
+    shift_next<P>(y, yn);
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      fx[q] = fy[q] = 0.0f;
+      if (lane * P + q < ne) {
+        const float2 f = edge_force(d, th[q], l0[q], x[q], y[q], xn[q], yn[q]);
+        fx[q] = f.x;
+        fy[q] = f.y;
+      }
+    }
+    shift_prev<P>(fx, fxp);
+    shift_prev<P>(fy, fyp);
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      const int j = lane * P + q;
+      if (j < nn) {
+        float ax = 0.0f, ay = 0.0f;
+        if (j < ne) {
+          ax = ax + fx[q];
+          ay = ay + fy[q];
+        }
+        if (j >= 1) {
+          ax = ax + (-fxp[q]);
+          ay = ay + (-fyp[q]);
+        }
+        x[q] = x[q] + ax / ndg[q];
+        y[q] = y[q] + ay / ndg[q];
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    const int j = lane * P + q;
+    if (j < ne) d.theta[e0 + j] = th[q];
+    if (j < nn) node_finish(d, n0 + j, x[q], y[q]);
+  }
+}
+
+// ---------------------------------------------------------------- general rods: CTA per rod
 __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
                        const int* __restrict__ tdev) {
   extern __shared__ float sm[];
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
-  const int comp = blockIdx.x - off[r];
+  const int comp = d.generic_comp[blockIdx.x - off[r]];
   const int n0 = d.comp_n[comp], nn = d.comp_n[comp + 1] - n0;
   const int e0 = d.comp_e[comp], ne = d.comp_e[comp + 1] - e0;
   const int b0 = d.comp_b[comp], nb = d.comp_b[comp + 1] - b0;
@@ -114,46 +342,26 @@ __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off,
   const int tid = threadIdx.x, bd = blockDim.x;
   const int t = *tdev;
 
-  // actuation (caller-side control of bending_rest_angles) and per-pair constants
   for (int b = tid; b < nb; b += bd) {
-    const int gb = b0 + b;
-    float a;
-    if (d.act_amp) {
-      const float arg = d.act_omega[gb] * (float)(d.act_t0 + t) + d.act_phase[gb];
-      a = d.act_c[gb] + d.act_amp[gb] * sinf(arg);
-      d.rest_ang[gb] = a;
-    } else {
-      a = d.rest_ang[gb];
-    }
-    ra[b] = a;
-    kb[b] = d.kb[gb];
+    ra[b] = rest_angle(d, b0 + b, t);
+    kb[b] = d.kb[b0 + b];
   }
   for (int e = tid; e < ne; e += bd) {
     th[e] = d.theta[e0 + e];
     l0[e] = d.rest_len[e0 + e];
   }
-  // steric displacement of the prediction (simulate.py:55-63)
   for (int i = tid; i < nn; i += bd) {
-    const int gi = n0 + i;
-    float qx = d.pred[2 * gi], qy = d.pred[2 * gi + 1];
-    if (d.enable_steric) {
-      const float2 f = steric_force(d, gi);
-      qx = qx + (f.x * d.st_strength) * d.dt;
-      qy = qy + (f.y * d.st_strength) * d.dt;
-    }
-    px[i] = qx;
-    py[i] = qy;
+    const float2 s = node_start(d, n0 + i);
+    px[i] = s.x;
+    py[i] = s.y;
   }
   __syncthreads();
 
-  const float W = (float)d.W, H = (float)d.H;
   for (int it = 0; it < d.cycles; ++it) {
     // theta pass over bending pairs (pbd.py:23-49)
     for (int b = tid; b < nb; b += bd) {
       const int ein = d.bpairs[2 * (b0 + b)] - e0, eout = d.bpairs[2 * (b0 + b) + 1] - e0;
-      float diff = th[eout] - th[ein];
-      diff = fmod_floor(diff + MC_PI_F, MC_2PI_F) - MC_PI_F;
-      corr[b] = ((diff - ra[b]) * kb[b]) * 0.5f;
+      corr[b] = bend_corr(th[ein], th[eout], ra[b], kb[b]);
     }
     __syncthreads();
     for (int e = tid; e < ne; e += bd) {
@@ -170,16 +378,9 @@ __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off,
     // position pass over edges (pbd.py:51-89)
     for (int e = tid; e < ne; e += bd) {
       const int s = d.pairs[2 * (e0 + e)] - n0, g = d.pairs[2 * (e0 + e) + 1] - n0;
-      const float dirx = cosf(th[e]), diry = sinf(th[e]);
-      const float L0 = l0[e];
-      const float tx = dirx * L0, ty = diry * L0;
-      const float2 cur = min_image(px[g], py[g], px[s], py[s], W, H);
-      const float L = sqrtf(cur.x * cur.x + cur.y * cur.y);
-      const float Lc = max_prop(L, 1e-8f);
-      const float stx = (cur.x / Lc) * (L - L0), sty = (cur.y / Lc) * (L - L0);
-      const float shx = (cur.x - tx) - stx, shy = (cur.y - ty) - sty;
-      fx[e] = ((stx + shx * d.k_shear) * d.k_stretch) * 0.5f;
-      fy[e] = ((sty + shy * d.k_shear) * d.k_stretch) * 0.5f;
+      const float2 f = edge_force(d, th[e], l0[e], px[s], py[s], px[g], py[g]);
+      fx[e] = f.x;
+      fy[e] = f.y;
     }
     __syncthreads();
     for (int i = tid; i < nn; i += bd) {
@@ -204,67 +405,20 @@ __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off,
   }
 
   for (int e = tid; e < ne; e += bd) d.theta[e0 + e] = th[e];
-  const int K = d.K, K2 = K * K;
-  for (int i = tid; i < nn; i += bd) {
-    const int gi = n0 + i;
-    const float x = px[i], y = py[i];
-    const float vx = (x - d.prev[2 * gi]) / d.dt, vy = (y - d.prev[2 * gi + 1]) / d.dt;
-    d.pos[2 * gi] = x;
-    d.pos[2 * gi + 1] = y;
-    d.vel[2 * gi] = vx;
-    d.vel[2 * gi + 1] = vy;
-    if (d.enable_steric) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) d.dep[d.c_cell[c * d.N + gi]] = 0.0f;
-    }
-    if (d.enable_fluid) {
-      // IB point in lattice units (fluid.py:236-239) and its K x K stencil (fluid.py:40-79)
-      const float gx = x * d.scale_x, gy = y * d.scale_y;
-      d.nvl[2 * gi] = (vx * d.scale_x) * d.dt;
-      d.nvl[2 * gi + 1] = (vy * d.scale_y) * d.dt;
-      const int half = (K - 1) / 2;
-      const float hw = (float)K / 2.0f;
-      const float sx = floorf(gx) - (float)half, sy = floorf(gy) - (float)half;
-      float wx[8], wy[8];
-#pragma unroll
-      for (int a = 0; a < 8; ++a) {
-        if (a < K) {
-          const float rx = fabsf((sx + (float)a) - gx) / hw;
-          const float ry = fabsf((sy + (float)a) - gy) / hw;
-          wx[a] = rx <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * rx) / 2.0f)) : 0.0f;
-          wy[a] = ry <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * ry) / 2.0f)) : 0.0f;
-        }
-      }
-      float sum = 0.0f;
-#pragma unroll
-      for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int b = 0; b < 8; ++b)
-          if (a < K && b < K) sum = sum + wx[a] * wy[b];
-      const float den = sum + MC_EPSIL;
-#pragma unroll
-      for (int a = 0; a < 8; ++a) {
-        if (a < K) {
-          const int cx = imod_floor((int)(sx + (float)a), d.W);
-#pragma unroll
-          for (int b = 0; b < 8; ++b) {
-            if (b < K) {
-              const int cy = imod_floor((int)(sy + (float)b), d.H);
-              const int k = gi * K2 + a * K + b;
-              d.ib_cell[k] = cy * d.W + cx;
-              d.ib_w[k] = (wx[a] * wy[b]) / den;
-              atomicAdd(d.ib_tcount + bin_tile(d, cy, cx), 1);
-            }
-          }
-        }
-      }
-    }
-  }
+  for (int i = tid; i < nn; i += bd) node_finish(d, n0 + i, px[i], py[i]);
 }
 
 void launch_predict(const Launch& L) { k_predict<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
 void launch_node(const Launch& L, const int* tdev, size_t smem, int bs) {
   k_node<<<L.grid, bs, smem, L.s>>>(L.d, L.off, L.n, tdev);
+}
+void launch_chain(const Launch& L, const int* tdev, int slots) {
+  switch (slots) {
+    case 1: k_chain<1><<<L.grid, 128, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
+    case 2: k_chain<2><<<L.grid, 128, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
+    case 4: k_chain<4><<<L.grid, 128, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
+    default: k_chain<8><<<L.grid, 128, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
+  }
 }
 cudaError_t node_set_smem(size_t bytes) {
   return cudaFuncSetAttribute(k_node, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);

@@ -37,7 +37,7 @@ mc_status cuda_fail(cudaError_t e, const char* where) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-enum Kind { K_NODES = 0, K_COMP, K_IB, K_CIC, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_COUNT };
+enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_COUNT };
 
 struct Region {
   size_t off = 0;
@@ -52,15 +52,17 @@ struct HostRollout {
   std::vector<int> comp_n, comp_e, comp_b, ep_off, ep_idx, ne_off, ne_idx;
   std::vector<float> edeg, ndeg;
   int ncomp = 0, max_cn = 0, max_ce = 0, max_cb = 0;
+  std::vector<int> chain_comp, generic_comp;  // components by kernel
+  int max_chain = 0;                          // longest chain (nodes)
   std::vector<int> fW, fH;
   std::vector<float2> twW, twH;
   std::vector<float> gW, gH;
   int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4;
   // workspace regions (offsets relative to the workspace base)
   Region r_h0, r_h1, r_fov, r_lflag, r_dep, r_tmp, r_prev, r_pred, r_nvl, r_delta;
-  Region r_ibcell, r_ibw, r_ibbin, r_ibsort, r_ibslot, r_scell, r_slen, r_srho, r_svx, r_svy, r_sinv, r_sucx,
-      r_sucy, r_sfx, r_sfy, r_ibtc, r_ibtf, r_ibto;
-  Region r_ccell, r_cw, r_cbin, r_csort, r_ctc, r_ctf, r_cto;
+  Region r_ibcell, r_ibw, r_ibstore, r_ibtc, r_ibovf, r_ibctl, r_ibslot, r_hcell, r_hstart, r_hlen, r_srho, r_svx,
+      r_svy, r_sinv, r_sucx, r_sucy, r_sfx, r_sfy;
+  Region r_ccell, r_cw, r_cstore, r_ctc, r_covf, r_cctl, r_chain, r_generic;
   Region r_pairs, r_bpairs, r_compn, r_compe, r_compb, r_epo, r_epi, r_neo, r_nei, r_edeg, r_ndeg;
   Region r_twW, r_twH, r_gW, r_gH, r_flags;
 };
@@ -80,6 +82,7 @@ struct mc_plan {
   int any_fluid = 0, any_steric = 0, max_iters = 0;
   size_t node_smem = 0, fftr_smem = 0, fftc_smem = 0;
   int node_bs = 32;
+  int max_chain = 0, chain_slots = 1;
   std::vector<RDesc> desc;
   cudaStream_t cap_stream = nullptr;
   // CUDA graphs, keyed by [steps-1][parity][recording variant][write_u]
@@ -230,6 +233,27 @@ mc_status build_topology(HostRollout& h) {
     h.comp_b = {0, B};
     h.ncomp = 1;
   }
+  // chains (edge i = (n0+i, n0+i+1), pair i = (e0+i, e0+i+1), <= 256 nodes) run on the
+  // warp kernel; every other component on the CTA kernel
+  h.chain_comp.clear();
+  h.generic_comp.clear();
+  h.max_chain = 0;
+  for (int c = 0; c < h.ncomp; ++c) {
+    const int n0 = h.comp_n[c], nn = h.comp_n[c + 1] - n0;
+    const int e0 = h.comp_e[c], ne = h.comp_e[c + 1] - e0;
+    const int b0 = h.comp_b[c], nb = h.comp_b[c + 1] - b0;
+    bool chain = nn >= 1 && nn <= 256 && ne == nn - 1 && nb == std::max(nn - 2, 0);
+    for (int i = 0; chain && i < ne; ++i)
+      chain = h.pairs[2 * (e0 + i)] == n0 + i && h.pairs[2 * (e0 + i) + 1] == n0 + i + 1;
+    for (int i = 0; chain && i < nb; ++i)
+      chain = h.bpairs[2 * (b0 + i)] == e0 + i && h.bpairs[2 * (b0 + i) + 1] == e0 + i + 1;
+    if (chain) {
+      h.chain_comp.push_back(c);
+      h.max_chain = std::max(h.max_chain, nn);
+    } else {
+      h.generic_comp.push_back(c);
+    }
+  }
   h.max_cn = h.max_ce = h.max_cb = 1;
   for (int c = 0; c < h.ncomp; ++c) {
     h.max_cn = std::max(h.max_cn, h.comp_n[c + 1] - h.comp_n[c]);
@@ -285,6 +309,7 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.scale_x = (float)sx;
   d.scale_y = (float)sy;
   d.vmax = (float)((double)c.max_fluid_velocity * (0.5 * (sx + sy)));
+  d.vmax_q4 = std::nextafter((float)(0.25 * (double)d.vmax * (double)d.vmax), 0.0f);
   d.sdt_x = d.scale_x * h.dt;
   d.sdt_y = d.scale_y * h.dt;
   d.relax = c.ibm_relaxation;
@@ -349,6 +374,7 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.max_comp_nodes = 0;
   int mcn = 1, mce = 1, mcb = 1;
   for (auto& o : p->R) {
+    if (o.generic_comp.empty()) continue;
     mcn = std::max(mcn, o.max_cn);
     mce = std::max(mce, o.max_ce);
     mcb = std::max(mcb, o.max_cb);
@@ -377,13 +403,17 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.pred = at<float>(b, h.r_pred);
   d.nvl = at<float>(b, h.r_nvl);
   d.delta = at<float>(b, h.r_delta);
+  d.ib_cap = mc::kIbCap;
   d.ib_cell = at<int>(b, h.r_ibcell);
   d.ib_w = at<float>(b, h.r_ibw);
-  d.ib_binned = at<int>(b, h.r_ibbin);
-  d.ib_sorted = at<int>(b, h.r_ibsort);
+  d.ib_store = at<int>(b, h.r_ibstore);
+  d.ib_tcount = at<int>(b, h.r_ibtc);
+  d.ib_ovf = at<int>(b, h.r_ibovf);
+  d.ib_ctl = at<int>(b, h.r_ibctl);
   d.ib_slot = at<int>(b, h.r_ibslot);
-  d.s_cell = at<int>(b, h.r_scell);
-  d.s_len = at<int>(b, h.r_slen);
+  d.h_cell = at<int>(b, h.r_hcell);
+  d.h_start = at<int>(b, h.r_hstart);
+  d.h_len = at<int>(b, h.r_hlen);
   d.s_rho = at<float>(b, h.r_srho);
   d.s_vx = at<float>(b, h.r_svx);
   d.s_vy = at<float>(b, h.r_svy);
@@ -392,16 +422,17 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.s_ucy = at<float>(b, h.r_sucy);
   d.s_fx = at<float>(b, h.r_sfx);
   d.s_fy = at<float>(b, h.r_sfy);
-  d.ib_tcount = at<int>(b, h.r_ibtc);
-  d.ib_tfill = at<int>(b, h.r_ibtf);
-  d.ib_toff = at<int>(b, h.r_ibto);
+  d.c_cap = mc::kCicCap;
   d.c_cell = at<int>(b, h.r_ccell);
   d.c_w = at<float>(b, h.r_cw);
-  d.c_binned = at<int>(b, h.r_cbin);
-  d.c_sorted = at<int>(b, h.r_csort);
+  d.c_store = at<int>(b, h.r_cstore);
   d.c_tcount = at<int>(b, h.r_ctc);
-  d.c_tfill = at<int>(b, h.r_ctf);
-  d.c_toff = at<int>(b, h.r_cto);
+  d.c_ovf = at<int>(b, h.r_covf);
+  d.c_ctl = at<int>(b, h.r_cctl);
+  d.nchain = (int)h.chain_comp.size();
+  d.ngeneric = (int)h.generic_comp.size();
+  d.chain_comp = at<int>(b, h.r_chain);
+  d.generic_comp = at<int>(b, h.r_generic);
   d.flags = at<unsigned>(b, h.r_flags);
   p->desc[i] = d;
 }
@@ -416,9 +447,9 @@ mc::Launch L(mc_plan* p, Kind k, cudaStream_t s) {
   return l;
 }
 
-const char* const kProfNames[] = {"predict", "cic_scan", "cic_scatter", "cic_sort", "fft_rows", "fft_cols",
-                                   "node", "ib_scan", "ib_scatter", "ib_sort", "ib_interp", "ib_spread",
-                                   "ib_finalize", "lbm", "reaction", "record_fields", "tick"};
+const char* const kProfNames[] = {"predict", "cic_bins",  "fft_rows",    "fft_cols", "chain",
+                                   "node",    "ib_bins",   "ib_interp",   "ib_spread", "ib_finalize",
+                                   "lbm",     "reaction",  "record_fields", "tick"};
 constexpr int kNumProf = sizeof(kProfNames) / sizeof(kProfNames[0]);
 
 cudaEvent_t take_event(mc_plan* p) {
@@ -459,40 +490,40 @@ int64_t enqueue_step(mc_plan* p, int parity, int write_u, int rec_fields, cudaSt
     ++k;
   }
   if (p->any_steric) {
-    timed(p, 1, s, capture, [&] { mc::launch_bin_scan(L(p, K_CIC, s), 1); });
-    timed(p, 2, s, capture, [&] { mc::launch_bin_scatter(L(p, K_CIC, s), 1); });
-    timed(p, 3, s, capture, [&] { mc::launch_bin_sort(L(p, K_TILES, s), 1, parity); });
-    timed(p, 4, s, capture, [&] { mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem); });
-    timed(p, 5, s, capture, [&] { mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem); });
-    k += 5;
+    timed(p, 1, s, capture, [&] { mc::launch_bin_tiles(L(p, K_TILES, s), 1, parity); });
+    timed(p, 2, s, capture, [&] { mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem); });
+    timed(p, 3, s, capture, [&] { mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem); });
+    k += 3;
+  }
+  if (p->grid[K_CHAIN]) {
+    timed(p, 4, s, capture, [&] { mc::launch_chain(L(p, K_CHAIN, s), tdev, p->chain_slots); });
+    ++k;
   }
   if (p->grid[K_COMP]) {
-    timed(p, 6, s, capture, [&] { mc::launch_node(L(p, K_COMP, s), tdev, p->node_smem, p->node_bs); });
+    timed(p, 5, s, capture, [&] { mc::launch_node(L(p, K_COMP, s), tdev, p->node_smem, p->node_bs); });
     ++k;
   }
   if (p->any_fluid) {
-    timed(p, 7, s, capture, [&] { mc::launch_bin_scan(L(p, K_IB, s), 0); });
-    timed(p, 8, s, capture, [&] { mc::launch_bin_scatter(L(p, K_IB, s), 0); });
-    timed(p, 9, s, capture, [&] { mc::launch_bin_sort(L(p, K_TILES, s), 0, parity); });
-    k += 3;
+    timed(p, 6, s, capture, [&] { mc::launch_bin_tiles(L(p, K_TILES, s), 0, parity); });
+    ++k;
     for (int it = 0; it < p->max_iters; ++it) {
-      timed(p, 10, s, capture, [&] { mc::launch_ib_interp(L(p, K_NODES, s), it); });
-      timed(p, 11, s, capture, [&] { mc::launch_ib_spread(L(p, K_IB, s), it); });
+      timed(p, 7, s, capture, [&] { mc::launch_ib_interp(L(p, K_NODES, s), it); });
+      timed(p, 8, s, capture, [&] { mc::launch_ib_spread(L(p, K_IB, s), it); });
       k += 2;
     }
-    timed(p, 12, s, capture, [&] { mc::launch_ib_finalize(L(p, K_IB, s)); });
-    timed(p, 13, s, capture, [&] { mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->R[0].vec); });
+    timed(p, 9, s, capture, [&] { mc::launch_ib_finalize(L(p, K_IB, s)); });
+    timed(p, 10, s, capture, [&] { mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->R[0].vec); });
     k += 2;
   }
   if (p->grid[K_NODES]) {
-    timed(p, 14, s, capture, [&] { mc::launch_reaction(L(p, K_NODES, s), tdev); });
+    timed(p, 11, s, capture, [&] { mc::launch_reaction(L(p, K_NODES, s), tdev); });
     ++k;
   }
   if (rec_fields) {
-    timed(p, 15, s, capture, [&] { mc::launch_record_fields(L(p, K_CELLS, s), tdev); });
+    timed(p, 12, s, capture, [&] { mc::launch_record_fields(L(p, K_CELLS, s), tdev); });
     ++k;
   }
-  timed(p, 16, s, capture, [&] { mc::launch_tick(tdev, s); });
+  timed(p, 13, s, capture, [&] { mc::launch_tick(tdev, s); });
   ++k;
   return k;
 }
@@ -636,11 +667,14 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     const size_t Mz = (size_t)M;
     h.r_ibcell = lay.take(Mz * 4);
     h.r_ibw = lay.take(Mz * 4);
-    h.r_ibbin = lay.take(Mz * 4);
-    h.r_ibsort = lay.take(Mz * 4);
+    h.r_ibstore = lay.take((nt * mc::kIbCap + 2 * Mz) * 4);
+    h.r_ibtc = lay.take(nt * 4);
+    h.r_ibovf = lay.take(Mz * 4);
+    h.r_ibctl = lay.take(4 * 4);
     h.r_ibslot = lay.take(Mz * 4);
-    h.r_scell = lay.take(Mz * 4);
-    h.r_slen = lay.take(Mz * 4);
+    h.r_hcell = lay.take(Mz * 4);
+    h.r_hstart = lay.take(Mz * 4);
+    h.r_hlen = lay.take(Mz * 4);
     h.r_srho = lay.take(Mz * 4);
     h.r_svx = lay.take(Mz * 4);
     h.r_svy = lay.take(Mz * 4);
@@ -649,16 +683,14 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.r_sucy = lay.take(Mz * 4);
     h.r_sfx = lay.take(Mz * 4);
     h.r_sfy = lay.take(Mz * 4);
-    h.r_ibtc = lay.take(nt * 4);
-    h.r_ibtf = lay.take(nt * 4);
-    h.r_ibto = lay.take((nt + 1) * 4);
     h.r_ccell = lay.take(4 * N * 4);
     h.r_cw = lay.take(4 * N * 4);
-    h.r_cbin = lay.take(4 * N * 4);
-    h.r_csort = lay.take(4 * N * 4);
+    h.r_cstore = lay.take((nt * mc::kCicCap + 8 * N) * 4);
     h.r_ctc = lay.take(nt * 4);
-    h.r_ctf = lay.take(nt * 4);
-    h.r_cto = lay.take((nt + 1) * 4);
+    h.r_covf = lay.take(4 * N * 4);
+    h.r_cctl = lay.take(4 * 4);
+    h.r_chain = lay.take(h.chain_comp.size() * 4);
+    h.r_generic = lay.take(h.generic_comp.size() * 4);
     h.r_pairs = lay.take(2 * E * 4);
     h.r_bpairs = lay.take(2 * B * 4);
     h.r_compn = lay.take((h.ncomp + 1) * 4);
@@ -696,24 +728,29 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     const long long HW = (long long)h.dims.H * h.dims.W;
     int cnt[K_COUNT];
     cnt[K_NODES] = div_up(h.dims.N, 256);
-    cnt[K_COMP] = h.dims.N > 0 ? h.ncomp : 0;
+    cnt[K_COMP] = h.dims.N > 0 ? (int)h.generic_comp.size() : 0;
+    cnt[K_CHAIN] = h.dims.N > 0 ? div_up((long long)h.chain_comp.size(), 4) : 0;
     cnt[K_IB] = div_up(h.M, 256);
-    cnt[K_CIC] = c.enable_steric ? div_up(4LL * h.dims.N, 256) : 0;
     cnt[K_TILES] = h.ntx * h.nty;
     cnt[K_LBM] = c.enable_fluid ? h.lbm_tx * h.lbm_ty : 0;
     cnt[K_CELLS] = std::min(div_up(HW, 256), 1024);
     cnt[K_FFTR] = c.enable_steric ? div_up(h.dims.H, 2) : 0;
     cnt[K_FFTC] = c.enable_steric ? div_up(h.dims.W, 2 * mc::kFftColsPerCta) : 0;
     for (int k = 0; k < K_COUNT; ++k) p->off[k][i + 1] = p->off[k][i] + cnt[k];
-    mcn = std::max(mcn, h.max_cn);
-    mce = std::max(mce, h.max_ce);
-    mcb = std::max(mcb, h.max_cb);
-    p->fftr_smem = std::max(p->fftr_smem, c.enable_steric ? (size_t)2 * h.dims.W * sizeof(float2) : 0);
+    if (!h.generic_comp.empty()) {
+      mcn = std::max(mcn, h.max_cn);
+      mce = std::max(mce, h.max_ce);
+      mcb = std::max(mcb, h.max_cb);
+    }
+    p->max_chain = std::max(p->max_chain, h.max_chain);
+    p->fftr_smem = std::max(p->fftr_smem, c.enable_steric ? (size_t)3 * h.dims.W * sizeof(float2) + h.dims.W * sizeof(float) : 0);
     p->fftc_smem = std::max(p->fftc_smem,
-                            c.enable_steric ? (size_t)2 * mc::kFftColsPerCta * h.dims.H * sizeof(float2) : 0);
+                            c.enable_steric ? (size_t)(2 * mc::kFftColsPerCta + 1) * h.dims.H * sizeof(float2) + h.dims.H * sizeof(float) : 0);
   }
   for (int k = 0; k < K_COUNT; ++k) p->grid[k] = p->off[k][n];
   p->node_smem = (size_t)(2 * mcn + 4 * mce + 3 * mcb) * sizeof(float);
+  p->chain_slots = 1;
+  while (p->chain_slots * 32 < p->max_chain) p->chain_slots *= 2;
   if (p->node_smem > 200 * 1024) {
     delete p;
     return fail(MC_ERR_UNSUPPORTED, "rod component too large for shared memory (> ~6000 nodes)");
@@ -763,6 +800,8 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
     MC_CUDA(up(h.r_nei, h.ne_idx.data(), h.ne_idx.size() * 4));
     MC_CUDA(up(h.r_edeg, h.edeg.data(), h.edeg.size() * 4));
     MC_CUDA(up(h.r_ndeg, h.ndeg.data(), h.ndeg.size() * 4));
+    MC_CUDA(up(h.r_chain, h.chain_comp.data(), h.chain_comp.size() * 4));
+    MC_CUDA(up(h.r_generic, h.generic_comp.data(), h.generic_comp.size() * 4));
     MC_CUDA(up(h.r_twW, h.twW.data(), h.twW.size() * 8));
     MC_CUDA(up(h.r_twH, h.twH.data(), h.twH.size() * 8));
     MC_CUDA(up(h.r_gW, h.gW.data(), h.gW.size() * 4));

@@ -34,7 +34,7 @@ __device__ __forceinline__ void stockham_pow2(const float2* __restrict__ in, flo
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       float2 a = x[j + r * S];
-      if (r > 0 && k > 0) a = cmul(a, __ldg(tw + r * k * twstep));
+      if (r > 0 && k > 0) a = cmul(a, tw[r * k * twstep]);
       v[r] = a;
     }
     if (R == 2) {
@@ -70,7 +70,7 @@ __device__ __noinline__ void stockham_generic(const float2* __restrict__ in, flo
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
       float2 a = x[j + r * S];
-      if (r > 0 && k > 0) a = cmul(a, __ldg(tw + r * k * twstep));
+      if (r > 0 && k > 0) a = cmul(a, tw[r * k * twstep]);
       v[r] = a;
     }
 #pragma unroll 1
@@ -78,7 +78,7 @@ __device__ __noinline__ void stockham_generic(const float2* __restrict__ in, flo
       float2 acc = v[0];
 #pragma unroll 1
       for (int r = 1; r < R; ++r) {
-        float2 p = cmul(v[r], __ldg(tw + ((r * q) % R) * rstep));
+        float2 p = cmul(v[r], tw[((r * q) % R) * rstep]);
         acc.x = acc.x + p.x;
         acc.y = acc.y + p.y;
       }
@@ -119,7 +119,7 @@ __device__ float2* filter_packed(float2* a, float2* b, int N, const int* fac, in
   float2* r = fft_forward(a, b, N, fac, nf, tw, nt);
   float2* o = (r == a) ? b : a;
   for (int idx = threadIdx.x; idx < nt * N; idx += blockDim.x) {
-    const float gk = __ldg(g + (idx % N));
+    const float gk = g[idx % N];
     float2 v = r[idx];
     r[idx] = make_float2(v.x * gk, -(v.y * gk));  // conj(G * X)
   }
@@ -140,11 +140,17 @@ __global__ void __launch_bounds__(256) k_fft_rows(const RDesc* __restrict__ D, c
   const int y0 = 2 * q, y1 = 2 * q + 1;
   float2* a = sm;
   float2* b = sm + W;
+  float2* tw = sm + 2 * W;
+  float* g = reinterpret_cast<float*>(sm + 3 * W);
   const float* r0 = d.dep + (size_t)y0 * W;
   const float* r1 = (y1 < H) ? d.dep + (size_t)y1 * W : nullptr;
-  for (int x = threadIdx.x; x < W; x += blockDim.x) a[x] = make_float2(r0[x], r1 ? r1[x] : 0.0f);
+  for (int x = threadIdx.x; x < W; x += blockDim.x) {
+    a[x] = make_float2(r0[x], r1 ? r1[x] : 0.0f);
+    tw[x] = d.twW[x];
+    g[x] = d.gW[x];
+  }
   __syncthreads();
-  float2* res = filter_packed(a, b, W, d.fftW_f, d.fftW_nf, d.twW, d.gW, 1);
+  float2* res = filter_packed(a, b, W, d.fftW_f, d.fftW_nf, tw, g, 1);
   float* o0 = d.tmp + (size_t)y0 * W;
   float* o1 = (y1 < H) ? d.tmp + (size_t)y1 * W : nullptr;
   for (int x = threadIdx.x; x < W; x += blockDim.x) {
@@ -164,6 +170,12 @@ __global__ void __launch_bounds__(256) k_fft_cols(const RDesc* __restrict__ D, c
   const int xbase = cblk * 2 * C;
   float2* a = sm;
   float2* b = sm + C * H;
+  float2* tw = sm + 2 * C * H;
+  float* g = reinterpret_cast<float*>(sm + 2 * C * H + H);
+  for (int y = threadIdx.x; y < H; y += blockDim.x) {
+    tw[y] = d.twH[y];
+    g[y] = d.gH[y];
+  }
   for (int idx = threadIdx.x; idx < C * H; idx += blockDim.x) {
     const int y = idx / C, t = idx - y * C;  // consecutive threads read consecutive columns
     const int xr = xbase + 2 * t, xi = xr + 1;
@@ -171,7 +183,7 @@ __global__ void __launch_bounds__(256) k_fft_cols(const RDesc* __restrict__ D, c
     a[t * H + y] = make_float2(xr < W ? row[xr] : 0.0f, xi < W ? row[xi] : 0.0f);
   }
   __syncthreads();
-  float2* res = filter_packed(a, b, H, d.fftH_f, d.fftH_nf, d.twH, d.gH, C);
+  float2* res = filter_packed(a, b, H, d.fftH_f, d.fftH_nf, tw, g, C);
   for (int idx = threadIdx.x; idx < C * H; idx += blockDim.x) {
     const int y = idx / C, t = idx - y * C;
     const int xr = xbase + 2 * t, xi = xr + 1;
