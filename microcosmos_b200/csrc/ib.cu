@@ -266,6 +266,66 @@ __global__ void __launch_bounds__(256) k_bin_tiles(const RDesc* __restrict__ D, 
   if (tid == 0) v.tcount[t] = 0;
 }
 
+// Weighted sum of a head-indexed field over the K*K stencil of one node, in stencil order
+// (the reference's sum over axis 1 of values * weights, fluid.py:90-97).
+template <int K2>
+__device__ __forceinline__ void stencil_sum(const RDesc& d, int node, const float* __restrict__ ax,
+                                            const float* __restrict__ ay, float& sx, float& sy) {
+  int slot[K2];
+  float w[K2];
+  const int base = node * K2;
+  if (K2 % 4 == 0) {
+#pragma unroll
+    for (int s = 0; s < K2; s += 4) {
+      const int4 q = *reinterpret_cast<const int4*>(d.ib_slot + base + s);
+      const float4 v = *reinterpret_cast<const float4*>(d.ib_w + base + s);
+      slot[s] = q.x; slot[s + 1] = q.y; slot[s + 2] = q.z; slot[s + 3] = q.w;
+      w[s] = v.x; w[s + 1] = v.y; w[s + 2] = v.z; w[s + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < K2; ++s) {
+      slot[s] = d.ib_slot[base + s];
+      w[s] = d.ib_w[base + s];
+    }
+  }
+  float vx[K2], vy[K2];
+#pragma unroll
+  for (int s = 0; s < K2; ++s) {
+    vx[s] = ax[slot[s]];
+    vy[s] = ay[slot[s]];
+  }
+  float x = 0.0f, y = 0.0f;
+#pragma unroll
+  for (int s = 0; s < K2; ++s) {
+    x = x + vx[s] * w[s];
+    y = y + vy[s] * w[s];
+  }
+  sx = x;
+  sy = y;
+}
+
+__device__ __forceinline__ void stencil_sum_any(const RDesc& d, int node, const float* __restrict__ ax,
+                                                const float* __restrict__ ay, float& sx, float& sy) {
+  switch (d.K) {
+    case 4: stencil_sum<16>(d, node, ax, ay, sx, sy); return;
+    case 2: stencil_sum<4>(d, node, ax, ay, sx, sy); return;
+    case 3: stencil_sum<9>(d, node, ax, ay, sx, sy); return;
+    default: break;
+  }
+  const int K2 = d.K * d.K;
+  float x = 0.0f, y = 0.0f;
+  for (int s = 0; s < K2; ++s) {
+    const int k = node * K2 + s;
+    const int p = d.ib_slot[k];
+    const float w = d.ib_w[k];
+    x = x + ax[p] * w;
+    y = y + ay[p] * w;
+  }
+  sx = x;
+  sy = y;
+}
+
 // Multi-direct forcing, interpolation half (fluid.py:292-302): per IB point, u at the point
 // = sum_s w_s u_corrected(cell_s); correction = (U_point - u) * relaxation, clamped.
 __global__ void __launch_bounds__(256) k_ib_interp(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
@@ -274,15 +334,8 @@ __global__ void __launch_bounds__(256) k_ib_interp(const RDesc* __restrict__ D, 
   const RDesc& d = D[r];
   const int node = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
   if (node >= d.N || it >= d.ib_iters) return;
-  const int K2 = d.K * d.K;
-  float ux = 0.0f, uy = 0.0f;
-  for (int s = 0; s < K2; ++s) {
-    const int k = node * K2 + s;
-    const int p = d.ib_slot[k];
-    const float w = d.ib_w[k];
-    ux = ux + d.s_ucx[p] * w;
-    uy = uy + d.s_ucy[p] * w;
-  }
+  float ux, uy;
+  stencil_sum_any(d, node, d.s_ucx, d.s_ucy, ux, uy);
   const float sx = (d.nvl[2 * node] - ux) * d.relax;
   const float sy = (d.nvl[2 * node + 1] - uy) * d.relax;
   const float cf = clamp_factor(sx, sy, d.vmax);
@@ -303,7 +356,27 @@ __global__ void __launch_bounds__(256) k_ib_spread(const RDesc* __restrict__ D, 
   const int* run = d.ib_store + d.h_start[p];
   const int K2 = d.K * d.K;
   float dx = 0.0f, dy = 0.0f;
-  for (int j = 0; j < len; ++j) {
+  int j = 0;
+  // runs are short: fetch up to 8 entries at a time so their loads overlap
+  for (; j + 8 <= len; j += 8) {
+    int k[8];
+    float w[8], ex[8], ey[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) k[q] = run[j + q];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int node = k[q] / K2;
+      w[q] = d.ib_w[k[q]];
+      ex[q] = d.delta[2 * node];
+      ey[q] = d.delta[2 * node + 1];
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      dx = dx + ex[q] * w[q];
+      dy = dy + ey[q] * w[q];
+    }
+  }
+  for (; j < len; ++j) {
     const int k = run[j];
     const int node = k / K2;
     const float w = d.ib_w[k];
@@ -359,15 +432,8 @@ __global__ void __launch_bounds__(256) k_reaction(const RDesc* __restrict__ D, c
   if (node >= d.N) return;
   float vx = d.vel[2 * node], vy = d.vel[2 * node + 1];
   if (d.enable_fluid) {
-    const int K2 = d.K * d.K;
-    float fx = 0.0f, fy = 0.0f;
-    for (int s = 0; s < K2; ++s) {
-      const int k = node * K2 + s;
-      const int p = d.ib_slot[k];
-      const float w = d.ib_w[k];
-      fx = fx + d.s_fx[p] * w;
-      fy = fy + d.s_fy[p] * w;
-    }
+    float fx, fy;
+    stencil_sum_any(d, node, d.s_fx, d.s_fy, fx, fy);
     vx = vx - (fx / d.node_mass) / d.sdt_x;
     vy = vy - (fy / d.node_mass) / d.sdt_y;
     d.vel[2 * node] = vx;

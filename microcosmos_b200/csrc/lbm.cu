@@ -33,6 +33,19 @@ __device__ __forceinline__ void pull_dir(const float* __restrict__ plane, int H,
       if (lane == 31 || x0c + 4 >= W) dn = __ldg(row + (x0c + 4 >= W ? x0c + 4 - W : x0c + 4));
       v[0] = a.y; v[1] = a.z; v[2] = a.w; v[3] = dn;
     }
+  } else if (VEC == 2) {
+    float2 a = __ldg(reinterpret_cast<const float2*>(row + x0c));
+    if (cx == 0) {
+      v[0] = a.x; v[1 % VEC] = a.y;
+    } else if (cx == 1) {
+      float up = __shfl_up_sync(0xffffffffu, a.y, 1);
+      if (lane == 0) up = __ldg(row + (x0c == 0 ? W - 1 : x0c - 1));
+      v[0] = up; v[1 % VEC] = a.x;
+    } else {
+      float dn = __shfl_down_sync(0xffffffffu, a.x, 1);
+      if (lane == 31 || x0c + 2 >= W) dn = __ldg(row + (x0c + 2 >= W ? x0c + 2 - W : x0c + 2));
+      v[0] = a.y; v[1 % VEC] = dn;
+    }
   } else {
     int xs = x0c - cx;
     xs = xs < 0 ? xs + W : (xs >= W ? xs - W : xs);
@@ -117,6 +130,14 @@ __global__ void __launch_bounds__(256) k_lbm(const RDesc* __restrict__ D, const 
           *reinterpret_cast<float4*>(d.fluid_vel + base) = make_float4(usx[0], usx[1], usx[2], usx[3]);
           *reinterpret_cast<float4*>(d.fluid_vel + HW + base) = make_float4(usy[0], usy[1], usy[2], usy[3]);
         }
+      } else if (VEC == 2) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+          *reinterpret_cast<float2*>(hout + i * HW + base) = make_float2(out[i][0], out[i][1 % VEC]);
+        if (write_u) {
+          *reinterpret_cast<float2*>(d.fluid_vel + base) = make_float2(usx[0], usx[1 % VEC]);
+          *reinterpret_cast<float2*>(d.fluid_vel + HW + base) = make_float2(usy[0], usy[1 % VEC]);
+        }
       } else {
 #pragma unroll
         for (int i = 0; i < 9; ++i) hout[i * HW + base] = out[i][0];
@@ -200,6 +221,8 @@ void launch_lbm(const Launch& L, int parity, int write_u, int vec) {
   dim3 block(32, kLbmTileY);
   if (vec == 4)
     k_lbm<4><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u);
+  else if (vec == 2)
+    k_lbm<2><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u);
   else
     k_lbm<1><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u);
 }

@@ -74,8 +74,10 @@ __device__ __forceinline__ void collide(const float f[9], float rho, float vx, f
                                         float wp, float wm, float cp, float cm, float out[9],
                                         float& usx_o, float& usy_o) {
   const float half = 0.5f;
-  float usx = vx + (half * Fx) / rho;
-  float usy = vy + (half * Fy) / rho;
+  const bool force = !(Fx == 0.0f && Fy == 0.0f);
+  // with F = 0, u* = u + (0.5 * 0) / rho = u exactly
+  float usx = force ? vx + (half * Fx) / rho : vx;
+  float usy = force ? vy + (half * Fy) / rho : vy;
   float usq = usx * usx + usy * usy;
   float eu[9];
   eu[0] = 0.0f;
@@ -113,7 +115,7 @@ __device__ __forceinline__ void collide(const float f[9], float rho, float vx, f
     out[i] = (f[i] - wp * sym) - wm * anti;
     out[o] = (f[o] - wp * sym) - wm * (-anti);
   }
-  if (Fx == 0.0f && Fy == 0.0f) {
+  if (!force) {
     // zero force: the Guo source is exactly zero and u* = u
 #pragma unroll
     for (int i = 0; i < 9; ++i) out[i] = max_prop(out[i], MC_EPSIL);

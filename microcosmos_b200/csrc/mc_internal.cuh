@@ -92,6 +92,7 @@ struct RDesc {
   float* tmp;          // (H,W) FFT row-pass output
   float* prev;         // (N,2)
   float* pred;         // (N,2)
+  float* predw;        // (N,2) prediction wrapped into the domain (steric sampling)
   float* nvl;          // (N,2) node velocity in lattice units
   float* delta;        // (N,2) IB per-iteration correction
   // Deterministic scatter-add bins.  Contribution k goes to bin tile t at
@@ -147,9 +148,22 @@ __device__ __forceinline__ int find_rollout(const int* __restrict__ off, int n, 
   return lo;
 }
 
-// Floored float modulo, the semantics of jnp.mod / numpy.mod for floats.
+// Floored float modulo, the semantics of jnp.mod / numpy.mod for floats (y > 0 here):
+// r = fmodf(x, y); r += y if r is nonzero with the sign opposite to y.
+// For |x| < 2y, fmodf(x, y) is x or x -/+ y, and both subtractions are exact (Sterbenz),
+// so the shortcut below returns the same bits as the fmodf route.
 __device__ __forceinline__ float fmod_floor(float x, float y) {
-  float r = fmodf(x, y);
+  float r;
+  if (fabsf(x) < 2.0f * y) {
+    if (x >= 0.0f) {
+      r = (x >= y) ? x - y : x;
+    } else {
+      r = (x <= -y) ? x + y : x;
+      if (r < 0.0f) r += y;
+    }
+    return r;
+  }
+  r = fmodf(x, y);
   if (r != 0.0f && ((r < 0.0f) != (y < 0.0f))) r += y;
   return r;
 }

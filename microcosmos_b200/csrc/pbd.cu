@@ -50,6 +50,8 @@ __global__ void __launch_bounds__(256) k_predict(const RDesc* __restrict__ D, co
   // update_steric_potential (forces.py:84-115): CIC weights of the wrapped prediction
   const float W = (float)d.W, H = (float)d.H;
   const float x = fmod_floor(qx, W), y = fmod_floor(qy, H);
+  d.predw[2 * node] = x;
+  d.predw[2 * node + 1] = y;
   const float fx = floorf(x), fy = floorf(y);
   const int x0 = imod_floor((int)fx, d.W), y0 = imod_floor((int)fy, d.H);
   const int x1 = (x0 + 1) % d.W, y1 = (y0 + 1) % d.H;
@@ -87,7 +89,7 @@ __device__ __forceinline__ float sample_wrap(const float* __restrict__ V, int H,
 // gi-n..gi+n (the 0 <= j < N mask only, as in the reference).
 __device__ float2 steric_force(const RDesc& d, int gi) {
   const float W = (float)d.W, H = (float)d.H;
-  const float px = fmod_floor(d.pred[2 * gi], W), py = fmod_floor(d.pred[2 * gi + 1], H);
+  const float px = d.predw[2 * gi], py = d.predw[2 * gi + 1];
   const float* V = d.steric;
   const float gx = (sample_wrap(V, d.H, d.W, py, px + 0.5f) - sample_wrap(V, d.H, d.W, py, px - 0.5f)) / 1.0f;
   const float gy = (sample_wrap(V, d.H, d.W, py + 0.5f, px) - sample_wrap(V, d.H, d.W, py - 0.5f, px)) / 1.0f;
@@ -99,7 +101,7 @@ __device__ float2 steric_force(const RDesc& d, int gi) {
       const int j = gi + o;
       const float valid = (j >= 0 && j < d.N) ? 1.0f : 0.0f;
       const int js = j < 0 ? 0 : (j >= d.N ? d.N - 1 : j);
-      const float qx = fmod_floor(d.pred[2 * js], W), qy = fmod_floor(d.pred[2 * js + 1], H);
+      const float qx = d.predw[2 * js], qy = d.predw[2 * js + 1];
       const float2 rr = min_image(px, py, qx, qy, W, H);
       const float d2 = rr.x * rr.x + rr.y * rr.y;
       const float K = expf(-d2 / d.st_2s2) / d.st_norm;
@@ -260,8 +262,9 @@ __global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, cons
       ra[q] = rest_angle(d, b0 + j, t);
       kb[q] = d.kb[b0 + j];
     }
-    edg[q] = fmaxf((float)((j < nb) + (j >= 1 && j - 1 < nb)), 1.0f);
-    ndg[q] = fmaxf((float)((j < ne) + (j >= 1 && j - 1 < ne)), 1.0f);
+    // chain degrees are 1 or 2, so x / deg == x * (1 / deg) exactly
+    edg[q] = ((j < nb) + (j >= 1 && j - 1 < nb)) == 2 ? 0.5f : 1.0f;
+    ndg[q] = ((j < ne) + (j >= 1 && j - 1 < ne)) == 2 ? 0.5f : 1.0f;
   }
   const int cycles = d.cycles;
   for (int it = 0; it < cycles; ++it) {
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, cons
         float acc = 0.0f;
         if (j < nb) acc = acc + c[q];
         if (j >= 1 && j - 1 < nb) acc = acc + (-pv[q]);
-        th[q] = th[q] + (acc / edg[q]) * 1.8f;
+        th[q] = th[q] + (acc * edg[q]) * 1.8f;
       }
     }
     float xn[P], yn[P], fx[P], fy[P], fxp[P], fyp[P];
@@ -307,8 +310,8 @@ __global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, cons
           ax = ax + (-fxp[q]);
           ay = ay + (-fyp[q]);
         }
-        x[q] = x[q] + ax / ndg[q];
-        y[q] = y[q] + ay / ndg[q];
+        x[q] = x[q] + ax * ndg[q];
+        y[q] = y[q] + ay * ndg[q];
       }
     }
   }

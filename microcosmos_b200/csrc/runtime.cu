@@ -59,7 +59,7 @@ struct HostRollout {
   std::vector<float> gW, gH;
   int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4;
   // workspace regions (offsets relative to the workspace base)
-  Region r_h0, r_h1, r_fov, r_lflag, r_dep, r_tmp, r_prev, r_pred, r_nvl, r_delta;
+  Region r_h0, r_h1, r_fov, r_lflag, r_dep, r_tmp, r_prev, r_pred, r_predw, r_nvl, r_delta;
   Region r_ibcell, r_ibw, r_ibstore, r_ibtc, r_ibovf, r_ibctl, r_ibslot, r_hcell, r_hstart, r_hlen, r_srho, r_svx,
       r_svy, r_sinv, r_sucx, r_sucy, r_sfx, r_sfy;
   Region r_ccell, r_cw, r_cstore, r_ctc, r_covf, r_cctl, r_chain, r_generic;
@@ -85,9 +85,13 @@ struct mc_plan {
   int max_chain = 0, chain_slots = 1;
   std::vector<RDesc> desc;
   cudaStream_t cap_stream = nullptr;
-  // CUDA graphs, keyed by [steps-1][parity][recording variant][write_u]
-  cudaGraphExec_t graph[2][2][3][2] = {};
-  int64_t graph_kernels[2][2][3][2] = {};
+  // CUDA graphs, keyed by [steps-1][parity][recording variant][write_u][runs next pipeline]
+  cudaGraphExec_t graph[2][2][3][2][2] = {};
+  int64_t graph_kernels[2][2][3][2][2] = {};
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool pending_next = false;  // the next step's pipeline has already been launched
+  bool need_pipeline = false; // step 0's pipeline is still to be launched
   int64_t last_launches = 0;
   // rollout in progress (mc_rollout_begin .. mc_rollout_end)
   bool active = false;
@@ -401,6 +405,7 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.tmp = at<float>(b, h.r_tmp);
   d.prev = at<float>(b, h.r_prev);
   d.pred = at<float>(b, h.r_pred);
+  d.predw = at<float>(b, h.r_predw);
   d.nvl = at<float>(b, h.r_nvl);
   d.delta = at<float>(b, h.r_delta);
   d.ib_cap = mc::kIbCap;
@@ -481,8 +486,15 @@ void timed(mc_plan* p, int kind, cudaStream_t s, bool capture, F&& launch) {
   p->ev_pending.push_back({kind, a, b});
 }
 
-// The launch sequence of one step (src/microcosmos/simulate.py:37-100).
-int64_t enqueue_step(mc_plan* p, int parity, int write_u, int rec_fields, cudaStream_t s, bool capture) {
+// One step (src/microcosmos/simulate.py:37-100) is launched as three pieces:
+//   pipeline(t): predict, CIC deposit, steric filter, rod kernels      (simulate.py:41-84)
+//   ib(t):       IB bins, multi-direct forcing iterations, body force   (fluid.py:268-339)
+//   lbm(t):      the dense stream + collide pass                        (fluid.py:341-357)
+//   tail(t):     node reaction, wrap, recording, step counter           (fluid.py:359-382)
+// pipeline(t+1) depends only on tail(t), so it runs on a second stream concurrently with
+// lbm(t); ib(t+1) joins both.  Per-step field recording needs lbm(t) before tail(t)'s
+// field copy and before pipeline(t+1) rewrites the steric field, so it runs sequentially.
+int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
   int* tdev = at<int>(p->ws, p->r_tdev);
   int64_t k = 0;
   if (p->grid[K_NODES]) {
@@ -490,7 +502,7 @@ int64_t enqueue_step(mc_plan* p, int parity, int write_u, int rec_fields, cudaSt
     ++k;
   }
   if (p->any_steric) {
-    timed(p, 1, s, capture, [&] { mc::launch_bin_tiles(L(p, K_TILES, s), 1, parity); });
+    timed(p, 1, s, capture, [&] { mc::launch_bin_tiles(L(p, K_TILES, s), 1, 0); });
     timed(p, 2, s, capture, [&] { mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem); });
     timed(p, 3, s, capture, [&] { mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem); });
     k += 3;
@@ -503,18 +515,32 @@ int64_t enqueue_step(mc_plan* p, int parity, int write_u, int rec_fields, cudaSt
     timed(p, 5, s, capture, [&] { mc::launch_node(L(p, K_COMP, s), tdev, p->node_smem, p->node_bs); });
     ++k;
   }
-  if (p->any_fluid) {
-    timed(p, 6, s, capture, [&] { mc::launch_bin_tiles(L(p, K_TILES, s), 0, parity); });
-    ++k;
-    for (int it = 0; it < p->max_iters; ++it) {
-      timed(p, 7, s, capture, [&] { mc::launch_ib_interp(L(p, K_NODES, s), it); });
-      timed(p, 8, s, capture, [&] { mc::launch_ib_spread(L(p, K_IB, s), it); });
-      k += 2;
-    }
-    timed(p, 9, s, capture, [&] { mc::launch_ib_finalize(L(p, K_IB, s)); });
-    timed(p, 10, s, capture, [&] { mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->R[0].vec); });
+  return k;
+}
+
+int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
+  if (!p->any_fluid) return 0;
+  int64_t k = 0;
+  timed(p, 6, s, capture, [&] { mc::launch_bin_tiles(L(p, K_TILES, s), 0, parity); });
+  ++k;
+  for (int it = 0; it < p->max_iters; ++it) {
+    timed(p, 7, s, capture, [&] { mc::launch_ib_interp(L(p, K_NODES, s), it); });
+    timed(p, 8, s, capture, [&] { mc::launch_ib_spread(L(p, K_IB, s), it); });
     k += 2;
   }
+  timed(p, 9, s, capture, [&] { mc::launch_ib_finalize(L(p, K_IB, s)); });
+  return k + 1;
+}
+
+int64_t enqueue_lbm(mc_plan* p, int parity, int write_u, cudaStream_t s, bool capture) {
+  if (!p->any_fluid) return 0;
+  timed(p, 10, s, capture, [&] { mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->R[0].vec); });
+  return 1;
+}
+
+int64_t enqueue_tail(mc_plan* p, int rec_fields, cudaStream_t s, bool capture) {
+  int* tdev = at<int>(p->ws, p->r_tdev);
+  int64_t k = 0;
   if (p->grid[K_NODES]) {
     timed(p, 11, s, capture, [&] { mc::launch_reaction(L(p, K_NODES, s), tdev); });
     ++k;
@@ -524,28 +550,63 @@ int64_t enqueue_step(mc_plan* p, int parity, int write_u, int rec_fields, cudaSt
     ++k;
   }
   timed(p, 13, s, capture, [&] { mc::launch_tick(tdev, s); });
-  ++k;
+  return k + 1;
+}
+
+// Everything of step t after its pipeline, plus pipeline(t+1) when has_next.
+int64_t enqueue_body(mc_plan* p, int parity, int write_u, int rec_fields, bool has_next, cudaStream_t s,
+                     bool capture, mc_status* err) {
+  int64_t k = enqueue_ib(p, parity, s, capture);
+  if (rec_fields) {
+    k += enqueue_lbm(p, parity, write_u, s, capture);
+    k += enqueue_tail(p, rec_fields, s, capture);
+    if (has_next) k += enqueue_pipeline(p, s, capture);
+    return k;
+  }
+  cudaStream_t s2 = p->side_stream;
+  cudaError_t e = cudaEventRecord(p->ev_fork, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, p->ev_fork, 0);
+  if (e != cudaSuccess) {
+    *err = cuda_fail(e, "fork to the side stream");
+    return k;
+  }
+  k += enqueue_tail(p, 0, s2, capture);
+  if (has_next) k += enqueue_pipeline(p, s2, capture);
+  k += enqueue_lbm(p, parity, write_u, s, capture);
+  e = cudaEventRecord(p->ev_join, s2);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, p->ev_join, 0);
+  if (e != cudaSuccess) *err = cuda_fail(e, "join from the side stream");
   return k;
 }
 
 mc_status run_steps(mc_plan* p, int num, int use_graph, int last, cudaStream_t s, int64_t& launches) {
   const int recv = p->rec_fields ? (p->rec_fluid ? 2 : 1) : 0;
+  if (p->need_pipeline && num > 0) {
+    launches += enqueue_pipeline(p, s, false);
+    p->need_pipeline = false;
+  }
   int remaining = num;
   while (remaining > 0) {
     const int parity = p->step & 1;
     const bool is_last = last && remaining == 1;
     const int write_u = (is_last || p->rec_fluid) ? 1 : 0;
+    const bool has_next = !is_last;
+    mc_status err = MC_OK;
     if (use_graph && !p->profiling) {
+      // two steps per graph where possible (parity 0 then 1, neither the final step)
       const int ns = (parity == 0 && remaining >= 3) ? 2 : 1;
       const int wu = ns == 2 ? p->rec_fluid : write_u;
-      cudaGraphExec_t& g = p->graph[ns - 1][parity][recv][wu];
+      const int nx = has_next ? 1 : 0;
+      cudaGraphExec_t& g = p->graph[ns - 1][parity][recv][wu][nx];
       if (!g) {
         cudaGraph_t graph;
         MC_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
         int64_t kk = 0;
-        for (int j = 0; j < ns; ++j)
-          kk += enqueue_step(p, (parity + j) & 1, wu, p->rec_fields, p->cap_stream, true);
+        for (int j = 0; j < ns && err == MC_OK; ++j)
+          kk += enqueue_body(p, (parity + j) & 1, wu, p->rec_fields, j + 1 < ns ? true : has_next, p->cap_stream,
+                             true, &err);
         cudaError_t e = cudaStreamEndCapture(p->cap_stream, &graph);
+        if (err != MC_OK) return err;
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
         e = cudaGraphInstantiate(&g, graph, 0);
         cudaGraphDestroy(graph);
@@ -553,17 +614,20 @@ mc_status run_steps(mc_plan* p, int num, int use_graph, int last, cudaStream_t s
           g = nullptr;
           return cuda_fail(e, "cudaGraphInstantiate");
         }
-        p->graph_kernels[ns - 1][parity][recv][wu] = kk;
+        p->graph_kernels[ns - 1][parity][recv][wu][nx] = kk;
       }
       MC_CUDA(cudaGraphLaunch(g, s));
-      launches += p->graph_kernels[ns - 1][parity][recv][wu];
+      launches += p->graph_kernels[ns - 1][parity][recv][wu][nx];
       p->step += ns;
       remaining -= ns;
+      p->pending_next = has_next;
       continue;
     }
-    launches += enqueue_step(p, parity, write_u, p->rec_fields, s, false);
+    launches += enqueue_body(p, parity, write_u, p->rec_fields, has_next, s, false, &err);
+    if (err != MC_OK) return err;
     p->step += 1;
     remaining -= 1;
+    p->pending_next = has_next;
   }
   return MC_OK;
 }
@@ -572,11 +636,12 @@ void destroy_graphs(mc_plan* p) {
   for (auto& a : p->graph)
     for (auto& b : a)
       for (auto& c : b)
-        for (auto& g : c)
-          if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-          }
+        for (auto& e : c)
+          for (auto& g : e)
+            if (g) {
+              cudaGraphExecDestroy(g);
+              g = nullptr;
+            }
 }
 
 }  // namespace
@@ -648,7 +713,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       fft_tables(D.W, c.steric_sigma, h.twW, h.gW);
       fft_tables(D.H, c.steric_sigma, h.twH, h.gH);
     }
-    h.vec = (D.W % 4 == 0) ? 4 : 1;
+    h.vec = (D.W % 2 == 0) ? 2 : 1;
     if (vec_all == -1) vec_all = h.vec;
     if (vec_all != h.vec) vec_all = 1;
     h.ntx = div_up(D.W, mc::kBinTile);
@@ -662,6 +727,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.r_tmp = lay.take(HW * 4);
     h.r_prev = lay.take(2 * N * 4);
     h.r_pred = lay.take(2 * N * 4);
+    h.r_predw = lay.take(2 * N * 4);
     h.r_nvl = lay.take(2 * N * 4);
     h.r_delta = lay.take(2 * N * 4);
     const size_t Mz = (size_t)M;
@@ -771,6 +837,9 @@ void mc_plan_destroy(mc_plan* p) {
   }
   for (auto e : p->ev_pool) cudaEventDestroy(e);
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+  if (p->side_stream) cudaStreamDestroy(p->side_stream);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
   delete p;
 }
 
@@ -817,6 +886,9 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
   MC_CUDA(cudaGetLastError());
   destroy_graphs(p);
   if (!p->cap_stream) MC_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+  if (!p->side_stream) MC_CUDA(cudaStreamCreateWithFlags(&p->side_stream, cudaStreamNonBlocking));
+  if (!p->ev_fork) MC_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+  if (!p->ev_join) MC_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
   p->bound = true;
   return MC_OK;
 }
@@ -860,6 +932,8 @@ mc_status mc_rollout_begin(mc_plan* p, const mc_state* states, const mc_actuatio
     mc::launch_unstream(L(p, K_CELLS, s));
     p->last_launches += 1;
   }
+  p->need_pipeline = true;  // the first advance launches step 0's pipeline
+  p->pending_next = false;
   MC_CUDA(cudaGetLastError());
   return MC_OK;
 }
@@ -881,6 +955,10 @@ mc_status mc_rollout_end(mc_plan* p, void* stream) {
   g_err.clear();
   if (!p) return fail(MC_ERR_INVALID, "null plan");
   if (!p->active) return fail(MC_ERR_INVALID, "mc_rollout_begin() was not called");
+  if (p->pending_next) {
+    p->active = false;
+    return fail(MC_ERR_INVALID, "the last mc_rollout_advance() before mc_rollout_end() must pass last != 0");
+  }
   if (p->any_fluid) {
     mc::launch_stream_out(L(p, K_CELLS, (cudaStream_t)stream), p->step & 1);
     p->last_launches += 1;

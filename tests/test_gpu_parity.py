@@ -209,3 +209,31 @@ def test_non_finite_state_is_flagged():
     torch.cuda.synchronize()
     assert plan.read_flags(clear=True) == [1]
     assert plan.read_flags() == [0]
+
+
+def test_pipelined_and_sequential_schedules_agree():
+    """Without field recording the next step's node pipeline overlaps the dense pass on a
+    second stream; with it the step runs sequentially.  Both give the same bits."""
+    sc = scenarios.make_scenario(96, 128, 5, 30, seed=21)
+    cfg = baseline_config()
+    outs = []
+    for record in (False, True):
+        st = DeviceState.from_scenario(sc)
+        plan = Plan.for_states([st], [cfg], [0.01])
+        rec = Record.allocate(st, 11, every=1) if record else None
+        plan.rollout([st], 11, actuations=[Actuation.from_scenario(sc)], records=[rec])
+        torch.cuda.synchronize()
+        outs.append(st.host())
+    for k in outs[0]:
+        np.testing.assert_array_equal(outs[0][k], outs[1][k])
+
+
+def test_zero_steps_leave_state_unchanged():
+    sc = scenarios.make_scenario(32, 32, 2, 10, seed=8)
+    st = DeviceState.from_scenario(sc)
+    plan = Plan.for_states([st], [baseline_config()], [0.01])
+    plan.rollout([st], 0, actuations=[Actuation.from_scenario(sc)])
+    torch.cuda.synchronize()
+    out = st.host()
+    np.testing.assert_array_equal(out["position"], sc.position)
+    np.testing.assert_array_equal(out["f_grid"], sc.f_grid)
