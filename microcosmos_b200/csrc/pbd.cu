@@ -15,9 +15,19 @@ __device__ __forceinline__ int bin_tile(const RDesc& d, int cy, int cx) {
   return (cy / kBinTile) * d.ntile_x + cx / kBinTile;
 }
 
-// Append contribution k of cell (cy, cx) to its tile's bin (or the overflow list).
+// Append contribution k to bin `tile` (or the overflow list).  Lanes of a warp that push to
+// the same tile are grouped (__match_any_sync) and take their slots with one atomic, which
+// keeps the counters of busy tiles from serialising.  Slot order inside a bin is arbitrary;
+// the per-tile sort restores the reference order.
 __device__ __forceinline__ void bin_push(int* store, int* tcount, int* ovf, int* ctl, int cap, int tile, int k) {
-  const int pos = atomicAdd(tcount + tile, 1);
+  const unsigned active = __activemask();
+  const unsigned group = __match_any_sync(active, tile);
+  const int leader = __ffs(group) - 1;
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(tcount + tile, __popc(group));
+  base = __shfl_sync(group, base, leader);
+  const int pos = base + __popc(group & ((1u << lane) - 1u));
   if (pos < cap) {
     store[(size_t)tile * cap + pos] = k;
   } else {

@@ -557,7 +557,8 @@ int64_t enqueue_tail(mc_plan* p, int rec_fields, cudaStream_t s, bool capture) {
 int64_t enqueue_body(mc_plan* p, int parity, int write_u, int rec_fields, bool has_next, cudaStream_t s,
                      bool capture, mc_status* err) {
   int64_t k = enqueue_ib(p, parity, s, capture);
-  if (rec_fields) {
+  if (rec_fields || p->profiling) {
+    // sequential: field recording needs this order; profiling times kernels one at a time
     k += enqueue_lbm(p, parity, write_u, s, capture);
     k += enqueue_tail(p, rec_fields, s, capture);
     if (has_next) k += enqueue_pipeline(p, s, capture);
