@@ -390,7 +390,8 @@ __global__ void __launch_bounds__(256) k_ib_spread(const RDesc* __restrict__ D, 
 
 // Post-accumulation clamp and body force F = (u_corrected - u) rho (fluid.py:327-339),
 // published to the dense pass through the force overlay.
-__global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+__global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
+                                                     int parity) {
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D
   d.fov[cell] = Fx;
   d.fov[HW + cell] = Fy;
   const int y = cell / d.W, x = cell - y * d.W;
-  d.lbm_flag[(y / kLbmTileY) * d.lbm_tx + x / d.lbm_tw] = 1;
+  d.lbm_flag[(parity & 1) * d.lbm_tx * d.lbm_ty + (y / kLbmTileY) * d.lbm_tx + x / d.lbm_tw] = 1;
 }
 
 // Node reaction (fluid.py:364-382), final wrap (simulate.py:97-98), non-finite check and
@@ -487,7 +488,9 @@ void launch_bin_tiles(const Launch& L, int which, int parity) {
 }
 void launch_ib_interp(const Launch& L, int it) { k_ib_interp<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
 void launch_ib_spread(const Launch& L, int it) { k_ib_spread<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
-void launch_ib_finalize(const Launch& L) { k_ib_finalize<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
+void launch_ib_finalize(const Launch& L, int parity) {
+  k_ib_finalize<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, parity);
+}
 void launch_reaction(const Launch& L, const int* tdev) { k_reaction<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, tdev); }
 void launch_record_fields(const Launch& L, const int* tdev) {
   k_record_fields<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, tdev);

@@ -70,9 +70,12 @@ __global__ void __launch_bounds__(256) k_lbm(const RDesc* __restrict__ D, const 
   const size_t HW = (size_t)H * W;
   const float* __restrict__ hin = d.h[parity];
   float* __restrict__ hout = d.h[parity ^ 1];
+  // tile flags are double-buffered by step parity: this step's finalize set flag[parity];
+  // the other set belongs to the previous step and is cleared here for the next one
+  const int nflag = d.lbm_tx * d.lbm_ty;
   const int flag_idx = ty * d.lbm_tx + tx;
-  const bool has_ov = d.lbm_flag[flag_idx] != 0;
-  __syncthreads();  // every thread has read the tile flag before it is cleared below
+  const bool has_ov = d.lbm_flag[parity * nflag + flag_idx] != 0;
+  if (threadIdx.x == 0 && threadIdx.y == 0) d.lbm_flag[(parity ^ 1) * nflag + flag_idx] = 0;
 
   if (row_ok) {
     float fin[9][VEC];
@@ -148,10 +151,6 @@ __global__ void __launch_bounds__(256) k_lbm(const RDesc* __restrict__ D, const 
       }
     }
   }
-  if (has_ov) {
-    __syncthreads();
-    if (threadIdx.x == 0 && threadIdx.y == 0) d.lbm_flag[flag_idx] = 0;
-  }
 }
 
 // h_i(y, x) = f_grid_i((y + cy) % H, (x + cx) % W): the inverse of the push streaming, so
@@ -168,7 +167,7 @@ __global__ void k_unstream(const RDesc* __restrict__ D, const int* __restrict__ 
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
       int ys = imod_floor(y + ey[i], d.H), xs = imod_floor(x + ex[i], d.W);
-      d.h[0][i * HW + idx] = d.f_grid[i * HW + (size_t)ys * d.W + xs];
+      d.h[0][i * HW + idx] = max_prop(d.f_grid[i * HW + (size_t)ys * d.W + xs], MC_EPSIL);
     }
   }
 }
@@ -209,7 +208,7 @@ __global__ void k_clear_ws(const RDesc* __restrict__ D, const int* __restrict__ 
     d.ib_tcount[i] = 0;
     d.c_tcount[i] = 0;
   }
-  for (size_t i = t0; i < (size_t)d.lbm_tx * d.lbm_ty; i += stride) d.lbm_flag[i] = 0;
+  for (size_t i = t0; i < (size_t)2 * d.lbm_tx * d.lbm_ty; i += stride) d.lbm_flag[i] = 0;
   if (t0 < 4) {
     d.ib_ctl[t0] = 0;
     d.c_ctl[t0] = 0;

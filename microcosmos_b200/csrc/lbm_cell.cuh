@@ -29,11 +29,11 @@ __device__ __forceinline__ float clamp_factor_fast(float x, float y, float vmax,
   return min_prop(1.0f, vmax / (sqrtf(m2) + MC_EPSIL));
 }
 
-// f = max(f, EPSIL); rho = max(sum f, 0.1); u = sum e f / rho; velocity clamp
-// (fluid.py:136-142, 268-274).  Returns rho and the clamped velocity.
-__device__ __forceinline__ void macroscopic(float f[9], float vmax, float q4, float& rho, float& vx, float& vy) {
-#pragma unroll
-  for (int i = 0; i < 9; ++i) f[i] = max_prop(f[i], MC_EPSIL);
+// rho = max(sum f, 0.1); u = sum e f / rho; velocity clamp (fluid.py:136-142, 268-274).
+// The reference first floors f at EPSIL (fluid.py:268); the pull-scheme state only holds
+// values that already passed that floor (the entry conversion applies it, every
+// collision output re-applies it), so f is used as is.  Returns rho and the clamped velocity.
+__device__ __forceinline__ void macroscopic(const float f[9], float vmax, float q4, float& rho, float& vx, float& vy) {
   float r = f[0];
 #pragma unroll
   for (int i = 1; i < 9; ++i) r = r + f[i];

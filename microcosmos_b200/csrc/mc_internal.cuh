@@ -87,7 +87,7 @@ struct RDesc {
   // workspace
   float* h[2];         // pull-scheme post-collision populations (9,H,W)
   float* fov;          // (2,H,W) force overlay, NaN = no IB force at the cell
-  int* lbm_flag;       // (lbm_ty*lbm_tx) tile has overlay entries
+  int* lbm_flag;       // (2 * lbm_ty*lbm_tx) tile has overlay entries, one set per step parity
   float* dep;          // (H,W) CIC deposit (kept zero between steps)
   float* tmp;          // (H,W) FFT row-pass output
   float* prev;         // (N,2)
@@ -200,9 +200,11 @@ void launch_fft_rows(const Launch& L, size_t smem);
 void launch_fft_cols(const Launch& L, size_t smem);
 void launch_node(const Launch& L, const int* tdev, size_t smem, int bs);
 void launch_chain(const Launch& L, const int* tdev, int slots);
+void launch_steric(const Launch& L);
+void launch_stencil(const Launch& L);
 void launch_ib_interp(const Launch& L, int it);
 void launch_ib_spread(const Launch& L, int it);
-void launch_ib_finalize(const Launch& L);
+void launch_ib_finalize(const Launch& L, int parity);
 void launch_lbm(const Launch& L, int parity, int write_u, int vec);
 void launch_reaction(const Launch& L, const int* tdev);
 void launch_record_fields(const Launch& L, const int* tdev);

@@ -1,39 +1,19 @@
 // Node-side kernels of one step (src/microcosmos/simulate.py:37-84):
 //   k_predict: damping, inertial prediction, steric cloud-in-cell contributions;
+//   k_steric:  per node, the steric force added to the prediction (forces.py:41-81);
 //   k_chain:   one warp per chain rod (the topology make_edges(.., "line", F) builds),
 //              node/edge state in registers, neighbours exchanged with shuffles;
 //   k_node:    one CTA per rod of any other topology (trees, loops), state in shared
 //              memory, scatter-adds as gather lists in the reference's order.
-// Both rod kernels compute the steric force (forces.py:41-81), the curvature actuation,
-// cycles_per_step Jacobi iterations of pbd_rod_constraint (solver/pbd.py:14-91), the
-// velocity from positions, and every node's IB stencil (solver/fluid.py:40-87).
+//   k_stencil: per node, the velocity from positions and the IB stencil (fluid.py:40-87).
+// Both rod kernels evaluate the curvature actuation and run cycles_per_step Jacobi
+// iterations of pbd_rod_constraint (solver/pbd.py:14-91).
 #include "lbm_cell.cuh"
 
 namespace mc {
 
 __device__ __forceinline__ int bin_tile(const RDesc& d, int cy, int cx) {
   return (cy / kBinTile) * d.ntile_x + cx / kBinTile;
-}
-
-// Append contribution k to bin `tile` (or the overflow list).  Lanes of a warp that push to
-// the same tile are grouped (__match_any_sync) and take their slots with one atomic, which
-// keeps the counters of busy tiles from serialising.  Slot order inside a bin is arbitrary;
-// the per-tile sort restores the reference order.
-__device__ __forceinline__ void bin_push(int* store, int* tcount, int* ovf, int* ctl, int cap, int tile, int k) {
-  const unsigned active = __activemask();
-  const unsigned group = __match_any_sync(active, tile);
-  const int leader = __ffs(group) - 1;
-  const int lane = threadIdx.x & 31;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(tcount + tile, __popc(group));
-  base = __shfl_sync(group, base, leader);
-  const int pos = base + __popc(group & ((1u << lane) - 1u));
-  if (pos < cap) {
-    store[(size_t)tile * cap + pos] = k;
-  } else {
-    const int o = atomicAdd(ctl, 1);
-    ovf[o] = k;
-  }
 }
 
 __global__ void __launch_bounds__(256) k_predict(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
@@ -70,12 +50,39 @@ __global__ void __launch_bounds__(256) k_predict(const RDesc* __restrict__ D, co
   const float w[4] = {((1.0f - dx) * (1.0f - dy)) * s, (dx * (1.0f - dy)) * s, ((1.0f - dx) * dy) * s, (dx * dy) * s};
   const int cy[4] = {y0, y0, y1, y1};
   const int cx[4] = {x0, x1, x0, x1};
+  int tile[4], first[4], cnt[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    tile[c] = bin_tile(d, cy[c], cx[c]);
+    first[c] = c;
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (e < c && tile[e] == tile[c] && first[c] == c) first[c] = e;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    cnt[c] = 0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) cnt[c] += (first[e] == c) ? 1 : 0;
+  }
+  int base[4], rank[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    base[c] = cnt[c] ? atomicAdd(d.c_tcount + tile[c], cnt[c]) : 0;
+    rank[c] = 0;
+  }
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
     const int k = c * d.N + node;
     d.c_cell[k] = cy[c] * d.W + cx[c];
     d.c_w[k] = w[c];
-    bin_push(d.c_store, d.c_tcount, d.c_ovf, d.c_ctl, d.c_cap, bin_tile(d, cy[c], cx[c]), k);
+    const int g = first[c];
+    const int pos = base[g] + rank[g]++;
+    if (pos < d.c_cap) {
+      d.c_store[(size_t)tile[c] * d.c_cap + pos] = k;
+    } else {
+      d.c_ovf[atomicAdd(d.c_ctl, 1)] = k;
+    }
   }
 }
 
@@ -165,13 +172,17 @@ __device__ __forceinline__ float2 edge_force(const RDesc& d, float th, float L0,
   return make_float2(((stx + shx * d.k_shear) * d.k_stretch) * 0.5f, ((sty + shy * d.k_shear) * d.k_stretch) * 0.5f);
 }
 
-// After the iterations: velocity (simulate.py:83-84), the IB point in lattice units
-// (fluid.py:236-239), its K x K stencil (fluid.py:40-79) appended to the IB bins, and the
-// clearing of the node's CIC deposit cells (the deposit grid stays zero between steps).
-__device__ __forceinline__ void node_finish(const RDesc& d, int gi, float x, float y) {
+// Velocity (simulate.py:83-84), the IB point in lattice units (fluid.py:236-239) and its
+// K x K stencil (fluid.py:40-79) appended to the IB bins, and the clearing of the node's
+// CIC deposit cells (the deposit grid stays zero between steps).  The stencil spans at
+// most 2 x 2 bin tiles, so its contributions take their bin slots with one atomic per tile.
+__global__ void __launch_bounds__(256) k_stencil(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int gi = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
+  if (gi >= d.N) return;
+  const float x = d.pos[2 * gi], y = d.pos[2 * gi + 1];
   const float vx = (x - d.prev[2 * gi]) / d.dt, vy = (y - d.prev[2 * gi + 1]) / d.dt;
-  d.pos[2 * gi] = x;
-  d.pos[2 * gi + 1] = y;
   d.vel[2 * gi] = vx;
   d.vel[2 * gi + 1] = vy;
   if (d.enable_steric) {
@@ -187,6 +198,7 @@ __device__ __forceinline__ void node_finish(const RDesc& d, int gi, float x, flo
   const float hw = (float)K / 2.0f;
   const float sx = floorf(gx) - (float)half, sy = floorf(gy) - (float)half;
   float wx[8], wy[8];
+  int cx[8], cy[8];
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
     if (a < K) {
@@ -194,6 +206,8 @@ __device__ __forceinline__ void node_finish(const RDesc& d, int gi, float x, flo
       const float ry = fabsf((sy + (float)a) - gy) / hw;
       wx[a] = rx <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * rx) / 2.0f)) : 0.0f;
       wy[a] = ry <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * ry) / 2.0f)) : 0.0f;
+      cx[a] = imod_floor((int)(sx + (float)a), d.W);
+      cy[a] = imod_floor((int)(sy + (float)a), d.H);
     }
   }
   float sum = 0.0f;
@@ -203,22 +217,81 @@ __device__ __forceinline__ void node_finish(const RDesc& d, int gi, float x, flo
     for (int b = 0; b < 8; ++b)
       if (a < K && b < K) sum = sum + wx[a] * wy[b];
   const float den = sum + MC_EPSIL;
+  // tile split of the stencil: columns (rows) whose tile differs from the first one's.
+  // A window of K <= 8 consecutive cells meets at most two tiles unless the grid's last
+  // tile is narrower than the window; then every contribution takes its own slot.
+  const int tx0 = cx[0] / kBinTile, ty0 = cy[0] / kBinTile;
+  int txo = -1, tyo = -1, nx1 = 0, ny1 = 0;
+  bool split_ok = true;
+#pragma unroll
+  for (int a = 1; a < 8; ++a) {
+    if (a < K) {
+      const int tx = cx[a] / kBinTile, ty = cy[a] / kBinTile;
+      if (tx != tx0) {
+        if (txo >= 0 && tx != txo) split_ok = false;
+        txo = tx;
+        ++nx1;
+      }
+      if (ty != ty0) {
+        if (tyo >= 0 && ty != tyo) split_ok = false;
+        tyo = ty;
+        ++ny1;
+      }
+    }
+  }
+  if (txo < 0) txo = tx0;
+  if (tyo < 0) tyo = ty0;
+  const int nx0 = K - nx1, ny0 = K - ny1;
+  int base[4];
+  const int tiles[4] = {ty0 * d.ntile_x + tx0, ty0 * d.ntile_x + txo, tyo * d.ntile_x + tx0, tyo * d.ntile_x + txo};
+  const int counts[4] = {nx0 * ny0, nx1 * ny0, nx0 * ny1, nx1 * ny1};
+  if (split_ok) {
+#pragma unroll
+    for (int g = 0; g < 4; ++g) base[g] = counts[g] ? atomicAdd(d.ib_tcount + tiles[g], counts[g]) : 0;
+  }
+  int rank[4] = {0, 0, 0, 0};
+  const int cap = d.ib_cap;
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
     if (a < K) {
-      const int cx = imod_floor((int)(sx + (float)a), d.W);
+      const int xs = (cx[a] / kBinTile != tx0) ? 1 : 0;
 #pragma unroll
       for (int b = 0; b < 8; ++b) {
         if (b < K) {
-          const int cy = imod_floor((int)(sy + (float)b), d.H);
+          const int ys = (cy[b] / kBinTile != ty0) ? 1 : 0;
+          const int g = xs + 2 * ys;
           const int k = gi * K2 + a * K + b;
-          d.ib_cell[k] = cy * d.W + cx;
+          d.ib_cell[k] = cy[b] * d.W + cx[a];
           d.ib_w[k] = (wx[a] * wy[b]) / den;
-          bin_push(d.ib_store, d.ib_tcount, d.ib_ovf, d.ib_ctl, d.ib_cap, bin_tile(d, cy, cx), k);
+          int tile, pos;
+          if (split_ok) {
+            tile = tiles[g];
+            pos = base[g] + rank[g]++;
+          } else {
+            tile = (cy[b] / kBinTile) * d.ntile_x + cx[a] / kBinTile;
+            pos = atomicAdd(d.ib_tcount + tile, 1);
+          }
+          if (pos < cap) {
+            d.ib_store[(size_t)tile * cap + pos] = k;
+          } else {
+            d.ib_ovf[atomicAdd(d.ib_ctl, 1)] = k;
+          }
         }
       }
     }
   }
+}
+
+// The prediction displaced by the steric force (simulate.py:55-65), written to the node
+// positions the rod kernels start from.
+__global__ void __launch_bounds__(256) k_steric(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int gi = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
+  if (gi >= d.N) return;
+  const float2 s = node_start(d, gi);
+  d.pos[2 * gi] = s.x;
+  d.pos[2 * gi + 1] = s.y;
 }
 
 // ---------------------------------------------------------------- chains: warp per rod
@@ -260,9 +333,8 @@ __global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, cons
     const int j = lane * P + q;
     x[q] = y[q] = th[q] = l0[q] = ra[q] = kb[q] = 0.0f;
     if (j < nn) {
-      const float2 s = node_start(d, n0 + j);
-      x[q] = s.x;
-      y[q] = s.y;
+      x[q] = d.pos[2 * (n0 + j)];
+      y[q] = d.pos[2 * (n0 + j) + 1];
     }
     if (j < ne) {
       th[q] = d.theta[e0 + j];
@@ -329,7 +401,10 @@ __global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, cons
   for (int q = 0; q < P; ++q) {
     const int j = lane * P + q;
     if (j < ne) d.theta[e0 + j] = th[q];
-    if (j < nn) node_finish(d, n0 + j, x[q], y[q]);
+    if (j < nn) {
+      d.pos[2 * (n0 + j)] = x[q];
+      d.pos[2 * (n0 + j) + 1] = y[q];
+    }
   }
 }
 
@@ -364,9 +439,8 @@ __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off,
     l0[e] = d.rest_len[e0 + e];
   }
   for (int i = tid; i < nn; i += bd) {
-    const float2 s = node_start(d, n0 + i);
-    px[i] = s.x;
-    py[i] = s.y;
+    px[i] = d.pos[2 * (n0 + i)];
+    py[i] = d.pos[2 * (n0 + i) + 1];
   }
   __syncthreads();
 
@@ -418,10 +492,15 @@ __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off,
   }
 
   for (int e = tid; e < ne; e += bd) d.theta[e0 + e] = th[e];
-  for (int i = tid; i < nn; i += bd) node_finish(d, n0 + i, px[i], py[i]);
+  for (int i = tid; i < nn; i += bd) {
+    d.pos[2 * (n0 + i)] = px[i];
+    d.pos[2 * (n0 + i) + 1] = py[i];
+  }
 }
 
 void launch_predict(const Launch& L) { k_predict<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
+void launch_steric(const Launch& L) { k_steric<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
+void launch_stencil(const Launch& L) { k_stencil<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
 void launch_node(const Launch& L, const int* tdev, size_t smem, int bs) {
   k_node<<<L.grid, bs, smem, L.s>>>(L.d, L.off, L.n, tdev);
 }

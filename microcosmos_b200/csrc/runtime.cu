@@ -454,7 +454,8 @@ mc::Launch L(mc_plan* p, Kind k, cudaStream_t s) {
 
 const char* const kProfNames[] = {"predict", "cic_bins",  "fft_rows",    "fft_cols", "chain",
                                    "node",    "ib_bins",   "ib_interp",   "ib_spread", "ib_finalize",
-                                   "lbm",     "reaction",  "record_fields", "tick"};
+                                   "lbm",     "reaction",  "record_fields", "tick",    "steric",
+                                   "stencil"};
 constexpr int kNumProf = sizeof(kProfNames) / sizeof(kProfNames[0]);
 
 cudaEvent_t take_event(mc_plan* p) {
@@ -507,12 +508,20 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
     timed(p, 3, s, capture, [&] { mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem); });
     k += 3;
   }
+  if (p->grid[K_NODES]) {
+    timed(p, 14, s, capture, [&] { mc::launch_steric(L(p, K_NODES, s)); });
+    ++k;
+  }
   if (p->grid[K_CHAIN]) {
     timed(p, 4, s, capture, [&] { mc::launch_chain(L(p, K_CHAIN, s), tdev, p->chain_slots); });
     ++k;
   }
   if (p->grid[K_COMP]) {
     timed(p, 5, s, capture, [&] { mc::launch_node(L(p, K_COMP, s), tdev, p->node_smem, p->node_bs); });
+    ++k;
+  }
+  if (p->grid[K_NODES]) {
+    timed(p, 15, s, capture, [&] { mc::launch_stencil(L(p, K_NODES, s)); });
     ++k;
   }
   return k;
@@ -528,7 +537,7 @@ int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
     timed(p, 8, s, capture, [&] { mc::launch_ib_spread(L(p, K_IB, s), it); });
     k += 2;
   }
-  timed(p, 9, s, capture, [&] { mc::launch_ib_finalize(L(p, K_IB, s)); });
+  timed(p, 9, s, capture, [&] { mc::launch_ib_finalize(L(p, K_IB, s), parity); });
   return k + 1;
 }
 
@@ -783,7 +792,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.vec = vec_all;
     h.lbm_tx = div_up(h.dims.W, 32 * h.vec);
     h.lbm_ty = div_up(h.dims.H, mc::kLbmTileY);
-    h.r_lflag = lay.take((size_t)h.lbm_tx * h.lbm_ty * 4);
+    h.r_lflag = lay.take((size_t)2 * h.lbm_tx * h.lbm_ty * 4);
   }
   p->ws_bytes = lay.cur;
   // CTA offset tables
