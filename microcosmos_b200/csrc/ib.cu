@@ -73,26 +73,15 @@ __device__ __forceinline__ int lower_bound_u(const unsigned* a, int len, unsigne
   return lo;
 }
 
-// Work for one touched cell: its contributions are run[0..len) in increasing k.
-// which == 0 (IB): coverage -> 1/max(cov, 1), the macroscopic state pulled from h[parity]
-//   (density, clamped velocity), u_corrected = velocity, contribution -> head links
-//   (fluid.py:268-290).   which == 1 (CIC): deposit value = in-order sum (forces.py:98-115).
-__device__ __forceinline__ void head_work(const RDesc& d, const BinView& v, int which, int parity, const int* run,
-                                          int len, int run_pos) {
-  const int k0 = run[0];
-  const int cell = v.cell[k0];
-  float acc = v.w[k0];
-  for (int j = 1; j < len; ++j) acc = acc + v.w[run[j]];
-  if (which == 1) {
-    d.dep[cell] = acc;
-    return;
-  }
-  const int slot = atomicAdd(v.ctl + 2, 1);
+// Per-cell reduction work.  IB: coverage -> 1/max(cov, 1), the macroscopic state pulled
+// from h[parity] (density, clamped velocity), u_corrected = velocity (fluid.py:268-290);
+// the caller has already linked the run's contributions to `slot`.
+__device__ __forceinline__ void ib_head(const RDesc& d, int parity, int cell, float cov, int slot, int len,
+                                        int run_pos) {
   d.h_cell[slot] = cell;
   d.h_start[slot] = run_pos;
   d.h_len[slot] = len;
-  d.s_inv[slot] = 1.0f / max_prop(acc, 1.0f);
-  for (int j = 0; j < len; ++j) d.ib_slot[run[j]] = slot;
+  d.s_inv[slot] = 1.0f / max_prop(cov, 1.0f);
   const int y = cell / d.W, x = cell - y * d.W;
   const size_t HW = (size_t)d.H * d.W;
   const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
@@ -113,14 +102,34 @@ __device__ __forceinline__ void head_work(const RDesc& d, const BinView& v, int 
   d.s_ucy[slot] = vy;
 }
 
+// Work for one touched cell whose contributions are run[0..len) in increasing k, read
+// from global memory (spilled tiles only).  CIC: deposit = in-order sum (forces.py:98-115).
+__device__ __forceinline__ void head_work(const RDesc& d, const BinView& v, int which, int parity, const int* run,
+                                          int len, int run_pos) {
+  const int k0 = run[0];
+  const int cell = v.cell[k0];
+  float acc = v.w[k0];
+  for (int j = 1; j < len; ++j) acc = acc + v.w[run[j]];
+  if (which == 1) {
+    d.dep[cell] = acc;
+    return;
+  }
+  const int slot = atomicAdd(v.ctl + 2, 1);
+  for (int j = 0; j < len; ++j) d.ib_slot[run[j]] = slot;
+  ib_head(d, parity, cell, acc, slot, len, run_pos);
+}
+
 // One CTA (256 threads) per bin tile: sort the tile's contributions by (cell, k) and
 // reduce every cell's run.
 __global__ void __launch_bounds__(256) k_bin_tiles(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
                                                    int which, int parity) {
+  constexpr int kCapS = kSortCap / 4;  // entries handled in shared memory (>= every bin capacity)
   __shared__ unsigned skeys[kSortCap];
   __shared__ int cnt[kBinTile * kBinTile];
   __shared__ int cpos[kBinTile * kBinTile];
-  __shared__ int s_spill;
+  __shared__ int hpos[kBinTile * kBinTile];  // rank of a touched cell among the tile's touched cells
+  __shared__ int s_spill, s_heads, s_base;
+  static_assert(kIbCap <= kCapS && kCicCap <= kCapS, "bin capacity exceeds the shared-memory sort");
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const BinView v = bin_view(d, which);
@@ -133,65 +142,97 @@ __global__ void __launch_bounds__(256) k_bin_tiles(const RDesc* __restrict__ D, 
   int* bin = v.store + (size_t)t * v.cap;
 
   if (total <= v.cap) {
+    // shared layout: [0, C) packed (cell, rank) | [C, 2C) k | [2C, 3C) sorted k | [3C, 4C) sorted w
+    unsigned* lr = skeys;
+    int* kin = reinterpret_cast<int*>(skeys + kCapS);
+    int* kout = reinterpret_cast<int*>(skeys + 2 * kCapS);
+    float* wout = reinterpret_cast<float*>(skeys + 3 * kCapS);
+    for (int c = tid; c < kBinTile * kBinTile; c += blockDim.x) cnt[c] = 0;
+    if (tid == 0) s_heads = 0;
+    __syncthreads();
     // counting sort by local cell; positions inside a cell come from shared atomics
     // (arbitrary order), so each cell's run is then ordered by k
-    for (int c = tid; c < kBinTile * kBinTile; c += blockDim.x) cnt[c] = 0;
-    __syncthreads();
     for (int i = tid; i < total; i += blockDim.x) {
       const int k = bin[i];
       const unsigned lc = local_of(d, v.cell[k]);
       const int pos = atomicAdd(cnt + lc, 1);
-      skeys[i] = (lc << 24) | (unsigned)pos;  // (cell, rank inside the cell)
-      skeys[kSortCap / 2 + i] = (unsigned)k;
+      lr[i] = (lc << 24) | (unsigned)pos;
+      kin[i] = k;
     }
     __syncthreads();
-    // exclusive scan of the 256 cell counts (one warp, 8 per lane)
+    // exclusive scan of the 256 cell counts (one warp, 8 per lane) and the head count
     if (tid < 32) {
       int loc[8];
-      int sum = 0;
+      int sum = 0, nz = 0;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         loc[q] = cnt[tid * 8 + q];
         sum += loc[q];
+        nz += loc[q] > 0;
       }
-      int incl = sum;
+      int incl = sum, inz = nz;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (tid >= o) incl += y;
+        int z = __shfl_up_sync(0xffffffffu, inz, o);
+        if (tid >= o) {
+          incl += y;
+          inz += z;
+        }
       }
-      int run = incl - sum;
+      int run = incl - sum, hrun = inz - nz;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         cpos[tid * 8 + q] = run;
+        hpos[tid * 8 + q] = hrun;
         run += loc[q];
+        hrun += loc[q] > 0;
       }
+      if (tid == 31) s_heads = inz;
     }
     __syncthreads();
-    // scatter into cell order (a bin holds at most cap <= kSortCap / 2 entries)
+    // one slot range per tile for its touched cells (IB)
+    if (which == 0 && tid == 0) s_base = atomicAdd(v.ctl + 2, s_heads);
     for (int i = tid; i < total; i += blockDim.x) {
-      const unsigned key = skeys[i];
+      const unsigned key = lr[i];
       const int lc = (int)(key >> 24), pos = (int)(key & 0xffffffu);
-      bin[cpos[lc] + pos] = (int)skeys[kSortCap / 2 + i];
+      const int k = kin[i];
+      kout[cpos[lc] + pos] = k;
+      wout[cpos[lc] + pos] = v.w[k];
     }
     __syncthreads();
     // one thread per cell: order its run by k (runs are short), then reduce it
     for (int c = tid; c < kBinTile * kBinTile; c += blockDim.x) {
       const int len = cnt[c];
       if (len == 0) continue;
-      int* run = bin + cpos[c];
+      int* rk = kout + cpos[c];
+      float* rw = wout + cpos[c];
       for (int a = 1; a < len; ++a) {
-        const int key = run[a];
+        const int key = rk[a];
+        const float kw = rw[a];
         int b = a - 1;
-        while (b >= 0 && run[b] > key) {
-          run[b + 1] = run[b];
+        while (b >= 0 && rk[b] > key) {
+          rk[b + 1] = rk[b];
+          rw[b + 1] = rw[b];
           --b;
         }
-        run[b + 1] = key;
+        rk[b + 1] = key;
+        rw[b + 1] = kw;
       }
-      head_work(d, v, which, parity, run, len, t * v.cap + cpos[c]);
+      float acc = rw[0];
+      for (int j = 1; j < len; ++j) acc = acc + rw[j];
+      const int cell = v.cell[rk[0]];
+      if (which == 1) {
+        d.dep[cell] = acc;
+      } else {
+        const int slot = s_base + hpos[c];
+        for (int j = 0; j < len; ++j) d.ib_slot[rk[j]] = slot;
+        ib_head(d, parity, cell, acc, slot, len, t * v.cap + cpos[c]);
+      }
     }
     __syncthreads();
+    if (which == 0)
+      for (int i = tid; i < total; i += blockDim.x) bin[i] = kout[i];
     if (tid == 0) v.tcount[t] = 0;
     return;
   }

@@ -202,6 +202,7 @@ void launch_node(const Launch& L, const int* tdev, size_t smem, int bs);
 void launch_chain(const Launch& L, const int* tdev, int slots);
 void launch_steric(const Launch& L);
 void launch_stencil(const Launch& L);
+void launch_stencil16(const Launch& L);
 void launch_ib_interp(const Launch& L, int it);
 void launch_ib_spread(const Launch& L, int it);
 void launch_ib_finalize(const Launch& L, int parity);

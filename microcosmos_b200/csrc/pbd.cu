@@ -282,6 +282,66 @@ __global__ void __launch_bounds__(256) k_stencil(const RDesc* __restrict__ D, co
   }
 }
 
+// The same work with one 16-lane group per node (K <= 4): lane s = a*K + b owns stencil
+// entry s.  The weight normalisation sum is taken by the group's first lane in entry
+// order, so the result equals the one-thread-per-node kernel's; bin slots are taken with
+// one atomic per (warp, tile) group.
+__global__ void __launch_bounds__(256) k_stencil16(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int t = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
+  const int gi = t >> 4, s = t & 15;
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = 0xffffu << (lane & 16);
+  if (gi >= d.N) return;  // both halves of a warp exit together unless N is odd
+  const float x = d.pos[2 * gi], y = d.pos[2 * gi + 1];
+  const float vx = (x - d.prev[2 * gi]) / d.dt, vy = (y - d.prev[2 * gi + 1]) / d.dt;
+  if (s == 0) {
+    d.vel[2 * gi] = vx;
+    d.vel[2 * gi + 1] = vy;
+  }
+  if (d.enable_steric && s < 4) d.dep[d.c_cell[s * d.N + gi]] = 0.0f;
+  if (!d.enable_fluid) return;
+  const int K = d.K, K2 = K * K;
+  const float gx = x * d.scale_x, gy = y * d.scale_y;
+  if (s == 0) {
+    d.nvl[2 * gi] = (vx * d.scale_x) * d.dt;
+    d.nvl[2 * gi + 1] = (vy * d.scale_y) * d.dt;
+  }
+  const int half = (K - 1) / 2;
+  const float hw = (float)K / 2.0f;
+  const float sx = floorf(gx) - (float)half, sy = floorf(gy) - (float)half;
+  const int a = s / K, b = s - (s / K) * K;
+  const bool act = s < K2;
+  const float rx = fabsf((sx + (float)a) - gx) / hw;
+  const float ry = fabsf((sy + (float)b) - gy) / hw;
+  const float wxa = rx <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * rx) / 2.0f)) : 0.0f;
+  const float wyb = ry <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * ry) / 2.0f)) : 0.0f;
+  const float w = wxa * wyb;
+  float sum = 0.0f;
+  for (int q = 0; q < K2; ++q) sum = sum + __shfl_sync(gmask, w, q, 16);
+  const float den = sum + MC_EPSIL;
+  if (!act) return;
+  const int cx = imod_floor((int)(sx + (float)a), d.W);
+  const int cy = imod_floor((int)(sy + (float)b), d.H);
+  const int k = gi * K2 + s;
+  d.ib_cell[k] = cy * d.W + cx;
+  d.ib_w[k] = w / den;
+  const int tile = (cy / kBinTile) * d.ntile_x + cx / kBinTile;
+  const unsigned active = __activemask();
+  const unsigned group = __match_any_sync(active, tile);
+  const int leader = __ffs(group) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(d.ib_tcount + tile, __popc(group));
+  base = __shfl_sync(group, base, leader);
+  const int pos = base + __popc(group & ((1u << lane) - 1u));
+  if (pos < d.ib_cap) {
+    d.ib_store[(size_t)tile * d.ib_cap + pos] = k;
+  } else {
+    d.ib_ovf[atomicAdd(d.ib_ctl, 1)] = k;
+  }
+}
+
 // The prediction displaced by the steric force (simulate.py:55-65), written to the node
 // positions the rod kernels start from.
 __global__ void __launch_bounds__(256) k_steric(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
@@ -501,6 +561,7 @@ __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off,
 void launch_predict(const Launch& L) { k_predict<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
 void launch_steric(const Launch& L) { k_steric<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
 void launch_stencil(const Launch& L) { k_stencil<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
+void launch_stencil16(const Launch& L) { k_stencil16<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
 void launch_node(const Launch& L, const int* tdev, size_t smem, int bs) {
   k_node<<<L.grid, bs, smem, L.s>>>(L.d, L.off, L.n, tdev);
 }

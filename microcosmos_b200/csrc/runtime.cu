@@ -37,7 +37,7 @@ mc_status cuda_fail(cudaError_t e, const char* where) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_COUNT };
+enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_COUNT };
 
 struct Region {
   size_t off = 0;
@@ -83,6 +83,7 @@ struct mc_plan {
   size_t node_smem = 0, fftr_smem = 0, fftc_smem = 0;
   int node_bs = 32;
   int max_chain = 0, chain_slots = 1;
+  int max_k = 0;  // largest IB kernel size of the plan
   std::vector<RDesc> desc;
   cudaStream_t cap_stream = nullptr;
   // CUDA graphs, keyed by [steps-1][parity][recording variant][write_u][runs next pipeline]
@@ -521,7 +522,10 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
     ++k;
   }
   if (p->grid[K_NODES]) {
-    timed(p, 15, s, capture, [&] { mc::launch_stencil(L(p, K_NODES, s)); });
+    if (p->max_k <= 4)
+      timed(p, 15, s, capture, [&] { mc::launch_stencil16(L(p, K_NODES16, s)); });
+    else
+      timed(p, 15, s, capture, [&] { mc::launch_stencil(L(p, K_NODES, s)); });
     ++k;
   }
   return k;
@@ -786,6 +790,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     if (c.enable_fluid) p->any_fluid = 1;
     if (c.enable_steric) p->any_steric = 1;
     p->max_iters = std::max(p->max_iters, c.enable_fluid ? c.ibm_iterations : 0);
+    p->max_k = std::max(p->max_k, c.ibm_kernel_size);
   }
   for (int i = 0; i < n; ++i) {
     HostRollout& h = p->R[i];
@@ -804,6 +809,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     const long long HW = (long long)h.dims.H * h.dims.W;
     int cnt[K_COUNT];
     cnt[K_NODES] = div_up(h.dims.N, 256);
+    cnt[K_NODES16] = div_up(16LL * h.dims.N, 256);
     cnt[K_COMP] = h.dims.N > 0 ? (int)h.generic_comp.size() : 0;
     cnt[K_CHAIN] = h.dims.N > 0 ? div_up((long long)h.chain_comp.size(), 4) : 0;
     cnt[K_IB] = div_up(h.M, 256);
