@@ -43,6 +43,7 @@ typedef enum mc_status {
 
 /* Per-rollout flag bits reported by mc_plan_read_flags(). */
 #define MC_FLAG_NONFINITE 1u /* a node position/velocity became NaN/Inf */
+#define MC_FLAG_TIMEOUT 2u   /* a bounded device-side wait gave up; the step's results are invalid */
 
 /* Scalar fields of ConstraintSolverConfig used by the PBD scheme
  * (src/microcosmos/solver/config.py:9-72).  The callable `bending_constraint` is fixed
@@ -160,6 +161,13 @@ mc_status mc_plan_read_flags(mc_plan* plan, uint32_t* flags, int32_t clear, void
 /* Number of kernel launches the last mc_rollout() enqueued (graph replays count the
  * kernels inside the graph). */
 int64_t mc_plan_last_launch_count(const mc_plan* plan);
+
+/* The multi-direct forcing iterations run as one cooperative kernel with device-side
+ * barriers when every CTA of it fits on the GPU at once (the default), else as separate
+ * interpolate / spread launches.  Both give identical results; this switch (after
+ * mc_plan_bind, outside a rollout) selects the separate launches (enable = 0). */
+mc_status mc_plan_set_fused_ib(mc_plan* plan, int32_t enable);
+int32_t mc_plan_uses_fused_ib(const mc_plan* plan);
 
 /* Per-kernel CUDA-event timing.  While enabled, steps are launched directly (no graph)
  * and each kernel launch is bracketed by two events; mc_plan_profile_read() returns the

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libmicrocosmos_b200.so")
 
 MC_OK, MC_ERR_INVALID, MC_ERR_CUDA, MC_ERR_WORKSPACE, MC_ERR_UNSUPPORTED, MC_ERR_NOT_BOUND = range(6)
 MC_FLAG_NONFINITE = 1
+MC_FLAG_TIMEOUT = 2
 
 c_float_p = ctypes.POINTER(ctypes.c_float)
 c_int_p = ctypes.POINTER(ctypes.c_int32)
@@ -90,6 +91,8 @@ SIGNATURES = {
                                           ctypes.c_void_p]),
     "mc_rollout_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "mc_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(McState), ctypes.c_void_p]),
+    "mc_plan_set_fused_ib": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "mc_plan_uses_fused_ib": (ctypes.c_int32, [ctypes.c_void_p]),
     "mc_plan_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "mc_plan_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_int64)]),

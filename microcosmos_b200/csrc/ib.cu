@@ -429,6 +429,151 @@ __global__ void __launch_bounds__(256) k_ib_spread(const RDesc* __restrict__ D, 
   d.s_ucy[p] = d.s_ucy[p] + dy * inv;
 }
 
+// ---------------------------------------------------------------- fused IB iterations
+// Barrier among the CTAs of one rollout inside a cooperative launch (all CTAs resident).
+// The spin is bounded: on timeout the rollout's MC_FLAG_TIMEOUT is set and the kernel
+// continues (its results are then invalid) instead of hanging the device.
+__device__ __forceinline__ void rollout_barrier(int* ctl, int nb, unsigned* flags) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile int* gen = ctl + 4;
+    const int g = *gen;
+    __threadfence();
+    if (atomicAdd(ctl + 3, 1) == nb - 1) {
+      atomicExch(ctl + 3, 0);
+      __threadfence();
+      atomicAdd(ctl + 4, 1);
+    } else {
+      unsigned it = 0;
+      while (*gen == g) {
+        __nanosleep(64);
+        if (++it > (1u << 21)) {
+          atomicOr(flags, 2u);
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// All ibm_iterations of the multi-direct forcing and the body force of every rollout in one
+// cooperative launch: [interpolate (nodes) | barrier | spread (touched cells) | barrier] x
+// iterations, then the finalize of every touched cell.  Same arithmetic and order as
+// k_ib_interp / k_ib_spread / k_ib_finalize; values written in one phase and read in the
+// next are loaded with __ldcg (L2, not the SM's L1).
+__global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
+                                                 int parity) {
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int nb = off[r + 1] - off[r];
+  const int lb = blockIdx.x - off[r];
+  const int stride = nb * blockDim.x;
+  const int t0 = lb * blockDim.x + threadIdx.x;
+  const int nheads = __ldcg(d.ib_ctl + 2);
+  const int K2 = d.K * d.K;
+  for (int it = 0; it < d.ib_iters; ++it) {
+    for (int node = t0; node < d.N; node += stride) {
+      float ux = 0.0f, uy = 0.0f;
+      const int base = node * K2;
+      if (K2 == 16) {
+        int slot[16];
+        float w[16];
+#pragma unroll
+        for (int q = 0; q < 16; q += 4) {
+          const int4 a = *reinterpret_cast<const int4*>(d.ib_slot + base + q);
+          const float4 b = *reinterpret_cast<const float4*>(d.ib_w + base + q);
+          slot[q] = a.x; slot[q + 1] = a.y; slot[q + 2] = a.z; slot[q + 3] = a.w;
+          w[q] = b.x; w[q + 1] = b.y; w[q + 2] = b.z; w[q + 3] = b.w;
+        }
+        float vx[16], vy[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          vx[q] = __ldcg(d.s_ucx + slot[q]);
+          vy[q] = __ldcg(d.s_ucy + slot[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          ux = ux + vx[q] * w[q];
+          uy = uy + vy[q] * w[q];
+        }
+      } else {
+        for (int q = 0; q < K2; ++q) {
+          const int sl = d.ib_slot[base + q];
+          const float w = d.ib_w[base + q];
+          ux = ux + __ldcg(d.s_ucx + sl) * w;
+          uy = uy + __ldcg(d.s_ucy + sl) * w;
+        }
+      }
+      const float sx = (d.nvl[2 * node] - ux) * d.relax;
+      const float sy = (d.nvl[2 * node + 1] - uy) * d.relax;
+      const float cf = clamp_factor(sx, sy, d.vmax);
+      d.delta[2 * node] = sx * cf;
+      d.delta[2 * node + 1] = sy * cf;
+    }
+    rollout_barrier(d.ib_ctl, nb, d.flags);
+    for (int p = t0; p < nheads; p += stride) {
+      const int len = d.h_len[p];
+      const int* run = d.ib_store + d.h_start[p];
+      float dx = 0.0f, dy = 0.0f;
+      int j = 0;
+      for (; j + 8 <= len; j += 8) {
+        int k[8];
+        float w[8], ex[8], ey[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) k[q] = run[j + q];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int node = k[q] / K2;
+          w[q] = d.ib_w[k[q]];
+          ex[q] = __ldcg(d.delta + 2 * node);
+          ey[q] = __ldcg(d.delta + 2 * node + 1);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          dx = dx + ex[q] * w[q];
+          dy = dy + ey[q] * w[q];
+        }
+      }
+      for (; j < len; ++j) {
+        const int k = run[j];
+        const int node = k / K2;
+        const float w = d.ib_w[k];
+        dx = dx + __ldcg(d.delta + 2 * node) * w;
+        dy = dy + __ldcg(d.delta + 2 * node + 1) * w;
+      }
+      const float inv = d.s_inv[p];
+      d.s_ucx[p] = __ldcg(d.s_ucx + p) + dx * inv;
+      d.s_ucy[p] = __ldcg(d.s_ucy + p) + dy * inv;
+    }
+    rollout_barrier(d.ib_ctl, nb, d.flags);
+  }
+  const size_t HW = (size_t)d.H * d.W;
+  const int nflag = d.lbm_tx * d.lbm_ty;
+  for (int p = t0; p < nheads; p += stride) {
+    float ucx = __ldcg(d.s_ucx + p), ucy = __ldcg(d.s_ucy + p);
+    const float c2 = clamp_factor(ucx, ucy, d.vmax);
+    ucx = ucx * c2;
+    ucy = ucy * c2;
+    const float rho = d.s_rho[p];
+    float Fx = (ucx - d.s_vx[p]) * rho;
+    float Fy = (ucy - d.s_vy[p]) * rho;
+    if (d.force_clamp) {
+      const float c3 = clamp_factor(Fx, Fy, d.vmax);
+      Fx = Fx * c3;
+      Fy = Fy * c3;
+    }
+    d.s_fx[p] = Fx;
+    d.s_fy[p] = Fy;
+    const int cell = d.h_cell[p];
+    d.fov[cell] = Fx;
+    d.fov[HW + cell] = Fy;
+    const int y = cell / d.W, x = cell - y * d.W;
+    d.lbm_flag[(parity & 1) * nflag + (y / kLbmTileY) * d.lbm_tx + x / d.lbm_tw] = 1;
+  }
+}
+
 // Post-accumulation clamp and body force F = (u_corrected - u) rho (fluid.py:327-339),
 // published to the dense pass through the force overlay.
 __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
@@ -529,6 +674,23 @@ void launch_bin_tiles(const Launch& L, int which, int parity) {
 }
 void launch_ib_interp(const Launch& L, int it) { k_ib_interp<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
 void launch_ib_spread(const Launch& L, int it) { k_ib_spread<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
+cudaError_t launch_ib_coop(const Launch& L, int parity) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(L.grid);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = L.s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_ib_coop, L.d, L.off, L.n, parity);
+}
+cudaError_t ib_coop_blocks_per_sm(int* out) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_ib_coop, 256, 0);
+}
+
 void launch_ib_finalize(const Launch& L, int parity) {
   k_ib_finalize<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, parity);
 }

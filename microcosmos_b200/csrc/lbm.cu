@@ -209,7 +209,7 @@ __global__ void k_clear_ws(const RDesc* __restrict__ D, const int* __restrict__ 
     d.c_tcount[i] = 0;
   }
   for (size_t i = t0; i < (size_t)2 * d.lbm_tx * d.lbm_ty; i += stride) d.lbm_flag[i] = 0;
-  if (t0 < 4) {
+  if (t0 < 8) {
     d.ib_ctl[t0] = 0;
     d.c_ctl[t0] = 0;
   }

@@ -98,7 +98,8 @@ struct RDesc {
   // Deterministic scatter-add bins.  Contribution k goes to bin tile t at
   // store[t * cap + atomic position]; a tile that fills up spills into the overflow list.
   // store[ntiles * cap ...] is an arena for sorting tiles with more than cap entries.
-  // ctl[0] = overflow count, ctl[1] = arena use, ctl[2] = touched-cell (head) count.
+  // ctl[0] = overflow count, ctl[1] = arena use, ctl[2] = touched-cell (head) count,
+  // ctl[3], ctl[4] = arrival count and generation of the fused IB kernel's barrier.
   int ib_cap;
   int* ib_cell;     // (M) cell of contribution k = n*K*K + s
   float* ib_w;      // (M) normalised stencil weight
@@ -206,6 +207,8 @@ void launch_stencil16(const Launch& L);
 void launch_ib_interp(const Launch& L, int it);
 void launch_ib_spread(const Launch& L, int it);
 void launch_ib_finalize(const Launch& L, int parity);
+cudaError_t launch_ib_coop(const Launch& L, int parity);
+cudaError_t ib_coop_blocks_per_sm(int* out);
 void launch_lbm(const Launch& L, int parity, int write_u, int vec);
 void launch_reaction(const Launch& L, const int* tdev);
 void launch_record_fields(const Launch& L, const int* tdev);

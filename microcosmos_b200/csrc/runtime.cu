@@ -37,7 +37,7 @@ mc_status cuda_fail(cudaError_t e, const char* where) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_COUNT };
+enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_COUNT };
 
 struct Region {
   size_t off = 0;
@@ -84,6 +84,10 @@ struct mc_plan {
   int node_bs = 32;
   int max_chain = 0, chain_slots = 1;
   int max_k = 0;  // largest IB kernel size of the plan
+  bool use_coop = false, coop_cap_checked = false;
+  bool fused_ib = true;  // mc_plan_set_fused_ib
+  bool coop_possible = false;
+  cudaError_t coop_err = cudaSuccess;
   std::vector<RDesc> desc;
   cudaStream_t cap_stream = nullptr;
   // CUDA graphs, keyed by [steps-1][parity][recording variant][write_u][runs next pipeline]
@@ -456,7 +460,7 @@ mc::Launch L(mc_plan* p, Kind k, cudaStream_t s) {
 const char* const kProfNames[] = {"predict", "cic_bins",  "fft_rows",    "fft_cols", "chain",
                                    "node",    "ib_bins",   "ib_interp",   "ib_spread", "ib_finalize",
                                    "lbm",     "reaction",  "record_fields", "tick",    "steric",
-                                   "stencil"};
+                                   "stencil", "ib_fused"};
 constexpr int kNumProf = sizeof(kProfNames) / sizeof(kProfNames[0]);
 
 cudaEvent_t take_event(mc_plan* p) {
@@ -536,6 +540,10 @@ int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
   int64_t k = 0;
   timed(p, 6, s, capture, [&] { mc::launch_bin_tiles(L(p, K_TILES, s), 0, parity); });
   ++k;
+  if (p->use_coop) {
+    timed(p, 16, s, capture, [&] { p->coop_err = mc::launch_ib_coop(L(p, K_IBCOOP, s), parity); });
+    return k + 1;
+  }
   for (int it = 0; it < p->max_iters; ++it) {
     timed(p, 7, s, capture, [&] { mc::launch_ib_interp(L(p, K_NODES, s), it); });
     timed(p, 8, s, capture, [&] { mc::launch_ib_spread(L(p, K_IB, s), it); });
@@ -750,7 +758,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.r_ibstore = lay.take((nt * mc::kIbCap + 2 * Mz) * 4);
     h.r_ibtc = lay.take(nt * 4);
     h.r_ibovf = lay.take(Mz * 4);
-    h.r_ibctl = lay.take(4 * 4);
+    h.r_ibctl = lay.take(8 * 4);
     h.r_ibslot = lay.take(Mz * 4);
     h.r_hcell = lay.take(Mz * 4);
     h.r_hstart = lay.take(Mz * 4);
@@ -768,7 +776,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.r_cstore = lay.take((nt * mc::kCicCap + 8 * N) * 4);
     h.r_ctc = lay.take(nt * 4);
     h.r_covf = lay.take(4 * N * 4);
-    h.r_cctl = lay.take(4 * 4);
+    h.r_cctl = lay.take(8 * 4);
     h.r_chain = lay.take(h.chain_comp.size() * 4);
     h.r_generic = lay.take(h.generic_comp.size() * 4);
     h.r_pairs = lay.take(2 * E * 4);
@@ -810,6 +818,8 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     int cnt[K_COUNT];
     cnt[K_NODES] = div_up(h.dims.N, 256);
     cnt[K_NODES16] = div_up(16LL * h.dims.N, 256);
+    // fused IB kernel: about one thread per touched-cell candidate / 4, at most 128 CTAs
+    cnt[K_IBCOOP] = c.enable_fluid ? std::max(1, std::min(128, div_up(h.M, 1024))) : 0;
     cnt[K_COMP] = h.dims.N > 0 ? (int)h.generic_comp.size() : 0;
     cnt[K_CHAIN] = h.dims.N > 0 ? div_up((long long)h.chain_comp.size(), 4) : 0;
     cnt[K_IB] = div_up(h.M, 256);
@@ -830,6 +840,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
                             c.enable_steric ? (size_t)(2 * mc::kFftColsPerCta + 1) * h.dims.H * sizeof(float2) + h.dims.H * sizeof(float) : 0);
   }
   for (int k = 0; k < K_COUNT; ++k) p->grid[k] = p->off[k][n];
+  p->coop_cap_checked = false;
   p->node_smem = (size_t)(2 * mcn + 4 * mce + 3 * mcb) * sizeof(float);
   p->chain_slots = 1;
   while (p->chain_slots * 32 < p->max_chain) p->chain_slots *= 2;
@@ -903,6 +914,16 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
   destroy_graphs(p);
   if (!p->cap_stream) MC_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
   if (!p->side_stream) MC_CUDA(cudaStreamCreateWithFlags(&p->side_stream, cudaStreamNonBlocking));
+  {
+    // the fused IB kernel needs every CTA resident at once (cooperative launch)
+    int dev = 0, sms = 0, per_sm = 0, coop = 0;
+    MC_CUDA(cudaGetDevice(&dev));
+    MC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    MC_CUDA(mc::ib_coop_blocks_per_sm(&per_sm));
+    p->coop_possible = coop && p->grid[K_IBCOOP] > 0 && p->grid[K_IBCOOP] <= per_sm * sms;
+    p->use_coop = p->fused_ib && p->coop_possible;
+  }
   if (!p->ev_fork) MC_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
   if (!p->ev_join) MC_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
   p->bound = true;
@@ -962,6 +983,11 @@ mc_status mc_rollout_advance(mc_plan* p, int32_t num_steps, int32_t use_graph, i
   int64_t launches = 0;
   mc_status st = run_steps(p, num_steps, use_graph, last, (cudaStream_t)stream, launches);
   p->last_launches += launches;
+  if (p->coop_err != cudaSuccess) {
+    cudaError_t e = p->coop_err;
+    p->coop_err = cudaSuccess;
+    return cuda_fail(e, "cooperative launch of the fused IB kernel");
+  }
   if (st != MC_OK) return st;
   MC_CUDA(cudaGetLastError());
   return MC_OK;
@@ -996,6 +1022,18 @@ mc_status mc_rollout(mc_plan* p, const mc_state* states, int32_t num_steps, cons
   }
   return mc_rollout_end(p, stream);
 }
+
+mc_status mc_plan_set_fused_ib(mc_plan* p, int32_t enable) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (p->active) return fail(MC_ERR_INVALID, "cannot change the IB kernel layout inside a rollout");
+  p->fused_ib = enable != 0;
+  p->use_coop = p->fused_ib && p->coop_possible;
+  destroy_graphs(p);
+  return MC_OK;
+}
+
+int32_t mc_plan_uses_fused_ib(const mc_plan* p) { return p && p->use_coop ? 1 : 0; }
 
 mc_status mc_plan_profile(mc_plan* p, int32_t enable) {
   if (!p) return fail(MC_ERR_INVALID, "null plan");

@@ -266,6 +266,12 @@ class Plan:
     def end(self, stream=None):
         _lib.check(_lib.load().mc_rollout_end(self._h, self._stream(stream)))
 
+    def set_fused_ib(self, enable=True):
+        _lib.check(_lib.load().mc_plan_set_fused_ib(self._h, int(bool(enable))))
+
+    def uses_fused_ib(self):
+        return bool(_lib.load().mc_plan_uses_fused_ib(self._h))
+
     def profile(self, enable=True):
         _lib.check(_lib.load().mc_plan_profile(self._h, int(bool(enable))))
 

@@ -237,3 +237,23 @@ def test_zero_steps_leave_state_unchanged():
     out = st.host()
     np.testing.assert_array_equal(out["position"], sc.position)
     np.testing.assert_array_equal(out["f_grid"], sc.f_grid)
+
+
+def test_fused_and_separate_ib_kernels_agree():
+    """The cooperative fused IB kernel and the separate interpolate/spread launches give the
+    same bits, for a single rollout and a batch."""
+    scs = [scenarios.make_scenario(128, 128, 6, 40, seed=31), scenarios.make_scenario(64, 96, 2, 20, seed=32)]
+    cfg = baseline_config()
+    results = []
+    for fused in (True, False):
+        sts = [DeviceState.from_scenario(s) for s in scs]
+        plan = Plan.for_states(sts, [cfg] * 2, [0.01] * 2)
+        plan.set_fused_ib(fused)
+        assert plan.uses_fused_ib() == fused
+        plan.rollout(sts, 13, actuations=[Actuation.from_scenario(s) for s in scs])
+        torch.cuda.synchronize()
+        assert plan.read_flags() == [0, 0]
+        results.append([st.host() for st in sts])
+    for a, b in zip(*results):
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k])
