@@ -446,8 +446,7 @@ __device__ __forceinline__ void rollout_barrier(int* ctl, int nb, unsigned* flag
     } else {
       unsigned it = 0;
       while (*gen == g) {
-        __nanosleep(64);
-        if (++it > (1u << 21)) {
+        if (++it > (1u << 22)) {
           atomicOr(flags, 2u);
           break;
         }

@@ -818,8 +818,9 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     int cnt[K_COUNT];
     cnt[K_NODES] = div_up(h.dims.N, 256);
     cnt[K_NODES16] = div_up(16LL * h.dims.N, 256);
-    // fused IB kernel: about one thread per touched-cell candidate / 4, at most 128 CTAs
-    cnt[K_IBCOOP] = c.enable_fluid ? std::max(1, std::min(128, div_up(h.M, 1024))) : 0;
+    // fused IB kernel: one thread per touched-cell candidate / 4 (scaled down at bind if
+    // the plan's CTAs would not all be resident)
+    cnt[K_IBCOOP] = c.enable_fluid ? std::max(1, div_up(h.M, 1024)) : 0;
     cnt[K_COMP] = h.dims.N > 0 ? (int)h.generic_comp.size() : 0;
     cnt[K_CHAIN] = h.dims.N > 0 ? div_up((long long)h.chain_comp.size(), 4) : 0;
     cnt[K_IB] = div_up(h.M, 256);
