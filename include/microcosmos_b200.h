@@ -162,10 +162,10 @@ mc_status mc_plan_read_flags(mc_plan* plan, uint32_t* flags, int32_t clear, void
  * kernels inside the graph). */
 int64_t mc_plan_last_launch_count(const mc_plan* plan);
 
-/* The multi-direct forcing iterations run as one cooperative kernel with device-side
- * barriers when every CTA of it fits on the GPU at once (the default), else as separate
- * interpolate / spread launches.  Both give identical results; this switch (after
- * mc_plan_bind, outside a rollout) selects the separate launches (enable = 0). */
+/* The multi-direct forcing iterations run either as separate interpolate / spread launches
+ * (the default) or, with enable != 0, as one cooperative kernel with bounded device-side
+ * barriers (used only when all of its CTAs fit on the GPU at once).  Both give identical
+ * results.  Call after mc_plan_bind, outside a rollout. */
 mc_status mc_plan_set_fused_ib(mc_plan* plan, int32_t enable);
 int32_t mc_plan_uses_fused_ib(const mc_plan* plan);
 

@@ -85,7 +85,7 @@ struct mc_plan {
   int max_chain = 0, chain_slots = 1;
   int max_k = 0;  // largest IB kernel size of the plan
   bool use_coop = false, coop_cap_checked = false;
-  bool fused_ib = true;  // mc_plan_set_fused_ib
+  bool fused_ib = false;  // mc_plan_set_fused_ib (separate launches measured faster)
   bool coop_possible = false;
   cudaError_t coop_err = cudaSuccess;
   std::vector<RDesc> desc;
