@@ -332,7 +332,7 @@ def main():
                     "api": "microcosmos_b200.simulate.run (pinned host inputs -> host outputs)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_lbm<4> (fused pull stream + TRT/Guo collide)",
+                         "kernel": "k_lbm (fused pull stream + TRT/Guo collide, float2 rows)",
                          "algorithmic_bytes_per_launch": BYTES_PER_CELL * cells,
                          "ms_per_launch": lbm_s * 1e3},
             "cpu_baseline": cpu,
