@@ -908,8 +908,18 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
   for (int k = 0; k < K_COUNT; ++k) MC_CUDA(up(p->r_off[k], p->off[k].data(), p->off[k].size() * 4));
   MC_CUDA(up(p->r_desc, p->desc.data(), p->desc.size() * sizeof(RDesc)));
   // zero the binning counters of every tile before the first clear kernel runs
-  MC_CUDA(mc::node_set_smem(std::max<size_t>(p->node_smem, 1)));
-  if (p->any_steric) MC_CUDA(mc::fft_set_smem(p->fftr_smem, p->fftc_smem));
+  {
+    // The dynamic shared memory limit is a per-kernel attribute shared by every plan of the
+    // process: raise it to the device's opt-in maximum (never lower it to this plan's need,
+    // which would break plans with larger grids).
+    int dev = 0, optin = 0;
+    MC_CUDA(cudaGetDevice(&dev));
+    MC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (p->node_smem > (size_t)optin || p->fftr_smem > (size_t)optin || p->fftc_smem > (size_t)optin)
+      return fail(MC_ERR_UNSUPPORTED, "shared memory needed by the plan exceeds the device limit");
+    MC_CUDA(mc::node_set_smem((size_t)optin));
+    if (p->any_steric) MC_CUDA(mc::fft_set_smem((size_t)optin, (size_t)optin));
+  }
   mc::launch_clear_ws(L(p, K_CELLS, s));
   MC_CUDA(cudaGetLastError());
   destroy_graphs(p);

@@ -257,3 +257,18 @@ def test_fused_and_separate_ib_kernels_agree():
     for a, b in zip(*results):
         for k in a:
             np.testing.assert_array_equal(a[k], b[k])
+
+
+def test_plans_of_different_sizes_coexist():
+    """Binding a plan with a small grid must not break a plan with a larger one."""
+    big = scenarios.make_scenario(256, 256, 2, 20, seed=51)
+    small = scenarios.make_scenario(32, 32, 1, 10, seed=52)
+    cfg = baseline_config()
+    st_big = DeviceState.from_scenario(big)
+    plan_big = Plan.for_states([st_big], [cfg], [0.01])
+    st_small = DeviceState.from_scenario(small)
+    Plan.for_states([st_small], [cfg], [0.01]).rollout([st_small], 2)
+    plan_big.rollout([st_big], 3, actuations=[Actuation.from_scenario(big)])
+    torch.cuda.synchronize()
+    ref = _oracle_run(big, 3)
+    assert rel(st_big.position, ref.position) < TOL
