@@ -178,6 +178,28 @@ mc_status mc_plan_profile_read(mc_plan* plan, const char* kernel, double* total_
 mc_status mc_plan_profile_reset(mc_plan* plan);
 const char* mc_profile_kernel_names(void);
 
+/* Steric potential field of N node positions without any device allocation.
+ *
+ * No counterpart in the reference: it computes the same field as the reference's
+ * update_steric_potential (cloud-in-cell deposit of the wrapped positions followed by the
+ * spectral Gaussian of width sigma) and as fields.steric after a step from these positions
+ * with zero velocity, but for callers that cannot call cudaMalloc — e.g. a custom call
+ * inside a framework that owns all device memory and gave it no workspace buffer, or a
+ * host loop that must not allocate once it is running.  position (N,2) and steric_out
+ * (H,W) are caller-owned device arrays; nothing else is passed in.
+ *
+ * Limits: 1 <= N <= MC_NOALLOC_MAX_NODES, 4 <= H, W <= MC_NOALLOC_MAX_GRID (prime factors
+ * <= 13); larger sizes return MC_ERR_INVALID.  The scratch (about 6.6 MB) is one
+ * file-scope __device__ array that every GPU loading this library keeps until the process
+ * exits.  The first call made on a device looks up that array's device address (set-up);
+ * make that first call before any stream capture.  All calls share the array and each call
+ * re-initialises what must start at zero, so calls that overlap on the GPU (different
+ * streams, no ordering between them) race and must not be issued. */
+#define MC_NOALLOC_MAX_GRID 512
+#define MC_NOALLOC_MAX_NODES 16384
+mc_status mc_steric_potential_noalloc(const float* position, int32_t N, int32_t H, int32_t W, float sigma,
+                                      float scatter_value, float* steric_out, void* stream);
+
 /* Text of the last error of this thread ("" if none). */
 const char* mc_last_error(void);
 

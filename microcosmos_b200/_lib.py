@@ -101,6 +101,8 @@ SIGNATURES = {
     "mc_plan_read_flags": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int32,
                                           ctypes.c_void_p]),
     "mc_plan_last_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
+    "mc_steric_potential_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                   ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]),
     "mc_last_error": (ctypes.c_char_p, []),
     "mc_version": (ctypes.c_char_p, []),
 }

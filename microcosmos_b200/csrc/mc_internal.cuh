@@ -217,6 +217,7 @@ void launch_stream_out(const Launch& L, int parity);
 void launch_clear_ws(const Launch& L);
 void launch_tick(int* tdev, cudaStream_t s);
 cudaError_t fft_set_smem(size_t rows, size_t cols);
+void set_last_error(const char* msg);  // text returned by mc_last_error() on this thread
 cudaError_t node_set_smem(size_t bytes);
 
 }  // namespace mc

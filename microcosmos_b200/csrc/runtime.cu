@@ -668,6 +668,10 @@ void destroy_graphs(mc_plan* p) {
 
 }  // namespace
 
+namespace mc {
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace mc
+
 extern "C" {
 
 const char* mc_last_error(void) { return g_err.c_str(); }
