@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--config", default="scale", choices=["scale", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=100)
+    ap.add_argument("--batch-rollouts", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--no-batch", action="store_true")
     return ap.parse_args()
 
 
@@ -153,6 +156,84 @@ def cpu_baseline(sc, cfg_steps_budget_s=15.0):
     return {"value": cells * n / dt / 1e6, "unit": "MLUPS", "cores": 1, "kind": "port",
             "sample": f"{n} steps of the {sc.H}x{sc.W} workload after 1 warm-up step (numpy restatement, not JAX; "
                       f"{dt:.1f} s)", "seconds_per_step": dt / n}
+
+
+def batch_section(args, flush):
+    """Batching configuration: an evolutionary-search population of uneven rollouts (side
+    ~U{128,192,256,384,512}, filaments ~U{1..32}, nodes/filament ~U{16..128}, amplitude
+    ~N(0.2, 0.05), 2000-step rollouts) stepped together as one plan (every kernel launched
+    once per step for the whole population, steps replayed from CUDA graphs), against the
+    plain path: the same rollouts as one plan each, run one after another.  Rollouts/s are
+    for 2000-step rollouts, from the per-step device time of a bounded number of steps."""
+    import torch
+    from microcosmos_b200 import baseline_config, scenarios
+    from microcosmos_b200.engine import Actuation, DeviceState, Plan
+    cfg = baseline_config()
+    scs = scenarios.config_batch(args.batch_rollouts, seed=0)
+    cells = sum(s.H * s.W for s in scs)
+    nodes = sum(s.N for s in scs)
+    sts = [DeviceState.from_scenario(s) for s in scs]
+    acts = [Actuation.from_scenario(s) for s in scs]
+    plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs))
+    stream = torch.cuda.current_stream()
+    plan.begin(sts, actuations=acts)
+    plan.advance(6, use_graph=True)
+    K = args.batch_steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    torch.cuda.synchronize()
+    for i in range(K):
+        flush.zero_()
+        ev[i][0].record(stream)
+        plan.advance(1, use_graph=True, last=(i == K - 1))
+        ev[i][1].record(stream)
+    plan.end()
+    torch.cuda.synchronize()
+    t_batch = sum(a.elapsed_time(b) for a, b in ev) / K  # ms per step, whole population
+    flags = plan.read_flags()
+    # dense-pass share of a batched step (per-kernel events, sequential schedule)
+    plan.profile(True)
+    plan.begin(sts, actuations=acts)
+    plan.advance(1, use_graph=False)
+    plan.profile_reset()
+    for i in range(10):
+        flush.zero_()
+        plan.advance(1, use_graph=False, last=(i == 9))
+    plan.end()
+    torch.cuda.synchronize()
+    prof = plan.profile_read()
+    plan.profile(False)
+    lbm_ms = prof["lbm"][0] / max(prof["lbm"][1], 1)
+    del plan
+    # plain: one plan per rollout, run sequentially (a bounded subset of the population)
+    nplain = min(len(scs), 32)
+    t_plain = 0.0
+    for s, st, a in zip(scs[:nplain], sts[:nplain], acts[:nplain]):
+        p1 = Plan.for_states([st], [cfg], [0.01])
+        p1.begin([st], actuations=[a])
+        p1.advance(4, use_graph=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        p1.advance(K, use_graph=True, last=True)
+        e1.record(stream)
+        p1.end()
+        torch.cuda.synchronize()
+        t_plain += e0.elapsed_time(e1) / K  # ms per step of this rollout
+        del p1
+    t_plain_pop = t_plain / nplain * len(scs)  # ms per step, population run sequentially
+    steps = 2000
+    return {
+        "workload": f"{len(scs)} uneven rollouts (side U{{128..512}}, 1-32 filaments x 16-128 nodes), "
+                    f"{cells} cells, {nodes} nodes in total; rollouts/s for 2000-step rollouts",
+        "steps_timed": K, "ms_per_step": t_batch, "mlups": cells / (t_batch / 1e3) / 1e6,
+        "rollouts_per_s": len(scs) / (t_batch / 1e3 * steps),
+        "plain_rollouts_per_s": len(scs) / (t_plain_pop / 1e3 * steps),
+        "plain_sample": f"{nplain} rollouts, one plan each, {K} graph-launched steps each",
+        "speedup_vs_plain": t_plain_pop / t_batch,
+        "lbm_ms_per_launch": lbm_ms, "lbm_frac_of_peak": BYTES_PER_CELL * cells / (lbm_ms / 1e3) / 1e9 / 6541.5,
+        "roofline_frac_mlups": cells / (t_batch / 1e3) / 1e6 / (6541.5e9 / BYTES_PER_CELL / 1e6),
+        "flags_nonzero": int(sum(1 for f in flags if f)),
+        "l2": "flushed (256 MiB write) before every timed step"}
 
 
 def dist_setup():
@@ -316,6 +397,9 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(sc)
+    batch = None
+    if ws == 1 and not args.no_batch:
+        batch = batch_section(args, flush)
 
     if rank == 0:
         value = cells * K * ws / (t_ms / 1e3) / 1e6
@@ -340,6 +424,7 @@ def main():
             "gpu_launches": int(launches),
             "kernels": per_step,
             "flags": flags,
+            "batch": batch,
             "step_kernel_ms": step_kernel_ms / P,
         }
         print(json.dumps(out))
