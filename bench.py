@@ -230,7 +230,8 @@ def batch_section(args, flush):
         "plain_rollouts_per_s": len(scs) / (t_plain_pop / 1e3 * steps),
         "plain_sample": f"{nplain} rollouts, one plan each, {K} graph-launched steps each",
         "speedup_vs_plain": t_plain_pop / t_batch,
-        "lbm_ms_per_launch": lbm_ms, "lbm_frac_of_peak": BYTES_PER_CELL * cells / (lbm_ms / 1e3) / 1e9 / 6541.5,
+        "lbm_ms_per_launch": lbm_ms,
+        "kernels_ms_per_step": {k: ms / 10 for k, (ms, n) in prof.items() if n}, "lbm_frac_of_peak": BYTES_PER_CELL * cells / (lbm_ms / 1e3) / 1e9 / 6541.5,
         "roofline_frac_mlups": cells / (t_batch / 1e3) / 1e6 / (6541.5e9 / BYTES_PER_CELL / 1e6),
         "flags_nonzero": int(sum(1 for f in flags if f)),
         "l2": "flushed (256 MiB write) before every timed step"}

@@ -119,10 +119,9 @@ __device__ __forceinline__ void head_work(const RDesc& d, const BinView& v, int 
   ib_head(d, parity, cell, acc, slot, len, run_pos);
 }
 
-// One CTA (256 threads) per bin tile: sort the tile's contributions by (cell, k) and
+// One CTA (256 threads) on one bin tile: sort the tile's contributions by (cell, k) and
 // reduce every cell's run.
-__global__ void __launch_bounds__(256) k_bin_tiles(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
-                                                   int which, int parity) {
+__device__ void tile_work(const RDesc& d, int which, int parity, int t) {
   constexpr int kCapS = kSortCap / 4;  // entries handled in shared memory (>= every bin capacity)
   __shared__ unsigned skeys[kSortCap];
   __shared__ int cnt[kBinTile * kBinTile];
@@ -130,11 +129,8 @@ __global__ void __launch_bounds__(256) k_bin_tiles(const RDesc* __restrict__ D, 
   __shared__ int hpos[kBinTile * kBinTile];  // rank of a touched cell among the tile's touched cells
   __shared__ int s_spill, s_heads, s_base;
   static_assert(kIbCap <= kCapS && kCicCap <= kCapS, "bin capacity exceeds the shared-memory sort");
-  const int r = find_rollout(off, n, blockIdx.x);
-  const RDesc& d = D[r];
   const BinView v = bin_view(d, which);
   if (v.count == 0) return;
-  const int t = blockIdx.x - off[r];
   const int total = v.tcount[t];
   if (total == 0) return;
   const int tid = threadIdx.x;
@@ -305,6 +301,19 @@ __global__ void __launch_bounds__(256) k_bin_tiles(const RDesc* __restrict__ D, 
   }
   __syncthreads();
   if (tid == 0) v.tcount[t] = 0;
+}
+
+// The bin tiles that received contributions this step, listed by the producers as
+// (rollout, tile) pairs; a fixed grid of CTAs walks the list (most tiles of a large or
+// batched grid are empty and are never visited).
+__global__ void __launch_bounds__(256) k_bin_tiles(const RDesc* __restrict__ D, const int2* __restrict__ wl,
+                                                   const int* __restrict__ wl_count, int which, int parity) {
+  const int count = *wl_count;
+  for (int i = blockIdx.x; i < count; i += gridDim.x) {
+    const int2 item = wl[i];
+    tile_work(D[item.x], which, parity, item.y);
+    __syncthreads();  // the shared arrays are reused by the next item
+  }
 }
 
 // Weighted sum of a head-indexed field over the K*K stencil of one node, in stencil order
@@ -615,6 +624,7 @@ __global__ void __launch_bounds__(256) k_reaction(const RDesc* __restrict__ D, c
     d.c_ctl[0] = 0;
     d.c_ctl[1] = 0;
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) d.wl_ctl[1] = 0;  // the plan's CIC tile list
   if (node >= d.N) return;
   float vx = d.vel[2 * node], vy = d.vel[2 * node + 1];
   if (d.enable_fluid) {
@@ -668,8 +678,8 @@ __global__ void k_record_fields(const RDesc* __restrict__ D, const int* __restri
 
 __global__ void k_tick(int* tdev) { *tdev += 1; }
 
-void launch_bin_tiles(const Launch& L, int which, int parity) {
-  k_bin_tiles<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, which, parity);
+void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity) {
+  k_bin_tiles<<<L.grid, 256, 0, L.s>>>(L.d, wl, wl_count, which, parity);
 }
 void launch_ib_interp(const Launch& L, int it) { k_ib_interp<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
 void launch_ib_spread(const Launch& L, int it) { k_ib_spread<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }

@@ -128,6 +128,11 @@ struct RDesc {
   int* c_tcount;
   int* c_ovf;       // (4N)
   int* c_ctl;       // (4)
+  // plan-wide lists of bin tiles that received contributions this step: (rollout, tile)
+  int ridx;            // this rollout's index in the plan
+  int2* wl_ib;
+  int2* wl_cic;
+  int* wl_ctl;         // [0] IB list length, [1] CIC list length
   // rod components: chains (warp kernel) and general graphs (CTA kernel)
   int nchain, ngeneric;
   const int* chain_comp;    // (nchain) component index
@@ -196,7 +201,7 @@ struct Launch {
 };
 
 void launch_predict(const Launch& L);
-void launch_bin_tiles(const Launch& L, int which, int parity);
+void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity);
 void launch_fft_rows(const Launch& L, size_t smem);
 void launch_fft_cols(const Launch& L, size_t smem);
 void launch_node(const Launch& L, const int* tdev, size_t smem, int bs);

@@ -44,7 +44,9 @@ constexpr size_t kOffTwH = kOffTwW + al(kNaMaxGrid * 8);
 constexpr size_t kOffGW = kOffTwH + al(kNaMaxGrid * 8);
 constexpr size_t kOffGH = kOffGW + al(kNaMaxGrid * 4);
 constexpr size_t kOffFlags = kOffGH + al(kNaMaxGrid * 4);
-constexpr size_t kNaBytes = kOffFlags + 256;  // about 6.6 MB
+constexpr size_t kOffWl = kOffFlags + 256;                                    // tile list (int2)
+constexpr size_t kOffWlCtl = kOffWl + al(kNaMaxTiles * 8);
+constexpr size_t kNaBytes = kOffWlCtl + 256;  // about 6.6 MB
 
 // The scratch.  Every GPU that loads this library holds one copy until the process exits.
 // In host code `g_na_scratch` only names the symbol; its device address comes from
@@ -156,6 +158,10 @@ extern "C" mc_status mc_steric_potential_noalloc(const float* position, int32_t 
   d.c_ctl = reinterpret_cast<int*>(P(kOffCtl));
   d.ib_ctl = reinterpret_cast<int*>(P(kOffCtl)) + 8;
   d.flags = reinterpret_cast<unsigned*>(P(kOffFlags));
+  d.ridx = 0;
+  d.wl_cic = reinterpret_cast<int2*>(P(kOffWl));
+  d.wl_ib = reinterpret_cast<int2*>(P(kOffWl));  // unused (no IB here); k_predict resets its length
+  d.wl_ctl = reinterpret_cast<int*>(P(kOffWlCtl));
 
   // CTA offset tables of the four kernels: deposit (nodes), bin tiles, FFT rows, FFT columns
   const int cnt[4] = {(N + 255) / 256, d.ntile_x * d.ntile_y, (H + 1) / 2,
@@ -183,6 +189,7 @@ extern "C" mc_status mc_steric_potential_noalloc(const float* position, int32_t 
   chk(cudaMemsetAsync(P(kOffTcount), 0, (size_t)d.ntile_x * d.ntile_y * 4, s));
   chk(cudaMemsetAsync(P(kOffCtl), 0, 16 * 4, s));
   chk(cudaMemsetAsync(P(kOffDep), 0, HW * 4, s));
+  chk(cudaMemsetAsync(P(kOffWlCtl), 0, 4 * sizeof(int), s));
   if (e != cudaSuccess) return na_fail(MC_ERR_CUDA, std::string("scratch set-up copy: ") + cudaGetErrorString(e));
   // cudaMemcpyAsync from pageable host memory returns after the source has been staged,
   // so the host arrays above may go out of scope
@@ -191,8 +198,9 @@ extern "C" mc_status mc_steric_potential_noalloc(const float* position, int32_t 
   mc::Launch l{dd, off, 1, cnt[0], s};
   mc::launch_predict(l);
   l.off = off + 2;
-  l.grid = cnt[1];
-  mc::launch_bin_tiles(l, 1, 0);
+  l.grid = cnt[1] < 1184 ? cnt[1] : 1184;
+  mc::launch_bin_tiles(l, reinterpret_cast<const int2*>(P(kOffWl)), reinterpret_cast<const int*>(P(kOffWlCtl)) + 1, 1,
+                       0);
   l.off = off + 4;
   l.grid = cnt[2];
   mc::launch_fft_rows(l, (size_t)3 * W * sizeof(float2) + W * sizeof(float));

@@ -26,6 +26,7 @@ __global__ void __launch_bounds__(256) k_predict(const RDesc* __restrict__ D, co
     d.ib_ctl[1] = 0;
     d.ib_ctl[2] = 0;
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) d.wl_ctl[0] = 0;  // the plan's IB tile list
   if (node >= d.N) return;
   const float px = d.pos[2 * node], py = d.pos[2 * node + 1];
   const float vx = d.vel[2 * node] * d.damping, vy = d.vel[2 * node + 1] * d.damping;
@@ -68,7 +69,8 @@ __global__ void __launch_bounds__(256) k_predict(const RDesc* __restrict__ D, co
   int base[4], rank[4];
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    base[c] = cnt[c] ? atomicAdd(d.c_tcount + tile[c], cnt[c]) : 0;
+    base[c] = cnt[c] ? atomicAdd(d.c_tcount + tile[c], cnt[c]) : -1;
+    if (base[c] == 0) d.wl_cic[atomicAdd(d.wl_ctl + 1, 1)] = make_int2(d.ridx, tile[c]);
     rank[c] = 0;
   }
 #pragma unroll
@@ -247,7 +249,10 @@ __global__ void __launch_bounds__(256) k_stencil(const RDesc* __restrict__ D, co
   const int counts[4] = {nx0 * ny0, nx1 * ny0, nx0 * ny1, nx1 * ny1};
   if (split_ok) {
 #pragma unroll
-    for (int g = 0; g < 4; ++g) base[g] = counts[g] ? atomicAdd(d.ib_tcount + tiles[g], counts[g]) : 0;
+    for (int g = 0; g < 4; ++g) {
+      base[g] = counts[g] ? atomicAdd(d.ib_tcount + tiles[g], counts[g]) : -1;
+      if (base[g] == 0) d.wl_ib[atomicAdd(d.wl_ctl, 1)] = make_int2(d.ridx, tiles[g]);
+    }
   }
   int rank[4] = {0, 0, 0, 0};
   const int cap = d.ib_cap;
@@ -270,6 +275,7 @@ __global__ void __launch_bounds__(256) k_stencil(const RDesc* __restrict__ D, co
           } else {
             tile = (cy[b] / kBinTile) * d.ntile_x + cx[a] / kBinTile;
             pos = atomicAdd(d.ib_tcount + tile, 1);
+            if (pos == 0) d.wl_ib[atomicAdd(d.wl_ctl, 1)] = make_int2(d.ridx, tile);
           }
           if (pos < cap) {
             d.ib_store[(size_t)tile * cap + pos] = k;
@@ -332,7 +338,10 @@ __global__ void __launch_bounds__(256) k_stencil16(const RDesc* __restrict__ D, 
   const unsigned group = __match_any_sync(active, tile);
   const int leader = __ffs(group) - 1;
   int base = 0;
-  if (lane == leader) base = atomicAdd(d.ib_tcount + tile, __popc(group));
+  if (lane == leader) {
+    base = atomicAdd(d.ib_tcount + tile, __popc(group));
+    if (base == 0) d.wl_ib[atomicAdd(d.wl_ctl, 1)] = make_int2(d.ridx, tile);
+  }
   base = __shfl_sync(group, base, leader);
   const int pos = base + __popc(group & ((1u << lane) - 1u));
   if (pos < d.ib_cap) {

@@ -73,7 +73,8 @@ struct mc_plan {
   int n = 0;
   std::vector<HostRollout> R;
   size_t ws_bytes = 0;
-  Region r_desc, r_tdev;
+  Region r_desc, r_tdev, r_wl_ib, r_wl_cic, r_wl_ctl;
+  int tile_grid = 1;  // CTAs walking the tile lists
   Region r_off[K_COUNT];
   std::vector<int> off[K_COUNT];
   int grid[K_COUNT] = {};
@@ -439,6 +440,10 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.c_tcount = at<int>(b, h.r_ctc);
   d.c_ovf = at<int>(b, h.r_covf);
   d.c_ctl = at<int>(b, h.r_cctl);
+  d.ridx = i;
+  d.wl_ib = at<int2>(b, p->r_wl_ib);
+  d.wl_cic = at<int2>(b, p->r_wl_cic);
+  d.wl_ctl = at<int>(b, p->r_wl_ctl);
   d.nchain = (int)h.chain_comp.size();
   d.ngeneric = (int)h.generic_comp.size();
   d.chain_comp = at<int>(b, h.r_chain);
@@ -508,7 +513,11 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
     ++k;
   }
   if (p->any_steric) {
-    timed(p, 1, s, capture, [&] { mc::launch_bin_tiles(L(p, K_TILES, s), 1, 0); });
+    timed(p, 1, s, capture, [&] {
+      mc::Launch l = L(p, K_TILES, s);
+      l.grid = p->tile_grid;
+      mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_cic), at<int>(p->ws, p->r_wl_ctl) + 1, 1, 0);
+    });
     timed(p, 2, s, capture, [&] { mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem); });
     timed(p, 3, s, capture, [&] { mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem); });
     k += 3;
@@ -538,7 +547,11 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
 int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
   if (!p->any_fluid) return 0;
   int64_t k = 0;
-  timed(p, 6, s, capture, [&] { mc::launch_bin_tiles(L(p, K_TILES, s), 0, parity); });
+  timed(p, 6, s, capture, [&] {
+    mc::Launch l = L(p, K_TILES, s);
+    l.grid = p->tile_grid;
+    mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_ib), at<int>(p->ws, p->r_wl_ctl), 0, parity);
+  });
   ++k;
   if (p->use_coop) {
     timed(p, 16, s, capture, [&] { p->coop_err = mc::launch_ib_coop(L(p, K_IBCOOP, s), parity); });
@@ -688,6 +701,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
   Layout lay;
   p->r_desc = lay.take(sizeof(RDesc) * n);
   p->r_tdev = lay.take(sizeof(int));
+  p->r_wl_ctl = lay.take(4 * sizeof(int));
   for (int k = 0; k < K_COUNT; ++k) p->r_off[k] = lay.take(sizeof(int) * (n + 1));
   int vec_all = -1;
   for (int i = 0; i < n; ++i) {
@@ -811,6 +825,13 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.lbm_ty = div_up(h.dims.H, mc::kLbmTileY);
     h.r_lflag = lay.take((size_t)2 * h.lbm_tx * h.lbm_ty * 4);
   }
+  {
+    long long tiles = 0;
+    for (auto& h : p->R) tiles += (long long)h.ntx * h.nty;
+    p->r_wl_ib = lay.take((size_t)tiles * sizeof(int2));
+    p->r_wl_cic = lay.take((size_t)tiles * sizeof(int2));
+    p->tile_grid = (int)std::max(1LL, std::min(tiles, 148LL * 8));
+  }
   p->ws_bytes = lay.cur;
   // CTA offset tables
   for (int k = 0; k < K_COUNT; ++k) p->off[k].assign(n + 1, 0);
@@ -924,6 +945,7 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
     MC_CUDA(mc::node_set_smem((size_t)optin));
     if (p->any_steric) MC_CUDA(mc::fft_set_smem((size_t)optin, (size_t)optin));
   }
+  MC_CUDA(cudaMemsetAsync(p->ws + p->r_wl_ctl.off, 0, 4 * sizeof(int), s));
   mc::launch_clear_ws(L(p, K_CELLS, s));
   MC_CUDA(cudaGetLastError());
   destroy_graphs(p);
