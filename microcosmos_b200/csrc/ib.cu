@@ -120,15 +120,15 @@ __device__ __forceinline__ void head_work(const RDesc& d, const BinView& v, int 
 }
 
 // One CTA (256 threads) on one bin tile: sort the tile's contributions by (cell, k) and
-// reduce every cell's run.
-__device__ void tile_work(const RDesc& d, int which, int parity, int t) {
-  constexpr int kCapS = kSortCap / 4;  // entries handled in shared memory (>= every bin capacity)
-  __shared__ unsigned skeys[kSortCap];
+// reduce every cell's run.  skeys: dynamic shared memory of 4 * capS words, capS >= the
+// bin capacity of every rollout of the launch (a power of two).
+__device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned* skeys, int capS) {
+  const int kCapS = capS;
+  const int kChunk = 4 * capS;  // keys per shared-memory chunk sort on the spill path
   __shared__ int cnt[kBinTile * kBinTile];
   __shared__ int cpos[kBinTile * kBinTile];
   __shared__ int hpos[kBinTile * kBinTile];  // rank of a touched cell among the tile's touched cells
-  __shared__ int s_spill, s_heads, s_base;
-  static_assert(kIbCap <= kCapS && kCicCap <= kCapS, "bin capacity exceeds the shared-memory sort");
+  __shared__ int s_spill, s_heads, s_base, s_fill;
   const BinView v = bin_view(d, which);
   if (v.count == 0) return;
   const int total = v.tcount[t];
@@ -244,19 +244,21 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t) {
     const int k = bin[i];
     bufB[i] = (local_of(d, v.cell[k]) << 24) | (unsigned)k;
   }
-  if (tid == 0) {
-    // the overflow list is unordered: collect this tile's entries sequentially
-    int m = v.cap;
+  if (tid == 0) s_fill = v.cap;
+  __syncthreads();
+  {
+    // the overflow list is unordered: every thread scans a stride of it for this tile's
+    // entries (their order is restored by the sort below)
     const int no = v.ctl[0];
-    for (int i = 0; i < no && m < total; ++i) {
+    for (int i = tid; i < no; i += blockDim.x) {
       const int k = v.ovf[i];
-      if (tile_of(d, v.cell[k]) == t) bufB[m++] = (local_of(d, v.cell[k]) << 24) | (unsigned)k;
+      if (tile_of(d, v.cell[k]) == t) bufB[atomicAdd(&s_fill, 1)] = (local_of(d, v.cell[k]) << 24) | (unsigned)k;
     }
   }
   __syncthreads();
   const int m = total;
-  for (int c0 = 0; c0 < m; c0 += kSortCap) {
-    const int len = min(kSortCap, m - c0);
+  for (int c0 = 0; c0 < m; c0 += kChunk) {
+    const int len = min(kChunk, m - c0);
     int P = 1;
     while (P < len) P <<= 1;
     for (int i = tid; i < P; i += blockDim.x) skeys[i] = i < len ? bufB[c0 + i] : 0xffffffffu;
@@ -267,7 +269,7 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t) {
   }
   unsigned* src = bufA;
   unsigned* dst = bufB;
-  for (int wdt = kSortCap; wdt < m; wdt <<= 1) {
+  for (int wdt = kChunk; wdt < m; wdt <<= 1) {
     for (int i = tid; i < m; i += blockDim.x) {
       const int ps = (i / (2 * wdt)) * (2 * wdt);
       const int a_len = min(wdt, m - ps);
@@ -307,11 +309,12 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t) {
 // (rollout, tile) pairs; a fixed grid of CTAs walks the list (most tiles of a large or
 // batched grid are empty and are never visited).
 __global__ void __launch_bounds__(256) k_bin_tiles(const RDesc* __restrict__ D, const int2* __restrict__ wl,
-                                                   const int* __restrict__ wl_count, int which, int parity) {
+                                                   const int* __restrict__ wl_count, int which, int parity, int capS) {
+  extern __shared__ unsigned dyn[];
   const int count = *wl_count;
   for (int i = blockIdx.x; i < count; i += gridDim.x) {
     const int2 item = wl[i];
-    tile_work(D[item.x], which, parity, item.y);
+    tile_work(D[item.x], which, parity, item.y, dyn, capS);
     __syncthreads();  // the shared arrays are reused by the next item
   }
 }
@@ -678,8 +681,11 @@ __global__ void k_record_fields(const RDesc* __restrict__ D, const int* __restri
 
 __global__ void k_tick(int* tdev) { *tdev += 1; }
 
-void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity) {
-  k_bin_tiles<<<L.grid, 256, 0, L.s>>>(L.d, wl, wl_count, which, parity);
+void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity, int capS) {
+  k_bin_tiles<<<L.grid, 256, (size_t)4 * capS * sizeof(unsigned), L.s>>>(L.d, wl, wl_count, which, parity, capS);
+}
+cudaError_t tiles_set_smem(size_t bytes) {
+  return cudaFuncSetAttribute(k_bin_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 void launch_ib_interp(const Launch& L, int it) { k_ib_interp<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
 void launch_ib_spread(const Launch& L, int it) { k_ib_spread<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }

@@ -18,9 +18,9 @@ namespace mc {
 constexpr int kBinTile = 16;       // binning tile edge for the deterministic reductions
 constexpr int kLbmTileX = 128;     // dense LBM CTA tile: 32 lanes x 4 cells
 constexpr int kLbmTileY = 8;       //                    8 rows
-constexpr int kSortCap = 4096;     // keys sorted in shared memory per pass (>= every bin capacity)
-constexpr int kIbCap = 1024;       // IB contributions per 16x16 bin tile before spilling
-constexpr int kCicCap = 512;       // CIC contributions per bin tile before spilling
+constexpr int kIbCap = 1024;       // minimum IB bin capacity per 16x16 tile (grown with node density)
+constexpr int kCicCap = 512;       // minimum CIC bin capacity per tile
+constexpr int kMaxBinCap = 8192;   // largest bin capacity (the tile sort keeps 4 x cap words in shared memory)
 constexpr int kFftMaxN = 4096;     // largest FFT length (shared memory)
 constexpr int kFftMaxFactors = 16;
 constexpr int kFftColsPerCta = 2;  // complex columns per column-pass CTA (4 real columns)
@@ -201,7 +201,8 @@ struct Launch {
 };
 
 void launch_predict(const Launch& L);
-void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity);
+void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity, int capS);
+cudaError_t tiles_set_smem(size_t bytes);
 void launch_fft_rows(const Launch& L, size_t smem);
 void launch_fft_cols(const Launch& L, size_t smem);
 void launch_node(const Launch& L, const int* tdev, size_t smem, int bs);

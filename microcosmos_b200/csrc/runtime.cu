@@ -58,6 +58,7 @@ struct HostRollout {
   std::vector<float2> twW, twH;
   std::vector<float> gW, gH;
   int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4;
+  int ib_cap = 0, c_cap = 0;  // bin capacities (powers of two)
   // workspace regions (offsets relative to the workspace base)
   Region r_h0, r_h1, r_fov, r_lflag, r_dep, r_tmp, r_prev, r_pred, r_predw, r_nvl, r_delta;
   Region r_ibcell, r_ibw, r_ibstore, r_ibtc, r_ibovf, r_ibctl, r_ibslot, r_hcell, r_hstart, r_hlen, r_srho, r_svx,
@@ -75,6 +76,7 @@ struct mc_plan {
   size_t ws_bytes = 0;
   Region r_desc, r_tdev, r_wl_ib, r_wl_cic, r_wl_ctl;
   int tile_grid = 1;  // CTAs walking the tile lists
+  int ib_capS = 0, c_capS = 0;  // largest bin capacity of the plan (tile-sort shared memory)
   Region r_off[K_COUNT];
   std::vector<int> off[K_COUNT];
   int grid[K_COUNT] = {};
@@ -414,7 +416,7 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.predw = at<float>(b, h.r_predw);
   d.nvl = at<float>(b, h.r_nvl);
   d.delta = at<float>(b, h.r_delta);
-  d.ib_cap = mc::kIbCap;
+  d.ib_cap = h.ib_cap;
   d.ib_cell = at<int>(b, h.r_ibcell);
   d.ib_w = at<float>(b, h.r_ibw);
   d.ib_store = at<int>(b, h.r_ibstore);
@@ -433,7 +435,7 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.s_ucy = at<float>(b, h.r_sucy);
   d.s_fx = at<float>(b, h.r_sfx);
   d.s_fy = at<float>(b, h.r_sfy);
-  d.c_cap = mc::kCicCap;
+  d.c_cap = h.c_cap;
   d.c_cell = at<int>(b, h.r_ccell);
   d.c_w = at<float>(b, h.r_cw);
   d.c_store = at<int>(b, h.r_cstore);
@@ -516,7 +518,7 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
     timed(p, 1, s, capture, [&] {
       mc::Launch l = L(p, K_TILES, s);
       l.grid = p->tile_grid;
-      mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_cic), at<int>(p->ws, p->r_wl_ctl) + 1, 1, 0);
+      mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_cic), at<int>(p->ws, p->r_wl_ctl) + 1, 1, 0, p->c_capS);
     });
     timed(p, 2, s, capture, [&] { mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem); });
     timed(p, 3, s, capture, [&] { mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem); });
@@ -550,7 +552,7 @@ int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
   timed(p, 6, s, capture, [&] {
     mc::Launch l = L(p, K_TILES, s);
     l.grid = p->tile_grid;
-    mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_ib), at<int>(p->ws, p->r_wl_ctl), 0, parity);
+    mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_ib), at<int>(p->ws, p->r_wl_ctl), 0, parity, p->ib_capS);
   });
   ++k;
   if (p->use_coop) {
@@ -773,7 +775,16 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     const size_t Mz = (size_t)M;
     h.r_ibcell = lay.take(Mz * 4);
     h.r_ibw = lay.take(Mz * 4);
-    h.r_ibstore = lay.take((nt * mc::kIbCap + 2 * Mz) * 4);
+    // bin capacity: at least 3x the mean contributions per tile, a power of two
+    auto cap_for = [&](long long contributions, int minimum) {
+      long long want = std::max<long long>(minimum, (3 * contributions + (long long)nt - 1) / (long long)nt);
+      int c = 1;
+      while (c < want && c < mc::kMaxBinCap) c <<= 1;
+      return c;
+    };
+    h.ib_cap = cap_for((long long)Mz, mc::kIbCap);
+    h.c_cap = cap_for(4LL * (long long)N, mc::kCicCap);
+    h.r_ibstore = lay.take((nt * h.ib_cap + 2 * Mz) * 4);
     h.r_ibtc = lay.take(nt * 4);
     h.r_ibovf = lay.take(Mz * 4);
     h.r_ibctl = lay.take(8 * 4);
@@ -791,7 +802,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.r_sfy = lay.take(Mz * 4);
     h.r_ccell = lay.take(4 * N * 4);
     h.r_cw = lay.take(4 * N * 4);
-    h.r_cstore = lay.take((nt * mc::kCicCap + 8 * N) * 4);
+    h.r_cstore = lay.take((nt * h.c_cap + 8 * N) * 4);
     h.r_ctc = lay.take(nt * 4);
     h.r_covf = lay.take(4 * N * 4);
     h.r_cctl = lay.take(8 * 4);
@@ -831,6 +842,10 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     p->r_wl_ib = lay.take((size_t)tiles * sizeof(int2));
     p->r_wl_cic = lay.take((size_t)tiles * sizeof(int2));
     p->tile_grid = (int)std::max(1LL, std::min(tiles, 148LL * 8));
+    for (auto& h : p->R) {
+      p->ib_capS = std::max(p->ib_capS, h.ib_cap);
+      p->c_capS = std::max(p->c_capS, h.c_cap);
+    }
   }
   p->ws_bytes = lay.cur;
   // CTA offset tables
@@ -943,6 +958,7 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
     if (p->node_smem > (size_t)optin || p->fftr_smem > (size_t)optin || p->fftc_smem > (size_t)optin)
       return fail(MC_ERR_UNSUPPORTED, "shared memory needed by the plan exceeds the device limit");
     MC_CUDA(mc::node_set_smem((size_t)optin));
+    MC_CUDA(mc::tiles_set_smem((size_t)optin));
     if (p->any_steric) MC_CUDA(mc::fft_set_smem((size_t)optin, (size_t)optin));
   }
   MC_CUDA(cudaMemsetAsync(p->ws + p->r_wl_ctl.off, 0, 4 * sizeof(int), s));
