@@ -684,8 +684,13 @@ __global__ void k_tick(int* tdev) { *tdev += 1; }
 void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity, int capS) {
   k_bin_tiles<<<L.grid, 256, (size_t)4 * capS * sizeof(unsigned), L.s>>>(L.d, wl, wl_count, which, parity, capS);
 }
+// `bytes` is the per-block opt-in limit; the kernel's static shared memory comes off it.
 cudaError_t tiles_set_smem(size_t bytes) {
-  return cudaFuncSetAttribute(k_bin_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, k_bin_tiles);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_bin_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(bytes - a.sharedSizeBytes));
 }
 void launch_ib_interp(const Launch& L, int it) { k_ib_interp<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
 void launch_ib_spread(const Launch& L, int it) { k_ib_spread<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
