@@ -45,6 +45,8 @@ struct RDesc {
   float sdt_x, sdt_y;       // scale * dt (float32)
   // FFT plans (steric filter)
   int fftW_nf, fftH_nf;
+  // power-of-two fast path: threads per transform, transforms per CTA, log2 of the length
+  int fft_T_r, fft_tpc_r, fft_logW, fft_T_c, fft_tpc_c, fft_logH;
   int fftW_f[kFftMaxFactors], fftH_f[kFftMaxFactors];
   const float2* twW;  // W roots exp(-2 pi i k / W)
   const float2* twH;
@@ -223,6 +225,9 @@ void launch_stream_out(const Launch& L, int parity);
 void launch_clear_ws(const Launch& L);
 void launch_tick(int* tdev, cudaStream_t s);
 cudaError_t fft_set_smem(size_t rows, size_t cols);
+void launch_fft_rows_p2(const Launch& L, size_t smem);
+void launch_fft_cols_p2(const Launch& L, size_t smem);
+cudaError_t fft_p2_set_smem(size_t bytes);
 void set_last_error(const char* msg);  // text returned by mc_last_error() on this thread
 cudaError_t node_set_smem(size_t bytes);
 

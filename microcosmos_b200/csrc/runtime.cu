@@ -37,7 +37,7 @@ mc_status cuda_fail(cudaError_t e, const char* where) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_COUNT };
+enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_FFTR2, K_FFTC2, K_COUNT };
 
 struct Region {
   size_t off = 0;
@@ -59,6 +59,8 @@ struct HostRollout {
   std::vector<float> gW, gH;
   int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4;
   int ib_cap = 0, c_cap = 0;  // bin capacities (powers of two)
+  int logW = -1, logH = -1;   // log2 of power-of-two grid sides (-1: mixed radix path)
+  int T_r = 0, P_r = 0, T_c = 0, P_c = 0;
   // workspace regions (offsets relative to the workspace base)
   Region r_h0, r_h1, r_fov, r_lflag, r_dep, r_tmp, r_prev, r_pred, r_predw, r_nvl, r_delta;
   Region r_ibcell, r_ibw, r_ibstore, r_ibtc, r_ibovf, r_ibctl, r_ibslot, r_hcell, r_hstart, r_hlen, r_srho, r_svx,
@@ -83,7 +85,7 @@ struct mc_plan {
   char* ws = nullptr;
   bool bound = false;
   int any_fluid = 0, any_steric = 0, max_iters = 0;
-  size_t node_smem = 0, fftr_smem = 0, fftc_smem = 0;
+  size_t node_smem = 0, fftr_smem = 0, fftc_smem = 0, fftr2_smem = 0, fftc2_smem = 0;
   int node_bs = 32;
   int max_chain = 0, chain_slots = 1;
   int max_k = 0;  // largest IB kernel size of the plan
@@ -350,6 +352,12 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.enable_fluid = c.enable_fluid ? 1 : 0;
   d.enable_steric = c.enable_steric ? 1 : 0;
   d.force_clamp = c.enable_force_clamp ? 1 : 0;
+  d.fft_T_r = h.T_r;
+  d.fft_tpc_r = h.P_r;
+  d.fft_logW = h.logW;
+  d.fft_T_c = h.T_c;
+  d.fft_tpc_c = h.P_c;
+  d.fft_logH = h.logH;
   d.fftW_nf = (int)h.fW.size();
   d.fftH_nf = (int)h.fH.size();
   for (size_t k = 0; k < h.fW.size(); ++k) d.fftW_f[k] = h.fW[k];
@@ -520,9 +528,23 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
       l.grid = p->tile_grid;
       mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_cic), at<int>(p->ws, p->r_wl_ctl) + 1, 1, 0, p->c_capS);
     });
-    timed(p, 2, s, capture, [&] { mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem); });
-    timed(p, 3, s, capture, [&] { mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem); });
-    k += 3;
+    k += 1;
+    if (p->grid[K_FFTR2]) {
+      timed(p, 2, s, capture, [&] { mc::launch_fft_rows_p2(L(p, K_FFTR2, s), p->fftr2_smem); });
+      ++k;
+    }
+    if (p->grid[K_FFTR]) {
+      timed(p, 2, s, capture, [&] { mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem); });
+      ++k;
+    }
+    if (p->grid[K_FFTC2]) {
+      timed(p, 3, s, capture, [&] { mc::launch_fft_cols_p2(L(p, K_FFTC2, s), p->fftc2_smem); });
+      ++k;
+    }
+    if (p->grid[K_FFTC]) {
+      timed(p, 3, s, capture, [&] { mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem); });
+      ++k;
+    }
   }
   if (p->grid[K_NODES]) {
     timed(p, 14, s, capture, [&] { mc::launch_steric(L(p, K_NODES, s)); });
@@ -754,6 +776,22 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       }
       fft_tables(D.W, c.steric_sigma, h.twW, h.gW);
       fft_tables(D.H, c.steric_sigma, h.twH, h.gH);
+      auto log2_if_pow2 = [](int v) {
+        int l = 0;
+        while ((1 << l) < v) ++l;
+        return (1 << l) == v && v >= 16 ? l : -1;
+      };
+      auto clampi = [](int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); };
+      h.logW = log2_if_pow2(D.W);
+      h.logH = log2_if_pow2(D.H);
+      if (h.logW >= 0) {
+        h.T_r = clampi(D.W / 8, 32, 256);
+        h.P_r = 256 / h.T_r;
+      }
+      if (h.logH >= 0) {
+        h.T_c = clampi(D.H / 8, 32, 512);
+        h.P_c = 512 / h.T_c;
+      }
     }
     h.vec = (D.W % 2 == 0) ? 2 : 1;
     if (vec_all == -1) vec_all = h.vec;
@@ -867,8 +905,14 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     cnt[K_TILES] = h.ntx * h.nty;
     cnt[K_LBM] = c.enable_fluid ? h.lbm_tx * h.lbm_ty : 0;
     cnt[K_CELLS] = std::min(div_up(HW, 256), 1024);
-    cnt[K_FFTR] = c.enable_steric ? div_up(h.dims.H, 2) : 0;
-    cnt[K_FFTC] = c.enable_steric ? div_up(h.dims.W, 2 * mc::kFftColsPerCta) : 0;
+    cnt[K_FFTR] = (c.enable_steric && h.logW < 0) ? div_up(h.dims.H, 2) : 0;
+    cnt[K_FFTC] = (c.enable_steric && h.logH < 0) ? div_up(h.dims.W, 2 * mc::kFftColsPerCta) : 0;
+    cnt[K_FFTR2] = (c.enable_steric && h.logW >= 0) ? div_up(div_up(h.dims.H, 2), h.P_r) : 0;
+    cnt[K_FFTC2] = (c.enable_steric && h.logH >= 0) ? div_up(h.dims.W, 2 * h.P_c) : 0;
+    if (c.enable_steric && h.logW >= 0)
+      p->fftr2_smem = std::max(p->fftr2_smem, (size_t)2 * h.P_r * h.dims.W * sizeof(float2));
+    if (c.enable_steric && h.logH >= 0)
+      p->fftc2_smem = std::max(p->fftc2_smem, (size_t)2 * h.P_c * (h.dims.H + 1) * sizeof(float2));
     for (int k = 0; k < K_COUNT; ++k) p->off[k][i + 1] = p->off[k][i] + cnt[k];
     if (!h.generic_comp.empty()) {
       mcn = std::max(mcn, h.max_cn);
@@ -955,11 +999,15 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
     int dev = 0, optin = 0;
     MC_CUDA(cudaGetDevice(&dev));
     MC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (p->node_smem > (size_t)optin || p->fftr_smem > (size_t)optin || p->fftc_smem > (size_t)optin)
+    if (p->node_smem > (size_t)optin || p->fftr_smem > (size_t)optin || p->fftc_smem > (size_t)optin ||
+        p->fftr2_smem > (size_t)optin || p->fftc2_smem + 1024 > (size_t)optin)
       return fail(MC_ERR_UNSUPPORTED, "shared memory needed by the plan exceeds the device limit");
     MC_CUDA(mc::node_set_smem((size_t)optin));
     MC_CUDA(mc::tiles_set_smem((size_t)optin));
-    if (p->any_steric) MC_CUDA(mc::fft_set_smem((size_t)optin, (size_t)optin));
+    if (p->any_steric) {
+      MC_CUDA(mc::fft_set_smem((size_t)optin, (size_t)optin));
+      MC_CUDA(mc::fft_p2_set_smem((size_t)optin));
+    }
   }
   MC_CUDA(cudaMemsetAsync(p->ws + p->r_wl_ctl.off, 0, 4 * sizeof(int), s));
   mc::launch_clear_ws(L(p, K_CELLS, s));

@@ -194,6 +194,156 @@ __global__ void __launch_bounds__(256) k_fft_cols(const RDesc* __restrict__ D, c
   }
 }
 
+// ---------------------------------------------------------------- power-of-two lengths
+// Radix-4 Stockham stages (and one radix-2 stage for odd log2 N) with shifts instead of
+// divisions; several transforms share a CTA, T threads each, all in lockstep.  The roots of
+// unity and the spectrum are read through the read-only data cache.
+__device__ float2* fft_pow2(float2* x, float2* y, int logN, const float2* __restrict__ tw, int lt, int T) {
+  const int N = 1 << logN;
+  const int Q = N >> 2;
+  int logNs = 0;
+  while (logNs + 2 <= logN) {
+    const int Ns = 1 << logNs;
+    const int sh = logN - logNs - 2;  // twiddle step N / (4 Ns) as a shift
+    for (int j = lt; j < Q; j += T) {
+      const int k = j & (Ns - 1);
+      float2 v0 = x[j], v1 = x[j + Q], v2 = x[j + 2 * Q], v3 = x[j + 3 * Q];
+      if (k > 0) {
+        v1 = cmul(v1, __ldg(tw + ((1 * k) << sh)));
+        v2 = cmul(v2, __ldg(tw + ((2 * k) << sh)));
+        v3 = cmul(v3, __ldg(tw + ((3 * k) << sh)));
+      }
+      const float2 a0 = make_float2(v0.x + v2.x, v0.y + v2.y);
+      const float2 a1 = make_float2(v0.x - v2.x, v0.y - v2.y);
+      const float2 b0 = make_float2(v1.x + v3.x, v1.y + v3.y);
+      const float2 b1 = make_float2(v1.x - v3.x, v1.y - v3.y);
+      const float2 b1m = make_float2(b1.y, -b1.x);  // b1 * (-i)
+      const int dst = ((j - k) << 2) + k;
+      y[dst] = make_float2(a0.x + b0.x, a0.y + b0.y);
+      y[dst + Ns] = make_float2(a1.x + b1m.x, a1.y + b1m.y);
+      y[dst + 2 * Ns] = make_float2(a0.x - b0.x, a0.y - b0.y);
+      y[dst + 3 * Ns] = make_float2(a1.x - b1m.x, a1.y - b1m.y);
+    }
+    __syncthreads();
+    float2* t = x;
+    x = y;
+    y = t;
+    logNs += 2;
+  }
+  if (logNs < logN) {
+    const int Ns = 1 << logNs;
+    const int H2 = N >> 1;
+    for (int j = lt; j < H2; j += T) {
+      const int k = j & (Ns - 1);
+      const float2 v0 = x[j];
+      float2 v1 = x[j + H2];
+      if (k > 0) v1 = cmul(v1, __ldg(tw + k));  // N / (2 Ns) = 1 on the last stage
+      const int dst = ((j - k) << 1) + k;
+      y[dst] = make_float2(v0.x + v1.x, v0.y + v1.y);
+      y[dst + Ns] = make_float2(v0.x - v1.x, v0.y - v1.y);
+    }
+    __syncthreads();
+    float2* t = x;
+    x = y;
+    y = t;
+  }
+  return x;
+}
+
+// x -> IFFT(G * FFT(x)) for one packed transform (1/N folded into G), as filter_packed.
+__device__ float2* filter_pow2(float2* a, float2* b, int logN, const float2* __restrict__ tw,
+                               const float* __restrict__ g, int lt, int T) {
+  const int N = 1 << logN;
+  float2* r = fft_pow2(a, b, logN, tw, lt, T);
+  float2* o = (r == a) ? b : a;
+  for (int i = lt; i < N; i += T) {
+    const float gk = __ldg(g + i);
+    const float2 v = r[i];
+    r[i] = make_float2(v.x * gk, -(v.y * gk));  // conj(G * X)
+  }
+  __syncthreads();
+  r = fft_pow2(r, o, logN, tw, lt, T);
+  for (int i = lt; i < N; i += T) r[i].y = -r[i].y;
+  __syncthreads();
+  return r;
+}
+
+// Row pass for power-of-two W: each CTA filters fft_tpc_r row pairs, fft_T_r threads each.
+__global__ void __launch_bounds__(256) k_fft_rows_p2(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+  extern __shared__ float2 sm[];
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int W = d.W, H = d.H, T = d.fft_T_r, P = d.fft_tpc_r, logW = d.fft_logW;
+  const int tr = threadIdx.x / T, lt = threadIdx.x - tr * T;  // P * T == blockDim.x
+  const int q = (blockIdx.x - off[r]) * P + tr;
+  const int y0 = 2 * q, y1 = 2 * q + 1;
+  float2* a = sm + (size_t)tr * W;
+  float2* b = sm + (size_t)(P + tr) * W;
+  const bool act0 = y0 < H, act1 = y1 < H;
+  const float* r0 = d.dep + (size_t)(act0 ? y0 : 0) * W;
+  const float* r1 = d.dep + (size_t)(act1 ? y1 : 0) * W;
+  for (int x = lt; x < W; x += T) a[x] = make_float2(act0 ? r0[x] : 0.0f, act1 ? r1[x] : 0.0f);
+  __syncthreads();
+  const float2* res = filter_pow2(a, b, logW, d.twW, d.gW, lt, T);
+  if (act0) {
+    float* o0 = d.tmp + (size_t)y0 * W;
+    for (int x = lt; x < W; x += T) o0[x] = res[x].x;
+  }
+  if (act1) {
+    float* o1 = d.tmp + (size_t)y1 * W;
+    for (int x = lt; x < W; x += T) o1[x] = res[x].y;
+  }
+}
+
+// Column pass for power-of-two H: each CTA filters fft_tpc_c column pairs (2 * fft_tpc_c
+// real columns), fft_T_c threads each; columns are stored with stride H + 1 so that the
+// transposing loads and stores hit distinct shared-memory banks.
+__global__ void __launch_bounds__(512) k_fft_cols_p2(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+  extern __shared__ float2 sm[];
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int W = d.W, H = d.H, T = d.fft_T_c, P = d.fft_tpc_c, logH = d.fft_logH;
+  const int S = H + 1;
+  const int xbase = (blockIdx.x - off[r]) * 2 * P;
+  float2* a = sm;
+  float2* b = sm + (size_t)P * S;
+  for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
+    const int y = idx / P, t = idx - y * P;  // consecutive threads read consecutive columns of a row
+    const int xr = xbase + 2 * t, xi = xr + 1;
+    const float* row = d.tmp + (size_t)y * W;
+    a[t * S + y] = make_float2(xr < W ? row[xr] : 0.0f, xi < W ? row[xi] : 0.0f);
+  }
+  __syncthreads();
+  const int tr = threadIdx.x / T, lt = threadIdx.x - tr * T;  // P * T == blockDim.x
+  const float2* res = filter_pow2(a + (size_t)tr * S, b + (size_t)tr * S, logH, d.twH, d.gH, lt, T);
+  // every transform of the CTA ends in the same buffer (same number of stages)
+  const float2* base = (res == a + (size_t)tr * S) ? a : b;
+  for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
+    const int y = idx / P, t = idx - y * P;
+    const int xr = xbase + 2 * t, xi = xr + 1;
+    float* row = d.steric + (size_t)y * W;
+    const float2 v = base[t * S + y];
+    if (xr < W) row[xr] = v.x;
+    if (xi < W) row[xi] = v.y;
+  }
+}
+
+void launch_fft_rows_p2(const Launch& L, size_t smem) {
+  k_fft_rows_p2<<<L.grid, 256, smem, L.s>>>(L.d, L.off, L.n);
+}
+void launch_fft_cols_p2(const Launch& L, size_t smem) {
+  k_fft_cols_p2<<<L.grid, 512, smem, L.s>>>(L.d, L.off, L.n);
+}
+cudaError_t fft_p2_set_smem(size_t bytes) {
+  cudaError_t e = cudaFuncSetAttribute(k_fft_rows_p2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return e;
+  cudaFuncAttributes a;
+  e = cudaFuncGetAttributes(&a, k_fft_cols_p2);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_fft_cols_p2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(bytes - a.sharedSizeBytes));
+}
+
 void launch_fft_rows(const Launch& L, size_t smem) {
   k_fft_rows<<<L.grid, 256, smem, L.s>>>(L.d, L.off, L.n);
 }
