@@ -227,8 +227,15 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
       }
     }
     __syncthreads();
-    if (which == 0)
-      for (int i = tid; i < total; i += blockDim.x) bin[i] = kout[i];
+    if (which == 0) {
+      // runs for the spread: contributing node and weight, contiguous per touched cell
+      const int K2 = d.K * d.K;
+      float* binw = d.ib_store_w + (size_t)t * v.cap;
+      for (int i = tid; i < total; i += blockDim.x) {
+        bin[i] = kout[i] / K2;
+        binw[i] = wout[i];
+      }
+    }
     if (tid == 0) v.tcount[t] = 0;
     return;
   }
@@ -302,6 +309,14 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
     head_work(d, v, which, parity, kv + i, len, kv_pos + i);
   }
   __syncthreads();
+  if (which == 0) {
+    const int K2 = d.K * d.K;
+    for (int i = tid; i < m; i += blockDim.x) {
+      const int k = kv[i];
+      d.ib_store_w[kv_pos + i] = v.w[k];
+      kv[i] = k / K2;
+    }
+  }
   if (tid == 0) v.tcount[t] = 0;
 }
 
@@ -406,22 +421,23 @@ __global__ void __launch_bounds__(256) k_ib_spread(const RDesc* __restrict__ D, 
   const int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
   if (it >= d.ib_iters || p >= d.ib_ctl[2]) return;
   const int len = d.h_len[p];
-  const int* run = d.ib_store + d.h_start[p];
-  const int K2 = d.K * d.K;
+  const int* rn = d.ib_store + d.h_start[p];      // contributing nodes, in k order
+  const float* rw = d.ib_store_w + d.h_start[p];  // their weights
   float dx = 0.0f, dy = 0.0f;
   int j = 0;
   // runs are short: fetch up to 8 entries at a time so their loads overlap
   for (; j + 8 <= len; j += 8) {
-    int k[8];
+    int nd[8];
     float w[8], ex[8], ey[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) k[q] = run[j + q];
+    for (int q = 0; q < 8; ++q) {
+      nd[q] = rn[j + q];
+      w[q] = rw[j + q];
+    }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const int node = k[q] / K2;
-      w[q] = d.ib_w[k[q]];
-      ex[q] = d.delta[2 * node];
-      ey[q] = d.delta[2 * node + 1];
+      ex[q] = d.delta[2 * nd[q]];
+      ey[q] = d.delta[2 * nd[q] + 1];
     }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -430,9 +446,8 @@ __global__ void __launch_bounds__(256) k_ib_spread(const RDesc* __restrict__ D, 
     }
   }
   for (; j < len; ++j) {
-    const int k = run[j];
-    const int node = k / K2;
-    const float w = d.ib_w[k];
+    const int node = rn[j];
+    const float w = rw[j];
     dx = dx + d.delta[2 * node] * w;
     dy = dy + d.delta[2 * node + 1] * w;
   }
@@ -526,20 +541,22 @@ __global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, co
     rollout_barrier(d.ib_ctl, nb, d.flags);
     for (int p = t0; p < nheads; p += stride) {
       const int len = d.h_len[p];
-      const int* run = d.ib_store + d.h_start[p];
+      const int* rn = d.ib_store + d.h_start[p];
+      const float* rw = d.ib_store_w + d.h_start[p];
       float dx = 0.0f, dy = 0.0f;
       int j = 0;
       for (; j + 8 <= len; j += 8) {
-        int k[8];
+        int nd[8];
         float w[8], ex[8], ey[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) k[q] = run[j + q];
+        for (int q = 0; q < 8; ++q) {
+          nd[q] = rn[j + q];
+          w[q] = rw[j + q];
+        }
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const int node = k[q] / K2;
-          w[q] = d.ib_w[k[q]];
-          ex[q] = __ldcg(d.delta + 2 * node);
-          ey[q] = __ldcg(d.delta + 2 * node + 1);
+          ex[q] = __ldcg(d.delta + 2 * nd[q]);
+          ey[q] = __ldcg(d.delta + 2 * nd[q] + 1);
         }
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
@@ -548,9 +565,8 @@ __global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, co
         }
       }
       for (; j < len; ++j) {
-        const int k = run[j];
-        const int node = k / K2;
-        const float w = d.ib_w[k];
+        const int node = rn[j];
+        const float w = rw[j];
         dx = dx + __ldcg(d.delta + 2 * node) * w;
         dy = dy + __ldcg(d.delta + 2 * node + 1) * w;
       }

@@ -105,7 +105,8 @@ struct RDesc {
   int ib_cap;
   int* ib_cell;     // (M) cell of contribution k = n*K*K + s
   float* ib_w;      // (M) normalised stencil weight
-  int* ib_store;    // (ntiles * ib_cap + 2 * M)
+  int* ib_store;    // (ntiles * ib_cap + 2 * M); after the tile sort: contributing node per run entry
+  float* ib_store_w;  // same indexing: the run entry's weight
   int* ib_tcount;   // (ntiles)
   int* ib_ovf;      // (M)
   int* ib_ctl;      // (4)

@@ -63,7 +63,7 @@ struct HostRollout {
   int T_r = 0, P_r = 0, T_c = 0, P_c = 0;
   // workspace regions (offsets relative to the workspace base)
   Region r_h0, r_h1, r_fov, r_lflag, r_dep, r_tmp, r_prev, r_pred, r_predw, r_nvl, r_delta;
-  Region r_ibcell, r_ibw, r_ibstore, r_ibtc, r_ibovf, r_ibctl, r_ibslot, r_hcell, r_hstart, r_hlen, r_srho, r_svx,
+  Region r_ibcell, r_ibw, r_ibstore, r_ibstorew, r_ibtc, r_ibovf, r_ibctl, r_ibslot, r_hcell, r_hstart, r_hlen, r_srho, r_svx,
       r_svy, r_sinv, r_sucx, r_sucy, r_sfx, r_sfy;
   Region r_ccell, r_cw, r_cstore, r_ctc, r_covf, r_cctl, r_chain, r_generic;
   Region r_pairs, r_bpairs, r_compn, r_compe, r_compb, r_epo, r_epi, r_neo, r_nei, r_edeg, r_ndeg;
@@ -428,6 +428,7 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.ib_cell = at<int>(b, h.r_ibcell);
   d.ib_w = at<float>(b, h.r_ibw);
   d.ib_store = at<int>(b, h.r_ibstore);
+  d.ib_store_w = at<float>(b, h.r_ibstorew);
   d.ib_tcount = at<int>(b, h.r_ibtc);
   d.ib_ovf = at<int>(b, h.r_ibovf);
   d.ib_ctl = at<int>(b, h.r_ibctl);
@@ -823,6 +824,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.ib_cap = cap_for((long long)Mz, mc::kIbCap);
     h.c_cap = cap_for(4LL * (long long)N, mc::kCicCap);
     h.r_ibstore = lay.take((nt * h.ib_cap + 2 * Mz) * 4);
+    h.r_ibstorew = lay.take((nt * h.ib_cap + 2 * Mz) * 4);
     h.r_ibtc = lay.take(nt * 4);
     h.r_ibovf = lay.take(Mz * 4);
     h.r_ibctl = lay.take(8 * 4);
