@@ -771,9 +771,9 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       return st;
     }
     if (c.enable_steric) {
-      if (!factorize(D.W, h.fW) || !factorize(D.H, h.fH) || D.W > mc::kFftMaxN || D.H > 2048) {
+      if (!factorize(D.W, h.fW) || !factorize(D.H, h.fH) || D.W > mc::kFftMaxN || D.H > mc::kFftMaxN) {
         delete p;
-        return fail(MC_ERR_UNSUPPORTED, "steric FFT needs H, W with prime factors <= 13, W <= 4096, H <= 2048");
+        return fail(MC_ERR_UNSUPPORTED, "steric FFT needs H, W with prime factors <= 13 and at most 4096");
       }
       fft_tables(D.W, c.steric_sigma, h.twW, h.gW);
       fft_tables(D.H, c.steric_sigma, h.twH, h.gH);
@@ -782,17 +782,19 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
         while ((1 << l) < v) ++l;
         return (1 << l) == v && v >= 16 ? l : -1;
       };
-      auto clampi = [](int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); };
+      // threads per transform: one radix-4 butterfly each (N / 4), a power of two dividing the
+      // CTA size; transforms per CTA fill the CTA (256 threads for rows, 512 for columns)
+      auto threads_for = [](int len, int cta) {
+        int t = 32;
+        while (t * 2 <= len / 4 && t * 2 <= cta) t *= 2;
+        return t;
+      };
       h.logW = log2_if_pow2(D.W);
       h.logH = log2_if_pow2(D.H);
-      if (h.logW >= 0) {
-        h.T_r = clampi(D.W / 8, 32, 256);
-        h.P_r = 256 / h.T_r;
-      }
-      if (h.logH >= 0) {
-        h.T_c = clampi(D.H / 8, 32, 512);
-        h.P_c = 512 / h.T_c;
-      }
+      h.T_r = threads_for(D.W, 256);
+      h.P_r = 256 / h.T_r;
+      h.T_c = threads_for(D.H, 512);
+      h.P_c = 512 / h.T_c;
     }
     h.vec = (D.W % 2 == 0) ? 2 : 1;
     if (vec_all == -1) vec_all = h.vec;
@@ -907,14 +909,16 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     cnt[K_TILES] = h.ntx * h.nty;
     cnt[K_LBM] = c.enable_fluid ? h.lbm_tx * h.lbm_ty : 0;
     cnt[K_CELLS] = std::min(div_up(HW, 256), 1024);
-    cnt[K_FFTR] = (c.enable_steric && h.logW < 0) ? div_up(h.dims.H, 2) : 0;
-    cnt[K_FFTC] = (c.enable_steric && h.logH < 0) ? div_up(h.dims.W, 2 * mc::kFftColsPerCta) : 0;
-    cnt[K_FFTR2] = (c.enable_steric && h.logW >= 0) ? div_up(div_up(h.dims.H, 2), h.P_r) : 0;
-    cnt[K_FFTC2] = (c.enable_steric && h.logH >= 0) ? div_up(h.dims.W, 2 * h.P_c) : 0;
-    if (c.enable_steric && h.logW >= 0)
+    // every length goes through the multi-transform kernels (the one-transform-per-CTA
+    // kernels serve the allocation-free entry point)
+    cnt[K_FFTR] = 0;
+    cnt[K_FFTC] = 0;
+    cnt[K_FFTR2] = c.enable_steric ? div_up(div_up(h.dims.H, 2), h.P_r) : 0;
+    cnt[K_FFTC2] = c.enable_steric ? div_up(h.dims.W, 2 * h.P_c) : 0;
+    if (c.enable_steric) {
       p->fftr2_smem = std::max(p->fftr2_smem, (size_t)2 * h.P_r * h.dims.W * sizeof(float2));
-    if (c.enable_steric && h.logH >= 0)
       p->fftc2_smem = std::max(p->fftc2_smem, (size_t)2 * h.P_c * (h.dims.H + 1) * sizeof(float2));
+    }
     for (int k = 0; k < K_COUNT; ++k) p->off[k][i + 1] = p->off[k][i] + cnt[k];
     if (!h.generic_comp.empty()) {
       mcn = std::max(mcn, h.max_cn);

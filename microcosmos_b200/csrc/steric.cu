@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) k_fft_cols(const RDesc* __restrict__ D, c
   }
 }
 
-// ---------------------------------------------------------------- power-of-two lengths
+// ---------------------------------------------------------------- several transforms per CTA
 // Radix-4 Stockham stages (and one radix-2 stage for odd log2 N) with shifts instead of
 // divisions; several transforms share a CTA, T threads each, all in lockstep.  The roots of
 // unity and the spectrum are read through the read-only data cache.
@@ -250,11 +250,95 @@ __device__ float2* fft_pow2(float2* x, float2* y, int logN, const float2* __rest
   return x;
 }
 
+// One mixed-radix Stockham stage for one transform, T threads with local index lt.
+template <int R>
+__device__ __forceinline__ void stage_t(const float2* __restrict__ x, float2* __restrict__ y, int N, int Ns,
+                                        const float2* __restrict__ tw, int lt, int T) {
+  const int S = N / R;
+  const int twstep = N / (Ns * R);
+  const int rstep = N / R;
+  for (int j = lt; j < S; j += T) {
+    const int k = j % Ns;
+    const int dst = (j - k) * R + k;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      float2 a = x[j + r * S];
+      if (r > 0 && k > 0) a = cmul(a, __ldg(tw + r * k * twstep));
+      v[r] = a;
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      float2 acc = v[0];
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const float2 p = cmul(v[r], __ldg(tw + ((r * q) % R) * rstep));
+        acc.x = acc.x + p.x;
+        acc.y = acc.y + p.y;
+      }
+      y[dst + q * Ns] = acc;
+    }
+  }
+}
+
+__device__ __noinline__ void stage_t_generic(const float2* __restrict__ x, float2* __restrict__ y, int N, int R,
+                                             int Ns, const float2* __restrict__ tw, int lt, int T) {
+  const int S = N / R;
+  const int twstep = N / (Ns * R);
+  const int rstep = N / R;
+  for (int j = lt; j < S; j += T) {
+    const int k = j % Ns;
+    const int dst = (j - k) * R + k;
+    float2 v[13];
+#pragma unroll 1
+    for (int r = 0; r < R; ++r) {
+      float2 a = x[j + r * S];
+      if (r > 0 && k > 0) a = cmul(a, __ldg(tw + r * k * twstep));
+      v[r] = a;
+    }
+#pragma unroll 1
+    for (int q = 0; q < R; ++q) {
+      float2 acc = v[0];
+#pragma unroll 1
+      for (int r = 1; r < R; ++r) {
+        const float2 p = cmul(v[r], __ldg(tw + ((r * q) % R) * rstep));
+        acc.x = acc.x + p.x;
+        acc.y = acc.y + p.y;
+      }
+      y[dst + q * Ns] = acc;
+    }
+  }
+}
+
+// Forward transform of one length-N sequence (prime factors <= 13): radix-4 stages with
+// shifts when N is a power of two, else the factor list (4s, 2, 3, 5, 7, 11, 13), the
+// stage sequence of fft_forward.
+__device__ float2* fft_any(float2* x, float2* y, int N, int logN, const int* fac, int nf,
+                           const float2* __restrict__ tw, int lt, int T) {
+  if (logN >= 0) return fft_pow2(x, y, logN, tw, lt, T);
+  int Ns = 1;
+  for (int s = 0; s < nf; ++s) {
+    const int R = fac[s];
+    switch (R) {
+      case 4: stage_t<4>(x, y, N, Ns, tw, lt, T); break;
+      case 2: stage_t<2>(x, y, N, Ns, tw, lt, T); break;
+      case 3: stage_t<3>(x, y, N, Ns, tw, lt, T); break;
+      case 5: stage_t<5>(x, y, N, Ns, tw, lt, T); break;
+      default: stage_t_generic(x, y, N, R, Ns, tw, lt, T); break;
+    }
+    __syncthreads();
+    float2* t = x;
+    x = y;
+    y = t;
+    Ns *= R;
+  }
+  return x;
+}
+
 // x -> IFFT(G * FFT(x)) for one packed transform (1/N folded into G), as filter_packed.
-__device__ float2* filter_pow2(float2* a, float2* b, int logN, const float2* __restrict__ tw,
-                               const float* __restrict__ g, int lt, int T) {
-  const int N = 1 << logN;
-  float2* r = fft_pow2(a, b, logN, tw, lt, T);
+__device__ float2* filter_any(float2* a, float2* b, int N, int logN, const int* fac, int nf,
+                              const float2* __restrict__ tw, const float* __restrict__ g, int lt, int T) {
+  float2* r = fft_any(a, b, N, logN, fac, nf, tw, lt, T);
   float2* o = (r == a) ? b : a;
   for (int i = lt; i < N; i += T) {
     const float gk = __ldg(g + i);
@@ -262,13 +346,13 @@ __device__ float2* filter_pow2(float2* a, float2* b, int logN, const float2* __r
     r[i] = make_float2(v.x * gk, -(v.y * gk));  // conj(G * X)
   }
   __syncthreads();
-  r = fft_pow2(r, o, logN, tw, lt, T);
+  r = fft_any(r, o, N, logN, fac, nf, tw, lt, T);
   for (int i = lt; i < N; i += T) r[i].y = -r[i].y;
   __syncthreads();
   return r;
 }
 
-// Row pass for power-of-two W: each CTA filters fft_tpc_r row pairs, fft_T_r threads each.
+// Row pass: each CTA filters fft_tpc_r row pairs, fft_T_r threads each.
 __global__ void __launch_bounds__(256) k_fft_rows_p2(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
   extern __shared__ float2 sm[];
   const int r = find_rollout(off, n, blockIdx.x);
@@ -284,7 +368,7 @@ __global__ void __launch_bounds__(256) k_fft_rows_p2(const RDesc* __restrict__ D
   const float* r1 = d.dep + (size_t)(act1 ? y1 : 0) * W;
   for (int x = lt; x < W; x += T) a[x] = make_float2(act0 ? r0[x] : 0.0f, act1 ? r1[x] : 0.0f);
   __syncthreads();
-  const float2* res = filter_pow2(a, b, logW, d.twW, d.gW, lt, T);
+  const float2* res = filter_any(a, b, W, logW, d.fftW_f, d.fftW_nf, d.twW, d.gW, lt, T);
   if (act0) {
     float* o0 = d.tmp + (size_t)y0 * W;
     for (int x = lt; x < W; x += T) o0[x] = res[x].x;
@@ -295,7 +379,7 @@ __global__ void __launch_bounds__(256) k_fft_rows_p2(const RDesc* __restrict__ D
   }
 }
 
-// Column pass for power-of-two H: each CTA filters fft_tpc_c column pairs (2 * fft_tpc_c
+// Column pass: each CTA filters fft_tpc_c column pairs (2 * fft_tpc_c
 // real columns), fft_T_c threads each; columns are stored with stride H + 1 so that the
 // transposing loads and stores hit distinct shared-memory banks.
 __global__ void __launch_bounds__(512) k_fft_cols_p2(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
@@ -315,7 +399,8 @@ __global__ void __launch_bounds__(512) k_fft_cols_p2(const RDesc* __restrict__ D
   }
   __syncthreads();
   const int tr = threadIdx.x / T, lt = threadIdx.x - tr * T;  // P * T == blockDim.x
-  const float2* res = filter_pow2(a + (size_t)tr * S, b + (size_t)tr * S, logH, d.twH, d.gH, lt, T);
+  const float2* res = filter_any(a + (size_t)tr * S, b + (size_t)tr * S, H, logH, d.fftH_f, d.fftH_nf, d.twH, d.gH,
+                                 lt, T);
   // every transform of the CTA ends in the same buffer (same number of stages)
   const float2* base = (res == a + (size_t)tr * S) ? a : b;
   for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
