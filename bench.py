@@ -31,6 +31,9 @@ import time
 
 import numpy as np
 
+# more hardware work queues, so that the served rollouts' streams overlap (set before CUDA starts)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
@@ -50,6 +53,10 @@ def parse():
     ap.add_argument("--batch-rollouts", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=96)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-plain-sample", type=int, default=12)
+    ap.add_argument("--no-serve", action="store_true")
     return ap.parse_args()
 
 
@@ -237,6 +244,54 @@ def batch_section(args, flush):
         "l2": "flushed (256 MiB write) before every timed step"}
 
 
+def serve_section(args):
+    """Serving configuration: a seeded Poisson stream (mean ``--serve-rate`` requests/s) of
+    rollouts with grid side ~U{64..1024} step 64, filaments ~U{1..128}, nodes/filament
+    ~U{16..128}, steps ~U{500..5000}, 20% marked as asking for gradients, served by the
+    continuous-batching server (admission by a 180 GB budget, up to 64 rollouts in flight,
+    100-step graph-replayed chunks, one stream per rollout).  Latency = completion minus
+    arrival, wall clock.  The plain path runs a sample of the same requests one after
+    another, one plan each."""
+    import torch
+    from microcosmos_b200 import baseline_config, serve
+    cfg = baseline_config()
+    reqs = serve.poisson_requests(args.serve_requests, args.serve_rate, seed=0)
+    be = serve.CudaBackend(cfg, dt=0.01)
+    # warm the allocator and the module (one tiny request); not part of the measurement
+    serve.run_plain(be, serve.poisson_requests(1, 1.0, seed=99, sides=(64,), filaments=(1, 1), nodes=(16, 16),
+                                               steps=(8, 8)))
+    torch.cuda.synchronize()
+    srv = serve.Server(be, hbm_budget_bytes=180e9, max_active=64, chunk=100, keep_state=False)
+    t0 = time.perf_counter()
+    res = srv.run(reqs, realtime=True)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    summ = serve.summarize(res, wall)
+    k = min(args.serve_plain_sample, len(reqs))
+    sample = reqs[:k]
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    serve.run_plain(be, sample)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t1
+    cs_sample = sum(r.scenario.H * r.scenario.W * r.steps for r in sample)
+    cs_all = sum(r.scenario.H * r.scenario.W * r.steps for r in reqs)
+    plain_mlups = cs_sample / t_plain / 1e6
+    # plain rollouts/s for this request mix: the sample's cell-steps rate applied to the whole stream
+    plain_rps = len(reqs) / (cs_all / (plain_mlups * 1e6))
+    return dict(summ, workload=f"{len(reqs)} Poisson requests at {args.serve_rate:g}/s (side U{{64..1024}} step 64, "
+                                f"1-128 filaments x 16-128 nodes, 500-5000 steps); {cs_all} cell-steps",
+                grad_requests=int(sum(r.want_grad for r in reqs)),
+                grad_note="gradient requests are served as forward rollouts",
+                flags_nonzero=int(sum(1 for r in res if r.flags)),
+                peak_active=srv.peak_active, peak_bytes=srv.peak_bytes,
+                plain_mlups=plain_mlups, plain_rollouts_per_s=plain_rps,
+                plain_sample=f"first {k} requests, one plan each, sequential ({t_plain:.2f} s)",
+                speedup_vs_plain=summ["mlups"] / plain_mlups,
+                roofline_frac_mlups=summ["mlups"] / (6541.5e9 / BYTES_PER_CELL / 1e6),
+                timing="wall clock from the first arrival to the last completion")
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -401,6 +456,9 @@ def main():
     batch = None
     if ws == 1 and not args.no_batch:
         batch = batch_section(args, flush)
+    served = None
+    if ws == 1 and not args.no_serve:
+        served = serve_section(args)
 
     if rank == 0:
         value = cells * K * ws / (t_ms / 1e3) / 1e6
@@ -426,6 +484,7 @@ def main():
             "kernels": per_step,
             "flags": flags,
             "batch": batch,
+            "serve": served,
             "step_kernel_ms": step_kernel_ms / P,
         }
         print(json.dumps(out))

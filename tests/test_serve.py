@@ -1,0 +1,144 @@
+"""The continuous-batching server: admission and ordering on CPU with a fake backend, and
+on the GPU that every rollout's result is the same alone and in the mix."""
+import numpy as np
+import pytest
+
+from microcosmos_b200 import serve
+
+
+class FakeBackend:
+    """Chunks complete a fixed number of polls after they are issued; memory = cells."""
+
+    def __init__(self, polls_per_chunk=2):
+        self.polls = polls_per_chunk
+        self.live = set()
+        self.log = []
+
+    def bytes_needed(self, r):
+        return r.scenario.H * r.scenario.W
+
+    def start(self, r):
+        self.live.add(r.rid)
+        self.log.append(("start", r.rid))
+        return {"rid": r.rid, "q": [], "steps": 0, "last": False}
+
+    def advance(self, h, n, last):
+        h["q"].append(self.polls)
+        h["steps"] += n
+        h["last"] = last
+
+    def inflight(self, h):
+        h["q"] = [p - 1 for p in h["q"] if p - 1 > 0]
+        return len(h["q"])
+
+    def finish(self, h):
+        assert h["last"] or h["steps"] == 0
+        self.live.discard(h["rid"])
+        self.log.append(("finish", h["rid"]))
+        return {"steps": h["steps"]}, 0
+
+
+class _Sc:
+    def __init__(self, side):
+        self.H = self.W = side
+
+
+class ManualClock:
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        self.t += 1e-4
+        return self.t
+
+    def sleep(self, s):
+        self.t += max(s, 1e-4)
+
+
+def _reqs(sides, steps, arrivals=None):
+    arrivals = arrivals or [0.0] * len(sides)
+    return [serve.Request(rid=i, arrival=a, scenario=_Sc(s), steps=n)
+            for i, (s, n, a) in enumerate(zip(sides, steps, arrivals))]
+
+
+def test_every_request_completes_with_its_step_count():
+    be = FakeBackend()
+    reqs = _reqs([8, 16, 32, 8, 64], [0, 5, 250, 99, 100])
+    clock = ManualClock()
+    res = serve.Server(be, hbm_budget_bytes=1e9, chunk=40, clock=clock, sleep=clock.sleep).run(reqs)
+    assert [r.rid for r in res] == [0, 1, 2, 3, 4]
+    assert [r.state["steps"] for r in res] == [0, 5, 250, 99, 100]
+    assert not be.live
+
+
+def test_budget_and_slots_are_never_exceeded():
+    sides = [30, 20, 10, 30, 25, 5, 40, 12]
+    budget = 2000
+
+    class Checking(FakeBackend):
+        def start(self, r):
+            h = super().start(r)
+            live_bytes = sum(s * s for i, s in enumerate(sides) if i in self.live)
+            assert live_bytes <= budget
+            assert len(self.live) <= 3
+            return h
+
+    be = Checking()
+    clock = ManualClock()
+    srv = serve.Server(be, hbm_budget_bytes=budget, max_active=3, chunk=7, clock=clock, sleep=clock.sleep)
+    res = srv.run(_reqs(sides, [20] * len(sides)))
+    assert len(res) == len(sides)
+    assert srv.peak_bytes <= budget and srv.peak_active <= 3
+
+
+def test_admission_follows_arrival_and_overlaps_running_work():
+    be = FakeBackend(polls_per_chunk=50)
+    clock = ManualClock()
+    reqs = _reqs([8, 8, 8], [400, 400, 400], arrivals=[0.0, 0.001, 0.002])
+    res = serve.Server(be, hbm_budget_bytes=1e6, chunk=100, clock=clock, sleep=clock.sleep).run(reqs)
+    starts = [rid for kind, rid in be.log if kind == "start"]
+    assert starts == [0, 1, 2]
+    # the later requests were admitted while the first was still running
+    assert be.log.index(("start", 2)) < be.log.index(("finish", 0))
+    assert all(r.admitted >= r.arrival for r in res)
+
+
+def test_request_larger_than_budget_is_rejected():
+    with pytest.raises(ValueError, match="budget"):
+        serve.Server(FakeBackend(), hbm_budget_bytes=100).run(_reqs([11], [10]))
+
+
+def test_summary_percentiles():
+    res = [serve.Result(rid=i, arrival=0.0, admitted=0.0, done=float(i + 1), steps=10, cells=100) for i in range(100)]
+    s = serve.summarize(res, wall_s=10.0)
+    assert s["requests"] == 100 and s["rollouts_per_s"] == 10.0
+    assert abs(s["p50_latency_s"] - 50.5) < 1e-9 and s["p99_latency_s"] > 99.0
+    assert s["mlups"] == 100 * 100 * 10 / 10.0 / 1e6
+
+
+def test_poisson_stream_is_seeded_and_in_range():
+    a = serve.poisson_requests(12, 200.0, seed=3, filaments=(1, 4), nodes=(16, 24))
+    b = serve.poisson_requests(12, 200.0, seed=3, filaments=(1, 4), nodes=(16, 24))
+    assert [r.arrival for r in a] == [r.arrival for r in b]
+    assert all(np.array_equal(x.scenario.position, y.scenario.position) for x, y in zip(a, b))
+    assert all(64 <= r.scenario.H <= 1024 and r.scenario.H % 64 == 0 for r in a)
+    assert all(500 <= r.steps <= 5000 for r in a)
+    assert np.all(np.diff([r.arrival for r in a]) > 0)
+
+
+@pytest.mark.gpu
+def test_results_identical_alone_and_in_the_mix():
+    torch = pytest.importorskip("torch")
+    from microcosmos_b200 import baseline_config
+    cfg = baseline_config()
+    reqs = serve.poisson_requests(8, 2000.0, seed=11, sides=(64, 128, 192), filaments=(1, 6), nodes=(16, 40),
+                                  steps=(30, 160))
+    be = serve.CudaBackend(cfg, dt=0.01)
+    mixed = serve.Server(be, hbm_budget_bytes=4e9, max_active=8, chunk=16).run(reqs)
+    alone = serve.run_plain(be, reqs)
+    torch.cuda.synchronize()
+    assert len(mixed) == len(reqs)
+    for r, (rid, state, flags) in zip(mixed, alone):
+        assert r.rid == rid and r.flags == 0 and flags == 0
+        for k in ("position", "velocity", "f_grid", "steric", "fluid_velocity"):
+            assert np.array_equal(r.state[k], state[k]), (rid, k)
