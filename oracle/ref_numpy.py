@@ -398,12 +398,17 @@ class IBResult:
     vel_before: np.ndarray
 
 
-def ib_lbm(H, W, grid_shape, pos, vel, f_grid, cfg, dtstep):
+def ib_lbm(H, W, grid_shape, pos, vel, f_grid, cfg, dtstep, ib_positions=None):
     """immersed_boundary_interaction (src/microcosmos/solver/fluid.py:202-386) for
     synthetic_node_width = 0: macroscopic + clamp, multi-direct forcing
     (ibm_iterations x interpolate/clamp/spread), post clamp, F = (u_corr - u) rho,
     TRT+Guo collide, stream, node reaction.  ``grid_shape`` is the domain grid; the
-    scale keeps the reference's axis order scale = (w / grid_shape[0], h / grid_shape[1])."""
+    scale keeps the reference's axis order scale = (w / grid_shape[0], h / grid_shape[1]).
+
+    ``ib_positions`` (default: ``pos``) are the positions the Peskin stencils are built
+    from.  The reference wraps them in ``jax.lax.stop_gradient`` (fluid.py:239), so a
+    finite-difference check of its gradients holds them at the unperturbed trajectory's
+    values."""
     dt = f_grid.dtype
     t = dt.type
     h, w = f_grid.shape[1], f_grid.shape[2]
@@ -412,7 +417,7 @@ def ib_lbm(H, W, grid_shape, pos, vel, f_grid, cfg, dtstep):
     vmax = cfg.max_fluid_velocity * mean_scale
     eps = t(EPSIL32)
     node_vel = vel * scale * t(dtstep)
-    gpos = pos * scale
+    gpos = (pos if ib_positions is None else ib_positions) * scale
     if cfg.synthetic_node_width > 0.0:
         raise NotImplementedError("synthetic_node_width > 0 is not part of this oracle")
     f = np.maximum(f_grid, eps)
@@ -481,10 +486,10 @@ def ib_lbm(H, W, grid_shape, pos, vel, f_grid, cfg, dtstep):
 
 
 # ----------------------------------------------------------------------------- step / simulate
-def step(s: State, cfg: Config, dtstep: float, rest_angles=None):
+def step(s: State, cfg: Config, dtstep: float, rest_angles=None, ib_positions=None):
     """One simulate.step (src/microcosmos/simulate.py:37-100) for the PBD solver.
     ``rest_angles`` overrides edges.bending_rest_angles for this step (the caller-side
-    curvature actuation)."""
+    curvature actuation); ``ib_positions`` see ``ib_lbm``."""
     dt = s.position.dtype
     t = dt.type
     H, W = s.H, s.W
@@ -504,7 +509,7 @@ def step(s: State, cfg: Config, dtstep: float, rest_angles=None):
                                    s.bending_rest_angles, s.bending_stiffness, cfg)
     vel = (pos - prev) / t(dtstep)
     if cfg.enable_fluid:
-        r = ib_lbm(H, W, (H, W), pos, vel, s.f_grid, cfg, dtstep)
+        r = ib_lbm(H, W, (H, W), pos, vel, s.f_grid, cfg, dtstep, ib_positions)
         vel = r.velocity
         s.f_grid = r.f_grid
         s.fluid_velocity = r.fluid_velocity
