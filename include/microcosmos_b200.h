@@ -200,6 +200,58 @@ const char* mc_profile_kernel_names(void);
 mc_status mc_steric_potential_noalloc(const float* position, int32_t N, int32_t H, int32_t W, float sigma,
                                       float scatter_value, float* steric_out, void* stream);
 
+/* ------------------------------------------------------------------ gradients
+ * Reverse-mode derivative of a rollout of ONE instance, with the derivative conventions
+ * jax.grad applies to the reference's simulate() (src/microcosmos/simulate.py:15-35):
+ * the IB stencil positions are stop_gradient-ed (src/microcosmos/solver/fluid.py:239),
+ * floor has derivative 0, mod derivative 1, max/min split ties evenly.  It replaces the
+ * jax.grad / jax.value_and_grad calls on simulate() in the reference's
+ * tests/test_differentiability.py:45,65 (there through XLA's autodiff; here through
+ * hand-written adjoint kernels of stream+collide, IB, PBD and steric).
+ *
+ * mc_grad_forward runs the rollout with the same kernels as mc_rollout, keeping a
+ * checkpoint of (position, velocity, theta, f_grid) every `checkpoint_every` steps
+ * (<= 0: ceil(sqrt(num_steps))).  mc_grad_backward recomputes each segment's step inputs
+ * from its checkpoint and runs the adjoint steps in reverse: device memory is
+ * O(sqrt(T)) states, compute about three forward rollouts plus the adjoint.
+ * Cotangents of the outputs steric and fluid_velocity are taken as zero.
+ * Actuation, if given to mc_grad_forward, must have t0 = 0; its omega is not
+ * differentiated.  enable_force_clamp != 0 is not supported. */
+typedef struct mc_state_cot {
+  float* position; /* (N,2) */
+  float* velocity; /* (N,2) */
+  float* theta;    /* (E,)  */
+  float* f_grid;   /* (9,H,W) */
+} mc_state_cot;
+
+/* Gradient outputs, any may be NULL.  rest_angles: the static bending_rest_angles (used
+ * when mc_grad_forward had no actuation); act_c/act_amp/act_phase: the actuation arrays. */
+typedef struct mc_param_grads {
+  float* rest_angles;       /* (B,) */
+  float* act_c;             /* (B,) */
+  float* act_amp;           /* (B,) */
+  float* act_phase;         /* (B,) */
+  float* rest_lengths;      /* (E,) */
+  float* bending_stiffness; /* (B,) */
+} mc_param_grads;
+
+typedef struct mc_grad_plan mc_grad_plan;
+
+mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float dt, const int32_t* pairs,
+                              const int32_t* bending_pairs, int32_t num_steps, int32_t checkpoint_every,
+                              mc_grad_plan** out);
+void mc_grad_plan_destroy(mc_grad_plan* plan);
+size_t mc_grad_plan_workspace_bytes(const mc_grad_plan* plan);
+int32_t mc_grad_plan_checkpoint_every(const mc_grad_plan* plan);
+mc_status mc_grad_plan_bind(mc_grad_plan* plan, void* workspace, size_t bytes, void* stream);
+/* Forward rollout of num_steps steps; the state is read and overwritten with the final
+ * state (all mc_state arrays as in mc_rollout). */
+mc_status mc_grad_forward(mc_grad_plan* plan, const mc_state* state, const mc_actuation* act, void* stream);
+/* Given the cotangent of the final state (NULL arrays = zero), write the cotangent of the
+ * initial state and the parameter gradients.  final_cot and initial_cot may alias. */
+mc_status mc_grad_backward(mc_grad_plan* plan, const mc_state_cot* final_cot, mc_state_cot* initial_cot,
+                           mc_param_grads* grads, void* stream);
+
 /* Text of the last error of this thread ("" if none). */
 const char* mc_last_error(void);
 

@@ -73,6 +73,17 @@ class McRecord(ctypes.Structure):
                 ("fluid_velocity", ctypes.c_void_p), ("every", ctypes.c_int32)]
 
 
+class McStateCot(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_void_p), ("velocity", ctypes.c_void_p), ("theta", ctypes.c_void_p),
+                ("f_grid", ctypes.c_void_p)]
+
+
+class McParamGrads(ctypes.Structure):
+    _fields_ = [("rest_angles", ctypes.c_void_p), ("act_c", ctypes.c_void_p), ("act_amp", ctypes.c_void_p),
+                ("act_phase", ctypes.c_void_p), ("rest_lengths", ctypes.c_void_p),
+                ("bending_stiffness", ctypes.c_void_p)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/microcosmos_b200.h
 SIGNATURES = {
     "mc_plan_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(McDims), ctypes.POINTER(McConfig),
@@ -103,6 +114,17 @@ SIGNATURES = {
     "mc_plan_last_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "mc_steric_potential_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                    ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]),
+    "mc_grad_plan_create": (ctypes.c_int, [ctypes.POINTER(McDims), ctypes.POINTER(McConfig), ctypes.c_float,
+                                           c_int_p, c_int_p, ctypes.c_int32, ctypes.c_int32,
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "mc_grad_plan_destroy": (None, [ctypes.c_void_p]),
+    "mc_grad_plan_workspace_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
+    "mc_grad_plan_checkpoint_every": (ctypes.c_int32, [ctypes.c_void_p]),
+    "mc_grad_plan_bind": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    "mc_grad_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(McState), ctypes.POINTER(McActuation),
+                                       ctypes.c_void_p]),
+    "mc_grad_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(McStateCot), ctypes.POINTER(McStateCot),
+                                        ctypes.POINTER(McParamGrads), ctypes.c_void_p]),
     "mc_last_error": (ctypes.c_char_p, []),
     "mc_version": (ctypes.c_char_p, []),
 }

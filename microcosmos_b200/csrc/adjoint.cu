@@ -1,0 +1,1454 @@
+// Reverse-mode derivative of a rollout (the gradient path behind the autograd bindings).
+//
+// A gradient plan wraps one forward plan (the same kernels as mc_rollout) and adds:
+//   * checkpoints of the state every S steps during the forward rollout (S ~ sqrt(T));
+//   * per segment, a recompute of its S step inputs with the forward plan;
+//   * per step, in reverse, a "tape" recompute of the step's intermediates (steric-corrected
+//     prediction, the PBD iterates, the IB stencils and multi-direct forcing iterates) and
+//     the adjoint kernels of stream+collide, IB, PBD and steric.
+//
+// Derivative conventions are those jax.grad applies to the reference: the Peskin stencil
+// positions are stop_gradient-ed (src/microcosmos/solver/fluid.py:237-239), floor has
+// derivative 0, mod derivative 1, max/min pass the cotangent to the selected argument and
+// split it on ties.  Every scatter-add of the adjoint (IB spread, node reaction, steric
+// sample weights) goes through a cell-sorted list (CSR) whose entries are ordered by their
+// flat index, so sums are taken in a fixed order and gradients are reproducible bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/microcosmos_b200.h"
+#include "lbm_cell.cuh"
+#include "mc_internal.cuh"
+
+namespace {
+
+constexpr int kMaxKK = 64;       // stencil entries per node (kernel size <= 8)
+constexpr int kScanChunk = 4096;  // cells per scan block (1024 threads x 4)
+constexpr int kPbdThreads = 1024;
+
+struct AD {
+  int H, W, N, E, B, HW, C, iters, K, KK, steric, fluid, nskip, has_act;
+  float dt, damp, st_strength, sigma, scatter, kstretch, kshear, vmax, relax, mass, wp, wm, cp, cm;
+  float scx, scy, sdtx, sdty;
+  // topology
+  const int2* pairs;
+  const int2* bpairs;
+  const int* n_start;  // node -> incident edges: entry = e * 2 + role (0: src, 1: tgt)
+  const int* n_list;
+  const int* e_start;  // edge -> incident bending pairs: entry = b * 2 + role (0: e_in, 1: e_out)
+  const int* e_list;
+  const float* ndeg;
+  const float* edeg;
+  const float* rest_len;
+  const float* kb;
+  const float* rest_static;
+  const float* act_c;
+  const float* act_amp;
+  const float* act_om;
+  const float* act_ph;
+  // tape
+  float* rest;   // (B) rest angles of the current step
+  float2* pred0;  // (N)
+  float2* pp;     // (C+1) x N PBD iterates
+  float* tt;      // (C+1) x E
+  int* ib_idx;    // N x KK
+  float* ib_w;    // N x KK
+  float2* sraw;   // iters x N
+  float2* s_tmp;  // N
+  float* uc;      // 2 x HW
+  float* inv;     // HW
+  // CSR over cells
+  int* cnt;    // HW (all zero between builds)
+  int* start;  // HW + 1
+  int* bsum;   // scan block sums
+  int* ent;    // entries
+  // adjoint
+  float* lf0p;   // 9 x HW
+  float* lv;     // 2 x HW
+  float* lrho;   // HW
+  float* luc;    // 2 x HW
+  float2* lnv;   // N
+  float2* lprev;  // N
+  float2* lpos;   // N   (state cotangent)
+  float2* lvel;   // N
+  float* lth;     // E
+  float2* lp[2];  // N
+  float* lt[2];   // E
+  float2* lcur;   // E
+  float* lthn;    // E
+  float* gb;      // B
+  float* rest_acc;  // B (this step)
+  float* d_c;
+  float* d_amp;
+  float* d_ph;
+  float* d_rest;
+  float* d_len;
+  float* d_kb;
+  // steric
+  int* st_cell;    // 16 N
+  float* st_val;   // 16 N
+  float2* lpred1;  // N
+  float2* lpred0p;  // N
+  float* lV;       // HW
+  float* ctmp;     // HW
+  float* ldep;     // HW
+  const float* gtW;  // taps along x
+  const float* gtH;  // taps along y
+  int ntW, baseW, ntH, baseH;
+};
+
+__device__ __forceinline__ float dmaxf(float x, float c) { return x > c ? 1.0f : (x == c ? 0.5f : 0.0f); }
+
+// cotangent of (x, y) through (x c, y c), c = min(1, vmax / (sqrt(x^2+y^2+eps)+eps))
+__device__ __forceinline__ float2 clamp_vjp(float x, float y, float vmax, float gx, float gy) {
+  const float mag = sqrtf((x * x + y * y) + MC_EPSIL);
+  const float a = vmax / (mag + MC_EPSIL);
+  const float c = mc::min_prop(1.0f, a);
+  const float sel = a < 1.0f ? 1.0f : (a == 1.0f ? 0.5f : 0.0f);
+  const float gc = x * gx + y * gy;
+  const float da = -vmax / ((mag + MC_EPSIL) * (mag + MC_EPSIL));
+  const float k = ((gc * sel) * da) / mag;
+  return make_float2(c * gx + k * x, c * gy + k * y);
+}
+
+__device__ __forceinline__ int cell_of(int y, int x, int H, int W) { return mc::imod_floor(y, H) * W + mc::imod_floor(x, W); }
+
+// map_coordinates(order=1, mode="wrap") of field V at (yy, xx)
+__device__ __forceinline__ float sample_wrap(const float* V, int H, int W, float yy, float xx) {
+  const float ly = floorf(yy), lx = floorf(xx);
+  const float ty = yy - ly, tx = xx - lx;
+  const float wy0 = 1.0f - ty, wx0 = 1.0f - tx;
+  const int iy = (int)ly, ix = (int)lx;
+  const int y0 = mc::imod_floor(iy, H), y1 = mc::imod_floor(iy + 1, H);
+  const int x0 = mc::imod_floor(ix, W), x1 = mc::imod_floor(ix + 1, W);
+  float acc = (wy0 * wx0) * V[y0 * W + x0];
+  acc = acc + (wy0 * tx) * V[y0 * W + x1];
+  acc = acc + (ty * wx0) * V[y1 * W + x0];
+  acc = acc + (ty * tx) * V[y1 * W + x1];
+  return acc;
+}
+
+// ------------------------------------------------------------------ tape: prediction + steric
+__global__ void k_rest(AD d, int t) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.B) return;
+  float r;
+  if (d.has_act) {
+    const float arg = d.act_om[b] * (float)t + d.act_ph[b];
+    r = d.act_c[b] + d.act_amp[b] * sinf(arg);
+  } else {
+    r = d.rest_static[b];
+  }
+  d.rest[b] = r;
+  d.rest_acc[b] = 0.0f;
+}
+
+__global__ void k_pred(AD d, const float2* __restrict__ pos, const float2* __restrict__ vel,
+                       const float* __restrict__ theta, const float* __restrict__ V) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < d.E) d.tt[i] = theta[i];
+  if (i >= d.N) return;
+  const float2 p = pos[i], v = vel[i];
+  float2 q = make_float2(p.x + (v.x * d.damp) * d.dt, p.y + (v.y * d.damp) * d.dt);
+  d.pred0[i] = q;
+  if (d.steric) {
+    const float Wf = (float)d.W, Hf = (float)d.H;
+    const float x = mc::fmod_floor(q.x, Wf), y = mc::fmod_floor(q.y, Hf);
+    const float e = 0.5f, den = 1.0f;
+    const float gx = (sample_wrap(V, d.H, d.W, y, x + e) - sample_wrap(V, d.H, d.W, y, x - e)) / den;
+    const float gy = (sample_wrap(V, d.H, d.W, y + e, x) - sample_wrap(V, d.H, d.W, y - e, x)) / den;
+    float fx = -gx, fy = -gy;
+    if (d.nskip > 0) {
+      const float inv2s2 = 2.0f * d.sigma * d.sigma;
+      const float norm = (float)(2.0 * M_PI) * d.sigma * d.sigma;
+      float ax = 0.0f, ay = 0.0f;
+      // the neighbours' wrapped predictions, recomputed from their positions and velocities
+      for (int o = -d.nskip; o <= d.nskip; ++o) {
+        const int j = i + o;
+        if (j < 0 || j >= d.N) continue;
+        const float2 pj0 = pos[j], vj = vel[j];
+        const float qx = pj0.x + (vj.x * d.damp) * d.dt, qy = pj0.y + (vj.y * d.damp) * d.dt;
+        const float2 r = mc::min_image(x, y, mc::fmod_floor(qx, Wf), mc::fmod_floor(qy, Hf), Wf, Hf);
+        const float d2 = r.x * r.x + r.y * r.y;
+        const float K = expf(-d2 / inv2s2) / norm;
+        ax = ax + K * r.x;
+        ay = ay + K * r.y;
+      }
+      const float pre = d.scatter / (d.sigma * d.sigma);
+      fx = fx - pre * ax;
+      fy = fy - pre * ay;
+    }
+    q.x = q.x + (fx * d.st_strength) * d.dt;
+    q.y = q.y + (fy * d.st_strength) * d.dt;
+  }
+  d.pp[i] = q;
+}
+
+// ------------------------------------------------------------------ tape: PBD iterates (one CTA)
+__device__ __forceinline__ float bend_corr(const AD& d, const float* th, int b) {
+  const int2 bp = d.bpairs[b];
+  const float pi = (float)M_PI;
+  const float diff = mc::fmod_floor((th[bp.y] - th[bp.x]) + pi, (float)(2.0 * M_PI)) - pi;
+  return ((diff - d.rest[b]) * d.kb[b]) * 0.5f;
+}
+
+__device__ __forceinline__ float2 edge_force(const AD& d, const float2* p, float thn, int e) {
+  const int2 pr = d.pairs[e];
+  const float L0 = d.rest_len[e];
+  const float tx = cosf(thn) * L0, ty = sinf(thn) * L0;
+  const float2 cur = mc::min_image(p[pr.y].x, p[pr.y].y, p[pr.x].x, p[pr.x].y, (float)d.W, (float)d.H);
+  const float L = sqrtf(cur.x * cur.x + cur.y * cur.y);
+  const float m = mc::max_prop(L, 1e-8f);
+  const float sx = (cur.x / m) * (L - L0), sy = (cur.y / m) * (L - L0);
+  const float shx = (cur.x - tx) - sx, shy = (cur.y - ty) - sy;
+  return make_float2(((sx + shx * d.kshear) * d.kstretch) * 0.5f, ((sy + shy * d.kshear) * d.kstretch) * 0.5f);
+}
+
+__global__ void __launch_bounds__(kPbdThreads) k_pbd_fwd(AD d) {
+  for (int k = 0; k < d.C; ++k) {
+    const float* th = d.tt + (size_t)k * d.E;
+    float* thn = d.tt + (size_t)(k + 1) * d.E;
+    for (int e = threadIdx.x; e < d.E; e += blockDim.x) {
+      float acc = 0.0f;
+      for (int q = d.e_start[e]; q < d.e_start[e + 1]; ++q) {
+        const int en = d.e_list[q];
+        const float c = bend_corr(d, th, en >> 1);
+        acc = acc + ((en & 1) ? -c : c);
+      }
+      thn[e] = th[e] + (acc / d.edeg[e]) * 1.8f;
+    }
+    __syncthreads();
+    const float2* p = d.pp + (size_t)k * d.N;
+    float2* pn = d.pp + (size_t)(k + 1) * d.N;
+    for (int n = threadIdx.x; n < d.N; n += blockDim.x) {
+      float ax = 0.0f, ay = 0.0f;
+      for (int q = d.n_start[n]; q < d.n_start[n + 1]; ++q) {
+        const int en = d.n_list[q];
+        const int e = en >> 1;
+        const float2 f = edge_force(d, p, thn[e], e);
+        if (en & 1) {
+          ax = ax + (-f.x);
+          ay = ay + (-f.y);
+        } else {
+          ax = ax + f.x;
+          ay = ay + f.y;
+        }
+      }
+      const float dg = d.ndeg[n];
+      pn[n] = make_float2(p[n].x + ax / dg, p[n].y + ay / dg);
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ tape: IB stencils
+__global__ void k_ib_weights(AD d) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= d.N) return;
+  const float2 p = d.pp[(size_t)d.C * d.N + n];
+  const float x = p.x * d.scx, y = p.y * d.scy;
+  const int K = d.K;
+  const float half = (float)((K - 1) / 2);
+  const float hw = (float)K / 2.0f;
+  const float sx = floorf(x) - half, sy = floorf(y) - half;
+  float w[kMaxKK];
+  float s = 0.0f;
+  for (int a = 0; a < K; ++a) {
+    for (int b = 0; b < K; ++b) {
+      const float nx = sx + (float)a, ny = sy + (float)b;
+      const float rx = fabsf(nx - x) / hw, ry = fabsf(ny - y) / hw;
+      const float px = rx <= 2.0f ? 0.25f * (1.0f + cosf(((float)M_PI * rx) / 2.0f)) : 0.0f;
+      const float py = ry <= 2.0f ? 0.25f * (1.0f + cosf(((float)M_PI * ry) / 2.0f)) : 0.0f;
+      const int q = a * K + b;
+      w[q] = px * py;
+      s = s + w[q];
+      d.ib_idx[(size_t)n * d.KK + q] = cell_of((int)ny, (int)nx, d.H, d.W);
+    }
+  }
+  for (int q = 0; q < d.KK; ++q) d.ib_w[(size_t)n * d.KK + q] = w[q] / (s + MC_EPSIL);
+}
+
+// ------------------------------------------------------------------ CSR over cells
+__global__ void k_csr_count(const int* __restrict__ cells, int M, int* cnt) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < M) atomicAdd(cnt + cells[e], 1);
+}
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* smem, int& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) smem[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int w = lane < (int)(blockDim.x >> 5) ? smem[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    smem[lane] = w;
+  }
+  __syncthreads();
+  const int before = (wid > 0 ? smem[wid - 1] : 0) + x - v;
+  total = smem[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return before;
+}
+
+__global__ void __launch_bounds__(1024) k_scan1(const int* __restrict__ cnt, int n, int* start, int* bsum) {
+  __shared__ int smem[32];
+  const int base = blockIdx.x * kScanChunk + threadIdx.x * 4;
+  int v[4];
+  int s = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    v[j] = base + j < n ? cnt[base + j] : 0;
+    s += v[j];
+  }
+  int total;
+  int run = block_exclusive_scan(s, smem, total);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (base + j < n) start[base + j] = run;
+    run += v[j];
+  }
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan2(int* bsum, int nb) {
+  __shared__ int smem[32];
+  const int base = threadIdx.x * 4;
+  int v[4];
+  int s = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    v[j] = base + j < nb ? bsum[base + j] : 0;
+    s += v[j];
+  }
+  int total;
+  int run = block_exclusive_scan(s, smem, total);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (base + j < nb) bsum[base + j] = run;
+    run += v[j];
+  }
+}
+
+__global__ void k_scan3(int* start, const int* __restrict__ bsum, int n, int M) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) start[i] += bsum[i / kScanChunk];
+  if (i == 0) start[n] = M;
+}
+
+__global__ void k_csr_fill(const int* __restrict__ cells, int M, const int* __restrict__ start, int* cnt, int* ent) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M) return;
+  const int c = cells[e];
+  const int slot = start[c] + atomicSub(cnt + c, 1) - 1;  // leaves cnt at zero
+  ent[slot] = e;
+}
+
+// entries of each cell in increasing flat index (the order np.add.at applies them)
+__global__ void k_csr_sort(const int* __restrict__ start, int n, int* ent) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int a = start[c], b = start[c + 1];
+  for (int i = a + 1; i < b; ++i) {
+    const int v = ent[i];
+    int j = i - 1;
+    while (j >= a && ent[j] > v) {
+      ent[j + 1] = ent[j];
+      --j;
+    }
+    ent[j + 1] = v;
+  }
+}
+
+// ------------------------------------------------------------------ tape: macroscopic + IB iterations
+__global__ void k_macro(AD d, const float* __restrict__ f) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.HW) return;
+  float r = mc::max_prop(f[c], MC_EPSIL);
+  float fv[9];
+  fv[0] = r;
+#pragma unroll
+  for (int i = 1; i < 9; ++i) {
+    fv[i] = mc::max_prop(f[(size_t)i * d.HW + c], MC_EPSIL);
+    r = r + fv[i];
+  }
+  const float rho = mc::max_prop(r, 0.1f);
+  const float ux = (((((fv[1] - fv[3]) + fv[5]) - fv[6]) - fv[7]) + fv[8]) / rho;
+  const float uy = (((((fv[2] - fv[4]) + fv[5]) + fv[6]) - fv[7]) - fv[8]) / rho;
+  const float c1 = mc::clamp_factor(ux, uy, d.vmax);
+  d.uc[c] = ux * c1;
+  d.uc[d.HW + c] = uy * c1;
+  float cov = 0.0f;
+  for (int q = d.start[c]; q < d.start[c + 1]; ++q) cov = cov + d.ib_w[d.ent[q]];
+  d.inv[c] = 1.0f / mc::max_prop(cov, 1.0f);
+}
+
+__global__ void k_ib_interp(AD d, const float2* __restrict__ prev, int it) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= d.N) return;
+  float ix = 0.0f, iy = 0.0f;
+  for (int q = 0; q < d.KK; ++q) {
+    const int c = d.ib_idx[(size_t)n * d.KK + q];
+    const float w = d.ib_w[(size_t)n * d.KK + q];
+    ix = ix + d.uc[c] * w;
+    iy = iy + d.uc[d.HW + c] * w;
+  }
+  const float2 pc = d.pp[(size_t)d.C * d.N + n], p0 = prev[n];
+  const float v1x = (pc.x - p0.x) / d.dt, v1y = (pc.y - p0.y) / d.dt;
+  const float nvx = (v1x * d.scx) * d.dt, nvy = (v1y * d.scy) * d.dt;
+  const float sx = (nvx - ix) * d.relax, sy = (nvy - iy) * d.relax;
+  d.sraw[(size_t)it * d.N + n] = make_float2(sx, sy);
+  const float cf = mc::clamp_factor(sx, sy, d.vmax);
+  d.s_tmp[n] = make_float2(sx * cf, sy * cf);
+}
+
+__global__ void k_ib_spread(AD d) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.HW) return;
+  const int a = d.start[c], b = d.start[c + 1];
+  if (a == b) return;
+  float ax = 0.0f, ay = 0.0f;
+  for (int q = a; q < b; ++q) {
+    const int e = d.ent[q];
+    const float w = d.ib_w[e];
+    const float2 s = d.s_tmp[e / d.KK];
+    ax = ax + s.x * w;
+    ay = ay + s.y * w;
+  }
+  const float iv = d.inv[c];
+  d.uc[c] = d.uc[c] + ax * iv;
+  d.uc[d.HW + c] = d.uc[d.HW + c] + ay * iv;
+}
+
+// ------------------------------------------------------------------ adjoint: stream + collide + F
+__constant__ float kW9[9] = {4.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f,
+                             1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f};
+__constant__ int kOpp[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+
+__global__ void k_lbm_adj1(AD d, const float* __restrict__ f, const float* __restrict__ lfn) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.HW) return;
+  const int y = c / d.W, x = c - y * d.W;
+  float f0[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) f0[i] = mc::max_prop(f[(size_t)i * d.HW + c], MC_EPSIL);
+  float rr = f0[0];
+#pragma unroll
+  for (int i = 1; i < 9; ++i) rr = rr + f0[i];
+  const float rho = mc::max_prop(rr, 0.1f);
+  const float ux = ((((f0[1] - f0[3]) + f0[5]) - f0[6]) - f0[7]) + f0[8];
+  const float uy = ((((f0[2] - f0[4]) + f0[5]) + f0[6]) - f0[7]) - f0[8];
+  const float c1 = mc::clamp_factor(ux / rho, uy / rho, d.vmax);
+  const float vx = (ux / rho) * c1, vy = (uy / rho) * c1;
+  const float u5x = d.uc[c], u5y = d.uc[d.HW + c];
+  const float c2 = mc::clamp_factor(u5x, u5y, d.vmax);
+  const float ucx = u5x * c2, ucy = u5y * c2;
+  const float Fx = (ucx - vx) * rho, Fy = (ucy - vy) * rho;
+  // forward collide for the floor masks
+  float post[9], us_x, us_y;
+  mc::collide(f0, rho, vx, vy, Fx, Fy, d.wp, d.wm, d.cp, d.cm, post, us_x, us_y);
+  // recompute the unfloored collide output for the first mask
+  const float half = 0.5f;
+  const float usx = vx + half * Fx / rho, usy = vy + half * Fy / rho;
+  const float usq = usx * usx + usy * usy;
+  const float udF = usx * Fx + usy * Fy;
+  float eu[9], eF[9], feq[9], raw[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    eu[i] = (float)mc::kEx[i] * usx + (float)mc::kEy[i] * usy;
+    eF[i] = (float)mc::kEx[i] * Fx + (float)mc::kEy[i] * Fy;
+    feq[i] = (rho * kW9[i]) * (((1.0f + 3.0f * eu[i]) + 4.5f * (eu[i] * eu[i])) - 1.5f * usq);
+    raw[i] = kW9[i] * (3.0f * (eF[i] - udF) + (9.0f * eu[i]) * eF[i]);
+  }
+  float g[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const int o = kOpp[i];
+    const float pr = f0[i] - d.wp * (half * (f0[i] + f0[o]) - half * (feq[i] + feq[o])) -
+                     d.wm * (half * (f0[i] - f0[o]) - half * (feq[i] - feq[o]));
+    const float src = d.cp * (half * (raw[i] + raw[o])) + d.cm * (half * (raw[i] - raw[o]));
+    const int xn = x + mc::kEx[i], yn = y + mc::kEy[i];
+    const float lin = lfn[(size_t)i * d.HW + cell_of(yn, xn, d.H, d.W)];
+    g[i] = (lin * dmaxf(post[i], MC_EPSIL)) * dmaxf(pr + src, MC_EPSIL);
+  }
+  float lf0[9];
+  float lrho = 0.0f, lusx = 0.0f, lusy = 0.0f, lFx = 0.0f, lFy = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const int o = kOpp[i];
+    const float gp = half * (g[i] + g[o]), gm = half * (g[i] - g[o]);
+    lf0[i] = g[i] - d.wp * gp - d.wm * gm;
+    const float lfeq = d.wp * gp + d.wm * gm;
+    const float lraw = (1.0f - half * d.wp) * gp + (1.0f - half * d.wm) * gm;
+    const float ex = (float)mc::kEx[i], ey = (float)mc::kEy[i];
+    lrho += lfeq * kW9[i] * (1.0f + 3.0f * eu[i] + 4.5f * eu[i] * eu[i] - 1.5f * usq);
+    const float a = lfeq * rho * kW9[i];
+    lusx += a * (3.0f * ex + 9.0f * eu[i] * ex - 3.0f * usx);
+    lusy += a * (3.0f * ey + 9.0f * eu[i] * ey - 3.0f * usy);
+    const float b = lraw * kW9[i];
+    lusx += b * (-3.0f * Fx + 9.0f * eF[i] * ex);
+    lusy += b * (-3.0f * Fy + 9.0f * eF[i] * ey);
+    lFx += b * (3.0f * ex - 3.0f * usx + 9.0f * eu[i] * ex);
+    lFy += b * (3.0f * ey - 3.0f * usy + 9.0f * eu[i] * ey);
+  }
+  float lvx = lusx, lvy = lusy;
+  lFx += half * lusx / rho;
+  lFy += half * lusy / rho;
+  lrho -= half * (lusx * Fx + lusy * Fy) / (rho * rho);
+  // node reaction: vel_out = vel1 - (nf / m) / sdt, nf = sum_s w F[idx]
+  float rx = 0.0f, ry = 0.0f;
+  for (int q = d.start[c]; q < d.start[c + 1]; ++q) {
+    const int e = d.ent[q];
+    const float w = d.ib_w[e];
+    const float2 lv = d.lvel[e / d.KK];
+    rx = rx + w * ((-lv.x / d.mass) / d.sdtx);
+    ry = ry + w * ((-lv.y / d.mass) / d.sdty);
+  }
+  lFx = rx + lFx;
+  lFy = ry + lFy;
+  // F = (ucc - v) rho
+  const float lccx = lFx * rho, lccy = lFy * rho;
+  lvx -= lFx * rho;
+  lvy -= lFy * rho;
+  lrho += lFx * (ucx - vx) + lFy * (ucy - vy);
+  const float2 l5 = clamp_vjp(u5x, u5y, d.vmax, lccx, lccy);
+  d.luc[c] = l5.x;
+  d.luc[d.HW + c] = l5.y;
+  d.lv[c] = lvx;
+  d.lv[d.HW + c] = lvy;
+  d.lrho[c] = lrho;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) d.lf0p[(size_t)i * d.HW + c] = lf0[i];
+}
+
+__global__ void k_ib_rev_node(AD d, int it) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= d.N) return;
+  float sx = 0.0f, sy = 0.0f;
+  for (int q = 0; q < d.KK; ++q) {
+    const int c = d.ib_idx[(size_t)n * d.KK + q];
+    const float w = d.ib_w[(size_t)n * d.KK + q];
+    const float iv = d.inv[c];
+    sx = sx + (iv * d.luc[c]) * w;
+    sy = sy + (iv * d.luc[d.HW + c]) * w;
+  }
+  const float2 r = d.sraw[(size_t)it * d.N + n];
+  const float2 lr = clamp_vjp(r.x, r.y, d.vmax, sx, sy);
+  float2 a = d.lnv[n];
+  a.x += d.relax * lr.x;
+  a.y += d.relax * lr.y;
+  d.lnv[n] = a;
+  d.s_tmp[n] = make_float2(-d.relax * lr.x, -d.relax * lr.y);
+}
+
+__global__ void k_ib_rev_cell(AD d) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.HW) return;
+  const int a = d.start[c], b = d.start[c + 1];
+  if (a == b) return;
+  float ax = 0.0f, ay = 0.0f;
+  for (int q = a; q < b; ++q) {
+    const int e = d.ent[q];
+    const float w = d.ib_w[e];
+    const float2 s = d.s_tmp[e / d.KK];
+    ax = ax + s.x * w;
+    ay = ay + s.y * w;
+  }
+  d.luc[c] = d.luc[c] + ax;
+  d.luc[d.HW + c] = d.luc[d.HW + c] + ay;
+}
+
+__global__ void k_lbm_adj2(AD d, const float* __restrict__ f, float* __restrict__ lf_out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.HW) return;
+  float f0[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) f0[i] = mc::max_prop(f[(size_t)i * d.HW + c], MC_EPSIL);
+  float rr = f0[0];
+#pragma unroll
+  for (int i = 1; i < 9; ++i) rr = rr + f0[i];
+  const float rho = mc::max_prop(rr, 0.1f);
+  const float ux = (((((f0[1] - f0[3]) + f0[5]) - f0[6]) - f0[7]) + f0[8]) / rho;
+  const float uy = (((((f0[2] - f0[4]) + f0[5]) + f0[6]) - f0[7]) - f0[8]) / rho;
+  const float lvx = d.lv[c] + d.luc[c], lvy = d.lv[d.HW + c] + d.luc[d.HW + c];
+  const float2 lu = clamp_vjp(ux, uy, d.vmax, lvx, lvy);
+  const float lrho = d.lrho[c] - (lu.x * ux + lu.y * uy) / rho;
+  const float lraw = lrho * dmaxf(rr, 0.1f);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const float l0 = d.lf0p[(size_t)i * d.HW + c] + lraw + ((float)mc::kEx[i] * lu.x + (float)mc::kEy[i] * lu.y) / rho;
+    lf_out[(size_t)i * d.HW + c] = l0 * dmaxf(f[(size_t)i * d.HW + c], MC_EPSIL);
+  }
+}
+
+// ------------------------------------------------------------------ adjoint: node velocity / position
+__global__ void k_node_adj(AD d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < d.E) d.lt[0][i] = d.lth[i];
+  if (i >= d.N) return;
+  float2 lv1 = d.lvel[i];
+  if (d.fluid) {
+    const float2 a = d.lnv[i];
+    lv1.x = lv1.x + (a.x * d.scx) * d.dt;
+    lv1.y = lv1.y + (a.y * d.scy) * d.dt;
+  }
+  const float2 lp = d.lpos[i];
+  d.lp[0][i] = make_float2(lp.x + lv1.x / d.dt, lp.y + lv1.y / d.dt);
+  d.lprev[i] = make_float2(-lv1.x / d.dt, -lv1.y / d.dt);
+}
+
+// ------------------------------------------------------------------ adjoint: PBD iterations (one CTA)
+__global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d, int t) {
+  int cur = 0;
+  const float ks = d.kshear, kst = d.kstretch;
+  for (int k = d.C - 1; k >= 0; --k) {
+    const float2* p = d.pp + (size_t)k * d.N;
+    const float* th = d.tt + (size_t)k * d.E;
+    const float* thn = d.tt + (size_t)(k + 1) * d.E;
+    const float2* lpi = d.lp[cur];
+    float2* lpo = d.lp[cur ^ 1];
+    const float* lti = d.lt[cur];
+    float* lto = d.lt[cur ^ 1];
+    // position pass
+    for (int e = threadIdx.x; e < d.E; e += blockDim.x) {
+      const int2 pr = d.pairs[e];
+      const float ns = d.ndeg[pr.x], nt = d.ndeg[pr.y];
+      const float hx = ((lpi[pr.x].x / ns - lpi[pr.y].x / nt) * kst) * 0.5f;
+      const float hy = ((lpi[pr.x].y / ns - lpi[pr.y].y / nt) * kst) * 0.5f;
+      const float2 cur_v = mc::min_image(p[pr.y].x, p[pr.y].y, p[pr.x].x, p[pr.x].y, (float)d.W, (float)d.H);
+      const float L = sqrtf(cur_v.x * cur_v.x + cur_v.y * cur_v.y);
+      const float L0 = d.rest_len[e];
+      const float m = mc::max_prop(L, 1e-8f);
+      const float a = (L - L0) / m;
+      const float da = (1.0f / m - (L - L0) * dmaxf(L, 1e-8f) / (m * m)) / L;
+      const float lsx = (1.0f - ks) * hx, lsy = (1.0f - ks) * hy;
+      const float sdot = cur_v.x * lsx + cur_v.y * lsy;
+      const float lcx = ks * hx + a * lsx + (sdot * da) * cur_v.x;
+      const float lcy = ks * hy + a * lsy + (sdot * da) * cur_v.y;
+      const float ltx = -ks * hx, lty = -ks * hy;
+      float cs, sn;
+      sincosf(thn[e], &sn, &cs);
+      d.d_len[e] += -sdot / m + (cs * ltx + sn * lty);
+      d.lthn[e] = lti[e] + L0 * (-sn * ltx + cs * lty);
+      d.lcur[e] = make_float2(lcx, lcy);
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < d.N; n += blockDim.x) {
+      float ax = lpi[n].x, ay = lpi[n].y;
+      for (int q = d.n_start[n]; q < d.n_start[n + 1]; ++q) {
+        const int en = d.n_list[q];
+        const float2 lc = d.lcur[en >> 1];
+        if (en & 1) {
+          ax += lc.x;
+          ay += lc.y;
+        } else {
+          ax -= lc.x;
+          ay -= lc.y;
+        }
+      }
+      lpo[n] = make_float2(ax, ay);
+    }
+    for (int b = threadIdx.x; b < d.B; b += blockDim.x) {
+      const int2 bp = d.bpairs[b];
+      const float lcorr = 1.8f * (d.lthn[bp.x] / d.edeg[bp.x] - d.lthn[bp.y] / d.edeg[bp.y]);
+      const float g = lcorr * d.kb[b] * 0.5f;
+      d.gb[b] = g;
+      d.rest_acc[b] -= g;
+      const float pi = (float)M_PI;
+      const float diff = mc::fmod_floor((th[bp.y] - th[bp.x]) + pi, (float)(2.0 * M_PI)) - pi;
+      d.d_kb[b] += lcorr * (diff - d.rest[b]) * 0.5f;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < d.E; e += blockDim.x) {
+      float a = d.lthn[e];
+      for (int q = d.e_start[e]; q < d.e_start[e + 1]; ++q) {
+        const int en = d.e_list[q];
+        const float g = d.gb[en >> 1];
+        a += (en & 1) ? g : -g;
+      }
+      lto[e] = a;
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  for (int n = threadIdx.x; n < d.N; n += blockDim.x) d.lpred1[n] = d.lp[cur][n];
+  for (int e = threadIdx.x; e < d.E; e += blockDim.x) d.lth[e] = d.lt[cur][e];
+  for (int b = threadIdx.x; b < d.B; b += blockDim.x) {
+    const float G = d.rest_acc[b];
+    if (d.has_act) {
+      const float arg = d.act_om[b] * (float)t + d.act_ph[b];
+      float sn, cs;
+      sincosf(arg, &sn, &cs);
+      d.d_c[b] += G;
+      d.d_amp[b] += G * sn;
+      d.d_ph[b] += G * d.act_amp[b] * cs;
+    } else {
+      d.d_rest[b] += G;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ adjoint: steric
+__device__ __forceinline__ void sample_adj(const AD& d, const float* V, float yy, float xx, float coef, int n, int qs,
+                                           float& lpx, float& lpy) {
+  const float ly = floorf(yy), lx = floorf(xx);
+  const float ty = yy - ly, tx = xx - lx;
+  const int iy = (int)ly, ix = (int)lx;
+  const int y0 = mc::imod_floor(iy, d.H), y1 = mc::imod_floor(iy + 1, d.H);
+  const int x0 = mc::imod_floor(ix, d.W), x1 = mc::imod_floor(ix + 1, d.W);
+  const float v00 = V[y0 * d.W + x0], v01 = V[y0 * d.W + x1], v10 = V[y1 * d.W + x0], v11 = V[y1 * d.W + x1];
+  lpx += coef * ((1.0f - ty) * (v01 - v00) + ty * (v11 - v10));
+  lpy += coef * ((1.0f - tx) * (v10 - v00) + tx * (v11 - v01));
+  const size_t base = (size_t)n * 16 + qs * 4;
+  d.st_cell[base + 0] = y0 * d.W + x0;
+  d.st_val[base + 0] = coef * ((1.0f - ty) * (1.0f - tx));
+  d.st_cell[base + 1] = y0 * d.W + x1;
+  d.st_val[base + 1] = coef * ((1.0f - ty) * tx);
+  d.st_cell[base + 2] = y1 * d.W + x0;
+  d.st_val[base + 2] = coef * (ty * (1.0f - tx));
+  d.st_cell[base + 3] = y1 * d.W + x1;
+  d.st_val[base + 3] = coef * (ty * tx);
+}
+
+__global__ void k_steric_adj_node(AD d, const float* __restrict__ V) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= d.N) return;
+  const float Wf = (float)d.W, Hf = (float)d.H;
+  const float2 lp1 = d.lpred1[n];
+  const float lfx = (lp1.x * d.st_strength) * d.dt, lfy = (lp1.y * d.st_strength) * d.dt;
+  const float2 q = d.pred0[n];
+  const float x = mc::fmod_floor(q.x, Wf), y = mc::fmod_floor(q.y, Hf);
+  const float e = 0.5f;
+  float lpx = 0.0f, lpy = 0.0f;
+  sample_adj(d, V, y, x + e, -lfx, n, 0, lpx, lpy);
+  sample_adj(d, V, y, x - e, lfx, n, 1, lpx, lpy);
+  sample_adj(d, V, y + e, x, -lfy, n, 2, lpx, lpy);
+  sample_adj(d, V, y - e, x, lfy, n, 3, lpx, lpy);
+  if (d.nskip > 0) {
+    const float s2 = d.sigma * d.sigma;
+    const float inv2s2 = 2.0f * d.sigma * d.sigma;
+    const float norm = (float)(2.0 * M_PI) * d.sigma * d.sigma;
+    const float pre = d.scatter / (d.sigma * d.sigma);
+    for (int o = -d.nskip; o <= d.nskip; ++o) {
+      const int j = n + o;
+      if (o == 0 || j < 0 || j >= d.N) continue;
+      const float2 qj = d.pred0[j];
+      const float2 r = mc::min_image(x, y, mc::fmod_floor(qj.x, Wf), mc::fmod_floor(qj.y, Hf), Wf, Hf);
+      const float d2 = r.x * r.x + r.y * r.y;
+      const float K = expf(-d2 / inv2s2) / norm;
+      const float2 lpj = d.lpred1[j];
+      const float ljx = (lpj.x * d.st_strength) * d.dt, ljy = (lpj.y * d.st_strength) * d.dt;
+      // J(r) (g_n - g_j) with g = -pre * lf and J = K (I - r r^T / sigma^2)
+      const float gx = -pre * (lfx - ljx), gy = -pre * (lfy - ljy);
+      const float rg = (r.x * gx + r.y * gy) / s2;
+      lpx += K * (gx - r.x * rg);
+      lpy += K * (gy - r.y * rg);
+    }
+  }
+  d.lpred0p[n] = make_float2(lp1.x + lpx, lp1.y + lpy);
+}
+
+__global__ void k_gather_field(AD d, const float* __restrict__ val, float* out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.HW) return;
+  float a = 0.0f;
+  for (int q = d.start[c]; q < d.start[c + 1]; ++q) a = a + val[d.ent[q]];
+  out[c] = a;
+}
+
+// circular convolution along x (rows) or y (columns) with symmetric taps
+__global__ void k_conv_x(AD d, const float* __restrict__ in, float* out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.HW) return;
+  const int y = c / d.W, x = c - y * d.W;
+  float a = 0.0f;
+  for (int k = 0; k < d.ntW; ++k) a += d.gtW[k] * in[y * d.W + mc::imod_floor(x - (d.baseW + k), d.W)];
+  out[c] = a;
+}
+
+__global__ void k_conv_y(AD d, const float* __restrict__ in, float* out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.HW) return;
+  const int y = c / d.W, x = c - y * d.W;
+  float a = 0.0f;
+  for (int k = 0; k < d.ntH; ++k) a += d.gtH[k] * in[mc::imod_floor(y - (d.baseH + k), d.H) * d.W + x];
+  out[c] = a;
+}
+
+__global__ void k_steric_adj_cic(AD d) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= d.N) return;
+  float2 l0 = d.lpred0p[n];
+  if (d.steric) {
+    const float Wf = (float)d.W, Hf = (float)d.H;
+    const float2 q = d.pred0[n];
+    const float x = mc::fmod_floor(q.x, Wf), y = mc::fmod_floor(q.y, Hf);
+    const float fx = floorf(x), fy = floorf(y);
+    const int x0 = mc::imod_floor((int)fx, d.W), y0 = mc::imod_floor((int)fy, d.H);
+    const int x1 = (x0 + 1) % d.W, y1 = (y0 + 1) % d.H;
+    const float dx = x - fx, dy = y - fy;
+    const float d00 = d.ldep[y0 * d.W + x0], d10 = d.ldep[y0 * d.W + x1];
+    const float d01 = d.ldep[y1 * d.W + x0], d11 = d.ldep[y1 * d.W + x1];
+    const float s = d.scatter;
+    l0.x += s * (-(1.0f - dy) * d00 + (1.0f - dy) * d10 - dy * d01 + dy * d11);
+    l0.y += s * (-(1.0f - dx) * d00 - dx * d10 + (1.0f - dx) * d01 + dx * d11);
+  }
+  const float2 lpv = d.lprev[n];
+  d.lpos[n] = make_float2(lpv.x + l0.x, lpv.y + l0.y);
+  d.lvel[n] = make_float2((l0.x * d.damp) * d.dt, (l0.y * d.damp) * d.dt);
+}
+
+__global__ void k_copy_lpred(AD d) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < d.N) d.lpred0p[n] = d.lpred1[n];
+}
+
+inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+// ------------------------------------------------------------------ host plan
+struct mc_grad_plan {
+  mc_dims dims{};
+  mc_config cfg{};
+  float dt = 0.f;
+  int T = 0, S = 1, nseg = 0;
+  std::vector<int> pairs, bpairs, n_start, n_list, e_start, e_list;
+  std::vector<float> ndeg, edeg, gW, gH;
+  int baseW = 0, baseH = 0;
+  mc_plan* fwd = nullptr;
+  size_t fwd_bytes = 0, total = 0;
+  unsigned char* ws = nullptr;
+  bool bound = false, have_forward = false, has_act = false;
+  // region offsets
+  struct R {
+    size_t off = 0, bytes = 0;
+  };
+  R r_fwd, r_pairs, r_bpairs, r_nst, r_nl, r_est, r_el, r_ndeg, r_edeg, r_len, r_kb, r_rst, r_ac, r_aa, r_ao, r_ap, r_gW,
+      r_gH;
+  R r_wpos, r_wvel, r_wth, r_wra, r_wst, r_wfu, r_wf, r_ck, r_seg, r_segV;
+  R r_rest, r_pred0, r_pp, r_tt, r_ibidx, r_ibw, r_sraw, r_stmp, r_uc, r_inv, r_cnt, r_start, r_bsum, r_ent;
+  R r_lf0p, r_lv, r_lrho, r_luc, r_lnv, r_lprev, r_lpos, r_lvel, r_lth, r_lp0, r_lp1, r_lt0, r_lt1, r_lcur, r_lthn,
+      r_gb, r_racc, r_dc, r_da, r_dp, r_dr, r_dl, r_dk, r_stc, r_stv, r_lpred1, r_lpred0p, r_lV, r_ctmp, r_ldep, r_lf0,
+      r_lf1;
+  size_t state_ck_bytes = 0;  // one checkpoint: pos, vel, theta, f
+  AD ad{};
+};
+
+namespace {
+
+thread_local std::string g_gerr;
+
+mc_status gfail(mc_status s, const std::string& m) {
+  mc::set_last_error(m.c_str());
+  return s;
+}
+
+#define GC(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) return gfail(MC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+size_t al(size_t x) { return (x + 255) / 256 * 256; }
+
+// periodic Gaussian taps of the spectral filter exp(-2 pi^2 sigma^2 f^2) on N points:
+// g[k] = (1/N) sum_j kf_j cos(2 pi j k / N), kept where |g| > 1e-12 g[0]
+void taps(int N, double sigma, std::vector<float>& g, int& base) {
+  std::vector<double> full(N);
+  for (int k = 0; k < N; ++k) {
+    double s = 0.0;
+    for (int j = 0; j < N; ++j) {
+      const double fj = (j < (N + 1) / 2 ? j : j - N) / (double)N;
+      s += std::exp(-2.0 * M_PI * M_PI * sigma * sigma * fj * fj) * std::cos(2.0 * M_PI * (double)j * k / N);
+    }
+    full[k] = s / N;
+  }
+  int R = 0;
+  while (R + 1 <= N / 2 && std::fabs(full[R + 1]) > 1e-12 * std::fabs(full[0])) ++R;
+  g.clear();
+  if (2 * R + 1 >= N) {
+    base = 0;
+    for (int k = 0; k < N; ++k) g.push_back((float)full[k]);
+  } else {
+    base = -R;
+    for (int k = -R; k <= R; ++k) g.push_back((float)full[(k + N) % N]);
+  }
+}
+
+template <typename T>
+T* at(unsigned char* ws, const mc_grad_plan::R& r) {
+  return reinterpret_cast<T*>(ws + r.off);
+}
+
+void csr_build(const AD& d, const int* cells, int M, cudaStream_t s) {
+  const int nb = nblk(d.HW, kScanChunk);
+  if (M > 0) k_csr_count<<<nblk(M, 256), 256, 0, s>>>(cells, M, d.cnt);
+  k_scan1<<<nb, 1024, 0, s>>>(d.cnt, d.HW, d.start, d.bsum);
+  k_scan2<<<1, 1024, 0, s>>>(d.bsum, nb);
+  k_scan3<<<nblk(d.HW, 256), 256, 0, s>>>(d.start, d.bsum, d.HW, M);
+  if (M > 0) k_csr_fill<<<nblk(M, 256), 256, 0, s>>>(cells, M, d.start, d.cnt, d.ent);
+  k_csr_sort<<<nblk(d.HW, 256), 256, 0, s>>>(d.start, d.HW, d.ent);
+}
+
+mc_status copy_state_to(mc_grad_plan* p, float* pos, float* vel, float* th, float* f, const float* spos, const float* svel,
+                        const float* sth, const float* sf, cudaStream_t s) {
+  const mc_dims& D = p->dims;
+  const size_t HW = (size_t)D.H * D.W;
+  GC(cudaMemcpyAsync(pos, spos, (size_t)D.N * 8, cudaMemcpyDeviceToDevice, s));
+  GC(cudaMemcpyAsync(vel, svel, (size_t)D.N * 8, cudaMemcpyDeviceToDevice, s));
+  if (D.E) GC(cudaMemcpyAsync(th, sth, (size_t)D.E * 4, cudaMemcpyDeviceToDevice, s));
+  GC(cudaMemcpyAsync(f, sf, 9 * HW * 4, cudaMemcpyDeviceToDevice, s));
+  return MC_OK;
+}
+
+// checkpoint / segment slot layout: pos (2N), vel (2N), theta (E), f (9 HW), each 256-aligned
+struct Slot {
+  float *pos, *vel, *th, *f;
+};
+Slot slot(mc_grad_plan* p, const mc_grad_plan::R& r, int k) {
+  const mc_dims& D = p->dims;
+  unsigned char* b = p->ws + r.off + (size_t)k * p->state_ck_bytes;
+  Slot s;
+  s.pos = reinterpret_cast<float*>(b);
+  b += al((size_t)D.N * 8);
+  s.vel = reinterpret_cast<float*>(b);
+  b += al((size_t)D.N * 8);
+  s.th = reinterpret_cast<float*>(b);
+  b += al((size_t)std::max(D.E, 1) * 4);
+  s.f = reinterpret_cast<float*>(b);
+  return s;
+}
+
+mc_state working_state(mc_grad_plan* p) {
+  mc_state w{};
+  w.position = at<float>(p->ws, p->r_wpos);
+  w.velocity = at<float>(p->ws, p->r_wvel);
+  w.theta = at<float>(p->ws, p->r_wth);
+  w.rest_lengths = at<float>(p->ws, p->r_len);
+  w.bending_rest_angles = at<float>(p->ws, p->r_wra);
+  w.bending_stiffness = at<float>(p->ws, p->r_kb);
+  w.steric = at<float>(p->ws, p->r_wst);
+  w.fluid_velocity = at<float>(p->ws, p->r_wfu);
+  w.f_grid = at<float>(p->ws, p->r_wf);
+  return w;
+}
+
+mc_status run_fwd(mc_grad_plan* p, int steps, int t0, cudaStream_t s) {
+  mc_state w = working_state(p);
+  mc_actuation a{};
+  const mc_actuation* ap = nullptr;
+  if (p->has_act) {
+    a.c = at<float>(p->ws, p->r_ac);
+    a.amp = at<float>(p->ws, p->r_aa);
+    a.omega = at<float>(p->ws, p->r_ao);
+    a.phase = at<float>(p->ws, p->r_ap);
+    a.t0 = t0;
+    ap = &a;
+  } else if (p->dims.B) {
+    // the static rest angles (the actuation, when used, overwrites this copy)
+    GC(cudaMemcpyAsync(w.bending_rest_angles, at<float>(p->ws, p->r_rst), (size_t)p->dims.B * 4,
+                       cudaMemcpyDeviceToDevice, s));
+  }
+  const mc_actuation* const acts[1] = {ap};
+  return mc_rollout(p->fwd, &w, steps, acts, nullptr, 1, s);
+}
+
+void reverse_step(mc_grad_plan* p, int t, const Slot& in, const float* V, int& lfcur, cudaStream_t s) {
+  AD& d = p->ad;
+  const int TB = 256;
+  const int nNE = std::max(d.N, d.E);
+  k_rest<<<nblk(std::max(d.B, 1), TB), TB, 0, s>>>(d, t);
+  k_pred<<<nblk(nNE, TB), TB, 0, s>>>(d, reinterpret_cast<const float2*>(in.pos),
+                                      reinterpret_cast<const float2*>(in.vel), in.th, V);
+  k_pbd_fwd<<<1, kPbdThreads, 0, s>>>(d);
+  float* lf_in = at<float>(p->ws, lfcur ? p->r_lf1 : p->r_lf0);
+  float* lf_out = at<float>(p->ws, lfcur ? p->r_lf0 : p->r_lf1);
+  if (d.fluid) {
+    k_ib_weights<<<nblk(d.N, TB), TB, 0, s>>>(d);
+    csr_build(d, d.ib_idx, d.N * d.KK, s);
+    k_macro<<<nblk(d.HW, TB), TB, 0, s>>>(d, in.f);
+    for (int it = 0; it < d.iters; ++it) {
+      k_ib_interp<<<nblk(d.N, TB), TB, 0, s>>>(d, reinterpret_cast<const float2*>(in.pos), it);
+      k_ib_spread<<<nblk(d.HW, TB), TB, 0, s>>>(d);
+    }
+    k_lbm_adj1<<<nblk(d.HW, TB), TB, 0, s>>>(d, in.f, lf_in);
+    cudaMemsetAsync(d.lnv, 0, (size_t)d.N * 8, s);
+    for (int it = d.iters - 1; it >= 0; --it) {
+      k_ib_rev_node<<<nblk(d.N, TB), TB, 0, s>>>(d, it);
+      k_ib_rev_cell<<<nblk(d.HW, TB), TB, 0, s>>>(d);
+    }
+    k_lbm_adj2<<<nblk(d.HW, TB), TB, 0, s>>>(d, in.f, lf_out);
+    lfcur ^= 1;
+  }
+  k_node_adj<<<nblk(nNE, TB), TB, 0, s>>>(d);
+  k_pbd_rev<<<1, kPbdThreads, 0, s>>>(d, t);
+  if (d.steric) {
+    k_steric_adj_node<<<nblk(d.N, TB), TB, 0, s>>>(d, V);
+    csr_build(d, d.st_cell, d.N * 16, s);
+    k_gather_field<<<nblk(d.HW, TB), TB, 0, s>>>(d, d.st_val, d.lV);
+    k_conv_x<<<nblk(d.HW, TB), TB, 0, s>>>(d, d.lV, d.ctmp);
+    k_conv_y<<<nblk(d.HW, TB), TB, 0, s>>>(d, d.ctmp, d.ldep);
+  } else {
+    k_copy_lpred<<<nblk(d.N, TB), TB, 0, s>>>(d);
+  }
+  k_steric_adj_cic<<<nblk(d.N, TB), TB, 0, s>>>(d);
+}
+
+}  // namespace
+
+extern "C" {
+
+mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float dt, const int32_t* pairs,
+                              const int32_t* bending_pairs, int32_t num_steps, int32_t checkpoint_every,
+                              mc_grad_plan** out) {
+  mc::set_last_error("");
+  if (!dims || !cfg || !out) return gfail(MC_ERR_INVALID, "null argument");
+  *out = nullptr;
+  const mc_dims D = *dims;
+  if (D.N < 1 || D.E < 0 || D.B < 0 || D.H < 4 || D.W < 4) return gfail(MC_ERR_INVALID, "bad dims");
+  if ((D.E && !pairs) || (D.B && !bending_pairs)) return gfail(MC_ERR_INVALID, "null topology");
+  if (num_steps < 0) return gfail(MC_ERR_INVALID, "negative num_steps");
+  if ((long long)D.H * D.W > (long long)kScanChunk * 4096) return gfail(MC_ERR_UNSUPPORTED, "grid too large for the gradient path");
+  if (cfg->ibm_kernel_size < 1 || cfg->ibm_kernel_size * cfg->ibm_kernel_size > kMaxKK)
+    return gfail(MC_ERR_UNSUPPORTED, "ibm_kernel_size outside 1..8");
+  if (cfg->enable_force_clamp) return gfail(MC_ERR_UNSUPPORTED, "enable_force_clamp has no adjoint here");
+  if (cfg->synthetic_node_width != 0.0f) return gfail(MC_ERR_UNSUPPORTED, "synthetic_node_width must be 0");
+  mc_grad_plan* p = new mc_grad_plan();
+  p->dims = D;
+  p->cfg = *cfg;
+  p->dt = dt;
+  p->T = num_steps;
+  int S = checkpoint_every;
+  if (S <= 0) S = std::max(1, (int)std::ceil(std::sqrt((double)std::max(num_steps, 1))));
+  p->S = S;
+  p->nseg = (num_steps + S - 1) / S;
+  p->pairs.assign(pairs, pairs + 2 * (size_t)D.E);
+  p->bpairs.assign(bending_pairs, bending_pairs + 2 * (size_t)D.B);
+  for (int e = 0; e < D.E; ++e)
+    for (int j = 0; j < 2; ++j)
+      if (p->pairs[2 * e + j] < 0 || p->pairs[2 * e + j] >= D.N) {
+        delete p;
+        return gfail(MC_ERR_INVALID, "pairs index out of range");
+      }
+  for (int b = 0; b < D.B; ++b)
+    for (int j = 0; j < 2; ++j)
+      if (p->bpairs[2 * b + j] < 0 || p->bpairs[2 * b + j] >= D.E) {
+        delete p;
+        return gfail(MC_ERR_INVALID, "bending_pairs index out of range");
+      }
+  // gather lists in scatter order: sources first (in edge order), then targets
+  p->n_start.assign(D.N + 1, 0);
+  std::vector<std::vector<int>> nl(D.N);
+  for (int e = 0; e < D.E; ++e) nl[p->pairs[2 * e]].push_back(e * 2);
+  for (int e = 0; e < D.E; ++e) nl[p->pairs[2 * e + 1]].push_back(e * 2 + 1);
+  p->ndeg.resize(D.N);
+  for (int n = 0; n < D.N; ++n) {
+    p->n_start[n + 1] = p->n_start[n] + (int)nl[n].size();
+    p->n_list.insert(p->n_list.end(), nl[n].begin(), nl[n].end());
+    p->ndeg[n] = std::max((float)nl[n].size(), 1.0f);
+  }
+  p->e_start.assign(D.E + 1, 0);
+  std::vector<std::vector<int>> el(D.E);
+  for (int b = 0; b < D.B; ++b) el[p->bpairs[2 * b]].push_back(b * 2);
+  for (int b = 0; b < D.B; ++b) el[p->bpairs[2 * b + 1]].push_back(b * 2 + 1);
+  p->edeg.resize(D.E);
+  for (int e = 0; e < D.E; ++e) {
+    p->e_start[e + 1] = p->e_start[e] + (int)el[e].size();
+    p->e_list.insert(p->e_list.end(), el[e].begin(), el[e].end());
+    p->edeg[e] = std::max((float)el[e].size(), 1.0f);
+  }
+  taps(D.W, cfg->steric_sigma, p->gW, p->baseW);
+  taps(D.H, cfg->steric_sigma, p->gH, p->baseH);
+  // forward plan (same kernels as mc_rollout)
+  const int32_t* pp[1] = {pairs};
+  const int32_t* bb[1] = {bending_pairs};
+  mc_status st = mc_plan_create(1, &D, cfg, &dt, pp, bb, &p->fwd);
+  if (st != MC_OK) {
+    delete p;
+    return st;
+  }
+  p->fwd_bytes = mc_plan_workspace_bytes(p->fwd);
+  // layout
+  const size_t N = D.N, E = std::max(D.E, 1), B = std::max(D.B, 1), HW = (size_t)D.H * D.W;
+  const int C = cfg->cycles_per_step, KK = cfg->ibm_kernel_size * cfg->ibm_kernel_size;
+  const int iters = std::max(cfg->ibm_iterations, 1);
+  size_t o = 0;
+  auto take = [&](mc_grad_plan::R& r, size_t bytes) {
+    r.off = o;
+    r.bytes = bytes;
+    o += al(std::max<size_t>(bytes, 4));
+  };
+  take(p->r_fwd, p->fwd_bytes);
+  take(p->r_pairs, E * 8);
+  take(p->r_bpairs, B * 8);
+  take(p->r_nst, (N + 1) * 4);
+  take(p->r_nl, std::max<size_t>(p->n_list.size(), 1) * 4);
+  take(p->r_est, (E + 1) * 4);
+  take(p->r_el, std::max<size_t>(p->e_list.size(), 1) * 4);
+  take(p->r_ndeg, N * 4);
+  take(p->r_edeg, E * 4);
+  take(p->r_len, E * 4);
+  take(p->r_kb, B * 4);
+  take(p->r_rst, B * 4);
+  take(p->r_ac, B * 4);
+  take(p->r_aa, B * 4);
+  take(p->r_ao, B * 4);
+  take(p->r_ap, B * 4);
+  take(p->r_gW, p->gW.size() * 4);
+  take(p->r_gH, p->gH.size() * 4);
+  take(p->r_wpos, N * 8);
+  take(p->r_wvel, N * 8);
+  take(p->r_wth, E * 4);
+  take(p->r_wra, B * 4);
+  take(p->r_wst, HW * 4);
+  take(p->r_wfu, 2 * HW * 4);
+  take(p->r_wf, 9 * HW * 4);
+  p->state_ck_bytes = al(N * 8) * 2 + al(E * 4) + al(9 * HW * 4);
+  take(p->r_ck, std::max(p->nseg, 1) * p->state_ck_bytes);
+  take(p->r_seg, (size_t)S * p->state_ck_bytes);
+  take(p->r_segV, (size_t)S * al(HW * 4));
+  take(p->r_rest, B * 4);
+  take(p->r_pred0, N * 8);
+  take(p->r_pp, (size_t)(C + 1) * N * 8);
+  take(p->r_tt, (size_t)(C + 1) * E * 4);
+  take(p->r_ibidx, N * KK * 4);
+  take(p->r_ibw, N * KK * 4);
+  take(p->r_sraw, (size_t)iters * N * 8);
+  take(p->r_stmp, N * 8);
+  take(p->r_uc, 2 * HW * 4);
+  take(p->r_inv, HW * 4);
+  take(p->r_cnt, HW * 4);
+  take(p->r_start, (HW + 1) * 4);
+  take(p->r_bsum, 4096 * 4);
+  take(p->r_ent, std::max<size_t>(N * KK, 16 * N) * 4);
+  take(p->r_lf0p, 9 * HW * 4);
+  take(p->r_lv, 2 * HW * 4);
+  take(p->r_lrho, HW * 4);
+  take(p->r_luc, 2 * HW * 4);
+  take(p->r_lnv, N * 8);
+  take(p->r_lprev, N * 8);
+  take(p->r_lpos, N * 8);
+  take(p->r_lvel, N * 8);
+  take(p->r_lth, E * 4);
+  take(p->r_lp0, N * 8);
+  take(p->r_lp1, N * 8);
+  take(p->r_lt0, E * 4);
+  take(p->r_lt1, E * 4);
+  take(p->r_lcur, E * 8);
+  take(p->r_lthn, E * 4);
+  take(p->r_gb, B * 4);
+  take(p->r_racc, B * 4);
+  take(p->r_dc, B * 4);
+  take(p->r_da, B * 4);
+  take(p->r_dp, B * 4);
+  take(p->r_dr, B * 4);
+  take(p->r_dl, E * 4);
+  take(p->r_dk, B * 4);
+  take(p->r_stc, 16 * N * 4);
+  take(p->r_stv, 16 * N * 4);
+  take(p->r_lpred1, N * 8);
+  take(p->r_lpred0p, N * 8);
+  take(p->r_lV, HW * 4);
+  take(p->r_ctmp, HW * 4);
+  take(p->r_ldep, HW * 4);
+  take(p->r_lf0, 9 * HW * 4);
+  take(p->r_lf1, 9 * HW * 4);
+  p->total = o;
+  *out = p;
+  return MC_OK;
+}
+
+void mc_grad_plan_destroy(mc_grad_plan* p) {
+  if (!p) return;
+  if (p->fwd) mc_plan_destroy(p->fwd);
+  delete p;
+}
+
+size_t mc_grad_plan_workspace_bytes(const mc_grad_plan* p) { return p ? p->total : 0; }
+
+int32_t mc_grad_plan_checkpoint_every(const mc_grad_plan* p) { return p ? p->S : 0; }
+
+mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void* stream) {
+  mc::set_last_error("");
+  if (!p) return gfail(MC_ERR_INVALID, "null plan");
+  if (!workspace || bytes < p->total || ((uintptr_t)workspace & 255))
+    return gfail(MC_ERR_WORKSPACE, "workspace missing, too small or not 256-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  p->ws = (unsigned char*)workspace;
+  mc_status st = mc_plan_bind(p->fwd, p->ws + p->r_fwd.off, p->fwd_bytes, stream);
+  if (st != MC_OK) return st;
+  auto up = [&](const mc_grad_plan::R& r, const void* src, size_t n) -> cudaError_t {
+    if (n == 0) return cudaSuccess;
+    return cudaMemcpyAsync(p->ws + r.off, src, n, cudaMemcpyHostToDevice, s);
+  };
+  GC(up(p->r_pairs, p->pairs.data(), p->pairs.size() * 4));
+  GC(up(p->r_bpairs, p->bpairs.data(), p->bpairs.size() * 4));
+  GC(up(p->r_nst, p->n_start.data(), p->n_start.size() * 4));
+  GC(up(p->r_nl, p->n_list.data(), p->n_list.size() * 4));
+  GC(up(p->r_est, p->e_start.data(), p->e_start.size() * 4));
+  GC(up(p->r_el, p->e_list.data(), p->e_list.size() * 4));
+  GC(up(p->r_ndeg, p->ndeg.data(), p->ndeg.size() * 4));
+  GC(up(p->r_edeg, p->edeg.data(), p->edeg.size() * 4));
+  GC(up(p->r_gW, p->gW.data(), p->gW.size() * 4));
+  GC(up(p->r_gH, p->gH.data(), p->gH.size() * 4));
+  GC(cudaMemsetAsync(p->ws + p->r_cnt.off, 0, p->r_cnt.bytes, s));
+  GC(cudaStreamSynchronize(s));  // the host tables above are temporaries of this call's scope
+  const mc_config& c = p->cfg;
+  const mc_dims& D = p->dims;
+  AD& d = p->ad;
+  d = AD{};
+  d.H = D.H;
+  d.W = D.W;
+  d.N = D.N;
+  d.E = D.E;
+  d.B = D.B;
+  d.HW = D.H * D.W;
+  d.C = c.cycles_per_step;
+  d.iters = c.ibm_iterations;
+  d.K = c.ibm_kernel_size;
+  d.KK = d.K * d.K;
+  d.steric = c.enable_steric;
+  d.fluid = c.enable_fluid;
+  d.nskip = c.steric_neighbor_skip;
+  d.dt = p->dt;
+  d.damp = c.damping;
+  d.st_strength = c.steric_strength;
+  d.sigma = c.steric_sigma;
+  d.scatter = c.steric_scatter_value;
+  d.kstretch = c.stiffness_stretch;
+  d.kshear = c.stiffness_shear;
+  const float scx = (float)D.W / (float)D.H, scy = (float)D.H / (float)D.W;
+  d.scx = scx;
+  d.scy = scy;
+  d.vmax = (float)(c.max_fluid_velocity * (0.5 * ((double)D.W / D.H + (double)D.H / D.W)));
+  d.relax = c.ibm_relaxation;
+  d.mass = c.node_mass;
+  {
+    // omega+ = clip(1/(3 nu + 0.5), 0, 1.9); omega- from the magic parameter (fluid.py:155-161)
+    const float wp = std::min(std::max((float)(1.0 / (3.0 * c.viscosity + 0.5)), 0.0f), 1.9f);
+    const float eps = 1.1920928955078125e-07f;
+    const float off = 1.0f / std::max(wp, eps) - 0.5f;
+    const float wm = 1.0f / (c.lambda_trt / std::max(off, eps) + 0.5f);
+    d.wp = wp;
+    d.wm = wm;
+    d.cp = 1.0f - 0.5f * wp;
+    d.cm = 1.0f - 0.5f * wm;
+  }
+  d.sdtx = scx * p->dt;
+  d.sdty = scy * p->dt;
+  unsigned char* w = p->ws;
+  d.pairs = at<int2>(w, p->r_pairs);
+  d.bpairs = at<int2>(w, p->r_bpairs);
+  d.n_start = at<int>(w, p->r_nst);
+  d.n_list = at<int>(w, p->r_nl);
+  d.e_start = at<int>(w, p->r_est);
+  d.e_list = at<int>(w, p->r_el);
+  d.ndeg = at<float>(w, p->r_ndeg);
+  d.edeg = at<float>(w, p->r_edeg);
+  d.rest_len = at<float>(w, p->r_len);
+  d.kb = at<float>(w, p->r_kb);
+  d.rest_static = at<float>(w, p->r_rst);
+  d.act_c = at<float>(w, p->r_ac);
+  d.act_amp = at<float>(w, p->r_aa);
+  d.act_om = at<float>(w, p->r_ao);
+  d.act_ph = at<float>(w, p->r_ap);
+  d.rest = at<float>(w, p->r_rest);
+  d.pred0 = at<float2>(w, p->r_pred0);
+  d.pp = at<float2>(w, p->r_pp);
+  d.tt = at<float>(w, p->r_tt);
+  d.ib_idx = at<int>(w, p->r_ibidx);
+  d.ib_w = at<float>(w, p->r_ibw);
+  d.sraw = at<float2>(w, p->r_sraw);
+  d.s_tmp = at<float2>(w, p->r_stmp);
+  d.uc = at<float>(w, p->r_uc);
+  d.inv = at<float>(w, p->r_inv);
+  d.cnt = at<int>(w, p->r_cnt);
+  d.start = at<int>(w, p->r_start);
+  d.bsum = at<int>(w, p->r_bsum);
+  d.ent = at<int>(w, p->r_ent);
+  d.lf0p = at<float>(w, p->r_lf0p);
+  d.lv = at<float>(w, p->r_lv);
+  d.lrho = at<float>(w, p->r_lrho);
+  d.luc = at<float>(w, p->r_luc);
+  d.lnv = at<float2>(w, p->r_lnv);
+  d.lprev = at<float2>(w, p->r_lprev);
+  d.lpos = at<float2>(w, p->r_lpos);
+  d.lvel = at<float2>(w, p->r_lvel);
+  d.lth = at<float>(w, p->r_lth);
+  d.lp[0] = at<float2>(w, p->r_lp0);
+  d.lp[1] = at<float2>(w, p->r_lp1);
+  d.lt[0] = at<float>(w, p->r_lt0);
+  d.lt[1] = at<float>(w, p->r_lt1);
+  d.lcur = at<float2>(w, p->r_lcur);
+  d.lthn = at<float>(w, p->r_lthn);
+  d.gb = at<float>(w, p->r_gb);
+  d.rest_acc = at<float>(w, p->r_racc);
+  d.d_c = at<float>(w, p->r_dc);
+  d.d_amp = at<float>(w, p->r_da);
+  d.d_ph = at<float>(w, p->r_dp);
+  d.d_rest = at<float>(w, p->r_dr);
+  d.d_len = at<float>(w, p->r_dl);
+  d.d_kb = at<float>(w, p->r_dk);
+  d.st_cell = at<int>(w, p->r_stc);
+  d.st_val = at<float>(w, p->r_stv);
+  d.lpred1 = at<float2>(w, p->r_lpred1);
+  d.lpred0p = at<float2>(w, p->r_lpred0p);
+  d.lV = at<float>(w, p->r_lV);
+  d.ctmp = at<float>(w, p->r_ctmp);
+  d.ldep = at<float>(w, p->r_ldep);
+  d.gtW = at<float>(w, p->r_gW);
+  d.gtH = at<float>(w, p->r_gH);
+  d.ntW = (int)p->gW.size();
+  d.baseW = p->baseW;
+  d.ntH = (int)p->gH.size();
+  d.baseH = p->baseH;
+  p->bound = true;
+  return MC_OK;
+}
+
+mc_status mc_grad_forward(mc_grad_plan* p, const mc_state* state, const mc_actuation* act, void* stream) {
+  mc::set_last_error("");
+  if (!p || !state) return gfail(MC_ERR_INVALID, "null argument");
+  if (!p->bound) return gfail(MC_ERR_NOT_BOUND, "mc_grad_plan_bind() was not called");
+  cudaStream_t s = (cudaStream_t)stream;
+  const mc_dims& D = p->dims;
+  const size_t HW = (size_t)D.H * D.W;
+  unsigned char* w = p->ws;
+  auto cp = [&](const mc_grad_plan::R& r, const void* src, size_t n) -> cudaError_t {
+    if (n == 0 || !src) return cudaSuccess;
+    return cudaMemcpyAsync(w + r.off, src, n, cudaMemcpyDeviceToDevice, s);
+  };
+  if (!state->position || !state->velocity || !state->f_grid || (D.E && (!state->theta || !state->rest_lengths)) ||
+      (D.B && (!state->bending_rest_angles || !state->bending_stiffness)))
+    return gfail(MC_ERR_INVALID, "null state array");
+  GC(cp(p->r_wpos, state->position, (size_t)D.N * 8));
+  GC(cp(p->r_wvel, state->velocity, (size_t)D.N * 8));
+  GC(cp(p->r_wth, state->theta, (size_t)D.E * 4));
+  GC(cp(p->r_len, state->rest_lengths, (size_t)D.E * 4));
+  GC(cp(p->r_kb, state->bending_stiffness, (size_t)D.B * 4));
+  GC(cp(p->r_rst, state->bending_rest_angles, (size_t)D.B * 4));
+  GC(cp(p->r_wra, state->bending_rest_angles, (size_t)D.B * 4));
+  if (state->steric) GC(cp(p->r_wst, state->steric, HW * 4));
+  else GC(cudaMemsetAsync(w + p->r_wst.off, 0, HW * 4, s));
+  if (state->fluid_velocity) GC(cp(p->r_wfu, state->fluid_velocity, 2 * HW * 4));
+  else GC(cudaMemsetAsync(w + p->r_wfu.off, 0, 2 * HW * 4, s));
+  GC(cp(p->r_wf, state->f_grid, 9 * HW * 4));
+  p->has_act = act != nullptr;
+  if (act) {
+    if (D.B && (!act->c || !act->amp || !act->omega || !act->phase)) return gfail(MC_ERR_INVALID, "null actuation array");
+    if (act->t0 != 0) return gfail(MC_ERR_UNSUPPORTED, "the gradient path starts its actuation clock at t0 = 0");
+    GC(cp(p->r_ac, act->c, (size_t)D.B * 4));
+    GC(cp(p->r_aa, act->amp, (size_t)D.B * 4));
+    GC(cp(p->r_ao, act->omega, (size_t)D.B * 4));
+    GC(cp(p->r_ap, act->phase, (size_t)D.B * 4));
+  }
+  p->ad.has_act = p->has_act ? 1 : 0;
+  for (int k = 0; k < p->nseg; ++k) {
+    Slot ck = slot(p, p->r_ck, k);
+    mc_status st = copy_state_to(p, ck.pos, ck.vel, ck.th, ck.f, at<float>(w, p->r_wpos), at<float>(w, p->r_wvel),
+                                 at<float>(w, p->r_wth), at<float>(w, p->r_wf), s);
+    if (st != MC_OK) return st;
+    const int len = std::min(p->S, p->T - k * p->S);
+    st = run_fwd(p, len, k * p->S, s);
+    if (st != MC_OK) return st;
+  }
+  // final state back to the caller
+  auto back = [&](void* dst, const mc_grad_plan::R& r, size_t n) -> cudaError_t {
+    if (!dst || n == 0) return cudaSuccess;
+    return cudaMemcpyAsync(dst, w + r.off, n, cudaMemcpyDeviceToDevice, s);
+  };
+  GC(back(state->position, p->r_wpos, (size_t)D.N * 8));
+  GC(back(state->velocity, p->r_wvel, (size_t)D.N * 8));
+  GC(back(state->theta, p->r_wth, (size_t)D.E * 4));
+  GC(back(state->bending_rest_angles, p->r_wra, (size_t)D.B * 4));
+  GC(back(state->steric, p->r_wst, HW * 4));
+  GC(back(state->fluid_velocity, p->r_wfu, 2 * HW * 4));
+  GC(back(state->f_grid, p->r_wf, 9 * HW * 4));
+  GC(cudaGetLastError());
+  p->have_forward = true;
+  return MC_OK;
+}
+
+mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_state_cot* initial_cot,
+                           mc_param_grads* grads, void* stream) {
+  mc::set_last_error("");
+  if (!p || !final_cot || !initial_cot) return gfail(MC_ERR_INVALID, "null argument");
+  if (!p->bound) return gfail(MC_ERR_NOT_BOUND, "mc_grad_plan_bind() was not called");
+  if (!p->have_forward) return gfail(MC_ERR_INVALID, "mc_grad_forward() has not run on this plan");
+  cudaStream_t s = (cudaStream_t)stream;
+  const mc_dims& D = p->dims;
+  const size_t HW = (size_t)D.H * D.W;
+  unsigned char* w = p->ws;
+  AD& d = p->ad;
+  auto seed = [&](const mc_grad_plan::R& r, const float* src, size_t n) -> cudaError_t {
+    if (n == 0) return cudaSuccess;
+    if (!src) return cudaMemsetAsync(w + r.off, 0, n, s);
+    return cudaMemcpyAsync(w + r.off, src, n, cudaMemcpyDeviceToDevice, s);
+  };
+  GC(seed(p->r_lpos, final_cot->position, (size_t)D.N * 8));
+  GC(seed(p->r_lvel, final_cot->velocity, (size_t)D.N * 8));
+  GC(seed(p->r_lth, final_cot->theta, (size_t)D.E * 4));
+  GC(seed(p->r_lf0, final_cot->f_grid, 9 * HW * 4));
+  for (const mc_grad_plan::R* r : {&p->r_dc, &p->r_da, &p->r_dp, &p->r_dr, &p->r_dl, &p->r_dk})
+    GC(cudaMemsetAsync(w + r->off, 0, r->bytes, s));
+  int lfcur = 0;
+  for (int k = p->nseg - 1; k >= 0; --k) {
+    const int t0 = k * p->S;
+    const int len = std::min(p->S, p->T - t0);
+    Slot ck = slot(p, p->r_ck, k);
+    mc_status st = copy_state_to(p, at<float>(w, p->r_wpos), at<float>(w, p->r_wvel), at<float>(w, p->r_wth),
+                                 at<float>(w, p->r_wf), ck.pos, ck.vel, ck.th, ck.f, s);
+    if (st != MC_OK) return st;
+    for (int j = 0; j < len; ++j) {
+      Slot sj = slot(p, p->r_seg, j);
+      st = copy_state_to(p, sj.pos, sj.vel, sj.th, sj.f, at<float>(w, p->r_wpos), at<float>(w, p->r_wvel),
+                         at<float>(w, p->r_wth), at<float>(w, p->r_wf), s);
+      if (st != MC_OK) return st;
+      st = run_fwd(p, 1, t0 + j, s);
+      if (st != MC_OK) return st;
+      GC(cudaMemcpyAsync(w + p->r_segV.off + (size_t)j * al(HW * 4), w + p->r_wst.off, HW * 4,
+                         cudaMemcpyDeviceToDevice, s));
+    }
+    for (int j = len - 1; j >= 0; --j) {
+      Slot sj = slot(p, p->r_seg, j);
+      const float* V = reinterpret_cast<const float*>(w + p->r_segV.off + (size_t)j * al(HW * 4));
+      reverse_step(p, t0 + j, sj, V, lfcur, s);
+      GC(cudaGetLastError());
+    }
+  }
+  (void)d;
+  auto out = [&](float* dst, const mc_grad_plan::R& r, size_t n) -> cudaError_t {
+    if (!dst || n == 0) return cudaSuccess;
+    return cudaMemcpyAsync(dst, w + r.off, n, cudaMemcpyDeviceToDevice, s);
+  };
+  GC(out(initial_cot->position, p->r_lpos, (size_t)D.N * 8));
+  GC(out(initial_cot->velocity, p->r_lvel, (size_t)D.N * 8));
+  GC(out(initial_cot->theta, p->r_lth, (size_t)D.E * 4));
+  GC(out(initial_cot->f_grid, lfcur ? p->r_lf1 : p->r_lf0, 9 * HW * 4));
+  if (grads) {
+    GC(out(grads->act_c, p->r_dc, (size_t)D.B * 4));
+    GC(out(grads->act_amp, p->r_da, (size_t)D.B * 4));
+    GC(out(grads->act_phase, p->r_dp, (size_t)D.B * 4));
+    GC(out(grads->rest_angles, p->r_dr, (size_t)D.B * 4));
+    GC(out(grads->rest_lengths, p->r_dl, (size_t)D.E * 4));
+    GC(out(grads->bending_stiffness, p->r_dk, (size_t)D.B * 4));
+  }
+  GC(cudaGetLastError());
+  return MC_OK;
+}
+
+}  // extern "C"
