@@ -183,7 +183,9 @@ def batch_section(args, flush):
     nodes = sum(s.N for s in scs)
     sts = [DeviceState.from_scenario(s) for s in scs]
     acts = [Actuation.from_scenario(s) for s in scs]
-    plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs))
+    from microcosmos_b200 import autotune
+    shape, shape_ms = autotune.tune(sts, [cfg] * len(scs), [0.01] * len(scs), actuations=acts, steps=10, warmup=4)
+    plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs), lbm_shape=shape)
     stream = torch.cuda.current_stream()
     plan.begin(sts, actuations=acts)
     plan.advance(6, use_graph=True)
@@ -239,6 +241,8 @@ def batch_section(args, flush):
         "plain_rollouts_per_s": len(scs) / (t_plain_pop / 1e3 * steps),
         "plain_sample": f"{nplain} rollouts, one plan each, {K} graph-launched steps each",
         "speedup_vs_plain": t_plain_pop / t_batch,
+        "autotune": {"dense_pass_shape": {"cells_per_lane": shape[0], "rows_per_cta": shape[1]},
+                     "ms_per_step_by_shape": {f"{v}x{r}": ms for (v, r), ms in shape_ms.items()}},
         "lbm_ms_per_launch": lbm_ms,
         "kernels_ms_per_step": {k: ms / 10 for k, (ms, n) in prof.items() if n}, "lbm_frac_of_peak": BYTES_PER_CELL * cells / (lbm_ms / 1e3) / 1e9 / 6541.5,
         "roofline_frac_mlups": cells / (t_batch / 1e3) / 1e6 / (6541.5e9 / BYTES_PER_CELL / 1e6),

@@ -126,6 +126,14 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
                          mc_plan** out);
 void mc_plan_destroy(mc_plan* plan);
 
+/* Tile shape of the dense stream+collide pass: each CTA covers 32 * cells_per_lane columns
+ * (1, 2 or 4 cells per thread, vector loads and stores; it must divide every rollout's W)
+ * by rows_per_cta rows (2, 4 or 8).  0 keeps the current value.  Results do not depend on
+ * the shape.  Only before mc_plan_bind(); microcosmos_b200.autotune picks it by timing.
+ * No counterpart in the reference (XLA chooses its own fusion tiling). */
+mc_status mc_plan_set_lbm_shape(mc_plan* plan, int32_t cells_per_lane, int32_t rows_per_cta);
+mc_status mc_plan_get_lbm_shape(const mc_plan* plan, int32_t* cells_per_lane, int32_t* rows_per_cta);
+
 /* Bytes of device workspace the plan needs (all rollouts). */
 size_t mc_plan_workspace_bytes(const mc_plan* plan);
 

@@ -597,7 +597,7 @@ __global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, co
     d.fov[cell] = Fx;
     d.fov[HW + cell] = Fy;
     const int y = cell / d.W, x = cell - y * d.W;
-    d.lbm_flag[(parity & 1) * nflag + (y / kLbmTileY) * d.lbm_tx + x / d.lbm_tw] = 1;
+    d.lbm_flag[(parity & 1) * nflag + (y / d.lbm_th) * d.lbm_tx + x / d.lbm_tw] = 1;
   }
 }
 
@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D
   d.fov[cell] = Fx;
   d.fov[HW + cell] = Fy;
   const int y = cell / d.W, x = cell - y * d.W;
-  d.lbm_flag[(parity & 1) * d.lbm_tx * d.lbm_ty + (y / kLbmTileY) * d.lbm_tx + x / d.lbm_tw] = 1;
+  d.lbm_flag[(parity & 1) * d.lbm_tx * d.lbm_ty + (y / d.lbm_th) * d.lbm_tx + x / d.lbm_tw] = 1;
 }
 
 // Node reaction (fluid.py:364-382), final wrap (simulate.py:97-98), non-finite check and

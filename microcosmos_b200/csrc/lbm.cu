@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) k_lbm(const RDesc* __restrict__ D, const 
   const int tx = lb % d.lbm_tx, ty = lb / d.lbm_tx;
   const int lane = threadIdx.x;
   const int H = d.H, W = d.W;
-  const int y = ty * kLbmTileY + threadIdx.y;
+  const int y = ty * d.lbm_th + threadIdx.y;
   const int x0 = tx * (32 * VEC) + lane * VEC;
   const bool row_ok = y < H;
   const bool x_ok = x0 < W;
@@ -216,8 +216,8 @@ __global__ void k_clear_ws(const RDesc* __restrict__ D, const int* __restrict__ 
   if (t0 == 0) *d.flags = 0u;
 }
 
-void launch_lbm(const Launch& L, int parity, int write_u, int vec) {
-  dim3 block(32, kLbmTileY);
+void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows) {
+  dim3 block(32, rows);
   if (vec == 4)
     k_lbm<4><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u);
   else if (vec == 2)

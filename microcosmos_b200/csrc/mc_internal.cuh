@@ -17,7 +17,8 @@ namespace mc {
 
 constexpr int kBinTile = 16;       // binning tile edge for the deterministic reductions
 constexpr int kLbmTileX = 128;     // dense LBM CTA tile: 32 lanes x 4 cells
-constexpr int kLbmTileY = 8;       //                    8 rows
+constexpr int kLbmTileY = 8;      // default LBM tile height (rows per CTA)
+constexpr int kLbmMinTileY = 2;   // smallest tile height a plan may be tuned to       //                    8 rows
 constexpr int kIbCap = 1024;       // minimum IB bin capacity per 16x16 tile (grown with node density)
 constexpr int kCicCap = 512;       // minimum CIC bin capacity per tile
 constexpr int kMaxBinCap = 8192;   // largest bin capacity (the tile sort keeps 4 x cap words in shared memory)
@@ -34,6 +35,7 @@ struct RDesc {
   int ntile_x, ntile_y;  // binning tiles (kBinTile)
   int lbm_tx, lbm_ty;    // LBM tiles
   int lbm_tw;            // LBM tile width in cells (32 * cells per lane)
+  int lbm_th;            // LBM tile height in rows (threads per CTA = 32 * lbm_th)
   int max_comp_nodes, max_comp_edges, max_comp_pairs;
   // configuration
   float dt, damping, k_stretch, k_shear, vmax, relax, node_mass, wp, wm;
@@ -218,7 +220,7 @@ void launch_ib_spread(const Launch& L, int it);
 void launch_ib_finalize(const Launch& L, int parity);
 cudaError_t launch_ib_coop(const Launch& L, int parity);
 cudaError_t ib_coop_blocks_per_sm(int* out);
-void launch_lbm(const Launch& L, int parity, int write_u, int vec);
+void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows);
 void launch_reaction(const Launch& L, const int* tdev);
 void launch_record_fields(const Launch& L, const int* tdev);
 void launch_unstream(const Launch& L);

@@ -57,7 +57,7 @@ struct HostRollout {
   std::vector<int> fW, fH;
   std::vector<float2> twW, twH;
   std::vector<float> gW, gH;
-  int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4;
+  int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4, lbm_th = mc::kLbmTileY;
   int ib_cap = 0, c_cap = 0;  // bin capacities (powers of two)
   int logW = -1, logH = -1;   // log2 of power-of-two grid sides (-1: mixed radix path)
   int T_r = 0, P_r = 0, T_c = 0, P_c = 0;
@@ -313,6 +313,7 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.lbm_tx = h.lbm_tx;
   d.lbm_ty = h.lbm_ty;
   d.lbm_tw = 32 * h.vec;
+  d.lbm_th = h.lbm_th;
   const mc_config& c = h.cfg;
   d.dt = h.dt;
   d.damping = c.damping;
@@ -593,7 +594,7 @@ int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
 
 int64_t enqueue_lbm(mc_plan* p, int parity, int write_u, cudaStream_t s, bool capture) {
   if (!p->any_fluid) return 0;
-  timed(p, 10, s, capture, [&] { mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->R[0].vec); });
+  timed(p, 10, s, capture, [&] { mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->R[0].vec, p->R[0].lbm_th); });
   return 1;
 }
 
@@ -874,9 +875,11 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
   for (int i = 0; i < n; ++i) {
     HostRollout& h = p->R[i];
     h.vec = vec_all;
+    h.lbm_th = mc::kLbmTileY;
     h.lbm_tx = div_up(h.dims.W, 32 * h.vec);
-    h.lbm_ty = div_up(h.dims.H, mc::kLbmTileY);
-    h.r_lflag = lay.take((size_t)2 * h.lbm_tx * h.lbm_ty * 4);
+    h.lbm_ty = div_up(h.dims.H, h.lbm_th);
+    // sized for the smallest tiles a plan can be tuned to (mc_plan_set_lbm_shape)
+    h.r_lflag = lay.take((size_t)2 * div_up(h.dims.W, 32) * div_up(h.dims.H, mc::kLbmMinTileY) * 4);
   }
   {
     long long tiles = 0;
@@ -943,6 +946,39 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
   p->node_bs = std::min(256, std::max(32, (work + 31) / 32 * 32));
   p->desc.resize(n);
   *out = p;
+  return MC_OK;
+}
+
+mc_status mc_plan_set_lbm_shape(mc_plan* p, int32_t cells_per_lane, int32_t rows_per_cta) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (p->bound) return fail(MC_ERR_INVALID, "the dense-pass tile shape is set before mc_plan_bind()");
+  int vec = cells_per_lane > 0 ? cells_per_lane : p->R[0].vec;
+  int rows = rows_per_cta > 0 ? rows_per_cta : p->R[0].lbm_th;
+  if (vec != 1 && vec != 2 && vec != 4) return fail(MC_ERR_INVALID, "cells_per_lane must be 1, 2 or 4");
+  if (rows != 2 && rows != 4 && rows != 8) return fail(MC_ERR_INVALID, "rows_per_cta must be 2, 4 or 8");
+  for (auto& h : p->R)
+    if (h.dims.W % vec != 0 || h.dims.W < vec)
+      return fail(MC_ERR_UNSUPPORTED, "cells_per_lane must divide every rollout's W");
+  int prev = 0;
+  for (int i = 0; i < p->n; ++i) {
+    HostRollout& h = p->R[i];
+    h.vec = vec;
+    h.lbm_th = rows;
+    h.lbm_tx = div_up(h.dims.W, 32 * vec);
+    h.lbm_ty = div_up(h.dims.H, rows);
+    p->off[K_LBM][i] = prev;
+    prev += h.cfg.enable_fluid ? h.lbm_tx * h.lbm_ty : 0;
+  }
+  p->off[K_LBM][p->n] = prev;
+  p->grid[K_LBM] = prev;
+  return MC_OK;
+}
+
+mc_status mc_plan_get_lbm_shape(const mc_plan* p, int32_t* cells_per_lane, int32_t* rows_per_cta) {
+  if (!p || !cells_per_lane || !rows_per_cta) return fail(MC_ERR_INVALID, "null argument");
+  *cells_per_lane = p->R[0].vec;
+  *rows_per_cta = p->R[0].lbm_th;
   return MC_OK;
 }
 

@@ -185,8 +185,10 @@ class Record:
 class Plan:
     """A bound plan for a list of rollouts (dims + config + dt + topology each)."""
 
-    def __init__(self, specs, device="cuda"):
-        """specs: list of (H, W, N, pairs(E,2) int32, bending_pairs(B,2) int32, cfg, dt)."""
+    def __init__(self, specs, device="cuda", lbm_shape=None):
+        """specs: list of (H, W, N, pairs(E,2) int32, bending_pairs(B,2) int32, cfg, dt).
+        ``lbm_shape`` = (cells_per_lane, rows_per_cta) of the dense pass (default: the
+        library's choice; ``microcosmos_b200.autotune`` picks one by timing)."""
         _require_cuda()
         lib = _lib.load()
         n = len(specs)
@@ -210,6 +212,8 @@ class Plan:
         self._h = h
         self.n = n
         self.specs = specs
+        if lbm_shape is not None:
+            _lib.check(lib.mc_plan_set_lbm_shape(h, int(lbm_shape[0]), int(lbm_shape[1])))
         nbytes = lib.mc_plan_workspace_bytes(h)
         self.workspace = torch.empty(nbytes + 256, dtype=torch.uint8, device=device)
         base = self.workspace.data_ptr()
@@ -219,9 +223,15 @@ class Plan:
         _lib.check(lib.mc_plan_bind(h, ctypes.c_void_p(self._ws_ptr), nbytes, ctypes.c_void_p(stream)))
 
     @classmethod
-    def for_states(cls, states, cfgs, dts, device="cuda"):
+    def for_states(cls, states, cfgs, dts, device="cuda", lbm_shape=None):
         specs = [(s.H, s.W, s.N, s.pairs, s.bending_pairs, c, d) for s, c, d in zip(states, cfgs, dts)]
-        return cls(specs, device=device)
+        return cls(specs, device=device, lbm_shape=lbm_shape)
+
+    def lbm_shape(self):
+        """(cells_per_lane, rows_per_cta) of the dense pass."""
+        a, b = ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(_lib.load().mc_plan_get_lbm_shape(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def _arrays(self, states, actuations, records):
         n = self.n

@@ -114,3 +114,36 @@ def test_batch_plan_of_uneven_rollouts(lib):
     st, h = _create([(s.H, s.W, s.N, s.pairs, s.bending_pairs, baseline_config(), 0.01) for s in scs])
     assert st == _lib.MC_OK, lib.mc_last_error()
     lib.mc_plan_destroy(h)
+
+
+def test_lbm_shape_setter_validates_and_reports(lib):
+    sc = scenarios.make_scenario(64, 96, 2, 12, seed=0)
+    st, h = _create([(64, 96, sc.N, sc.pairs, sc.bending_pairs, baseline_config(), 0.01)])
+    assert st == _lib.MC_OK
+    a, b = ctypes.c_int32(), ctypes.c_int32()
+    assert lib.mc_plan_get_lbm_shape(h, ctypes.byref(a), ctypes.byref(b)) == _lib.MC_OK
+    assert (a.value, b.value) == (2, 8)  # the library's default
+    assert lib.mc_plan_set_lbm_shape(h, 4, 2) == _lib.MC_OK
+    lib.mc_plan_get_lbm_shape(h, ctypes.byref(a), ctypes.byref(b))
+    assert (a.value, b.value) == (4, 2)
+    assert lib.mc_plan_set_lbm_shape(h, 3, 0) == _lib.MC_ERR_INVALID
+    assert lib.mc_plan_set_lbm_shape(h, 0, 16) == _lib.MC_ERR_INVALID
+    lib.mc_plan_destroy(h)
+    # 4 cells per lane must divide W
+    sc2 = scenarios.make_scenario(64, 66, 1, 10, seed=0)
+    st, h2 = _create([(64, 66, sc2.N, sc2.pairs, sc2.bending_pairs, baseline_config(), 0.01)])
+    assert st == _lib.MC_OK
+    assert lib.mc_plan_set_lbm_shape(h2, 4, 4) == _lib.MC_ERR_UNSUPPORTED
+    lib.mc_plan_destroy(h2)
+
+
+def test_autotune_candidates_respect_widths():
+    from microcosmos_b200 import autotune
+
+    class S:
+        def __init__(self, W):
+            self.W = W
+
+    assert autotune.candidates([S(64), S(128)]) == [(v, r) for v in (1, 2, 4) for r in (2, 4, 8)]
+    assert autotune.candidates([S(64), S(66)]) == [(v, r) for v in (1, 2) for r in (2, 4, 8)]
+    assert autotune.candidates([S(63)]) == [(1, r) for r in (2, 4, 8)]
