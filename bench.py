@@ -215,6 +215,19 @@ def batch_section(args, flush):
     plan.profile(False)
     lbm_ms = prof["lbm"][0] / max(prof["lbm"][1], 1)
     del plan
+    # the same population with the direct-convolution steric filter (opt-in: ~6e-7 rel-L2 from the FFT's)
+    plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs), lbm_shape=shape, steric_method=2)
+    plan.begin(sts, actuations=acts)
+    plan.advance(4, use_graph=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    plan.advance(K, use_graph=True, last=True)
+    e1.record(stream)
+    plan.end()
+    torch.cuda.synchronize()
+    t_direct = e0.elapsed_time(e1) / K
+    del plan
     # plain: one plan per rollout, run sequentially (a bounded subset of the population)
     nplain = min(len(scs), 32)
     t_plain = 0.0
@@ -241,6 +254,8 @@ def batch_section(args, flush):
         "plain_rollouts_per_s": len(scs) / (t_plain_pop / 1e3 * steps),
         "plain_sample": f"{nplain} rollouts, one plan each, {K} graph-launched steps each",
         "speedup_vs_plain": t_plain_pop / t_batch,
+        "direct_steric_filter": {"ms_per_step": t_direct, "mlups": cells / (t_direct / 1e3) / 1e6,
+                                 "note": "opt-in steric_method=2, no L2 flush between steps"},
         "autotune": {"dense_pass_shape": {"cells_per_lane": shape[0], "rows_per_cta": shape[1]},
                      "ms_per_step_by_shape": {f"{v}x{r}": ms for (v, r), ms in shape_ms.items()}},
         "lbm_ms_per_launch": lbm_ms,

@@ -134,6 +134,19 @@ void mc_plan_destroy(mc_plan* plan);
 mc_status mc_plan_set_lbm_shape(mc_plan* plan, int32_t cells_per_lane, int32_t rows_per_cta);
 mc_status mc_plan_get_lbm_shape(const mc_plan* plan, int32_t* cells_per_lane, int32_t* rows_per_cta);
 
+/* How the steric potential's spectral Gaussian (src/microcosmos/utils.py:35-49) is applied:
+ * 1 = FFT along rows, then columns (H, W with prime factors <= 13, at most 4096): the
+ *     reference's operator, to float32 rounding;
+ * 2 = direct circular convolution with the filter's periodic kernel kept to radius 24 (one
+ *     32 x 32 tile per CTA; needs 2 * 24 + 1 <= H, W).  The Nyquist cut-off of the spectral
+ *     Gaussian leaves a ~1e-6 tail in that kernel beyond the Gaussian core, which this
+ *     drops: the field differs from the FFT's by ~6e-7 rel-L2 (sigma = 1.5);
+ * 0 = per rollout, the FFT where it exists, else the direct form (the default).
+ * Only before mc_plan_bind().  mc_plan_steric_method returns 1 (all FFT), 2 (all direct),
+ * 3 (mixed) or 0 (no steric rollout). */
+mc_status mc_plan_set_steric_method(mc_plan* plan, int32_t method);
+int32_t mc_plan_steric_method(const mc_plan* plan);
+
 /* Bytes of device workspace the plan needs (all rollouts). */
 size_t mc_plan_workspace_bytes(const mc_plan* plan);
 

@@ -18,7 +18,9 @@ namespace mc {
 constexpr int kBinTile = 16;       // binning tile edge for the deterministic reductions
 constexpr int kLbmTileX = 128;     // dense LBM CTA tile: 32 lanes x 4 cells
 constexpr int kLbmTileY = 8;      // default LBM tile height (rows per CTA)
-constexpr int kLbmMinTileY = 2;   // smallest tile height a plan may be tuned to       //                    8 rows
+constexpr int kLbmMinTileY = 2;   // smallest tile height a plan may be tuned to
+constexpr int kConvTile = 32;     // steric direct convolution: 32 x 32 outputs per CTA
+constexpr int kConvMaxR = 24;     // largest tap radius of the direct convolution       //                    8 rows
 constexpr int kIbCap = 1024;       // minimum IB bin capacity per 16x16 tile (grown with node density)
 constexpr int kCicCap = 512;       // minimum CIC bin capacity per tile
 constexpr int kMaxBinCap = 8192;   // largest bin capacity (the tile sort keeps 4 x cap words in shared memory)
@@ -54,6 +56,11 @@ struct RDesc {
   const float2* twH;
   const float* gW;    // separable spectral Gaussian / W
   const float* gH;    // ... / H
+  // direct-convolution form of the same filter: the periodic kernel of the spectral
+  // Gaussian along x / y, taps for offsets -R..R (symmetric)
+  const float* conv_gW;
+  const float* conv_gH;
+  int conv_RW, conv_RH, conv_ntx;
   // state (caller buffers)
   float* pos;
   float* vel;
@@ -221,6 +228,7 @@ void launch_ib_finalize(const Launch& L, int parity);
 cudaError_t launch_ib_coop(const Launch& L, int parity);
 cudaError_t ib_coop_blocks_per_sm(int* out);
 void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows);
+void launch_steric_conv(const Launch& L, size_t smem);
 void launch_reaction(const Launch& L, const int* tdev);
 void launch_record_fields(const Launch& L, const int* tdev);
 void launch_unstream(const Launch& L);

@@ -37,7 +37,7 @@ mc_status cuda_fail(cudaError_t e, const char* where) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_FFTR2, K_FFTC2, K_COUNT };
+enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_FFTR2, K_FFTC2, K_SCONV, K_COUNT };
 
 struct Region {
   size_t off = 0;
@@ -57,6 +57,10 @@ struct HostRollout {
   std::vector<int> fW, fH;
   std::vector<float2> twW, twH;
   std::vector<float> gW, gH;
+  std::vector<float> cgW, cgH;  // direct-convolution taps of the steric filter
+  int cRW = 0, cRH = 0;
+  bool fft_ok = false, conv_ok = false, use_conv = false;
+  Region r_cgW, r_cgH;
   int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4, lbm_th = mc::kLbmTileY;
   int ib_cap = 0, c_cap = 0;  // bin capacities (powers of two)
   int logW = -1, logH = -1;   // log2 of power-of-two grid sides (-1: mixed radix path)
@@ -85,7 +89,7 @@ struct mc_plan {
   char* ws = nullptr;
   bool bound = false;
   int any_fluid = 0, any_steric = 0, max_iters = 0;
-  size_t node_smem = 0, fftr_smem = 0, fftc_smem = 0, fftr2_smem = 0, fftc2_smem = 0;
+  size_t node_smem = 0, fftr_smem = 0, fftc_smem = 0, fftr2_smem = 0, fftc2_smem = 0, sconv_smem = 0;
   int node_bs = 32;
   int max_chain = 0, chain_slots = 1;
   int max_k = 0;  // largest IB kernel size of the plan
@@ -128,6 +132,31 @@ bool factorize(int N, std::vector<int>& f) {
   for (int p : ps)
     while (N % p == 0) { f.push_back(p); N /= p; }
   return N == 1 && (int)f.size() <= mc::kFftMaxFactors;
+}
+
+// Periodic kernel of the spectral Gaussian exp(-2 pi^2 sigma^2 f^2) on N points (numpy
+// fftfreq abscissae): g[k] = (1/N) sum_j kf_j cos(2 pi j k / N), even in k.  The filter is
+// cut off at the Nyquist frequency, where it is still exp(-pi^2 sigma^2 / 2) (1.5e-5 for
+// sigma = 1.5), so g has a slowly decaying tail of ~1e-6 g[0] beyond the Gaussian core.
+// Returns the radius R = min(N/2, kConvMaxR) up to which taps are kept (or the radius where
+// |g| first drops below 1e-10 g[0], if that is smaller) and the taps for offsets -R..R.
+// Dropping the tail changes the filtered field by ~1e-6 relative (1.4e-6 rel-L2 measured
+// for sigma = 1.5 at R = 12, 6e-7 at R = 24).
+int conv_taps(int N, double sigma, std::vector<float>& taps) {
+  std::vector<double> g(N / 2 + 1);
+  for (int k = 0; k <= N / 2; ++k) {
+    double s = 0.0;
+    for (int j = 0; j < N; ++j) {
+      const double f = (j < (N + 1) / 2 ? (double)j : (double)(j - N)) / (double)N;
+      s += std::exp(-2.0 * M_PI * M_PI * sigma * sigma * f * f) * std::cos(2.0 * M_PI * (double)j * k / N);
+    }
+    g[k] = s / N;
+  }
+  int R = 0;
+  while (R + 1 <= N / 2 && R + 1 <= mc::kConvMaxR && std::fabs(g[R + 1]) > 1e-10 * std::fabs(g[0])) ++R;
+  taps.clear();
+  for (int k = -R; k <= R; ++k) taps.push_back((float)g[std::abs(k)]);
+  return R;
 }
 
 void fft_tables(int N, double sigma, std::vector<float2>& tw, std::vector<float>& g) {
@@ -367,6 +396,11 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.twH = at<float2>(b, h.r_twH);
   d.gW = at<float>(b, h.r_gW);
   d.gH = at<float>(b, h.r_gH);
+  d.conv_gW = at<float>(b, h.r_cgW);
+  d.conv_gH = at<float>(b, h.r_cgH);
+  d.conv_RW = h.cRW;
+  d.conv_RH = h.cRH;
+  d.conv_ntx = div_up(h.dims.W, mc::kConvTile);
   if (st) {
     d.pos = st->position;
     d.vel = st->velocity;
@@ -477,7 +511,7 @@ mc::Launch L(mc_plan* p, Kind k, cudaStream_t s) {
 const char* const kProfNames[] = {"predict", "cic_bins",  "fft_rows",    "fft_cols", "chain",
                                    "node",    "ib_bins",   "ib_interp",   "ib_spread", "ib_finalize",
                                    "lbm",     "reaction",  "record_fields", "tick",    "steric",
-                                   "stencil", "ib_fused"};
+                                   "stencil", "ib_fused", "steric_conv"};
 constexpr int kNumProf = sizeof(kProfNames) / sizeof(kProfNames[0]);
 
 cudaEvent_t take_event(mc_plan* p) {
@@ -545,6 +579,10 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
     }
     if (p->grid[K_FFTC]) {
       timed(p, 3, s, capture, [&] { mc::launch_fft_cols(L(p, K_FFTC, s), p->fftc_smem); });
+      ++k;
+    }
+    if (p->grid[K_SCONV]) {
+      timed(p, 17, s, capture, [&] { mc::launch_steric_conv(L(p, K_SCONV, s), p->sconv_smem); });
       ++k;
     }
   }
@@ -772,10 +810,27 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       return st;
     }
     if (c.enable_steric) {
-      if (!factorize(D.W, h.fW) || !factorize(D.H, h.fH) || D.W > mc::kFftMaxN || D.H > mc::kFftMaxN) {
-        delete p;
-        return fail(MC_ERR_UNSUPPORTED, "steric FFT needs H, W with prime factors <= 13 and at most 4096");
+      h.cRW = conv_taps(D.W, c.steric_sigma, h.cgW);
+      h.cRH = conv_taps(D.H, c.steric_sigma, h.cgH);
+      h.conv_ok = 2 * h.cRW + 1 <= D.W && 2 * h.cRH + 1 <= D.H;
+      h.fft_ok = factorize(D.W, h.fW) && factorize(D.H, h.fH) && D.W <= mc::kFftMaxN && D.H <= mc::kFftMaxN;
+      h.use_conv = h.conv_ok && !h.fft_ok;
+      if (!h.fft_ok) {
+        h.fW.clear();
+        h.fH.clear();
       }
+      if (!h.conv_ok) {
+        h.cgW.clear();
+        h.cgH.clear();
+      }
+    }
+    if (c.enable_steric && !h.conv_ok && !h.fft_ok) {
+      delete p;
+      return fail(MC_ERR_UNSUPPORTED,
+                  "steric filter: the FFT needs H, W with prime factors <= 13 and at most 4096, the direct "
+                  "convolution a kernel radius below min(H, W) / 2 and 24");
+    }
+    if (c.enable_steric && h.fft_ok) {
       fft_tables(D.W, c.steric_sigma, h.twW, h.gW);
       fft_tables(D.H, c.steric_sigma, h.twH, h.gH);
       auto log2_if_pow2 = [](int v) {
@@ -866,6 +921,8 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.r_twH = lay.take(h.twH.size() * 8);
     h.r_gW = lay.take(h.gW.size() * 4);
     h.r_gH = lay.take(h.gH.size() * 4);
+    h.r_cgW = lay.take(h.cgW.size() * 4);
+    h.r_cgH = lay.take(h.cgH.size() * 4);
     h.r_flags = lay.take(4);
     if (c.enable_fluid) p->any_fluid = 1;
     if (c.enable_steric) p->any_steric = 1;
@@ -916,9 +973,13 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     // kernels serve the allocation-free entry point)
     cnt[K_FFTR] = 0;
     cnt[K_FFTC] = 0;
-    cnt[K_FFTR2] = c.enable_steric ? div_up(div_up(h.dims.H, 2), h.P_r) : 0;
-    cnt[K_FFTC2] = c.enable_steric ? div_up(h.dims.W, 2 * h.P_c) : 0;
-    if (c.enable_steric) {
+    cnt[K_FFTR2] = c.enable_steric && !h.use_conv ? div_up(div_up(h.dims.H, 2), h.P_r) : 0;
+    cnt[K_FFTC2] = c.enable_steric && !h.use_conv ? div_up(h.dims.W, 2 * h.P_c) : 0;
+    cnt[K_SCONV] = c.enable_steric && h.use_conv ? div_up(h.dims.W, mc::kConvTile) * div_up(h.dims.H, mc::kConvTile) : 0;
+    if (h.conv_ok)
+      p->sconv_smem = std::max(p->sconv_smem, (size_t)(mc::kConvTile + 2 * h.cRH) *
+                                                  (mc::kConvTile + 2 * h.cRW + mc::kConvTile) * sizeof(float));
+    if (c.enable_steric && h.fft_ok) {
       p->fftr2_smem = std::max(p->fftr2_smem, (size_t)2 * h.P_r * h.dims.W * sizeof(float2));
       p->fftc2_smem = std::max(p->fftc2_smem, (size_t)2 * h.P_c * (h.dims.H + 1) * sizeof(float2));
     }
@@ -929,9 +990,9 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       mcb = std::max(mcb, h.max_cb);
     }
     p->max_chain = std::max(p->max_chain, h.max_chain);
-    p->fftr_smem = std::max(p->fftr_smem, c.enable_steric ? (size_t)3 * h.dims.W * sizeof(float2) + h.dims.W * sizeof(float) : 0);
+    p->fftr_smem = std::max(p->fftr_smem, c.enable_steric && h.fft_ok ? (size_t)3 * h.dims.W * sizeof(float2) + h.dims.W * sizeof(float) : 0);
     p->fftc_smem = std::max(p->fftc_smem,
-                            c.enable_steric ? (size_t)(2 * mc::kFftColsPerCta + 1) * h.dims.H * sizeof(float2) + h.dims.H * sizeof(float) : 0);
+                            c.enable_steric && h.fft_ok ? (size_t)(2 * mc::kFftColsPerCta + 1) * h.dims.H * sizeof(float2) + h.dims.H * sizeof(float) : 0);
   }
   for (int k = 0; k < K_COUNT; ++k) p->grid[k] = p->off[k][n];
   p->coop_cap_checked = false;
@@ -947,6 +1008,48 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
   p->desc.resize(n);
   *out = p;
   return MC_OK;
+}
+
+mc_status mc_plan_set_steric_method(mc_plan* p, int32_t method) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (p->bound) return fail(MC_ERR_INVALID, "the steric filter method is set before mc_plan_bind()");
+  if (method < 0 || method > 2) return fail(MC_ERR_INVALID, "method must be 0 (auto), 1 (FFT) or 2 (direct)");
+  for (auto& h : p->R) {
+    if (!h.cfg.enable_steric) continue;
+    if (method == 1 && !h.fft_ok) return fail(MC_ERR_UNSUPPORTED, "a rollout's grid has no FFT plan");
+    if (method == 2 && !h.conv_ok) return fail(MC_ERR_UNSUPPORTED, "a rollout's grid is too small for the direct filter");
+  }
+  int o1 = 0, o2 = 0, o3 = 0;
+  for (int i = 0; i < p->n; ++i) {
+    HostRollout& h = p->R[i];
+    h.use_conv = method == 0 ? (h.conv_ok && !h.fft_ok) : method == 2;
+    p->off[K_FFTR2][i] = o1;
+    p->off[K_FFTC2][i] = o2;
+    p->off[K_SCONV][i] = o3;
+    if (!h.cfg.enable_steric) continue;
+    if (h.use_conv) {
+      o3 += div_up(h.dims.W, mc::kConvTile) * div_up(h.dims.H, mc::kConvTile);
+    } else {
+      o1 += div_up(div_up(h.dims.H, 2), h.P_r);
+      o2 += div_up(h.dims.W, 2 * h.P_c);
+    }
+  }
+  p->off[K_FFTR2][p->n] = o1;
+  p->off[K_FFTC2][p->n] = o2;
+  p->off[K_SCONV][p->n] = o3;
+  p->grid[K_FFTR2] = o1;
+  p->grid[K_FFTC2] = o2;
+  p->grid[K_SCONV] = o3;
+  return MC_OK;
+}
+
+int32_t mc_plan_steric_method(const mc_plan* p) {
+  if (!p) return -1;
+  int conv = 0, fft = 0;
+  for (auto& h : p->R)
+    if (h.cfg.enable_steric) (h.use_conv ? conv : fft) = 1;
+  return conv && fft ? 3 : conv ? 2 : fft ? 1 : 0;
 }
 
 mc_status mc_plan_set_lbm_shape(mc_plan* p, int32_t cells_per_lane, int32_t rows_per_cta) {
@@ -1029,6 +1132,8 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
     MC_CUDA(up(h.r_twH, h.twH.data(), h.twH.size() * 8));
     MC_CUDA(up(h.r_gW, h.gW.data(), h.gW.size() * 4));
     MC_CUDA(up(h.r_gH, h.gH.data(), h.gH.size() * 4));
+    MC_CUDA(up(h.r_cgW, h.cgW.data(), h.cgW.size() * 4));
+    MC_CUDA(up(h.r_cgH, h.cgH.data(), h.cgH.size() * 4));
     fill_desc(p, i, nullptr, nullptr, nullptr);
   }
   for (int k = 0; k < K_COUNT; ++k) MC_CUDA(up(p->r_off[k], p->off[k].data(), p->off[k].size() * 4));
@@ -1042,7 +1147,7 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
     MC_CUDA(cudaGetDevice(&dev));
     MC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (p->node_smem > (size_t)optin || p->fftr_smem > (size_t)optin || p->fftc_smem > (size_t)optin ||
-        p->fftr2_smem > (size_t)optin || p->fftc2_smem + 1024 > (size_t)optin)
+        p->fftr2_smem > (size_t)optin || p->fftc2_smem + 1024 > (size_t)optin || p->sconv_smem > (size_t)optin)
       return fail(MC_ERR_UNSUPPORTED, "shared memory needed by the plan exceeds the device limit");
     MC_CUDA(mc::node_set_smem((size_t)optin));
     MC_CUDA(mc::tiles_set_smem((size_t)optin));

@@ -442,4 +442,54 @@ cudaError_t fft_set_smem(size_t rows, size_t cols) {
   return cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cols);
 }
 
+
+// The spectral Gaussian of update_steric_potential (src/microcosmos/utils.py:35-49) as a
+// direct circular convolution: real(ifft2(fft2(dep) * exp(-2 pi^2 sigma^2 (r^2 + c^2))))
+// is separable, and along each axis equals the circular convolution of dep with the
+// filter's periodic kernel g[k] = (1/N) sum_j exp(-2 pi^2 sigma^2 f_j^2) cos(2 pi j k / N)
+// (computed in double on the host).  Taps beyond radius R are below 1e-10 of g[0] and are
+// dropped.  One CTA: a 32 x 32 output tile, its input tile with an R halo staged in
+// shared memory (wrapped), the x pass into a second shared buffer, then the y pass.
+__global__ void __launch_bounds__(256) k_steric_conv(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int lb = blockIdx.x - off[r];
+  const int tx = lb % d.conv_ntx, ty = lb / d.conv_ntx;
+  const int H = d.H, W = d.W, Rx = d.conv_RW, Ry = d.conv_RH;
+  const int iw = kConvTile + 2 * Rx, ih = kConvTile + 2 * Ry;
+  extern __shared__ float conv_sm[];
+  float* in = conv_sm;             // ih x iw
+  float* mid = conv_sm + ih * iw;  // ih x kConvTile
+  const int x0 = tx * kConvTile - Rx, y0 = ty * kConvTile - Ry;
+  const int nt = blockDim.x;
+  for (int i = threadIdx.x; i < ih * iw; i += nt) {
+    const int yy = i / iw, xx = i - yy * iw;
+    in[i] = d.dep[(size_t)imod_floor(y0 + yy, H) * W + imod_floor(x0 + xx, W)];
+  }
+  __syncthreads();
+  const float* gx = d.conv_gW;
+  for (int i = threadIdx.x; i < ih * kConvTile; i += nt) {
+    const int yy = i / kConvTile, xx = i - yy * kConvTile;
+    const float* row = in + yy * iw + xx;
+    float a = 0.0f;
+    for (int k = 0; k <= 2 * Rx; ++k) a = a + gx[k] * row[2 * Rx - k];
+    mid[i] = a;
+  }
+  __syncthreads();
+  const float* gy = d.conv_gH;
+  for (int i = threadIdx.x; i < kConvTile * kConvTile; i += nt) {
+    const int yy = i / kConvTile, xx = i - yy * kConvTile;
+    const int oy = ty * kConvTile + yy, ox = tx * kConvTile + xx;
+    if (oy >= H || ox >= W) continue;
+    const float* col = mid + yy * kConvTile + xx;
+    float a = 0.0f;
+    for (int k = 0; k <= 2 * Ry; ++k) a = a + gy[k] * col[(2 * Ry - k) * kConvTile];
+    d.steric[(size_t)oy * W + ox] = a;
+  }
+}
+
+void launch_steric_conv(const Launch& L, size_t smem) {
+  k_steric_conv<<<L.grid, 256, smem, L.s>>>(L.d, L.off, L.n);
+}
+
 }  // namespace mc

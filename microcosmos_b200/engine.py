@@ -185,10 +185,12 @@ class Record:
 class Plan:
     """A bound plan for a list of rollouts (dims + config + dt + topology each)."""
 
-    def __init__(self, specs, device="cuda", lbm_shape=None):
+    def __init__(self, specs, device="cuda", lbm_shape=None, steric_method=0):
         """specs: list of (H, W, N, pairs(E,2) int32, bending_pairs(B,2) int32, cfg, dt).
         ``lbm_shape`` = (cells_per_lane, rows_per_cta) of the dense pass (default: the
-        library's choice; ``microcosmos_b200.autotune`` picks one by timing)."""
+        library's choice; ``microcosmos_b200.autotune`` picks one by timing).
+        ``steric_method``: 0 = per rollout (direct convolution where it applies, else
+        FFT), 1 = FFT, 2 = direct convolution."""
         _require_cuda()
         lib = _lib.load()
         n = len(specs)
@@ -214,6 +216,8 @@ class Plan:
         self.specs = specs
         if lbm_shape is not None:
             _lib.check(lib.mc_plan_set_lbm_shape(h, int(lbm_shape[0]), int(lbm_shape[1])))
+        if steric_method:
+            _lib.check(lib.mc_plan_set_steric_method(h, int(steric_method)))
         nbytes = lib.mc_plan_workspace_bytes(h)
         self.workspace = torch.empty(nbytes + 256, dtype=torch.uint8, device=device)
         base = self.workspace.data_ptr()
@@ -223,9 +227,13 @@ class Plan:
         _lib.check(lib.mc_plan_bind(h, ctypes.c_void_p(self._ws_ptr), nbytes, ctypes.c_void_p(stream)))
 
     @classmethod
-    def for_states(cls, states, cfgs, dts, device="cuda", lbm_shape=None):
+    def for_states(cls, states, cfgs, dts, device="cuda", lbm_shape=None, steric_method=0):
         specs = [(s.H, s.W, s.N, s.pairs, s.bending_pairs, c, d) for s, c, d in zip(states, cfgs, dts)]
-        return cls(specs, device=device, lbm_shape=lbm_shape)
+        return cls(specs, device=device, lbm_shape=lbm_shape, steric_method=steric_method)
+
+    def steric_method(self):
+        """1: FFT, 2: direct convolution, 3: mixed across rollouts, 0: no steric."""
+        return int(_lib.load().mc_plan_steric_method(self._h))
 
     def lbm_shape(self):
         """(cells_per_lane, rows_per_cta) of the dense pass."""

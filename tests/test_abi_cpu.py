@@ -91,12 +91,18 @@ def test_plan_rejects_unsupported_config(lib):
     st, _ = _create([(32, 32, sc.N, sc.pairs, sc.bending_pairs,
                       dataclasses.replace(baseline_config(), synthetic_node_width=1.0), 0.01)])
     assert st == _lib.MC_ERR_UNSUPPORTED
-    # steric FFT sizes need prime factors <= 13
+    # 34 x 34: no FFT plan (prime factor 17) and too small for the direct filter (radius 17)
     st, _ = _create([(34, 34, sc.N, sc.pairs, sc.bending_pairs, baseline_config(), 0.01)])
     assert st == _lib.MC_ERR_UNSUPPORTED
     st, _ = _create([(34, 34, sc.N, sc.pairs, sc.bending_pairs,
                       dataclasses.replace(baseline_config(), enable_steric=False), 0.01)])
     assert st == _lib.MC_OK
+    # 51 x 51 has no FFT plan: the direct filter
+    st, h = _create([(51, 51, sc.N, sc.pairs, sc.bending_pairs, baseline_config(), 0.01)])
+    assert st == _lib.MC_OK
+    assert lib.mc_plan_steric_method(h) == 2
+    assert lib.mc_plan_set_steric_method(h, 1) == _lib.MC_ERR_UNSUPPORTED
+    lib.mc_plan_destroy(h)
     st, _ = _create([(32, 32, sc.N, sc.pairs, sc.bending_pairs, baseline_config(), 0.0)])
     assert st == _lib.MC_ERR_INVALID
 
