@@ -184,8 +184,10 @@ def batch_section(args, flush):
     sts = [DeviceState.from_scenario(s) for s in scs]
     acts = [Actuation.from_scenario(s) for s in scs]
     from microcosmos_b200 import autotune
-    shape, shape_ms = autotune.tune(sts, [cfg] * len(scs), [0.01] * len(scs), actuations=acts, steps=10, warmup=4)
-    plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs), lbm_shape=shape)
+    tuned, tune_ms = autotune.tune(sts, [cfg] * len(scs), [0.01] * len(scs), actuations=acts, steps=10, warmup=4)
+    shape = tuned["lbm_shape"]
+    plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs), lbm_shape=shape,
+                           fft_values=tuned["fft_values"])
     stream = torch.cuda.current_stream()
     plan.begin(sts, actuations=acts)
     plan.advance(6, use_graph=True)
@@ -216,7 +218,8 @@ def batch_section(args, flush):
     lbm_ms = prof["lbm"][0] / max(prof["lbm"][1], 1)
     del plan
     # the same population with the direct-convolution steric filter (opt-in: ~6e-7 rel-L2 from the FFT's)
-    plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs), lbm_shape=shape, steric_method=2)
+    plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs), lbm_shape=shape, steric_method=2,
+                           fft_values=tuned["fft_values"])
     plan.begin(sts, actuations=acts)
     plan.advance(4, use_graph=True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -257,7 +260,7 @@ def batch_section(args, flush):
         "direct_steric_filter": {"ms_per_step": t_direct, "mlups": cells / (t_direct / 1e3) / 1e6,
                                  "note": "opt-in steric_method=2, no L2 flush between steps"},
         "autotune": {"dense_pass_shape": {"cells_per_lane": shape[0], "rows_per_cta": shape[1]},
-                     "ms_per_step_by_shape": {f"{v}x{r}": ms for (v, r), ms in shape_ms.items()}},
+                     "fft_values_per_thread": tuned["fft_values"], "ms_per_step_by_candidate": tune_ms},
         "lbm_ms_per_launch": lbm_ms,
         "kernels_ms_per_step": {k: ms / 10 for k, (ms, n) in prof.items() if n}, "lbm_frac_of_peak": BYTES_PER_CELL * cells / (lbm_ms / 1e3) / 1e9 / 6541.5,
         "roofline_frac_mlups": cells / (t_batch / 1e3) / 1e6 / (6541.5e9 / BYTES_PER_CELL / 1e6),

@@ -147,6 +147,15 @@ mc_status mc_plan_get_lbm_shape(const mc_plan* plan, int32_t* cells_per_lane, in
 mc_status mc_plan_set_steric_method(mc_plan* plan, int32_t method);
 int32_t mc_plan_steric_method(const mc_plan* plan);
 
+/* Values each thread holds in registers in the FFT kernels of power-of-two sides (4, 8 or
+ * 16; 0 = the library's choice from the plan's total size).  More values per thread take
+ * fewer instructions per value, fewer give more threads: small single rollouts want 4,
+ * large batches 16.  Results do not depend on it beyond float32 rounding of the transform
+ * order.  Only before mc_plan_bind(); microcosmos_b200.autotune picks it by timing.  No
+ * counterpart in the reference. */
+mc_status mc_plan_set_fft_values_per_thread(mc_plan* plan, int32_t values);
+int32_t mc_plan_fft_values_per_thread(const mc_plan* plan);
+
 /* Bytes of device workspace the plan needs (all rollouts). */
 size_t mc_plan_workspace_bytes(const mc_plan* plan);
 

@@ -1,13 +1,17 @@
-"""Autotuner for the tile shape of the dense stream+collide pass.
+"""Autotuner for the launch shapes of a plan.
 
-The dense pass is the one kernel whose CTA shape is a free choice: each CTA covers
-32 x cells_per_lane columns (1, 2 or 4 cells per thread, vector loads/stores) by
-rows_per_cta rows (2, 4 or 8).  Which shape is fastest depends on the rollout sizes of
-a plan (grid widths, how many CTAs a step launches, how many tiles carry IB forcing),
-so the tuner times whole graph-replayed steps of the actual plan for every candidate
-on scratch copies of the states and keeps the fastest.  Results are cached per plan
-signature (sizes, configs, dt) for the life of the process.  The shape changes no
-result, only the time.
+Two kernels have a free shape:
+  * the dense stream+collide pass: each CTA covers 32 x cells_per_lane columns (1, 2 or 4
+    cells per thread, vector loads/stores) by rows_per_cta rows (2, 4 or 8);
+  * the power-of-two FFT kernels of the steric filter: each thread holds 4, 8 or 16
+    values in registers (more values: fewer instructions per value; fewer: more threads).
+Which shape is fastest depends on the rollout sizes of a plan (grid widths, how many CTAs
+a step launches, how many tiles carry IB forcing), so the tuner times whole
+graph-replayed steps of the actual plan on scratch copies of the states: first the FFT
+shape with the default dense-pass shape, then the dense-pass shapes with the chosen FFT
+shape.  Results are cached per plan signature (sizes, configs, dt) for the life of the
+process.  The dense-pass shape changes no result; the FFT shape changes the float32
+rounding of the transform only.
 """
 from __future__ import annotations
 
@@ -20,8 +24,9 @@ from .engine import DeviceState, Plan
 
 CELLS_PER_LANE = (1, 2, 4)
 ROWS_PER_CTA = (2, 4, 8)
+FFT_VALUES = (4, 8, 16)
 
-_cache: dict[str, tuple[tuple[int, int], dict]] = {}
+_cache: dict[str, tuple[dict, dict]] = {}
 
 
 def signature(states, cfgs, dts) -> str:
@@ -46,33 +51,48 @@ def _clone(s: DeviceState) -> DeviceState:
                                      if isinstance(getattr(s, f.name), torch.Tensor)})
 
 
-def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, use_cache=True):
-    """Time ``steps`` graph-replayed steps of the plan for every candidate shape and return
-    ``(best_shape, {shape: ms_per_step})``.  The caller's states are not modified."""
+def _time(scratch, cfgs, dts, actuations, steps, warmup, **shape):
+    plan = Plan.for_states(scratch, cfgs, dts, **shape)
+    plan.begin(scratch, actuations=actuations)
+    plan.advance(warmup, use_graph=True)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    plan.advance(steps, use_graph=True, last=True)
+    b.record()
+    plan.end()
+    torch.cuda.synchronize()
+    plan.close()
+    return a.elapsed_time(b) / steps
+
+
+def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, fft_values=None, use_cache=True):
+    """Time ``steps`` graph-replayed steps of the plan for the candidate shapes and return
+    ``(best, timings)``: best = {"lbm_shape": (cells_per_lane, rows_per_cta),
+    "fft_values": 4 | 8 | 16}, timings = {label: ms per step}.  The caller's states are
+    not modified."""
     key = signature(states, cfgs, dts)
     if use_cache and key in _cache:
         return _cache[key]
     scratch = [_clone(s) for s in states]
     timings = {}
+    steric = any(getattr(c, "enable_steric", True) for c in cfgs)
+    fft_best = 0
+    if steric:
+        ft = {}
+        for e in (fft_values or FFT_VALUES):
+            ft[e] = _time(scratch, cfgs, dts, actuations, steps, warmup, fft_values=e)
+            timings[f"fft{e}"] = ft[e]
+        fft_best = min(ft, key=ft.get)
+    lt = {}
     for shape in (shapes or candidates(states)):
-        plan = Plan.for_states(scratch, cfgs, dts, lbm_shape=shape)
-        plan.begin(scratch, actuations=actuations)
-        plan.advance(warmup, use_graph=True)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        plan.advance(steps, use_graph=True, last=True)
-        b.record()
-        plan.end()
-        torch.cuda.synchronize()
-        timings[shape] = a.elapsed_time(b) / steps
-        plan.close()
-        del plan
-    best = min(timings, key=timings.get)
+        lt[shape] = _time(scratch, cfgs, dts, actuations, steps, warmup, lbm_shape=shape, fft_values=fft_best)
+        timings[f"lbm{shape[0]}x{shape[1]}"] = lt[shape]
+    best = {"lbm_shape": min(lt, key=lt.get), "fft_values": fft_best}
     _cache[key] = (best, timings)
     return best, timings
 
 
 def tuned_plan(states, cfgs, dts, actuations=None, **kw) -> Plan:
-    """A plan for these rollouts with the autotuned dense-pass tile shape."""
+    """A plan for these rollouts with the autotuned launch shapes."""
     best, _ = tune(states, cfgs, dts, actuations=actuations, **kw)
-    return Plan.for_states(states, cfgs, dts, lbm_shape=best)
+    return Plan.for_states(states, cfgs, dts, lbm_shape=best["lbm_shape"], fft_values=best["fft_values"])

@@ -37,7 +37,14 @@ mc_status cuda_fail(cudaError_t e, const char* where) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_FFTR2, K_FFTC2, K_SCONV, K_COUNT };
+enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16, K_COUNT };
+
+// CTAs of the steric filter kernels for one rollout: the radix-16 register kernels for
+// power-of-two sides >= 16, the mixed-radix Stockham kernels for the other FFT sides, or
+// the direct convolution.
+struct StericCtas {
+  int fftr2 = 0, fftc2 = 0, sconv = 0, fr16 = 0, fc16 = 0;
+};
 
 struct Region {
   size_t off = 0;
@@ -93,6 +100,7 @@ struct mc_plan {
   int node_bs = 32;
   int max_chain = 0, chain_slots = 1;
   int max_k = 0;  // largest IB kernel size of the plan
+  int fft_e = 4;  // values per thread of the register-radix FFT kernels
   bool use_coop = false, coop_cap_checked = false;
   bool fused_ib = false;  // mc_plan_set_fused_ib (separate launches measured faster)
   bool coop_possible = false;
@@ -551,6 +559,50 @@ void timed(mc_plan* p, int kind, cudaStream_t s, bool capture, F&& launch) {
 // pipeline(t+1) depends only on tail(t), so it runs on a second stream concurrently with
 // lbm(t); ib(t+1) joins both.  Per-step field recording needs lbm(t) before tail(t)'s
 // field copy and before pipeline(t+1) rewrites the steric field, so it runs sequentially.
+// e: values per thread of the register-radix kernels (4, 8 or 16); a side of length N takes
+// them when it is a power of two with E <= N <= 256 E
+StericCtas steric_ctas(const HostRollout& h, int e) {
+  StericCtas c;
+  if (!h.cfg.enable_steric) return c;
+  if (h.use_conv) {
+    c.sconv = div_up(h.dims.W, mc::kConvTile) * div_up(h.dims.H, mc::kConvTile);
+    return c;
+  }
+  const int W = h.dims.W, H = h.dims.H;
+  if (h.logW >= 4 && W >= e && W <= 256 * e) c.fr16 = div_up(div_up(H, 2), 256 * e / W);
+  else c.fftr2 = div_up(div_up(H, 2), h.P_r);
+  if (h.logH >= 4 && H >= e && H <= 256 * e) c.fc16 = div_up(div_up(W, 2), 4096 / H);
+  else c.fftc2 = div_up(W, 2 * h.P_c);
+  return c;
+}
+
+// Values per thread of the register-radix FFT kernels for a plan: enough threads to fill
+// the GPU (148 SMs x 1024) with the fewest instructions per value.
+int default_fft_values(const std::vector<HostRollout>& R) {
+  long long cplx = 0;
+  for (auto& h : R)
+    if (h.cfg.enable_steric && !h.use_conv) cplx += (long long)h.dims.H * h.dims.W / 2;
+  const long long fill = 148LL * 1024;
+  if (cplx >= 16 * fill) return 16;
+  if (cplx >= 8 * fill) return 8;
+  return 4;
+}
+
+void recount_steric(mc_plan* p);
+
+void recount_steric(mc_plan* p) {
+  for (int k : {K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16}) p->off[k][0] = 0;
+  for (int i = 0; i < p->n; ++i) {
+    const StericCtas c = steric_ctas(p->R[i], p->fft_e);
+    p->off[K_FFTR2][i + 1] = p->off[K_FFTR2][i] + c.fftr2;
+    p->off[K_FFTC2][i + 1] = p->off[K_FFTC2][i] + c.fftc2;
+    p->off[K_SCONV][i + 1] = p->off[K_SCONV][i] + c.sconv;
+    p->off[K_FR16][i + 1] = p->off[K_FR16][i] + c.fr16;
+    p->off[K_FC16][i + 1] = p->off[K_FC16][i] + c.fc16;
+  }
+  for (int k : {K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16}) p->grid[k] = p->off[k][p->n];
+}
+
 int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
   int* tdev = at<int>(p->ws, p->r_tdev);
   int64_t k = 0;
@@ -565,12 +617,20 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
       mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_cic), at<int>(p->ws, p->r_wl_ctl) + 1, 1, 0, p->c_capS);
     });
     k += 1;
+    if (p->grid[K_FR16]) {
+      timed(p, 2, s, capture, [&] { mc::launch_fftreg_rows(L(p, K_FR16, s), p->fft_e); });
+      ++k;
+    }
     if (p->grid[K_FFTR2]) {
       timed(p, 2, s, capture, [&] { mc::launch_fft_rows_p2(L(p, K_FFTR2, s), p->fftr2_smem); });
       ++k;
     }
     if (p->grid[K_FFTR]) {
       timed(p, 2, s, capture, [&] { mc::launch_fft_rows(L(p, K_FFTR, s), p->fftr_smem); });
+      ++k;
+    }
+    if (p->grid[K_FC16]) {
+      timed(p, 3, s, capture, [&] { mc::launch_fftreg_cols(L(p, K_FC16, s), p->fft_e); });
       ++k;
     }
     if (p->grid[K_FFTC2]) {
@@ -973,9 +1033,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     // kernels serve the allocation-free entry point)
     cnt[K_FFTR] = 0;
     cnt[K_FFTC] = 0;
-    cnt[K_FFTR2] = c.enable_steric && !h.use_conv ? div_up(div_up(h.dims.H, 2), h.P_r) : 0;
-    cnt[K_FFTC2] = c.enable_steric && !h.use_conv ? div_up(h.dims.W, 2 * h.P_c) : 0;
-    cnt[K_SCONV] = c.enable_steric && h.use_conv ? div_up(h.dims.W, mc::kConvTile) * div_up(h.dims.H, mc::kConvTile) : 0;
+    cnt[K_FFTR2] = cnt[K_FFTC2] = cnt[K_SCONV] = cnt[K_FR16] = cnt[K_FC16] = 0;  // recount_steric
     if (h.conv_ok)
       p->sconv_smem = std::max(p->sconv_smem, (size_t)(mc::kConvTile + 2 * h.cRH) *
                                                   (mc::kConvTile + 2 * h.cRW + mc::kConvTile) * sizeof(float));
@@ -995,6 +1053,8 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
                             c.enable_steric && h.fft_ok ? (size_t)(2 * mc::kFftColsPerCta + 1) * h.dims.H * sizeof(float2) + h.dims.H * sizeof(float) : 0);
   }
   for (int k = 0; k < K_COUNT; ++k) p->grid[k] = p->off[k][n];
+  p->fft_e = default_fft_values(p->R);
+  recount_steric(p);
   p->coop_cap_checked = false;
   p->node_smem = (size_t)(2 * mcn + 4 * mce + 3 * mcb) * sizeof(float);
   p->chain_slots = 1;
@@ -1010,6 +1070,19 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
   return MC_OK;
 }
 
+mc_status mc_plan_set_fft_values_per_thread(mc_plan* p, int32_t values) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (p->bound) return fail(MC_ERR_INVALID, "the FFT shape is set before mc_plan_bind()");
+  if (values != 0 && values != 4 && values != 8 && values != 16)
+    return fail(MC_ERR_INVALID, "values per thread must be 0 (default), 4, 8 or 16");
+  p->fft_e = values ? values : default_fft_values(p->R);
+  recount_steric(p);
+  return MC_OK;
+}
+
+int32_t mc_plan_fft_values_per_thread(const mc_plan* p) { return p ? p->fft_e : 0; }
+
 mc_status mc_plan_set_steric_method(mc_plan* p, int32_t method) {
   g_err.clear();
   if (!p) return fail(MC_ERR_INVALID, "null plan");
@@ -1020,27 +1093,11 @@ mc_status mc_plan_set_steric_method(mc_plan* p, int32_t method) {
     if (method == 1 && !h.fft_ok) return fail(MC_ERR_UNSUPPORTED, "a rollout's grid has no FFT plan");
     if (method == 2 && !h.conv_ok) return fail(MC_ERR_UNSUPPORTED, "a rollout's grid is too small for the direct filter");
   }
-  int o1 = 0, o2 = 0, o3 = 0;
   for (int i = 0; i < p->n; ++i) {
     HostRollout& h = p->R[i];
     h.use_conv = method == 0 ? (h.conv_ok && !h.fft_ok) : method == 2;
-    p->off[K_FFTR2][i] = o1;
-    p->off[K_FFTC2][i] = o2;
-    p->off[K_SCONV][i] = o3;
-    if (!h.cfg.enable_steric) continue;
-    if (h.use_conv) {
-      o3 += div_up(h.dims.W, mc::kConvTile) * div_up(h.dims.H, mc::kConvTile);
-    } else {
-      o1 += div_up(div_up(h.dims.H, 2), h.P_r);
-      o2 += div_up(h.dims.W, 2 * h.P_c);
-    }
   }
-  p->off[K_FFTR2][p->n] = o1;
-  p->off[K_FFTC2][p->n] = o2;
-  p->off[K_SCONV][p->n] = o3;
-  p->grid[K_FFTR2] = o1;
-  p->grid[K_FFTC2] = o2;
-  p->grid[K_SCONV] = o3;
+  recount_steric(p);
   return MC_OK;
 }
 

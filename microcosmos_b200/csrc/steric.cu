@@ -492,4 +492,248 @@ void launch_steric_conv(const Launch& L, size_t smem) {
   k_steric_conv<<<L.grid, 256, smem, L.s>>>(L.d, L.off, L.n);
 }
 
+
+// ---------------------------------------------------------------- register-radix path
+// Power-of-two lengths: G = N / E threads per transform, each holding E = 4, 8 or 16
+// complex values in registers.  A Stockham pass of radix R (E, or a smaller power of two
+// for the last pass) loads R-strided operands from shared memory, twiddles them, runs an
+// R-point DFT in registers and stores the autosorted result back in place: a length-1024
+// transform takes three shared-memory passes with E = 16 (16, 16, 4), five with E = 4.
+// Fewer values per thread give more threads for small problems; more give fewer
+// instructions per value for large batches.  Shared-memory addresses are padded by one
+// element every 16 (a -> a + a / 16) so the strided stores of the first pass spread over
+// the banks.  Twiddles are read from the float64-derived root table.
+
+__device__ __forceinline__ int pad16(int a) { return a + (a >> 4); }
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }  // a * (-i)
+
+// cos(2 pi k / 16), sin(2 pi k / 16) for k = 0..3 (the forward root is cos - i sin)
+constexpr float kC16[4] = {1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f};
+constexpr float kS16[4] = {0.0f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128674f};
+
+// a * exp(-2 pi i e / 16) for a compile-time exponent e in 0..15
+template <int E>
+__device__ __forceinline__ float2 rot16(float2 a) {
+  constexpr int e = E & 15;
+  if (e == 0) return a;
+  if (e == 4) return mul_mi(a);
+  if (e == 8) return make_float2(-a.x, -a.y);
+  if (e == 12) return make_float2(-a.y, a.x);
+  constexpr int q = e & 3, h = e >> 2;  // angle = h * 90 + q * 22.5 degrees
+  const float c = kC16[q], sn = kS16[q];
+  float2 r = make_float2(a.x * c + a.y * sn, a.y * c - a.x * sn);  // a * (c - i s)
+  if (h == 1) return mul_mi(r);
+  if (h == 2) return make_float2(-r.x, -r.y);
+  if (h == 3) return make_float2(-r.y, r.x);
+  return r;
+}
+
+__device__ __forceinline__ void dft2(float2& a, float2& b) {
+  const float2 t = a;
+  a = cadd(t, b);
+  b = csub(t, b);
+}
+
+__device__ __forceinline__ void dft4(float2& a, float2& b, float2& c, float2& d) {
+  const float2 t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), t3 = mul_mi(csub(b, d));
+  a = cadd(t0, t2);
+  c = csub(t0, t2);
+  b = cadd(t1, t3);
+  d = csub(t1, t3);
+}
+
+// R-point forward DFT of v[0..R-1] in registers; X[k] ends in v[perm(k)]:
+// R = 2, 4: natural order; R = 8: X[k2 + 4 k1] in v[2 k2 + k1]; R = 16: X[k2 + 4 k1] in v[4 k2 + k1].
+template <int R>
+__device__ __forceinline__ void dft_reg(float2* v) {
+  if constexpr (R == 2) {
+    dft2(v[0], v[1]);
+  } else if constexpr (R == 4) {
+    dft4(v[0], v[1], v[2], v[3]);
+  } else if constexpr (R == 8) {
+    // n = n1 + 2 n2: length-4 DFTs over n2, twiddle W8^(n1 k2), length-2 DFTs over n1
+    dft4(v[0], v[2], v[4], v[6]);
+    dft4(v[1], v[3], v[5], v[7]);
+    v[3] = rot16<2>(v[3]);
+    v[5] = rot16<4>(v[5]);
+    v[7] = rot16<6>(v[7]);
+    dft2(v[0], v[1]);
+    dft2(v[2], v[3]);
+    dft2(v[4], v[5]);
+    dft2(v[6], v[7]);
+  } else {
+    // n = n1 + 4 n2: length-4 DFTs over n2, twiddle W16^(n1 k2), length-4 DFTs over n1
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) dft4(v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12]);
+    v[5] = rot16<1>(v[5]);
+    v[9] = rot16<2>(v[9]);
+    v[13] = rot16<3>(v[13]);
+    v[6] = rot16<2>(v[6]);
+    v[10] = rot16<4>(v[10]);
+    v[14] = rot16<6>(v[14]);
+    v[7] = rot16<3>(v[7]);
+    v[11] = rot16<6>(v[11]);
+    v[15] = rot16<9>(v[15]);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) dft4(v[4 * k2], v[4 * k2 + 1], v[4 * k2 + 2], v[4 * k2 + 3]);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ constexpr int dft_slot(int k) {
+  if (R == 8) return 2 * (k & 3) + (k >> 2);
+  if (R == 16) return 4 * (k & 3) + (k >> 2);
+  return k;
+}
+
+// One in-place Stockham pass of radix R over a padded buffer of N = 2^logN values,
+// G = N / E threads (local index lt) holding E values each, Ns = 2^logNs.
+template <int E, int R>
+__device__ __forceinline__ void pass_reg(float2* buf, int logN, int logNs, int lt, const float2* __restrict__ tw) {
+  constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
+  constexpr int LE = E == 4 ? 2 : E == 8 ? 3 : 4;
+  constexpr int C = E / R;  // butterflies per thread
+  const int G = 1 << (logN - LE);
+  const int S = 1 << (logN - LR);  // butterflies in the pass
+  const int Ns = 1 << logNs;
+  const int tsh = logN - logNs - LR;  // twiddle index step as a shift
+  float2 v[E];
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int j = lt + c * G;
+    const int k = j & (Ns - 1);
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      float2 a = buf[pad16(j + m * S)];
+      if (m > 0 && k > 0) a = cmul(a, __ldg(tw + ((m * k) << tsh)));
+      v[c * R + m] = a;
+    }
+    dft_reg<R>(v + c * R);
+  }
+  (void)S;
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int j = lt + c * G;
+    const int k = j & (Ns - 1);
+    const int dst = ((j - k) << LR) + k;
+#pragma unroll
+    for (int m = 0; m < R; ++m) buf[pad16(dst + m * Ns)] = v[c * R + dft_slot<R>(m)];
+  }
+  __syncthreads();
+}
+
+// Forward transform in place (natural order in and out), N = 2^logN >= E.
+template <int E>
+__device__ __forceinline__ void fft_reg(float2* buf, int logN, int lt, const float2* __restrict__ tw) {
+  constexpr int LE = E == 4 ? 2 : E == 8 ? 3 : 4;
+  int logNs = 0;
+  while (logNs + LE <= logN) {
+    pass_reg<E, E>(buf, logN, logNs, lt, tw);
+    logNs += LE;
+  }
+  const int rem = logN - logNs;
+  if (rem == 1) pass_reg<E, 2>(buf, logN, logNs, lt, tw);
+  if constexpr (E >= 8) {
+    if (rem == 2) pass_reg<E, 4>(buf, logN, logNs, lt, tw);
+  }
+  if constexpr (E >= 16) {
+    if (rem == 3) pass_reg<E, 8>(buf, logN, logNs, lt, tw);
+  }
+}
+
+// x -> IFFT(G * FFT(x)) with 1/N folded into g: conj(FFT(conj(G * FFT(x)))).
+template <int E>
+__device__ __forceinline__ void filter_reg(float2* buf, int logN, int lt, const float2* __restrict__ tw,
+                                           const float* __restrict__ g) {
+  const int N = 1 << logN, G = N / E;
+  fft_reg<E>(buf, logN, lt, tw);
+  for (int i = lt; i < N; i += G) {
+    const float gk = __ldg(g + i);
+    const float2 v = buf[pad16(i)];
+    buf[pad16(i)] = make_float2(v.x * gk, -(v.y * gk));
+  }
+  __syncthreads();
+  fft_reg<E>(buf, logN, lt, tw);
+}
+
+// Row pass: 256 / G row pairs per CTA (one packed transform each), G = W / E.
+template <int E>
+__global__ void __launch_bounds__(256) k_fftreg_rows(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+  extern __shared__ float2 smr[];
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int W = d.W, H = d.H, logN = d.fft_logW;
+  const int G = W / E, P = 256 / G;
+  const int tr = threadIdx.x / G, lt = threadIdx.x - tr * G;
+  const int q = (blockIdx.x - off[r]) * P + tr;
+  const int y0 = 2 * q, y1 = 2 * q + 1;
+  float2* buf = smr + (size_t)tr * (W + (W >> 4));
+  const bool act0 = y0 < H, act1 = y1 < H;
+  const float* r0 = d.dep + (size_t)(act0 ? y0 : 0) * W;
+  const float* r1 = d.dep + (size_t)(act1 ? y1 : 0) * W;
+  for (int x = lt; x < W; x += G) buf[pad16(x)] = make_float2(act0 ? r0[x] : 0.0f, act1 ? r1[x] : 0.0f);
+  __syncthreads();
+  filter_reg<E>(buf, logN, lt, d.twW, d.gW);
+  if (act0) {
+    float* o = d.tmp + (size_t)y0 * W;
+    for (int x = lt; x < W; x += G) o[x] = buf[pad16(x)].x;
+  }
+  if (act1) {
+    float* o = d.tmp + (size_t)y1 * W;
+    for (int x = lt; x < W; x += G) o[x] = -buf[pad16(x)].y;
+  }
+}
+
+// Column pass: 4096 / H column pairs per CTA of 4096 / E threads (G = H / E per pair),
+// staged from the row-pass output: at H = 1024 a CTA reads 32-byte row segments.
+template <int E>
+__global__ void __launch_bounds__(4096 / E) k_fftreg_cols(const RDesc* __restrict__ D, const int* __restrict__ off,
+                                                          int n) {
+  extern __shared__ float2 smr[];
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int W = d.W, H = d.H, logN = d.fft_logH;
+  const int G = H / E, P = blockDim.x / G;
+  const int S = H + (H >> 4);
+  const int xbase = (blockIdx.x - off[r]) * 2 * P;
+  for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
+    const int y = idx / P, t = idx - y * P;
+    const int xr = xbase + 2 * t, xi = xr + 1;
+    const float* row = d.tmp + (size_t)y * W;
+    smr[(size_t)t * S + pad16(y)] = make_float2(xr < W ? row[xr] : 0.0f, xi < W ? row[xi] : 0.0f);
+  }
+  __syncthreads();
+  const int tr = threadIdx.x / G, lt = threadIdx.x - tr * G;
+  filter_reg<E>(smr + (size_t)tr * S, logN, lt, d.twH, d.gH);
+  for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
+    const int y = idx / P, t = idx - y * P;
+    const int xr = xbase + 2 * t, xi = xr + 1;
+    const float2 v = smr[(size_t)t * S + pad16(y)];
+    float* row = d.steric + (size_t)y * W;
+    if (xr < W) row[xr] = v.x;
+    if (xi < W) row[xi] = -v.y;
+  }
+}
+
+// shared memory of a CTA: (row pass, 256 threads) 256 E / N transforms or (column pass,
+// 4096 / E threads) 4096 / N transforms, of N + N / 16 values each
+size_t fftreg_smem(int e) { return (size_t)256 * e * 17 / 16 * sizeof(float2); }
+constexpr size_t kFftColsSmem = (size_t)4096 * 17 / 16 * sizeof(float2);
+
+void launch_fftreg_rows(const Launch& L, int e) {
+  if (e == 16) k_fftreg_rows<16><<<L.grid, 256, fftreg_smem(16), L.s>>>(L.d, L.off, L.n);
+  else if (e == 8) k_fftreg_rows<8><<<L.grid, 256, fftreg_smem(8), L.s>>>(L.d, L.off, L.n);
+  else k_fftreg_rows<4><<<L.grid, 256, fftreg_smem(4), L.s>>>(L.d, L.off, L.n);
+}
+void launch_fftreg_cols(const Launch& L, int e) {
+  if (e == 16) k_fftreg_cols<16><<<L.grid, 256, kFftColsSmem, L.s>>>(L.d, L.off, L.n);
+  else if (e == 8) k_fftreg_cols<8><<<L.grid, 512, kFftColsSmem, L.s>>>(L.d, L.off, L.n);
+  else k_fftreg_cols<4><<<L.grid, 1024, kFftColsSmem, L.s>>>(L.d, L.off, L.n);
+}
+
+
 }  // namespace mc

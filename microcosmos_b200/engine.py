@@ -185,12 +185,13 @@ class Record:
 class Plan:
     """A bound plan for a list of rollouts (dims + config + dt + topology each)."""
 
-    def __init__(self, specs, device="cuda", lbm_shape=None, steric_method=0):
+    def __init__(self, specs, device="cuda", lbm_shape=None, steric_method=0, fft_values=0):
         """specs: list of (H, W, N, pairs(E,2) int32, bending_pairs(B,2) int32, cfg, dt).
         ``lbm_shape`` = (cells_per_lane, rows_per_cta) of the dense pass (default: the
         library's choice; ``microcosmos_b200.autotune`` picks one by timing).
         ``steric_method``: 0 = per rollout (direct convolution where it applies, else
-        FFT), 1 = FFT, 2 = direct convolution."""
+        FFT), 1 = FFT, 2 = direct convolution.  ``fft_values``: values per thread of the
+        power-of-two FFT kernels (4, 8, 16; 0 = the library's choice)."""
         _require_cuda()
         lib = _lib.load()
         n = len(specs)
@@ -218,6 +219,8 @@ class Plan:
             _lib.check(lib.mc_plan_set_lbm_shape(h, int(lbm_shape[0]), int(lbm_shape[1])))
         if steric_method:
             _lib.check(lib.mc_plan_set_steric_method(h, int(steric_method)))
+        if fft_values:
+            _lib.check(lib.mc_plan_set_fft_values_per_thread(h, int(fft_values)))
         nbytes = lib.mc_plan_workspace_bytes(h)
         self.workspace = torch.empty(nbytes + 256, dtype=torch.uint8, device=device)
         base = self.workspace.data_ptr()
@@ -227,9 +230,13 @@ class Plan:
         _lib.check(lib.mc_plan_bind(h, ctypes.c_void_p(self._ws_ptr), nbytes, ctypes.c_void_p(stream)))
 
     @classmethod
-    def for_states(cls, states, cfgs, dts, device="cuda", lbm_shape=None, steric_method=0):
+    def for_states(cls, states, cfgs, dts, device="cuda", lbm_shape=None, steric_method=0, fft_values=0):
         specs = [(s.H, s.W, s.N, s.pairs, s.bending_pairs, c, d) for s, c, d in zip(states, cfgs, dts)]
-        return cls(specs, device=device, lbm_shape=lbm_shape, steric_method=steric_method)
+        return cls(specs, device=device, lbm_shape=lbm_shape, steric_method=steric_method, fft_values=fft_values)
+
+    def fft_values(self):
+        """Values per thread of the power-of-two FFT kernels."""
+        return int(_lib.load().mc_plan_fft_values_per_thread(self._h))
 
     def steric_method(self):
         """1: FFT, 2: direct convolution, 3: mixed across rollouts, 0: no steric."""
