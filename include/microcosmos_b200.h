@@ -156,6 +156,13 @@ int32_t mc_plan_steric_method(const mc_plan* plan);
 mc_status mc_plan_set_fft_values_per_thread(mc_plan* plan, int32_t values);
 int32_t mc_plan_fft_values_per_thread(const mc_plan* plan);
 
+/* Threads per CTA of the tile kernel that sorts the IB and cloud-in-cell contributions of
+ * each touched 16 x 16 tile (64, 128 or 256; 0 = 256).  Sparse tiles favour small CTAs.
+ * Results do not depend on it.  Only before mc_plan_bind().  No counterpart in the
+ * reference. */
+mc_status mc_plan_set_bin_threads(mc_plan* plan, int32_t threads);
+int32_t mc_plan_bin_threads(const mc_plan* plan);
+
 /* Bytes of device workspace the plan needs (all rollouts). */
 size_t mc_plan_workspace_bytes(const mc_plan* plan);
 

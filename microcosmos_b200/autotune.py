@@ -1,15 +1,17 @@
 """Autotuner for the launch shapes of a plan.
 
-Two kernels have a free shape:
+Three kernels have a free shape:
   * the dense stream+collide pass: each CTA covers 32 x cells_per_lane columns (1, 2 or 4
     cells per thread, vector loads/stores) by rows_per_cta rows (2, 4 or 8);
   * the power-of-two FFT kernels of the steric filter: each thread holds 4, 8 or 16
-    values in registers (more values: fewer instructions per value; fewer: more threads).
+    values in registers (more values: fewer instructions per value; fewer: more threads);
+  * the tile kernel that sorts the IB and cloud-in-cell contributions: 128 or 256 threads
+    per CTA.
 Which shape is fastest depends on the rollout sizes of a plan (grid widths, how many CTAs
 a step launches, how many tiles carry IB forcing), so the tuner times whole
 graph-replayed steps of the actual plan on scratch copies of the states: first the FFT
-shape with the default dense-pass shape, then the dense-pass shapes with the chosen FFT
-shape.  Results are cached per plan signature (sizes, configs, dt) for the life of the
+shape, then the dense-pass shapes with the chosen FFT shape, then the tile-kernel CTA
+size with both.  Results are cached per plan signature (sizes, configs, dt) for the life of the
 process.  The dense-pass shape changes no result; the FFT shape changes the float32
 rounding of the transform only.
 """
@@ -25,6 +27,7 @@ from .engine import DeviceState, Plan
 CELLS_PER_LANE = (1, 2, 4)
 ROWS_PER_CTA = (2, 4, 8)
 FFT_VALUES = (4, 8, 16)
+BIN_THREADS = (256, 128)
 
 _cache: dict[str, tuple[dict, dict]] = {}
 
@@ -68,7 +71,7 @@ def _time(scratch, cfgs, dts, actuations, steps, warmup, **shape):
 def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, fft_values=None, use_cache=True):
     """Time ``steps`` graph-replayed steps of the plan for the candidate shapes and return
     ``(best, timings)``: best = {"lbm_shape": (cells_per_lane, rows_per_cta),
-    "fft_values": 4 | 8 | 16}, timings = {label: ms per step}.  The caller's states are
+    "fft_values": 4 | 8 | 16, "bin_threads": 128 | 256}, timings = {label: ms per step}.  The caller's states are
     not modified."""
     key = signature(states, cfgs, dts)
     if use_cache and key in _cache:
@@ -87,7 +90,14 @@ def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, ff
     for shape in (shapes or candidates(states)):
         lt[shape] = _time(scratch, cfgs, dts, actuations, steps, warmup, lbm_shape=shape, fft_values=fft_best)
         timings[f"lbm{shape[0]}x{shape[1]}"] = lt[shape]
-    best = {"lbm_shape": min(lt, key=lt.get), "fft_values": fft_best}
+    lbm_best = min(lt, key=lt.get)
+    bt = {256: lt[lbm_best]}
+    for t in BIN_THREADS:
+        if t not in bt:
+            bt[t] = _time(scratch, cfgs, dts, actuations, steps, warmup, lbm_shape=lbm_best, fft_values=fft_best,
+                          bin_threads=t)
+        timings[f"bins{t}"] = bt[t]
+    best = {"lbm_shape": lbm_best, "fft_values": fft_best, "bin_threads": min(bt, key=bt.get)}
     _cache[key] = (best, timings)
     return best, timings
 
@@ -95,4 +105,5 @@ def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, ff
 def tuned_plan(states, cfgs, dts, actuations=None, **kw) -> Plan:
     """A plan for these rollouts with the autotuned launch shapes."""
     best, _ = tune(states, cfgs, dts, actuations=actuations, **kw)
-    return Plan.for_states(states, cfgs, dts, lbm_shape=best["lbm_shape"], fft_values=best["fft_values"])
+    return Plan.for_states(states, cfgs, dts, lbm_shape=best["lbm_shape"], fft_values=best["fft_values"],
+                           bin_threads=best["bin_threads"])

@@ -697,8 +697,9 @@ __global__ void k_record_fields(const RDesc* __restrict__ D, const int* __restri
 
 __global__ void k_tick(int* tdev) { *tdev += 1; }
 
-void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity, int capS) {
-  k_bin_tiles<<<L.grid, 256, (size_t)4 * capS * sizeof(unsigned), L.s>>>(L.d, wl, wl_count, which, parity, capS);
+void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity, int capS,
+                      int threads) {
+  k_bin_tiles<<<L.grid, threads, (size_t)4 * capS * sizeof(unsigned), L.s>>>(L.d, wl, wl_count, which, parity, capS);
 }
 // `bytes` is the per-block opt-in limit; the kernel's static shared memory comes off it.
 cudaError_t tiles_set_smem(size_t bytes) {

@@ -213,7 +213,8 @@ struct Launch {
 };
 
 void launch_predict(const Launch& L);
-void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity, int capS);
+void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity, int capS,
+                      int threads = 256);
 cudaError_t tiles_set_smem(size_t bytes);
 void launch_fft_rows(const Launch& L, size_t smem);
 void launch_fft_cols(const Launch& L, size_t smem);

@@ -89,6 +89,8 @@ struct mc_plan {
   size_t ws_bytes = 0;
   Region r_desc, r_tdev, r_wl_ib, r_wl_cic, r_wl_ctl;
   int tile_grid = 1;  // CTAs walking the tile lists
+  long long n_tiles = 0;  // bin tiles of all rollouts
+  int bin_threads = 256;  // threads per CTA of the tile kernel
   int ib_capS = 0, c_capS = 0;  // largest bin capacity of the plan (tile-sort shared memory)
   Region r_off[K_COUNT];
   std::vector<int> off[K_COUNT];
@@ -614,7 +616,8 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
     timed(p, 1, s, capture, [&] {
       mc::Launch l = L(p, K_TILES, s);
       l.grid = p->tile_grid;
-      mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_cic), at<int>(p->ws, p->r_wl_ctl) + 1, 1, 0, p->c_capS);
+      mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_cic), at<int>(p->ws, p->r_wl_ctl) + 1, 1, 0, p->c_capS,
+                           p->bin_threads);
     });
     k += 1;
     if (p->grid[K_FR16]) {
@@ -674,7 +677,8 @@ int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
   timed(p, 6, s, capture, [&] {
     mc::Launch l = L(p, K_TILES, s);
     l.grid = p->tile_grid;
-    mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_ib), at<int>(p->ws, p->r_wl_ctl), 0, parity, p->ib_capS);
+    mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_ib), at<int>(p->ws, p->r_wl_ctl), 0, parity, p->ib_capS,
+                         p->bin_threads);
   });
   ++k;
   if (p->use_coop) {
@@ -1003,7 +1007,8 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     for (auto& h : p->R) tiles += (long long)h.ntx * h.nty;
     p->r_wl_ib = lay.take((size_t)tiles * sizeof(int2));
     p->r_wl_cic = lay.take((size_t)tiles * sizeof(int2));
-    p->tile_grid = (int)std::max(1LL, std::min(tiles, 148LL * 8));
+    p->n_tiles = tiles;
+    p->tile_grid = (int)std::max(1LL, std::min(tiles, 148LL * 8 * (256 / p->bin_threads)));
     for (auto& h : p->R) {
       p->ib_capS = std::max(p->ib_capS, h.ib_cap);
       p->c_capS = std::max(p->c_capS, h.c_cap);
@@ -1069,6 +1074,19 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
   *out = p;
   return MC_OK;
 }
+
+mc_status mc_plan_set_bin_threads(mc_plan* p, int32_t threads) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (p->bound) return fail(MC_ERR_INVALID, "the tile kernel shape is set before mc_plan_bind()");
+  if (threads != 0 && threads != 64 && threads != 128 && threads != 256)
+    return fail(MC_ERR_INVALID, "threads must be 0 (default), 64, 128 or 256");
+  p->bin_threads = threads ? threads : 256;
+  p->tile_grid = (int)std::max(1LL, std::min(p->n_tiles, 148LL * 8 * (256 / p->bin_threads)));
+  return MC_OK;
+}
+
+int32_t mc_plan_bin_threads(const mc_plan* p) { return p ? p->bin_threads : 0; }
 
 mc_status mc_plan_set_fft_values_per_thread(mc_plan* p, int32_t values) {
   g_err.clear();

@@ -153,3 +153,15 @@ def test_autotune_candidates_respect_widths():
     assert autotune.candidates([S(64), S(128)]) == [(v, r) for v in (1, 2, 4) for r in (2, 4, 8)]
     assert autotune.candidates([S(64), S(66)]) == [(v, r) for v in (1, 2) for r in (2, 4, 8)]
     assert autotune.candidates([S(63)]) == [(1, r) for r in (2, 4, 8)]
+
+
+def test_tile_kernel_threads_setter(lib):
+    sc = scenarios.make_scenario(64, 64, 2, 12, seed=0)
+    st, h = _create([(64, 64, sc.N, sc.pairs, sc.bending_pairs, baseline_config(), 0.01)])
+    assert st == _lib.MC_OK
+    assert lib.mc_plan_bin_threads(h) == 256
+    assert lib.mc_plan_set_bin_threads(h, 128) == _lib.MC_OK and lib.mc_plan_bin_threads(h) == 128
+    assert lib.mc_plan_set_bin_threads(h, 96) == _lib.MC_ERR_INVALID
+    assert lib.mc_plan_set_fft_values_per_thread(h, 8) == _lib.MC_OK and lib.mc_plan_fft_values_per_thread(h) == 8
+    assert lib.mc_plan_set_fft_values_per_thread(h, 5) == _lib.MC_ERR_INVALID
+    lib.mc_plan_destroy(h)
