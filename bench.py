@@ -424,7 +424,8 @@ def main():
     from microcosmos_b200.simulate import run as api_run
     from microcosmos_b200.structs import Edges, Fields, Nodes
 
-    sc, cfgj = workload(args.config, rank)
+    from microcosmos_b200.replicas import job_totals, replica_seed
+    sc, cfgj = workload(args.config, replica_seed(0, rank))
     cfg = baseline_config()
     H, W = sc.H, sc.W
     cells = H * W
@@ -459,10 +460,8 @@ def main():
     plan.end()
     torch.cuda.synchronize()
     t_ms = sum(a.elapsed_time(b) for a, b in ev)
-    t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    t_ms = float(t.item())
+    # job time = max over ranks, job work = sum over ranks (replicas: no data exchange)
+    t_ms, job_cell_steps = job_totals(t_ms, cells * K, device="cuda")
     flags = plan.read_flags()
 
     # ---------------- per-kernel event pass (roofline), L2 flushed before each step
@@ -521,10 +520,7 @@ def main():
                                                    sc.bending_rest_angles, sc.bending_stiffness, sc.f_grid,
                                                    sc.steric, sc.fluid_velocity))
     d2h = sum(int(v.numel() * 4) for v in outs.values())
-    te_t = torch.tensor([te], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(te_t, op=dist.ReduceOp.MAX)
-    te = float(te_t.item())
+    te, job_cell_steps_e = job_totals(te, cells * Ke, device="cuda")
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -540,7 +536,7 @@ def main():
         served = serve_section(args)
 
     if rank == 0:
-        value = cells * K * ws / (t_ms / 1e3) / 1e6
+        value = job_cell_steps / (t_ms / 1e3) / 1e6
         out = {
             "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": ws, "steps": K, "warmup": args.warmup,
             "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -548,7 +544,7 @@ def main():
             "config": dict(cfgj, l2="flushed (256 MiB write) before every timed step; each step timed alone with "
                                     "CUDA events", parallelism=f"replicas x{ws}", dt=0.01,
                            timed="device-resident: one graph-launched simulate.step per event pair"),
-            "e2e": {"value": cells * Ke * ws / (te / 1e3) / 1e6, "unit": "MLUPS",
+            "e2e": {"value": job_cell_steps_e / (te / 1e3) / 1e6, "unit": "MLUPS",
                     "h2d_bytes_per_step": h2d / Ke, "d2h_bytes_per_step": d2h / Ke, "steps_per_call": Ke,
                     "h2d_bytes_per_call": h2d, "d2h_bytes_per_call": d2h,
                     "api": "microcosmos_b200.simulate.run (pinned host inputs -> host outputs)"},

@@ -424,32 +424,30 @@ __global__ void __launch_bounds__(256) k_ib_spread(const RDesc* __restrict__ D, 
   const int* rn = d.ib_store + d.h_start[p];      // contributing nodes, in k order
   const float* rw = d.ib_store_w + d.h_start[p];  // their weights
   float dx = 0.0f, dy = 0.0f;
-  int j = 0;
-  // runs are short: fetch up to 8 entries at a time so their loads overlap
-  for (; j + 8 <= len; j += 8) {
+  // runs are short: fetch 8 entries at a time (the last group predicated) so that all
+  // their loads are in flight together; the sum keeps the run order
+  for (int j = 0; j < len; j += 8) {
     int nd[8];
     float w[8], ex[8], ey[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      nd[q] = rn[j + q];
-      w[q] = rw[j + q];
+      const bool ok = j + q < len;
+      nd[q] = ok ? rn[j + q] : 0;
+      w[q] = ok ? rw[j + q] : 0.0f;
     }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      ex[q] = d.delta[2 * nd[q]];
-      ey[q] = d.delta[2 * nd[q] + 1];
+      const bool ok = j + q < len;
+      ex[q] = ok ? d.delta[2 * nd[q]] : 0.0f;
+      ey[q] = ok ? d.delta[2 * nd[q] + 1] : 0.0f;
     }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      dx = dx + ex[q] * w[q];
-      dy = dy + ey[q] * w[q];
+      if (j + q < len) {
+        dx = dx + ex[q] * w[q];
+        dy = dy + ey[q] * w[q];
+      }
     }
-  }
-  for (; j < len; ++j) {
-    const int node = rn[j];
-    const float w = rw[j];
-    dx = dx + d.delta[2 * node] * w;
-    dy = dy + d.delta[2 * node + 1] * w;
   }
   const float inv = d.s_inv[p];
   d.s_ucx[p] = d.s_ucx[p] + dx * inv;
