@@ -1,0 +1,66 @@
+"""Run a named workload for a fixed number of steps, untimed, for external profilers.
+
+    python -m microcosmos_b200.workload --workload scale --steps 5
+    python -m microcosmos_b200.workload --workload batch --rollouts 64 --steps 10
+    python -m microcosmos_b200.workload --workload grad --steps 20
+
+Workloads (seeded synthetic inputs):
+  scale  one 1024x1024 lattice, 256 filaments x 64 nodes (Poisson-disk placement)
+  small  one 128x128 lattice, 4 filaments x 32 nodes
+  batch  a population of uneven rollouts (side U{128..512}, 1-32 filaments x 16-128 nodes)
+         as one plan with the library's default launch shapes
+  grad   the 256x256, 8 x 48 differentiation workload: forward with checkpoints + backward
+Steps are launched directly (no CUDA graph) unless --graph is given, so that every kernel
+launch is visible to a profiler.
+"""
+from __future__ import annotations
+
+import argparse
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="scale", choices=["scale", "small", "batch", "grad"])
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=2)
+    ap.add_argument("--rollouts", type=int, default=64)
+    ap.add_argument("--graph", action="store_true")
+    a = ap.parse_args(argv)
+    import numpy as np
+    import torch
+
+    from . import baseline_config, scenarios
+    from .engine import Actuation, DeviceState, Plan
+    cfg = baseline_config()
+    if a.workload == "grad":
+        from .autodiff import GradPlan
+        sc = scenarios.make_scenario(256, 256, 8, 48, seed=0, amp=0.2, period=200.0)
+        st = DeviceState.from_scenario(sc)
+        plan = GradPlan(sc.H, sc.W, st.N, sc.pairs, sc.bending_pairs, cfg, 0.01, a.steps)
+        plan.forward(st, Actuation.from_scenario(sc))
+        seed = torch.zeros((st.N, 2), dtype=torch.float32, device="cuda")
+        seed[:, 0] = 1.0 / st.N
+        g = plan.backward(seed)
+        torch.cuda.synchronize()
+        print("grad ok", float(g["act_amp"].norm()))
+        return
+    if a.workload == "batch":
+        scs = scenarios.config_batch(a.rollouts, seed=0)
+    elif a.workload == "small":
+        scs = [scenarios.config_small(seed=0)]
+    else:
+        scs = [scenarios.config_scale(seed=0)]
+    sts = [DeviceState.from_scenario(s) for s in scs]
+    acts = [Actuation.from_scenario(s) for s in scs]
+    plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs))
+    plan.begin(sts, actuations=acts)
+    plan.advance(a.warmup, use_graph=a.graph)
+    plan.advance(a.steps, use_graph=a.graph, last=True)
+    plan.end()
+    torch.cuda.synchronize()
+    print(a.workload, "ok", len(scs), "rollouts", int(sum(s.H * s.W for s in scs)), "cells",
+          "flags", int(np.count_nonzero(plan.read_flags())))
+
+
+if __name__ == "__main__":
+    main()
