@@ -376,35 +376,61 @@ def dist_setup():
     return ws, rank, local
 
 
-def run_reference(args):
-    ws, rank, _ = dist_setup()
-    if rank != 0:
-        return
-    sc, cfgj = workload(args.config, 0)
+def _ref_replica(job):
+    """One CPU process: warm-up, then timed steps of its own copy of the workload for about
+    `budget_s` seconds (numpy restatement of the reference step, one thread)."""
+    name, steps_max, warmup, budget_s = job
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    sys.path.insert(0, HERE)
     from oracle import ref_numpy as O
+    sc, _ = workload(name, 0)
     s = O.state_from_scenario(sc)
     act = (sc.act_c, sc.act_amp, sc.act_omega, sc.act_phase)
     cfg = O.Config()
-    # warm-up then a bounded number of timed steps (the reference CPU path is ~1 s/step at 1024^2)
-    w = max(1, min(args.warmup, 2))
-    s, _ = O.simulate(s, cfg, 0.01, w, act=act)
+    s, _ = O.simulate(s, cfg, 0.01, warmup, act=act)
     t0 = time.perf_counter()
-    k = 1
-    s, _ = O.simulate(s, cfg, 0.01, 1, act=act, t0=w)
-    per = time.perf_counter() - t0
-    k_more = int(max(0, min(args.steps - 1, 60.0 / max(per, 1e-6) - 1)))
-    if k_more:
-        s, _ = O.simulate(s, cfg, 0.01, k_more, act=act, t0=w + 1)
-        k += k_more
-    dt = time.perf_counter() - t0
-    v = sc.H * sc.W * k / dt / 1e6
+    k = 0
+    while k < steps_max and (k == 0 or time.perf_counter() - t0 < budget_s):
+        s, _ = O.simulate(s, cfg, 0.01, 1, act=act, t0=warmup + k)
+        k += 1
+    return k, time.perf_counter() - t0, sc.H * sc.W
+
+
+def run_reference(args):
+    """The reference's CPU path on the host cores: JAX is not installed, so the numpy
+    restatement of the reference step runs instead, as independent replicas of the
+    workload on all usable cores (one single-threaded process each, bounded by memory),
+    each for about 45 s; value = all replicas' cell updates / the slowest replica's time."""
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    sc, cfgj = workload(args.config, 0)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    per_replica = 48 * sc.H * sc.W * 4 + (256 << 20)  # state, tapes of the numpy step and interpreter
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+        procs = max(1, min(cores, int(0.6 * avail // per_replica)))
+    except Exception:
+        procs = max(1, min(cores, 8))
+    w = max(1, min(args.warmup, 2))
+    jobs = [(args.config, max(1, args.steps), w, 45.0)] * procs
+    with mp.get_context("spawn").Pool(procs) as pool:
+        res = pool.map(_ref_replica, jobs)
+    k_tot = sum(k for k, _, _ in res)
+    dt = max(t for _, t, _ in res)
+    cells = res[0][2]
+    v = cells * k_tot / dt / 1e6
+    sample = (f"{procs} single-threaded replicas x {min(k for k, _, _ in res)}-{max(k for k, _, _ in res)} steps of "
+              f"the {sc.H}x{sc.W} workload ({dt:.0f} s; numpy restatement of the reference step: JAX is not "
+              f"installed, so the reference itself cannot run)")
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus, "steps": k,
-        "warmup": w, "ms_per_step": dt / k * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy.random)", "config": cfgj,
-        "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": 1, "kind": "port",
-                         "sample": f"{k} steps of the {sc.H}x{sc.W} workload (numpy restatement of the reference "
-                                   f"step; JAX is not installed, so the reference itself cannot run)"},
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus, "steps": k_tot,
+        "warmup": w, "ms_per_step": dt / max(1, k_tot // procs) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy.random)",
+        "config": cfgj,
+        "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": procs, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
