@@ -28,7 +28,20 @@ namespace {
 
 constexpr int kMaxKK = 64;       // stencil entries per node (kernel size <= 8)
 constexpr int kScanChunk = 4096;  // cells per scan block (1024 threads x 4)
-constexpr int kPbdThreads = 1024;
+constexpr int kPbdThreads = 128;  // threads per rod component in the PBD kernels
+
+// Per-step inputs of one reverse step, read on the device so that the same CUDA graph
+// replays every step of a segment (sa[*jp], jp counts down).
+struct StepArgs {
+  int t;
+  const float* pos;
+  const float* vel;
+  const float* th;
+  const float* f;
+  const float* V;
+  float* lf_in;
+  float* lf_out;
+};
 
 struct AD {
   int H, W, N, E, B, HW, C, iters, K, KK, steric, fluid, nskip, has_act;
@@ -41,6 +54,17 @@ struct AD {
   const int* n_list;
   const int* e_start;  // edge -> incident bending pairs: entry = b * 2 + role (0: e_in, 1: e_out)
   const int* e_list;
+  // rod components (connected by edges): their nodes, edges and bending pairs, ascending
+  int ncomp;
+  const int* c_nstart;
+  const int* c_nodes;
+  const int* c_estart;
+  const int* c_edges;
+  const int* c_bstart;
+  const int* c_bps;
+  // per-step inputs of the reverse step being replayed
+  const StepArgs* sa;
+  int* jp;
   const float* ndeg;
   const float* edeg;
   const float* rest_len;
@@ -133,9 +157,10 @@ __device__ __forceinline__ float sample_wrap(const float* V, int H, int W, float
 }
 
 // ------------------------------------------------------------------ tape: prediction + steric
-__global__ void k_rest(AD d, int t) {
+__global__ void k_rest(AD d) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.B) return;
+  const int t = d.sa[*d.jp].t;
   float r;
   if (d.has_act) {
     const float arg = d.act_om[b] * (float)t + d.act_ph[b];
@@ -147,8 +172,12 @@ __global__ void k_rest(AD d, int t) {
   d.rest_acc[b] = 0.0f;
 }
 
-__global__ void k_pred(AD d, const float2* __restrict__ pos, const float2* __restrict__ vel,
-                       const float* __restrict__ theta, const float* __restrict__ V) {
+__global__ void k_pred(AD d) {
+  const StepArgs a = d.sa[*d.jp];
+  const float2* __restrict__ pos = reinterpret_cast<const float2*>(a.pos);
+  const float2* __restrict__ vel = reinterpret_cast<const float2*>(a.vel);
+  const float* __restrict__ theta = a.th;
+  const float* __restrict__ V = a.V;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < d.E) d.tt[i] = theta[i];
   if (i >= d.N) return;
@@ -208,11 +237,15 @@ __device__ __forceinline__ float2 edge_force(const AD& d, const float2* p, float
   return make_float2(((sx + shx * d.kshear) * d.kstretch) * 0.5f, ((sy + shy * d.kshear) * d.kstretch) * 0.5f);
 }
 
+// one CTA per rod component: the components never interact in the PBD passes
 __global__ void __launch_bounds__(kPbdThreads) k_pbd_fwd(AD d) {
+  const int c = blockIdx.x;
+  const int ea = d.c_estart[c], eb = d.c_estart[c + 1], na = d.c_nstart[c], nb = d.c_nstart[c + 1];
   for (int k = 0; k < d.C; ++k) {
     const float* th = d.tt + (size_t)k * d.E;
     float* thn = d.tt + (size_t)(k + 1) * d.E;
-    for (int e = threadIdx.x; e < d.E; e += blockDim.x) {
+    for (int ie = ea + threadIdx.x; ie < eb; ie += blockDim.x) {
+      const int e = d.c_edges[ie];
       float acc = 0.0f;
       for (int q = d.e_start[e]; q < d.e_start[e + 1]; ++q) {
         const int en = d.e_list[q];
@@ -224,7 +257,8 @@ __global__ void __launch_bounds__(kPbdThreads) k_pbd_fwd(AD d) {
     __syncthreads();
     const float2* p = d.pp + (size_t)k * d.N;
     float2* pn = d.pp + (size_t)(k + 1) * d.N;
-    for (int n = threadIdx.x; n < d.N; n += blockDim.x) {
+    for (int in = na + threadIdx.x; in < nb; in += blockDim.x) {
+      const int n = d.c_nodes[in];
       float ax = 0.0f, ay = 0.0f;
       for (int q = d.n_start[n]; q < d.n_start[n + 1]; ++q) {
         const int en = d.n_list[q];
@@ -374,7 +408,8 @@ __global__ void k_csr_sort(const int* __restrict__ start, int n, int* ent) {
 }
 
 // ------------------------------------------------------------------ tape: macroscopic + IB iterations
-__global__ void k_macro(AD d, const float* __restrict__ f) {
+__global__ void k_macro(AD d) {
+  const float* __restrict__ f = d.sa[*d.jp].f;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.HW) return;
   float r = mc::max_prop(f[c], MC_EPSIL);
@@ -396,7 +431,8 @@ __global__ void k_macro(AD d, const float* __restrict__ f) {
   d.inv[c] = 1.0f / mc::max_prop(cov, 1.0f);
 }
 
-__global__ void k_ib_interp(AD d, const float2* __restrict__ prev, int it) {
+__global__ void k_ib_interp(AD d, int it) {
+  const float2* __restrict__ prev = reinterpret_cast<const float2*>(d.sa[*d.jp].pos);
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= d.N) return;
   float ix = 0.0f, iy = 0.0f;
@@ -438,7 +474,10 @@ __constant__ float kW9[9] = {4.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f,
                              1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f};
 __constant__ int kOpp[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
 
-__global__ void k_lbm_adj1(AD d, const float* __restrict__ f, const float* __restrict__ lfn) {
+__global__ void k_lbm_adj1(AD d) {
+  const StepArgs a = d.sa[*d.jp];
+  const float* __restrict__ f = a.f;
+  const float* __restrict__ lfn = a.lf_in;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.HW) return;
   const int y = c / d.W, x = c - y * d.W;
@@ -571,7 +610,10 @@ __global__ void k_ib_rev_cell(AD d) {
   d.luc[d.HW + c] = d.luc[d.HW + c] + ay;
 }
 
-__global__ void k_lbm_adj2(AD d, const float* __restrict__ f, float* __restrict__ lf_out) {
+__global__ void k_lbm_adj2(AD d) {
+  const StepArgs a = d.sa[*d.jp];
+  const float* __restrict__ f = a.f;
+  float* __restrict__ lf_out = a.lf_out;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.HW) return;
   float f0[9];
@@ -610,8 +652,12 @@ __global__ void k_node_adj(AD d) {
   d.lprev[i] = make_float2(-lv1.x / d.dt, -lv1.y / d.dt);
 }
 
-// ------------------------------------------------------------------ adjoint: PBD iterations (one CTA)
-__global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d, int t) {
+// ------------------------------------------------------------------ adjoint: PBD iterations (one CTA per rod component)
+__global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d) {
+  const int t = d.sa[*d.jp].t;
+  const int c = blockIdx.x;
+  const int ea = d.c_estart[c], eb = d.c_estart[c + 1], na = d.c_nstart[c], nb = d.c_nstart[c + 1];
+  const int ba = d.c_bstart[c], bb = d.c_bstart[c + 1];
   int cur = 0;
   const float ks = d.kshear, kst = d.kstretch;
   for (int k = d.C - 1; k >= 0; --k) {
@@ -623,7 +669,8 @@ __global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d, int t) {
     const float* lti = d.lt[cur];
     float* lto = d.lt[cur ^ 1];
     // position pass
-    for (int e = threadIdx.x; e < d.E; e += blockDim.x) {
+    for (int ie = ea + threadIdx.x; ie < eb; ie += blockDim.x) {
+      const int e = d.c_edges[ie];
       const int2 pr = d.pairs[e];
       const float ns = d.ndeg[pr.x], nt = d.ndeg[pr.y];
       const float hx = ((lpi[pr.x].x / ns - lpi[pr.y].x / nt) * kst) * 0.5f;
@@ -646,7 +693,8 @@ __global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d, int t) {
       d.lcur[e] = make_float2(lcx, lcy);
     }
     __syncthreads();
-    for (int n = threadIdx.x; n < d.N; n += blockDim.x) {
+    for (int in = na + threadIdx.x; in < nb; in += blockDim.x) {
+      const int n = d.c_nodes[in];
       float ax = lpi[n].x, ay = lpi[n].y;
       for (int q = d.n_start[n]; q < d.n_start[n + 1]; ++q) {
         const int en = d.n_list[q];
@@ -661,7 +709,8 @@ __global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d, int t) {
       }
       lpo[n] = make_float2(ax, ay);
     }
-    for (int b = threadIdx.x; b < d.B; b += blockDim.x) {
+    for (int ib = ba + threadIdx.x; ib < bb; ib += blockDim.x) {
+      const int b = d.c_bps[ib];
       const int2 bp = d.bpairs[b];
       const float lcorr = 1.8f * (d.lthn[bp.x] / d.edeg[bp.x] - d.lthn[bp.y] / d.edeg[bp.y]);
       const float g = lcorr * d.kb[b] * 0.5f;
@@ -672,7 +721,8 @@ __global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d, int t) {
       d.d_kb[b] += lcorr * (diff - d.rest[b]) * 0.5f;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < d.E; e += blockDim.x) {
+    for (int ie = ea + threadIdx.x; ie < eb; ie += blockDim.x) {
+      const int e = d.c_edges[ie];
       float a = d.lthn[e];
       for (int q = d.e_start[e]; q < d.e_start[e + 1]; ++q) {
         const int en = d.e_list[q];
@@ -684,9 +734,10 @@ __global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d, int t) {
     __syncthreads();
     cur ^= 1;
   }
-  for (int n = threadIdx.x; n < d.N; n += blockDim.x) d.lpred1[n] = d.lp[cur][n];
-  for (int e = threadIdx.x; e < d.E; e += blockDim.x) d.lth[e] = d.lt[cur][e];
-  for (int b = threadIdx.x; b < d.B; b += blockDim.x) {
+  for (int in = na + threadIdx.x; in < nb; in += blockDim.x) d.lpred1[d.c_nodes[in]] = d.lp[cur][d.c_nodes[in]];
+  for (int ie = ea + threadIdx.x; ie < eb; ie += blockDim.x) d.lth[d.c_edges[ie]] = d.lt[cur][d.c_edges[ie]];
+  for (int ib = ba + threadIdx.x; ib < bb; ib += blockDim.x) {
+    const int b = d.c_bps[ib];
     const float G = d.rest_acc[b];
     if (d.has_act) {
       const float arg = d.act_om[b] * (float)t + d.act_ph[b];
@@ -723,7 +774,8 @@ __device__ __forceinline__ void sample_adj(const AD& d, const float* V, float yy
   d.st_val[base + 3] = coef * (ty * tx);
 }
 
-__global__ void k_steric_adj_node(AD d, const float* __restrict__ V) {
+__global__ void k_steric_adj_node(AD d) {
+  const float* __restrict__ V = d.sa[*d.jp].V;
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= d.N) return;
   const float Wf = (float)d.W, Hf = (float)d.H;
@@ -811,6 +863,10 @@ __global__ void k_steric_adj_cic(AD d) {
   d.lvel[n] = make_float2((l0.x * d.damp) * d.dt, (l0.y * d.damp) * d.dt);
 }
 
+__global__ void k_step_next(AD d) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *d.jp -= 1;
+}
+
 __global__ void k_copy_lpred(AD d) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n < d.N) d.lpred0p[n] = d.lpred1[n];
@@ -846,6 +902,12 @@ struct mc_grad_plan {
       r_lf1;
   size_t state_ck_bytes = 0;  // one checkpoint: pos, vel, theta, f
   AD ad{};
+  std::vector<int> c_nstart, c_nodes, c_estart, c_edges, c_bstart, c_bps;  // rod components
+  R r_cns, r_cn, r_ces, r_ce, r_cbs, r_cb, r_sargs, r_jp;
+  std::vector<StepArgs> sargs;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t rev_graph = nullptr;  // one reverse step, replayed per step
+  int rev_graph_act = -1;               // has_act the graph was captured with
 };
 
 namespace {
@@ -967,37 +1029,35 @@ mc_status run_fwd(mc_grad_plan* p, int steps, int t0, cudaStream_t s) {
   return mc_rollout(p->fwd, &w, steps, acts, nullptr, 1, s);
 }
 
-void reverse_step(mc_grad_plan* p, int t, const Slot& in, const float* V, int& lfcur, cudaStream_t s) {
+// The kernels of one reverse step; its per-step inputs come from sa[*jp], and the last
+// kernel moves jp to the previous step, so one captured graph replays a whole segment.
+void reverse_step(mc_grad_plan* p, cudaStream_t s) {
   AD& d = p->ad;
   const int TB = 256;
   const int nNE = std::max(d.N, d.E);
-  k_rest<<<nblk(std::max(d.B, 1), TB), TB, 0, s>>>(d, t);
-  k_pred<<<nblk(nNE, TB), TB, 0, s>>>(d, reinterpret_cast<const float2*>(in.pos),
-                                      reinterpret_cast<const float2*>(in.vel), in.th, V);
-  k_pbd_fwd<<<1, kPbdThreads, 0, s>>>(d);
-  float* lf_in = at<float>(p->ws, lfcur ? p->r_lf1 : p->r_lf0);
-  float* lf_out = at<float>(p->ws, lfcur ? p->r_lf0 : p->r_lf1);
+  k_rest<<<nblk(std::max(d.B, 1), TB), TB, 0, s>>>(d);
+  k_pred<<<nblk(nNE, TB), TB, 0, s>>>(d);
+  k_pbd_fwd<<<d.ncomp, kPbdThreads, 0, s>>>(d);
   if (d.fluid) {
     k_ib_weights<<<nblk(d.N, TB), TB, 0, s>>>(d);
     csr_build(d, d.ib_idx, d.N * d.KK, s);
-    k_macro<<<nblk(d.HW, TB), TB, 0, s>>>(d, in.f);
+    k_macro<<<nblk(d.HW, TB), TB, 0, s>>>(d);
     for (int it = 0; it < d.iters; ++it) {
-      k_ib_interp<<<nblk(d.N, TB), TB, 0, s>>>(d, reinterpret_cast<const float2*>(in.pos), it);
+      k_ib_interp<<<nblk(d.N, TB), TB, 0, s>>>(d, it);
       k_ib_spread<<<nblk(d.HW, TB), TB, 0, s>>>(d);
     }
-    k_lbm_adj1<<<nblk(d.HW, TB), TB, 0, s>>>(d, in.f, lf_in);
+    k_lbm_adj1<<<nblk(d.HW, TB), TB, 0, s>>>(d);
     cudaMemsetAsync(d.lnv, 0, (size_t)d.N * 8, s);
     for (int it = d.iters - 1; it >= 0; --it) {
       k_ib_rev_node<<<nblk(d.N, TB), TB, 0, s>>>(d, it);
       k_ib_rev_cell<<<nblk(d.HW, TB), TB, 0, s>>>(d);
     }
-    k_lbm_adj2<<<nblk(d.HW, TB), TB, 0, s>>>(d, in.f, lf_out);
-    lfcur ^= 1;
+    k_lbm_adj2<<<nblk(d.HW, TB), TB, 0, s>>>(d);
   }
   k_node_adj<<<nblk(nNE, TB), TB, 0, s>>>(d);
-  k_pbd_rev<<<1, kPbdThreads, 0, s>>>(d, t);
+  k_pbd_rev<<<d.ncomp, kPbdThreads, 0, s>>>(d);
   if (d.steric) {
-    k_steric_adj_node<<<nblk(d.N, TB), TB, 0, s>>>(d, V);
+    k_steric_adj_node<<<nblk(d.N, TB), TB, 0, s>>>(d);
     csr_build(d, d.st_cell, d.N * 16, s);
     k_gather_field<<<nblk(d.HW, TB), TB, 0, s>>>(d, d.st_val, d.lV);
     k_conv_x<<<nblk(d.HW, TB), TB, 0, s>>>(d, d.lV, d.ctmp);
@@ -1006,6 +1066,7 @@ void reverse_step(mc_grad_plan* p, int t, const Slot& in, const float* V, int& l
     k_copy_lpred<<<nblk(d.N, TB), TB, 0, s>>>(d);
   }
   k_steric_adj_cic<<<nblk(d.N, TB), TB, 0, s>>>(d);
+  k_step_next<<<1, 32, 0, s>>>(d);
 }
 
 }  // namespace
@@ -1070,6 +1131,44 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
     p->e_start[e + 1] = p->e_start[e] + (int)el[e].size();
     p->e_list.insert(p->e_list.end(), el[e].begin(), el[e].end());
     p->edeg[e] = std::max((float)el[e].size(), 1.0f);
+  }
+  {
+    // rod components: union-find over the edges; members listed in ascending order
+    std::vector<int> par(D.N);
+    for (int n = 0; n < D.N; ++n) par[n] = n;
+    auto find = [&](int x) {
+      while (par[x] != x) {
+        par[x] = par[par[x]];
+        x = par[x];
+      }
+      return x;
+    };
+    for (int e = 0; e < D.E; ++e) {
+      const int a = find(p->pairs[2 * e]), b = find(p->pairs[2 * e + 1]);
+      if (a != b) par[std::max(a, b)] = std::min(a, b);
+    }
+    std::vector<int> cid(D.N, -1);
+    int nc = 0;
+    for (int n = 0; n < D.N; ++n) {
+      const int r = find(n);
+      if (cid[r] < 0) cid[r] = nc++;
+      cid[n] = cid[r];
+    }
+    std::vector<std::vector<int>> cn(nc), ce(nc), cb(nc);
+    for (int n = 0; n < D.N; ++n) cn[cid[n]].push_back(n);
+    for (int e = 0; e < D.E; ++e) ce[cid[p->pairs[2 * e]]].push_back(e);
+    for (int b = 0; b < D.B; ++b) cb[cid[p->pairs[2 * p->bpairs[2 * b]]]].push_back(b);
+    p->c_nstart.assign(1, 0);
+    p->c_estart.assign(1, 0);
+    p->c_bstart.assign(1, 0);
+    for (int c = 0; c < nc; ++c) {
+      p->c_nodes.insert(p->c_nodes.end(), cn[c].begin(), cn[c].end());
+      p->c_edges.insert(p->c_edges.end(), ce[c].begin(), ce[c].end());
+      p->c_bps.insert(p->c_bps.end(), cb[c].begin(), cb[c].end());
+      p->c_nstart.push_back((int)p->c_nodes.size());
+      p->c_estart.push_back((int)p->c_edges.size());
+      p->c_bstart.push_back((int)p->c_bps.size());
+    }
   }
   taps(D.W, cfg->steric_sigma, p->gW, p->baseW);
   taps(D.H, cfg->steric_sigma, p->gH, p->baseH);
@@ -1167,6 +1266,14 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   take(p->r_ldep, HW * 4);
   take(p->r_lf0, 9 * HW * 4);
   take(p->r_lf1, 9 * HW * 4);
+  take(p->r_cns, p->c_nstart.size() * 4);
+  take(p->r_cn, std::max<size_t>(p->c_nodes.size(), 1) * 4);
+  take(p->r_ces, p->c_estart.size() * 4);
+  take(p->r_ce, std::max<size_t>(p->c_edges.size(), 1) * 4);
+  take(p->r_cbs, p->c_bstart.size() * 4);
+  take(p->r_cb, std::max<size_t>(p->c_bps.size(), 1) * 4);
+  take(p->r_sargs, (size_t)S * sizeof(StepArgs));
+  take(p->r_jp, 4);
   p->total = o;
   *out = p;
   return MC_OK;
@@ -1174,6 +1281,8 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
 
 void mc_grad_plan_destroy(mc_grad_plan* p) {
   if (!p) return;
+  if (p->rev_graph) cudaGraphExecDestroy(p->rev_graph);
+  if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
   if (p->fwd) mc_plan_destroy(p->fwd);
   delete p;
 }
@@ -1205,6 +1314,17 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   GC(up(p->r_edeg, p->edeg.data(), p->edeg.size() * 4));
   GC(up(p->r_gW, p->gW.data(), p->gW.size() * 4));
   GC(up(p->r_gH, p->gH.data(), p->gH.size() * 4));
+  GC(up(p->r_cns, p->c_nstart.data(), p->c_nstart.size() * 4));
+  GC(up(p->r_cn, p->c_nodes.data(), p->c_nodes.size() * 4));
+  GC(up(p->r_ces, p->c_estart.data(), p->c_estart.size() * 4));
+  GC(up(p->r_ce, p->c_edges.data(), p->c_edges.size() * 4));
+  GC(up(p->r_cbs, p->c_bstart.data(), p->c_bstart.size() * 4));
+  GC(up(p->r_cb, p->c_bps.data(), p->c_bps.size() * 4));
+  if (p->rev_graph) {
+    cudaGraphExecDestroy(p->rev_graph);
+    p->rev_graph = nullptr;
+  }
+  if (!p->cap_stream) GC(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
   GC(cudaMemsetAsync(p->ws + p->r_cnt.off, 0, p->r_cnt.bytes, s));
   GC(cudaStreamSynchronize(s));  // the host tables above are temporaries of this call's scope
   const mc_config& c = p->cfg;
@@ -1316,6 +1436,15 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   d.baseW = p->baseW;
   d.ntH = (int)p->gH.size();
   d.baseH = p->baseH;
+  d.ncomp = (int)p->c_nstart.size() - 1;
+  d.c_nstart = at<int>(w, p->r_cns);
+  d.c_nodes = at<int>(w, p->r_cn);
+  d.c_estart = at<int>(w, p->r_ces);
+  d.c_edges = at<int>(w, p->r_ce);
+  d.c_bstart = at<int>(w, p->r_cbs);
+  d.c_bps = at<int>(w, p->r_cb);
+  d.sa = at<StepArgs>(w, p->r_sargs);
+  d.jp = at<int>(w, p->r_jp);
   p->bound = true;
   return MC_OK;
 }
@@ -1423,12 +1552,45 @@ mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_st
       GC(cudaMemcpyAsync(w + p->r_segV.off + (size_t)j * al(HW * 4), w + p->r_wst.off, HW * 4,
                          cudaMemcpyDeviceToDevice, s));
     }
+    // per-step inputs of the segment (the cotangent of f alternates between two buffers)
+    p->sargs.assign(len, StepArgs{});
     for (int j = len - 1; j >= 0; --j) {
       Slot sj = slot(p, p->r_seg, j);
-      const float* V = reinterpret_cast<const float*>(w + p->r_segV.off + (size_t)j * al(HW * 4));
-      reverse_step(p, t0 + j, sj, V, lfcur, s);
-      GC(cudaGetLastError());
+      StepArgs& a = p->sargs[j];
+      a.t = t0 + j;
+      a.pos = sj.pos;
+      a.vel = sj.vel;
+      a.th = sj.th;
+      a.f = sj.f;
+      a.V = reinterpret_cast<const float*>(w + p->r_segV.off + (size_t)j * al(HW * 4));
+      a.lf_in = at<float>(w, lfcur ? p->r_lf1 : p->r_lf0);
+      a.lf_out = at<float>(w, lfcur ? p->r_lf0 : p->r_lf1);
+      if (d.fluid) lfcur ^= 1;
     }
+    GC(cudaMemcpyAsync(w + p->r_sargs.off, p->sargs.data(), len * sizeof(StepArgs), cudaMemcpyHostToDevice, s));
+    const int jlast = len - 1;
+    GC(cudaMemcpyAsync(w + p->r_jp.off, &jlast, sizeof(int), cudaMemcpyHostToDevice, s));
+    GC(cudaStreamSynchronize(s));  // the host copies above are sources of asynchronous copies
+    if (!p->rev_graph || p->rev_graph_act != d.has_act) {
+      if (p->rev_graph) {
+        cudaGraphExecDestroy(p->rev_graph);
+        p->rev_graph = nullptr;
+      }
+      cudaGraph_t g;
+      GC(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
+      reverse_step(p, p->cap_stream);
+      cudaError_t e = cudaStreamEndCapture(p->cap_stream, &g);
+      if (e != cudaSuccess) return gfail(MC_ERR_CUDA, std::string("capture of the reverse step: ") + cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&p->rev_graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        p->rev_graph = nullptr;
+        return gfail(MC_ERR_CUDA, std::string("instantiating the reverse step: ") + cudaGetErrorString(e));
+      }
+      p->rev_graph_act = d.has_act;
+    }
+    for (int j = len - 1; j >= 0; --j) GC(cudaGraphLaunch(p->rev_graph, s));
+    GC(cudaGetLastError());
   }
   (void)d;
   auto out = [&](float* dst, const mc_grad_plan::R& r, size_t n) -> cudaError_t {
