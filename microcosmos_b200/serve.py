@@ -130,7 +130,7 @@ class Server:
     while the host services the others.
     """
 
-    def __init__(self, backend, hbm_budget_bytes: float = 180e9, max_active: int = 64, chunk: int = 100,
+    def __init__(self, backend, hbm_budget_bytes: float = 180e9, max_active: int = 16, chunk: int = 200,
                  depth: int = 2, clock: Callable[[], float] | None = None, sleep: Callable[[float], None] | None = None,
                  keep_state: bool = True):
         if chunk < 1 or depth < 1 or max_active < 1:
