@@ -90,6 +90,9 @@ struct AD {
   int* start;  // HW + 1
   int* bsum;   // scan block sums
   int* ent;    // entries
+  int* touched;   // cells with at least one entry (any order), M entries at most
+  int* ntouched;  // their count
+  int max_entries;
   // adjoint
   float* lf0p;   // 9 x HW
   float* lv;     // 2 x HW
@@ -120,9 +123,6 @@ struct AD {
   float* lV;       // HW
   float* ctmp;     // HW
   float* ldep;     // HW
-  const float* gtW;  // taps along x
-  const float* gtH;  // taps along y
-  int ntW, baseW, ntH, baseH;
 };
 
 __device__ __forceinline__ float dmaxf(float x, float c) { return x > c ? 1.0f : (x == c ? 0.5f : 0.0f); }
@@ -392,9 +392,19 @@ __global__ void k_csr_fill(const int* __restrict__ cells, int M, const int* __re
 }
 
 // entries of each cell in increasing flat index (the order np.add.at applies them)
-__global__ void k_csr_sort(const int* __restrict__ start, int n, int* ent) {
+// the cells that received entries, compacted (their order does not matter: every
+// per-cell kernel below writes only its own cell)
+__global__ void k_csr_touched(const int* __restrict__ start, int n, int* touched, int* ntouched) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
+  if (c >= n || start[c + 1] == start[c]) return;
+  touched[atomicAdd(ntouched, 1)] = c;
+}
+
+__global__ void k_csr_sort(const int* __restrict__ start, const int* __restrict__ touched,
+                           const int* __restrict__ ntouched, int* ent) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *ntouched) return;
+  const int c = touched[i];
   const int a = start[c], b = start[c + 1];
   for (int i = a + 1; i < b; ++i) {
     const int v = ent[i];
@@ -452,10 +462,10 @@ __global__ void k_ib_interp(AD d, int it) {
 }
 
 __global__ void k_ib_spread(AD d) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.HW) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *d.ntouched) return;
+  const int c = d.touched[i];
   const int a = d.start[c], b = d.start[c + 1];
-  if (a == b) return;
   float ax = 0.0f, ay = 0.0f;
   for (int q = a; q < b; ++q) {
     const int e = d.ent[q];
@@ -594,10 +604,10 @@ __global__ void k_ib_rev_node(AD d, int it) {
 }
 
 __global__ void k_ib_rev_cell(AD d) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.HW) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *d.ntouched) return;
+  const int c = d.touched[i];
   const int a = d.start[c], b = d.start[c + 1];
-  if (a == b) return;
   float ax = 0.0f, ay = 0.0f;
   for (int q = a; q < b; ++q) {
     const int e = d.ent[q];
@@ -813,30 +823,13 @@ __global__ void k_steric_adj_node(AD d) {
   d.lpred0p[n] = make_float2(lp1.x + lpx, lp1.y + lpy);
 }
 
+// out must be zero outside the touched cells
 __global__ void k_gather_field(AD d, const float* __restrict__ val, float* out) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.HW) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *d.ntouched) return;
+  const int c = d.touched[i];
   float a = 0.0f;
   for (int q = d.start[c]; q < d.start[c + 1]; ++q) a = a + val[d.ent[q]];
-  out[c] = a;
-}
-
-// circular convolution along x (rows) or y (columns) with symmetric taps
-__global__ void k_conv_x(AD d, const float* __restrict__ in, float* out) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.HW) return;
-  const int y = c / d.W, x = c - y * d.W;
-  float a = 0.0f;
-  for (int k = 0; k < d.ntW; ++k) a += d.gtW[k] * in[y * d.W + mc::imod_floor(x - (d.baseW + k), d.W)];
-  out[c] = a;
-}
-
-__global__ void k_conv_y(AD d, const float* __restrict__ in, float* out) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.HW) return;
-  const int y = c / d.W, x = c - y * d.W;
-  float a = 0.0f;
-  for (int k = 0; k < d.ntH; ++k) a += d.gtH[k] * in[mc::imod_floor(y - (d.baseH + k), d.H) * d.W + x];
   out[c] = a;
 }
 
@@ -883,8 +876,7 @@ struct mc_grad_plan {
   float dt = 0.f;
   int T = 0, S = 1, nseg = 0;
   std::vector<int> pairs, bpairs, n_start, n_list, e_start, e_list;
-  std::vector<float> ndeg, edeg, gW, gH;
-  int baseW = 0, baseH = 0;
+  std::vector<float> ndeg, edeg;
   mc_plan* fwd = nullptr;
   size_t fwd_bytes = 0, total = 0;
   unsigned char* ws = nullptr;
@@ -893,10 +885,11 @@ struct mc_grad_plan {
   struct R {
     size_t off = 0, bytes = 0;
   };
-  R r_fwd, r_pairs, r_bpairs, r_nst, r_nl, r_est, r_el, r_ndeg, r_edeg, r_len, r_kb, r_rst, r_ac, r_aa, r_ao, r_ap, r_gW,
-      r_gH;
+  R r_fwd, r_pairs, r_bpairs, r_nst, r_nl, r_est, r_el, r_ndeg, r_edeg, r_len, r_kb, r_rst, r_ac, r_aa, r_ao, r_ap,
+      r_fdesc;
+  bool filter_ready = false;
   R r_wpos, r_wvel, r_wth, r_wra, r_wst, r_wfu, r_wf, r_ck, r_seg, r_segV;
-  R r_rest, r_pred0, r_pp, r_tt, r_ibidx, r_ibw, r_sraw, r_stmp, r_uc, r_inv, r_cnt, r_start, r_bsum, r_ent;
+  R r_rest, r_pred0, r_pp, r_tt, r_ibidx, r_ibw, r_sraw, r_stmp, r_uc, r_inv, r_cnt, r_start, r_bsum, r_ent, r_touch;
   R r_lf0p, r_lv, r_lrho, r_luc, r_lnv, r_lprev, r_lpos, r_lvel, r_lth, r_lp0, r_lp1, r_lt0, r_lt1, r_lcur, r_lthn,
       r_gb, r_racc, r_dc, r_da, r_dp, r_dr, r_dl, r_dk, r_stc, r_stv, r_lpred1, r_lpred0p, r_lV, r_ctmp, r_ldep, r_lf0,
       r_lf1;
@@ -927,30 +920,6 @@ mc_status gfail(mc_status s, const std::string& m) {
 
 size_t al(size_t x) { return (x + 255) / 256 * 256; }
 
-// periodic Gaussian taps of the spectral filter exp(-2 pi^2 sigma^2 f^2) on N points:
-// g[k] = (1/N) sum_j kf_j cos(2 pi j k / N), kept where |g| > 1e-12 g[0]
-void taps(int N, double sigma, std::vector<float>& g, int& base) {
-  std::vector<double> full(N);
-  for (int k = 0; k < N; ++k) {
-    double s = 0.0;
-    for (int j = 0; j < N; ++j) {
-      const double fj = (j < (N + 1) / 2 ? j : j - N) / (double)N;
-      s += std::exp(-2.0 * M_PI * M_PI * sigma * sigma * fj * fj) * std::cos(2.0 * M_PI * (double)j * k / N);
-    }
-    full[k] = s / N;
-  }
-  int R = 0;
-  while (R + 1 <= N / 2 && std::fabs(full[R + 1]) > 1e-12 * std::fabs(full[0])) ++R;
-  g.clear();
-  if (2 * R + 1 >= N) {
-    base = 0;
-    for (int k = 0; k < N; ++k) g.push_back((float)full[k]);
-  } else {
-    base = -R;
-    for (int k = -R; k <= R; ++k) g.push_back((float)full[(k + N) % N]);
-  }
-}
-
 template <typename T>
 T* at(unsigned char* ws, const mc_grad_plan::R& r) {
   return reinterpret_cast<T*>(ws + r.off);
@@ -963,7 +932,9 @@ void csr_build(const AD& d, const int* cells, int M, cudaStream_t s) {
   k_scan2<<<1, 1024, 0, s>>>(d.bsum, nb);
   k_scan3<<<nblk(d.HW, 256), 256, 0, s>>>(d.start, d.bsum, d.HW, M);
   if (M > 0) k_csr_fill<<<nblk(M, 256), 256, 0, s>>>(cells, M, d.start, d.cnt, d.ent);
-  k_csr_sort<<<nblk(d.HW, 256), 256, 0, s>>>(d.start, d.HW, d.ent);
+  cudaMemsetAsync(d.ntouched, 0, sizeof(int), s);
+  k_csr_touched<<<nblk(d.HW, 256), 256, 0, s>>>(d.start, d.HW, d.touched, d.ntouched);
+  k_csr_sort<<<nblk(std::max(M, 1), 256), 256, 0, s>>>(d.start, d.touched, d.ntouched, d.ent);
 }
 
 mc_status copy_state_to(mc_grad_plan* p, float* pos, float* vel, float* th, float* f, const float* spos, const float* svel,
@@ -1044,13 +1015,13 @@ void reverse_step(mc_grad_plan* p, cudaStream_t s) {
     k_macro<<<nblk(d.HW, TB), TB, 0, s>>>(d);
     for (int it = 0; it < d.iters; ++it) {
       k_ib_interp<<<nblk(d.N, TB), TB, 0, s>>>(d, it);
-      k_ib_spread<<<nblk(d.HW, TB), TB, 0, s>>>(d);
+      k_ib_spread<<<nblk(d.N * d.KK, TB), TB, 0, s>>>(d);
     }
     k_lbm_adj1<<<nblk(d.HW, TB), TB, 0, s>>>(d);
     cudaMemsetAsync(d.lnv, 0, (size_t)d.N * 8, s);
     for (int it = d.iters - 1; it >= 0; --it) {
       k_ib_rev_node<<<nblk(d.N, TB), TB, 0, s>>>(d, it);
-      k_ib_rev_cell<<<nblk(d.HW, TB), TB, 0, s>>>(d);
+      k_ib_rev_cell<<<nblk(d.N * d.KK, TB), TB, 0, s>>>(d);
     }
     k_lbm_adj2<<<nblk(d.HW, TB), TB, 0, s>>>(d);
   }
@@ -1059,9 +1030,11 @@ void reverse_step(mc_grad_plan* p, cudaStream_t s) {
   if (d.steric) {
     k_steric_adj_node<<<nblk(d.N, TB), TB, 0, s>>>(d);
     csr_build(d, d.st_cell, d.N * 16, s);
-    k_gather_field<<<nblk(d.HW, TB), TB, 0, s>>>(d, d.st_val, d.lV);
-    k_conv_x<<<nblk(d.HW, TB), TB, 0, s>>>(d, d.lV, d.ctmp);
-    k_conv_y<<<nblk(d.HW, TB), TB, 0, s>>>(d, d.ctmp, d.ldep);
+    cudaMemsetAsync(d.lV, 0, (size_t)d.HW * 4, s);
+    k_gather_field<<<nblk(d.N * 16, TB), TB, 0, s>>>(d, d.st_val, d.lV);
+    // the spectral filter is real and even, so it is its own adjoint: the forward plan's
+    // filter kernels map the sample cotangent lV to the deposit cotangent ldep
+    mc::filter_launch(p->fwd, p->ws + p->r_fdesc.off, s);
   } else {
     k_copy_lpred<<<nblk(d.N, TB), TB, 0, s>>>(d);
   }
@@ -1170,8 +1143,6 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
       p->c_bstart.push_back((int)p->c_bps.size());
     }
   }
-  taps(D.W, cfg->steric_sigma, p->gW, p->baseW);
-  taps(D.H, cfg->steric_sigma, p->gH, p->baseH);
   // forward plan (same kernels as mc_rollout)
   const int32_t* pp[1] = {pairs};
   const int32_t* bb[1] = {bending_pairs};
@@ -1207,8 +1178,6 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   take(p->r_aa, B * 4);
   take(p->r_ao, B * 4);
   take(p->r_ap, B * 4);
-  take(p->r_gW, p->gW.size() * 4);
-  take(p->r_gH, p->gH.size() * 4);
   take(p->r_wpos, N * 8);
   take(p->r_wvel, N * 8);
   take(p->r_wth, E * 4);
@@ -1234,6 +1203,7 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   take(p->r_start, (HW + 1) * 4);
   take(p->r_bsum, 4096 * 4);
   take(p->r_ent, std::max<size_t>(N * KK, 16 * N) * 4);
+  take(p->r_touch, std::max<size_t>(N * KK, 16 * N) * 4 + 256);
   take(p->r_lf0p, 9 * HW * 4);
   take(p->r_lv, 2 * HW * 4);
   take(p->r_lrho, HW * 4);
@@ -1273,6 +1243,7 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   take(p->r_cbs, p->c_bstart.size() * 4);
   take(p->r_cb, std::max<size_t>(p->c_bps.size(), 1) * 4);
   take(p->r_sargs, (size_t)S * sizeof(StepArgs));
+  take(p->r_fdesc, mc::filter_desc_bytes());
   take(p->r_jp, 4);
   p->total = o;
   *out = p;
@@ -1312,8 +1283,6 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   GC(up(p->r_el, p->e_list.data(), p->e_list.size() * 4));
   GC(up(p->r_ndeg, p->ndeg.data(), p->ndeg.size() * 4));
   GC(up(p->r_edeg, p->edeg.data(), p->edeg.size() * 4));
-  GC(up(p->r_gW, p->gW.data(), p->gW.size() * 4));
-  GC(up(p->r_gH, p->gH.data(), p->gH.size() * 4));
   GC(up(p->r_cns, p->c_nstart.data(), p->c_nstart.size() * 4));
   GC(up(p->r_cn, p->c_nodes.data(), p->c_nodes.size() * 4));
   GC(up(p->r_ces, p->c_estart.data(), p->c_estart.size() * 4));
@@ -1324,6 +1293,7 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
     cudaGraphExecDestroy(p->rev_graph);
     p->rev_graph = nullptr;
   }
+  p->filter_ready = false;
   if (!p->cap_stream) GC(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
   GC(cudaMemsetAsync(p->ws + p->r_cnt.off, 0, p->r_cnt.bytes, s));
   GC(cudaStreamSynchronize(s));  // the host tables above are temporaries of this call's scope
@@ -1400,6 +1370,8 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   d.start = at<int>(w, p->r_start);
   d.bsum = at<int>(w, p->r_bsum);
   d.ent = at<int>(w, p->r_ent);
+  d.ntouched = at<int>(w, p->r_touch);
+  d.touched = d.ntouched + 64;
   d.lf0p = at<float>(w, p->r_lf0p);
   d.lv = at<float>(w, p->r_lv);
   d.lrho = at<float>(w, p->r_lrho);
@@ -1430,12 +1402,6 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   d.lV = at<float>(w, p->r_lV);
   d.ctmp = at<float>(w, p->r_ctmp);
   d.ldep = at<float>(w, p->r_ldep);
-  d.gtW = at<float>(w, p->r_gW);
-  d.gtH = at<float>(w, p->r_gH);
-  d.ntW = (int)p->gW.size();
-  d.baseW = p->baseW;
-  d.ntH = (int)p->gH.size();
-  d.baseH = p->baseH;
   d.ncomp = (int)p->c_nstart.size() - 1;
   d.c_nstart = at<int>(w, p->r_cns);
   d.c_nodes = at<int>(w, p->r_cn);
@@ -1534,6 +1500,11 @@ mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_st
   GC(seed(p->r_lf0, final_cot->f_grid, 9 * HW * 4));
   for (const mc_grad_plan::R* r : {&p->r_dc, &p->r_da, &p->r_dp, &p->r_dr, &p->r_dl, &p->r_dk})
     GC(cudaMemsetAsync(w + r->off, 0, r->bytes, s));
+  if (d.steric && !p->filter_ready) {
+    // the forward plan's descriptor exists once mc_grad_forward has run a rollout call
+    GC(mc::filter_prepare(p->fwd, w + p->r_fdesc.off, d.lV, d.ctmp, d.ldep, s));
+    p->filter_ready = true;
+  }
   int lfcur = 0;
   for (int k = p->nseg - 1; k >= 0; --k) {
     const int t0 = k * p->S;

@@ -243,6 +243,21 @@ void launch_fft_rows_p2(const Launch& L, size_t smem);
 void launch_fft_cols_p2(const Launch& L, size_t smem);
 cudaError_t fft_p2_set_smem(size_t bytes);
 void set_last_error(const char* msg);  // text returned by mc_last_error() on this thread
+
+}  // namespace mc
+
+struct mc_plan;
+
+namespace mc {
+
+// The steric filter of rollout 0 of a plan applied to other arrays (the gradient path uses
+// it: the filter is its own adjoint).  filter_prepare writes a descriptor and CTA offset
+// tables (filter_desc_bytes() bytes at `dev`) naming in -> tmp -> out; it needs the plan's
+// descriptor of a rollout call (mc_rollout_begin has run once).  filter_launch enqueues
+// the same row and column kernels as a step.
+size_t filter_desc_bytes();
+cudaError_t filter_prepare(mc_plan* p, void* dev, const float* in, float* tmp, float* out, cudaStream_t s);
+void filter_launch(mc_plan* p, const void* dev, cudaStream_t s);
 cudaError_t node_set_smem(size_t bytes);
 
 }  // namespace mc

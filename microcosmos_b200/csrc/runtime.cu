@@ -811,6 +811,52 @@ void destroy_graphs(mc_plan* p) {
 
 namespace mc {
 void set_last_error(const char* msg) { g_err = msg; }
+
+namespace {
+constexpr int kFilterKinds[5] = {K_FR16, K_FFTR2, K_SCONV, K_FC16, K_FFTC2};
+}
+
+size_t filter_desc_bytes() { return align_up(sizeof(RDesc), 256) + 5 * 256; }
+
+cudaError_t filter_prepare(mc_plan* p, void* dev, const float* in, float* tmp, float* out, cudaStream_t s) {
+  if (p->desc.empty()) return cudaErrorInvalidValue;
+  RDesc d = p->desc[0];
+  d.dep = const_cast<float*>(in);
+  d.tmp = tmp;
+  d.steric = out;
+  const StericCtas c = steric_ctas(p->R[0], p->fft_e);
+  const int cnt[5] = {c.fr16, c.fftr2, c.sconv, c.fc16, c.fftc2};
+  std::vector<unsigned char> host(filter_desc_bytes(), 0);
+  std::memcpy(host.data(), &d, sizeof(RDesc));
+  for (int k = 0; k < 5; ++k) {
+    const int off[2] = {0, cnt[k]};
+    std::memcpy(host.data() + align_up(sizeof(RDesc), 256) + 256 * k, off, sizeof(off));
+  }
+  cudaError_t e = cudaMemcpyAsync(dev, host.data(), host.size(), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(s);  // `host` is a temporary
+}
+
+void filter_launch(mc_plan* p, const void* dev, cudaStream_t s) {
+  const unsigned char* b = static_cast<const unsigned char*>(dev);
+  const StericCtas c = steric_ctas(p->R[0], p->fft_e);
+  const int cnt[5] = {c.fr16, c.fftr2, c.sconv, c.fc16, c.fftc2};
+  auto launch = [&](int k) {
+    Launch l;
+    l.d = reinterpret_cast<const RDesc*>(b);
+    l.off = reinterpret_cast<const int*>(b + align_up(sizeof(RDesc), 256) + 256 * k);
+    l.n = 1;
+    l.grid = cnt[k];
+    l.s = s;
+    return l;
+  };
+  if (cnt[0]) launch_fftreg_rows(launch(0), p->fft_e);
+  if (cnt[1]) launch_fft_rows_p2(launch(1), p->fftr2_smem);
+  if (cnt[2]) launch_steric_conv(launch(2), p->sconv_smem);
+  if (cnt[3]) launch_fftreg_cols(launch(3), p->fft_e);
+  if (cnt[4]) launch_fft_cols_p2(launch(4), p->fftc2_smem);
+  (void)kFilterKinds;
+}
 }  // namespace mc
 
 extern "C" {

@@ -14,14 +14,21 @@ float atomics), so a rollout's result is bit-for-bit the same whatever else is i
 More hardware queues than CUDA's default of 8 let more rollouts overlap: set
 ``CUDA_DEVICE_MAX_CONNECTIONS`` (e.g. 32) before the process first touches the GPU.
 
+Requests that ask for gradients get the gradient of the mean centre-of-mass x
+displacement of their final state with respect to the actuation (c, amplitude, phase of
+every bending pair) and the initial positions: the forward rollout with checkpoints and
+the adjoint run as one job on a worker thread (own stream, own gradient plan, see
+``microcosmos_b200.autodiff``), overlapping with the chunked forward rollouts.
+
 The scheduler is written against a small backend interface (``bytes_needed``, ``start``,
 ``advance``, ``inflight``, ``finish``) so that its admission and ordering logic is tested
 without a GPU; ``CudaBackend`` is the device implementation over
-``microcosmos_b200.engine``.
+``microcosmos_b200.engine`` and ``microcosmos_b200.autodiff``.
 """
 from __future__ import annotations
 
 import collections
+import concurrent.futures
 import ctypes
 import dataclasses
 import time
@@ -56,15 +63,18 @@ class Result:
 
 
 class CudaBackend:
-    """Device backend: one bound plan + workspace + CUDA stream per admitted rollout."""
+    """Device backend: one bound plan + workspace + CUDA stream per admitted rollout;
+    gradient requests run as one job each on a small thread pool."""
 
-    def __init__(self, cfg, dt=0.01, device="cuda"):
+    def __init__(self, cfg, dt=0.01, device="cuda", grad_workers=2):
         self.cfg = cfg
         self.dt = float(dt)
         self.device = device
+        self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=max(1, int(grad_workers)))
 
     def bytes_needed(self, req: Request) -> int:
-        """Device bytes of the rollout: its plan workspace (mc_plan_workspace_bytes) plus state."""
+        """Device bytes of the rollout: its plan workspace (mc_plan_workspace_bytes, or
+        mc_grad_plan_workspace_bytes for a gradient request) plus state."""
         from . import _lib
         from .engine import mc_config
         sc = req.scenario
@@ -73,23 +83,56 @@ class CudaBackend:
         bp = np.ascontiguousarray(sc.bending_pairs, np.int32).reshape(-1, 2)
         dims = _lib.McDims(sc.H, sc.W, sc.position.shape[0], pairs.shape[0], bp.shape[0])
         cfg = mc_config(self.cfg)
-        dt = ctypes.c_float(self.dt)
-        pp = (_lib.c_int_p * 1)(pairs.ctypes.data_as(_lib.c_int_p))
-        bb = (_lib.c_int_p * 1)(bp.ctypes.data_as(_lib.c_int_p))
         h = ctypes.c_void_p()
-        _lib.check(lib.mc_plan_create(1, ctypes.byref(dims), ctypes.byref(cfg), ctypes.byref(dt), pp, bb,
-                                      ctypes.byref(h)))
-        try:
-            ws = int(lib.mc_plan_workspace_bytes(h))
-        finally:
-            lib.mc_plan_destroy(h)
+        if req.want_grad:
+            _lib.check(lib.mc_grad_plan_create(ctypes.byref(dims), ctypes.byref(cfg), self.dt,
+                                               pairs.ctypes.data_as(_lib.c_int_p), bp.ctypes.data_as(_lib.c_int_p),
+                                               int(req.steps), 0, ctypes.byref(h)))
+            try:
+                ws = int(lib.mc_grad_plan_workspace_bytes(h))
+            finally:
+                lib.mc_grad_plan_destroy(h)
+        else:
+            dt = ctypes.c_float(self.dt)
+            pp = (_lib.c_int_p * 1)(pairs.ctypes.data_as(_lib.c_int_p))
+            bb = (_lib.c_int_p * 1)(bp.ctypes.data_as(_lib.c_int_p))
+            _lib.check(lib.mc_plan_create(1, ctypes.byref(dims), ctypes.byref(cfg), ctypes.byref(dt), pp, bb,
+                                          ctypes.byref(h)))
+            try:
+                ws = int(lib.mc_plan_workspace_bytes(h))
+            finally:
+                lib.mc_plan_destroy(h)
         N = sc.position.shape[0]
         state = 4 * (12 * sc.H * sc.W + 8 * N + 4 * bp.shape[0]) + 256
         return ws + state
 
+    def _grad_job(self, req: Request):
+        import torch
+        from .autodiff import GradPlan
+        from .engine import Actuation, DeviceState
+        stream = torch.cuda.Stream(device=self.device)
+        with torch.cuda.stream(stream):
+            sc = req.scenario
+            st = DeviceState.from_scenario(sc, device=self.device)
+            act = Actuation.from_scenario(sc, device=self.device)
+            plan = GradPlan(sc.H, sc.W, st.N, sc.pairs, sc.bending_pairs, self.cfg, self.dt, req.steps,
+                            device=self.device)
+            plan.forward(st, act)
+            seed = torch.zeros((st.N, 2), dtype=torch.float32, device=self.device)
+            seed[:, 0] = 1.0 / st.N  # d(mean x of the final positions)
+            g = plan.backward(seed)
+            g["position"][:, 0] -= 1.0 / st.N  # the loss subtracts the initial mean x
+            state = st.host()
+            state["grad"] = {k: v.cpu().numpy() for k, v in g.items()}
+            stream.synchronize()
+            plan.close()
+        return state, 0
+
     def start(self, req: Request):
         import torch
         from .engine import Actuation, DeviceState, Plan
+        if req.want_grad:
+            return {"future": self.pool.submit(self._grad_job, req)}
         stream = torch.cuda.Stream(device=self.device)
         with torch.cuda.stream(stream):
             st = DeviceState.from_scenario(req.scenario, device=self.device)
@@ -100,6 +143,8 @@ class CudaBackend:
 
     def advance(self, h, steps: int, last: bool):
         import torch
+        if "future" in h:
+            return  # the gradient job runs all its steps at once
         h["plan"].advance(steps, use_graph=True, last=last, stream=h["stream"].cuda_stream)
         ev = torch.cuda.Event()
         ev.record(h["stream"])
@@ -107,6 +152,8 @@ class CudaBackend:
 
     def inflight(self, h) -> int:
         """Chunks issued and not finished yet."""
+        if "future" in h:
+            return 0 if h["future"].done() else 1
         q = h["events"]
         while q and q[0].query():
             q.popleft()
@@ -114,6 +161,8 @@ class CudaBackend:
 
     def finish(self, h):
         import torch
+        if "future" in h:
+            return h["future"].result()
         with torch.cuda.stream(h["stream"]):
             h["plan"].end(stream=h["stream"].cuda_stream)
             flags = h["plan"].read_flags()[0]
@@ -219,12 +268,24 @@ def run_plain(backend, requests: list[Request]):
     return out
 
 
-def summarize(results: list[Result], wall_s: float) -> dict:
+def summarize(results: list[Result], wall_s: float, grad_ids=()) -> dict:
+    """Throughput and latency; MLUPS counts forward cell updates of every request (a
+    gradient request's adjoint work is not counted)."""
     lat = np.array([r.latency for r in results]) if results else np.zeros(1)
     cell_steps = sum(r.cells * r.steps for r in results)
-    return {"requests": len(results), "wall_s": wall_s, "rollouts_per_s": len(results) / wall_s,
-            "mlups": cell_steps / wall_s / 1e6, "p50_latency_s": float(np.percentile(lat, 50)),
-            "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean())}
+    out = {"requests": len(results), "wall_s": wall_s, "rollouts_per_s": len(results) / wall_s,
+           "mlups": cell_steps / wall_s / 1e6, "p50_latency_s": float(np.percentile(lat, 50)),
+           "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean())}
+    g = set(grad_ids)
+    if g:
+        gl = np.array([r.latency for r in results if r.rid in g])
+        fl = np.array([r.latency for r in results if r.rid not in g])
+        out["grad_requests"] = len(gl)
+        if len(gl):
+            out["grad_p50_latency_s"] = float(np.percentile(gl, 50))
+        if len(fl):
+            out["forward_p50_latency_s"] = float(np.percentile(fl, 50))
+    return out
 
 
 def poisson_requests(n, rate_per_s, seed=0, sides=None, filaments=(1, 128), nodes=(16, 128), steps=(500, 5000),

@@ -132,7 +132,7 @@ def test_results_identical_alone_and_in_the_mix():
     from microcosmos_b200 import baseline_config
     cfg = baseline_config()
     reqs = serve.poisson_requests(8, 2000.0, seed=11, sides=(64, 128, 192), filaments=(1, 6), nodes=(16, 40),
-                                  steps=(30, 160))
+                                  steps=(30, 160), grad_fraction=0.0)
     be = serve.CudaBackend(cfg, dt=0.01)
     mixed = serve.Server(be, hbm_budget_bytes=4e9, max_active=8, chunk=16).run(reqs)
     alone = serve.run_plain(be, reqs)
@@ -142,3 +142,32 @@ def test_results_identical_alone_and_in_the_mix():
         assert r.rid == rid and r.flags == 0 and flags == 0
         for k in ("position", "velocity", "f_grid", "steric", "fluid_velocity"):
             assert np.array_equal(r.state[k], state[k]), (rid, k)
+
+
+@pytest.mark.gpu
+def test_gradient_requests_in_the_mix_match_a_gradient_run_alone():
+    torch = pytest.importorskip("torch")
+    from microcosmos_b200 import baseline_config
+    from microcosmos_b200.autodiff import GradPlan
+    from microcosmos_b200.engine import Actuation, DeviceState
+    cfg = baseline_config()
+    reqs = serve.poisson_requests(6, 2000.0, seed=12, sides=(64, 128), filaments=(1, 4), nodes=(16, 30),
+                                  steps=(20, 60), grad_fraction=0.5)
+    assert any(r.want_grad for r in reqs) and not all(r.want_grad for r in reqs)
+    be = serve.CudaBackend(cfg, dt=0.01)
+    res = serve.Server(be, hbm_budget_bytes=4e9, max_active=4, chunk=16).run(reqs)
+    for r, q in zip(res, reqs):
+        if not q.want_grad:
+            assert "grad" not in r.state
+            continue
+        sc = q.scenario
+        st = DeviceState.from_scenario(sc)
+        plan = GradPlan(sc.H, sc.W, st.N, sc.pairs, sc.bending_pairs, cfg, 0.01, q.steps)
+        plan.forward(st, Actuation.from_scenario(sc))
+        seed = torch.zeros((st.N, 2), dtype=torch.float32, device="cuda")
+        seed[:, 0] = 1.0 / st.N
+        g = plan.backward(seed)
+        torch.cuda.synchronize()
+        for k in ("act_c", "act_amp", "act_phase"):
+            assert np.array_equal(r.state["grad"][k], g[k].cpu().numpy()), (q.rid, k)
+        assert np.array_equal(r.state["position"], st.position.cpu().numpy())
