@@ -231,6 +231,8 @@ cudaError_t ib_coop_blocks_per_sm(int* out);
 void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows);
 void launch_steric_conv(const Launch& L, size_t smem);
 void launch_fftreg_rows(const Launch& L, int values_per_thread);
+void launch_fft12_rows(const Launch& L);
+void launch_fft12_cols(const Launch& L);
 void launch_fftreg_cols(const Launch& L, int values_per_thread);
 void launch_reaction(const Launch& L, const int* tdev);
 void launch_record_fields(const Launch& L, const int* tdev);

@@ -37,14 +37,21 @@ mc_status cuda_fail(cudaError_t e, const char* where) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16, K_COUNT };
+enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16, K_FR12, K_FC12, K_COUNT };
 
 // CTAs of the steric filter kernels for one rollout: the radix-16 register kernels for
 // power-of-two sides >= 16, the mixed-radix Stockham kernels for the other FFT sides, or
 // the direct convolution.
 struct StericCtas {
-  int fftr2 = 0, fftc2 = 0, sconv = 0, fr16 = 0, fc16 = 0;
+  int fftr2 = 0, fftc2 = 0, sconv = 0, fr16 = 0, fc16 = 0, fr12 = 0, fc12 = 0;
 };
+
+// N = 3 * 2^a with 12 <= N <= 1536: the twelve-values-per-thread register kernels
+bool three_pow2(int N) {
+  if (N % 3 != 0 || N < 12 || N > 1536) return false;
+  const int q = N / 3;
+  return (q & (q - 1)) == 0;
+}
 
 struct Region {
   size_t off = 0;
@@ -572,8 +579,10 @@ StericCtas steric_ctas(const HostRollout& h, int e) {
   }
   const int W = h.dims.W, H = h.dims.H;
   if (h.logW >= 4 && W >= e && W <= 256 * e) c.fr16 = div_up(div_up(H, 2), 256 * e / W);
+  else if (three_pow2(W)) c.fr12 = div_up(div_up(H, 2), 256 / (W / 12));
   else c.fftr2 = div_up(div_up(H, 2), h.P_r);
   if (h.logH >= 4 && H >= e && H <= 256 * e) c.fc16 = div_up(div_up(W, 2), 4096 / H);
+  else if (three_pow2(H)) c.fc12 = div_up(div_up(W, 2), 384 / (H / 12));
   else c.fftc2 = div_up(W, 2 * h.P_c);
   return c;
 }
@@ -593,7 +602,7 @@ int default_fft_values(const std::vector<HostRollout>& R) {
 void recount_steric(mc_plan* p);
 
 void recount_steric(mc_plan* p) {
-  for (int k : {K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16}) p->off[k][0] = 0;
+  for (int k : {K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16, K_FR12, K_FC12}) p->off[k][0] = 0;
   for (int i = 0; i < p->n; ++i) {
     const StericCtas c = steric_ctas(p->R[i], p->fft_e);
     p->off[K_FFTR2][i + 1] = p->off[K_FFTR2][i] + c.fftr2;
@@ -601,8 +610,10 @@ void recount_steric(mc_plan* p) {
     p->off[K_SCONV][i + 1] = p->off[K_SCONV][i] + c.sconv;
     p->off[K_FR16][i + 1] = p->off[K_FR16][i] + c.fr16;
     p->off[K_FC16][i + 1] = p->off[K_FC16][i] + c.fc16;
+    p->off[K_FR12][i + 1] = p->off[K_FR12][i] + c.fr12;
+    p->off[K_FC12][i + 1] = p->off[K_FC12][i] + c.fc12;
   }
-  for (int k : {K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16}) p->grid[k] = p->off[k][p->n];
+  for (int k : {K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16, K_FR12, K_FC12}) p->grid[k] = p->off[k][p->n];
 }
 
 int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
@@ -624,6 +635,10 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
       timed(p, 2, s, capture, [&] { mc::launch_fftreg_rows(L(p, K_FR16, s), p->fft_e); });
       ++k;
     }
+    if (p->grid[K_FR12]) {
+      timed(p, 2, s, capture, [&] { mc::launch_fft12_rows(L(p, K_FR12, s)); });
+      ++k;
+    }
     if (p->grid[K_FFTR2]) {
       timed(p, 2, s, capture, [&] { mc::launch_fft_rows_p2(L(p, K_FFTR2, s), p->fftr2_smem); });
       ++k;
@@ -634,6 +649,10 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
     }
     if (p->grid[K_FC16]) {
       timed(p, 3, s, capture, [&] { mc::launch_fftreg_cols(L(p, K_FC16, s), p->fft_e); });
+      ++k;
+    }
+    if (p->grid[K_FC12]) {
+      timed(p, 3, s, capture, [&] { mc::launch_fft12_cols(L(p, K_FC12, s)); });
       ++k;
     }
     if (p->grid[K_FFTC2]) {
@@ -812,11 +831,7 @@ void destroy_graphs(mc_plan* p) {
 namespace mc {
 void set_last_error(const char* msg) { g_err = msg; }
 
-namespace {
-constexpr int kFilterKinds[5] = {K_FR16, K_FFTR2, K_SCONV, K_FC16, K_FFTC2};
-}
-
-size_t filter_desc_bytes() { return align_up(sizeof(RDesc), 256) + 5 * 256; }
+size_t filter_desc_bytes() { return align_up(sizeof(RDesc), 256) + 7 * 256; }
 
 cudaError_t filter_prepare(mc_plan* p, void* dev, const float* in, float* tmp, float* out, cudaStream_t s) {
   if (p->desc.empty()) return cudaErrorInvalidValue;
@@ -825,10 +840,10 @@ cudaError_t filter_prepare(mc_plan* p, void* dev, const float* in, float* tmp, f
   d.tmp = tmp;
   d.steric = out;
   const StericCtas c = steric_ctas(p->R[0], p->fft_e);
-  const int cnt[5] = {c.fr16, c.fftr2, c.sconv, c.fc16, c.fftc2};
+  const int cnt[7] = {c.fr16, c.fftr2, c.sconv, c.fc16, c.fftc2, c.fr12, c.fc12};
   std::vector<unsigned char> host(filter_desc_bytes(), 0);
   std::memcpy(host.data(), &d, sizeof(RDesc));
-  for (int k = 0; k < 5; ++k) {
+  for (int k = 0; k < 7; ++k) {
     const int off[2] = {0, cnt[k]};
     std::memcpy(host.data() + align_up(sizeof(RDesc), 256) + 256 * k, off, sizeof(off));
   }
@@ -840,7 +855,7 @@ cudaError_t filter_prepare(mc_plan* p, void* dev, const float* in, float* tmp, f
 void filter_launch(mc_plan* p, const void* dev, cudaStream_t s) {
   const unsigned char* b = static_cast<const unsigned char*>(dev);
   const StericCtas c = steric_ctas(p->R[0], p->fft_e);
-  const int cnt[5] = {c.fr16, c.fftr2, c.sconv, c.fc16, c.fftc2};
+  const int cnt[7] = {c.fr16, c.fftr2, c.sconv, c.fc16, c.fftc2, c.fr12, c.fc12};
   auto launch = [&](int k) {
     Launch l;
     l.d = reinterpret_cast<const RDesc*>(b);
@@ -851,11 +866,12 @@ void filter_launch(mc_plan* p, const void* dev, cudaStream_t s) {
     return l;
   };
   if (cnt[0]) launch_fftreg_rows(launch(0), p->fft_e);
+  if (cnt[5]) launch_fft12_rows(launch(5));
   if (cnt[1]) launch_fft_rows_p2(launch(1), p->fftr2_smem);
   if (cnt[2]) launch_steric_conv(launch(2), p->sconv_smem);
   if (cnt[3]) launch_fftreg_cols(launch(3), p->fft_e);
+  if (cnt[6]) launch_fft12_cols(launch(6));
   if (cnt[4]) launch_fft_cols_p2(launch(4), p->fftc2_smem);
-  (void)kFilterKinds;
 }
 }  // namespace mc
 

@@ -551,6 +551,15 @@ template <int R>
 __device__ __forceinline__ void dft_reg(float2* v) {
   if constexpr (R == 2) {
     dft2(v[0], v[1]);
+  } else if constexpr (R == 3) {
+    // X1,2 = a - (b + c) / 2 -/+ i (sqrt(3) / 2) (b - c)
+    const float2 a = v[0], t1 = cadd(v[1], v[2]), dd = csub(v[1], v[2]);
+    const float2 t2 = make_float2(a.x - 0.5f * t1.x, a.y - 0.5f * t1.y);
+    const float s3 = 0.86602540378443865f;
+    const float2 t3 = make_float2(s3 * dd.y, -(s3 * dd.x));
+    v[0] = cadd(a, t1);
+    v[1] = cadd(t2, t3);
+    v[2] = csub(t2, t3);
   } else if constexpr (R == 4) {
     dft4(v[0], v[1], v[2], v[3]);
   } else if constexpr (R == 8) {
@@ -718,6 +727,130 @@ __global__ void __launch_bounds__(4096 / E) k_fftreg_cols(const RDesc* __restric
     if (xi < W) row[xi] = -v.y;
   }
 }
+
+// ---------------------------------------------------------------- sides N = 3 * 2^a
+// Twelve values per thread (G = N / 12 threads per transform): the power-of-two factor
+// in radix-4 passes (three butterflies per thread; one radix-2 pass if a is odd), then a
+// final radix-3 pass (four butterflies per thread) with Ns = N / 3, so every k = j mod Ns
+// is still a mask.  Twiddle index steps N / (Ns R) are integers but not powers of two.
+template <int R>
+__device__ __forceinline__ void pass12(float2* buf, int N, int Ns, int lt, const float2* __restrict__ tw) {
+  constexpr int C = 12 / R;
+  const int G = N / 12;
+  const int S = N / R;
+  const int step = N / (Ns * R);
+  float2 v[12];
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int j = lt + c * G;
+    const int k = j & (Ns - 1);
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      float2 a = buf[pad16(j + m * S)];
+      if (m > 0 && k > 0) a = cmul(a, __ldg(tw + m * k * step));
+      v[c * R + m] = a;
+    }
+    dft_reg<R>(v + c * R);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int j = lt + c * G;
+    const int k = j & (Ns - 1);
+    const int dst = (j - k) * R + k;
+#pragma unroll
+    for (int m = 0; m < R; ++m) buf[pad16(dst + m * Ns)] = v[c * R + dft_slot<R>(m)];
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void fft12(float2* buf, int N, int lt, const float2* __restrict__ tw) {
+  const int P = N / 3;  // power of two >= 4
+  int Ns = 1;
+  while (Ns * 4 <= P) {
+    pass12<4>(buf, N, Ns, lt, tw);
+    Ns *= 4;
+  }
+  if (Ns < P) {
+    pass12<2>(buf, N, Ns, lt, tw);
+    Ns *= 2;
+  }
+  pass12<3>(buf, N, Ns, lt, tw);
+}
+
+__device__ __forceinline__ void filter12(float2* buf, int N, int lt, const float2* __restrict__ tw,
+                                         const float* __restrict__ g) {
+  const int G = N / 12;
+  fft12(buf, N, lt, tw);
+  for (int i = lt; i < N; i += G) {
+    const float gk = __ldg(g + i);
+    const float2 v = buf[pad16(i)];
+    buf[pad16(i)] = make_float2(v.x * gk, -(v.y * gk));
+  }
+  __syncthreads();
+  fft12(buf, N, lt, tw);
+}
+
+// Row pass for W = 3 * 2^a: 256 / G row pairs per CTA, G = W / 12.
+__global__ void __launch_bounds__(256) k_fft12_rows(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+  extern __shared__ float2 sm12[];
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int W = d.W, H = d.H;
+  const int G = W / 12, P = 256 / G;
+  const int tr = threadIdx.x / G, lt = threadIdx.x - tr * G;
+  const int q = (blockIdx.x - off[r]) * P + tr;
+  const int y0 = 2 * q, y1 = 2 * q + 1;
+  float2* buf = sm12 + (size_t)tr * (W + (W >> 4));
+  const bool act0 = y0 < H, act1 = y1 < H;
+  const float* r0 = d.dep + (size_t)(act0 ? y0 : 0) * W;
+  const float* r1 = d.dep + (size_t)(act1 ? y1 : 0) * W;
+  for (int x = lt; x < W; x += G) buf[pad16(x)] = make_float2(act0 ? r0[x] : 0.0f, act1 ? r1[x] : 0.0f);
+  __syncthreads();
+  filter12(buf, W, lt, d.twW, d.gW);
+  if (act0) {
+    float* o = d.tmp + (size_t)y0 * W;
+    for (int x = lt; x < W; x += G) o[x] = buf[pad16(x)].x;
+  }
+  if (act1) {
+    float* o = d.tmp + (size_t)y1 * W;
+    for (int x = lt; x < W; x += G) o[x] = -buf[pad16(x)].y;
+  }
+}
+
+// Column pass for H = 3 * 2^a: 384 / G column pairs per CTA of 384 threads, G = H / 12.
+__global__ void __launch_bounds__(384) k_fft12_cols(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
+  extern __shared__ float2 sm12[];
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int W = d.W, H = d.H;
+  const int G = H / 12, P = blockDim.x / G;
+  const int S = H + (H >> 4);
+  const int xbase = (blockIdx.x - off[r]) * 2 * P;
+  for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
+    const int y = idx / P, t = idx - y * P;
+    const int xr = xbase + 2 * t, xi = xr + 1;
+    const float* row = d.tmp + (size_t)y * W;
+    sm12[(size_t)t * S + pad16(y)] = make_float2(xr < W ? row[xr] : 0.0f, xi < W ? row[xi] : 0.0f);
+  }
+  __syncthreads();
+  const int tr = threadIdx.x / G, lt = threadIdx.x - tr * G;
+  filter12(sm12 + (size_t)tr * S, H, lt, d.twH, d.gH);
+  for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
+    const int y = idx / P, t = idx - y * P;
+    const int xr = xbase + 2 * t, xi = xr + 1;
+    const float2 v = sm12[(size_t)t * S + pad16(y)];
+    float* row = d.steric + (size_t)y * W;
+    if (xr < W) row[xr] = v.x;
+    if (xi < W) row[xi] = -v.y;
+  }
+}
+
+// 256 * 12 / N (rows) or 384 * 12 / N (columns) transforms of N + N / 16 values
+constexpr size_t kFft12RowsSmem = (size_t)256 * 12 * 17 / 16 * sizeof(float2) + 256;
+constexpr size_t kFft12ColsSmem = (size_t)384 * 12 * 17 / 16 * sizeof(float2) + 256;
+void launch_fft12_rows(const Launch& L) { k_fft12_rows<<<L.grid, 256, kFft12RowsSmem, L.s>>>(L.d, L.off, L.n); }
+void launch_fft12_cols(const Launch& L) { k_fft12_cols<<<L.grid, 384, kFft12ColsSmem, L.s>>>(L.d, L.off, L.n); }
 
 // shared memory of a CTA: (row pass, 256 threads) 256 E / N transforms or (column pass,
 // 4096 / E threads) 4096 / N transforms, of N + N / 16 values each

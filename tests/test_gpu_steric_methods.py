@@ -50,3 +50,13 @@ def test_direct_filter_rollout_against_the_oracle():
     assert O.rel_l2(st.f_grid.cpu().numpy(), s.f_grid) <= 1e-5
     # the field of the final positions, which carry 20 steps of drift: the parity bar
     assert O.rel_l2(st.steric.cpu().numpy(), s.steric) <= 1e-5
+
+
+@pytest.mark.parametrize("H,W", [(96, 192), (384, 48), (24, 1536), (12, 12), (192, 128)])
+def test_three_times_power_of_two_sides(H, W):
+    # sides 3 * 2^a take the twelve-values-per-thread register FFT (radix-4 passes + radix 3)
+    sc = scenarios.make_scenario(H, W, 3, 6 if min(H, W) < 24 else 16, seed=7)
+    cfg = baseline_config()
+    ref = O.update_steric_potential(H, W, sc.position, cfg.steric_sigma, cfg.steric_scatter_value)
+    got = _steric(sc, 1)
+    assert O.rel_l2(got, ref) <= 1e-5, (H, W, O.rel_l2(got, ref))
