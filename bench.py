@@ -188,7 +188,8 @@ def batch_section(args, flush):
     tuned, tune_ms = autotune.tune(sts, [cfg] * len(scs), [0.01] * len(scs), actuations=acts, steps=10, warmup=4)
     shape = tuned["lbm_shape"]
     plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs), lbm_shape=shape,
-                           fft_values=tuned["fft_values"], bin_threads=tuned["bin_threads"])
+                           fft_values=tuned["fft_values"], bin_threads=tuned["bin_threads"],
+                           bin_sort_capacity=tuned["bin_sort_capacity"])
     stream = torch.cuda.current_stream()
     plan.begin(sts, actuations=acts)
     plan.advance(6, use_graph=True)
@@ -262,6 +263,7 @@ def batch_section(args, flush):
                                  "note": "opt-in steric_method=2, no L2 flush between steps"},
         "autotune": {"dense_pass_shape": {"cells_per_lane": shape[0], "rows_per_cta": shape[1]},
                      "fft_values_per_thread": tuned["fft_values"], "bin_threads": tuned["bin_threads"],
+                     "bin_sort_capacity": tuned["bin_sort_capacity"],
                      "ms_per_step_by_candidate": tune_ms},
         "lbm_ms_per_launch": lbm_ms,
         "kernels_ms_per_step": {k: ms / 10 for k, (ms, n) in prof.items() if n},

@@ -97,6 +97,8 @@ SIGNATURES = {
     "mc_plan_fft_values_per_thread": (ctypes.c_int32, [ctypes.c_void_p]),
     "mc_plan_set_bin_threads": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "mc_plan_bin_threads": (ctypes.c_int32, [ctypes.c_void_p]),
+    "mc_plan_set_bin_sort_capacity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "mc_plan_bin_sort_capacity": (ctypes.c_int32, [ctypes.c_void_p]),
     "mc_plan_get_lbm_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
                                              ctypes.POINTER(ctypes.c_int32)]),
     "mc_plan_workspace_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),

@@ -6,7 +6,7 @@ Three kernels have a free shape:
   * the power-of-two FFT kernels of the steric filter: each thread holds 4, 8 or 16
     values in registers (more values: fewer instructions per value; fewer: more threads);
   * the tile kernel that sorts the IB and cloud-in-cell contributions: 128 or 256 threads
-    per CTA.
+    per CTA, and 512 or 1024 contributions per tile sorted in shared memory.
 Which shape is fastest depends on the rollout sizes of a plan (grid widths, how many CTAs
 a step launches, how many tiles carry IB forcing), so the tuner times whole
 graph-replayed steps of the actual plan on scratch copies of the states: first the FFT
@@ -27,7 +27,7 @@ from .engine import DeviceState, Plan
 CELLS_PER_LANE = (1, 2, 4)
 ROWS_PER_CTA = (2, 4, 8)
 FFT_VALUES = (4, 8, 16)
-BIN_THREADS = (256, 128)
+BIN_SHAPES = ((256, 1024), (128, 1024), (128, 512), (256, 512))  # (threads per CTA, shared sort capacity)
 
 _cache: dict[str, tuple[dict, dict]] = {}
 
@@ -71,7 +71,8 @@ def _time(scratch, cfgs, dts, actuations, steps, warmup, **shape):
 def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, fft_values=None, use_cache=True):
     """Time ``steps`` graph-replayed steps of the plan for the candidate shapes and return
     ``(best, timings)``: best = {"lbm_shape": (cells_per_lane, rows_per_cta),
-    "fft_values": 4 | 8 | 16, "bin_threads": 128 | 256}, timings = {label: ms per step}.  The caller's states are
+    "fft_values": 4 | 8 | 16, "bin_threads": 128 | 256, "bin_sort_capacity": 512 | 1024},
+    timings = {label: ms per step}.  The caller's states are
     not modified."""
     key = signature(states, cfgs, dts)
     if use_cache and key in _cache:
@@ -91,13 +92,15 @@ def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, ff
         lt[shape] = _time(scratch, cfgs, dts, actuations, steps, warmup, lbm_shape=shape, fft_values=fft_best)
         timings[f"lbm{shape[0]}x{shape[1]}"] = lt[shape]
     lbm_best = min(lt, key=lt.get)
-    bt = {256: lt[lbm_best]}
-    for t in BIN_THREADS:
-        if t not in bt:
-            bt[t] = _time(scratch, cfgs, dts, actuations, steps, warmup, lbm_shape=lbm_best, fft_values=fft_best,
-                          bin_threads=t)
-        timings[f"bins{t}"] = bt[t]
-    best = {"lbm_shape": lbm_best, "fft_values": fft_best, "bin_threads": min(bt, key=bt.get)}
+    bt = {(256, 1024): lt[lbm_best]}
+    for t, cap in BIN_SHAPES:
+        if (t, cap) not in bt:
+            bt[(t, cap)] = _time(scratch, cfgs, dts, actuations, steps, warmup, lbm_shape=lbm_best,
+                                 fft_values=fft_best, bin_threads=t, bin_sort_capacity=cap)
+        timings[f"bins{t}x{cap}"] = bt[(t, cap)]
+    bins_best = min(bt, key=bt.get)
+    best = {"lbm_shape": lbm_best, "fft_values": fft_best, "bin_threads": bins_best[0],
+            "bin_sort_capacity": bins_best[1]}
     _cache[key] = (best, timings)
     return best, timings
 
@@ -106,4 +109,4 @@ def tuned_plan(states, cfgs, dts, actuations=None, **kw) -> Plan:
     """A plan for these rollouts with the autotuned launch shapes."""
     best, _ = tune(states, cfgs, dts, actuations=actuations, **kw)
     return Plan.for_states(states, cfgs, dts, lbm_shape=best["lbm_shape"], fft_values=best["fft_values"],
-                           bin_threads=best["bin_threads"])
+                           bin_threads=best["bin_threads"], bin_sort_capacity=best["bin_sort_capacity"])

@@ -119,8 +119,9 @@ __device__ __forceinline__ void head_work(const RDesc& d, const BinView& v, int 
   ib_head(d, parity, cell, acc, slot, len, run_pos);
 }
 
-// One CTA (256 threads) on one bin tile: sort the tile's contributions by (cell, k) and
-// reduce every cell's run.  skeys: dynamic shared memory of 4 * capS words, capS >= the
+// One CTA on one bin tile: sort the tile's contributions by (cell, k) and reduce every
+// touched cell's run.  Tiles of at most capS contributions are sorted in shared memory;
+// larger ones take the global-arena path.  skeys: dynamic shared memory of 4 * capS words, capS <= the
 // bin capacity of every rollout of the launch (a power of two).
 __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned* skeys, int capS) {
   const int kCapS = capS;
@@ -128,6 +129,7 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
   __shared__ int cnt[kBinTile * kBinTile];
   __shared__ int cpos[kBinTile * kBinTile];
   __shared__ int hpos[kBinTile * kBinTile];  // rank of a touched cell among the tile's touched cells
+  __shared__ int tlist[kBinTile * kBinTile];  // the touched cells, by rank
   __shared__ int s_spill, s_heads, s_base, s_fill;
   const BinView v = bin_view(d, which);
   if (v.count == 0) return;
@@ -137,7 +139,8 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
   const int ntiles = d.ntile_x * d.ntile_y;
   int* bin = v.store + (size_t)t * v.cap;
 
-  if (total <= v.cap) {
+  // fast path: the whole tile sorted in shared memory (capacity capS <= the bin capacity)
+  if (total <= min(v.cap, kCapS)) {
     // shared layout: [0, C) packed (cell, rank) | [C, 2C) k | [2C, 3C) sorted k | [3C, 4C) sorted w
     unsigned* lr = skeys;
     int* kin = reinterpret_cast<int*>(skeys + kCapS);
@@ -187,8 +190,10 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
       if (tid == 31) s_heads = inz;
     }
     __syncthreads();
-    // one slot range per tile for its touched cells (IB)
+    // one slot range per tile for its touched cells (IB); the touched cells listed by rank
     if (which == 0 && tid == 0) s_base = atomicAdd(v.ctl + 2, s_heads);
+    for (int c = tid; c < kBinTile * kBinTile; c += blockDim.x)
+      if (cnt[c] > 0) tlist[hpos[c]] = c;
     for (int i = tid; i < total; i += blockDim.x) {
       const unsigned key = lr[i];
       const int lc = (int)(key >> 24), pos = (int)(key & 0xffffffu);
@@ -197,10 +202,11 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
       wout[cpos[lc] + pos] = v.w[k];
     }
     __syncthreads();
-    // one thread per cell: order its run by k (runs are short), then reduce it
-    for (int c = tid; c < kBinTile * kBinTile; c += blockDim.x) {
+    // one thread per touched cell: order its run by k (runs are short), then reduce it
+    const int nheads = s_heads;
+    for (int hi = tid; hi < nheads; hi += blockDim.x) {
+      const int c = tlist[hi];
       const int len = cnt[c];
-      if (len == 0) continue;
       int* rk = kout + cpos[c];
       float* rw = wout + cpos[c];
       for (int a = 1; a < len; ++a) {
@@ -247,13 +253,14 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
   const int base = ntiles * v.cap + s_spill;
   unsigned* bufA = reinterpret_cast<unsigned*>(v.store) + base;
   unsigned* bufB = bufA + total;
-  for (int i = tid; i < v.cap; i += blockDim.x) {
+  const int nbin = min(total, v.cap);
+  for (int i = tid; i < nbin; i += blockDim.x) {
     const int k = bin[i];
     bufB[i] = (local_of(d, v.cell[k]) << 24) | (unsigned)k;
   }
-  if (tid == 0) s_fill = v.cap;
+  if (tid == 0) s_fill = nbin;
   __syncthreads();
-  {
+  if (total > v.cap) {
     // the overflow list is unordered: every thread scans a stride of it for this tile's
     // entries (their order is restored by the sort below)
     const int no = v.ctl[0];

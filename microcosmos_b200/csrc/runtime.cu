@@ -98,7 +98,8 @@ struct mc_plan {
   int tile_grid = 1;  // CTAs walking the tile lists
   long long n_tiles = 0;  // bin tiles of all rollouts
   int bin_threads = 256;  // threads per CTA of the tile kernel
-  int ib_capS = 0, c_capS = 0;  // largest bin capacity of the plan (tile-sort shared memory)
+  int ib_capS = 0, c_capS = 0;  // largest bin capacity of the plan
+  int ib_smem = 0, c_smem = 0;  // contributions a tile may hold to be sorted in shared memory
   Region r_off[K_COUNT];
   std::vector<int> off[K_COUNT];
   int grid[K_COUNT] = {};
@@ -627,7 +628,7 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
     timed(p, 1, s, capture, [&] {
       mc::Launch l = L(p, K_TILES, s);
       l.grid = p->tile_grid;
-      mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_cic), at<int>(p->ws, p->r_wl_ctl) + 1, 1, 0, p->c_capS,
+      mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_cic), at<int>(p->ws, p->r_wl_ctl) + 1, 1, 0, p->c_smem,
                            p->bin_threads);
     });
     k += 1;
@@ -696,7 +697,7 @@ int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
   timed(p, 6, s, capture, [&] {
     mc::Launch l = L(p, K_TILES, s);
     l.grid = p->tile_grid;
-    mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_ib), at<int>(p->ws, p->r_wl_ctl), 0, parity, p->ib_capS,
+    mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_ib), at<int>(p->ws, p->r_wl_ctl), 0, parity, p->ib_smem,
                          p->bin_threads);
   });
   ++k;
@@ -1075,6 +1076,11 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       p->ib_capS = std::max(p->ib_capS, h.ib_cap);
       p->c_capS = std::max(p->c_capS, h.c_cap);
     }
+    // at most 1024 contributions per tile are sorted in shared memory (16 KB per CTA): one
+    // dense rollout of a batch (whose bins are sized for its density) must not cut the
+    // residency of every CTA of the launch; its denser tiles sort in the global arena
+    p->ib_smem = std::min(p->ib_capS, 1024);
+    p->c_smem = std::min(p->c_capS, 1024);
   }
   p->ws_bytes = lay.cur;
   // CTA offset tables
@@ -1149,6 +1155,20 @@ mc_status mc_plan_set_bin_threads(mc_plan* p, int32_t threads) {
 }
 
 int32_t mc_plan_bin_threads(const mc_plan* p) { return p ? p->bin_threads : 0; }
+
+mc_status mc_plan_set_bin_sort_capacity(mc_plan* p, int32_t entries) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (p->bound) return fail(MC_ERR_INVALID, "the tile sort capacity is set before mc_plan_bind()");
+  if (entries != 0 && (entries < 256 || entries > 8192 || (entries & (entries - 1))))
+    return fail(MC_ERR_INVALID, "entries must be 0 (default 1024) or a power of two in 256..8192");
+  const int e = entries ? entries : 1024;
+  p->ib_smem = std::min(p->ib_capS, e);
+  p->c_smem = std::min(p->c_capS, e);
+  return MC_OK;
+}
+
+int32_t mc_plan_bin_sort_capacity(const mc_plan* p) { return p ? p->ib_smem : 0; }
 
 mc_status mc_plan_set_fft_values_per_thread(mc_plan* p, int32_t values) {
   g_err.clear();

@@ -185,14 +185,16 @@ class Record:
 class Plan:
     """A bound plan for a list of rollouts (dims + config + dt + topology each)."""
 
-    def __init__(self, specs, device="cuda", lbm_shape=None, steric_method=0, fft_values=0, bin_threads=0):
+    def __init__(self, specs, device="cuda", lbm_shape=None, steric_method=0, fft_values=0, bin_threads=0,
+                 bin_sort_capacity=0):
         """specs: list of (H, W, N, pairs(E,2) int32, bending_pairs(B,2) int32, cfg, dt).
         ``lbm_shape`` = (cells_per_lane, rows_per_cta) of the dense pass (default: the
         library's choice; ``microcosmos_b200.autotune`` picks one by timing).
         ``steric_method``: 0 = per rollout (direct convolution where it applies, else
         FFT), 1 = FFT, 2 = direct convolution.  ``fft_values``: values per thread of the
         power-of-two FFT kernels (4, 8, 16; 0 = the library's choice).  ``bin_threads``:
-        threads per CTA of the contribution-sorting tile kernel (64, 128, 256; 0 = 256)."""
+        threads per CTA of the contribution-sorting tile kernel (64, 128, 256; 0 = 256).
+        ``bin_sort_capacity``: contributions per tile sorted in shared memory (0 = 1024)."""
         _require_cuda()
         lib = _lib.load()
         n = len(specs)
@@ -224,6 +226,8 @@ class Plan:
             _lib.check(lib.mc_plan_set_fft_values_per_thread(h, int(fft_values)))
         if bin_threads:
             _lib.check(lib.mc_plan_set_bin_threads(h, int(bin_threads)))
+        if bin_sort_capacity:
+            _lib.check(lib.mc_plan_set_bin_sort_capacity(h, int(bin_sort_capacity)))
         nbytes = lib.mc_plan_workspace_bytes(h)
         self.workspace = torch.empty(nbytes + 256, dtype=torch.uint8, device=device)
         base = self.workspace.data_ptr()
@@ -234,10 +238,10 @@ class Plan:
 
     @classmethod
     def for_states(cls, states, cfgs, dts, device="cuda", lbm_shape=None, steric_method=0, fft_values=0,
-                   bin_threads=0):
+                   bin_threads=0, bin_sort_capacity=0):
         specs = [(s.H, s.W, s.N, s.pairs, s.bending_pairs, c, d) for s, c, d in zip(states, cfgs, dts)]
         return cls(specs, device=device, lbm_shape=lbm_shape, steric_method=steric_method, fft_values=fft_values,
-                   bin_threads=bin_threads)
+                   bin_threads=bin_threads, bin_sort_capacity=bin_sort_capacity)
 
     def bin_threads(self):
         return int(_lib.load().mc_plan_bin_threads(self._h))

@@ -164,4 +164,7 @@ def test_tile_kernel_threads_setter(lib):
     assert lib.mc_plan_set_bin_threads(h, 96) == _lib.MC_ERR_INVALID
     assert lib.mc_plan_set_fft_values_per_thread(h, 8) == _lib.MC_OK and lib.mc_plan_fft_values_per_thread(h) == 8
     assert lib.mc_plan_set_fft_values_per_thread(h, 5) == _lib.MC_ERR_INVALID
+    assert lib.mc_plan_bin_sort_capacity(h) == 1024
+    assert lib.mc_plan_set_bin_sort_capacity(h, 512) == _lib.MC_OK and lib.mc_plan_bin_sort_capacity(h) == 512
+    assert lib.mc_plan_set_bin_sort_capacity(h, 300) == _lib.MC_ERR_INVALID
     lib.mc_plan_destroy(h)
