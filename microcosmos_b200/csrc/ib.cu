@@ -425,43 +425,40 @@ __global__ void __launch_bounds__(256) k_ib_spread(const RDesc* __restrict__ D, 
                                                    int it) {
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
-  if (it >= d.ib_iters) return;
-  const int nheads = d.ib_ctl[2];
-  const int stride = (off[r + 1] - off[r]) * blockDim.x;  // the rollout's CTAs cover its heads in strides
-  for (int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x; p < nheads; p += stride) {
-    const int len = d.h_len[p];
-    const int* rn = d.ib_store + d.h_start[p];      // contributing nodes, in k order
-    const float* rw = d.ib_store_w + d.h_start[p];  // their weights
-    float dx = 0.0f, dy = 0.0f;
-    // runs are short: fetch 8 entries at a time (the last group predicated) so that all
-    // their loads are in flight together; the sum keeps the run order
-    for (int j = 0; j < len; j += 8) {
-      int nd[8];
-      float w[8], ex[8], ey[8];
+  const int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
+  if (it >= d.ib_iters || p >= d.ib_ctl[2]) return;
+  const int len = d.h_len[p];
+  const int* rn = d.ib_store + d.h_start[p];      // contributing nodes, in k order
+  const float* rw = d.ib_store_w + d.h_start[p];  // their weights
+  float dx = 0.0f, dy = 0.0f;
+  // runs are short: fetch 8 entries at a time (the last group predicated) so that all
+  // their loads are in flight together; the sum keeps the run order
+  for (int j = 0; j < len; j += 8) {
+    int nd[8];
+    float w[8], ex[8], ey[8];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const bool ok = j + q < len;
-        nd[q] = ok ? rn[j + q] : 0;
-        w[q] = ok ? rw[j + q] : 0.0f;
-      }
+    for (int q = 0; q < 8; ++q) {
+      const bool ok = j + q < len;
+      nd[q] = ok ? rn[j + q] : 0;
+      w[q] = ok ? rw[j + q] : 0.0f;
+    }
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const bool ok = j + q < len;
-        ex[q] = ok ? d.delta[2 * nd[q]] : 0.0f;
-        ey[q] = ok ? d.delta[2 * nd[q] + 1] : 0.0f;
-      }
+    for (int q = 0; q < 8; ++q) {
+      const bool ok = j + q < len;
+      ex[q] = ok ? d.delta[2 * nd[q]] : 0.0f;
+      ey[q] = ok ? d.delta[2 * nd[q] + 1] : 0.0f;
+    }
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        if (j + q < len) {
-          dx = dx + ex[q] * w[q];
-          dy = dy + ey[q] * w[q];
-        }
+    for (int q = 0; q < 8; ++q) {
+      if (j + q < len) {
+        dx = dx + ex[q] * w[q];
+        dy = dy + ey[q] * w[q];
       }
     }
-    const float inv = d.s_inv[p];
-    d.s_ucx[p] = d.s_ucx[p] + dx * inv;
-    d.s_ucy[p] = d.s_ucy[p] + dy * inv;
   }
+  const float inv = d.s_inv[p];
+  d.s_ucx[p] = d.s_ucx[p] + dx * inv;
+  d.s_ucy[p] = d.s_ucy[p] + dy * inv;
 }
 
 // ---------------------------------------------------------------- fused IB iterations
@@ -615,9 +612,8 @@ __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D
                                                      int parity) {
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
-  const int nheads = d.ib_ctl[2];
-  const int stride = (off[r + 1] - off[r]) * blockDim.x;
-  for (int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x; p < nheads; p += stride) {
+  const int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
+  if (p >= d.ib_ctl[2]) return;
   float ucx = d.s_ucx[p], ucy = d.s_ucy[p];
   const float c2 = clamp_factor(ucx, ucy, d.vmax);
   ucx = ucx * c2;
@@ -638,7 +634,6 @@ __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D
   d.fov[HW + cell] = Fy;
   const int y = cell / d.W, x = cell - y * d.W;
   d.lbm_flag[(parity & 1) * d.lbm_tx * d.lbm_ty + (y / d.lbm_th) * d.lbm_tx + x / d.lbm_tw] = 1;
-  }
 }
 
 // Node reaction (fluid.py:364-382), final wrap (simulate.py:97-98), non-finite check and

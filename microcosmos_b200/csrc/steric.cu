@@ -707,7 +707,9 @@ __global__ void __launch_bounds__(4096 / E) k_fftreg_cols(const RDesc* __restric
   const RDesc& d = D[r];
   const int W = d.W, H = d.H, logN = d.fft_logH;
   const int G = H / E, P = blockDim.x / G;
-  const int S = H + (H >> 4);
+  // one extra slot per column pair staggers the pairs over the shared-memory banks when the
+  // tile is staged row by row
+  const int S = H + (H >> 4) + 1;
   const int xbase = (blockIdx.x - off[r]) * 2 * P;
   for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
     const int y = idx / P, t = idx - y * P;
@@ -825,7 +827,7 @@ __global__ void __launch_bounds__(384) k_fft12_cols(const RDesc* __restrict__ D,
   const RDesc& d = D[r];
   const int W = d.W, H = d.H;
   const int G = H / 12, P = blockDim.x / G;
-  const int S = H + (H >> 4);
+  const int S = H + (H >> 4) + 1;  // staggered over the banks, as in k_fftreg_cols
   const int xbase = (blockIdx.x - off[r]) * 2 * P;
   for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
     const int y = idx / P, t = idx - y * P;
@@ -848,14 +850,14 @@ __global__ void __launch_bounds__(384) k_fft12_cols(const RDesc* __restrict__ D,
 
 // 256 * 12 / N (rows) or 384 * 12 / N (columns) transforms of N + N / 16 values
 constexpr size_t kFft12RowsSmem = (size_t)256 * 12 * 17 / 16 * sizeof(float2) + 256;
-constexpr size_t kFft12ColsSmem = (size_t)384 * 12 * 17 / 16 * sizeof(float2) + 256;
+constexpr size_t kFft12ColsSmem = ((size_t)384 * 12 * 17 / 16 + 384) * sizeof(float2) + 256;
 void launch_fft12_rows(const Launch& L) { k_fft12_rows<<<L.grid, 256, kFft12RowsSmem, L.s>>>(L.d, L.off, L.n); }
 void launch_fft12_cols(const Launch& L) { k_fft12_cols<<<L.grid, 384, kFft12ColsSmem, L.s>>>(L.d, L.off, L.n); }
 
 // shared memory of a CTA: (row pass, 256 threads) 256 E / N transforms or (column pass,
 // 4096 / E threads) 4096 / N transforms, of N + N / 16 values each
 size_t fftreg_smem(int e) { return (size_t)256 * e * 17 / 16 * sizeof(float2); }
-constexpr size_t kFftColsSmem = (size_t)4096 * 17 / 16 * sizeof(float2);
+constexpr size_t kFftColsSmem = ((size_t)4096 * 17 / 16 + 256) * sizeof(float2);
 
 void launch_fftreg_rows(const Launch& L, int e) {
   if (e == 16) k_fftreg_rows<16><<<L.grid, 256, fftreg_smem(16), L.s>>>(L.d, L.off, L.n);
