@@ -45,9 +45,14 @@ typedef enum mc_status {
 #define MC_FLAG_NONFINITE 1u /* a node position/velocity became NaN/Inf */
 #define MC_FLAG_TIMEOUT 2u   /* a bounded device-side wait gave up; the step's results are invalid */
 
-/* Scalar fields of ConstraintSolverConfig used by the PBD scheme
- * (src/microcosmos/solver/config.py:9-72).  The callable `bending_constraint` is fixed
- * to pbd_rod_constraint; `cycles_per_constraint` is never read by the reference. */
+/* Scalar fields of ConstraintSolverConfig (src/microcosmos/solver/config.py:9-72).  The
+ * callable `bending_constraint` plugin slot is selected by solver_type:
+ * MC_SOLVER_PBD = pbd_rod_constraint (solver/pbd.py:14-91), MC_SOLVER_COSSERAT =
+ * stable_cosserat_constraint (solver/stable_cosserat.py:13-119, inertia weight
+ * 1/solver_dt^2 where solver_dt is the config's own `dt` field).
+ * `cycles_per_constraint` is never read by the reference. */
+#define MC_SOLVER_PBD 0
+#define MC_SOLVER_COSSERAT 1
 typedef struct mc_config {
   int32_t cycles_per_step;
   float stiffness_stretch;
@@ -57,7 +62,7 @@ typedef struct mc_config {
   float viscosity;
   float max_fluid_velocity;
   int32_t ibm_iterations;
-  float synthetic_node_width; /* must be 0 (the reference default) */
+  float synthetic_node_width; /* >= 0; > 0 puts a pair of IB points at +- width along the chain normal */
   int32_t ibm_kernel_size;    /* 1..8 */
   float ibm_relaxation;
   float node_mass;
@@ -68,6 +73,8 @@ typedef struct mc_config {
   float steric_sigma;
   int32_t steric_neighbor_skip;
   float steric_scatter_value;
+  int32_t solver_type;        /* MC_SOLVER_PBD or MC_SOLVER_COSSERAT */
+  double solver_dt;           /* ConstraintSolverConfig.dt (a Python float; Cosserat inertia weight), > 0 */
 } mc_config;
 
 /* Sizes of one rollout.  H, W: grid_shape (the fluid grid equals the domain grid). */

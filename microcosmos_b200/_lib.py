@@ -41,6 +41,8 @@ class McConfig(ctypes.Structure):
         ("steric_sigma", ctypes.c_float),
         ("steric_neighbor_skip", ctypes.c_int32),
         ("steric_scatter_value", ctypes.c_float),
+        ("solver_type", ctypes.c_int32),
+        ("solver_dt", ctypes.c_double),
     ]
 
 

@@ -1,9 +1,11 @@
 """Solver configuration, mirroring ``ConstraintSolverConfig`` and its presets
 (src/microcosmos/solver/config.py:9-171).
 
-``bending_constraint`` keeps the reference's plugin slot.  The device implements the
-PBD rod constraint (src/microcosmos/solver/pbd.py:14-91) only; selecting the
-stable-Cosserat plugin raises ``NotImplementedError`` when a plan is built.
+``bending_constraint`` keeps the reference's plugin slot.  The device implements both of
+the reference's rod constraints: the PBD rod constraint (src/microcosmos/solver/pbd.py:14-91)
+and the stable-Cosserat projective-dynamics constraint
+(src/microcosmos/solver/stable_cosserat.py:13-119); any other callable raises
+``NotImplementedError`` when a plan is built.
 """
 from __future__ import annotations
 
@@ -18,9 +20,10 @@ def pbd_rod_constraint(*args, **kwargs):
 
 
 def stable_cosserat_constraint(*args, **kwargs):
-    """Marker for the stable-Cosserat plugin (src/microcosmos/solver/stable_cosserat.py:13),
-    which this library does not implement."""
-    raise NotImplementedError("the stable Cosserat constraint is not implemented on the device")
+    """Marker for the stable-Cosserat plugin (src/microcosmos/solver/stable_cosserat.py:13).
+    It runs on the device inside ``simulate``/``step`` (with ``solver_type="cosserat"``);
+    it is not callable on host arrays."""
+    raise NotImplementedError("stable_cosserat_constraint runs on the device inside simulate()/step()")
 
 
 @dataclasses.dataclass(frozen=True)

@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(256) k_ib_interp(const RDesc* __restrict__ D, 
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int node = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
-  if (node >= d.N || it >= d.ib_iters) return;
+  if (node >= d.NI || it >= d.ib_iters) return;  // node = IB point
   float ux, uy;
   stencil_sum_any(d, node, d.s_ucx, d.s_ucy, ux, uy);
   const float sx = (d.nvl[2 * node] - ux) * d.relax;
@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, co
   const int nheads = __ldcg(d.ib_ctl + 2);
   const int K2 = d.K * d.K;
   for (int it = 0; it < d.ib_iters; ++it) {
-    for (int node = t0; node < d.N; node += stride) {
+    for (int node = t0; node < d.NI; node += stride) {  // IB points
       float ux = 0.0f, uy = 0.0f;
       const int base = node * K2;
       if (K2 == 16) {
@@ -654,6 +654,13 @@ __global__ void __launch_bounds__(256) k_reaction(const RDesc* __restrict__ D, c
   if (d.enable_fluid) {
     float fx, fy;
     stencil_sum_any(d, node, d.s_fx, d.s_fy, fx, fy);
+    if (d.NI > d.N) {
+      // synthetic pair: the mean of the two points' forces (fluid.py:371-374)
+      float gx, gy;
+      stencil_sum_any(d, node + d.N, d.s_fx, d.s_fy, gx, gy);
+      fx = 0.5f * (fx + gx);
+      fy = 0.5f * (fy + gy);
+    }
     vx = vx - (fx / d.node_mass) / d.sdt_x;
     vy = vy - (fy / d.node_mass) / d.sdt_y;
     d.vel[2 * node] = vx;

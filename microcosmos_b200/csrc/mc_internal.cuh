@@ -33,7 +33,8 @@ struct RDesc {
   // sizes
   int H, W, N, E, B, K;  // K = ibm_kernel_size
   int ncomp;             // rod components
-  int M;                 // IB contributions = N*K*K
+  int NI;                // IB points: N, or 2N with synthetic node pairs
+  int M;                 // IB contributions = NI*K*K
   int ntile_x, ntile_y;  // binning tiles (kBinTile)
   int lbm_tx, lbm_ty;    // LBM tiles
   int lbm_tw;            // LBM tile width in cells (32 * cells per lane)
@@ -41,6 +42,10 @@ struct RDesc {
   int max_comp_nodes, max_comp_edges, max_comp_pairs;
   // configuration
   float dt, damping, k_stretch, k_shear, vmax, relax, node_mass, wp, wm;
+  int solver;       // 0 = PBD rod constraint, 1 = stable Cosserat (projective dynamics)
+  float cos_w;      // Cosserat inertia weight 1 / dt_config^2 (float32 of the double value)
+  float syn_w;      // synthetic_node_width (0: the IB points are the nodes)
+  float syn_ms;     // mean of the two grid scales (float32), multiplies the synthetic offset
   float vmax_q4;  // (vmax / 2)^2 rounded down: below it every velocity clamp factor is exactly 1
   float st_strength, st_sigma, st_scatter;
   float st_2s2, st_norm, st_coef;  // 2 sigma^2, 2 pi sigma^2, scatter / sigma^2 (float32 of the double values)
@@ -104,8 +109,8 @@ struct RDesc {
   float* prev;         // (N,2)
   float* pred;         // (N,2)
   float* predw;        // (N,2) prediction wrapped into the domain (steric sampling)
-  float* nvl;          // (N,2) node velocity in lattice units
-  float* delta;        // (N,2) IB per-iteration correction
+  float* nvl;          // (NI,2) IB point velocity in lattice units
+  float* delta;        // (NI,2) IB per-iteration correction
   // Deterministic scatter-add bins.  Contribution k goes to bin tile t at
   // store[t * cap + atomic position]; a tile that fills up spills into the overflow list.
   // store[ntiles * cap ...] is an arena for sorting tiles with more than cap entries.

@@ -174,6 +174,28 @@ __device__ __forceinline__ float2 edge_force(const RDesc& d, float th, float L0,
   return make_float2(((stx + shx * d.k_shear) * d.k_stretch) * 0.5f, ((sty + shy * d.k_shear) * d.k_stretch) * 0.5f);
 }
 
+// IB point p in lattice units (fluid.py:236-263): node p's position times the grid scale,
+// or with synthetic pairs (p < N: +, p >= N: -, node = p mod N) that point moved by
+// width * perp * mean_scale, where perp is the normal of the chain tangent, the sum of the
+// node's edge vectors in the reference's update order (src updates, then tgt updates),
+// normalised by sqrt(|t|^2 + EPSIL).
+__device__ __forceinline__ float2 ib_point(const RDesc& d, int p, int node, float x, float y) {
+  const float gx = x * d.scale_x, gy = y * d.scale_y;
+  if (!(d.syn_w > 0.0f)) return make_float2(gx, gy);
+  float tx = 0.0f, ty = 0.0f;
+  for (int j = d.ne_off[node]; j < d.ne_off[node + 1]; ++j) {
+    const int e = d.ne_idx[j] >> 1;
+    const int s = d.pairs[2 * e], g = d.pairs[2 * e + 1];
+    const float2 ev = min_image(d.pos[2 * g], d.pos[2 * g + 1], d.pos[2 * s], d.pos[2 * s + 1], (float)d.W, (float)d.H);
+    tx = tx + ev.x;
+    ty = ty + ev.y;
+  }
+  const float nrm = sqrtf((tx * tx + ty * ty) + MC_EPSIL);
+  const float ux = tx / nrm, uy = ty / nrm;
+  const float ox = (d.syn_w * (-uy)) * d.syn_ms, oy = (d.syn_w * ux) * d.syn_ms;
+  return p < d.N ? make_float2(gx + ox, gy + oy) : make_float2(gx - ox, gy - oy);
+}
+
 // Velocity (simulate.py:83-84), the IB point in lattice units (fluid.py:236-239) and its
 // K x K stencil (fluid.py:40-79) appended to the IB bins, and the clearing of the node's
 // CIC deposit cells (the deposit grid stays zero between steps).  The stencil spans at
@@ -181,21 +203,25 @@ __device__ __forceinline__ float2 edge_force(const RDesc& d, float th, float L0,
 __global__ void __launch_bounds__(256) k_stencil(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
-  const int gi = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
-  if (gi >= d.N) return;
+  const int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;  // IB point
+  if (p >= d.NI) return;
+  const int gi = p < d.N ? p : p - d.N;
   const float x = d.pos[2 * gi], y = d.pos[2 * gi + 1];
   const float vx = (x - d.prev[2 * gi]) / d.dt, vy = (y - d.prev[2 * gi + 1]) / d.dt;
-  d.vel[2 * gi] = vx;
-  d.vel[2 * gi + 1] = vy;
-  if (d.enable_steric) {
+  if (p < d.N) {
+    d.vel[2 * gi] = vx;
+    d.vel[2 * gi + 1] = vy;
+    if (d.enable_steric) {
 #pragma unroll
-    for (int c = 0; c < 4; ++c) d.dep[d.c_cell[c * d.N + gi]] = 0.0f;
+      for (int c = 0; c < 4; ++c) d.dep[d.c_cell[c * d.N + gi]] = 0.0f;
+    }
   }
   if (!d.enable_fluid) return;
   const int K = d.K, K2 = K * K;
-  const float gx = x * d.scale_x, gy = y * d.scale_y;
-  d.nvl[2 * gi] = (vx * d.scale_x) * d.dt;
-  d.nvl[2 * gi + 1] = (vy * d.scale_y) * d.dt;
+  const float2 gp = ib_point(d, p, gi, x, y);
+  const float gx = gp.x, gy = gp.y;
+  d.nvl[2 * p] = (vx * d.scale_x) * d.dt;
+  d.nvl[2 * p + 1] = (vy * d.scale_y) * d.dt;
   const int half = (K - 1) / 2;
   const float hw = (float)K / 2.0f;
   const float sx = floorf(gx) - (float)half, sy = floorf(gy) - (float)half;
@@ -265,7 +291,7 @@ __global__ void __launch_bounds__(256) k_stencil(const RDesc* __restrict__ D, co
         if (b < K) {
           const int ys = (cy[b] / kBinTile != ty0) ? 1 : 0;
           const int g = xs + 2 * ys;
-          const int k = gi * K2 + a * K + b;
+          const int k = p * K2 + a * K + b;
           d.ib_cell[k] = cy[b] * d.W + cx[a];
           d.ib_w[k] = (wx[a] * wy[b]) / den;
           int tile, pos;
@@ -296,23 +322,27 @@ __global__ void __launch_bounds__(256) k_stencil16(const RDesc* __restrict__ D, 
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int t = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
-  const int gi = t >> 4, s = t & 15;
+  const int p = t >> 4, s = t & 15;  // IB point, stencil entry
   const int lane = threadIdx.x & 31;
   const unsigned gmask = 0xffffu << (lane & 16);
-  if (gi >= d.N) return;  // both halves of a warp exit together unless N is odd
+  if (p >= d.NI) return;  // both halves of a warp exit together unless NI is odd
+  const int gi = p < d.N ? p : p - d.N;
   const float x = d.pos[2 * gi], y = d.pos[2 * gi + 1];
   const float vx = (x - d.prev[2 * gi]) / d.dt, vy = (y - d.prev[2 * gi + 1]) / d.dt;
-  if (s == 0) {
-    d.vel[2 * gi] = vx;
-    d.vel[2 * gi + 1] = vy;
+  if (p < d.N) {
+    if (s == 0) {
+      d.vel[2 * gi] = vx;
+      d.vel[2 * gi + 1] = vy;
+    }
+    if (d.enable_steric && s < 4) d.dep[d.c_cell[s * d.N + gi]] = 0.0f;
   }
-  if (d.enable_steric && s < 4) d.dep[d.c_cell[s * d.N + gi]] = 0.0f;
   if (!d.enable_fluid) return;
   const int K = d.K, K2 = K * K;
-  const float gx = x * d.scale_x, gy = y * d.scale_y;
+  const float2 gp = ib_point(d, p, gi, x, y);
+  const float gx = gp.x, gy = gp.y;
   if (s == 0) {
-    d.nvl[2 * gi] = (vx * d.scale_x) * d.dt;
-    d.nvl[2 * gi + 1] = (vy * d.scale_y) * d.dt;
+    d.nvl[2 * p] = (vx * d.scale_x) * d.dt;
+    d.nvl[2 * p + 1] = (vy * d.scale_y) * d.dt;
   }
   const int half = (K - 1) / 2;
   const float hw = (float)K / 2.0f;
@@ -330,7 +360,7 @@ __global__ void __launch_bounds__(256) k_stencil16(const RDesc* __restrict__ D, 
   if (!act) return;
   const int cx = imod_floor((int)(sx + (float)a), d.W);
   const int cy = imod_floor((int)(sy + (float)b), d.H);
-  const int k = gi * K2 + s;
+  const int k = p * K2 + s;
   d.ib_cell[k] = cy * d.W + cx;
   d.ib_w[k] = w / den;
   const int tile = (cy / kBinTile) * d.ntile_x + cx / kBinTile;
@@ -383,6 +413,80 @@ __device__ __forceinline__ void shift_prev(const float (&v)[P], float (&pv)[P]) 
   pv[0] = last_prev;
 }
 
+// Stable-Cosserat iterations of one chain rod (solver/stable_cosserat.py:13-119), same
+// lane layout as the PBD loop below.  Phase 1: the bending pass without over-relaxation,
+// then theta += wrap(atan2(r) - theta) * 0.05 with r the segment's min-image vector.
+// Phase 2: x += (w (y0 - x) + f_j - f_{j-1}) / ((w + H_j) + H_{j-1}), f = (k_s/l)(r/l - d),
+// H = k_s/l^2, y0 the inertial prediction (the positions the kernel started from).
+__device__ __forceinline__ float cos_pull(float th, float sx, float sy) {
+  const float alpha = atan2f(sy, sx);
+  return th + (fmod_floor((alpha - th) + MC_PI_F, MC_2PI_F) - MC_PI_F) * 0.05f;
+}
+
+template <int P>
+__device__ __forceinline__ void cosserat_chain(const RDesc& d, int lane, int nn, int ne, int nb, float (&x)[P],
+                                               float (&y)[P], float (&th)[P], const float (&l0)[P],
+                                               const float (&ra)[P], const float (&kb)[P], const float (&edg)[P]) {
+  const float W = (float)d.W, H = (float)d.H;
+  const float ks = d.k_stretch, w = d.cos_w;
+  float x0[P], y0[P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    x0[q] = x[q];
+    y0[q] = y[q];
+  }
+  for (int it = 0; it < d.cycles; ++it) {
+    float nx[P], pv[P], c[P], xn[P], yn[P];
+    shift_next<P>(th, nx);
+#pragma unroll
+    for (int q = 0; q < P; ++q) c[q] = (lane * P + q < nb) ? bend_corr(th[q], nx[q], ra[q], kb[q]) : 0.0f;
+    shift_prev<P>(c, pv);
+    shift_next<P>(x, xn);
+    shift_next<P>(y, yn);
+    float fx[P], fy[P], he[P], fxp[P], fyp[P], hep[P];
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      const int j = lane * P + q;
+      fx[q] = fy[q] = he[q] = 0.0f;
+      if (j < ne) {
+        float acc = 0.0f;
+        if (j < nb) acc = acc + c[q];
+        if (j >= 1 && j - 1 < nb) acc = acc + (-pv[q]);
+        const float2 r = min_image(xn[q], yn[q], x[q], y[q], W, H);
+        th[q] = cos_pull(th[q] + acc * edg[q], r.x, r.y);
+        float sn, cs;
+        sincosf(th[q], &sn, &cs);
+        const float kl = ks / l0[q];
+        fx[q] = kl * (r.x / l0[q] - cs);
+        fy[q] = kl * (r.y / l0[q] - sn);
+        he[q] = ks / (l0[q] * l0[q]);
+      }
+    }
+    shift_prev<P>(fx, fxp);
+    shift_prev<P>(fy, fyp);
+    shift_prev<P>(he, hep);
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      const int j = lane * P + q;
+      if (j < nn) {
+        float ax = w * (x0[q] - x[q]), ay = w * (y0[q] - y[q]), hh = w;
+        if (j < ne) {
+          ax = ax + fx[q];
+          ay = ay + fy[q];
+          hh = hh + he[q];
+        }
+        if (j >= 1) {
+          ax = ax + (-fxp[q]);
+          ay = ay + (-fyp[q]);
+          hh = hh + hep[q];
+        }
+        x[q] = x[q] + ax / hh;
+        y[q] = y[q] + ay / hh;
+      }
+    }
+  }
+}
+
 template <int P>
 __global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
                                                const int* __restrict__ tdev) {
@@ -418,6 +522,19 @@ __global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, cons
     ndg[q] = ((j < ne) + (j >= 1 && j - 1 < ne)) == 2 ? 0.5f : 1.0f;
   }
   const int cycles = d.cycles;
+  if (d.solver == 1) {
+    cosserat_chain<P>(d, lane, nn, ne, nb, x, y, th, l0, ra, kb, edg);
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      const int j = lane * P + q;
+      if (j < ne) d.theta[e0 + j] = th[q];
+      if (j < nn) {
+        d.pos[2 * (n0 + j)] = x[q];
+        d.pos[2 * (n0 + j) + 1] = y[q];
+      }
+    }
+    return;
+  }
   for (int it = 0; it < cycles; ++it) {
     float nx[P], pv[P], c[P];
     shift_next<P>(th, nx);
@@ -513,8 +630,9 @@ __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off,
   }
   __syncthreads();
 
+  const bool cosserat = d.solver == 1;
   for (int it = 0; it < d.cycles; ++it) {
-    // theta pass over bending pairs (pbd.py:23-49)
+    // theta pass over bending pairs (pbd.py:23-49; stable_cosserat.py:55-82)
     for (int b = tid; b < nb; b += bd) {
       const int ein = d.bpairs[2 * (b0 + b)] - e0, eout = d.bpairs[2 * (b0 + b) + 1] - e0;
       corr[b] = bend_corr(th[ein], th[eout], ra[b], kb[b]);
@@ -528,17 +646,57 @@ __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off,
         const float c = corr[(code >> 1) - b0];
         acc = (code & 1) ? acc + (-c) : acc + c;
       }
-      th[e] = th[e] + (acc / d.edeg[ge]) * 1.8f;
+      if (cosserat) {
+        const int s = d.pairs[2 * ge] - n0, g = d.pairs[2 * ge + 1] - n0;
+        const float2 r = min_image(px[g], py[g], px[s], py[s], (float)d.W, (float)d.H);
+        th[e] = cos_pull(th[e] + acc / d.edeg[ge], r.x, r.y);
+      } else {
+        th[e] = th[e] + (acc / d.edeg[ge]) * 1.8f;
+      }
     }
     __syncthreads();
-    // position pass over edges (pbd.py:51-89)
+    // position pass over edges (pbd.py:51-89; stable_cosserat.py:84-119)
     for (int e = tid; e < ne; e += bd) {
       const int s = d.pairs[2 * (e0 + e)] - n0, g = d.pairs[2 * (e0 + e) + 1] - n0;
-      const float2 f = edge_force(d, th[e], l0[e], px[s], py[s], px[g], py[g]);
-      fx[e] = f.x;
-      fy[e] = f.y;
+      if (cosserat) {
+        const float2 r = min_image(px[g], py[g], px[s], py[s], (float)d.W, (float)d.H);
+        float sn, cs;
+        sincosf(th[e], &sn, &cs);
+        const float kl = d.k_stretch / l0[e];
+        fx[e] = kl * (r.x / l0[e] - cs);
+        fy[e] = kl * (r.y / l0[e] - sn);
+      } else {
+        const float2 f = edge_force(d, th[e], l0[e], px[s], py[s], px[g], py[g]);
+        fx[e] = f.x;
+        fy[e] = f.y;
+      }
     }
     __syncthreads();
+    if (cosserat) {
+      // implicit update with inertia: per node (w (y0 - x) + sum +-f_e) / (w + sum k_s/l_e^2),
+      // y0 = the positions this kernel started from (still in global memory)
+      const float w = d.cos_w;
+      for (int i = tid; i < nn; i += bd) {
+        const int gi = n0 + i;
+        float ax = w * (d.pos[2 * gi] - px[i]), ay = w * (d.pos[2 * gi + 1] - py[i]), hh = w;
+        for (int j = d.ne_off[gi]; j < d.ne_off[gi + 1]; ++j) {
+          const int code = d.ne_idx[j];
+          const int e = (code >> 1) - e0;
+          if (code & 1) {
+            ax = ax + (-fx[e]);
+            ay = ay + (-fy[e]);
+          } else {
+            ax = ax + fx[e];
+            ay = ay + fy[e];
+          }
+          hh = hh + d.k_stretch / (l0[e] * l0[e]);
+        }
+        px[i] = px[i] + ax / hh;
+        py[i] = py[i] + ay / hh;
+      }
+      __syncthreads();
+      continue;
+    }
     for (int i = tid; i < nn; i += bd) {
       const int gi = n0 + i;
       float ax = 0.0f, ay = 0.0f;

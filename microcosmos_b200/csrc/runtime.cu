@@ -355,6 +355,7 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.K = h.cfg.ibm_kernel_size;
   d.ncomp = h.ncomp;
   d.M = h.M;
+  d.NI = h.dims.N * (h.cfg.synthetic_node_width > 0.0f ? 2 : 1);
   d.ntile_x = h.ntx;
   d.ntile_y = h.nty;
   d.lbm_tx = h.lbm_tx;
@@ -366,10 +367,14 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.damping = c.damping;
   d.k_stretch = c.stiffness_stretch;
   d.k_shear = c.stiffness_shear;
+  d.solver = c.solver_type;
+  d.syn_w = c.synthetic_node_width;
+  d.cos_w = (float)(1.0 / (c.solver_dt * c.solver_dt));
   // mean_scale = 1 (fluid grid == domain grid) but scale keeps the reference's axis order
   const double sx = (double)h.dims.W / (double)h.dims.H, sy = (double)h.dims.H / (double)h.dims.W;
   d.scale_x = (float)sx;
   d.scale_y = (float)sy;
+  d.syn_ms = (float)(0.5 * (sx + sy));
   d.vmax = (float)((double)c.max_fluid_velocity * (0.5 * (sx + sy)));
   d.vmax_q4 = std::nextafter((float)(0.25 * (double)d.vmax * (double)d.vmax), 0.0f);
   d.sdt_x = d.scale_x * h.dt;
@@ -395,7 +400,9 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.st_norm = (float)(2.0 * M_PI * sg * sg);
   d.st_coef = (float)((double)c.steric_scatter_value / (sg * sg));
   d.st_skip = c.steric_neighbor_skip;
-  d.ib_iters = c.ibm_iterations;
+  // a rollout without fluid has no IB contributions: the batch's IB iteration kernels
+  // must not visit its nodes
+  d.ib_iters = c.enable_fluid ? c.ibm_iterations : 0;
   d.cycles = c.cycles_per_step;
   d.enable_fluid = c.enable_fluid ? 1 : 0;
   d.enable_steric = c.enable_steric ? 1 : 0;
@@ -910,9 +917,17 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       delete p;
       return fail(MC_ERR_INVALID, "null topology array");
     }
-    if (c.synthetic_node_width != 0.0f) {
+    if (!(c.synthetic_node_width >= 0.0f)) {
       delete p;
-      return fail(MC_ERR_UNSUPPORTED, "synthetic_node_width > 0 is not implemented");
+      return fail(MC_ERR_INVALID, "synthetic_node_width must be >= 0");
+    }
+    if (c.solver_type != MC_SOLVER_PBD && c.solver_type != MC_SOLVER_COSSERAT) {
+      delete p;
+      return fail(MC_ERR_INVALID, "solver_type must be MC_SOLVER_PBD or MC_SOLVER_COSSERAT");
+    }
+    if (c.solver_type == MC_SOLVER_COSSERAT && !(c.solver_dt > 0.0)) {
+      delete p;
+      return fail(MC_ERR_INVALID, "the Cosserat solver's dt must be > 0");
     }
     if (c.ibm_kernel_size < 1 || c.ibm_kernel_size > 8) {
       delete p;
@@ -922,10 +937,12 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       delete p;
       return fail(MC_ERR_INVALID, "dt must be > 0");
     }
-    const long long M = c.enable_fluid ? (long long)D.N * c.ibm_kernel_size * c.ibm_kernel_size : 0;
+    // IB points: the nodes, or a synthetic pair per node (fluid.py:244-263)
+    const long long NI = (long long)D.N * (c.synthetic_node_width > 0.0f ? 2 : 1);
+    const long long M = c.enable_fluid ? NI * c.ibm_kernel_size * c.ibm_kernel_size : 0;
     if (M >= (1LL << 24) || 4LL * D.N >= (1LL << 24)) {
       delete p;
-      return fail(MC_ERR_UNSUPPORTED, "too many IB contributions for 24-bit sort keys (N*K*K < 2^24)");
+      return fail(MC_ERR_UNSUPPORTED, "too many IB contributions for 24-bit sort keys (IB points*K*K < 2^24)");
     }
     h.M = (int)M;
     h.pairs.assign(pairs[i] ? pairs[i] : nullptr, pairs[i] ? pairs[i] + 2 * (size_t)D.E : nullptr);
@@ -994,8 +1011,9 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.r_prev = lay.take(2 * N * 4);
     h.r_pred = lay.take(2 * N * 4);
     h.r_predw = lay.take(2 * N * 4);
-    h.r_nvl = lay.take(2 * N * 4);
-    h.r_delta = lay.take(2 * N * 4);
+    const size_t NIz = N * (c.synthetic_node_width > 0.0f ? 2 : 1);
+    h.r_nvl = lay.take(2 * NIz * 4);
+    h.r_delta = lay.take(2 * NIz * 4);
     const size_t Mz = (size_t)M;
     h.r_ibcell = lay.take(Mz * 4);
     h.r_ibw = lay.take(Mz * 4);
@@ -1091,8 +1109,11 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     const mc_config& c = h.cfg;
     const long long HW = (long long)h.dims.H * h.dims.W;
     int cnt[K_COUNT];
-    cnt[K_NODES] = div_up(h.dims.N, 256);
-    cnt[K_NODES16] = div_up(16LL * h.dims.N, 256);
+    // node kernels cover the IB points too (twice the nodes with synthetic pairs); the
+    // node-only kernels return for indices >= N
+    const long long npts = (long long)h.dims.N * (c.synthetic_node_width > 0.0f ? 2 : 1);
+    cnt[K_NODES] = div_up(npts, 256);
+    cnt[K_NODES16] = div_up(16LL * npts, 256);
     // fused IB kernel: one thread per touched-cell candidate / 4 (scaled down at bind if
     // the plan's CTAs would not all be resident)
     cnt[K_IBCOOP] = c.enable_fluid ? std::max(1, div_up(h.M, 1024)) : 0;

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .config import ConstraintSolverConfig, pbd_rod_constraint
+from .config import ConstraintSolverConfig, pbd_rod_constraint, stable_cosserat_constraint
 
 _F32 = torch.float32
 
@@ -24,10 +24,21 @@ def _require_cuda():
         raise RuntimeError("microcosmos_b200 needs a CUDA device; there is no CPU fallback")
 
 
+SOLVERS = {"pbd": 0, "cosserat": 1}
+
+
 def mc_config(cfg: ConstraintSolverConfig) -> _lib.McConfig:
-    if cfg.bending_constraint is not pbd_rod_constraint or cfg.solver_type != "pbd":
-        raise NotImplementedError("only the PBD rod constraint plugin (pbd_rod_constraint) is implemented")
+    """The C-ABI mirror of a ConstraintSolverConfig.  The plugin slot must hold one of the
+    two device solvers, matching ``solver_type`` (simulate.py:68-71 switches on it)."""
+    plugin = {pbd_rod_constraint: "pbd", stable_cosserat_constraint: "cosserat"}.get(cfg.bending_constraint)
+    if plugin is None:
+        raise NotImplementedError("bending_constraint must be pbd_rod_constraint or stable_cosserat_constraint; "
+                                  "a host-side Python constraint cannot run inside the device step")
+    if cfg.solver_type not in SOLVERS or cfg.solver_type != plugin:
+        raise ValueError(f"solver_type {cfg.solver_type!r} does not match the {plugin} bending_constraint")
     c = _lib.McConfig()
+    c.solver_type = SOLVERS[cfg.solver_type]
+    c.solver_dt = float(cfg.dt)
     c.cycles_per_step = int(cfg.cycles_per_step)
     c.stiffness_stretch = float(cfg.stiffness_stretch)
     c.stiffness_shear = float(cfg.stiffness_shear)

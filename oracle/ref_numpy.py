@@ -56,6 +56,10 @@ class Config:
     steric_sigma: float = 1.5
     steric_neighbor_skip: int = 5
     steric_scatter_value: float = 1.0
+    # rod solver: "pbd" (solver/pbd.py) or "cosserat" (solver/stable_cosserat.py), whose
+    # inertia weight is 1 / dt**2 with this dt (solver/config.py:29-31)
+    solver_type: str = "pbd"
+    dt: float = 0.05
 
 
 @dataclasses.dataclass
@@ -278,6 +282,71 @@ def pbd_iteration(H, W, pos, theta, pairs, bpairs, rest_len, rest_ang, k_bend, c
     return pos + disp, theta
 
 
+def cosserat_iteration(H, W, pos, y, theta, pairs, bpairs, rest_len, rest_ang, k_bend, cfg):
+    """One iteration of stable_cosserat_constraint (src/microcosmos/solver/stable_cosserat.py:13-119).
+    Phase 1: the bending pass of pbd.py without the 1.8 over-relaxation, then a pull of
+    theta toward the segment direction, wrap(atan2(r) - theta) * 0.05.  Phase 2: one
+    implicit position update with the inertia weight w = 1/dt**2 (cfg.dt):
+    x += (w (y - x) + sum of +-(k_s/l)(r/l - d(theta))) / (w + sum of k_s/l**2), with the
+    scatter order of the reference (all src updates, then all tgt updates)."""
+    dt = pos.dtype
+    t = dt.type
+    Ecount = theta.shape[0]
+    N = pos.shape[0]
+    src, tgt = pairs[:, 0], pairs[:, 1]
+    ein, eout = bpairs[:, 0], bpairs[:, 1]
+    edeg = np.zeros(Ecount, dt)
+    np.add.at(edeg, ein, t(1.0))
+    np.add.at(edeg, eout, t(1.0))
+    edeg = np.maximum(edeg, t(1.0))
+    pi = t(np.pi)
+    twopi = t(2 * np.pi)
+    diff = theta[eout] - theta[ein]
+    diff = np.mod(diff + pi, twopi) - pi
+    corr = (diff - rest_ang) * k_bend * t(0.5)
+    delta = np.zeros(Ecount, dt)
+    np.add.at(delta, ein, corr)
+    np.add.at(delta, eout, -corr)
+    theta_new = theta + delta / edeg
+    seg = displacement(H, W, pos[tgt], pos[src])
+    alpha = np.arctan2(seg[:, 1], seg[:, 0])
+    pull = np.mod(alpha - theta_new + pi, twopi) - pi
+    theta_new = theta_new + pull * t(0.05)
+
+    ks = t(cfg.stiffness_stretch)
+    w = t(1.0 / (cfg.dt ** 2))
+    d = np.stack([np.cos(theta_new), np.sin(theta_new)], axis=-1)
+    c = seg / rest_len[:, None] - d
+    f_edge = (ks / rest_len)[:, None] * c
+    h_edge = ks / (rest_len * rest_len)
+    f_node = w * (y - pos)
+    h_node = np.full(N, w, dt)
+    np.add.at(f_node, src, f_edge)
+    np.add.at(f_node, tgt, -f_edge)
+    np.add.at(h_node, src, h_edge)
+    np.add.at(h_node, tgt, h_edge)
+    return pos + f_node / h_node[:, None], theta_new
+
+
+def synthetic_ib_positions(H, W, pos, pairs, gpos, width, mean_scale):
+    """Synthetic IB node pairs (src/microcosmos/solver/fluid.py:241-263): the chain tangent
+    at each node is the sum of its edges' min-image vectors (all src updates, then all tgt
+    updates), normalised by sqrt(|t|^2 + EPSIL); the points are gpos +- width*perp*mean_scale,
+    perp = (-t_y, t_x), the + set first."""
+    dt = pos.dtype
+    t = dt.type
+    src, tgt = pairs[:, 0], pairs[:, 1]
+    ev = displacement(H, W, pos[tgt], pos[src])
+    raw = np.zeros_like(pos)
+    np.add.at(raw, src, ev)
+    np.add.at(raw, tgt, ev)
+    nrm = np.sqrt(raw[:, 0] * raw[:, 0] + raw[:, 1] * raw[:, 1] + t(EPSIL32))[:, None]
+    tan = raw / nrm
+    perp = np.stack([-tan[:, 1], tan[:, 0]], axis=-1)
+    off = t(width) * perp * t(mean_scale)
+    return np.concatenate([gpos + off, gpos - off], axis=0)
+
+
 # ----------------------------------------------------------------------------- IB + LBM
 def peskin_weights(H, W, gpos, K):
     """Per-point K x K stencil (src/microcosmos/solver/fluid.py:31-87): start at
@@ -398,9 +467,9 @@ class IBResult:
     vel_before: np.ndarray
 
 
-def ib_lbm(H, W, grid_shape, pos, vel, f_grid, cfg, dtstep, ib_positions=None):
-    """immersed_boundary_interaction (src/microcosmos/solver/fluid.py:202-386) for
-    synthetic_node_width = 0: macroscopic + clamp, multi-direct forcing
+def ib_lbm(H, W, grid_shape, pos, vel, f_grid, cfg, dtstep, ib_positions=None, pairs=None):
+    """immersed_boundary_interaction (src/microcosmos/solver/fluid.py:202-386):
+    macroscopic + clamp, multi-direct forcing
     (ibm_iterations x interpolate/clamp/spread), post clamp, F = (u_corr - u) rho,
     TRT+Guo collide, stream, node reaction.  ``grid_shape`` is the domain grid; the
     scale keeps the reference's axis order scale = (w / grid_shape[0], h / grid_shape[1]).
@@ -408,7 +477,9 @@ def ib_lbm(H, W, grid_shape, pos, vel, f_grid, cfg, dtstep, ib_positions=None):
     ``ib_positions`` (default: ``pos``) are the positions the Peskin stencils are built
     from.  The reference wraps them in ``jax.lax.stop_gradient`` (fluid.py:239), so a
     finite-difference check of its gradients holds them at the unperturbed trajectory's
-    values."""
+    values.  With ``synthetic_node_width > 0`` the IB points are the synthetic pairs
+    (``synthetic_ib_positions``, needs ``pairs``) carrying their node's velocity, and each
+    node's reaction is the mean of its two points' forces (fluid.py:371-374)."""
     dt = f_grid.dtype
     t = dt.type
     h, w = f_grid.shape[1], f_grid.shape[2]
@@ -418,8 +489,11 @@ def ib_lbm(H, W, grid_shape, pos, vel, f_grid, cfg, dtstep, ib_positions=None):
     eps = t(EPSIL32)
     node_vel = vel * scale * t(dtstep)
     gpos = (pos if ib_positions is None else ib_positions) * scale
+    nn = pos.shape[0]
     if cfg.synthetic_node_width > 0.0:
-        raise NotImplementedError("synthetic_node_width > 0 is not part of this oracle")
+        gpos = synthetic_ib_positions(grid_shape[0], grid_shape[1], pos if ib_positions is None else ib_positions,
+                                      pairs, gpos, cfg.synthetic_node_width, mean_scale)
+        node_vel = np.concatenate([node_vel, node_vel], axis=0)
     f = np.maximum(f_grid, eps)
     rho, ux, uy = macroscopic(f)
     c1 = velocity_clamp_factor(ux, uy, vmax)
@@ -477,6 +551,9 @@ def ib_lbm(H, W, grid_shape, pos, vel, f_grid, cfg, dtstep, ib_positions=None):
     for k in range(nst):
         nfx = nfx + gx[:, k]
         nfy = nfy + gy[:, k]
+    if cfg.synthetic_node_width > 0.0:
+        nfx = t(0.5) * (nfx[:nn] + nfx[nn:])
+        nfy = t(0.5) * (nfy[:nn] + nfy[nn:])
     sdt = scale * t(dtstep)
     dvx = (nfx / t(cfg.node_mass)) / sdt[0]
     dvy = (nfy / t(cfg.node_mass)) / sdt[1]
@@ -487,7 +564,9 @@ def ib_lbm(H, W, grid_shape, pos, vel, f_grid, cfg, dtstep, ib_positions=None):
 
 # ----------------------------------------------------------------------------- step / simulate
 def step(s: State, cfg: Config, dtstep: float, rest_angles=None, ib_positions=None):
-    """One simulate.step (src/microcosmos/simulate.py:37-100) for the PBD solver.
+    """One simulate.step (src/microcosmos/simulate.py:37-100) with the PBD or the
+    stable-Cosserat rod solver (cfg.solver_type; the Cosserat inertial prediction is the
+    position after the steric displacement, simulate.py:70-71).
     ``rest_angles`` overrides edges.bending_rest_angles for this step (the caller-side
     curvature actuation); ``ib_positions`` see ``ib_lbm``."""
     dt = s.position.dtype
@@ -505,11 +584,15 @@ def step(s: State, cfg: Config, dtstep: float, rest_angles=None, ib_positions=No
         pred = pred + fst * t(cfg.steric_strength) * t(dtstep)
     pos, theta = pred, s.theta
     for _ in range(cfg.cycles_per_step):
-        pos, theta = pbd_iteration(H, W, pos, theta, s.pairs, s.bending_pairs, s.rest_lengths,
-                                   s.bending_rest_angles, s.bending_stiffness, cfg)
+        if cfg.solver_type == "cosserat":
+            pos, theta = cosserat_iteration(H, W, pos, pred, theta, s.pairs, s.bending_pairs, s.rest_lengths,
+                                            s.bending_rest_angles, s.bending_stiffness, cfg)
+        else:
+            pos, theta = pbd_iteration(H, W, pos, theta, s.pairs, s.bending_pairs, s.rest_lengths,
+                                       s.bending_rest_angles, s.bending_stiffness, cfg)
     vel = (pos - prev) / t(dtstep)
     if cfg.enable_fluid:
-        r = ib_lbm(H, W, (H, W), pos, vel, s.f_grid, cfg, dtstep, ib_positions)
+        r = ib_lbm(H, W, (H, W), pos, vel, s.f_grid, cfg, dtstep, ib_positions, pairs=s.pairs)
         vel = r.velocity
         s.f_grid = r.f_grid
         s.fluid_velocity = r.fluid_velocity

@@ -36,6 +36,7 @@ def load_reference(ref_root):
     import microcosmos.solver.fluid as fluid_mod
     import microcosmos.solver.pbd as pbd_mod
     import microcosmos.solver.config as config_mod
+    import microcosmos.solver.stable_cosserat as cosserat_mod
     import microcosmos.graph as graph_mod
     from microcosmos.structs.nodes import Nodes
     from microcosmos.structs.edges import Edges
@@ -44,7 +45,7 @@ def load_reference(ref_root):
         if not hasattr(cls, "__replace__"):
             cls.__replace__ = lambda self, **kw: dataclasses.replace(self, **kw)
     return dict(simulate=simulate_mod, forces=forces_mod, utils=utils_mod, fluid=fluid_mod,
-                pbd=pbd_mod, config=config_mod, graph=graph_mod, Nodes=Nodes, Edges=Edges,
+                pbd=pbd_mod, stable_cosserat=cosserat_mod, config=config_mod, graph=graph_mod, Nodes=Nodes, Edges=Edges,
                 Fields=Fields)
 
 
@@ -66,10 +67,13 @@ CFG_KEYS = ["cycles_per_step", "stiffness_stretch", "stiffness_shear", "damping"
             "ibm_kernel_size", "ibm_relaxation", "node_mass", "lambda_trt", "enable_force_clamp",
             "enable_steric", "steric_strength", "steric_sigma", "steric_neighbor_skip",
             "steric_scatter_value"]
+# written only by the fixtures whose config uses them (stable-Cosserat solver)
+CFG_KEYS_SOLVER = ["solver_type", "dt"]
 
 
-def cfg_arrays(cfg):
-    return {"cfg_" + k: np.asarray(getattr(cfg, k)) for k in CFG_KEYS}
+def cfg_arrays(cfg, solver=False):
+    keys = CFG_KEYS + (CFG_KEYS_SOLVER if solver else [])
+    return {"cfg_" + k: np.asarray(getattr(cfg, k)) for k in keys}
 
 
 def state_arrays(prefix, nodes, edges, fields):
@@ -112,8 +116,20 @@ def save(name, **arrs):
     print("wrote", path, sum(v.nbytes for v in arrs.values()), "bytes")
 
 
-def main(ref_root):
+GROUPS = ("base", "cosserat", "synthetic")
+
+
+def main(ref_root, groups=GROUPS):
     R = load_reference(ref_root)
+    if "base" in groups:
+        base_cases(R)
+    if "cosserat" in groups:
+        cosserat_cases(R)
+    if "synthetic" in groups:
+        synthetic_cases(R)
+
+
+def base_cases(R):
     from microcosmos_b200 import scenarios as S
     U = R["utils"]
     jnp = sys.modules["jax"].numpy
@@ -229,5 +245,95 @@ def main(ref_root):
          **state_arrays("in_", nodes, edges, fields), **state_arrays("out_", nd2, ed2, fd2))
 
 
+def cosserat_cases(R):
+    """The stable-Cosserat plugin (solver/stable_cosserat.py:13-119): the constraint alone
+    (one iteration and a cycles_per_step loop with the inertial prediction in
+    debug_vector, as simulate.step sets it), and full steps with and without fluid."""
+    from microcosmos_b200 import scenarios as S
+    jnp = sys.modules["jax"].numpy
+    cfg_mod = R["config"]
+    rng = np.random.default_rng(4321)
+    for (H, W, F, n, seed) in [(20, 28, 3, 9, 21), (64, 64, 2, 24, 22)]:
+        sc = S.make_scenario(H, W, F, n, seed=seed, amp=0.3)
+        nodes, edges, fields = to_ref(R, sc)
+        y = sc.position + rng.normal(0, 0.2, size=sc.position.shape).astype(np.float32)
+        pos = jnp.array(y + rng.normal(0, 0.1, size=sc.position.shape).astype(np.float32))
+        th = jnp.array(sc.theta + rng.normal(0, 0.3, size=sc.theta.shape).astype(np.float32))
+        nodes = nodes.__replace__(position=pos, debug_vector=jnp.array(y))
+        edges = edges.__replace__(theta=th)
+        cfg = cfg_mod.COSSERAT_SCHEME_NO_FLUID
+        con = R["stable_cosserat"].stable_cosserat_constraint
+        n1, e1 = con(0, (nodes, edges), cfg, (H, W))
+        carry = (nodes, edges)
+        for i in range(cfg.cycles_per_step):
+            carry = con(i, carry, cfg, (H, W))
+        n20, e20 = carry
+        save(f"cosserat_{H}x{W}", H=np.int32(H), W=np.int32(W), **cfg_arrays(cfg, solver=True),
+             **state_arrays("in_", nodes, edges, None), in_y=A(y),
+             pos_1=A(n1.position), theta_1=A(e1.theta), pos_20=A(n20.position), theta_20=A(e20.theta))
+    # full steps: no fluid at the preset's dt; with fluid and steric at dt = 0.01 with the
+    # stiffness scaled to the inertia weight (k_s / l^2 = 1 / dt^2 for unit rest lengths)
+    cases = [("sim_cosserat_nofluid_24x32", 24, 32, 2, 10, 23, 0.05,
+              dataclasses.replace(cfg_mod.COSSERAT_SCHEME_NO_FLUID)),
+             ("sim_cosserat_fluid_32x32", 32, 32, 3, 12, 24, 0.01,
+              dataclasses.replace(cfg_mod.COSSERAT_SCHEME, dt=0.01, stiffness_stretch=10000.0,
+                                  stiffness_shear=10000.0, viscosity=0.1, ibm_kernel_size=4,
+                                  enable_steric=True))]
+    for (name, H, W, F, n, seed, dt, cfg) in cases:
+        sc = S.make_scenario(H, W, F, n, seed=seed, amp=0.2, period=20.0)
+        sc.velocity = rng.normal(0, 0.5, size=sc.velocity.shape).astype(np.float32)
+        nodes, edges, fields = to_ref(R, sc)
+        steps = 6
+        nd, ed, fd = nodes, edges, fields
+        traj = []
+        for t in range(steps):
+            ed = ed.__replace__(bending_rest_angles=jnp.array(S.actuation_rest_angles(sc, t)))
+            nd, ed, fd = R["simulate"].step(nd, ed, fd, dt, cfg)
+            traj.append(A(nd.position))
+        save(name, H=np.int32(H), W=np.int32(W), dt=np.float32(dt), steps=np.int32(steps),
+             **cfg_arrays(cfg, solver=True), **state_arrays("in_", nodes, edges, fields),
+             act_c=sc.act_c, act_amp=sc.act_amp, act_omega=sc.act_omega, act_phase=sc.act_phase,
+             act_position=np.stack(traj), act_velocity=A(nd.velocity), act_theta=A(ed.theta),
+             act_f_grid=A(fd.f_grid), act_steric=A(fd.steric), act_fluid_velocity=A(fd.fluid_velocity))
+
+
+def synthetic_cases(R):
+    """Synthetic IB node pairs (solver/fluid.py:241-263, 371-374): one
+    immersed_boundary_interaction with synthetic_node_width > 0, and full steps."""
+    from microcosmos_b200 import scenarios as S
+    jnp = sys.modules["jax"].numpy
+    cfg_mod = R["config"]
+    rng = np.random.default_rng(5678)
+    for (H, W, F, n, ks, width, seed) in [(24, 24, 2, 10, 4, 1.0, 31), (20, 28, 2, 8, 2, 0.5, 32)]:
+        sc = S.make_scenario(H, W, F, n, seed=seed, u0_std=1e-3)
+        nodes, edges, fields = to_ref(R, sc)
+        vel = jnp.array(rng.normal(0, 5.0, size=sc.position.shape).astype(np.float32))
+        nodes = nodes.__replace__(velocity=vel)
+        cfg = baseline_config(cfg_mod, ibm_kernel_size=ks, synthetic_node_width=width)
+        dt = 0.01
+        n2, f2, fnew = R["fluid"].immersed_boundary_interaction(nodes, edges, fields, fields.f_grid, dt, cfg)
+        save(f"ib_syn_{H}x{W}_k{ks}", H=np.int32(H), W=np.int32(W), dt=np.float32(dt), **cfg_arrays(cfg),
+             **state_arrays("in_", nodes, edges, fields),
+             velocity_out=A(n2.velocity), fluid_velocity_out=A(f2.fluid_velocity), f_grid_out=A(fnew))
+    sc = S.make_scenario(32, 32, 3, 12, seed=33, amp=0.2, period=20.0)
+    nodes, edges, fields = to_ref(R, sc)
+    cfg = baseline_config(cfg_mod, synthetic_node_width=1.0)
+    dt = 0.01
+    steps = 6
+    nd, ed, fd = nodes, edges, fields
+    traj = []
+    for t in range(steps):
+        ed = ed.__replace__(bending_rest_angles=jnp.array(S.actuation_rest_angles(sc, t)))
+        nd, ed, fd = R["simulate"].step(nd, ed, fd, dt, cfg)
+        traj.append(A(nd.position))
+    save("sim_syn_32x32", H=np.int32(32), W=np.int32(32), dt=np.float32(dt), steps=np.int32(steps),
+         **cfg_arrays(cfg), **state_arrays("in_", nodes, edges, fields),
+         act_c=sc.act_c, act_amp=sc.act_amp, act_omega=sc.act_omega, act_phase=sc.act_phase,
+         act_position=np.stack(traj), act_velocity=A(nd.velocity), act_theta=A(ed.theta),
+         act_f_grid=A(fd.f_grid), act_steric=A(fd.steric), act_fluid_velocity=A(fd.fluid_velocity))
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # usage: make_golden.py [reference root] [group,group,...]  (groups: base, cosserat, synthetic)
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    main(root, tuple(sys.argv[2].split(",")) if len(sys.argv) > 2 else GROUPS)

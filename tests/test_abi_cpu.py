@@ -89,8 +89,12 @@ def test_plan_rejects_unsupported_config(lib):
     sc = scenarios.make_scenario(32, 32, 1, 10, seed=0)
     import dataclasses
     st, _ = _create([(32, 32, sc.N, sc.pairs, sc.bending_pairs,
+                      dataclasses.replace(baseline_config(), synthetic_node_width=-1.0), 0.01)])
+    assert st == _lib.MC_ERR_INVALID
+    st, h = _create([(32, 32, sc.N, sc.pairs, sc.bending_pairs,
                       dataclasses.replace(baseline_config(), synthetic_node_width=1.0), 0.01)])
-    assert st == _lib.MC_ERR_UNSUPPORTED
+    assert st == _lib.MC_OK
+    lib.mc_plan_destroy(h)
     # 34 x 34: no FFT plan (prime factor 17) and too small for the direct filter (radius 17)
     st, _ = _create([(34, 34, sc.N, sc.pairs, sc.bending_pairs, baseline_config(), 0.01)])
     assert st == _lib.MC_ERR_UNSUPPORTED
@@ -107,11 +111,26 @@ def test_plan_rejects_unsupported_config(lib):
     assert st == _lib.MC_ERR_INVALID
 
 
-def test_stable_cosserat_plugin_is_rejected():
-    from microcosmos_b200 import COSSERAT_SCHEME
+def test_rod_solver_selection(lib):
+    """Both device rod solvers build plans; a foreign plugin, a solver_type that does not
+    match the plugin, and a non-positive Cosserat dt are rejected."""
+    import dataclasses
+    from microcosmos_b200 import COSSERAT_SCHEME, COSSERAT_SCHEME_NO_FLUID, PBD_SCHEME
     from microcosmos_b200.engine import mc_config
+    c = mc_config(COSSERAT_SCHEME)
+    assert c.solver_type == 1 and c.solver_dt == 0.05
+    assert mc_config(PBD_SCHEME).solver_type == 0
     with pytest.raises(NotImplementedError):
-        mc_config(COSSERAT_SCHEME)
+        mc_config(dataclasses.replace(PBD_SCHEME, bending_constraint=lambda *a, **k: a))
+    with pytest.raises(ValueError):
+        mc_config(dataclasses.replace(PBD_SCHEME, solver_type="cosserat"))
+    sc = scenarios.make_scenario(32, 32, 1, 10, seed=0)
+    for cfg in (COSSERAT_SCHEME, COSSERAT_SCHEME_NO_FLUID):
+        st, h = _create([(32, 32, sc.N, sc.pairs, sc.bending_pairs, cfg, 0.05)])
+        assert st == _lib.MC_OK
+        lib.mc_plan_destroy(h)
+    st, _ = _create([(32, 32, sc.N, sc.pairs, sc.bending_pairs, dataclasses.replace(COSSERAT_SCHEME, dt=0.0), 0.05)])
+    assert st == _lib.MC_ERR_INVALID
 
 
 def test_batch_plan_of_uneven_rollouts(lib):

@@ -46,12 +46,35 @@ def test_pbd(golden_dir, name):
     np.testing.assert_array_equal(t, z["theta_20"])
 
 
-@pytest.mark.parametrize("name", ["ib_24x24_k4", "ib_24x24_k2", "ib_20x28_k4", "ib_16x16_k4_clamp"])
+@pytest.mark.parametrize("name", ["cosserat_20x28", "cosserat_64x64"])
+def test_stable_cosserat(golden_dir, name):
+    """stable_cosserat_constraint (solver/stable_cosserat.py:13-119): one iteration and the
+    preset's cycles_per_step iterations, bit for bit."""
+    z = load(golden_dir, name)
+    H, W = int(z["H"]), int(z["W"])
+    cfg = O.config_from_npz(z)
+    assert cfg.solver_type == "cosserat" and cfg.dt == 0.05
+    args = (z["in_pairs"], z["in_bending_pairs"], z["in_rest_lengths"], z["in_bending_rest_angles"],
+            z["in_bending_stiffness"], cfg)
+    p, t = O.cosserat_iteration(H, W, z["in_position"], z["in_y"], z["in_theta"], *args)
+    np.testing.assert_array_equal(p, z["pos_1"])
+    np.testing.assert_array_equal(t, z["theta_1"])
+    p, t = z["in_position"], z["in_theta"]
+    for _ in range(cfg.cycles_per_step):
+        p, t = O.cosserat_iteration(H, W, p, z["in_y"], t, *args)
+    np.testing.assert_array_equal(p, z["pos_20"])
+    np.testing.assert_array_equal(t, z["theta_20"])
+
+
+@pytest.mark.parametrize("name", ["ib_24x24_k4", "ib_24x24_k2", "ib_20x28_k4", "ib_16x16_k4_clamp",
+                                  "ib_syn_24x24_k4", "ib_syn_20x28_k2"])
 def test_ib_lbm(golden_dir, name):
     z = load(golden_dir, name)
     H, W = int(z["H"]), int(z["W"])
-    r = O.ib_lbm(H, W, (H, W), z["in_position"], z["in_velocity"], z["in_f_grid"], O.config_from_npz(z),
-                 float(z["dt"]))
+    cfg = O.config_from_npz(z)
+    assert (cfg.synthetic_node_width > 0) == name.startswith("ib_syn")
+    r = O.ib_lbm(H, W, (H, W), z["in_position"], z["in_velocity"], z["in_f_grid"], cfg,
+                 float(z["dt"]), pairs=z["in_pairs"])
     assert O.rel_l2(r.velocity, z["velocity_out"]) < 1e-6
     assert O.rel_l2(r.fluid_velocity, z["fluid_velocity_out"]) < 1e-6
     assert O.rel_l2(r.f_grid, z["f_grid_out"]) < 1e-7
@@ -72,7 +95,8 @@ def test_simulate_timeseries(golden_dir, name):
     assert O.rel_l2(ts["fluid_velocity"], z["ts_fluid_velocity"]) < 1e-5
 
 
-@pytest.mark.parametrize("name", ["sim_24x32", "sim_32x32"])
+@pytest.mark.parametrize("name", ["sim_24x32", "sim_32x32", "sim_cosserat_nofluid_24x32",
+                                  "sim_cosserat_fluid_32x32", "sim_syn_32x32"])
 def test_actuated_steps(golden_dir, name):
     z = load(golden_dir, name)
     cfg = O.config_from_npz(z)
