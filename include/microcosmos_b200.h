@@ -195,8 +195,11 @@ mc_status mc_rollout(mc_plan* plan, const mc_state* states, int32_t num_steps,
 /* The three phases of mc_rollout, for callers that interleave their own work between
  * steps (timing, L2 flushes, host control).  begin: bind states/actuation/recording and
  * convert fields.f_grid to the internal layout; advance: run num_steps more steps
- * (last != 0: the final one of them writes fields.fluid_velocity); end: write
- * fields.f_grid back.  mc_rollout(...) == begin + advance(num_steps, last=1) + end. */
+ * (last != 0: the final one of them writes fields.fluid_velocity and the call returns with
+ * that step complete -- none of the next step is started -- so the caller may change the
+ * state's positions, velocities, rest lengths or rest angles before a further advance; the
+ * advance before end must pass last != 0); end: write fields.f_grid back.
+ * mc_rollout(...) == begin + advance(num_steps, last=1) + end. */
 mc_status mc_rollout_begin(mc_plan* plan, const mc_state* states, const mc_actuation* const* act,
                            const mc_record* const* rec, void* stream);
 mc_status mc_rollout_advance(mc_plan* plan, int32_t num_steps, int32_t use_graph, int32_t last, void* stream);
@@ -302,6 +305,51 @@ mc_status mc_grad_forward(mc_grad_plan* plan, const mc_state* state, const mc_ac
  * initial state and the parameter gradients.  final_cot and initial_cot may alias. */
 mc_status mc_grad_backward(mc_grad_plan* plan, const mc_state_cot* final_cot, mc_state_cot* initial_cot,
                            mc_param_grads* grads, void* stream);
+
+/* ------------------------------------------------------------------ gym environments
+ * The device work of the reference's gym Environment.step around one rollout step
+ * (src/microcosmos/gym/base.py:173-196), for a table of environments (the reference
+ * batches environments with jax.vmap): mc_env_act writes the step's rest lengths and
+ * rest angles from the episode's base values plus the action (base.py:177-182; then
+ * mc_rollout runs the step on the same buffers), mc_env_observe walks the energy source
+ * (base.py:187-190), writes the observation (base.py:112-121) and the reward (base.py:123-124;
+ * per node range for several creatures, multi_agent.py:201-212), advances the step counter
+ * and sets done = time >= max_steps (base.py:192-195).  All pointers are device pointers. */
+typedef struct mc_env {
+  int32_t N, E, B;                        /* nodes, edges, bending pairs */
+  int32_t H, W;                           /* grid_shape */
+  const float* base_rest_lengths;         /* (E,) the episode's rest lengths */
+  const float* base_bending_rest_angles;  /* (B,) */
+  const float* d_rest_length;             /* (E,) action; NULL = zero */
+  const float* d_bending_angle;           /* (B,) action; NULL = zero */
+  float* rest_lengths;                    /* (E,) out: the buffers the step reads */
+  float* bending_rest_angles;             /* (B,) out */
+  const float* position;                  /* (N,2) the state after the step */
+  const float* velocity;                  /* (N,2) */
+  float* energy_center;                   /* (2,) in/out */
+  const float* noise;                     /* (2,) standard-normal draws of this step; NULL = no walk */
+  float energy_walk_std;
+  float energy_amplitude;
+  float energy_two_size_sq;               /* float32 of 2 * energy_size^2 */
+  int32_t max_steps;
+  int32_t* time;                          /* () in/out */
+  int32_t* done;                          /* () out */
+  float* observation;                     /* (5N,) out: positions - mean (2N), velocities (2N), energy (N) */
+  float* reward;                          /* () out */
+  int32_t num_segments;                   /* node ranges ("creatures"), 0 or 1 = one */
+  const int32_t* segment_offsets;         /* (num_segments+1,) node offsets; NULL with one range */
+  float* segment_fitness;                 /* (num_segments,) out, may be NULL */
+} mc_env;
+
+/* Device bytes of a table of n environments; mc_env_table_upload copies the host structs
+ * into such a caller-owned device buffer (stream-ordered; the host array may be freed on
+ * return). */
+size_t mc_env_table_bytes(int32_t n);
+mc_status mc_env_table_upload(const mc_env* envs, int32_t n, void* table, void* stream);
+mc_status mc_env_act(const void* table, int32_t n, void* stream);
+/* advance = 0: the observation, reward and fitness of the current state only (reset,
+ * base.py:140-149); the energy source, step counter and done flag are left alone. */
+mc_status mc_env_observe(const void* table, int32_t n, int32_t advance, void* stream);
 
 /* Text of the last error of this thread ("" if none). */
 const char* mc_last_error(void);

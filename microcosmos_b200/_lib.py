@@ -86,6 +86,22 @@ class McParamGrads(ctypes.Structure):
                 ("bending_stiffness", ctypes.c_void_p)]
 
 
+class McEnv(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int32), ("E", ctypes.c_int32), ("B", ctypes.c_int32),
+                ("H", ctypes.c_int32), ("W", ctypes.c_int32),
+                ("base_rest_lengths", ctypes.c_void_p), ("base_bending_rest_angles", ctypes.c_void_p),
+                ("d_rest_length", ctypes.c_void_p), ("d_bending_angle", ctypes.c_void_p),
+                ("rest_lengths", ctypes.c_void_p), ("bending_rest_angles", ctypes.c_void_p),
+                ("position", ctypes.c_void_p), ("velocity", ctypes.c_void_p),
+                ("energy_center", ctypes.c_void_p), ("noise", ctypes.c_void_p),
+                ("energy_walk_std", ctypes.c_float), ("energy_amplitude", ctypes.c_float),
+                ("energy_two_size_sq", ctypes.c_float), ("max_steps", ctypes.c_int32),
+                ("time", ctypes.c_void_p), ("done", ctypes.c_void_p),
+                ("observation", ctypes.c_void_p), ("reward", ctypes.c_void_p),
+                ("num_segments", ctypes.c_int32), ("segment_offsets", ctypes.c_void_p),
+                ("segment_fitness", ctypes.c_void_p)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/microcosmos_b200.h
 SIGNATURES = {
     "mc_plan_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(McDims), ctypes.POINTER(McConfig),
@@ -138,6 +154,10 @@ SIGNATURES = {
                                        ctypes.c_void_p]),
     "mc_grad_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(McStateCot), ctypes.POINTER(McStateCot),
                                         ctypes.POINTER(McParamGrads), ctypes.c_void_p]),
+    "mc_env_table_bytes": (ctypes.c_size_t, [ctypes.c_int32]),
+    "mc_env_table_upload": (ctypes.c_int, [ctypes.POINTER(McEnv), ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
+    "mc_env_act": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    "mc_env_observe": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
     "mc_last_error": (ctypes.c_char_p, []),
     "mc_version": (ctypes.c_char_p, []),
 }

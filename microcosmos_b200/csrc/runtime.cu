@@ -123,7 +123,6 @@ struct mc_plan {
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool pending_next = false;  // the next step's pipeline has already been launched
-  bool need_pipeline = false; // step 0's pipeline is still to be launched
   int64_t last_launches = 0;
   // rollout in progress (mc_rollout_begin .. mc_rollout_end)
   bool active = false;
@@ -771,10 +770,9 @@ int64_t enqueue_body(mc_plan* p, int parity, int write_u, int rec_fields, bool h
 
 mc_status run_steps(mc_plan* p, int num, int use_graph, int last, cudaStream_t s, int64_t& launches) {
   const int recv = p->rec_fields ? (p->rec_fluid ? 2 : 1) : 0;
-  if (p->need_pipeline && num > 0) {
-    launches += enqueue_pipeline(p, s, false);
-    p->need_pipeline = false;
-  }
+  // the first step of this call needs its node pipeline unless the previous call left it
+  // pending (an advance with last != 0 finishes its step without starting the next one)
+  if (!p->pending_next && num > 0) launches += enqueue_pipeline(p, s, false);
   int remaining = num;
   while (remaining > 0) {
     const int parity = p->step & 1;
@@ -1395,8 +1393,7 @@ mc_status mc_rollout_begin(mc_plan* p, const mc_state* states, const mc_actuatio
     mc::launch_unstream(L(p, K_CELLS, s));
     p->last_launches += 1;
   }
-  p->need_pipeline = true;  // the first advance launches step 0's pipeline
-  p->pending_next = false;
+  p->pending_next = false;  // the first advance launches step 0's pipeline
   MC_CUDA(cudaGetLastError());
   return MC_OK;
 }

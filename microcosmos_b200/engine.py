@@ -92,6 +92,14 @@ class DeviceState:
     def N(self):
         return self.position.shape[0]
 
+    @property
+    def E(self):
+        return int(self.pairs.shape[0])
+
+    @property
+    def B(self):
+        return int(self.bending_pairs.shape[0])
+
     @classmethod
     def from_arrays(cls, H, W, position, velocity, pairs, theta, rest_lengths, bending_pairs,
                     bending_rest_angles, bending_stiffness, f_grid, steric=None, fluid_velocity=None,

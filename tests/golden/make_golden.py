@@ -116,7 +116,7 @@ def save(name, **arrs):
     print("wrote", path, sum(v.nbytes for v in arrs.values()), "bytes")
 
 
-GROUPS = ("base", "cosserat", "synthetic")
+GROUPS = ("base", "cosserat", "synthetic", "gym")
 
 
 def main(ref_root, groups=GROUPS):
@@ -127,6 +127,8 @@ def main(ref_root, groups=GROUPS):
         cosserat_cases(R)
     if "synthetic" in groups:
         synthetic_cases(R)
+    if "gym" in groups:
+        gym_cases(R)
 
 
 def base_cases(R):
@@ -331,6 +333,49 @@ def synthetic_cases(R):
          act_c=sc.act_c, act_amp=sc.act_amp, act_omega=sc.act_omega, act_phase=sc.act_phase,
          act_position=np.stack(traj), act_velocity=A(nd.velocity), act_theta=A(ed.theta),
          act_f_grid=A(fd.f_grid), act_steric=A(fd.steric), act_fluid_velocity=A(fd.fluid_velocity))
+
+
+def gym_cases(R):
+    """The reference's gym environments (src/microcosmos/gym/*.py): reset, then three steps
+    with seeded actions (energy source on, walk off, max_steps = 3)."""
+    jax = sys.modules["jax"]
+    jnp = jax.numpy
+    import microcosmos.gym as G
+    rng = np.random.default_rng(999)
+    common = dict(energy_amplitude=1.0, max_steps=3)
+    specs = [("gym_line", G.LineEnv, dict(num_nodes=12, grid_shape=(48, 48), energy_size=6.0)),
+             ("gym_ring", G.RingEnv, dict(num_nodes=12, grid_shape=(48, 48), energy_size=6.0)),
+             ("gym_tadpole", G.TadpoleEnv, dict(head_nodes=8, tail_nodes=6, grid_shape=(48, 64))),
+             ("gym_multi", G.MultiAgentEnv, dict(creatures=(G.LineTopology(num_nodes=10), G.RingTopology(num_nodes=12)),
+                                                 grid_shape=(64, 64), energy_size=8.0)),
+             ("gym_line_ring", G.LineRingEnv, dict(line_nodes=10, ring_nodes=12, centered_line=True,
+                                                   grid_shape=(64, 64), energy_size=8.0))]
+    for name, cls, kw in specs:
+        env = cls(**kw, **common)
+        key = jax.random.PRNGKey(0)
+        obs0, st = env.reset(key)
+        out = dict(H=np.int32(env.grid_shape[0]), W=np.int32(env.grid_shape[1]), dt=np.float32(env.dt),
+                   max_steps=np.int32(env.max_steps), energy_size=np.float32(env.energy_size),
+                   energy_amplitude=np.float32(env.energy_amplitude), obs0=A(obs0),
+                   center0=A(st.energy_center), **state_arrays("in_", st.nodes, st.edges, st.fields))
+        acts_r, acts_b, obs, rew, done = [], [], [], [], []
+        for t in range(3):
+            a = {"d_rest_length": jnp.array(rng.normal(0, 0.1, env.num_edges).astype(np.float32)),
+                 "d_bending_angle": jnp.array(rng.normal(0, 0.1, env.num_bending_pairs).astype(np.float32))}
+            key, sub = jax.random.split(key)
+            o, st, r, d, info = env.step(sub, st, a)
+            acts_r.append(A(a["d_rest_length"]))
+            acts_b.append(A(a["d_bending_angle"]))
+            obs.append(A(o))
+            rew.append(np.float32(A(r)))
+            done.append(bool(A(d)))
+        out.update(act_rest=np.stack(acts_r), act_bend=np.stack(acts_b), obs=np.stack(obs), reward=np.array(rew),
+                   done=np.array(done), time=np.int32(A(st.time)), center=A(st.energy_center),
+                   **state_arrays("out_", st.nodes, st.edges, st.fields))
+        if hasattr(env, "fitness_per_creature"):
+            out["fitness"] = A(env.fitness_per_creature(st))
+            out["segments"] = np.array([s.start for s in env.node_slices] + [env.node_slices[-1].stop], np.int32)
+        save(name, **out)
 
 
 if __name__ == "__main__":

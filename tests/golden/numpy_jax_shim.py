@@ -428,6 +428,30 @@ def _make_jax():
     image.resize = resize
     jax.image = image
 
+    # jax.random: NOT JAX's threefry stream.  Keys are uint32 pairs; draws come from a
+    # numpy Generator seeded by the key.  The gym fixtures use keys only where the drawn
+    # value is multiplied by zero (energy_walk_std = 0) or not at all.
+    rnd = types.ModuleType("jax.random")
+
+    def PRNGKey(seed):
+        return np.array([0, int(seed) & 0xffffffff], np.uint32)
+
+    def _gen(key):
+        return np.random.default_rng([int(v) for v in np.asarray(key, np.uint32).ravel()])
+
+    def split(key, num=2):
+        return _gen(key).integers(0, 2 ** 32, size=(num, 2), dtype=np.uint64).astype(np.uint32)
+
+    def normal(key, shape=(), dtype=None):
+        return _wrap(_gen(key).standard_normal(shape).astype(np.float32))
+
+    def uniform(key, shape=(), dtype=None, minval=0.0, maxval=1.0):
+        u = _gen(key).random(shape).astype(np.float32)
+        return _wrap((np.asarray(minval, np.float32) + u * (np.asarray(maxval, np.float32)
+                                                            - np.asarray(minval, np.float32))).astype(np.float32))
+    rnd.PRNGKey, rnd.key, rnd.split, rnd.normal, rnd.uniform = PRNGKey, PRNGKey, split, normal, uniform
+    jax.random = rnd
+
     jax.config = types.SimpleNamespace(update=lambda *a, **k: None)
     return jax
 
@@ -447,4 +471,5 @@ def install():
     sys.modules["jax.scipy"] = jax.scipy
     sys.modules["jax.scipy.ndimage"] = jax.scipy.ndimage
     sys.modules["jax.image"] = jax.image
+    sys.modules["jax.random"] = jax.random
     return jax
