@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--grad-steps", type=int, default=2000)
     ap.add_argument("--no-grad", action="store_true")
+    ap.add_argument("--gym-envs", type=int, default=256)
+    ap.add_argument("--gym-steps", type=int, default=50)
+    ap.add_argument("--no-gym", action="store_true")
     return ap.parse_args()
 
 
@@ -385,6 +388,52 @@ def grad_section(args):
                                   "VJP oracle and float64 central differences in the tests"}
 
 
+def gym_section(args):
+    """Gym caller of the step (gym/base.py:163-196): ``--gym-envs`` LineEnv environments
+    (the reference's defaults: 128x128, 16 nodes, PBD_SCHEME; energy source on) stepped
+    together by BatchedEnv (action kernel, one batched physics step, observation/reward
+    kernel), against one Environment stepped alone (functional step: state copy, action,
+    rollout call, observation).  Random actions, resident on the device."""
+    import torch
+    from microcosmos_b200.gym import BatchedEnv, LineEnv
+    env = LineEnv(energy_amplitude=1.0, max_steps=10 ** 9)
+    B, K = args.gym_envs, args.gym_steps
+    g = torch.Generator(device="cuda").manual_seed(0)
+    acts = [{"d_rest_length": 0.1 * torch.randn((B, env.num_edges), generator=g, device="cuda"),
+             "d_bending_angle": 0.2 * torch.randn((B, env.num_bending_pairs), generator=g, device="cuda")}
+            for _ in range(K)]
+    benv = BatchedEnv(env, B)
+    _, st = benv.reset(list(range(B)))
+    for t in range(3):
+        benv.step(None, st, acts[t])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for t in range(K):
+        obs, st, rew, done, _ = benv.step(None, st, acts[t])
+    e1.record()
+    torch.cuda.synchronize()
+    batch_ms = e0.elapsed_time(e1)
+    mean_reward = float(rew.mean().item())
+    _, s1 = env.reset(0)
+    one = [{k: v[0] for k, v in a.items()} for a in acts]
+    for t in range(3):
+        _, s1, _, _, _ = env.step(None, s1, one[t])
+    torch.cuda.synchronize()
+    e0.record()
+    for t in range(K):
+        _, s1, _, _, _ = env.step(None, s1, one[t])
+    e1.record()
+    torch.cuda.synchronize()
+    single_ms = e0.elapsed_time(e1)
+    H, W = env.grid_shape
+    return {"workload": f"{B} x LineEnv (128x128, 16 nodes, PBD_SCHEME, energy source on), {K} steps, random actions",
+            "batched_env_steps_per_s": B * K / (batch_ms / 1e3), "batched_ms_per_step": batch_ms / K,
+            "batched_mlups": B * H * W * K / (batch_ms / 1e3) / 1e6,
+            "single_env_steps_per_s": K / (single_ms / 1e3), "single_ms_per_step": single_ms / K,
+            "speedup_vs_single": (B * K / batch_ms) / (K / single_ms), "mean_reward_last_step": mean_reward}
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -577,6 +626,9 @@ def main():
     served = None
     if ws == 1 and not args.no_serve:
         served = serve_section(args)
+    gym = None
+    if ws == 1 and not args.no_gym:
+        gym = gym_section(args)
 
     if rank == 0:
         value = job_cell_steps / (t_ms / 1e3) / 1e6
@@ -604,6 +656,7 @@ def main():
             "batch": batch,
             "serve": served,
             "grad": graded,
+            "gym": gym,
             "step_kernel_ms": step_kernel_ms / P,
         }
         print(json.dumps(out))
