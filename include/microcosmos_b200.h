@@ -351,6 +351,19 @@ mc_status mc_env_act(const void* table, int32_t n, void* stream);
  * base.py:140-149); the energy source, step counter and done flag are left alone. */
 mc_status mc_env_observe(const void* table, int32_t n, int32_t advance, void* stream);
 
+/* ------------------------------------------------------------------ frames
+ * The reference's render() of a recorded rollout (src/microcosmos/rendering.py:20-80)
+ * into a caller-owned device buffer, no display or graphics API involved.  Inputs (device):
+ * position and debug_vector (T,N,2) (debug_vector may be NULL = zero), color_bend (N,)
+ * (the first frame's colours; NULL = 0), steric (T,H,W).  Output frames
+ * (T, size*H/max(H,W), size*W/max(H,W), 3) uint8 RGB.  scratch: mc_render_scratch_bytes
+ * (T,H,W) bytes of device memory (unused when render_particles == 0). */
+size_t mc_render_scratch_bytes(int32_t T, int32_t H, int32_t W);
+mc_status mc_render_frames(const float* position, const float* debug_vector, const float* color_bend,
+                           const float* steric, int32_t T, int32_t N, int32_t H, int32_t W, int32_t size,
+                           int32_t render_particles, int32_t uniform_color, int32_t* scratch, uint8_t* frames,
+                           void* stream);
+
 /* Text of the last error of this thread ("" if none). */
 const char* mc_last_error(void);
 

@@ -158,6 +158,11 @@ SIGNATURES = {
     "mc_env_table_upload": (ctypes.c_int, [ctypes.POINTER(McEnv), ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
     "mc_env_act": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     "mc_env_observe": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
+    "mc_render_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "mc_render_frames": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p]),
     "mc_last_error": (ctypes.c_char_p, []),
     "mc_version": (ctypes.c_char_p, []),
 }

@@ -116,7 +116,7 @@ def save(name, **arrs):
     print("wrote", path, sum(v.nbytes for v in arrs.values()), "bytes")
 
 
-GROUPS = ("base", "cosserat", "synthetic", "gym")
+GROUPS = ("base", "cosserat", "synthetic", "gym", "render")
 
 
 def main(ref_root, groups=GROUPS):
@@ -129,6 +129,8 @@ def main(ref_root, groups=GROUPS):
         synthetic_cases(R)
     if "gym" in groups:
         gym_cases(R)
+    if "render" in groups:
+        render_cases(R)
 
 
 def base_cases(R):
@@ -375,6 +377,41 @@ def gym_cases(R):
         if hasattr(env, "fitness_per_creature"):
             out["fitness"] = A(env.fitness_per_creature(st))
             out["segments"] = np.array([s.start for s in env.node_slices] + [env.node_slices[-1].stop], np.int32)
+        save(name, **out)
+
+
+def render_cases(R):
+    """rendering.render (src/microcosmos/rendering.py:20-80) on small recorded timeseries:
+    nodes inside, outside and on top of each other, debug vectors, steric values below 0
+    and above 1; square and non-square grids, up- and down-sampling sizes, uniform colour
+    and no particles.  The module's display imports (cv2, matplotlib) are stubbed: render()
+    does not use them."""
+    import types
+    for name in ("matplotlib", "matplotlib.pyplot", "matplotlib.cm", "cv2"):
+        if name not in sys.modules:
+            sys.modules[name] = types.ModuleType(name)
+    sys.modules["matplotlib"].pyplot = sys.modules["matplotlib.pyplot"]
+    sys.modules["matplotlib"].cm = sys.modules["matplotlib.cm"]
+    import microcosmos.rendering as rendering
+    jnp = sys.modules["jax"].numpy
+    rng = np.random.default_rng(77)
+    cases = [("render_32x32", 32, 32, 3, 20, [(64, True, False), (16, True, False), (32, True, True), (48, False, False)]),
+             ("render_24x40", 24, 40, 2, 15, [(50, True, False), (20, True, False)])]
+    for name, H, W, T, N, variants in cases:
+        pos = rng.uniform(-3, [W + 3, H + 3], size=(T, N, 2)).astype(np.float32)
+        pos[:, 1] = pos[:, 0]  # a pixel hit by two nodes
+        dbg = rng.normal(0, 2.0, size=(T, N, 2)).astype(np.float32)
+        dbg[:, ::3] = 0.0      # debug pixels on top of their node
+        color = (np.arange(N) % 3).astype(np.int32)
+        steric = rng.uniform(-0.3, 1.4, size=(T, H, W)).astype(np.float32)
+        nodes = R["Nodes"](position=jnp.array(pos), velocity=jnp.zeros_like(jnp.array(pos)),
+                           color_bend=jnp.array(np.broadcast_to(color, (T, N)).copy()), debug_vector=jnp.array(dbg))
+        fields = R["Fields"](grid_shape=(H, W), steric=jnp.array(steric), fluid_velocity=jnp.zeros((T, 2, H, W)),
+                             f_grid=None)
+        out = dict(H=np.int32(H), W=np.int32(W), position=pos, debug_vector=dbg, color_bend=color, steric=steric)
+        for sz, particles, uniform in variants:
+            img = rendering.render(nodes, fields, sz, render_particles=particles, uniform_color=uniform)
+            out[f"frames_{sz}_{int(particles)}{int(uniform)}"] = A(img)
         save(name, **out)
 
 

@@ -212,7 +212,7 @@ def _make_jnp():
                  "all", "any", "allclose", "moveaxis", "argmax", "clip", "repeat", "tile",
                  "meshgrid", "square", "log", "isnan", "prod", "max", "min", "sign", "round",
                  "transpose", "reshape", "full_like", "ones_like", "linspace", "cumsum",
-                 "expand_dims", "squeeze", "diff", "dot", "outer", "cross", "atleast_1d"]:
+                 "expand_dims", "squeeze", "diff", "dot", "outer", "cross", "atleast_1d", "broadcast_to"]:
         setattr(jnp, name, passthrough(name))
 
     def zeros(shape, dtype=None):
@@ -265,6 +265,7 @@ def _make_jnp():
     jnp.pi = np.pi
     jnp.inf = np.inf
     jnp.float32, jnp.int32, jnp.float64, jnp.int64 = np.float32, np.int32, np.float64, np.int64
+    jnp.uint8 = np.uint8
     jnp.bool_ = np.bool_
     jnp.float_ = np.float32
     jnp.ndarray = Arr
@@ -423,8 +424,21 @@ def _make_jax():
 
     image = types.ModuleType("jax.image")
 
-    def resize(*a, **k):
-        raise NotImplementedError("jax.image.resize is not used when the fluid grid equals the domain grid")
+    def resize(x, shape, method, **k):
+        # method="nearest" as JAX's image resize evaluates it: along every axis whose size
+        # changes from m to n, output index o reads input floor((o + 0.5) * m / n), computed
+        # in float32.  (The linear method is used only when the fluid grid differs from the
+        # domain grid, which the fixtures do not do.)
+        if method != "nearest":
+            raise NotImplementedError("jax.image.resize(method=%r) is not restated" % method)
+        x = np.asarray(x)
+        for d, (m, n) in enumerate(zip(x.shape, shape)):
+            if m == n:
+                continue
+            o = ((np.arange(n, dtype=np.float32) + np.float32(0.5)) * np.float32(m)) / np.float32(n)
+            idx = np.floor(o).astype(np.int32)
+            x = np.take(x, idx, axis=d)
+        return _wrap(x)
     image.resize = resize
     jax.image = image
 
