@@ -77,12 +77,16 @@ typedef struct mc_config {
   double solver_dt;           /* ConstraintSolverConfig.dt (a Python float; Cosserat inertia weight), > 0 */
 } mc_config;
 
-/* Sizes of one rollout.  H, W: grid_shape (the fluid grid equals the domain grid). */
+/* Sizes of one rollout.  H, W: grid_shape, the domain grid of positions and of the steric
+ * field.  fluid_H, fluid_W: the lattice of f_grid (src/microcosmos/solver/fluid.py:221-235:
+ * IB points at position * (fluid_W / H, fluid_H / W), velocities and the velocity clamp
+ * scaled to match); 0 = the domain grid. */
 typedef struct mc_dims {
   int32_t H, W;
   int32_t N; /* nodes */
   int32_t E; /* edges (pairs) */
   int32_t B; /* bending pairs */
+  int32_t fluid_H, fluid_W;
 } mc_dims;
 
 /* Device state of one rollout (Nodes / Edges / Fields of src/microcosmos/structs/*.py).
@@ -95,8 +99,8 @@ typedef struct mc_state {
   float* bending_rest_angles; /* (B,)  in/out (overwritten by the actuation, if any) */
   const float* bending_stiffness; /* (B,) in */
   float* steric;              /* (H,W) in/out */
-  float* fluid_velocity;      /* (2,H,W) in/out (u* of the last step) */
-  float* f_grid;              /* (9,H,W) in/out */
+  float* fluid_velocity;      /* (2,fluid_H,fluid_W) in/out (u* of the last step) */
+  float* f_grid;              /* (9,fluid_H,fluid_W) in/out */
 } mc_state;
 
 /* Optional caller-side curvature actuation, evaluated on the device before every step:
@@ -117,7 +121,8 @@ typedef struct mc_record {
   float* position;       /* (T,N,2) */
   float* velocity;       /* (T,N,2) */
   float* steric;         /* (T,H,W) */
-  float* fluid_velocity; /* (T,2,H,W) */
+  float* fluid_velocity; /* (T,2,H,W): u* on the domain grid, linearly resized from the
+                          * fluid grid when the two differ (simulate.py:24-29) */
   int32_t every;         /* >= 1 */
 } mc_record;
 

@@ -48,7 +48,7 @@ class McConfig(ctypes.Structure):
 
 class McDims(ctypes.Structure):
     _fields_ = [("H", ctypes.c_int32), ("W", ctypes.c_int32), ("N", ctypes.c_int32),
-                ("E", ctypes.c_int32), ("B", ctypes.c_int32)]
+                ("E", ctypes.c_int32), ("B", ctypes.c_int32), ("fluid_H", ctypes.c_int32), ("fluid_W", ctypes.c_int32)]
 
 
 class McState(ctypes.Structure):

@@ -1061,6 +1061,8 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
     return gfail(MC_ERR_UNSUPPORTED, "ibm_kernel_size outside 1..8");
   if (cfg->enable_force_clamp) return gfail(MC_ERR_UNSUPPORTED, "enable_force_clamp has no adjoint here");
   if (cfg->synthetic_node_width != 0.0f) return gfail(MC_ERR_UNSUPPORTED, "synthetic_node_width must be 0");
+  if ((D.fluid_H > 0 && D.fluid_H != D.H) || (D.fluid_W > 0 && D.fluid_W != D.W))
+    return gfail(MC_ERR_UNSUPPORTED, "the adjoint needs the fluid grid to be the domain grid");
   if (cfg->solver_type != MC_SOLVER_PBD)
     return gfail(MC_ERR_UNSUPPORTED, "the adjoint covers the PBD rod constraint only");
   mc_grad_plan* p = new mc_grad_plan();

@@ -22,6 +22,9 @@ struct BinView {
   int* ctl;
   int cap;
   int count;
+  int gw;      // width of the grid the cells index (lattice for IB, domain grid for CIC)
+  int ntx;     // bin tiles per row of that grid
+  int ntiles;  // bin tiles of that grid
 };
 
 __device__ __forceinline__ BinView bin_view(const RDesc& d, int which) {
@@ -29,19 +32,21 @@ __device__ __forceinline__ BinView bin_view(const RDesc& d, int which) {
   if (which == 0) {
     v.cell = d.ib_cell; v.w = d.ib_w; v.store = d.ib_store; v.tcount = d.ib_tcount; v.ovf = d.ib_ovf;
     v.ctl = d.ib_ctl; v.cap = d.ib_cap; v.count = d.M;
+    v.gw = d.lW; v.ntx = d.lntile_x; v.ntiles = d.lntile_x * d.lntile_y;
   } else {
     v.cell = d.c_cell; v.w = d.c_w; v.store = d.c_store; v.tcount = d.c_tcount; v.ovf = d.c_ovf;
     v.ctl = d.c_ctl; v.cap = d.c_cap; v.count = d.enable_steric ? 4 * d.N : 0;
+    v.gw = d.W; v.ntx = d.ntile_x; v.ntiles = d.ntile_x * d.ntile_y;
   }
   return v;
 }
 
-__device__ __forceinline__ int tile_of(const RDesc& d, int cell) {
-  const int cy = cell / d.W, cx = cell - cy * d.W;
-  return (cy / kBinTile) * d.ntile_x + cx / kBinTile;
+__device__ __forceinline__ int tile_of(const BinView& v, int cell) {
+  const int cy = cell / v.gw, cx = cell - cy * v.gw;
+  return (cy / kBinTile) * v.ntx + cx / kBinTile;
 }
-__device__ __forceinline__ unsigned local_of(const RDesc& d, int cell) {
-  const int cy = cell / d.W, cx = cell - cy * d.W;
+__device__ __forceinline__ unsigned local_of(const BinView& v, int cell) {
+  const int cy = cell / v.gw, cx = cell - cy * v.gw;
   return (unsigned)((cy % kBinTile) * kBinTile + (cx % kBinTile));
 }
 
@@ -82,16 +87,16 @@ __device__ __forceinline__ void ib_head(const RDesc& d, int parity, int cell, fl
   d.h_start[slot] = run_pos;
   d.h_len[slot] = len;
   d.s_inv[slot] = 1.0f / max_prop(cov, 1.0f);
-  const int y = cell / d.W, x = cell - y * d.W;
-  const size_t HW = (size_t)d.H * d.W;
+  const int y = cell / d.lW, x = cell - y * d.lW;
+  const size_t HW = (size_t)d.lH * d.lW;
   const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
   const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
   float f[9];
   const float* hp = d.h[parity];
 #pragma unroll
   for (int q = 0; q < 9; ++q) {
-    const int ys = imod_floor(y - ey[q], d.H), xs = imod_floor(x - ex[q], d.W);
-    f[q] = hp[q * HW + (size_t)ys * d.W + xs];
+    const int ys = imod_floor(y - ey[q], d.lH), xs = imod_floor(x - ex[q], d.lW);
+    f[q] = hp[q * HW + (size_t)ys * d.lW + xs];
   }
   float rho, vx, vy;
   macroscopic(f, d.vmax, d.vmax_q4, rho, vx, vy);
@@ -136,7 +141,7 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
   const int total = v.tcount[t];
   if (total == 0) return;
   const int tid = threadIdx.x;
-  const int ntiles = d.ntile_x * d.ntile_y;
+  const int ntiles = v.ntiles;
   int* bin = v.store + (size_t)t * v.cap;
 
   // fast path: the whole tile sorted in shared memory (capacity capS <= the bin capacity)
@@ -153,7 +158,7 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
     // (arbitrary order), so each cell's run is then ordered by k
     for (int i = tid; i < total; i += blockDim.x) {
       const int k = bin[i];
-      const unsigned lc = local_of(d, v.cell[k]);
+      const unsigned lc = local_of(v, v.cell[k]);
       const int pos = atomicAdd(cnt + lc, 1);
       lr[i] = (lc << 24) | (unsigned)pos;
       kin[i] = k;
@@ -256,7 +261,7 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
   const int nbin = min(total, v.cap);
   for (int i = tid; i < nbin; i += blockDim.x) {
     const int k = bin[i];
-    bufB[i] = (local_of(d, v.cell[k]) << 24) | (unsigned)k;
+    bufB[i] = (local_of(v, v.cell[k]) << 24) | (unsigned)k;
   }
   if (tid == 0) s_fill = nbin;
   __syncthreads();
@@ -266,7 +271,7 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
     const int no = v.ctl[0];
     for (int i = tid; i < no; i += blockDim.x) {
       const int k = v.ovf[i];
-      if (tile_of(d, v.cell[k]) == t) bufB[atomicAdd(&s_fill, 1)] = (local_of(d, v.cell[k]) << 24) | (unsigned)k;
+      if (tile_of(v, v.cell[k]) == t) bufB[atomicAdd(&s_fill, 1)] = (local_of(v, v.cell[k]) << 24) | (unsigned)k;
     }
   }
   __syncthreads();
@@ -581,7 +586,7 @@ __global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, co
     }
     rollout_barrier(d.ib_ctl, nb, d.flags);
   }
-  const size_t HW = (size_t)d.H * d.W;
+  const size_t HW = (size_t)d.lH * d.lW;
   const int nflag = d.lbm_tx * d.lbm_ty;
   for (int p = t0; p < nheads; p += stride) {
     float ucx = __ldcg(d.s_ucx + p), ucy = __ldcg(d.s_ucy + p);
@@ -601,7 +606,7 @@ __global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, co
     const int cell = d.h_cell[p];
     d.fov[cell] = Fx;
     d.fov[HW + cell] = Fy;
-    const int y = cell / d.W, x = cell - y * d.W;
+    const int y = cell / d.lW, x = cell - y * d.lW;
     d.lbm_flag[(parity & 1) * nflag + (y / d.lbm_th) * d.lbm_tx + x / d.lbm_tw] = 1;
   }
 }
@@ -629,10 +634,10 @@ __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D
   d.s_fx[p] = Fx;
   d.s_fy[p] = Fy;
   const int cell = d.h_cell[p];
-  const size_t HW = (size_t)d.H * d.W;
+  const size_t HW = (size_t)d.lH * d.lW;
   d.fov[cell] = Fx;
   d.fov[HW + cell] = Fy;
-  const int y = cell / d.W, x = cell - y * d.W;
+  const int y = cell / d.lW, x = cell - y * d.lW;
   d.lbm_flag[(parity & 1) * d.lbm_tx * d.lbm_ty + (y / d.lbm_th) * d.lbm_tx + x / d.lbm_tw] = 1;
 }
 
@@ -687,7 +692,39 @@ __global__ void __launch_bounds__(256) k_reaction(const RDesc* __restrict__ D, c
   }
 }
 
-// Per-step field recording (steric, fluid_velocity) on recording steps.
+// One output sample of a linear, antialiased resize along one axis (JAX's image resize,
+// method "linear": triangle kernel widened by max(m/n, 1), weights normalised by their sum
+// over the input, zero outside the sampled range): input m -> output n, output index o.
+// Writes the first input index and up to kResizeTaps normalised weights; returns the count.
+constexpr int kResizeTaps = 16;
+__device__ int resize_taps(int o, int m, int n, float inv, float ks, int& i0, float* w) {
+  if (m == n) {
+    i0 = o;
+    w[0] = 1.0f;
+    return 1;
+  }
+  const float sf = ((float)o + 0.5f) * inv - 0.5f;
+  int a = (int)floorf(sf - ks), b = (int)ceilf(sf + ks);
+  a = a < 0 ? 0 : a;
+  b = b > m - 1 ? m - 1 : b;
+  if (b - a + 1 > kResizeTaps) b = a + kResizeTaps - 1;  // plans keep the support within the taps
+  float tot = 0.0f;
+  for (int i = a; i <= b; ++i) {
+    float x = fabsf(sf - (float)i) / ks;
+    const float v = 1.0f - fabsf(x);
+    w[i - a] = v > 0.0f ? v : 0.0f;
+    tot = tot + w[i - a];
+  }
+  const bool inside = sf >= -0.5f && sf <= (float)m - 0.5f;
+  const bool norm = fabsf(tot) > 1000.0f * MC_EPSIL;
+  for (int i = a; i <= b; ++i) w[i - a] = (inside && norm) ? w[i - a] / tot : 0.0f;
+  i0 = a;
+  return b - a + 1;
+}
+
+// Per-step field recording (steric, fluid_velocity) on recording steps.  The recorded u*
+// is on the domain grid: a copy when the lattice is the domain grid, else the linear
+// resize of simulate.py:24-29.
 __global__ void k_record_fields(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
                                 const int* __restrict__ tdev) {
   const int r = find_rollout(off, n, blockIdx.x);
@@ -696,13 +733,31 @@ __global__ void k_record_fields(const RDesc* __restrict__ D, const int* __restri
   const int t = *tdev;
   if ((t + 1) % d.rec_every != 0) return;
   const size_t e = (size_t)((t + 1) / d.rec_every - 1);
-  const size_t HW = (size_t)d.H * d.W;
+  const size_t HW = (size_t)d.H * d.W, LHW = (size_t)d.lH * d.lW;
+  const bool same = d.lH == d.H && d.lW == d.W;
   const size_t stride = (size_t)(off[r + 1] - off[r]) * blockDim.x;
   for (size_t i = (size_t)(blockIdx.x - off[r]) * blockDim.x + threadIdx.x; i < HW; i += stride) {
     if (d.rec_steric) d.rec_steric[e * HW + i] = d.steric[i];
-    if (d.rec_fluid) {
+    if (!d.rec_fluid) continue;
+    if (same) {
       d.rec_fluid[e * 2 * HW + i] = d.fluid_vel[i];
       d.rec_fluid[e * 2 * HW + HW + i] = d.fluid_vel[HW + i];
+      continue;
+    }
+    const int y = (int)(i / d.W), x = (int)(i - (size_t)y * d.W);
+    float wy[kResizeTaps], wx[kResizeTaps];
+    int y0, x0;
+    const int ny = resize_taps(y, d.lH, d.H, d.rs_inv_y, d.rs_ks_y, y0, wy);
+    const int nx = resize_taps(x, d.lW, d.W, d.rs_inv_x, d.rs_ks_x, x0, wx);
+    for (int c = 0; c < 2; ++c) {
+      const float* u = d.fluid_vel + c * LHW;
+      float acc = 0.0f;
+      for (int a = 0; a < ny; ++a) {
+        float row = 0.0f;
+        for (int b = 0; b < nx; ++b) row = row + wx[b] * u[(size_t)(y0 + a) * d.lW + x0 + b];
+        acc = acc + wy[a] * row;
+      }
+      d.rec_fluid[e * 2 * HW + c * HW + i] = acc;
     }
   }
 }

@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(256) k_lbm(const RDesc* __restrict__ D, const 
   const int lb = blockIdx.x - off[r];
   const int tx = lb % d.lbm_tx, ty = lb / d.lbm_tx;
   const int lane = threadIdx.x;
-  const int H = d.H, W = d.W;
+  const int H = d.lH, W = d.lW;
   const int y = ty * d.lbm_th + threadIdx.y;
   const int x0 = tx * (32 * VEC) + lane * VEC;
   const bool row_ok = y < H;
@@ -159,15 +159,15 @@ __global__ void k_unstream(const RDesc* __restrict__ D, const int* __restrict__ 
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int lb = blockIdx.x - off[r];
-  const size_t HW = (size_t)d.H * d.W;
+  const size_t HW = (size_t)d.lH * d.lW;
   const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
   const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
   for (size_t idx = (size_t)lb * blockDim.x + threadIdx.x; idx < HW; idx += (size_t)(off[r + 1] - off[r]) * blockDim.x) {
-    int y = (int)(idx / d.W), x = (int)(idx % d.W);
+    int y = (int)(idx / d.lW), x = (int)(idx % d.lW);
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
-      int ys = imod_floor(y + ey[i], d.H), xs = imod_floor(x + ex[i], d.W);
-      d.h[0][i * HW + idx] = max_prop(d.f_grid[i * HW + (size_t)ys * d.W + xs], MC_EPSIL);
+      int ys = imod_floor(y + ey[i], d.lH), xs = imod_floor(x + ex[i], d.lW);
+      d.h[0][i * HW + idx] = max_prop(d.f_grid[i * HW + (size_t)ys * d.lW + xs], MC_EPSIL);
     }
   }
 }
@@ -178,16 +178,16 @@ __global__ void k_stream_out(const RDesc* __restrict__ D, const int* __restrict_
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int lb = blockIdx.x - off[r];
-  const size_t HW = (size_t)d.H * d.W;
+  const size_t HW = (size_t)d.lH * d.lW;
   const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
   const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
   const float* h = d.h[parity];
   for (size_t idx = (size_t)lb * blockDim.x + threadIdx.x; idx < HW; idx += (size_t)(off[r + 1] - off[r]) * blockDim.x) {
-    int y = (int)(idx / d.W), x = (int)(idx % d.W);
+    int y = (int)(idx / d.lW), x = (int)(idx % d.lW);
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
-      int ys = imod_floor(y - ey[i], d.H), xs = imod_floor(x - ex[i], d.W);
-      d.f_grid[i * HW + idx] = max_prop(h[i * HW + (size_t)ys * d.W + xs], MC_EPSIL);
+      int ys = imod_floor(y - ey[i], d.lH), xs = imod_floor(x - ex[i], d.lW);
+      d.f_grid[i * HW + idx] = max_prop(h[i * HW + (size_t)ys * d.lW + xs], MC_EPSIL);
     }
   }
 }
@@ -198,16 +198,14 @@ __global__ void k_clear_ws(const RDesc* __restrict__ D, const int* __restrict__ 
   const RDesc& d = D[r];
   const int lb = blockIdx.x - off[r];
   const size_t stride = (size_t)(off[r + 1] - off[r]) * blockDim.x;
-  const size_t HW = (size_t)d.H * d.W;
+  const size_t HW = (size_t)d.H * d.W, LHW = (size_t)d.lH * d.lW;
   const size_t t0 = (size_t)lb * blockDim.x + threadIdx.x;
-  for (size_t i = t0; i < 2 * HW; i += stride) d.fov[i] = nan_f();
+  for (size_t i = t0; i < 2 * LHW; i += stride) d.fov[i] = nan_f();
   if (d.dep)
     for (size_t i = t0; i < HW; i += stride) d.dep[i] = 0.0f;
-  const int nt = d.ntile_x * d.ntile_y;
-  for (size_t i = t0; i < (size_t)nt; i += stride) {
-    d.ib_tcount[i] = 0;
-    d.c_tcount[i] = 0;
-  }
+  const int nt = d.ntile_x * d.ntile_y, lnt = d.lntile_x * d.lntile_y;
+  for (size_t i = t0; i < (size_t)lnt; i += stride) d.ib_tcount[i] = 0;
+  for (size_t i = t0; i < (size_t)nt; i += stride) d.c_tcount[i] = 0;
   for (size_t i = t0; i < (size_t)2 * d.lbm_tx * d.lbm_ty; i += stride) d.lbm_flag[i] = 0;
   if (t0 < 8) {
     d.ib_ctl[t0] = 0;

@@ -31,11 +31,14 @@ constexpr int kFftColsPerCta = 2;  // complex columns per column-pass CTA (4 rea
 // Per-rollout descriptor.  All pointers are device pointers.
 struct RDesc {
   // sizes
-  int H, W, N, E, B, K;  // K = ibm_kernel_size
+  int H, W, N, E, B, K;  // H, W: the domain grid (positions, steric field); K = ibm_kernel_size
+  int lH, lW;            // the fluid lattice (f_grid, IB stencils, force overlay)
   int ncomp;             // rod components
   int NI;                // IB points: N, or 2N with synthetic node pairs
   int M;                 // IB contributions = NI*K*K
-  int ntile_x, ntile_y;  // binning tiles (kBinTile)
+  int ntile_x, ntile_y;  // binning tiles (kBinTile) of the domain grid (cloud-in-cell deposit)
+  int lntile_x, lntile_y;  // binning tiles of the lattice (IB contributions)
+  float rs_inv_y, rs_ks_y, rs_inv_x, rs_ks_x;  // lattice -> domain resize of the recorded u*: 1/scale, kernel width
   int lbm_tx, lbm_ty;    // LBM tiles
   int lbm_tw;            // LBM tile width in cells (32 * cells per lane)
   int lbm_th;            // LBM tile height in rows (threads per CTA = 32 * lbm_th)
@@ -101,8 +104,8 @@ struct RDesc {
   const float* edeg;   // (E,) max(bending degree, 1)
   const float* ndeg;   // (N,) max(node degree, 1)
   // workspace
-  float* h[2];         // pull-scheme post-collision populations (9,H,W)
-  float* fov;          // (2,H,W) force overlay, NaN = no IB force at the cell
+  float* h[2];         // pull-scheme post-collision populations (9,lH,lW)
+  float* fov;          // (2,lH,lW) force overlay, NaN = no IB force at the cell
   int* lbm_flag;       // (2 * lbm_ty*lbm_tx) tile has overlay entries, one set per step parity
   float* dep;          // (H,W) CIC deposit (kept zero between steps)
   float* tmp;          // (H,W) FFT row-pass output

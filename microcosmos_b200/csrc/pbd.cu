@@ -234,8 +234,8 @@ __global__ void __launch_bounds__(256) k_stencil(const RDesc* __restrict__ D, co
       const float ry = fabsf((sy + (float)a) - gy) / hw;
       wx[a] = rx <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * rx) / 2.0f)) : 0.0f;
       wy[a] = ry <= 2.0f ? 0.25f * (1.0f + cosf((MC_PI_F * ry) / 2.0f)) : 0.0f;
-      cx[a] = imod_floor((int)(sx + (float)a), d.W);
-      cy[a] = imod_floor((int)(sy + (float)a), d.H);
+      cx[a] = imod_floor((int)(sx + (float)a), d.lW);
+      cy[a] = imod_floor((int)(sy + (float)a), d.lH);
     }
   }
   float sum = 0.0f;
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(256) k_stencil(const RDesc* __restrict__ D, co
   if (tyo < 0) tyo = ty0;
   const int nx0 = K - nx1, ny0 = K - ny1;
   int base[4];
-  const int tiles[4] = {ty0 * d.ntile_x + tx0, ty0 * d.ntile_x + txo, tyo * d.ntile_x + tx0, tyo * d.ntile_x + txo};
+  const int tiles[4] = {ty0 * d.lntile_x + tx0, ty0 * d.lntile_x + txo, tyo * d.lntile_x + tx0, tyo * d.lntile_x + txo};
   const int counts[4] = {nx0 * ny0, nx1 * ny0, nx0 * ny1, nx1 * ny1};
   if (split_ok) {
 #pragma unroll
@@ -292,14 +292,14 @@ __global__ void __launch_bounds__(256) k_stencil(const RDesc* __restrict__ D, co
           const int ys = (cy[b] / kBinTile != ty0) ? 1 : 0;
           const int g = xs + 2 * ys;
           const int k = p * K2 + a * K + b;
-          d.ib_cell[k] = cy[b] * d.W + cx[a];
+          d.ib_cell[k] = cy[b] * d.lW + cx[a];
           d.ib_w[k] = (wx[a] * wy[b]) / den;
           int tile, pos;
           if (split_ok) {
             tile = tiles[g];
             pos = base[g] + rank[g]++;
           } else {
-            tile = (cy[b] / kBinTile) * d.ntile_x + cx[a] / kBinTile;
+            tile = (cy[b] / kBinTile) * d.lntile_x + cx[a] / kBinTile;
             pos = atomicAdd(d.ib_tcount + tile, 1);
             if (pos == 0) d.wl_ib[atomicAdd(d.wl_ctl, 1)] = make_int2(d.ridx, tile);
           }
@@ -358,12 +358,12 @@ __global__ void __launch_bounds__(256) k_stencil16(const RDesc* __restrict__ D, 
   for (int q = 0; q < K2; ++q) sum = sum + __shfl_sync(gmask, w, q, 16);
   const float den = sum + MC_EPSIL;
   if (!act) return;
-  const int cx = imod_floor((int)(sx + (float)a), d.W);
-  const int cy = imod_floor((int)(sy + (float)b), d.H);
+  const int cx = imod_floor((int)(sx + (float)a), d.lW);
+  const int cy = imod_floor((int)(sy + (float)b), d.lH);
   const int k = p * K2 + s;
-  d.ib_cell[k] = cy * d.W + cx;
+  d.ib_cell[k] = cy * d.lW + cx;
   d.ib_w[k] = w / den;
-  const int tile = (cy / kBinTile) * d.ntile_x + cx / kBinTile;
+  const int tile = (cy / kBinTile) * d.lntile_x + cx / kBinTile;
   const unsigned active = __activemask();
   const unsigned group = __match_any_sync(active, tile);
   const int leader = __ffs(group) - 1;

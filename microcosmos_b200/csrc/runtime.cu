@@ -76,6 +76,8 @@ struct HostRollout {
   bool fft_ok = false, conv_ok = false, use_conv = false;
   Region r_cgW, r_cgH;
   int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4, lbm_th = mc::kLbmTileY;
+  int lH = 0, lW = 0;      // the fluid lattice (= dims.H, dims.W unless dims.fluid_H/W are set)
+  int lntx = 0, lnty = 0;  // bin tiles of the lattice (IB); ntx, nty: of the domain grid (CIC)
   int ib_cap = 0, c_cap = 0;  // bin capacities (powers of two)
   int logW = -1, logH = -1;   // log2 of power-of-two grid sides (-1: mixed radix path)
   int T_r = 0, P_r = 0, T_c = 0, P_c = 0;
@@ -357,6 +359,10 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.NI = h.dims.N * (h.cfg.synthetic_node_width > 0.0f ? 2 : 1);
   d.ntile_x = h.ntx;
   d.ntile_y = h.nty;
+  d.lH = h.lH;
+  d.lW = h.lW;
+  d.lntile_x = h.lntx;
+  d.lntile_y = h.lnty;
   d.lbm_tx = h.lbm_tx;
   d.lbm_ty = h.lbm_ty;
   d.lbm_tw = 32 * h.vec;
@@ -370,7 +376,17 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.syn_w = c.synthetic_node_width;
   d.cos_w = (float)(1.0 / (c.solver_dt * c.solver_dt));
   // mean_scale = 1 (fluid grid == domain grid) but scale keeps the reference's axis order
-  const double sx = (double)h.dims.W / (double)h.dims.H, sy = (double)h.dims.H / (double)h.dims.W;
+  // scale = (w / grid_shape[0], h / grid_shape[1]) with (h, w) the lattice (fluid.py:222-226)
+  const double sx = (double)h.lW / (double)h.dims.H, sy = (double)h.lH / (double)h.dims.W;
+  {
+    // linear resize of the recorded u* from the lattice to the domain grid: 1/scale and the
+    // antialiasing kernel width max(1/scale, 1) per axis
+    const double iy = 1.0 / ((double)h.dims.H / (double)h.lH), ix = 1.0 / ((double)h.dims.W / (double)h.lW);
+    d.rs_inv_y = (float)iy;
+    d.rs_inv_x = (float)ix;
+    d.rs_ks_y = std::max((float)iy, 1.0f);
+    d.rs_ks_x = std::max((float)ix, 1.0f);
+  }
   d.scale_x = (float)sx;
   d.scale_y = (float)sy;
   d.syn_ms = (float)(0.5 * (sx + sy));
@@ -911,6 +927,13 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       delete p;
       return fail(MC_ERR_INVALID, "rollout " + std::to_string(i) + ": grid must be at least 4x4 and counts >= 0");
     }
+    h.lH = D.fluid_H > 0 ? D.fluid_H : D.H;
+    h.lW = D.fluid_W > 0 ? D.fluid_W : D.W;
+    if (D.fluid_H < 0 || D.fluid_W < 0 || h.lH < 4 || h.lW < 4 || h.lH > 7 * D.H || h.lW > 7 * D.W) {
+      delete p;
+      return fail(MC_ERR_INVALID, "rollout " + std::to_string(i) +
+                                      ": the fluid grid must be at least 4x4 and at most 7 times the domain grid");
+    }
     if ((D.E > 0 && !pairs[i]) || (D.B > 0 && !bending_pairs[i])) {
       delete p;
       return fail(MC_ERR_INVALID, "null topology array");
@@ -994,16 +1017,18 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       h.T_c = threads_for(D.H, 512);
       h.P_c = 512 / h.T_c;
     }
-    h.vec = (D.W % 2 == 0) ? 2 : 1;
+    h.vec = (h.lW % 2 == 0) ? 2 : 1;
     if (vec_all == -1) vec_all = h.vec;
     if (vec_all != h.vec) vec_all = 1;
     h.ntx = div_up(D.W, mc::kBinTile);
     h.nty = div_up(D.H, mc::kBinTile);
-    const size_t HW = (size_t)D.H * D.W;
-    const size_t N = D.N, E = D.E, B = D.B, nt = (size_t)h.ntx * h.nty;
-    h.r_h0 = lay.take(9 * HW * 4);
-    h.r_h1 = lay.take(9 * HW * 4);
-    h.r_fov = lay.take(2 * HW * 4);
+    h.lntx = div_up(h.lW, mc::kBinTile);
+    h.lnty = div_up(h.lH, mc::kBinTile);
+    const size_t HW = (size_t)D.H * D.W, LHW = (size_t)h.lH * h.lW;
+    const size_t N = D.N, E = D.E, B = D.B, nt = (size_t)h.ntx * h.nty, lnt = (size_t)h.lntx * h.lnty;
+    h.r_h0 = lay.take(9 * LHW * 4);
+    h.r_h1 = lay.take(9 * LHW * 4);
+    h.r_fov = lay.take(2 * LHW * 4);
     h.r_dep = lay.take(HW * 4);
     h.r_tmp = lay.take(HW * 4);
     h.r_prev = lay.take(2 * N * 4);
@@ -1016,17 +1041,17 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.r_ibcell = lay.take(Mz * 4);
     h.r_ibw = lay.take(Mz * 4);
     // bin capacity: at least 3x the mean contributions per tile, a power of two
-    auto cap_for = [&](long long contributions, int minimum) {
-      long long want = std::max<long long>(minimum, (3 * contributions + (long long)nt - 1) / (long long)nt);
+    auto cap_for = [&](long long contributions, int minimum, size_t tiles) {
+      long long want = std::max<long long>(minimum, (3 * contributions + (long long)tiles - 1) / (long long)tiles);
       int c = 1;
       while (c < want && c < mc::kMaxBinCap) c <<= 1;
       return c;
     };
-    h.ib_cap = cap_for((long long)Mz, mc::kIbCap);
-    h.c_cap = cap_for(4LL * (long long)N, mc::kCicCap);
-    h.r_ibstore = lay.take((nt * h.ib_cap + 2 * Mz) * 4);
-    h.r_ibstorew = lay.take((nt * h.ib_cap + 2 * Mz) * 4);
-    h.r_ibtc = lay.take(nt * 4);
+    h.ib_cap = cap_for((long long)Mz, mc::kIbCap, lnt);
+    h.c_cap = cap_for(4LL * (long long)N, mc::kCicCap, nt);
+    h.r_ibstore = lay.take((lnt * h.ib_cap + 2 * Mz) * 4);
+    h.r_ibstorew = lay.take((lnt * h.ib_cap + 2 * Mz) * 4);
+    h.r_ibtc = lay.take(lnt * 4);
     h.r_ibovf = lay.take(Mz * 4);
     h.r_ibctl = lay.take(8 * 4);
     h.r_ibslot = lay.take(Mz * 4);
@@ -1076,16 +1101,20 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     HostRollout& h = p->R[i];
     h.vec = vec_all;
     h.lbm_th = mc::kLbmTileY;
-    h.lbm_tx = div_up(h.dims.W, 32 * h.vec);
-    h.lbm_ty = div_up(h.dims.H, h.lbm_th);
+    h.lbm_tx = div_up(h.lW, 32 * h.vec);
+    h.lbm_ty = div_up(h.lH, h.lbm_th);
     // sized for the smallest tiles a plan can be tuned to (mc_plan_set_lbm_shape)
-    h.r_lflag = lay.take((size_t)2 * div_up(h.dims.W, 32) * div_up(h.dims.H, mc::kLbmMinTileY) * 4);
+    h.r_lflag = lay.take((size_t)2 * div_up(h.lW, 32) * div_up(h.lH, mc::kLbmMinTileY) * 4);
   }
   {
-    long long tiles = 0;
-    for (auto& h : p->R) tiles += (long long)h.ntx * h.nty;
-    p->r_wl_ib = lay.take((size_t)tiles * sizeof(int2));
+    long long tiles = 0, ltiles = 0;
+    for (auto& h : p->R) {
+      tiles += (long long)h.ntx * h.nty;
+      ltiles += (long long)h.lntx * h.lnty;
+    }
+    p->r_wl_ib = lay.take((size_t)ltiles * sizeof(int2));
     p->r_wl_cic = lay.take((size_t)tiles * sizeof(int2));
+    tiles = std::max(tiles, ltiles);
     p->n_tiles = tiles;
     p->tile_grid = (int)std::max(1LL, std::min(tiles, 148LL * 8 * (256 / p->bin_threads)));
     for (auto& h : p->R) {
@@ -1105,7 +1134,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
   for (int i = 0; i < n; ++i) {
     HostRollout& h = p->R[i];
     const mc_config& c = h.cfg;
-    const long long HW = (long long)h.dims.H * h.dims.W;
+    const long long HW = std::max((long long)h.dims.H * h.dims.W, (long long)h.lH * h.lW);
     int cnt[K_COUNT];
     // node kernels cover the IB points too (twice the nodes with synthetic pairs); the
     // node-only kernels return for indices >= N
@@ -1237,15 +1266,15 @@ mc_status mc_plan_set_lbm_shape(mc_plan* p, int32_t cells_per_lane, int32_t rows
   if (vec != 1 && vec != 2 && vec != 4) return fail(MC_ERR_INVALID, "cells_per_lane must be 1, 2 or 4");
   if (rows != 2 && rows != 4 && rows != 8) return fail(MC_ERR_INVALID, "rows_per_cta must be 2, 4 or 8");
   for (auto& h : p->R)
-    if (h.dims.W % vec != 0 || h.dims.W < vec)
-      return fail(MC_ERR_UNSUPPORTED, "cells_per_lane must divide every rollout's W");
+    if (h.lW % vec != 0 || h.lW < vec)
+      return fail(MC_ERR_UNSUPPORTED, "cells_per_lane must divide every rollout's lattice width");
   int prev = 0;
   for (int i = 0; i < p->n; ++i) {
     HostRollout& h = p->R[i];
     h.vec = vec;
     h.lbm_th = rows;
-    h.lbm_tx = div_up(h.dims.W, 32 * vec);
-    h.lbm_ty = div_up(h.dims.H, rows);
+    h.lbm_tx = div_up(h.lW, 32 * vec);
+    h.lbm_ty = div_up(h.lH, rows);
     p->off[K_LBM][i] = prev;
     prev += h.cfg.enable_fluid ? h.lbm_tx * h.lbm_ty : 0;
   }

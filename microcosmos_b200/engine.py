@@ -93,6 +93,15 @@ class DeviceState:
         return self.position.shape[0]
 
     @property
+    def lH(self):
+        """Rows of the fluid lattice (f_grid)."""
+        return int(self.f_grid.shape[1])
+
+    @property
+    def lW(self):
+        return int(self.f_grid.shape[2])
+
+    @property
     def E(self):
         return int(self.pairs.shape[0])
 
@@ -109,6 +118,9 @@ class DeviceState:
         bp_h = np.ascontiguousarray(
             bending_pairs.detach().cpu().numpy() if isinstance(bending_pairs, torch.Tensor) else bending_pairs,
             dtype=np.int32).reshape(-1, 2)
+        # f_grid (9, h, w) on its own lattice; a flat array is taken on the domain grid
+        fg = _dev(f_grid, device=device)
+        fg = (fg if fg.dim() == 3 else fg.reshape(9, H, W)).clone()
         return cls(
             H=int(H), W=int(W),
             position=_dev(position, device=device).reshape(-1, 2).clone(),
@@ -120,9 +132,8 @@ class DeviceState:
             steric=(_dev(steric, device=device).clone() if steric is not None
                     else torch.zeros((H, W), dtype=_F32, device=device)),
             fluid_velocity=(_dev(fluid_velocity, device=device).clone() if fluid_velocity is not None
-                            else torch.zeros((2, H, W), dtype=_F32, device=device)),
-            f_grid=_dev(f_grid, device=device).reshape(9, H, W).clone(),
-            pairs=pairs_h, bending_pairs=bp_h)
+                            else torch.zeros((2,) + tuple(fg.shape[1:]), dtype=_F32, device=device)),
+            f_grid=fg, pairs=pairs_h, bending_pairs=bp_h)
 
     @classmethod
     def from_scenario(cls, sc, device="cuda"):
@@ -206,7 +217,7 @@ class Plan:
 
     def __init__(self, specs, device="cuda", lbm_shape=None, steric_method=0, fft_values=0, bin_threads=0,
                  bin_sort_capacity=0):
-        """specs: list of (H, W, N, pairs(E,2) int32, bending_pairs(B,2) int32, cfg, dt).
+        """specs: list of (H, W, N, pairs(E,2) int32, bending_pairs(B,2) int32, cfg, dt[, (fluid_H, fluid_W)]).
         ``lbm_shape`` = (cells_per_lane, rows_per_cta) of the dense pass (default: the
         library's choice; ``microcosmos_b200.autotune`` picks one by timing).
         ``steric_method``: 0 = per rollout (direct convolution where it applies, else
@@ -223,11 +234,13 @@ class Plan:
         self._keep = []
         pp = (_lib.c_int_p * n)()
         bp = (_lib.c_int_p * n)()
-        for i, (H, W, N, pairs, bpairs, cfg, dt) in enumerate(specs):
+        for i, spec in enumerate(specs):
+            H, W, N, pairs, bpairs, cfg, dt = spec[:7]
+            fh, fw = spec[7] if len(spec) > 7 else (0, 0)
             pairs = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
             bpairs = np.ascontiguousarray(bpairs, dtype=np.int32).reshape(-1, 2)
             self._keep += [pairs, bpairs]
-            dims[i] = _lib.McDims(int(H), int(W), int(N), pairs.shape[0], bpairs.shape[0])
+            dims[i] = _lib.McDims(int(H), int(W), int(N), pairs.shape[0], bpairs.shape[0], int(fh), int(fw))
             cfgs[i] = mc_config(cfg)
             dts[i] = float(dt)
             pp[i] = pairs.ctypes.data_as(_lib.c_int_p)
@@ -258,7 +271,7 @@ class Plan:
     @classmethod
     def for_states(cls, states, cfgs, dts, device="cuda", lbm_shape=None, steric_method=0, fft_values=0,
                    bin_threads=0, bin_sort_capacity=0):
-        specs = [(s.H, s.W, s.N, s.pairs, s.bending_pairs, c, d) for s, c, d in zip(states, cfgs, dts)]
+        specs = [(s.H, s.W, s.N, s.pairs, s.bending_pairs, c, d, (s.lH, s.lW)) for s, c, d in zip(states, cfgs, dts)]
         return cls(specs, device=device, lbm_shape=lbm_shape, steric_method=steric_method, fft_values=fft_values,
                    bin_threads=bin_threads, bin_sort_capacity=bin_sort_capacity)
 

@@ -39,7 +39,7 @@ def _plan_for(state: DeviceState, cfg: ConstraintSolverConfig, dt: float) -> Pla
     h.update(state.pairs.tobytes())
     h.update(b"|")
     h.update(state.bending_pairs.tobytes())
-    key = (state.H, state.W, state.N, h.hexdigest(), cfg, float(dt), torch.cuda.current_device())
+    key = (state.H, state.W, state.lH, state.lW, state.N, h.hexdigest(), cfg, float(dt), torch.cuda.current_device())
     p = _PLAN_CACHE.get(key)
     if p is None:
         p = Plan.for_states([state], [cfg], [dt])
@@ -54,8 +54,8 @@ def _plan_for(state: DeviceState, cfg: ConstraintSolverConfig, dt: float) -> Pla
 def _state(nodes: Nodes, edges: Edges, fields: Fields) -> DeviceState:
     H, W = (int(v) for v in fields.grid_shape)
     f = fields.f_grid
-    if tuple(f.shape) != (9, H, W):
-        raise NotImplementedError("the fluid grid must equal grid_shape (fluid_grid_shape != grid_shape is not implemented)")
+    if len(tuple(f.shape)) != 3 or f.shape[0] != 9:
+        raise ValueError("f_grid must be (9, h, w): the fluid lattice, grid_shape or its own (fluid.py:221-235)")
     return DeviceState.from_arrays(H, W, nodes.position, nodes.velocity, _np(edges.pairs, np.int32), edges.theta,
                                    edges.rest_lengths, _np(edges.bending_pairs, np.int32),
                                    edges.bending_rest_angles, edges.bending_stiffness, f, fields.steric,

@@ -602,6 +602,28 @@ def step(s: State, cfg: Config, dtstep: float, rest_angles=None, ib_positions=No
     return s
 
 
+def resize_linear(x, shape):
+    """jax.image.resize(x, shape, method="linear") as the reference records u* on the domain
+    grid when the fluid lattice differs (simulate.py:24-29): along each axis whose size
+    changes (m -> n), output o = sum_i w[i, o] x[i] with the triangle kernel at
+    sample (o + 0.5) m/n - 0.5, widened by max(m/n, 1) (antialiasing), weights normalised
+    by their sum and zero outside [-0.5, m - 0.5].  Restated from JAX's published resize;
+    sums in index order (JAX's einsum order is unspecified)."""
+    out = np.asarray(x, np.float32)
+    for d, (m, n) in enumerate(zip(out.shape, shape)):
+        if m == n:
+            continue
+        inv = np.float32(1.0 / (n / m))
+        ks = max(inv, np.float32(1.0))
+        sf = (np.arange(n, dtype=np.float32) + np.float32(0.5)) * inv - np.float32(0.5)
+        w = np.maximum(np.float32(0.0), np.float32(1.0) - np.abs(sf[None, :] - np.arange(m, dtype=np.float32)[:, None]) / ks)
+        tot = w.sum(axis=0, keepdims=True)
+        w = np.where(np.abs(tot) > np.float32(1000.0 * EPSIL32), w / np.where(tot != 0, tot, 1), 0)
+        w = np.where(((sf >= -0.5) & (sf <= m - 0.5))[None, :], w, 0).astype(np.float32)
+        out = np.moveaxis(np.tensordot(np.moveaxis(out, d, -1), w, axes=([-1], [0])), -1, d).astype(np.float32)
+    return out
+
+
 def actuation(act, t):
     """rest[b](t) = c[b] + A sin(omega t + phase) (caller-side actuation closed form)."""
     c, amp, om, ph = act
@@ -622,7 +644,8 @@ def simulate(s: State, cfg: Config, dtstep: float, num_steps: int, act=None, rec
             ts["position"].append(s.position)
             ts["velocity"].append(s.velocity)
             ts["steric"].append(s.steric)
-            ts["fluid_velocity"].append(s.fluid_velocity)
+            u = s.fluid_velocity
+            ts["fluid_velocity"].append(u if u.shape[1:] == (s.H, s.W) else resize_linear(u, (2, s.H, s.W)))
     if record:
         ts = {k: np.stack(v) for k, v in ts.items()}
     return s, ts

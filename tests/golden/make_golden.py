@@ -116,7 +116,7 @@ def save(name, **arrs):
     print("wrote", path, sum(v.nbytes for v in arrs.values()), "bytes")
 
 
-GROUPS = ("base", "cosserat", "synthetic", "gym", "render")
+GROUPS = ("base", "cosserat", "synthetic", "gym", "render", "fluidgrid")
 
 
 def main(ref_root, groups=GROUPS):
@@ -131,6 +131,8 @@ def main(ref_root, groups=GROUPS):
         gym_cases(R)
     if "render" in groups:
         render_cases(R)
+    if "fluidgrid" in groups:
+        fluidgrid_cases(R)
 
 
 def base_cases(R):
@@ -413,6 +415,56 @@ def render_cases(R):
             img = rendering.render(nodes, fields, sz, render_particles=particles, uniform_color=uniform)
             out[f"frames_{sz}_{int(particles)}{int(uniform)}"] = A(img)
         save(name, **out)
+
+
+def _on_lattice(sc, h, w, rng, u0_std=1e-3):
+    """The scenario's fluid moved to an h x w lattice: feq(1, u0) with fresh u0."""
+    from microcosmos_b200 import scenarios as S
+    ux = rng.normal(0, u0_std, (h, w)).astype(np.float32)
+    uy = rng.normal(0, u0_std, (h, w)).astype(np.float32)
+    sc.f_grid = S.equilibrium(np.ones((h, w), np.float32), ux, uy)
+    sc.fluid_velocity = np.zeros((2, h, w), np.float32)
+    return sc
+
+
+def fluidgrid_cases(R):
+    """A fluid lattice different from the domain grid (solver/fluid.py:221-235: IB points
+    at position * (w / H, h / W), lattice velocities, velocity clamp and node reaction
+    scaled; simulate.py:24-29: recorded u* resized to the domain grid)."""
+    from microcosmos_b200 import scenarios as S
+    jnp = sys.modules["jax"].numpy
+    cfg_mod = R["config"]
+    rng = np.random.default_rng(2468)
+    for (H, W, h, w, F, n, ks, seed) in [(24, 24, 48, 48, 2, 10, 4, 41), (32, 32, 24, 24, 2, 12, 2, 42),
+                                         (20, 28, 30, 42, 2, 8, 4, 43)]:
+        sc = _on_lattice(S.make_scenario(H, W, F, n, seed=seed), h, w, rng)
+        nodes, edges, fields = to_ref(R, sc)
+        vel = jnp.array(rng.normal(0, 5.0, size=sc.position.shape).astype(np.float32))
+        nodes = nodes.__replace__(velocity=vel)
+        cfg = baseline_config(cfg_mod, ibm_kernel_size=ks)
+        n2, f2, fnew = R["fluid"].immersed_boundary_interaction(nodes, edges, fields, fields.f_grid, 0.01, cfg)
+        save(f"ib_lat_{H}x{W}_on_{h}x{w}", H=np.int32(H), W=np.int32(W), dt=np.float32(0.01), **cfg_arrays(cfg),
+             **state_arrays("in_", nodes, edges, fields),
+             velocity_out=A(n2.velocity), fluid_velocity_out=A(f2.fluid_velocity), f_grid_out=A(fnew))
+    for (H, W, h, w, seed, name) in [(32, 32, 64, 64, 44, "sim_lat_32_on_64"), (40, 40, 30, 30, 45, "sim_lat_40_on_30")]:
+        sc = _on_lattice(S.make_scenario(H, W, 3, 12, seed=seed, amp=0.2, period=20.0), h, w, rng)
+        nodes, edges, fields = to_ref(R, sc)
+        cfg = baseline_config(cfg_mod)
+        dt, steps = 0.01, 6
+        nts, fts = R["simulate"].simulate(nodes, edges, fields, dt, steps, cfg)
+        nd, ed, fd = nodes, edges, fields
+        traj = []
+        for t in range(steps):
+            ed = ed.__replace__(bending_rest_angles=jnp.array(S.actuation_rest_angles(sc, t)))
+            nd, ed, fd = R["simulate"].step(nd, ed, fd, dt, cfg)
+            traj.append(A(nd.position))
+        save(name, H=np.int32(H), W=np.int32(W), dt=np.float32(dt), steps=np.int32(steps),
+             **cfg_arrays(cfg), **state_arrays("in_", nodes, edges, fields),
+             act_c=sc.act_c, act_amp=sc.act_amp, act_omega=sc.act_omega, act_phase=sc.act_phase,
+             ts_position=A(nts.position), ts_velocity=A(nts.velocity), ts_steric=A(fts.steric),
+             ts_fluid_velocity=A(fts.fluid_velocity),
+             act_position=np.stack(traj), act_velocity=A(nd.velocity), act_theta=A(ed.theta),
+             act_f_grid=A(fd.f_grid), act_steric=A(fd.steric), act_fluid_velocity=A(fd.fluid_velocity))
 
 
 if __name__ == "__main__":

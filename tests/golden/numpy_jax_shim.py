@@ -429,6 +429,8 @@ def _make_jax():
         # changes from m to n, output index o reads input floor((o + 0.5) * m / n), computed
         # in float32.  (The linear method is used only when the fluid grid differs from the
         # domain grid, which the fixtures do not do.)
+        if method == "linear":
+            return _wrap(_resize_linear(np.asarray(x), shape))
         if method != "nearest":
             raise NotImplementedError("jax.image.resize(method=%r) is not restated" % method)
         x = np.asarray(x)
@@ -468,6 +470,32 @@ def _make_jax():
 
     jax.config = types.SimpleNamespace(update=lambda *a, **k: None)
     return jax
+
+
+def _linear_weights(m, n):
+    """JAX's linear resize weights, input m -> output n (antialiased: the triangle kernel
+    is widened by 1/scale when downsampling), float32: (m, n)."""
+    inv = np.float32(1.0 / (n / m))
+    ks = np.maximum(inv, np.float32(1.0))
+    sf = (np.arange(n, dtype=np.float32) + np.float32(0.5)) * inv - np.float32(0.5)
+    x = np.abs(sf[None, :] - np.arange(m, dtype=np.float32)[:, None]) / ks
+    w = np.maximum(np.float32(0.0), np.float32(1.0) - np.abs(x))
+    tot = np.sum(w, axis=0, keepdims=True)
+    w = np.where(np.abs(tot) > np.float32(1000.0 * np.finfo(np.float32).eps), w / np.where(tot != 0, tot, 1), 0)
+    inside = (sf >= -0.5) & (sf <= m - 0.5)
+    return np.where(inside[None, :], w, 0).astype(np.float32)
+
+
+def _resize_linear(x, shape):
+    """jax.image.resize(x, shape, "linear"): every axis whose size changes is contracted
+    with its weight matrix (in axis order; JAX contracts them in one einsum)."""
+    out = x.astype(np.float32)
+    for d, (m, n) in enumerate(zip(x.shape, shape)):
+        if m == n:
+            continue
+        w = _linear_weights(m, n)
+        out = np.moveaxis(np.tensordot(np.moveaxis(out, d, -1), w, axes=([-1], [0])), -1, d).astype(np.float32)
+    return out
 
 
 def install():

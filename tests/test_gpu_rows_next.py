@@ -225,3 +225,81 @@ def test_solver_plugin_mismatch_is_rejected():
     bad = dataclasses.replace(PBD_SCHEME, solver_type="cosserat")
     with pytest.raises(ValueError, match="solver_type"):
         gpu_run([sc], [bad], 1)
+
+
+# ---------------------------------------------------------------- fluid lattice != domain grid
+LATTICE_GOLDEN = ["sim_lat_32_on_64", "sim_lat_40_on_30"]
+
+
+def on_lattice(sc, h, w, seed):
+    """The scenario's fluid on an h x w lattice: feq(1, u0) with u0 ~ N(0, 1e-3)."""
+    rng = np.random.default_rng(seed)
+    ux = rng.normal(0, 1e-3, (h, w)).astype(np.float32)
+    uy = rng.normal(0, 1e-3, (h, w)).astype(np.float32)
+    sc.f_grid = scenarios.equilibrium(np.ones((h, w), np.float32), ux, uy)
+    sc.fluid_velocity = np.zeros((2, h, w), np.float32)
+    return sc
+
+
+@pytest.mark.parametrize("name", LATTICE_GOLDEN)
+def test_lattice_rollout_matches_reference_golden(golden_dir, name):
+    """f_grid on its own lattice (2x finer, 0.75x coarser than grid_shape): the final state of
+    actuated steps and simulate()'s timeseries, whose u* the reference resizes to the domain
+    grid (simulate.py:24-29)."""
+    from microcosmos_b200.simulate import simulate
+    z = np.load(f"{golden_dir}/{name}.npz")
+    cfg = cfg_from(z, base=baseline_config())
+    nodes, edges, fields = containers(z)
+    act = (z["act_c"], z["act_amp"], z["act_omega"], z["act_phase"])
+    n, e, f = run(nodes, edges, fields, float(z["dt"]), int(z["steps"]), cfg, actuation=act)
+    assert tuple(f.f_grid.shape) == z["act_f_grid"].shape
+    assert rel(n.position, z["act_position"][-1]) < TOL
+    assert rel(n.velocity, z["act_velocity"]) < VEL_TOL
+    assert rel(e.theta, z["act_theta"]) < TOL
+    assert rel(f.f_grid, z["act_f_grid"]) < TOL
+    assert rel(f.steric, z["act_steric"]) < TOL
+    assert rel(f.fluid_velocity, z["act_fluid_velocity"]) < 1e-4
+    nts, fts = simulate(nodes, edges, fields, float(z["dt"]), int(z["steps"]), cfg)
+    assert tuple(fts.fluid_velocity.shape[1:]) == (2, int(z["H"]), int(z["W"]))
+    assert rel(nts.position, z["ts_position"]) < TOL
+    assert rel(fts.steric, z["ts_steric"]) < TOL
+    assert rel(fts.fluid_velocity, z["ts_fluid_velocity"]) < 1e-4
+
+
+@pytest.mark.parametrize("H,W,h,w,K", [(32, 32, 48, 48, 4), (24, 40, 36, 60, 2), (48, 40, 24, 20, 4),
+                                       (32, 48, 32, 72, 3)])
+def test_lattice_rollouts_match_oracle(H, W, h, w, K):
+    """Finer, coarser and anisotropic lattices over 20 free-running steps."""
+    sc = on_lattice(scenarios.make_scenario(H, W, 2, 12, seed=H + w, amp=0.25, period=30.0), h, w, seed=H * w)
+    cfg = baseline_config(ibm_kernel_size=K)
+    out, = gpu_run([sc], [cfg], 20)
+    check(out, oracle_run(sc, cfg, 20), ref64=oracle_run(sc, cfg, 20, dtype=np.float64))
+
+
+def test_lattice_recording_matches_the_oracle_resize():
+    """Recorded u* on the domain grid: the kernels' linear resize against the oracle's."""
+    from microcosmos_b200.engine import Record
+    sc = on_lattice(scenarios.make_scenario(40, 40, 2, 12, seed=9), 100, 70, seed=9)
+    cfg = baseline_config()
+    st = DeviceState.from_scenario(sc)
+    plan = Plan.for_states([st], [cfg], [0.01])
+    rec = Record.allocate(st, 4, every=1)
+    plan.rollout([st], 4, actuations=[Actuation.from_scenario(sc)], records=[rec])
+    torch.cuda.synchronize()
+    assert tuple(rec.fluid_velocity.shape) == (4, 2, 40, 40)
+    want = O.resize_linear(st.fluid_velocity.cpu().numpy(), (2, 40, 40))
+    assert rel(rec.fluid_velocity[-1], want) < 1e-6
+    ref = oracle_run(sc, cfg, 4)
+    assert rel(st.f_grid, ref.f_grid) < TOL
+
+
+def test_lattices_in_one_batch_equal_alone():
+    scs = [on_lattice(scenarios.make_scenario(32, 32, 2, 12, seed=1), 64, 64, seed=1),
+           scenarios.make_scenario(48, 40, 2, 16, seed=2),
+           on_lattice(scenarios.make_scenario(40, 40, 1, 12, seed=3), 30, 30, seed=3)]
+    cfgs = [baseline_config()] * 3
+    both = gpu_run(scs, cfgs, 8)
+    for sc, cfg, b in zip(scs, cfgs, both):
+        alone, = gpu_run([sc], [cfg], 8)
+        for k in alone:
+            np.testing.assert_array_equal(b[k], alone[k])

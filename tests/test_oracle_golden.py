@@ -67,7 +67,8 @@ def test_stable_cosserat(golden_dir, name):
 
 
 @pytest.mark.parametrize("name", ["ib_24x24_k4", "ib_24x24_k2", "ib_20x28_k4", "ib_16x16_k4_clamp",
-                                  "ib_syn_24x24_k4", "ib_syn_20x28_k2"])
+                                  "ib_syn_24x24_k4", "ib_syn_20x28_k2", "ib_lat_24x24_on_48x48",
+                                  "ib_lat_32x32_on_24x24", "ib_lat_20x28_on_30x42"])
 def test_ib_lbm(golden_dir, name):
     z = load(golden_dir, name)
     H, W = int(z["H"]), int(z["W"])
@@ -84,7 +85,7 @@ def _state(z):
     return O.State(H=int(z["H"]), W=int(z["W"]), **{k[3:]: z[k] for k in z.files if k.startswith("in_")})
 
 
-@pytest.mark.parametrize("name", ["sim_24x32", "sim_32x32"])
+@pytest.mark.parametrize("name", ["sim_24x32", "sim_32x32", "sim_lat_32_on_64", "sim_lat_40_on_30"])
 def test_simulate_timeseries(golden_dir, name):
     z = load(golden_dir, name)
     cfg = O.config_from_npz(z)
@@ -96,7 +97,7 @@ def test_simulate_timeseries(golden_dir, name):
 
 
 @pytest.mark.parametrize("name", ["sim_24x32", "sim_32x32", "sim_cosserat_nofluid_24x32",
-                                  "sim_cosserat_fluid_32x32", "sim_syn_32x32"])
+                                  "sim_cosserat_fluid_32x32", "sim_syn_32x32", "sim_lat_32_on_64", "sim_lat_40_on_30"])
 def test_actuated_steps(golden_dir, name):
     z = load(golden_dir, name)
     cfg = O.config_from_npz(z)
