@@ -281,16 +281,16 @@ def serve_section(args):
     rollouts with grid side ~U{64..1024} step 64, filaments ~U{1..128}, nodes/filament
     ~U{16..128}, steps ~U{500..5000}, 20% marked as asking for gradients, served by the
     continuous-batching server (admission by a 180 GB budget, up to 16 rollouts in flight,
-    200-step graph-replayed chunks, one stream per rollout; 16 slots measured best among
-    16-64: fewer streams contend less for the GPU's hardware queues and finish requests
-    sooner).  Latency = completion minus
+    200-step graph-replayed chunks, one stream per rollout, up to 8 gradient jobs at once;
+    16 slots and 8 gradient workers measured best among 16-64 slots and 2-16 workers).
+    Latency = completion minus
     arrival, wall clock.  The plain path runs a sample of the same requests one after
     another, one plan each."""
     import torch
     from microcosmos_b200 import baseline_config, serve
     cfg = baseline_config()
     reqs = serve.poisson_requests(args.serve_requests, args.serve_rate, seed=0)
-    be = serve.CudaBackend(cfg, dt=0.01)
+    be = serve.CudaBackend(cfg, dt=0.01, grad_workers=8)
     # warm the allocator and the module (one tiny request); not part of the measurement
     serve.run_plain(be, serve.poisson_requests(1, 1.0, seed=99, sides=(64,), filaments=(1, 1), nodes=(16, 16),
                                                steps=(8, 8)))

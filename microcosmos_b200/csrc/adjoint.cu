@@ -482,7 +482,10 @@ __global__ void k_ib_spread(AD d) {
 // ------------------------------------------------------------------ adjoint: stream + collide + F
 __constant__ float kW9[9] = {4.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f,
                              1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f};
-__constant__ int kOpp[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+// opposite D2Q9 direction {0, 3, 4, 1, 2, 7, 8, 5, 6} as a compile-time function: in the
+// unrolled population loops the index folds to a constant and the per-cell arrays stay in
+// registers (a table lookup would put them in local memory)
+__device__ __forceinline__ constexpr int opp9(int i) { return i == 0 ? 0 : (i <= 4 ? (i + 1) % 4 + 1 : (i - 3) % 4 + 5); }
 
 __global__ void k_lbm_adj1(AD d) {
   const StepArgs a = d.sa[*d.jp];
@@ -525,7 +528,7 @@ __global__ void k_lbm_adj1(AD d) {
   float g[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
-    const int o = kOpp[i];
+    const int o = opp9(i);
     const float pr = f0[i] - d.wp * (half * (f0[i] + f0[o]) - half * (feq[i] + feq[o])) -
                      d.wm * (half * (f0[i] - f0[o]) - half * (feq[i] - feq[o]));
     const float src = d.cp * (half * (raw[i] + raw[o])) + d.cm * (half * (raw[i] - raw[o]));
@@ -537,7 +540,7 @@ __global__ void k_lbm_adj1(AD d) {
   float lrho = 0.0f, lusx = 0.0f, lusy = 0.0f, lFx = 0.0f, lFy = 0.0f;
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
-    const int o = kOpp[i];
+    const int o = opp9(i);
     const float gp = half * (g[i] + g[o]), gm = half * (g[i] - g[o]);
     lf0[i] = g[i] - d.wp * gp - d.wm * gm;
     const float lfeq = d.wp * gp + d.wm * gm;

