@@ -723,10 +723,12 @@ int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
                          p->bin_threads);
   });
   ++k;
-  if (p->use_coop) {
+  if (p->use_coop && p->grid[K_NODES]) {
     timed(p, 16, s, capture, [&] { p->coop_err = mc::launch_ib_coop(L(p, K_IBCOOP, s), parity); });
     return k + 1;
   }
+  // rollouts without nodes have no IB points: nothing to launch when no rollout has any
+  if (!p->grid[K_NODES] || !p->grid[K_IB]) return k;
   for (int it = 0; it < p->max_iters; ++it) {
     timed(p, 7, s, capture, [&] { mc::launch_ib_interp(L(p, K_NODES, s), it); });
     timed(p, 8, s, capture, [&] { mc::launch_ib_spread(L(p, K_IB, s), it); });
@@ -1394,7 +1396,7 @@ mc_status mc_rollout_begin(mc_plan* p, const mc_state* states, const mc_actuatio
   for (int i = 0; i < p->n; ++i) {
     const mc_state& st = states[i];
     const HostRollout& h = p->R[i];
-    if (!st.position || !st.velocity || (h.dims.E && (!st.theta || !st.rest_lengths)) ||
+    if ((h.dims.N && (!st.position || !st.velocity)) || (h.dims.E && (!st.theta || !st.rest_lengths)) ||
         (h.dims.B && (!st.bending_rest_angles || !st.bending_stiffness)) ||
         (h.cfg.enable_fluid && (!st.f_grid || !st.fluid_velocity)) || (h.cfg.enable_steric && !st.steric))
       return fail(MC_ERR_INVALID, "rollout " + std::to_string(i) + ": null state array");

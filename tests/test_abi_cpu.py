@@ -187,3 +187,28 @@ def test_tile_kernel_threads_setter(lib):
     assert lib.mc_plan_set_bin_sort_capacity(h, 512) == _lib.MC_OK and lib.mc_plan_bin_sort_capacity(h) == 512
     assert lib.mc_plan_set_bin_sort_capacity(h, 300) == _lib.MC_ERR_INVALID
     lib.mc_plan_destroy(h)
+
+
+def test_plan_limits(lib):
+    """Sort keys hold 24-bit contribution indices: N * K^2 >= 2^24 IB contributions are
+    refused (synthetic pairs double them); a lattice more than 7x the domain grid is refused."""
+    import dataclasses
+    N = 1 << 20
+    empty = np.zeros((0, 2), np.int32)
+    st, _ = _create([(4096, 4096, N, empty, empty, baseline_config(), 0.01)])
+    assert st == _lib.MC_ERR_UNSUPPORTED and b"24-bit" in lib.mc_last_error()
+    st, h = _create([(4096, 4096, N // 2 - 1, empty, empty, baseline_config(), 0.01)])
+    assert st == _lib.MC_OK
+    lib.mc_plan_destroy(h)
+    st, _ = _create([(4096, 4096, N // 2, empty, empty, baseline_config(synthetic_node_width=1.0), 0.01)])
+    assert st == _lib.MC_ERR_UNSUPPORTED
+    from microcosmos_b200.engine import mc_config
+    dims = _lib.McDims(32, 32, 0, 0, 0, 32 * 8, 32)
+    cfg = (_lib.McConfig * 1)(mc_config(baseline_config()))
+    h = ctypes.c_void_p()
+    dt = (ctypes.c_float * 1)(0.01)
+    nul = (_lib.c_int_p * 1)()
+    assert lib.mc_plan_create(1, ctypes.byref(dims), cfg, dt, nul, nul, ctypes.byref(h)) == _lib.MC_ERR_INVALID
+    dims = _lib.McDims(32, 32, 0, 0, 0, 64, 96)
+    assert lib.mc_plan_create(1, ctypes.byref(dims), cfg, dt, nul, nul, ctypes.byref(h)) == _lib.MC_OK
+    lib.mc_plan_destroy(h)
