@@ -34,11 +34,11 @@ class BatchedState:
 
     @property
     def time(self):
-        return torch.stack([s.time for s in self.states])
+        return self._owner._time
 
     @property
     def energy_center(self):
-        return torch.stack([s.energy_center for s in self.states])
+        return self._owner._centers
 
 
 class BatchedEnv:
@@ -61,14 +61,19 @@ class BatchedEnv:
         if len(keys) != B:
             raise ValueError(f"{len(keys)} keys for a batch of {B}")
         env = self.env
-        states = []
+        inits, centers = [], []
         for k in keys:
             rng = _rng(k)
-            init = env._init_state(rng)
+            inits.append(env._init_state(rng))
+            centers.append(env._sample_energy_center(rng))
+        # one counter array and one centre array for the batch; each state holds views of them
+        self._time = torch.zeros(B, dtype=torch.int32, device=self.device)
+        self._centers = torch.as_tensor(np.stack(centers).astype(np.float32), device=self.device)
+        states = []
+        for i, init in enumerate(inits):
             dev = env._device_state(init, self.device)
-            states.append(EnvState(dev, torch.zeros((), dtype=torch.int32, device=self.device),
-                                   torch.as_tensor(env._sample_energy_center(rng), dtype=_F32, device=self.device),
-                                   dev.rest_lengths.clone(), dev.bending_rest_angles.clone(), np.arange(dev.N) % 3))
+            states.append(EnvState(dev, self._time[i], self._centers[i], dev.rest_lengths.clone(),
+                                   dev.bending_rest_angles.clone(), np.arange(dev.N) % 3))
         d0 = states[0].device
         if self._plan is None:
             self._plan = Plan.for_states([s.device for s in states], [env.solver_config] * B, [env.dt] * B)
@@ -111,7 +116,7 @@ class BatchedEnv:
         self._plan.advance(1, last=True)
         self._observe(advance=True)
         out = self._table["out"]
-        info = {"steps": state.time, "energy_center": state.energy_center}
+        info = {"steps": state.time.clone(), "energy_center": state.energy_center.clone()}
         return out["obs"].clone(), state, out["reward"].clone(), out["done"].bool(), info
 
     def fitness_per_creature(self, state: BatchedState):

@@ -10,6 +10,7 @@ Workloads (seeded synthetic inputs):
   batch  a population of uneven rollouts (side U{128..512}, 1-32 filaments x 16-128 nodes)
          as one plan with the library's default launch shapes
   grad   the 256x256, 8 x 48 differentiation workload: forward with checkpoints + backward
+  gym    --rollouts LineEnv environments (128x128, 16 nodes) stepped together by BatchedEnv
 Steps are launched directly (no CUDA graph) unless --graph is given, so that every kernel
 launch is visible to a profiler.
 """
@@ -20,7 +21,7 @@ import argparse
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="scale", choices=["scale", "small", "batch", "grad"])
+    ap.add_argument("--workload", default="scale", choices=["scale", "small", "batch", "grad", "gym"])
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--rollouts", type=int, default=64)
@@ -43,6 +44,20 @@ def main(argv=None):
         g = plan.backward(seed)
         torch.cuda.synchronize()
         print("grad ok", float(g["act_amp"].norm()))
+        return
+    if a.workload == "gym":
+        from .gym import BatchedEnv, LineEnv
+        env = LineEnv(energy_amplitude=1.0, max_steps=10 ** 9)
+        benv = BatchedEnv(env, a.rollouts)
+        _, st = benv.reset(list(range(a.rollouts)))
+        g = torch.Generator(device="cuda").manual_seed(0)
+        for _ in range(a.warmup + a.steps):
+            act = {"d_rest_length": 0.1 * torch.randn((a.rollouts, env.num_edges), generator=g, device="cuda"),
+                   "d_bending_angle": 0.2 * torch.randn((a.rollouts, env.num_bending_pairs), generator=g,
+                                                        device="cuda")}
+            obs, st, rew, done, _ = benv.step(None, st, act)
+        torch.cuda.synchronize()
+        print("gym ok", a.rollouts, "environments, mean reward", float(rew.mean()))
         return
     if a.workload == "batch":
         scs = scenarios.config_batch(a.rollouts, seed=0)
