@@ -161,7 +161,7 @@ class Environment:
         plan = self._get_plan(new.device)
         acts = [_action_tensors(action, new.device)]
         noise = [self._noise(key, new.device)]
-        table = self._table([new], acts, noise, advance=True)
+        table = self._table([new], acts, noise)
         stream = torch.cuda.current_stream().cuda_stream
         lib = _lib.load()
         _lib.check(lib.mc_env_act(ctypes.c_void_p(table["ptr"]), 1, ctypes.c_void_p(stream)))
@@ -195,7 +195,7 @@ class Environment:
             self._seg_dev = torch.as_tensor(np.asarray(seg, np.int32), device=device)
         return self._seg_dev
 
-    def _table(self, states, actions, noises, advance=True, outputs=None):
+    def _table(self, states, actions, noises):
         """mc_env structs for ``states`` uploaded into a fresh device table; the output
         tensors live in the returned dict (and keep the table's pointers valid)."""
         n = len(states)
@@ -204,10 +204,10 @@ class Environment:
         N = dev0.N
         seg = self._segment_offsets(device)
         nseg = 1 if seg is None else int(seg.numel()) - 1
-        out = outputs or {"obs": torch.empty((n, 5 * N), dtype=_F32, device=device),
-                          "reward": torch.empty(n, dtype=_F32, device=device),
-                          "done": torch.zeros(n, dtype=torch.int32, device=device),
-                          "fitness": torch.empty((n, nseg), dtype=_F32, device=device)}
+        out = {"obs": torch.empty((n, 5 * N), dtype=_F32, device=device),
+               "reward": torch.empty(n, dtype=_F32, device=device),
+               "done": torch.zeros(n, dtype=torch.int32, device=device),
+               "fitness": torch.empty((n, nseg), dtype=_F32, device=device)}
         lib = _lib.load()
         envs = (_lib.McEnv * n)()
         keep = [out]
@@ -249,7 +249,7 @@ class Environment:
     def _observe(self, states, advance):
         """Observation / reward / done / per-creature fitness of ``states`` without a step;
         with ``advance`` the energy source walks and the step counter advances."""
-        t = self._table(states, [None] * len(states), [None] * len(states), advance)
+        t = self._table(states, [None] * len(states), [None] * len(states))
         stream = torch.cuda.current_stream().cuda_stream
         _lib.check(_lib.load().mc_env_observe(ctypes.c_void_p(t["ptr"]), len(states), int(bool(advance)),
                                               ctypes.c_void_p(stream)))
