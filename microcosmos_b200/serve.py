@@ -84,7 +84,8 @@ class CudaBackend:
         lib = _lib.load()
         pairs = np.ascontiguousarray(sc.pairs, np.int32).reshape(-1, 2)
         bp = np.ascontiguousarray(sc.bending_pairs, np.int32).reshape(-1, 2)
-        dims = _lib.McDims(sc.H, sc.W, sc.position.shape[0], pairs.shape[0], bp.shape[0])
+        fh, fw = (int(v) for v in np.shape(sc.f_grid)[-2:])  # the fluid lattice (may differ from H, W)
+        dims = _lib.McDims(sc.H, sc.W, sc.position.shape[0], pairs.shape[0], bp.shape[0], fh, fw)
         cfg = mc_config(self.cfg)
         h = ctypes.c_void_p()
         if req.want_grad:
@@ -106,7 +107,7 @@ class CudaBackend:
             finally:
                 lib.mc_plan_destroy(h)
         N = sc.position.shape[0]
-        state = 4 * (12 * sc.H * sc.W + 8 * N + 4 * bp.shape[0]) + 256
+        state = 4 * (11 * fh * fw + sc.H * sc.W + 8 * N + 4 * bp.shape[0]) + 256
         return ws + state
 
     def _grad_job(self, req: Request):
