@@ -116,7 +116,7 @@ def save(name, **arrs):
     print("wrote", path, sum(v.nbytes for v in arrs.values()), "bytes")
 
 
-GROUPS = ("base", "cosserat", "synthetic", "gym", "render", "fluidgrid")
+GROUPS = ("base", "cosserat", "synthetic", "gym", "render", "fluidgrid", "worm")
 
 
 def main(ref_root, groups=GROUPS):
@@ -133,6 +133,8 @@ def main(ref_root, groups=GROUPS):
         render_cases(R)
     if "fluidgrid" in groups:
         fluidgrid_cases(R)
+    if "worm" in groups:
+        worm_case(R)
 
 
 def base_cases(R):
@@ -465,6 +467,48 @@ def fluidgrid_cases(R):
              ts_fluid_velocity=A(fts.fluid_velocity),
              act_position=np.stack(traj), act_velocity=A(nd.velocity), act_theta=A(ed.theta),
              act_f_grid=A(fd.f_grid), act_steric=A(fd.steric), act_fluid_velocity=A(fd.fluid_velocity))
+
+
+def worm_case(R):
+    """The swimmer of the reference's end-to-end test (tests/test_worm.py): 20 nodes on a
+    sine wave over a 50x50 grid, rest angles from a phase advancing 0.1 rad per step, 200
+    steps of step() under PBD_SCHEME; the state after 50 and after 200 steps."""
+    jnp = sys.modules["jax"].numpy
+    G, U = R["graph"], R["utils"]
+    n, H, W = 20, 50, 50
+    pairs, dep = G.make_edges(n, graph="line", num_instances=1)
+    bp, _ = G.compute_bending_pairs(pairs, dep, n)
+    xs = jnp.linspace(W * 0.1, W * 0.9, n)
+    amp = H * 0.3
+    k = 2 * jnp.pi * 2 / (xs[-1] - xs[0])
+    pos = jnp.stack([xs, H / 2 + amp * jnp.sin(k * xs)], axis=1)
+    d = U.displacement((H, W), pos[pairs[:, 1]], pos[pairs[:, 0]])
+
+    def rest(phase):
+        tt = jnp.arctan(amp * k * jnp.cos(k * xs + phase))
+        return tt[1:-1] - tt[:-2]
+
+    nodes = R["Nodes"](position=pos, velocity=jnp.zeros_like(pos), color_bend=jnp.arange(n) % 3,
+                       debug_vector=jnp.zeros((n, 2)))
+    edges = R["Edges"](pairs=pairs, theta=jnp.arctan2(d[:, 1], d[:, 0]), rest_lengths=jnp.full(n - 1, 2.0),
+                       bending_pairs=bp, bending_rest_angles=rest(0.0), bending_stiffness=jnp.ones(n - 2) * 0.5)
+    w9 = jnp.array([4 / 9, 1 / 9, 1 / 9, 1 / 9, 1 / 9, 1 / 36, 1 / 36, 1 / 36, 1 / 36])
+    fields = R["Fields"](grid_shape=(H, W), steric=jnp.zeros((H, W)), fluid_velocity=jnp.zeros((2, H, W)),
+                         f_grid=jnp.zeros((9, H, W)).at[:].set(w9[:, None, None]))
+    out = dict(H=np.int32(H), W=np.int32(W), **state_arrays("in_", nodes, edges, fields))
+    rests = []
+    phase = 0.0
+    for t in range(200):
+        ra = rest(phase)
+        rests.append(A(ra))
+        edges = edges.__replace__(bending_rest_angles=ra)
+        nodes, edges, fields = R["simulate"].step(nodes, edges, fields, 0.01, R["config"].PBD_SCHEME)
+        if t == 49:
+            out["pos_50"] = A(nodes.position)
+        phase += 0.1
+    out.update(rest_angles=np.stack(rests), pos_200=A(nodes.position), vel_200=A(nodes.velocity),
+               f_grid_200=A(fields.f_grid))
+    save("worm_50x50", **out)
 
 
 if __name__ == "__main__":

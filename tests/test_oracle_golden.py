@@ -138,3 +138,21 @@ def test_reference_property_gaussian_filter():
     assert np.argmax(g) == 55
     np.testing.assert_allclose(g[5, 4], g[5, 6], rtol=1e-6)
     np.testing.assert_allclose(g[4, 5], g[6, 5], rtol=1e-6)
+
+
+def test_reference_worm_run(golden_dir):
+    """The reference's end-to-end swimmer (its tests/test_worm.py scenario): 200 steps with
+    the rest angles rewritten before each step; the reference asserts a centre-of-mass
+    displacement in (0.2, 50)."""
+    z = load(golden_dir, "worm_50x50")
+    from microcosmos_b200 import PBD_SCHEME
+    import dataclasses
+    cfg = O.Config(**{f.name: getattr(PBD_SCHEME, f.name) for f in dataclasses.fields(O.Config)})
+    s = _state(z)
+    for t in range(200):
+        s = O.step(s, cfg, 0.01, rest_angles=z["rest_angles"][t])
+        if t == 49:
+            np.testing.assert_array_equal(s.position, z["pos_50"])
+    assert O.rel_l2(s.position, z["pos_200"]) < 1e-6
+    d = abs(float(z["in_position"][:, 0].mean()) - float(s.position[:, 0].mean()))
+    assert 0.2 < d < 50
