@@ -139,8 +139,9 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
 void mc_plan_destroy(mc_plan* plan);
 
 /* Tile shape of the dense stream+collide pass: each CTA covers 32 * cells_per_lane columns
- * (1, 2 or 4 cells per thread, vector loads and stores; it must divide every rollout's W)
- * by rows_per_cta rows (2, 4 or 8).  0 keeps the current value.  Results do not depend on
+ * (1, 2 or 4 cells per thread, vector loads and stores; it must divide every rollout's
+ * lattice width) by rows_per_cta rows (2, 4 or 8); the default is 2 cells per lane (1 for an
+ * odd width) by 2 rows.  0 keeps the current value.  Results do not depend on
  * the shape.  Only before mc_plan_bind(); microcosmos_b200.autotune picks it by timing.
  * No counterpart in the reference (XLA chooses its own fusion tiling). */
 mc_status mc_plan_set_lbm_shape(mc_plan* plan, int32_t cells_per_lane, int32_t rows_per_cta);
@@ -169,7 +170,7 @@ mc_status mc_plan_set_fft_values_per_thread(mc_plan* plan, int32_t values);
 int32_t mc_plan_fft_values_per_thread(const mc_plan* plan);
 
 /* Threads per CTA of the tile kernel that sorts the IB and cloud-in-cell contributions of
- * each touched 16 x 16 tile (64, 128 or 256; 0 = 256).  Sparse tiles favour small CTAs.
+ * each touched 16 x 16 tile (64, 128 or 256; 0 = 128).  Sparse tiles favour small CTAs.
  * Results do not depend on it.  Only before mc_plan_bind().  No counterpart in the
  * reference. */
 mc_status mc_plan_set_bin_threads(mc_plan* plan, int32_t threads);

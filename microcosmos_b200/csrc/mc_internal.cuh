@@ -17,7 +17,7 @@ namespace mc {
 
 constexpr int kBinTile = 16;       // binning tile edge for the deterministic reductions
 constexpr int kLbmTileX = 128;     // dense LBM CTA tile: 32 lanes x 4 cells
-constexpr int kLbmTileY = 8;      // default LBM tile height (rows per CTA)
+constexpr int kLbmTileY = 2;      // default LBM tile height (rows per CTA): 64 threads, the most CTAs to spread
 constexpr int kLbmMinTileY = 2;   // smallest tile height a plan may be tuned to
 constexpr int kConvTile = 32;     // steric direct convolution: 32 x 32 outputs per CTA
 constexpr int kConvMaxR = 24;     // largest tap radius of the direct convolution       //                    8 rows

@@ -99,7 +99,7 @@ struct mc_plan {
   Region r_desc, r_tdev, r_wl_ib, r_wl_cic, r_wl_ctl;
   int tile_grid = 1;  // CTAs walking the tile lists
   long long n_tiles = 0;  // bin tiles of all rollouts
-  int bin_threads = 256;  // threads per CTA of the tile kernel
+  int bin_threads = 128;  // threads per CTA of the tile kernel
   int ib_capS = 0, c_capS = 0;  // largest bin capacity of the plan
   int ib_smem = 0, c_smem = 0;  // contributions a tile may hold to be sorted in shared memory
   Region r_off[K_COUNT];
@@ -1199,7 +1199,7 @@ mc_status mc_plan_set_bin_threads(mc_plan* p, int32_t threads) {
   if (p->bound) return fail(MC_ERR_INVALID, "the tile kernel shape is set before mc_plan_bind()");
   if (threads != 0 && threads != 64 && threads != 128 && threads != 256)
     return fail(MC_ERR_INVALID, "threads must be 0 (default), 64, 128 or 256");
-  p->bin_threads = threads ? threads : 256;
+  p->bin_threads = threads ? threads : 128;
   p->tile_grid = (int)std::max(1LL, std::min(p->n_tiles, 148LL * 8 * (256 / p->bin_threads)));
   return MC_OK;
 }

@@ -223,7 +223,7 @@ class Plan:
         ``steric_method``: 0 = per rollout (direct convolution where it applies, else
         FFT), 1 = FFT, 2 = direct convolution.  ``fft_values``: values per thread of the
         power-of-two FFT kernels (4, 8, 16; 0 = the library's choice).  ``bin_threads``:
-        threads per CTA of the contribution-sorting tile kernel (64, 128, 256; 0 = 256).
+        threads per CTA of the contribution-sorting tile kernel (64, 128, 256; 0 = 128).
         ``bin_sort_capacity``: contributions per tile sorted in shared memory (0 = 1024)."""
         _require_cuda()
         lib = _lib.load()

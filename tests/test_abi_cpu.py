@@ -147,7 +147,7 @@ def test_lbm_shape_setter_validates_and_reports(lib):
     assert st == _lib.MC_OK
     a, b = ctypes.c_int32(), ctypes.c_int32()
     assert lib.mc_plan_get_lbm_shape(h, ctypes.byref(a), ctypes.byref(b)) == _lib.MC_OK
-    assert (a.value, b.value) == (2, 8)  # the library's default
+    assert (a.value, b.value) == (2, 2)  # the library's default
     assert lib.mc_plan_set_lbm_shape(h, 4, 2) == _lib.MC_OK
     lib.mc_plan_get_lbm_shape(h, ctypes.byref(a), ctypes.byref(b))
     assert (a.value, b.value) == (4, 2)
@@ -178,7 +178,7 @@ def test_tile_kernel_threads_setter(lib):
     sc = scenarios.make_scenario(64, 64, 2, 12, seed=0)
     st, h = _create([(64, 64, sc.N, sc.pairs, sc.bending_pairs, baseline_config(), 0.01)])
     assert st == _lib.MC_OK
-    assert lib.mc_plan_bin_threads(h) == 256
+    assert lib.mc_plan_bin_threads(h) == 128
     assert lib.mc_plan_set_bin_threads(h, 128) == _lib.MC_OK and lib.mc_plan_bin_threads(h) == 128
     assert lib.mc_plan_set_bin_threads(h, 96) == _lib.MC_ERR_INVALID
     assert lib.mc_plan_set_fft_values_per_thread(h, 8) == _lib.MC_OK and lib.mc_plan_fft_values_per_thread(h) == 8
