@@ -303,3 +303,12 @@ def test_lattices_in_one_batch_equal_alone():
         alone, = gpu_run([sc], [cfg], 8)
         for k in alone:
             np.testing.assert_array_equal(b[k], alone[k])
+
+
+def test_lattice_with_synthetic_pairs_and_cosserat_matches_oracle():
+    """All three variants at once: the Cosserat solver, synthetic pairs (their offset scaled
+    by the mean lattice/domain ratio) and a 1.5x lattice."""
+    sc = on_lattice(scenarios.make_scenario(32, 32, 2, 14, seed=21, amp=0.25, period=30.0), 48, 48, seed=21)
+    cfg = cosserat_cfg(synthetic_node_width=0.75)
+    out, = gpu_run([sc], [cfg], 20)
+    check(out, oracle_run(sc, cfg, 20), ref64=oracle_run(sc, cfg, 20, dtype=np.float64))
