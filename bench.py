@@ -635,7 +635,7 @@ def main():
         out = {
             "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": ws, "steps": K, "warmup": args.warmup,
             "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded numpy.random, BASELINE config shapes)",
+            "dtype": "f32", "data": "synthetic (seeded numpy.random, the benchmark configurations' shapes)",
             "config": dict(cfgj, l2="flushed (256 MiB write) before every timed step; each step timed alone with "
                                     "CUDA events", parallelism=f"replicas x{ws}", dt=0.01,
                            timed="device-resident: one graph-launched simulate.step per event pair"),

@@ -5,7 +5,7 @@ Tolerances (float32 everywhere):
   * golden vectors / oracle after <= 20 steps: rel-L2 <= 1e-5 (the kernels round every
     elementwise op like the reference; remaining differences are the transcendental
     implementations, the FFT, and the reference's own summation order);
-  * BASELINE small configuration (128^2, 4 x 32 nodes): rel-L2 <= 1e-5 after 100 steps,
+  * the small benchmark configuration (128^2, 4 x 32 nodes): rel-L2 <= 1e-5 after 100 steps,
     <= 1e-3 after 1000 steps (chaotic growth of ulp-level differences);
   * node velocity = (x - x_prev) / dt is a difference of nearly equal positions (|x| ~ grid
     size, |x - x_prev| ~ 1e-2), so position differences of a few ulp appear amplified by
