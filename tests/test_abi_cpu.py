@@ -212,3 +212,21 @@ def test_plan_limits(lib):
     dims = _lib.McDims(32, 32, 0, 0, 0, 64, 96)
     assert lib.mc_plan_create(1, ctypes.byref(dims), cfg, dt, nul, nul, ctypes.byref(h)) == _lib.MC_OK
     lib.mc_plan_destroy(h)
+
+
+def test_env_and_render_entry_points_validate_on_the_host(lib):
+    """The gym and frame entry points reject bad tables / sizes before touching a device."""
+    env = (_lib.McEnv * 1)()
+    dummy = ctypes.c_void_p(256)
+    assert lib.mc_env_table_bytes(3) == 3 * ctypes.sizeof(_lib.McEnv)
+    assert lib.mc_env_table_upload(env, 0, dummy, None) == _lib.MC_ERR_INVALID
+    assert lib.mc_env_table_upload(env, 1, dummy, None) == _lib.MC_ERR_INVALID  # N = 0
+    env[0].N, env[0].E, env[0].B, env[0].H, env[0].W = 4, 3, 2, 16, 16
+    assert lib.mc_env_table_upload(env, 1, dummy, None) == _lib.MC_ERR_INVALID  # null buffers
+    assert b"null" in lib.mc_last_error()
+    assert lib.mc_env_act(None, 1, None) == _lib.MC_ERR_INVALID
+    assert lib.mc_env_observe(None, 1, 1, None) == _lib.MC_ERR_INVALID
+    assert lib.mc_render_scratch_bytes(2, 8, 10) == 2 * 8 * 10 * 4
+    assert lib.mc_render_frames(None, None, None, None, 0, 1, 8, 8, 16, 1, 0, None, None, None) == _lib.MC_ERR_INVALID
+    assert lib.mc_render_frames(None, None, None, dummy, 1, 4, 8, 8, 16, 1, 0, None, dummy, None) == _lib.MC_ERR_INVALID
+    assert lib.mc_render_frames(None, None, None, dummy, 1, 0, 8, 100, 1, 0, 0, None, dummy, None) == _lib.MC_ERR_INVALID
