@@ -24,6 +24,12 @@
 #include "lbm_cell.cuh"
 #include "mc_internal.cuh"
 
+namespace mc {
+// Inside a rollout of a one-rollout plan: the current populations in fields.f_grid layout
+// written to dst, the rollout left as it is (runtime.cu).
+mc_status rollout_snapshot_f(mc_plan* p, float* dst, cudaStream_t s);
+}  // namespace mc
+
 namespace {
 
 constexpr int kMaxKK = 64;       // stencil entries per node (kernel size <= 8)
@@ -983,6 +989,27 @@ mc_state working_state(mc_grad_plan* p) {
   return w;
 }
 
+// Open a rollout of the forward plan on the working state, actuated from step t0 (the
+// static rest angles restored first when there is no actuation).
+mc_status begin_fwd(mc_grad_plan* p, int t0, cudaStream_t s) {
+  mc_state w = working_state(p);
+  mc_actuation a{};
+  const mc_actuation* ap = nullptr;
+  if (p->has_act) {
+    a.c = at<float>(p->ws, p->r_ac);
+    a.amp = at<float>(p->ws, p->r_aa);
+    a.omega = at<float>(p->ws, p->r_ao);
+    a.phase = at<float>(p->ws, p->r_ap);
+    a.t0 = t0;
+    ap = &a;
+  } else if (p->dims.B) {
+    GC(cudaMemcpyAsync(w.bending_rest_angles, at<float>(p->ws, p->r_rst), (size_t)p->dims.B * 4,
+                       cudaMemcpyDeviceToDevice, s));
+  }
+  const mc_actuation* const acts[1] = {ap};
+  return mc_rollout_begin(p->fwd, &w, acts, nullptr, s);
+}
+
 mc_status run_fwd(mc_grad_plan* p, int steps, int t0, cudaStream_t s) {
   mc_state w = working_state(p);
   mc_actuation a{};
@@ -1520,16 +1547,28 @@ mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_st
     mc_status st = copy_state_to(p, at<float>(w, p->r_wpos), at<float>(w, p->r_wvel), at<float>(w, p->r_wth),
                                  at<float>(w, p->r_wf), ck.pos, ck.vel, ck.th, ck.f, s);
     if (st != MC_OK) return st;
+    // the segment's step inputs: one rollout over the segment, the populations of every
+    // step's input snapshot from the open rollout (no per-step entry/exit conversion)
+    st = begin_fwd(p, t0, s);
+    if (st != MC_OK) return st;
     for (int j = 0; j < len; ++j) {
       Slot sj = slot(p, p->r_seg, j);
-      st = copy_state_to(p, sj.pos, sj.vel, sj.th, sj.f, at<float>(w, p->r_wpos), at<float>(w, p->r_wvel),
-                         at<float>(w, p->r_wth), at<float>(w, p->r_wf), s);
-      if (st != MC_OK) return st;
-      st = run_fwd(p, 1, t0 + j, s);
+      GC(cudaMemcpyAsync(sj.pos, at<float>(w, p->r_wpos), (size_t)D.N * 8, cudaMemcpyDeviceToDevice, s));
+      GC(cudaMemcpyAsync(sj.vel, at<float>(w, p->r_wvel), (size_t)D.N * 8, cudaMemcpyDeviceToDevice, s));
+      if (D.E) GC(cudaMemcpyAsync(sj.th, at<float>(w, p->r_wth), (size_t)D.E * 4, cudaMemcpyDeviceToDevice, s));
+      if (d.fluid) {
+        st = mc::rollout_snapshot_f(p->fwd, sj.f, s);
+        if (st != MC_OK) return st;
+      } else {
+        GC(cudaMemcpyAsync(sj.f, at<float>(w, p->r_wf), 9 * HW * 4, cudaMemcpyDeviceToDevice, s));
+      }
+      st = mc_rollout_advance(p->fwd, 1, 1, 1, s);
       if (st != MC_OK) return st;
       GC(cudaMemcpyAsync(w + p->r_segV.off + (size_t)j * al(HW * 4), w + p->r_wst.off, HW * 4,
                          cudaMemcpyDeviceToDevice, s));
     }
+    st = mc_rollout_end(p->fwd, s);
+    if (st != MC_OK) return st;
     // per-step inputs of the segment (the cotangent of f alternates between two buffers)
     p->sargs.assign(len, StepArgs{});
     for (int j = len - 1; j >= 0; --j) {

@@ -174,7 +174,8 @@ __global__ void k_unstream(const RDesc* __restrict__ D, const int* __restrict__ 
 
 // fields.f_grid_i(y, x) = max(h_i((y - cy) % H, (x - cx) % W), EPSIL): the push streaming
 // of the reference (fluid.py:352-357) applied to the final post-collision state.
-__global__ void k_stream_out(const RDesc* __restrict__ D, const int* __restrict__ off, int n, int parity) {
+__global__ void k_stream_out(const RDesc* __restrict__ D, const int* __restrict__ off, int n, int parity,
+                             float* __restrict__ dst) {
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int lb = blockIdx.x - off[r];
@@ -182,12 +183,13 @@ __global__ void k_stream_out(const RDesc* __restrict__ D, const int* __restrict_
   const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
   const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
   const float* h = d.h[parity];
+  float* out = dst ? dst : d.f_grid;  // dst: a snapshot buffer of a one-rollout plan
   for (size_t idx = (size_t)lb * blockDim.x + threadIdx.x; idx < HW; idx += (size_t)(off[r + 1] - off[r]) * blockDim.x) {
     int y = (int)(idx / d.lW), x = (int)(idx % d.lW);
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
       int ys = imod_floor(y - ey[i], d.lH), xs = imod_floor(x - ex[i], d.lW);
-      d.f_grid[i * HW + idx] = max_prop(h[i * HW + (size_t)ys * d.lW + xs], MC_EPSIL);
+      out[i * HW + idx] = max_prop(h[i * HW + (size_t)ys * d.lW + xs], MC_EPSIL);
     }
   }
 }
@@ -225,7 +227,9 @@ void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows) {
 }
 
 void launch_unstream(const Launch& L) { k_unstream<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
-void launch_stream_out(const Launch& L, int parity) { k_stream_out<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, parity); }
+void launch_stream_out(const Launch& L, int parity, float* dst) {
+  k_stream_out<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, parity, dst);
+}
 void launch_clear_ws(const Launch& L) { k_clear_ws<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
 
 }  // namespace mc

@@ -245,7 +245,7 @@ void launch_fftreg_cols(const Launch& L, int values_per_thread);
 void launch_reaction(const Launch& L, const int* tdev);
 void launch_record_fields(const Launch& L, const int* tdev);
 void launch_unstream(const Launch& L);
-void launch_stream_out(const Launch& L, int parity);
+void launch_stream_out(const Launch& L, int parity, float* dst = nullptr);
 void launch_clear_ws(const Launch& L);
 void launch_tick(int* tdev, cudaStream_t s);
 cudaError_t fft_set_smem(size_t rows, size_t cols);

@@ -855,6 +855,17 @@ void destroy_graphs(mc_plan* p) {
 namespace mc {
 void set_last_error(const char* msg) { g_err = msg; }
 
+// Inside a rollout (between mc_rollout_begin and mc_rollout_end) of a one-rollout plan:
+// write the current populations in fields.f_grid layout into dst, leaving the rollout as
+// it is (the gradient plan's segment recompute snapshots every step's input this way).
+mc_status rollout_snapshot_f(mc_plan* p, float* dst, cudaStream_t s) {
+  if (!p || !p->active || p->n != 1 || !dst) return fail(MC_ERR_INVALID, "snapshot outside a one-rollout rollout");
+  if (p->pending_next) return fail(MC_ERR_INVALID, "snapshot while the next step's pipeline is in flight");
+  if (p->any_fluid) launch_stream_out(L(p, K_CELLS, s), p->step & 1, dst);
+  MC_CUDA(cudaGetLastError());
+  return MC_OK;
+}
+
 size_t filter_desc_bytes() { return align_up(sizeof(RDesc), 256) + 7 * 256; }
 
 cudaError_t filter_prepare(mc_plan* p, void* dev, const float* in, float* tmp, float* out, cudaStream_t s) {
