@@ -267,7 +267,7 @@ mc_status mc_steric_potential_noalloc(const float* position, int32_t N, int32_t 
  * floor has derivative 0, mod derivative 1, max/min split ties evenly.  It replaces the
  * jax.grad / jax.value_and_grad calls on simulate() in the reference's
  * tests/test_differentiability.py:45,65 (there through XLA's autodiff; here through
- * hand-written adjoint kernels of stream+collide, IB, PBD and steric).
+ * hand-written adjoint kernels of stream+collide, IB, PBD / stable Cosserat and steric).
  *
  * mc_grad_forward runs the rollout with the same kernels as mc_rollout, keeping a
  * checkpoint of (position, velocity, theta, f_grid) every `checkpoint_every` steps
@@ -276,7 +276,9 @@ mc_status mc_steric_potential_noalloc(const float* position, int32_t N, int32_t 
  * O(sqrt(T)) states, compute about three forward rollouts plus the adjoint.
  * Cotangents of the outputs steric and fluid_velocity are taken as zero.
  * Actuation, if given to mc_grad_forward, must have t0 = 0; its omega is not
- * differentiated.  enable_force_clamp != 0 is not supported. */
+ * differentiated.  Both rod solvers (MC_SOLVER_PBD, MC_SOLVER_COSSERAT) are
+ * differentiated; enable_force_clamp != 0, synthetic_node_width != 0 and a fluid lattice
+ * other than the domain grid return MC_ERR_UNSUPPORTED from mc_grad_plan_create. */
 typedef struct mc_state_cot {
   float* position; /* (N,2) */
   float* velocity; /* (N,2) */

@@ -51,7 +51,9 @@ struct StepArgs {
 
 struct AD {
   int H, W, N, E, B, HW, C, iters, K, KK, steric, fluid, nskip, has_act;
+  int solver;  // MC_SOLVER_PBD or MC_SOLVER_COSSERAT
   float dt, damp, st_strength, sigma, scatter, kstretch, kshear, vmax, relax, mass, wp, wm, cp, cm;
+  float cos_w;  // stable-Cosserat inertia weight 1 / solver_dt^2
   float scx, scy, sdtx, sdty;
   // topology
   const int2* pairs;
@@ -114,6 +116,9 @@ struct AD {
   float2* lcur;   // E
   float* lthn;    // E
   float* gb;      // B
+  float2* ly;     // N  stable-Cosserat: cotangent of the prediction the iterations pull toward
+  float2* lfn;    // N  stable-Cosserat: cotangent of a node's summed force
+  float* lhn;     // N  stable-Cosserat: cotangent of a node's summed stiffness
   float* rest_acc;  // B (this step)
   float* d_c;
   float* d_amp;
@@ -771,6 +776,196 @@ __global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d) {
   }
 }
 
+// ------------------------------------------------------------------ stable-Cosserat iterations
+// (solver/stable_cosserat.py:13-119), one CTA per rod component like the PBD kernels.
+// Iteration k: theta' = pull(theta + sum(+-corr) / edeg) toward the segment direction,
+// then x' = x + (w (y - x) + sum(+-f_e)) / (w + sum k_s / l_e^2) with
+// f_e = (k_s / l_e)(r_e / l_e - (cos theta'_e, sin theta'_e)), r_e the min-image segment,
+// y the prediction (pp[0]).  Same arithmetic and sum order as the forward rod kernels.
+__device__ __forceinline__ float2 cos_force(const AD& d, const float2* p, float thn, int e) {
+  const int2 pr = d.pairs[e];
+  const float L0 = d.rest_len[e];
+  const float2 r = mc::min_image(p[pr.y].x, p[pr.y].y, p[pr.x].x, p[pr.x].y, (float)d.W, (float)d.H);
+  float sn, cs;
+  sincosf(thn, &sn, &cs);
+  const float kl = d.kstretch / L0;
+  return make_float2(kl * (r.x / L0 - cs), kl * (r.y / L0 - sn));
+}
+
+// the summed force and stiffness of node n at iterate p, angles thn
+__device__ __forceinline__ void cos_node_sum(const AD& d, const float2* p, const float* thn, int n, float& ax,
+                                             float& ay, float& hh) {
+  const float w = d.cos_w;
+  ax = w * (d.pp[n].x - p[n].x);
+  ay = w * (d.pp[n].y - p[n].y);
+  hh = w;
+  for (int q = d.n_start[n]; q < d.n_start[n + 1]; ++q) {
+    const int en = d.n_list[q];
+    const int e = en >> 1;
+    const float2 f = cos_force(d, p, thn[e], e);
+    if (en & 1) {
+      ax = ax + (-f.x);
+      ay = ay + (-f.y);
+    } else {
+      ax = ax + f.x;
+      ay = ay + f.y;
+    }
+    const float L0 = d.rest_len[e];
+    hh = hh + d.kstretch / (L0 * L0);
+  }
+}
+
+__global__ void __launch_bounds__(kPbdThreads) k_cos_fwd(AD d) {
+  const int c = blockIdx.x;
+  const int ea = d.c_estart[c], eb = d.c_estart[c + 1], na = d.c_nstart[c], nb = d.c_nstart[c + 1];
+  for (int k = 0; k < d.C; ++k) {
+    const float* th = d.tt + (size_t)k * d.E;
+    float* thn = d.tt + (size_t)(k + 1) * d.E;
+    const float2* p = d.pp + (size_t)k * d.N;
+    float2* pn = d.pp + (size_t)(k + 1) * d.N;
+    for (int ie = ea + threadIdx.x; ie < eb; ie += blockDim.x) {
+      const int e = d.c_edges[ie];
+      float acc = 0.0f;
+      for (int q = d.e_start[e]; q < d.e_start[e + 1]; ++q) {
+        const int en = d.e_list[q];
+        const float cr = bend_corr(d, th, en >> 1);
+        acc = acc + ((en & 1) ? -cr : cr);
+      }
+      const int2 pr = d.pairs[e];
+      const float2 r = mc::min_image(p[pr.y].x, p[pr.y].y, p[pr.x].x, p[pr.x].y, (float)d.W, (float)d.H);
+      thn[e] = mc::cos_pull(th[e] + acc / d.edeg[e], r.x, r.y);
+    }
+    __syncthreads();
+    for (int in = na + threadIdx.x; in < nb; in += blockDim.x) {
+      const int n = d.c_nodes[in];
+      float ax, ay, hh;
+      cos_node_sum(d, p, thn, n, ax, ay, hh);
+      pn[n] = make_float2(p[n].x + ax / hh, p[n].y + ay / hh);
+    }
+    __syncthreads();
+  }
+}
+
+// Reverse of k_cos_fwd.  mod passes its cotangent through (derivative 1) and
+// d atan2(r_y, r_x) = (r_x dr_y - r_y dr_x) / |r|^2.
+__global__ void __launch_bounds__(kPbdThreads) k_cos_rev(AD d) {
+  const int t = d.sa[*d.jp].t;
+  const int c = blockIdx.x;
+  const int ea = d.c_estart[c], eb = d.c_estart[c + 1], na = d.c_nstart[c], nb = d.c_nstart[c + 1];
+  const int ba = d.c_bstart[c], bb = d.c_bstart[c + 1];
+  const float ks = d.kstretch, w = d.cos_w;
+  int cur = 0;
+  for (int in = na + threadIdx.x; in < nb; in += blockDim.x) d.ly[d.c_nodes[in]] = make_float2(0.0f, 0.0f);
+  for (int k = d.C - 1; k >= 0; --k) {
+    const float2* p = d.pp + (size_t)k * d.N;
+    const float* th = d.tt + (size_t)k * d.E;
+    const float* thn = d.tt + (size_t)(k + 1) * d.E;
+    const float2* lpi = d.lp[cur];
+    float2* lpo = d.lp[cur ^ 1];
+    const float* lti = d.lt[cur];
+    float* lto = d.lt[cur ^ 1];
+    // x' = x + F / h: cotangents of F, h, y and the direct part of x
+    for (int in = na + threadIdx.x; in < nb; in += blockDim.x) {
+      const int n = d.c_nodes[in];
+      float ax, ay, hh;
+      cos_node_sum(d, p, thn, n, ax, ay, hh);
+      const float2 lx = lpi[n];
+      const float lfx = lx.x / hh, lfy = lx.y / hh;
+      d.lfn[n] = make_float2(lfx, lfy);
+      d.lhn[n] = -(lx.x * ax + lx.y * ay) / (hh * hh);
+      const float2 yy = d.ly[n];
+      d.ly[n] = make_float2(yy.x + w * lfx, yy.y + w * lfy);
+      lpo[n] = make_float2(lx.x - w * lfx, lx.y - w * lfy);
+    }
+    __syncthreads();
+    // per edge: f_e and h_e -> segment, angle, rest length; then the pull
+    for (int ie = ea + threadIdx.x; ie < eb; ie += blockDim.x) {
+      const int e = d.c_edges[ie];
+      const int2 pr = d.pairs[e];
+      const float L0 = d.rest_len[e];
+      const float2 r = mc::min_image(p[pr.y].x, p[pr.y].y, p[pr.x].x, p[pr.x].y, (float)d.W, (float)d.H);
+      float sn, cs;
+      sincosf(thn[e], &sn, &cs);
+      const float2 a = d.lfn[pr.x], b = d.lfn[pr.y];
+      const float lfx = a.x - b.x, lfy = a.y - b.y;
+      const float kl = ks / L0;
+      float lrx = (kl / L0) * lfx, lry = (kl / L0) * lfy;
+      const float lthn = lti[e] + kl * (lfx * sn - lfy * cs);
+      const float cx = r.x / L0 - cs, cy = r.y / L0 - sn;
+      d.d_len[e] += -(kl / L0) * (lfx * cx + lfy * cy) - (kl / (L0 * L0)) * (lfx * r.x + lfy * r.y) +
+                    (d.lhn[pr.x] + d.lhn[pr.y]) * (-2.0f * ks / (L0 * L0 * L0));
+      const float la = 0.05f * lthn;
+      const float r2 = r.x * r.x + r.y * r.y;
+      lrx += -r.y * la / r2;
+      lry += r.x * la / r2;
+      d.lcur[e] = make_float2(lrx, lry);
+      d.lthn[e] = lthn - 0.05f * lthn;  // cotangent of the angle before the pull
+    }
+    __syncthreads();
+    for (int in = na + threadIdx.x; in < nb; in += blockDim.x) {
+      const int n = d.c_nodes[in];
+      float ax = lpo[n].x, ay = lpo[n].y;
+      for (int q = d.n_start[n]; q < d.n_start[n + 1]; ++q) {
+        const int en = d.n_list[q];
+        const float2 lc = d.lcur[en >> 1];
+        if (en & 1) {
+          ax += lc.x;
+          ay += lc.y;
+        } else {
+          ax -= lc.x;
+          ay -= lc.y;
+        }
+      }
+      lpo[n] = make_float2(ax, ay);
+    }
+    for (int ib = ba + threadIdx.x; ib < bb; ib += blockDim.x) {
+      const int b = d.c_bps[ib];
+      const int2 bp = d.bpairs[b];
+      const float lcorr = d.lthn[bp.x] / d.edeg[bp.x] - d.lthn[bp.y] / d.edeg[bp.y];
+      const float g = lcorr * d.kb[b] * 0.5f;
+      d.gb[b] = g;
+      d.rest_acc[b] -= g;
+      const float pi = (float)M_PI;
+      const float diff = mc::fmod_floor((th[bp.y] - th[bp.x]) + pi, (float)(2.0 * M_PI)) - pi;
+      d.d_kb[b] += lcorr * (diff - d.rest[b]) * 0.5f;
+    }
+    __syncthreads();
+    for (int ie = ea + threadIdx.x; ie < eb; ie += blockDim.x) {
+      const int e = d.c_edges[ie];
+      float a = d.lthn[e];
+      for (int q = d.e_start[e]; q < d.e_start[e + 1]; ++q) {
+        const int en = d.e_list[q];
+        const float g = d.gb[en >> 1];
+        a += (en & 1) ? g : -g;
+      }
+      lto[e] = a;
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  // the iterations start from the prediction and are pulled toward it
+  for (int in = na + threadIdx.x; in < nb; in += blockDim.x) {
+    const int n = d.c_nodes[in];
+    const float2 a = d.lp[cur][n], yy = d.ly[n];
+    d.lpred1[n] = make_float2(a.x + yy.x, a.y + yy.y);
+  }
+  for (int ie = ea + threadIdx.x; ie < eb; ie += blockDim.x) d.lth[d.c_edges[ie]] = d.lt[cur][d.c_edges[ie]];
+  for (int ib = ba + threadIdx.x; ib < bb; ib += blockDim.x) {
+    const int b = d.c_bps[ib];
+    const float G = d.rest_acc[b];
+    if (d.has_act) {
+      const float arg = d.act_om[b] * (float)t + d.act_ph[b];
+      float sn, cs;
+      sincosf(arg, &sn, &cs);
+      d.d_c[b] += G;
+      d.d_amp[b] += G * sn;
+      d.d_ph[b] += G * d.act_amp[b] * cs;
+    } else {
+      d.d_rest[b] += G;
+    }
+  }
+}
+
 // ------------------------------------------------------------------ adjoint: steric
 __device__ __forceinline__ void sample_adj(const AD& d, const float* V, float yy, float xx, float coef, int n, int qs,
                                            float& lpx, float& lpy) {
@@ -906,6 +1101,7 @@ struct mc_grad_plan {
   AD ad{};
   std::vector<int> c_nstart, c_nodes, c_estart, c_edges, c_bstart, c_bps;  // rod components
   R r_cns, r_cn, r_ces, r_ce, r_cbs, r_cb, r_sargs, r_jp;
+  R r_ly, r_lfn, r_lhn;
   std::vector<StepArgs> sargs;
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t rev_graph = nullptr;  // one reverse step, replayed per step
@@ -1038,7 +1234,10 @@ void reverse_step(mc_grad_plan* p, cudaStream_t s) {
   const int nNE = std::max(d.N, d.E);
   k_rest<<<nblk(std::max(d.B, 1), TB), TB, 0, s>>>(d);
   k_pred<<<nblk(nNE, TB), TB, 0, s>>>(d);
-  k_pbd_fwd<<<d.ncomp, kPbdThreads, 0, s>>>(d);
+  if (d.solver == MC_SOLVER_COSSERAT)
+    k_cos_fwd<<<d.ncomp, kPbdThreads, 0, s>>>(d);
+  else
+    k_pbd_fwd<<<d.ncomp, kPbdThreads, 0, s>>>(d);
   if (d.fluid) {
     k_ib_weights<<<nblk(d.N, TB), TB, 0, s>>>(d);
     csr_build(d, d.ib_idx, d.N * d.KK, s);
@@ -1056,7 +1255,10 @@ void reverse_step(mc_grad_plan* p, cudaStream_t s) {
     k_lbm_adj2<<<nblk(d.HW, TB), TB, 0, s>>>(d);
   }
   k_node_adj<<<nblk(nNE, TB), TB, 0, s>>>(d);
-  k_pbd_rev<<<d.ncomp, kPbdThreads, 0, s>>>(d);
+  if (d.solver == MC_SOLVER_COSSERAT)
+    k_cos_rev<<<d.ncomp, kPbdThreads, 0, s>>>(d);
+  else
+    k_pbd_rev<<<d.ncomp, kPbdThreads, 0, s>>>(d);
   if (d.steric) {
     k_steric_adj_node<<<nblk(d.N, TB), TB, 0, s>>>(d);
     csr_build(d, d.st_cell, d.N * 16, s);
@@ -1093,8 +1295,10 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   if (cfg->synthetic_node_width != 0.0f) return gfail(MC_ERR_UNSUPPORTED, "synthetic_node_width must be 0");
   if ((D.fluid_H > 0 && D.fluid_H != D.H) || (D.fluid_W > 0 && D.fluid_W != D.W))
     return gfail(MC_ERR_UNSUPPORTED, "the adjoint needs the fluid grid to be the domain grid");
-  if (cfg->solver_type != MC_SOLVER_PBD)
-    return gfail(MC_ERR_UNSUPPORTED, "the adjoint covers the PBD rod constraint only");
+  if (cfg->solver_type != MC_SOLVER_PBD && cfg->solver_type != MC_SOLVER_COSSERAT)
+    return gfail(MC_ERR_INVALID, "solver_type must be MC_SOLVER_PBD or MC_SOLVER_COSSERAT");
+  if (cfg->solver_type == MC_SOLVER_COSSERAT && !(cfg->solver_dt > 0.0))
+    return gfail(MC_ERR_INVALID, "the stable-Cosserat solver needs solver_dt > 0");
   mc_grad_plan* p = new mc_grad_plan();
   p->dims = D;
   p->cfg = *cfg;
@@ -1254,6 +1458,9 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   take(p->r_lcur, E * 8);
   take(p->r_lthn, E * 4);
   take(p->r_gb, B * 4);
+  take(p->r_ly, N * 8);
+  take(p->r_lfn, N * 8);
+  take(p->r_lhn, N * 4);
   take(p->r_racc, B * 4);
   take(p->r_dc, B * 4);
   take(p->r_da, B * 4);
@@ -1355,6 +1562,8 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   d.scatter = c.steric_scatter_value;
   d.kstretch = c.stiffness_stretch;
   d.kshear = c.stiffness_shear;
+  d.solver = c.solver_type;
+  d.cos_w = c.solver_type == MC_SOLVER_COSSERAT ? (float)(1.0 / (c.solver_dt * c.solver_dt)) : 0.0f;
   const float scx = (float)D.W / (float)D.H, scy = (float)D.H / (float)D.W;
   d.scx = scx;
   d.scy = scy;
@@ -1422,6 +1631,9 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   d.lcur = at<float2>(w, p->r_lcur);
   d.lthn = at<float>(w, p->r_lthn);
   d.gb = at<float>(w, p->r_gb);
+  d.ly = at<float2>(w, p->r_ly);
+  d.lfn = at<float2>(w, p->r_lfn);
+  d.lhn = at<float>(w, p->r_lhn);
   d.rest_acc = at<float>(w, p->r_racc);
   d.d_c = at<float>(w, p->r_dc);
   d.d_amp = at<float>(w, p->r_da);

@@ -206,6 +206,13 @@ __device__ __forceinline__ float2 min_image(float ax, float ay, float bx, float 
   return make_float2(fmod_floor((ax - bx) + hx, W) - hx, fmod_floor((ay - by) + hy, H) - hy);
 }
 
+// Stable-Cosserat pull of an edge angle toward its segment's direction (sx, sy):
+// th + wrap(atan2(sy, sx) - th) * 0.05 (solver/stable_cosserat.py:55-82)
+__device__ __forceinline__ float cos_pull(float th, float sx, float sy) {
+  const float alpha = atan2f(sy, sx);
+  return th + (fmod_floor((alpha - th) + MC_PI_F, MC_2PI_F) - MC_PI_F) * 0.05f;
+}
+
 __device__ __forceinline__ float nan_f() { return __int_as_float(0x7fffffff); }
 __device__ __forceinline__ bool is_sentinel(float v) { return __float_as_int(v) == 0x7fffffff; }
 

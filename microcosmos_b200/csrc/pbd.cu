@@ -418,11 +418,6 @@ __device__ __forceinline__ void shift_prev(const float (&v)[P], float (&pv)[P]) 
 // then theta += wrap(atan2(r) - theta) * 0.05 with r the segment's min-image vector.
 // Phase 2: x += (w (y0 - x) + f_j - f_{j-1}) / ((w + H_j) + H_{j-1}), f = (k_s/l)(r/l - d),
 // H = k_s/l^2, y0 the inertial prediction (the positions the kernel started from).
-__device__ __forceinline__ float cos_pull(float th, float sx, float sy) {
-  const float alpha = atan2f(sy, sx);
-  return th + (fmod_floor((alpha - th) + MC_PI_F, MC_2PI_F) - MC_PI_F) * 0.05f;
-}
-
 template <int P>
 __device__ __forceinline__ void cosserat_chain(const RDesc& d, int lane, int nn, int ne, int nb, float (&x)[P],
                                                float (&y)[P], float (&th)[P], const float (&l0)[P],

@@ -160,8 +160,12 @@ def step_tape(s: R.State, cfg: R.Config, dtstep: float, rest_angles, ib_position
     pos, theta = pred, s.theta
     pp, tt = [pos], [theta]
     for _ in range(cfg.cycles_per_step):
-        pos, theta = R.pbd_iteration(H, W, pos, theta, s.pairs, s.bending_pairs, s.rest_lengths, rest,
-                                     s.bending_stiffness, cfg)
+        if cfg.solver_type == "cosserat":
+            pos, theta = R.cosserat_iteration(H, W, pos, pred, theta, s.pairs, s.bending_pairs, s.rest_lengths,
+                                              rest, s.bending_stiffness, cfg)
+        else:
+            pos, theta = R.pbd_iteration(H, W, pos, theta, s.pairs, s.bending_pairs, s.rest_lengths, rest,
+                                         s.bending_stiffness, cfg)
         pp.append(pos)
         tt.append(theta)
     vel1 = (pos - prev) / t(dtstep)
@@ -451,6 +455,74 @@ def pbd_iteration_vjp(H, W, cfg, s, rest, pos, theta, lpos_out, ltheta_out):
     return lpos, ltheta, lrest, lL0, lkb
 
 
+def cosserat_iteration_vjp(H, W, cfg, s, rest, pos, y, theta, lpos_out, ltheta_out):
+    """Cotangents of (pos, y, theta, rest, rest_lengths, bending_stiffness) through one
+    ref_numpy.cosserat_iteration (y: the inertial prediction the iteration pulls toward).
+    mod has derivative 1 (so the pull's wrap passes its cotangent through), and
+    d atan2(r_y, r_x) = (r_x dr_y - r_y dr_x) / |r|^2."""
+    dt = pos.dtype
+    t = dt.type
+    Ecount = theta.shape[0]
+    N = pos.shape[0]
+    src, tgt = s.pairs[:, 0], s.pairs[:, 1]
+    ein, eout = s.bending_pairs[:, 0], s.bending_pairs[:, 1]
+    kb = s.bending_stiffness
+    L0 = s.rest_lengths
+    edeg = np.zeros(Ecount, dt)
+    np.add.at(edeg, ein, t(1.0))
+    np.add.at(edeg, eout, t(1.0))
+    edeg = np.maximum(edeg, t(1.0))
+    pi = t(np.pi)
+    twopi = t(2 * np.pi)
+    diff = np.mod(theta[eout] - theta[ein] + pi, twopi) - pi
+    corr = (diff - rest) * kb * t(0.5)
+    delta = np.zeros(Ecount, dt)
+    np.add.at(delta, ein, corr)
+    np.add.at(delta, eout, -corr)
+    th1 = theta + delta / edeg
+    seg = R.displacement(H, W, pos[tgt], pos[src])
+    alpha = np.arctan2(seg[:, 1], seg[:, 0])
+    thn = th1 + (np.mod(alpha - th1 + pi, twopi) - pi) * t(0.05)
+    ks = t(cfg.stiffness_stretch)
+    w = t(1.0 / (cfg.dt ** 2))
+    cs, sn = np.cos(thn), np.sin(thn)
+    f_edge = (ks / L0)[:, None] * (seg / L0[:, None] - np.stack([cs, sn], axis=-1))
+    f_node = w * (y - pos)
+    h_node = np.full(N, w, dt)
+    np.add.at(f_node, src, f_edge)
+    np.add.at(f_node, tgt, -f_edge)
+    np.add.at(h_node, src, ks / (L0 * L0))
+    np.add.at(h_node, tgt, ks / (L0 * L0))
+    # x_new = pos + f_node / h_node
+    lf = lpos_out / h_node[:, None]
+    lh = -np.sum(lpos_out * f_node, axis=1) / (h_node * h_node)
+    lpos = lpos_out - w * lf
+    ly = w * lf
+    lfe = lf[src] - lf[tgt]
+    # f_edge = (ks / L0) (seg / L0 - d(thn)), h_edge = ks / L0^2
+    lseg = (ks / L0 / L0)[:, None] * lfe
+    lthn = ltheta_out + (ks / L0) * (lfe[:, 0] * sn - lfe[:, 1] * cs)
+    lL0 = (np.sum(lfe * (-(ks / (L0 * L0))[:, None] * (seg / L0[:, None] - np.stack([cs, sn], axis=-1))
+                         - (ks / L0)[:, None] * seg / (L0 * L0)[:, None]), axis=1)
+           + (lh[src] + lh[tgt]) * (-t(2.0) * ks / (L0 * L0 * L0)))
+    # thn = th1 + wrap(alpha - th1) * 0.05
+    lth1 = lthn - t(0.05) * lthn
+    lalpha = t(0.05) * lthn
+    r2 = seg[:, 0] * seg[:, 0] + seg[:, 1] * seg[:, 1]
+    lseg = lseg + np.stack([-seg[:, 1] * lalpha / r2, seg[:, 0] * lalpha / r2], axis=-1)
+    np.add.at(lpos, tgt, lseg)
+    np.add.at(lpos, src, -lseg)
+    # th1 = theta + (sum_in corr - sum_out corr) / edeg
+    lcorr = lth1[ein] / edeg[ein] - lth1[eout] / edeg[eout]
+    ltheta = lth1.copy()
+    g = lcorr * kb * t(0.5)
+    np.add.at(ltheta, eout, g)
+    np.add.at(ltheta, ein, -g)
+    lrest = -g
+    lkb = lcorr * (diff - rest) * t(0.5)
+    return lpos, ly, ltheta, lrest, lL0, lkb
+
+
 @dataclasses.dataclass
 class StepCot:
     position: np.ndarray
@@ -482,12 +554,20 @@ def step_vjp(cfg: R.Config, dtstep: float, tape: Tape, cot: StepCot) -> StepCot:
     lrest = np.zeros_like(tape.rest)
     lL0 = np.zeros_like(s.rest_lengths)
     lkb = np.zeros_like(s.bending_stiffness)
+    ly = np.zeros_like(lpos)
     for k in reversed(range(cfg.cycles_per_step)):
-        lpos, ltheta, lr, ll, lk = pbd_iteration_vjp(H, W, cfg, s, tape.rest, tape.pbd_pos[k], tape.pbd_theta[k],
-                                                     lpos, ltheta)
+        if cfg.solver_type == "cosserat":
+            lpos, lyk, ltheta, lr, ll, lk = cosserat_iteration_vjp(H, W, cfg, s, tape.rest, tape.pbd_pos[k],
+                                                                   tape.pbd_pos[0], tape.pbd_theta[k], lpos, ltheta)
+            ly = ly + lyk
+        else:
+            lpos, ltheta, lr, ll, lk = pbd_iteration_vjp(H, W, cfg, s, tape.rest, tape.pbd_pos[k],
+                                                         tape.pbd_theta[k], lpos, ltheta)
         lrest += lr
         lL0 += ll
         lkb += lk
+    # the Cosserat iterations start from the prediction and are pulled toward it
+    lpos = lpos + ly
     if cfg.enable_steric:
         lpred0 = steric_vjp(H, W, cfg, dtstep, tape.pred0, tape.V, lpos)
     else:

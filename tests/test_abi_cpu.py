@@ -133,6 +133,34 @@ def test_rod_solver_selection(lib):
     assert st == _lib.MC_ERR_INVALID
 
 
+def test_gradient_plan_scope(lib):
+    """mc_grad_plan_create (host-only) takes both rod solvers; synthetic IB pairs and a
+    fluid lattice other than the domain grid have no adjoint and are refused as such."""
+    import dataclasses
+    from microcosmos_b200 import COSSERAT_SCHEME, PBD_SCHEME
+    from microcosmos_b200.engine import mc_config
+    sc = scenarios.make_scenario(32, 32, 2, 10, seed=0)
+    pairs = np.ascontiguousarray(sc.pairs, np.int32)
+    bpairs = np.ascontiguousarray(sc.bending_pairs, np.int32)
+
+    def create(cfg, fluid=(0, 0)):
+        dims = _lib.McDims(32, 32, sc.N, pairs.shape[0], bpairs.shape[0])
+        dims.fluid_H, dims.fluid_W = fluid
+        c = mc_config(cfg)
+        h = ctypes.c_void_p()
+        st = lib.mc_grad_plan_create(ctypes.byref(dims), ctypes.byref(c), 0.01, pairs.ctypes.data_as(_lib.c_int_p),
+                                     bpairs.ctypes.data_as(_lib.c_int_p), 10, 0, ctypes.byref(h))
+        if st == _lib.MC_OK:
+            lib.mc_grad_plan_destroy(h)
+        return st
+
+    assert create(PBD_SCHEME) == _lib.MC_OK
+    assert create(COSSERAT_SCHEME) == _lib.MC_OK
+    assert create(dataclasses.replace(COSSERAT_SCHEME, dt=0.0)) == _lib.MC_ERR_INVALID
+    assert create(dataclasses.replace(PBD_SCHEME, synthetic_node_width=0.5)) == _lib.MC_ERR_UNSUPPORTED
+    assert create(PBD_SCHEME, fluid=(16, 16)) == _lib.MC_ERR_UNSUPPORTED
+
+
 def test_batch_plan_of_uneven_rollouts(lib):
     scs = [scenarios.make_scenario(s, s, f, n, seed=i) for i, (s, f, n) in
            enumerate([(128, 3, 16), (192, 1, 100), (64, 5, 30)])]

@@ -77,6 +77,15 @@ def test_vjp_full_step_with_active_velocity_clamp():
     _check(dataclasses.replace(O.Config(), max_fluid_velocity=0.02), steps=3, seed=5)
 
 
+def test_vjp_cosserat_only():
+    _check(O.Config(enable_fluid=False, enable_steric=False, solver_type="cosserat", dt=0.05))
+
+
+def test_vjp_cosserat_full_step():
+    # the stable-Cosserat rods inside the full step (steric prediction, IB, lattice)
+    _check(O.Config(solver_type="cosserat", dt=0.05, stiffness_stretch=50.0), steps=3, seed=2)
+
+
 def test_vjp_nonsquare_grid_scale():
     _check(O.Config(), H=12, W=24, steps=2, seed=9)
 

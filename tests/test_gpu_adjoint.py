@@ -14,7 +14,7 @@ import pytest
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
-from microcosmos_b200 import PBD_SCHEME, scenarios  # noqa: E402
+from microcosmos_b200 import COSSERAT_SCHEME, PBD_SCHEME, scenarios  # noqa: E402
 from microcosmos_b200.autodiff import GradPlan, rollout  # noqa: E402
 from microcosmos_b200.engine import Actuation, DeviceState  # noqa: E402
 from oracle import adjoint_numpy as A  # noqa: E402
@@ -25,7 +25,8 @@ STATE = ("position", "velocity", "theta", "f_grid")
 
 
 def cfg_of(oc):
-    return dataclasses.replace(PBD_SCHEME, **{f.name: getattr(oc, f.name) for f in dataclasses.fields(O.Config)})
+    base = COSSERAT_SCHEME if oc.solver_type == "cosserat" else PBD_SCHEME
+    return dataclasses.replace(base, **{f.name: getattr(oc, f.name) for f in dataclasses.fields(O.Config)})
 
 
 def case(H, W, F, n, seed):
@@ -68,6 +69,10 @@ CONFIGS = {
     "pbd_steric": O.Config(enable_fluid=False),
     "pbd_fluid": O.Config(enable_steric=False),
     "full": O.Config(),
+    # the stable-Cosserat rod solver (solver_type "cosserat", inertia weight 1/dt^2)
+    "cosserat": O.Config(enable_fluid=False, enable_steric=False, solver_type="cosserat", dt=0.05,
+                         stiffness_stretch=50.0),
+    "cosserat_full": O.Config(solver_type="cosserat", dt=0.05, stiffness_stretch=50.0),
 }
 
 
