@@ -277,8 +277,8 @@ mc_status mc_steric_potential_noalloc(const float* position, int32_t N, int32_t 
  * Cotangents of the outputs steric and fluid_velocity are taken as zero.
  * Actuation, if given to mc_grad_forward, must have t0 = 0; its omega is not
  * differentiated.  Both rod solvers (MC_SOLVER_PBD, MC_SOLVER_COSSERAT) are
- * differentiated; enable_force_clamp != 0, synthetic_node_width != 0 and a fluid lattice
- * other than the domain grid return MC_ERR_UNSUPPORTED from mc_grad_plan_create. */
+ * differentiated, with or without synthetic IB pairs; enable_force_clamp != 0 and a fluid
+ * lattice other than the domain grid return MC_ERR_UNSUPPORTED from mc_grad_plan_create. */
 typedef struct mc_state_cot {
   float* position; /* (N,2) */
   float* velocity; /* (N,2) */

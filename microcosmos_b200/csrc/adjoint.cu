@@ -52,6 +52,8 @@ struct StepArgs {
 struct AD {
   int H, W, N, E, B, HW, C, iters, K, KK, steric, fluid, nskip, has_act;
   int solver;  // MC_SOLVER_PBD or MC_SOLVER_COSSERAT
+  int NI;      // IB points: N, or 2N with synthetic pairs (point p < N: node p, + side; else node p - N, - side)
+  float syn_w, syn_ms;  // synthetic_node_width and the mean lattice scale it is multiplied by
   float dt, damp, st_strength, sigma, scatter, kstretch, kshear, vmax, relax, mass, wp, wm, cp, cm;
   float cos_w;  // stable-Cosserat inertia weight 1 / solver_dt^2
   float scx, scy, sdtx, sdty;
@@ -87,10 +89,10 @@ struct AD {
   float2* pred0;  // (N)
   float2* pp;     // (C+1) x N PBD iterates
   float* tt;      // (C+1) x E
-  int* ib_idx;    // N x KK
-  float* ib_w;    // N x KK
-  float2* sraw;   // iters x N
-  float2* s_tmp;  // N
+  int* ib_idx;    // NI x KK
+  float* ib_w;    // NI x KK
+  float2* sraw;   // iters x NI
+  float2* s_tmp;  // NI
   float* uc;      // 2 x HW
   float* inv;     // HW
   // CSR over cells
@@ -106,7 +108,7 @@ struct AD {
   float* lv;     // 2 x HW
   float* lrho;   // HW
   float* luc;    // 2 x HW
-  float2* lnv;   // N
+  float2* lnv;   // NI
   float2* lprev;  // N
   float2* lpos;   // N   (state cotangent)
   float2* lvel;   // N
@@ -291,11 +293,36 @@ __global__ void __launch_bounds__(kPbdThreads) k_pbd_fwd(AD d) {
 }
 
 // ------------------------------------------------------------------ tape: IB stencils
+// The stencil of IB point n at the step's final PBD positions; with synthetic pairs the
+// point is offset by +-syn_w * syn_ms along the normal of its node's chain tangent (the sum
+// of its edges' min-image vectors, src roles first, as the forward computes it).  The
+// positions are stop_gradient-ed: constants of the derivative.
 __global__ void k_ib_weights(AD d) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= d.N) return;
-  const float2 p = d.pp[(size_t)d.C * d.N + n];
-  const float x = p.x * d.scx, y = p.y * d.scy;
+  if (n >= d.NI) return;
+  const int gi = n < d.N ? n : n - d.N;
+  const float2* pc = d.pp + (size_t)d.C * d.N;
+  const float2 p = pc[gi];
+  float x = p.x * d.scx, y = p.y * d.scy;
+  if (d.NI > d.N) {
+    float tx = 0.0f, ty = 0.0f;
+    for (int q = d.n_start[gi]; q < d.n_start[gi + 1]; ++q) {
+      const int2 pr = d.pairs[d.n_list[q] >> 1];
+      const float2 ev = mc::min_image(pc[pr.y].x, pc[pr.y].y, pc[pr.x].x, pc[pr.x].y, (float)d.W, (float)d.H);
+      tx = tx + ev.x;
+      ty = ty + ev.y;
+    }
+    const float nrm = sqrtf((tx * tx + ty * ty) + MC_EPSIL);
+    const float ux = tx / nrm, uy = ty / nrm;
+    const float ox = (d.syn_w * (-uy)) * d.syn_ms, oy = (d.syn_w * ux) * d.syn_ms;
+    if (n < d.N) {
+      x = x + ox;
+      y = y + oy;
+    } else {
+      x = x - ox;
+      y = y - oy;
+    }
+  }
   const int K = d.K;
   const float half = (float)((K - 1) / 2);
   const float hw = (float)K / 2.0f;
@@ -454,8 +481,9 @@ __global__ void k_macro(AD d) {
 
 __global__ void k_ib_interp(AD d, int it) {
   const float2* __restrict__ prev = reinterpret_cast<const float2*>(d.sa[*d.jp].pos);
-  int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= d.N) return;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;  // IB point
+  if (n >= d.NI) return;
+  const int gi = n < d.N ? n : n - d.N;
   float ix = 0.0f, iy = 0.0f;
   for (int q = 0; q < d.KK; ++q) {
     const int c = d.ib_idx[(size_t)n * d.KK + q];
@@ -463,11 +491,11 @@ __global__ void k_ib_interp(AD d, int it) {
     ix = ix + d.uc[c] * w;
     iy = iy + d.uc[d.HW + c] * w;
   }
-  const float2 pc = d.pp[(size_t)d.C * d.N + n], p0 = prev[n];
+  const float2 pc = d.pp[(size_t)d.C * d.N + gi], p0 = prev[gi];
   const float v1x = (pc.x - p0.x) / d.dt, v1y = (pc.y - p0.y) / d.dt;
   const float nvx = (v1x * d.scx) * d.dt, nvy = (v1y * d.scy) * d.dt;
   const float sx = (nvx - ix) * d.relax, sy = (nvy - iy) * d.relax;
-  d.sraw[(size_t)it * d.N + n] = make_float2(sx, sy);
+  d.sraw[(size_t)it * d.NI + n] = make_float2(sx, sy);
   const float cf = mc::clamp_factor(sx, sy, d.vmax);
   d.s_tmp[n] = make_float2(sx * cf, sy * cf);
 }
@@ -571,14 +599,22 @@ __global__ void k_lbm_adj1(AD d) {
   lFx += half * lusx / rho;
   lFy += half * lusy / rho;
   lrho -= half * (lusx * Fx + lusy * Fy) / (rho * rho);
-  // node reaction: vel_out = vel1 - (nf / m) / sdt, nf = sum_s w F[idx]
+  // node reaction: vel_out = vel1 - (nf / m) / sdt, nf = sum_s w F[idx] (with synthetic
+  // pairs, nf of a node = 0.5 (nf of its + point + nf of its - point))
+  const bool syn = d.NI > d.N;
   float rx = 0.0f, ry = 0.0f;
   for (int q = d.start[c]; q < d.start[c + 1]; ++q) {
     const int e = d.ent[q];
     const float w = d.ib_w[e];
-    const float2 lv = d.lvel[e / d.KK];
-    rx = rx + w * ((-lv.x / d.mass) / d.sdtx);
-    ry = ry + w * ((-lv.y / d.mass) / d.sdty);
+    const int pt = e / d.KK;
+    const float2 lv = d.lvel[pt < d.N ? pt : pt - d.N];
+    float gx = (-lv.x / d.mass) / d.sdtx, gy = (-lv.y / d.mass) / d.sdty;
+    if (syn) {
+      gx = 0.5f * gx;
+      gy = 0.5f * gy;
+    }
+    rx = rx + w * gx;
+    ry = ry + w * gy;
   }
   lFx = rx + lFx;
   lFy = ry + lFy;
@@ -598,8 +634,8 @@ __global__ void k_lbm_adj1(AD d) {
 }
 
 __global__ void k_ib_rev_node(AD d, int it) {
-  int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= d.N) return;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;  // IB point
+  if (n >= d.NI) return;
   float sx = 0.0f, sy = 0.0f;
   for (int q = 0; q < d.KK; ++q) {
     const int c = d.ib_idx[(size_t)n * d.KK + q];
@@ -608,7 +644,7 @@ __global__ void k_ib_rev_node(AD d, int it) {
     sx = sx + (iv * d.luc[c]) * w;
     sy = sy + (iv * d.luc[d.HW + c]) * w;
   }
-  const float2 r = d.sraw[(size_t)it * d.N + n];
+  const float2 r = d.sraw[(size_t)it * d.NI + n];
   const float2 lr = clamp_vjp(r.x, r.y, d.vmax, sx, sy);
   float2 a = d.lnv[n];
   a.x += d.relax * lr.x;
@@ -667,7 +703,12 @@ __global__ void k_node_adj(AD d) {
   if (i >= d.N) return;
   float2 lv1 = d.lvel[i];
   if (d.fluid) {
-    const float2 a = d.lnv[i];
+    float2 a = d.lnv[i];
+    if (d.NI > d.N) {  // both synthetic points carry the node's velocity
+      const float2 b = d.lnv[i + d.N];
+      a.x = a.x + b.x;
+      a.y = a.y + b.y;
+    }
     lv1.x = lv1.x + (a.x * d.scx) * d.dt;
     lv1.y = lv1.y + (a.y * d.scy) * d.dt;
   }
@@ -1239,18 +1280,18 @@ void reverse_step(mc_grad_plan* p, cudaStream_t s) {
   else
     k_pbd_fwd<<<d.ncomp, kPbdThreads, 0, s>>>(d);
   if (d.fluid) {
-    k_ib_weights<<<nblk(d.N, TB), TB, 0, s>>>(d);
-    csr_build(d, d.ib_idx, d.N * d.KK, s);
+    k_ib_weights<<<nblk(d.NI, TB), TB, 0, s>>>(d);
+    csr_build(d, d.ib_idx, d.NI * d.KK, s);
     k_macro<<<nblk(d.HW, TB), TB, 0, s>>>(d);
     for (int it = 0; it < d.iters; ++it) {
-      k_ib_interp<<<nblk(d.N, TB), TB, 0, s>>>(d, it);
-      k_ib_spread<<<nblk(d.N * d.KK, TB), TB, 0, s>>>(d);
+      k_ib_interp<<<nblk(d.NI, TB), TB, 0, s>>>(d, it);
+      k_ib_spread<<<nblk(d.NI * d.KK, TB), TB, 0, s>>>(d);
     }
     k_lbm_adj1<<<nblk(d.HW, TB), TB, 0, s>>>(d);
-    cudaMemsetAsync(d.lnv, 0, (size_t)d.N * 8, s);
+    cudaMemsetAsync(d.lnv, 0, (size_t)d.NI * 8, s);
     for (int it = d.iters - 1; it >= 0; --it) {
-      k_ib_rev_node<<<nblk(d.N, TB), TB, 0, s>>>(d, it);
-      k_ib_rev_cell<<<nblk(d.N * d.KK, TB), TB, 0, s>>>(d);
+      k_ib_rev_node<<<nblk(d.NI, TB), TB, 0, s>>>(d, it);
+      k_ib_rev_cell<<<nblk(d.NI * d.KK, TB), TB, 0, s>>>(d);
     }
     k_lbm_adj2<<<nblk(d.HW, TB), TB, 0, s>>>(d);
   }
@@ -1292,7 +1333,7 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   if (cfg->ibm_kernel_size < 1 || cfg->ibm_kernel_size * cfg->ibm_kernel_size > kMaxKK)
     return gfail(MC_ERR_UNSUPPORTED, "ibm_kernel_size outside 1..8");
   if (cfg->enable_force_clamp) return gfail(MC_ERR_UNSUPPORTED, "enable_force_clamp has no adjoint here");
-  if (cfg->synthetic_node_width != 0.0f) return gfail(MC_ERR_UNSUPPORTED, "synthetic_node_width must be 0");
+  if (cfg->synthetic_node_width < 0.0f) return gfail(MC_ERR_INVALID, "synthetic_node_width must be >= 0");
   if ((D.fluid_H > 0 && D.fluid_H != D.H) || (D.fluid_W > 0 && D.fluid_W != D.W))
     return gfail(MC_ERR_UNSUPPORTED, "the adjoint needs the fluid grid to be the domain grid");
   if (cfg->solver_type != MC_SOLVER_PBD && cfg->solver_type != MC_SOLVER_COSSERAT)
@@ -1392,6 +1433,7 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   p->fwd_bytes = mc_plan_workspace_bytes(p->fwd);
   // layout
   const size_t N = D.N, E = std::max(D.E, 1), B = std::max(D.B, 1), HW = (size_t)D.H * D.W;
+  const size_t NI = N * (cfg->enable_fluid && cfg->synthetic_node_width > 0.0f ? 2 : 1);  // IB points
   const int C = cfg->cycles_per_step, KK = cfg->ibm_kernel_size * cfg->ibm_kernel_size;
   const int iters = std::max(cfg->ibm_iterations, 1);
   size_t o = 0;
@@ -1431,22 +1473,22 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   take(p->r_pred0, N * 8);
   take(p->r_pp, (size_t)(C + 1) * N * 8);
   take(p->r_tt, (size_t)(C + 1) * E * 4);
-  take(p->r_ibidx, N * KK * 4);
-  take(p->r_ibw, N * KK * 4);
-  take(p->r_sraw, (size_t)iters * N * 8);
-  take(p->r_stmp, N * 8);
+  take(p->r_ibidx, NI * KK * 4);
+  take(p->r_ibw, NI * KK * 4);
+  take(p->r_sraw, (size_t)iters * NI * 8);
+  take(p->r_stmp, NI * 8);
   take(p->r_uc, 2 * HW * 4);
   take(p->r_inv, HW * 4);
   take(p->r_cnt, HW * 4);
   take(p->r_start, (HW + 1) * 4);
   take(p->r_bsum, 4096 * 4);
-  take(p->r_ent, std::max<size_t>(N * KK, 16 * N) * 4);
-  take(p->r_touch, std::max<size_t>(N * KK, 16 * N) * 4 + 256);
+  take(p->r_ent, std::max<size_t>(NI * KK, 16 * N) * 4);
+  take(p->r_touch, std::max<size_t>(NI * KK, 16 * N) * 4 + 256);
   take(p->r_lf0p, 9 * HW * 4);
   take(p->r_lv, 2 * HW * 4);
   take(p->r_lrho, HW * 4);
   take(p->r_luc, 2 * HW * 4);
-  take(p->r_lnv, N * 8);
+  take(p->r_lnv, NI * 8);
   take(p->r_lprev, N * 8);
   take(p->r_lpos, N * 8);
   take(p->r_lvel, N * 8);
@@ -1563,6 +1605,9 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   d.kstretch = c.stiffness_stretch;
   d.kshear = c.stiffness_shear;
   d.solver = c.solver_type;
+  d.NI = D.N * (c.enable_fluid && c.synthetic_node_width > 0.0f ? 2 : 1);
+  d.syn_w = c.synthetic_node_width;
+  d.syn_ms = (float)(0.5 * ((double)D.W / D.H + (double)D.H / D.W));
   d.cos_w = c.solver_type == MC_SOLVER_COSSERAT ? (float)(1.0 / (c.solver_dt * c.solver_dt)) : 0.0f;
   const float scx = (float)D.W / (float)D.H, scy = (float)D.H / (float)D.W;
   d.scx = scx;

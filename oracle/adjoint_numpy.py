@@ -71,8 +71,11 @@ class Tape:
     ib: dict | None
 
 
-def _ib_tape(H, W, pos, vel, f_grid, cfg, dtstep, ib_positions):
-    """ib_lbm with its intermediates kept (same arithmetic as ref_numpy.ib_lbm)."""
+def _ib_tape(H, W, pos, vel, f_grid, cfg, dtstep, ib_positions, pairs=None):
+    """ib_lbm with its intermediates kept (same arithmetic as ref_numpy.ib_lbm).  With
+    synthetic_node_width > 0 the IB points are the synthetic pairs, built from the
+    stop_gradient-ed stencil positions (constants of the derivative, fluid.py:259), each
+    carrying its node's velocity; a node's reaction is the mean of its two points'."""
     dt = f_grid.dtype
     t = dt.type
     h, w = H, W
@@ -81,6 +84,12 @@ def _ib_tape(H, W, pos, vel, f_grid, cfg, dtstep, ib_positions):
     eps = t(R.EPSIL32)
     node_vel = vel * scale * t(dtstep)
     gpos = (pos if ib_positions is None else ib_positions) * scale
+    nn = pos.shape[0]
+    syn = cfg.synthetic_node_width > 0.0
+    if syn:
+        gpos = R.synthetic_ib_positions(H, W, pos if ib_positions is None else ib_positions, pairs, gpos,
+                                        cfg.synthetic_node_width, 0.5 * (w / H + h / W))
+        node_vel = np.concatenate([node_vel, node_vel], axis=0)
     f0 = np.maximum(f_grid, eps)
     rho_raw = f0[0]
     for i in range(1, 9):
@@ -134,11 +143,13 @@ def _ib_tape(H, W, pos, vel, f_grid, cfg, dtstep, ib_positions):
         acc = np.zeros(g.shape[0], dt)
         for k in range(nst):
             acc = acc + g[:, k]
+        if syn:
+            acc = t(0.5) * (acc[:nn] + acc[nn:])
         nf.append(acc)
     sdt = scale * t(dtstep)
     vel_out = np.stack([vel[:, 0] - (nf[0] / t(cfg.node_mass)) / sdt[0],
                         vel[:, 1] - (nf[1] / t(cfg.node_mass)) / sdt[1]], axis=-1)
-    tape = dict(scale=scale, vmax=vmax, f=f_grid, f0=f0, rho_raw=rho_raw, rho=rho, ux=ux, uy=uy, vx=vx, vy=vy,
+    tape = dict(syn=syn, nn=nn, scale=scale, vmax=vmax, f=f_grid, f0=f0, rho_raw=rho_raw, rho=rho, ux=ux, uy=uy, vx=vx, vy=vy,
                 idx=idx, wts=wts, inv=inv, sraw=sraw, uc5=(uc5x, uc5y), ucc=(ucx_c, ucy_c), F=(Fx, Fy),
                 fpost=fpost, wp=wp, wm=wm, sdt=sdt)
     return vel_out, fnew, np.stack([usx, usy]), tape
@@ -174,7 +185,7 @@ def step_tape(s: R.State, cfg: R.Config, dtstep: float, rest_angles, ib_position
     ib = None
     vel = vel1
     if cfg.enable_fluid:
-        vel, fnew, fluid_u, ib = _ib_tape(H, W, pos, vel1, s.f_grid, cfg, dtstep, ib_positions)
+        vel, fnew, fluid_u, ib = _ib_tape(H, W, pos, vel1, s.f_grid, cfg, dtstep, ib_positions, s.pairs)
         out.f_grid = fnew
         out.fluid_velocity = fluid_u
     if V is not None:
@@ -260,6 +271,9 @@ def ib_vjp(H, W, cfg, dtstep, tp, lvel_out, lf_new):
     # node reaction: vel_out = vel1 - (nf / m) / sdt
     lvel1 = lvel_out.copy()
     lnf = [-lvel_out[:, 0] / t(cfg.node_mass) / tp["sdt"][0], -lvel_out[:, 1] / t(cfg.node_mass) / tp["sdt"][1]]
+    if tp["syn"]:
+        # a node's reaction is 0.5 (point + its pair): each point gets half the cotangent
+        lnf = [np.concatenate([t(0.5) * a, t(0.5) * a]) for a in lnf]
     lFx = _scatter(HW, idx, wts, lnf[0]).reshape(H, W)
     lFy = _scatter(HW, idx, wts, lnf[1]).reshape(H, W)
     # stream: f_new_i[y+cy, x+cx] = max(fpost_i[y, x], eps)
@@ -305,6 +319,9 @@ def ib_vjp(H, W, cfg, dtstep, tp, lvel_out, lf_new):
     for i in range(9):
         lf0[i] = lf0[i] + lraw + (t(E[i, 0]) * lux + t(E[i, 1]) * luy) / rho
     lf = lf0 * dmax(tp["f"], eps)
+    if tp["syn"]:
+        nn = tp["nn"]
+        lnode_vel = lnode_vel[:nn] + lnode_vel[nn:]
     lvel1 = lvel1 + lnode_vel * tp["scale"] * t(dtstep)
     return lvel1, lf
 

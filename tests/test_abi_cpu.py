@@ -134,8 +134,8 @@ def test_rod_solver_selection(lib):
 
 
 def test_gradient_plan_scope(lib):
-    """mc_grad_plan_create (host-only) takes both rod solvers; synthetic IB pairs and a
-    fluid lattice other than the domain grid have no adjoint and are refused as such."""
+    """mc_grad_plan_create (host-only) takes both rod solvers and synthetic IB pairs; a
+    fluid lattice other than the domain grid has no adjoint and is refused as such."""
     import dataclasses
     from microcosmos_b200 import COSSERAT_SCHEME, PBD_SCHEME
     from microcosmos_b200.engine import mc_config
@@ -157,7 +157,8 @@ def test_gradient_plan_scope(lib):
     assert create(PBD_SCHEME) == _lib.MC_OK
     assert create(COSSERAT_SCHEME) == _lib.MC_OK
     assert create(dataclasses.replace(COSSERAT_SCHEME, dt=0.0)) == _lib.MC_ERR_INVALID
-    assert create(dataclasses.replace(PBD_SCHEME, synthetic_node_width=0.5)) == _lib.MC_ERR_UNSUPPORTED
+    assert create(dataclasses.replace(PBD_SCHEME, synthetic_node_width=0.5)) == _lib.MC_OK
+    assert create(dataclasses.replace(COSSERAT_SCHEME, synthetic_node_width=0.5)) == _lib.MC_OK
     assert create(PBD_SCHEME, fluid=(16, 16)) == _lib.MC_ERR_UNSUPPORTED
 
 

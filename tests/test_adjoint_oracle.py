@@ -86,6 +86,12 @@ def test_vjp_cosserat_full_step():
     _check(O.Config(solver_type="cosserat", dt=0.05, stiffness_stretch=50.0), steps=3, seed=2)
 
 
+def test_vjp_synthetic_ib_pairs():
+    # two IB points per node off the chain tangent; their positions are stencil positions
+    # (held fixed), the node velocity feeds both and the reaction is their mean
+    _check(O.Config(synthetic_node_width=0.5), steps=3, seed=4)
+
+
 def test_vjp_nonsquare_grid_scale():
     _check(O.Config(), H=12, W=24, steps=2, seed=9)
 

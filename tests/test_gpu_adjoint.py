@@ -73,6 +73,10 @@ CONFIGS = {
     "cosserat": O.Config(enable_fluid=False, enable_steric=False, solver_type="cosserat", dt=0.05,
                          stiffness_stretch=50.0),
     "cosserat_full": O.Config(solver_type="cosserat", dt=0.05, stiffness_stretch=50.0),
+    # synthetic IB node pairs (2N IB points; positions held as stencil positions)
+    "synthetic": O.Config(synthetic_node_width=0.5),
+    "cosserat_synthetic": O.Config(solver_type="cosserat", dt=0.05, stiffness_stretch=50.0,
+                                   synthetic_node_width=0.5),
 }
 
 
