@@ -275,10 +275,9 @@ mc_status mc_steric_potential_noalloc(const float* position, int32_t N, int32_t 
  * from its checkpoint and runs the adjoint steps in reverse: device memory is
  * O(sqrt(T)) states, compute about three forward rollouts plus the adjoint.
  * Cotangents of the outputs steric and fluid_velocity are taken as zero.
- * Actuation, if given to mc_grad_forward, must have t0 = 0; its omega is not
- * differentiated.  Both rod solvers (MC_SOLVER_PBD, MC_SOLVER_COSSERAT) are
- * differentiated, with or without synthetic IB pairs; enable_force_clamp != 0 and a fluid
- * lattice other than the domain grid return MC_ERR_UNSUPPORTED from mc_grad_plan_create. */
+ * Actuation, if given to mc_grad_forward, must have t0 = 0.  Both rod solvers (MC_SOLVER_PBD, MC_SOLVER_COSSERAT) are
+ * differentiated, with or without synthetic IB pairs and the force clamp; a fluid lattice
+ * other than the domain grid returns MC_ERR_UNSUPPORTED from mc_grad_plan_create. */
 typedef struct mc_state_cot {
   float* position; /* (N,2) */
   float* velocity; /* (N,2) */
@@ -287,7 +286,8 @@ typedef struct mc_state_cot {
 } mc_state_cot;
 
 /* Gradient outputs, any may be NULL.  rest_angles: the static bending_rest_angles (used
- * when mc_grad_forward had no actuation); act_c/act_amp/act_phase: the actuation arrays. */
+ * when mc_grad_forward had no actuation); act_c/act_amp/act_phase/act_omega: the actuation
+ * arrays. */
 typedef struct mc_param_grads {
   float* rest_angles;       /* (B,) */
   float* act_c;             /* (B,) */
@@ -295,6 +295,7 @@ typedef struct mc_param_grads {
   float* act_phase;         /* (B,) */
   float* rest_lengths;      /* (E,) */
   float* bending_stiffness; /* (B,) */
+  float* act_omega;         /* (B,) */
 } mc_param_grads;
 
 typedef struct mc_grad_plan mc_grad_plan;

@@ -83,7 +83,7 @@ class McStateCot(ctypes.Structure):
 class McParamGrads(ctypes.Structure):
     _fields_ = [("rest_angles", ctypes.c_void_p), ("act_c", ctypes.c_void_p), ("act_amp", ctypes.c_void_p),
                 ("act_phase", ctypes.c_void_p), ("rest_lengths", ctypes.c_void_p),
-                ("bending_stiffness", ctypes.c_void_p)]
+                ("bending_stiffness", ctypes.c_void_p), ("act_omega", ctypes.c_void_p)]
 
 
 class McEnv(ctypes.Structure):

@@ -74,7 +74,7 @@ class GradPlan:
         out = {"position": z(self.N, 2), "velocity": z(self.N, 2), "theta": z(self.E),
                "f_grid": z(9, self.H, self.W), "rest_lengths": z(self.E), "bending_stiffness": z(self.B)}
         if self.has_act:
-            out.update(act_c=z(self.B), act_amp=z(self.B), act_phase=z(self.B))
+            out.update(act_c=z(self.B), act_amp=z(self.B), act_omega=z(self.B), act_phase=z(self.B))
         else:
             out["bending_rest_angles"] = z(self.B)
         ini = _lib.McStateCot(out["position"].data_ptr(), out["velocity"].data_ptr(), out["theta"].data_ptr(),
@@ -83,7 +83,8 @@ class GradPlan:
                               out["act_c"].data_ptr() if self.has_act else None,
                               out["act_amp"].data_ptr() if self.has_act else None,
                               out["act_phase"].data_ptr() if self.has_act else None,
-                              out["rest_lengths"].data_ptr(), out["bending_stiffness"].data_ptr())
+                              out["rest_lengths"].data_ptr(), out["bending_stiffness"].data_ptr(),
+                              out["act_omega"].data_ptr() if self.has_act else None)
         s = torch.cuda.current_stream().cuda_stream
         _lib.check(lib.mc_grad_backward(self._h, ctypes.byref(fin), ctypes.byref(ini), ctypes.byref(g),
                                         ctypes.c_void_p(s)))
@@ -110,9 +111,9 @@ def _c(t):
 class _Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, position, velocity, theta, f_grid, rest_lengths, bending_stiffness, bending_rest_angles,
-                act_c, act_amp, act_phase, spec):
+                act_c, act_amp, act_omega, act_phase, spec):
         from .engine import Actuation, DeviceState
-        H, W, pairs, bpairs, cfg, dt, num_steps, act_omega, ckpt = spec
+        H, W, pairs, bpairs, cfg, dt, num_steps, ckpt = spec
         st = DeviceState.from_arrays(H, W, position.detach(), velocity.detach(), pairs, theta.detach(),
                                      rest_lengths.detach(), bpairs, bending_rest_angles.detach(),
                                      bending_stiffness.detach(), f_grid.detach(), device=position.device)
@@ -131,11 +132,13 @@ class _Rollout(torch.autograd.Function):
     def backward(ctx, gpos, gvel, gth, gf, _gs, _gu):
         g = ctx.plan.backward(gpos, gvel, gth, gf)
         if ctx.has_act:
-            gr, gc, ga, gp = None, g["act_c"], g["act_amp"], g["act_phase"]
+            gr, gc, ga, go, gp = None, g["act_c"], g["act_amp"], g["act_omega"], g["act_phase"]
         else:
-            gr, gc, ga, gp = g["bending_rest_angles"], None, None, None
-        return (g["position"], g["velocity"], g["theta"], g["f_grid"], g["rest_lengths"], g["bending_stiffness"],
-                gr, gc, ga, gp, None)
+            gr, gc, ga, go, gp = g["bending_rest_angles"], None, None, None, None
+        grads = (g["position"], g["velocity"], g["theta"], g["f_grid"], g["rest_lengths"], g["bending_stiffness"],
+                 gr, gc, ga, go, gp)
+        # inputs given as arrays (e.g. a fixed omega) take no gradient
+        return tuple(x if need else None for x, need in zip(grads, ctx.needs_input_grad)) + (None,)
 
 
 def rollout(position, velocity, theta, f_grid, rest_lengths, bending_stiffness, bending_rest_angles, pairs,
@@ -143,7 +146,7 @@ def rollout(position, velocity, theta, f_grid, rest_lengths, bending_stiffness, 
     """Differentiable rollout (torch): returns (position, velocity, theta, f_grid, steric,
     fluid_velocity) after ``num_steps`` steps.  ``actuation`` = (c, amp, omega, phase) per
     bending pair (rest[b](t) = c + amp sin(omega t + phase)); gradients flow to every
-    float tensor argument except omega.  ``f_grid`` is (9, H, W)."""
+    float tensor argument.  ``f_grid`` is (9, H, W)."""
     f_grid = f_grid.reshape(9, *f_grid.shape[-2:])
     H, W = int(f_grid.shape[1]), int(f_grid.shape[2])
     pairs_h = np.ascontiguousarray(pairs.detach().cpu().numpy() if isinstance(pairs, torch.Tensor) else pairs,
@@ -153,6 +156,6 @@ def rollout(position, velocity, theta, f_grid, rest_lengths, bending_stiffness, 
     c = amp = om = ph = None
     if actuation is not None:
         c, amp, om, ph = actuation
-    spec = (H, W, pairs_h, bp_h, cfg, float(dt), int(num_steps), om, int(checkpoint_every))
+    spec = (H, W, pairs_h, bp_h, cfg, float(dt), int(num_steps), int(checkpoint_every))
     return _Rollout.apply(position, velocity, theta, f_grid, rest_lengths, bending_stiffness, bending_rest_angles,
-                          c, amp, ph, spec)
+                          c, amp, om, ph, spec)

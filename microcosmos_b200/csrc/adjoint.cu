@@ -52,6 +52,7 @@ struct StepArgs {
 struct AD {
   int H, W, N, E, B, HW, C, iters, K, KK, steric, fluid, nskip, has_act;
   int solver;  // MC_SOLVER_PBD or MC_SOLVER_COSSERAT
+  int force_clamp;  // enable_force_clamp: F = F_raw * clamp factor of F_raw
   int NI;      // IB points: N, or 2N with synthetic pairs (point p < N: node p, + side; else node p - N, - side)
   float syn_w, syn_ms;  // synthetic_node_width and the mean lattice scale it is multiplied by
   float dt, damp, st_strength, sigma, scatter, kstretch, kshear, vmax, relax, mass, wp, wm, cp, cm;
@@ -125,6 +126,7 @@ struct AD {
   float* d_c;
   float* d_amp;
   float* d_ph;
+  float* d_om;
   float* d_rest;
   float* d_len;
   float* d_kb;
@@ -547,7 +549,13 @@ __global__ void k_lbm_adj1(AD d) {
   const float u5x = d.uc[c], u5y = d.uc[d.HW + c];
   const float c2 = mc::clamp_factor(u5x, u5y, d.vmax);
   const float ucx = u5x * c2, ucy = u5y * c2;
-  const float Fx = (ucx - vx) * rho, Fy = (ucy - vy) * rho;
+  const float Frx = (ucx - vx) * rho, Fry = (ucy - vy) * rho;
+  float Fx = Frx, Fy = Fry;
+  if (d.force_clamp) {
+    const float c3 = mc::clamp_factor(Frx, Fry, d.vmax);
+    Fx = Frx * c3;
+    Fy = Fry * c3;
+  }
   // forward collide for the floor masks
   float post[9], us_x, us_y;
   mc::collide(f0, rho, vx, vy, Fx, Fy, d.wp, d.wm, d.cp, d.cm, post, us_x, us_y);
@@ -618,11 +626,16 @@ __global__ void k_lbm_adj1(AD d) {
   }
   lFx = rx + lFx;
   lFy = ry + lFy;
+  if (d.force_clamp) {
+    const float2 lr = clamp_vjp(Frx, Fry, d.vmax, lFx, lFy);
+    lFx = lr.x;
+    lFy = lr.y;
+  }
   // F = (ucc - v) rho
   const float lccx = lFx * rho, lccy = lFy * rho;
   lvx -= lFx * rho;
   lvy -= lFy * rho;
-  lrho += lFx * (ucx - vx) + lFy * (ucy - vy);
+  lrho += lFx * (ucx - vx) + lFy * (ucy - vy);  // through F_raw = (ucc - v) rho
   const float2 l5 = clamp_vjp(u5x, u5y, d.vmax, lccx, lccy);
   d.luc[c] = l5.x;
   d.luc[d.HW + c] = l5.y;
@@ -811,6 +824,7 @@ __global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d) {
       d.d_c[b] += G;
       d.d_amp[b] += G * sn;
       d.d_ph[b] += G * d.act_amp[b] * cs;
+      d.d_om[b] += G * d.act_amp[b] * cs * (float)t;
     } else {
       d.d_rest[b] += G;
     }
@@ -1001,6 +1015,7 @@ __global__ void __launch_bounds__(kPbdThreads) k_cos_rev(AD d) {
       d.d_c[b] += G;
       d.d_amp[b] += G * sn;
       d.d_ph[b] += G * d.act_amp[b] * cs;
+      d.d_om[b] += G * d.act_amp[b] * cs * (float)t;
     } else {
       d.d_rest[b] += G;
     }
@@ -1136,7 +1151,7 @@ struct mc_grad_plan {
   R r_wpos, r_wvel, r_wth, r_wra, r_wst, r_wfu, r_wf, r_ck, r_seg, r_segV;
   R r_rest, r_pred0, r_pp, r_tt, r_ibidx, r_ibw, r_sraw, r_stmp, r_uc, r_inv, r_cnt, r_start, r_bsum, r_ent, r_touch;
   R r_lf0p, r_lv, r_lrho, r_luc, r_lnv, r_lprev, r_lpos, r_lvel, r_lth, r_lp0, r_lp1, r_lt0, r_lt1, r_lcur, r_lthn,
-      r_gb, r_racc, r_dc, r_da, r_dp, r_dr, r_dl, r_dk, r_stc, r_stv, r_lpred1, r_lpred0p, r_lV, r_ctmp, r_ldep, r_lf0,
+      r_gb, r_racc, r_dc, r_da, r_dp, r_do, r_dr, r_dl, r_dk, r_stc, r_stv, r_lpred1, r_lpred0p, r_lV, r_ctmp, r_ldep, r_lf0,
       r_lf1;
   size_t state_ck_bytes = 0;  // one checkpoint: pos, vel, theta, f
   AD ad{};
@@ -1332,7 +1347,6 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   if ((long long)D.H * D.W > (long long)kScanChunk * 4096) return gfail(MC_ERR_UNSUPPORTED, "grid too large for the gradient path");
   if (cfg->ibm_kernel_size < 1 || cfg->ibm_kernel_size * cfg->ibm_kernel_size > kMaxKK)
     return gfail(MC_ERR_UNSUPPORTED, "ibm_kernel_size outside 1..8");
-  if (cfg->enable_force_clamp) return gfail(MC_ERR_UNSUPPORTED, "enable_force_clamp has no adjoint here");
   if (cfg->synthetic_node_width < 0.0f) return gfail(MC_ERR_INVALID, "synthetic_node_width must be >= 0");
   if ((D.fluid_H > 0 && D.fluid_H != D.H) || (D.fluid_W > 0 && D.fluid_W != D.W))
     return gfail(MC_ERR_UNSUPPORTED, "the adjoint needs the fluid grid to be the domain grid");
@@ -1507,6 +1521,7 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   take(p->r_dc, B * 4);
   take(p->r_da, B * 4);
   take(p->r_dp, B * 4);
+  take(p->r_do, B * 4);
   take(p->r_dr, B * 4);
   take(p->r_dl, E * 4);
   take(p->r_dk, B * 4);
@@ -1605,6 +1620,7 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   d.kstretch = c.stiffness_stretch;
   d.kshear = c.stiffness_shear;
   d.solver = c.solver_type;
+  d.force_clamp = c.enable_force_clamp;
   d.NI = D.N * (c.enable_fluid && c.synthetic_node_width > 0.0f ? 2 : 1);
   d.syn_w = c.synthetic_node_width;
   d.syn_ms = (float)(0.5 * ((double)D.W / D.H + (double)D.H / D.W));
@@ -1683,6 +1699,7 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   d.d_c = at<float>(w, p->r_dc);
   d.d_amp = at<float>(w, p->r_da);
   d.d_ph = at<float>(w, p->r_dp);
+  d.d_om = at<float>(w, p->r_do);
   d.d_rest = at<float>(w, p->r_dr);
   d.d_len = at<float>(w, p->r_dl);
   d.d_kb = at<float>(w, p->r_dk);
@@ -1789,7 +1806,7 @@ mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_st
   GC(seed(p->r_lvel, final_cot->velocity, (size_t)D.N * 8));
   GC(seed(p->r_lth, final_cot->theta, (size_t)D.E * 4));
   GC(seed(p->r_lf0, final_cot->f_grid, 9 * HW * 4));
-  for (const mc_grad_plan::R* r : {&p->r_dc, &p->r_da, &p->r_dp, &p->r_dr, &p->r_dl, &p->r_dk})
+  for (const mc_grad_plan::R* r : {&p->r_dc, &p->r_da, &p->r_dp, &p->r_do, &p->r_dr, &p->r_dl, &p->r_dk})
     GC(cudaMemsetAsync(w + r->off, 0, r->bytes, s));
   if (d.steric && !p->filter_ready) {
     // the forward plan's descriptor exists once mc_grad_forward has run a rollout call
@@ -1879,6 +1896,7 @@ mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_st
     GC(out(grads->act_c, p->r_dc, (size_t)D.B * 4));
     GC(out(grads->act_amp, p->r_da, (size_t)D.B * 4));
     GC(out(grads->act_phase, p->r_dp, (size_t)D.B * 4));
+    GC(out(grads->act_omega, p->r_do, (size_t)D.B * 4));
     GC(out(grads->rest_angles, p->r_dr, (size_t)D.B * 4));
     GC(out(grads->rest_lengths, p->r_dl, (size_t)D.E * 4));
     GC(out(grads->bending_stiffness, p->r_dk, (size_t)D.B * 4));

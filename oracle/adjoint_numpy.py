@@ -131,8 +131,13 @@ def _ib_tape(H, W, pos, vel, f_grid, cfg, dtstep, ib_positions, pairs=None):
     ucx_c, ucy_c = uc5x * c2, uc5y * c2
     Fx = (ucx_c - vx) * rho
     Fy = (ucy_c - vy) * rho
+    Fraw = None
     if cfg.enable_force_clamp:
-        raise NotImplementedError("enable_force_clamp is not part of the gradient oracle")
+        # the optional force clamp (fluid.py:336-339), same factor form as the velocity clamp
+        Fraw = (Fx, Fy)
+        c3 = R.velocity_clamp_factor(Fx, Fy, vmax)
+        Fx = Fx * c3
+        Fy = Fy * c3
     wp, wm = R.trt_rates(cfg, dt)
     fpost, usx, usy = R.collide(f0, rho, vx, vy, Fx, Fy, wp, wm)
     fnew = R.stream(fpost)
@@ -149,7 +154,7 @@ def _ib_tape(H, W, pos, vel, f_grid, cfg, dtstep, ib_positions, pairs=None):
     sdt = scale * t(dtstep)
     vel_out = np.stack([vel[:, 0] - (nf[0] / t(cfg.node_mass)) / sdt[0],
                         vel[:, 1] - (nf[1] / t(cfg.node_mass)) / sdt[1]], axis=-1)
-    tape = dict(syn=syn, nn=nn, scale=scale, vmax=vmax, f=f_grid, f0=f0, rho_raw=rho_raw, rho=rho, ux=ux, uy=uy, vx=vx, vy=vy,
+    tape = dict(syn=syn, nn=nn, Fraw=Fraw, scale=scale, vmax=vmax, f=f_grid, f0=f0, rho_raw=rho_raw, rho=rho, ux=ux, uy=uy, vx=vx, vy=vy,
                 idx=idx, wts=wts, inv=inv, sraw=sraw, uc5=(uc5x, uc5y), ucc=(ucx_c, ucy_c), F=(Fx, Fy),
                 fpost=fpost, wp=wp, wm=wm, sdt=sdt)
     return vel_out, fnew, np.stack([usx, usy]), tape
@@ -288,6 +293,8 @@ def ib_vjp(H, W, cfg, dtstep, tp, lvel_out, lf_new):
     lf0, lrho, lvx, lvy, cFx, cFy = collide_vjp(tp["f0"], rho, vx, vy, Fx, Fy, tp["wp"], tp["wm"], lpost)
     lFx = lFx + cFx
     lFy = lFy + cFy
+    if tp["Fraw"] is not None:
+        lFx, lFy = clamp_vjp(tp["Fraw"][0], tp["Fraw"][1], tp["vmax"], lFx, lFy)
     # F = (ucc - v) rho
     uccx, uccy = tp["ucc"]
     luccx, luccy = lFx * rho, lFy * rho
@@ -620,6 +627,7 @@ def rollout_vjp(cfg, dtstep, tapes, cot: StepCot, act=None, t0=0):
     lc = np.zeros_like(tapes[0].rest)
     lamp = np.zeros_like(lc)
     lph = np.zeros_like(lc)
+    lom = np.zeros_like(lc)
     lL0 = np.zeros_like(tapes[0].s.rest_lengths)
     lkb = np.zeros_like(tapes[0].s.bending_stiffness)
     for k in reversed(range(len(tapes))):
@@ -634,10 +642,11 @@ def rollout_vjp(cfg, dtstep, tapes, cot: StepCot, act=None, t0=0):
             lc += cot.rest
             lamp += cot.rest * np.sin(arg)
             lph += cot.rest * amp * np.cos(arg)
+            lom += cot.rest * amp * np.cos(arg) * tt(t0 + k)
     out = dict(position=cot.position, velocity=cot.velocity, theta=cot.theta, f_grid=cot.f_grid,
                rest_lengths=lL0, bending_stiffness=lkb)
     if act is None:
         out["rest"] = lrest_static
     else:
-        out.update(act_c=lc, act_amp=lamp, act_phase=lph)
+        out.update(act_c=lc, act_amp=lamp, act_omega=lom, act_phase=lph)
     return out

@@ -36,8 +36,8 @@ def _check(cfg, H=16, W=20, F=2, n=7, steps=3, seed=0, h=1e-6, tol=2e-6, ndir=3)
     cot = {k: rng.normal(size=getattr(sT, k).shape) for k in ("position", "velocity", "theta", "f_grid")}
     g = A.rollout_vjp(cfg, dt, tapes, A.StepCot(cot["position"], cot["velocity"], cot["theta"], cot["f_grid"]),
                       act)
-    names = ["position", "velocity", "theta", "f_grid", "act_c", "act_amp", "act_phase", "rest_lengths",
-             "bending_stiffness"]
+    names = ["position", "velocity", "theta", "f_grid", "act_c", "act_amp", "act_omega", "act_phase",
+             "rest_lengths", "bending_stiffness"]
     for _ in range(ndir):
         d = {k: rng.normal(size=(s0.f_grid.shape if k == "f_grid" else
                                  getattr(s0, k).shape if hasattr(s0, k) else act[0].shape)) for k in names}
@@ -47,7 +47,8 @@ def _check(cfg, H=16, W=20, F=2, n=7, steps=3, seed=0, h=1e-6, tol=2e-6, ndir=3)
             s = s0.copy()
             for k in ("position", "velocity", "theta", "f_grid", "rest_lengths", "bending_stiffness"):
                 setattr(s, k, getattr(s0, k) + eps * d[k])
-            a = (act[0] + eps * d["act_c"], act[1] + eps * d["act_amp"], act[2], act[3] + eps * d["act_phase"])
+            a = (act[0] + eps * d["act_c"], act[1] + eps * d["act_amp"], act[2] + eps * d["act_omega"],
+                 act[3] + eps * d["act_phase"])
             out, _ = A.rollout(s, cfg, dt, steps, a, ib_positions=ibp)
             return _loss(out, cot)
 
@@ -84,6 +85,13 @@ def test_vjp_cosserat_only():
 def test_vjp_cosserat_full_step():
     # the stable-Cosserat rods inside the full step (steric prediction, IB, lattice)
     _check(O.Config(solver_type="cosserat", dt=0.05, stiffness_stretch=50.0), steps=3, seed=2)
+
+
+def test_vjp_force_clamp():
+    # enable_force_clamp: |F| <= 2 vmax rho, so the clamp needs a low cap and full
+    # relaxation to act (here at 2-4 cells per step)
+    _check(dataclasses.replace(O.Config(), enable_force_clamp=True, max_fluid_velocity=0.004, ibm_relaxation=1.0),
+           steps=3, seed=6)
 
 
 def test_vjp_synthetic_ib_pairs():

@@ -75,6 +75,8 @@ CONFIGS = {
     "cosserat_full": O.Config(solver_type="cosserat", dt=0.05, stiffness_stretch=50.0),
     # synthetic IB node pairs (2N IB points; positions held as stencil positions)
     "synthetic": O.Config(synthetic_node_width=0.5),
+    # enable_force_clamp with a cap low enough for it to act (|F| <= 2 vmax rho)
+    "force_clamp": O.Config(enable_force_clamp=True, max_fluid_velocity=0.004, ibm_relaxation=1.0),
     "cosserat_synthetic": O.Config(solver_type="cosserat", dt=0.05, stiffness_stretch=50.0,
                                    synthetic_node_width=0.5),
 }
@@ -114,7 +116,7 @@ def test_adjoint_against_central_differences():
     acts = tuple(np.asarray(x, np.float64) for x in (sc.act_c, sc.act_amp, sc.act_omega, sc.act_phase))
     _, tapes = A.rollout(s0, oc, 0.01, steps, acts)
     ibp = A.ib_positions_of(tapes)
-    names = ["position", "velocity", "theta", "f_grid", "act_c", "act_amp", "act_phase"]
+    names = ["position", "velocity", "theta", "f_grid", "act_c", "act_amp", "act_omega", "act_phase"]
     rng = np.random.default_rng(0)
 
     def loss(s):
@@ -128,7 +130,8 @@ def test_adjoint_against_central_differences():
             s = s0.copy()
             for k in STATE:
                 setattr(s, k, getattr(s0, k) + eps * d[k])
-            a = (acts[0] + eps * d["act_c"], acts[1] + eps * d["act_amp"], acts[2], acts[3] + eps * d["act_phase"])
+            a = (acts[0] + eps * d["act_c"], acts[1] + eps * d["act_amp"], acts[2] + eps * d["act_omega"],
+                 acts[3] + eps * d["act_phase"])
             out, _ = A.rollout(s, oc, 0.01, steps, a, ib_positions=ibp)
             return loss(out)
 
@@ -191,7 +194,7 @@ def test_torch_autograd_binding_matches_the_plan():
     pos, vel, th, f = T(sc.position), T(sc.velocity), T(sc.theta), T(sc.f_grid)
     L0, kb, ra = T(sc.rest_lengths), T(sc.bending_stiffness), T(sc.bending_rest_angles)
     c, amp, ph = T(sc.act_c), T(sc.act_amp), T(sc.act_phase)
-    om = torch.as_tensor(sc.act_omega, device=dev)
+    om = T(sc.act_omega)
     out = rollout(pos, vel, th, f, L0, kb, ra, sc.pairs, sc.bending_pairs, cfg_of(oc), 0.01, 6,
                   actuation=(c, amp, om, ph))
     # loss: mean centre-of-mass x displacement
@@ -204,6 +207,11 @@ def test_torch_autograd_binding_matches_the_plan():
     gpos = g["position"].copy()
     gpos[:, 0] -= 1.0 / sc.position.shape[0]
     assert np.allclose(pos.grad.cpu().numpy(), gpos, rtol=1e-6, atol=1e-9)
-    for name, t in (("act_amp", amp), ("act_phase", ph), ("act_c", c), ("rest_lengths", L0), ("f_grid", f)):
+    for name, t in (("act_amp", amp), ("act_omega", om), ("act_phase", ph), ("act_c", c), ("rest_lengths", L0),
+                    ("f_grid", f)):
         assert np.array_equal(t.grad.cpu().numpy(), g[name]), name
     assert ra.grad is None or not ra.grad.abs().sum()
+    # omega given as a plain array takes no gradient
+    out = rollout(pos, vel, th, f, L0, kb, ra, sc.pairs, sc.bending_pairs, cfg_of(oc), 0.01, 2,
+                  actuation=(c, amp, np.asarray(sc.act_omega), ph))
+    out[0].sum().backward()
