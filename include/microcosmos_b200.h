@@ -276,8 +276,9 @@ mc_status mc_steric_potential_noalloc(const float* position, int32_t N, int32_t 
  * O(sqrt(T)) states, compute about three forward rollouts plus the adjoint.
  * Cotangents of the outputs steric and fluid_velocity are taken as zero.
  * Actuation, if given to mc_grad_forward, must have t0 = 0.  Both rod solvers (MC_SOLVER_PBD, MC_SOLVER_COSSERAT) are
- * differentiated, with or without synthetic IB pairs and the force clamp; a fluid lattice
- * other than the domain grid returns MC_ERR_UNSUPPORTED from mc_grad_plan_create. */
+ * differentiated, with or without synthetic IB pairs, the force clamp and a fluid lattice
+ * other than the domain grid (dims->fluid_H/fluid_W; f_grid arrays and cotangents are then
+ * (9, fluid_H, fluid_W)). */
 typedef struct mc_state_cot {
   float* position; /* (N,2) */
   float* velocity; /* (N,2) */

@@ -28,15 +28,21 @@ _F32 = torch.float32
 class GradPlan:
     """One rollout's gradient plan: topology, config, dt, step count and checkpoint interval."""
 
-    def __init__(self, H, W, N, pairs, bending_pairs, cfg, dt, num_steps, checkpoint_every=0, device="cuda"):
+    def __init__(self, H, W, N, pairs, bending_pairs, cfg, dt, num_steps, checkpoint_every=0, device="cuda",
+                 fluid_shape=None):
+        """(H, W) the domain grid; ``fluid_shape`` = (h, w) of the fluid lattice when it
+        differs from the domain grid (f_grid is then (9, h, w))."""
         _require_cuda()
         lib = _lib.load()
         self.pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1, 2)
         self.bpairs = np.ascontiguousarray(bending_pairs, np.int32).reshape(-1, 2)
         self.H, self.W, self.N = int(H), int(W), int(N)
+        self.lH, self.lW = (self.H, self.W) if fluid_shape is None else (int(fluid_shape[0]), int(fluid_shape[1]))
         self.E, self.B = self.pairs.shape[0], self.bpairs.shape[0]
         self.num_steps = int(num_steps)
         dims = _lib.McDims(self.H, self.W, self.N, self.E, self.B)
+        if (self.lH, self.lW) != (self.H, self.W):
+            dims.fluid_H, dims.fluid_W = self.lH, self.lW
         c = mc_config(cfg)
         h = ctypes.c_void_p()
         _lib.check(lib.mc_grad_plan_create(ctypes.byref(dims), ctypes.byref(c), float(dt),
@@ -72,7 +78,7 @@ class GradPlan:
         seeds = [_c(d_position), _c(d_velocity), _c(d_theta), _c(d_f_grid)]  # alive until the call returns
         fin = _lib.McStateCot(*[t.data_ptr() if t is not None else None for t in seeds])
         out = {"position": z(self.N, 2), "velocity": z(self.N, 2), "theta": z(self.E),
-               "f_grid": z(9, self.H, self.W), "rest_lengths": z(self.E), "bending_stiffness": z(self.B)}
+               "f_grid": z(9, self.lH, self.lW), "rest_lengths": z(self.E), "bending_stiffness": z(self.B)}
         if self.has_act:
             out.update(act_c=z(self.B), act_amp=z(self.B), act_omega=z(self.B), act_phase=z(self.B))
         else:
@@ -114,6 +120,7 @@ class _Rollout(torch.autograd.Function):
                 act_c, act_amp, act_omega, act_phase, spec):
         from .engine import Actuation, DeviceState
         H, W, pairs, bpairs, cfg, dt, num_steps, ckpt = spec
+        fluid_shape = (int(f_grid.shape[1]), int(f_grid.shape[2]))
         st = DeviceState.from_arrays(H, W, position.detach(), velocity.detach(), pairs, theta.detach(),
                                      rest_lengths.detach(), bpairs, bending_rest_angles.detach(),
                                      bending_stiffness.detach(), f_grid.detach(), device=position.device)
@@ -121,7 +128,8 @@ class _Rollout(torch.autograd.Function):
         if act_c is not None:
             dev = position.device
             act = Actuation(*[_c(torch.as_tensor(a, device=dev)) for a in (act_c, act_amp, act_omega, act_phase)], 0)
-        plan = GradPlan(H, W, st.N, pairs, bpairs, cfg, dt, num_steps, ckpt, device=position.device)
+        plan = GradPlan(H, W, st.N, pairs, bpairs, cfg, dt, num_steps, ckpt, device=position.device,
+                        fluid_shape=fluid_shape)
         plan.forward(st, act)
         ctx.plan = plan
         ctx.has_act = act is not None
@@ -142,13 +150,14 @@ class _Rollout(torch.autograd.Function):
 
 
 def rollout(position, velocity, theta, f_grid, rest_lengths, bending_stiffness, bending_rest_angles, pairs,
-            bending_pairs, cfg, dt, num_steps, actuation=None, checkpoint_every=0):
+            bending_pairs, cfg, dt, num_steps, actuation=None, checkpoint_every=0, grid_shape=None):
     """Differentiable rollout (torch): returns (position, velocity, theta, f_grid, steric,
     fluid_velocity) after ``num_steps`` steps.  ``actuation`` = (c, amp, omega, phase) per
     bending pair (rest[b](t) = c + amp sin(omega t + phase)); gradients flow to every
-    float tensor argument.  ``f_grid`` is (9, H, W)."""
+    float tensor argument.  ``f_grid`` is (9, h, w) on the fluid lattice; ``grid_shape`` =
+    (H, W) of the domain when it differs from the lattice (Fields.grid_shape)."""
     f_grid = f_grid.reshape(9, *f_grid.shape[-2:])
-    H, W = int(f_grid.shape[1]), int(f_grid.shape[2])
+    H, W = (int(f_grid.shape[1]), int(f_grid.shape[2])) if grid_shape is None else map(int, grid_shape)
     pairs_h = np.ascontiguousarray(pairs.detach().cpu().numpy() if isinstance(pairs, torch.Tensor) else pairs,
                                    np.int32).reshape(-1, 2)
     bp_h = np.ascontiguousarray(bending_pairs.detach().cpu().numpy() if isinstance(bending_pairs, torch.Tensor)

@@ -51,6 +51,7 @@ struct StepArgs {
 
 struct AD {
   int H, W, N, E, B, HW, C, iters, K, KK, steric, fluid, nskip, has_act;
+  int lH, lW, lHW;  // the fluid lattice (f_grid (9, lH, lW)); H, W, HW: the domain grid
   int solver;  // MC_SOLVER_PBD or MC_SOLVER_COSSERAT
   int force_clamp;  // enable_force_clamp: F = F_raw * clamp factor of F_raw
   int NI;      // IB points: N, or 2N with synthetic pairs (point p < N: node p, + side; else node p - N, - side)
@@ -94,21 +95,21 @@ struct AD {
   float* ib_w;    // NI x KK
   float2* sraw;   // iters x NI
   float2* s_tmp;  // NI
-  float* uc;      // 2 x HW
-  float* inv;     // HW
+  float* uc;      // 2 x lHW
+  float* inv;     // lHW
   // CSR over cells
-  int* cnt;    // HW (all zero between builds)
-  int* start;  // HW + 1
+  int* cnt;    // max(HW, lHW) (all zero between builds)
+  int* start;  // max(HW, lHW) + 1
   int* bsum;   // scan block sums
   int* ent;    // entries
   int* touched;   // cells with at least one entry (any order), M entries at most
   int* ntouched;  // their count
   int max_entries;
   // adjoint
-  float* lf0p;   // 9 x HW
-  float* lv;     // 2 x HW
-  float* lrho;   // HW
-  float* luc;    // 2 x HW
+  float* lf0p;   // 9 x lHW
+  float* lv;     // 2 x lHW
+  float* lrho;   // lHW
+  float* luc;    // 2 x lHW
   float2* lnv;   // NI
   float2* lprev;  // N
   float2* lpos;   // N   (state cotangent)
@@ -340,7 +341,7 @@ __global__ void k_ib_weights(AD d) {
       const int q = a * K + b;
       w[q] = px * py;
       s = s + w[q];
-      d.ib_idx[(size_t)n * d.KK + q] = cell_of((int)ny, (int)nx, d.H, d.W);
+      d.ib_idx[(size_t)n * d.KK + q] = cell_of((int)ny, (int)nx, d.lH, d.lW);
     }
   }
   for (int q = 0; q < d.KK; ++q) d.ib_w[(size_t)n * d.KK + q] = w[q] / (s + MC_EPSIL);
@@ -461,13 +462,13 @@ __global__ void k_csr_sort(const int* __restrict__ start, const int* __restrict_
 __global__ void k_macro(AD d) {
   const float* __restrict__ f = d.sa[*d.jp].f;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.HW) return;
+  if (c >= d.lHW) return;
   float r = mc::max_prop(f[c], MC_EPSIL);
   float fv[9];
   fv[0] = r;
 #pragma unroll
   for (int i = 1; i < 9; ++i) {
-    fv[i] = mc::max_prop(f[(size_t)i * d.HW + c], MC_EPSIL);
+    fv[i] = mc::max_prop(f[(size_t)i * d.lHW + c], MC_EPSIL);
     r = r + fv[i];
   }
   const float rho = mc::max_prop(r, 0.1f);
@@ -475,7 +476,7 @@ __global__ void k_macro(AD d) {
   const float uy = (((((fv[2] - fv[4]) + fv[5]) + fv[6]) - fv[7]) - fv[8]) / rho;
   const float c1 = mc::clamp_factor(ux, uy, d.vmax);
   d.uc[c] = ux * c1;
-  d.uc[d.HW + c] = uy * c1;
+  d.uc[d.lHW + c] = uy * c1;
   float cov = 0.0f;
   for (int q = d.start[c]; q < d.start[c + 1]; ++q) cov = cov + d.ib_w[d.ent[q]];
   d.inv[c] = 1.0f / mc::max_prop(cov, 1.0f);
@@ -491,7 +492,7 @@ __global__ void k_ib_interp(AD d, int it) {
     const int c = d.ib_idx[(size_t)n * d.KK + q];
     const float w = d.ib_w[(size_t)n * d.KK + q];
     ix = ix + d.uc[c] * w;
-    iy = iy + d.uc[d.HW + c] * w;
+    iy = iy + d.uc[d.lHW + c] * w;
   }
   const float2 pc = d.pp[(size_t)d.C * d.N + gi], p0 = prev[gi];
   const float v1x = (pc.x - p0.x) / d.dt, v1y = (pc.y - p0.y) / d.dt;
@@ -517,7 +518,7 @@ __global__ void k_ib_spread(AD d) {
   }
   const float iv = d.inv[c];
   d.uc[c] = d.uc[c] + ax * iv;
-  d.uc[d.HW + c] = d.uc[d.HW + c] + ay * iv;
+  d.uc[d.lHW + c] = d.uc[d.lHW + c] + ay * iv;
 }
 
 // ------------------------------------------------------------------ adjoint: stream + collide + F
@@ -533,11 +534,11 @@ __global__ void k_lbm_adj1(AD d) {
   const float* __restrict__ f = a.f;
   const float* __restrict__ lfn = a.lf_in;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.HW) return;
-  const int y = c / d.W, x = c - y * d.W;
+  if (c >= d.lHW) return;
+  const int y = c / d.lW, x = c - y * d.lW;
   float f0[9];
 #pragma unroll
-  for (int i = 0; i < 9; ++i) f0[i] = mc::max_prop(f[(size_t)i * d.HW + c], MC_EPSIL);
+  for (int i = 0; i < 9; ++i) f0[i] = mc::max_prop(f[(size_t)i * d.lHW + c], MC_EPSIL);
   float rr = f0[0];
 #pragma unroll
   for (int i = 1; i < 9; ++i) rr = rr + f0[i];
@@ -546,7 +547,7 @@ __global__ void k_lbm_adj1(AD d) {
   const float uy = ((((f0[2] - f0[4]) + f0[5]) + f0[6]) - f0[7]) - f0[8];
   const float c1 = mc::clamp_factor(ux / rho, uy / rho, d.vmax);
   const float vx = (ux / rho) * c1, vy = (uy / rho) * c1;
-  const float u5x = d.uc[c], u5y = d.uc[d.HW + c];
+  const float u5x = d.uc[c], u5y = d.uc[d.lHW + c];
   const float c2 = mc::clamp_factor(u5x, u5y, d.vmax);
   const float ucx = u5x * c2, ucy = u5y * c2;
   const float Frx = (ucx - vx) * rho, Fry = (ucy - vy) * rho;
@@ -580,7 +581,7 @@ __global__ void k_lbm_adj1(AD d) {
                      d.wm * (half * (f0[i] - f0[o]) - half * (feq[i] - feq[o]));
     const float src = d.cp * (half * (raw[i] + raw[o])) + d.cm * (half * (raw[i] - raw[o]));
     const int xn = x + mc::kEx[i], yn = y + mc::kEy[i];
-    const float lin = lfn[(size_t)i * d.HW + cell_of(yn, xn, d.H, d.W)];
+    const float lin = lfn[(size_t)i * d.lHW + cell_of(yn, xn, d.lH, d.lW)];
     g[i] = (lin * dmaxf(post[i], MC_EPSIL)) * dmaxf(pr + src, MC_EPSIL);
   }
   float lf0[9];
@@ -638,12 +639,12 @@ __global__ void k_lbm_adj1(AD d) {
   lrho += lFx * (ucx - vx) + lFy * (ucy - vy);  // through F_raw = (ucc - v) rho
   const float2 l5 = clamp_vjp(u5x, u5y, d.vmax, lccx, lccy);
   d.luc[c] = l5.x;
-  d.luc[d.HW + c] = l5.y;
+  d.luc[d.lHW + c] = l5.y;
   d.lv[c] = lvx;
-  d.lv[d.HW + c] = lvy;
+  d.lv[d.lHW + c] = lvy;
   d.lrho[c] = lrho;
 #pragma unroll
-  for (int i = 0; i < 9; ++i) d.lf0p[(size_t)i * d.HW + c] = lf0[i];
+  for (int i = 0; i < 9; ++i) d.lf0p[(size_t)i * d.lHW + c] = lf0[i];
 }
 
 __global__ void k_ib_rev_node(AD d, int it) {
@@ -655,7 +656,7 @@ __global__ void k_ib_rev_node(AD d, int it) {
     const float w = d.ib_w[(size_t)n * d.KK + q];
     const float iv = d.inv[c];
     sx = sx + (iv * d.luc[c]) * w;
-    sy = sy + (iv * d.luc[d.HW + c]) * w;
+    sy = sy + (iv * d.luc[d.lHW + c]) * w;
   }
   const float2 r = d.sraw[(size_t)it * d.NI + n];
   const float2 lr = clamp_vjp(r.x, r.y, d.vmax, sx, sy);
@@ -680,7 +681,7 @@ __global__ void k_ib_rev_cell(AD d) {
     ay = ay + s.y * w;
   }
   d.luc[c] = d.luc[c] + ax;
-  d.luc[d.HW + c] = d.luc[d.HW + c] + ay;
+  d.luc[d.lHW + c] = d.luc[d.lHW + c] + ay;
 }
 
 __global__ void k_lbm_adj2(AD d) {
@@ -688,24 +689,24 @@ __global__ void k_lbm_adj2(AD d) {
   const float* __restrict__ f = a.f;
   float* __restrict__ lf_out = a.lf_out;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.HW) return;
+  if (c >= d.lHW) return;
   float f0[9];
 #pragma unroll
-  for (int i = 0; i < 9; ++i) f0[i] = mc::max_prop(f[(size_t)i * d.HW + c], MC_EPSIL);
+  for (int i = 0; i < 9; ++i) f0[i] = mc::max_prop(f[(size_t)i * d.lHW + c], MC_EPSIL);
   float rr = f0[0];
 #pragma unroll
   for (int i = 1; i < 9; ++i) rr = rr + f0[i];
   const float rho = mc::max_prop(rr, 0.1f);
   const float ux = (((((f0[1] - f0[3]) + f0[5]) - f0[6]) - f0[7]) + f0[8]) / rho;
   const float uy = (((((f0[2] - f0[4]) + f0[5]) + f0[6]) - f0[7]) - f0[8]) / rho;
-  const float lvx = d.lv[c] + d.luc[c], lvy = d.lv[d.HW + c] + d.luc[d.HW + c];
+  const float lvx = d.lv[c] + d.luc[c], lvy = d.lv[d.lHW + c] + d.luc[d.lHW + c];
   const float2 lu = clamp_vjp(ux, uy, d.vmax, lvx, lvy);
   const float lrho = d.lrho[c] - (lu.x * ux + lu.y * uy) / rho;
   const float lraw = lrho * dmaxf(rr, 0.1f);
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
-    const float l0 = d.lf0p[(size_t)i * d.HW + c] + lraw + ((float)mc::kEx[i] * lu.x + (float)mc::kEy[i] * lu.y) / rho;
-    lf_out[(size_t)i * d.HW + c] = l0 * dmaxf(f[(size_t)i * d.HW + c], MC_EPSIL);
+    const float l0 = d.lf0p[(size_t)i * d.lHW + c] + lraw + ((float)mc::kEx[i] * lu.x + (float)mc::kEy[i] * lu.y) / rho;
+    lf_out[(size_t)i * d.lHW + c] = l0 * dmaxf(f[(size_t)i * d.lHW + c], MC_EPSIL);
   }
 }
 
@@ -1186,22 +1187,24 @@ T* at(unsigned char* ws, const mc_grad_plan::R& r) {
   return reinterpret_cast<T*>(ws + r.off);
 }
 
-void csr_build(const AD& d, const int* cells, int M, cudaStream_t s) {
-  const int nb = nblk(d.HW, kScanChunk);
+// CSR of M entries over ncells cells (the lattice for the IB stencils, the domain grid for
+// the steric samples)
+void csr_build(const AD& d, const int* cells, int M, int ncells, cudaStream_t s) {
+  const int nb = nblk(ncells, kScanChunk);
   if (M > 0) k_csr_count<<<nblk(M, 256), 256, 0, s>>>(cells, M, d.cnt);
-  k_scan1<<<nb, 1024, 0, s>>>(d.cnt, d.HW, d.start, d.bsum);
+  k_scan1<<<nb, 1024, 0, s>>>(d.cnt, ncells, d.start, d.bsum);
   k_scan2<<<1, 1024, 0, s>>>(d.bsum, nb);
-  k_scan3<<<nblk(d.HW, 256), 256, 0, s>>>(d.start, d.bsum, d.HW, M);
+  k_scan3<<<nblk(ncells, 256), 256, 0, s>>>(d.start, d.bsum, ncells, M);
   if (M > 0) k_csr_fill<<<nblk(M, 256), 256, 0, s>>>(cells, M, d.start, d.cnt, d.ent);
   cudaMemsetAsync(d.ntouched, 0, sizeof(int), s);
-  k_csr_touched<<<nblk(d.HW, 256), 256, 0, s>>>(d.start, d.HW, d.touched, d.ntouched);
+  k_csr_touched<<<nblk(ncells, 256), 256, 0, s>>>(d.start, ncells, d.touched, d.ntouched);
   k_csr_sort<<<nblk(std::max(M, 1), 256), 256, 0, s>>>(d.start, d.touched, d.ntouched, d.ent);
 }
 
 mc_status copy_state_to(mc_grad_plan* p, float* pos, float* vel, float* th, float* f, const float* spos, const float* svel,
                         const float* sth, const float* sf, cudaStream_t s) {
   const mc_dims& D = p->dims;
-  const size_t HW = (size_t)D.H * D.W;
+  const size_t HW = (size_t)p->ad.lHW;  // f_grid lives on the fluid lattice
   GC(cudaMemcpyAsync(pos, spos, (size_t)D.N * 8, cudaMemcpyDeviceToDevice, s));
   GC(cudaMemcpyAsync(vel, svel, (size_t)D.N * 8, cudaMemcpyDeviceToDevice, s));
   if (D.E) GC(cudaMemcpyAsync(th, sth, (size_t)D.E * 4, cudaMemcpyDeviceToDevice, s));
@@ -1209,7 +1212,7 @@ mc_status copy_state_to(mc_grad_plan* p, float* pos, float* vel, float* th, floa
   return MC_OK;
 }
 
-// checkpoint / segment slot layout: pos (2N), vel (2N), theta (E), f (9 HW), each 256-aligned
+// checkpoint / segment slot layout: pos (2N), vel (2N), theta (E), f (9 lHW), each 256-aligned
 struct Slot {
   float *pos, *vel, *th, *f;
 };
@@ -1296,19 +1299,19 @@ void reverse_step(mc_grad_plan* p, cudaStream_t s) {
     k_pbd_fwd<<<d.ncomp, kPbdThreads, 0, s>>>(d);
   if (d.fluid) {
     k_ib_weights<<<nblk(d.NI, TB), TB, 0, s>>>(d);
-    csr_build(d, d.ib_idx, d.NI * d.KK, s);
-    k_macro<<<nblk(d.HW, TB), TB, 0, s>>>(d);
+    csr_build(d, d.ib_idx, d.NI * d.KK, d.lHW, s);
+    k_macro<<<nblk(d.lHW, TB), TB, 0, s>>>(d);
     for (int it = 0; it < d.iters; ++it) {
       k_ib_interp<<<nblk(d.NI, TB), TB, 0, s>>>(d, it);
       k_ib_spread<<<nblk(d.NI * d.KK, TB), TB, 0, s>>>(d);
     }
-    k_lbm_adj1<<<nblk(d.HW, TB), TB, 0, s>>>(d);
+    k_lbm_adj1<<<nblk(d.lHW, TB), TB, 0, s>>>(d);
     cudaMemsetAsync(d.lnv, 0, (size_t)d.NI * 8, s);
     for (int it = d.iters - 1; it >= 0; --it) {
       k_ib_rev_node<<<nblk(d.NI, TB), TB, 0, s>>>(d, it);
       k_ib_rev_cell<<<nblk(d.NI * d.KK, TB), TB, 0, s>>>(d);
     }
-    k_lbm_adj2<<<nblk(d.HW, TB), TB, 0, s>>>(d);
+    k_lbm_adj2<<<nblk(d.lHW, TB), TB, 0, s>>>(d);
   }
   k_node_adj<<<nblk(nNE, TB), TB, 0, s>>>(d);
   if (d.solver == MC_SOLVER_COSSERAT)
@@ -1317,7 +1320,7 @@ void reverse_step(mc_grad_plan* p, cudaStream_t s) {
     k_pbd_rev<<<d.ncomp, kPbdThreads, 0, s>>>(d);
   if (d.steric) {
     k_steric_adj_node<<<nblk(d.N, TB), TB, 0, s>>>(d);
-    csr_build(d, d.st_cell, d.N * 16, s);
+    csr_build(d, d.st_cell, d.N * 16, d.HW, s);
     cudaMemsetAsync(d.lV, 0, (size_t)d.HW * 4, s);
     k_gather_field<<<nblk(d.N * 16, TB), TB, 0, s>>>(d, d.st_val, d.lV);
     // the spectral filter is real and even, so it is its own adjoint: the forward plan's
@@ -1348,8 +1351,10 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   if (cfg->ibm_kernel_size < 1 || cfg->ibm_kernel_size * cfg->ibm_kernel_size > kMaxKK)
     return gfail(MC_ERR_UNSUPPORTED, "ibm_kernel_size outside 1..8");
   if (cfg->synthetic_node_width < 0.0f) return gfail(MC_ERR_INVALID, "synthetic_node_width must be >= 0");
-  if ((D.fluid_H > 0 && D.fluid_H != D.H) || (D.fluid_W > 0 && D.fluid_W != D.W))
-    return gfail(MC_ERR_UNSUPPORTED, "the adjoint needs the fluid grid to be the domain grid");
+  if ((D.fluid_H > 0) != (D.fluid_W > 0) || D.fluid_H < 0 || D.fluid_W < 0)
+    return gfail(MC_ERR_INVALID, "fluid_H and fluid_W must both be 0 (the domain grid) or both > 0");
+  if ((long long)std::max(D.fluid_H, 0) * std::max(D.fluid_W, 0) > (long long)kScanChunk * 4096)
+    return gfail(MC_ERR_UNSUPPORTED, "fluid lattice too large for the gradient path");
   if (cfg->solver_type != MC_SOLVER_PBD && cfg->solver_type != MC_SOLVER_COSSERAT)
     return gfail(MC_ERR_INVALID, "solver_type must be MC_SOLVER_PBD or MC_SOLVER_COSSERAT");
   if (cfg->solver_type == MC_SOLVER_COSSERAT && !(cfg->solver_dt > 0.0))
@@ -1447,6 +1452,8 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   p->fwd_bytes = mc_plan_workspace_bytes(p->fwd);
   // layout
   const size_t N = D.N, E = std::max(D.E, 1), B = std::max(D.B, 1), HW = (size_t)D.H * D.W;
+  const size_t LHW = D.fluid_H > 0 ? (size_t)D.fluid_H * D.fluid_W : HW;  // fluid lattice cells
+  const size_t CHW = std::max(HW, LHW);                                    // CSR cells
   const size_t NI = N * (cfg->enable_fluid && cfg->synthetic_node_width > 0.0f ? 2 : 1);  // IB points
   const int C = cfg->cycles_per_step, KK = cfg->ibm_kernel_size * cfg->ibm_kernel_size;
   const int iters = std::max(cfg->ibm_iterations, 1);
@@ -1477,9 +1484,9 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   take(p->r_wth, E * 4);
   take(p->r_wra, B * 4);
   take(p->r_wst, HW * 4);
-  take(p->r_wfu, 2 * HW * 4);
-  take(p->r_wf, 9 * HW * 4);
-  p->state_ck_bytes = al(N * 8) * 2 + al(E * 4) + al(9 * HW * 4);
+  take(p->r_wfu, 2 * LHW * 4);
+  take(p->r_wf, 9 * LHW * 4);
+  p->state_ck_bytes = al(N * 8) * 2 + al(E * 4) + al(9 * LHW * 4);
   take(p->r_ck, std::max(p->nseg, 1) * p->state_ck_bytes);
   take(p->r_seg, (size_t)S * p->state_ck_bytes);
   take(p->r_segV, (size_t)S * al(HW * 4));
@@ -1491,17 +1498,17 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   take(p->r_ibw, NI * KK * 4);
   take(p->r_sraw, (size_t)iters * NI * 8);
   take(p->r_stmp, NI * 8);
-  take(p->r_uc, 2 * HW * 4);
-  take(p->r_inv, HW * 4);
-  take(p->r_cnt, HW * 4);
-  take(p->r_start, (HW + 1) * 4);
+  take(p->r_uc, 2 * LHW * 4);
+  take(p->r_inv, LHW * 4);
+  take(p->r_cnt, CHW * 4);
+  take(p->r_start, (CHW + 1) * 4);
   take(p->r_bsum, 4096 * 4);
   take(p->r_ent, std::max<size_t>(NI * KK, 16 * N) * 4);
   take(p->r_touch, std::max<size_t>(NI * KK, 16 * N) * 4 + 256);
-  take(p->r_lf0p, 9 * HW * 4);
-  take(p->r_lv, 2 * HW * 4);
-  take(p->r_lrho, HW * 4);
-  take(p->r_luc, 2 * HW * 4);
+  take(p->r_lf0p, 9 * LHW * 4);
+  take(p->r_lv, 2 * LHW * 4);
+  take(p->r_lrho, LHW * 4);
+  take(p->r_luc, 2 * LHW * 4);
   take(p->r_lnv, NI * 8);
   take(p->r_lprev, N * 8);
   take(p->r_lpos, N * 8);
@@ -1532,8 +1539,8 @@ mc_status mc_grad_plan_create(const mc_dims* dims, const mc_config* cfg, float d
   take(p->r_lV, HW * 4);
   take(p->r_ctmp, HW * 4);
   take(p->r_ldep, HW * 4);
-  take(p->r_lf0, 9 * HW * 4);
-  take(p->r_lf1, 9 * HW * 4);
+  take(p->r_lf0, 9 * LHW * 4);
+  take(p->r_lf1, 9 * LHW * 4);
   take(p->r_cns, p->c_nstart.size() * 4);
   take(p->r_cn, std::max<size_t>(p->c_nodes.size(), 1) * 4);
   take(p->r_ces, p->c_estart.size() * 4);
@@ -1605,6 +1612,9 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   d.E = D.E;
   d.B = D.B;
   d.HW = D.H * D.W;
+  d.lH = D.fluid_H > 0 ? D.fluid_H : D.H;
+  d.lW = D.fluid_W > 0 ? D.fluid_W : D.W;
+  d.lHW = d.lH * d.lW;
   d.C = c.cycles_per_step;
   d.iters = c.ibm_iterations;
   d.K = c.ibm_kernel_size;
@@ -1623,12 +1633,14 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   d.force_clamp = c.enable_force_clamp;
   d.NI = D.N * (c.enable_fluid && c.synthetic_node_width > 0.0f ? 2 : 1);
   d.syn_w = c.synthetic_node_width;
-  d.syn_ms = (float)(0.5 * ((double)D.W / D.H + (double)D.H / D.W));
+  // scale = (lW / H, lH / W): the reference's axis order (fluid.py:222-226)
+  const double sxd = (double)d.lW / (double)D.H, syd = (double)d.lH / (double)D.W;
+  d.syn_ms = (float)(0.5 * (sxd + syd));
   d.cos_w = c.solver_type == MC_SOLVER_COSSERAT ? (float)(1.0 / (c.solver_dt * c.solver_dt)) : 0.0f;
-  const float scx = (float)D.W / (float)D.H, scy = (float)D.H / (float)D.W;
+  const float scx = (float)sxd, scy = (float)syd;
   d.scx = scx;
   d.scy = scy;
-  d.vmax = (float)(c.max_fluid_velocity * (0.5 * ((double)D.W / D.H + (double)D.H / D.W)));
+  d.vmax = (float)((double)c.max_fluid_velocity * (0.5 * (sxd + syd)));
   d.relax = c.ibm_relaxation;
   d.mass = c.node_mass;
   {
@@ -1730,6 +1742,7 @@ mc_status mc_grad_forward(mc_grad_plan* p, const mc_state* state, const mc_actua
   cudaStream_t s = (cudaStream_t)stream;
   const mc_dims& D = p->dims;
   const size_t HW = (size_t)D.H * D.W;
+  const size_t LHW = (size_t)p->ad.lHW;  // fluid lattice cells
   unsigned char* w = p->ws;
   auto cp = [&](const mc_grad_plan::R& r, const void* src, size_t n) -> cudaError_t {
     if (n == 0 || !src) return cudaSuccess;
@@ -1747,9 +1760,9 @@ mc_status mc_grad_forward(mc_grad_plan* p, const mc_state* state, const mc_actua
   GC(cp(p->r_wra, state->bending_rest_angles, (size_t)D.B * 4));
   if (state->steric) GC(cp(p->r_wst, state->steric, HW * 4));
   else GC(cudaMemsetAsync(w + p->r_wst.off, 0, HW * 4, s));
-  if (state->fluid_velocity) GC(cp(p->r_wfu, state->fluid_velocity, 2 * HW * 4));
-  else GC(cudaMemsetAsync(w + p->r_wfu.off, 0, 2 * HW * 4, s));
-  GC(cp(p->r_wf, state->f_grid, 9 * HW * 4));
+  if (state->fluid_velocity) GC(cp(p->r_wfu, state->fluid_velocity, 2 * LHW * 4));
+  else GC(cudaMemsetAsync(w + p->r_wfu.off, 0, 2 * LHW * 4, s));
+  GC(cp(p->r_wf, state->f_grid, 9 * LHW * 4));
   p->has_act = act != nullptr;
   if (act) {
     if (D.B && (!act->c || !act->amp || !act->omega || !act->phase)) return gfail(MC_ERR_INVALID, "null actuation array");
@@ -1779,8 +1792,8 @@ mc_status mc_grad_forward(mc_grad_plan* p, const mc_state* state, const mc_actua
   GC(back(state->theta, p->r_wth, (size_t)D.E * 4));
   GC(back(state->bending_rest_angles, p->r_wra, (size_t)D.B * 4));
   GC(back(state->steric, p->r_wst, HW * 4));
-  GC(back(state->fluid_velocity, p->r_wfu, 2 * HW * 4));
-  GC(back(state->f_grid, p->r_wf, 9 * HW * 4));
+  GC(back(state->fluid_velocity, p->r_wfu, 2 * LHW * 4));
+  GC(back(state->f_grid, p->r_wf, 9 * LHW * 4));
   GC(cudaGetLastError());
   p->have_forward = true;
   return MC_OK;
@@ -1795,6 +1808,7 @@ mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_st
   cudaStream_t s = (cudaStream_t)stream;
   const mc_dims& D = p->dims;
   const size_t HW = (size_t)D.H * D.W;
+  const size_t LHW = (size_t)p->ad.lHW;  // fluid lattice cells
   unsigned char* w = p->ws;
   AD& d = p->ad;
   auto seed = [&](const mc_grad_plan::R& r, const float* src, size_t n) -> cudaError_t {
@@ -1805,7 +1819,7 @@ mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_st
   GC(seed(p->r_lpos, final_cot->position, (size_t)D.N * 8));
   GC(seed(p->r_lvel, final_cot->velocity, (size_t)D.N * 8));
   GC(seed(p->r_lth, final_cot->theta, (size_t)D.E * 4));
-  GC(seed(p->r_lf0, final_cot->f_grid, 9 * HW * 4));
+  GC(seed(p->r_lf0, final_cot->f_grid, 9 * LHW * 4));
   for (const mc_grad_plan::R* r : {&p->r_dc, &p->r_da, &p->r_dp, &p->r_do, &p->r_dr, &p->r_dl, &p->r_dk})
     GC(cudaMemsetAsync(w + r->off, 0, r->bytes, s));
   if (d.steric && !p->filter_ready) {
@@ -1834,7 +1848,7 @@ mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_st
         st = mc::rollout_snapshot_f(p->fwd, sj.f, s);
         if (st != MC_OK) return st;
       } else {
-        GC(cudaMemcpyAsync(sj.f, at<float>(w, p->r_wf), 9 * HW * 4, cudaMemcpyDeviceToDevice, s));
+        GC(cudaMemcpyAsync(sj.f, at<float>(w, p->r_wf), 9 * LHW * 4, cudaMemcpyDeviceToDevice, s));
       }
       st = mc_rollout_advance(p->fwd, 1, 1, 1, s);
       if (st != MC_OK) return st;
@@ -1891,7 +1905,7 @@ mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_st
   GC(out(initial_cot->position, p->r_lpos, (size_t)D.N * 8));
   GC(out(initial_cot->velocity, p->r_lvel, (size_t)D.N * 8));
   GC(out(initial_cot->theta, p->r_lth, (size_t)D.E * 4));
-  GC(out(initial_cot->f_grid, lfcur ? p->r_lf1 : p->r_lf0, 9 * HW * 4));
+  GC(out(initial_cot->f_grid, lfcur ? p->r_lf1 : p->r_lf0, 9 * LHW * 4));
   if (grads) {
     GC(out(grads->act_c, p->r_dc, (size_t)D.B * 4));
     GC(out(grads->act_amp, p->r_da, (size_t)D.B * 4));

@@ -78,7 +78,7 @@ def _ib_tape(H, W, pos, vel, f_grid, cfg, dtstep, ib_positions, pairs=None):
     carrying its node's velocity; a node's reaction is the mean of its two points'."""
     dt = f_grid.dtype
     t = dt.type
-    h, w = H, W
+    h, w = f_grid.shape[1], f_grid.shape[2]  # the fluid lattice; (H, W) is the domain grid
     scale = np.array([w / H, h / W], dtype=dt)
     vmax = cfg.max_fluid_velocity * 0.5 * (w / H + h / W)
     eps = t(R.EPSIL32)
@@ -267,11 +267,13 @@ def _scatter(n_cells, idx, wts, node_vals):
 
 
 def ib_vjp(H, W, cfg, dtstep, tp, lvel_out, lf_new):
-    """Cotangents of (vel1, f_grid) through _ib_tape's (vel_out, f_new)."""
+    """Cotangents of (vel1, f_grid) through _ib_tape's (vel_out, f_new).  Everything here
+    lives on the fluid lattice, whose shape is the tape's f_grid's."""
     dt = lf_new.dtype
     t = dt.type
     eps = t(R.EPSIL32)
     idx, wts, inv = tp["idx"], tp["wts"], tp["inv"]
+    H, W = tp["f"].shape[1], tp["f"].shape[2]
     HW = H * W
     # node reaction: vel_out = vel1 - (nf / m) / sdt
     lvel1 = lvel_out.copy()

@@ -134,8 +134,8 @@ def test_rod_solver_selection(lib):
 
 
 def test_gradient_plan_scope(lib):
-    """mc_grad_plan_create (host-only) takes both rod solvers and synthetic IB pairs; a
-    fluid lattice other than the domain grid has no adjoint and is refused as such."""
+    """mc_grad_plan_create (host-only) takes both rod solvers, synthetic IB pairs and a
+    fluid lattice other than the domain grid; a half-given lattice shape is refused."""
     import dataclasses
     from microcosmos_b200 import COSSERAT_SCHEME, PBD_SCHEME
     from microcosmos_b200.engine import mc_config
@@ -159,7 +159,9 @@ def test_gradient_plan_scope(lib):
     assert create(dataclasses.replace(COSSERAT_SCHEME, dt=0.0)) == _lib.MC_ERR_INVALID
     assert create(dataclasses.replace(PBD_SCHEME, synthetic_node_width=0.5)) == _lib.MC_OK
     assert create(dataclasses.replace(COSSERAT_SCHEME, synthetic_node_width=0.5)) == _lib.MC_OK
-    assert create(PBD_SCHEME, fluid=(16, 16)) == _lib.MC_ERR_UNSUPPORTED
+    assert create(PBD_SCHEME, fluid=(16, 16)) == _lib.MC_OK
+    assert create(PBD_SCHEME, fluid=(48, 40)) == _lib.MC_OK
+    assert create(PBD_SCHEME, fluid=(16, 0)) == _lib.MC_ERR_INVALID
 
 
 def test_batch_plan_of_uneven_rollouts(lib):

@@ -27,8 +27,14 @@ def _loss(s, cot):
             + np.sum(s.theta * cot["theta"]) + np.sum(s.f_grid * cot["f_grid"]))
 
 
-def _check(cfg, H=16, W=20, F=2, n=7, steps=3, seed=0, h=1e-6, tol=2e-6, ndir=3):
+def _check(cfg, H=16, W=20, F=2, n=7, steps=3, seed=0, h=1e-6, tol=2e-6, ndir=3, lattice=None):
     s0, act = _state(H, W, F, n, seed)
+    if lattice is not None:
+        # the fluid on its own (h, w) lattice (Fields.grid_shape stays (H, W))
+        rng = np.random.default_rng(seed + 200)
+        u = rng.normal(0, 2e-2, (2,) + lattice)
+        s0.f_grid = O.equilibrium(np.ones(lattice), u[0], u[1])
+        s0.fluid_velocity = np.zeros((2,) + lattice)
     dt = 0.01
     sT, tapes = A.rollout(s0, cfg, dt, steps, act)
     ibp = A.ib_positions_of(tapes)
@@ -92,6 +98,13 @@ def test_vjp_force_clamp():
     # relaxation to act (here at 2-4 cells per step)
     _check(dataclasses.replace(O.Config(), enable_force_clamp=True, max_fluid_velocity=0.004, ibm_relaxation=1.0),
            steps=3, seed=6)
+
+
+def test_vjp_fluid_lattice_finer_and_coarser():
+    # f_grid on a lattice other than the domain grid: scale = (w / H, h / W) into the
+    # lattice, the velocity cap and synthetic offsets by the mean scale
+    _check(O.Config(), lattice=(24, 30), steps=3, seed=7)
+    _check(O.Config(synthetic_node_width=0.5), lattice=(12, 14), steps=3, seed=8)
 
 
 def test_vjp_synthetic_ib_pairs():

@@ -47,7 +47,8 @@ def cotangent(sc, seed):
 def gpu_grads(sc, oc, steps, cot, ckpt=0, act=True):
     st = DeviceState.from_scenario(sc)
     a = Actuation.from_scenario(sc) if act else None
-    plan = GradPlan(sc.H, sc.W, st.N, sc.pairs, sc.bending_pairs, cfg_of(oc), 0.01, steps, ckpt)
+    plan = GradPlan(sc.H, sc.W, st.N, sc.pairs, sc.bending_pairs, cfg_of(oc), 0.01, steps, ckpt,
+                    fluid_shape=sc.f_grid.shape[1:])
     plan.forward(st, a)
     g = plan.backward(*[torch.as_tensor(cot[k], device="cuda") for k in STATE])
     torch.cuda.synchronize()
@@ -96,6 +97,30 @@ def test_adjoint_matches_gradient_oracle(name):
         e32 = O.rel_l2(g[k], g32[k])
         e64 = O.rel_l2(g[k], g64[k])
         print(f"{name} d/d{k}: rel-L2 {e32:.2e} vs float32 oracle, {e64:.2e} vs float64 oracle")
+        assert np.isfinite(g[k]).all()
+        assert e32 <= GRAD_TOL, (k, e32)
+
+
+@pytest.mark.parametrize("lattice,name", [((48, 64), "full"), ((16, 20), "full"), ((36, 40), "cosserat_synthetic")])
+def test_adjoint_on_a_fluid_lattice_other_than_the_domain(lattice, name):
+    """f_grid on its own lattice (finer, coarser; Fields.grid_shape stays 24 x 32)."""
+    oc = CONFIGS[name]
+    sc = case(24, 32, 2, 8, seed=3)
+    rng = np.random.default_rng(33)
+    u = rng.normal(0, 2e-2, (2,) + lattice).astype(np.float32)
+    sc.f_grid = scenarios.equilibrium(np.ones(lattice, np.float32), u[0], u[1])
+    sc.fluid_velocity = np.zeros((2,) + lattice, np.float32)
+    cot = cotangent(sc, 3)
+    steps = 4
+    fin, g = gpu_grads(sc, oc, steps, cot)
+    sT32, g32 = oracle_grads(sc, oc, steps, cot, np.float32)
+    _, g64 = oracle_grads(sc, oc, steps, cot, np.float64)
+    assert g["f_grid"].shape == (9,) + lattice
+    assert O.rel_l2(fin["position"], sT32.position) < 1e-5
+    for k in g32:
+        e32 = O.rel_l2(g[k], g32[k])
+        print(f"lattice {lattice} {name} d/d{k}: rel-L2 {e32:.2e} vs float32 oracle, "
+              f"{O.rel_l2(g[k], g64[k]):.2e} vs float64")
         assert np.isfinite(g[k]).all()
         assert e32 <= GRAD_TOL, (k, e32)
 
