@@ -8,7 +8,7 @@ from .structs import Edges, Fields, Nodes
 
 __all__ = ["ConstraintSolverConfig", "PBD_SCHEME", "PBD_SCHEME_NO_FLUID", "COSSERAT_SCHEME",
            "COSSERAT_SCHEME_NO_FLUID", "baseline_config", "pbd_rod_constraint", "stable_cosserat_constraint",
-           "Nodes", "Edges", "Fields", "simulate", "step", "run"]
+           "Nodes", "Edges", "Fields", "simulate", "step", "run", "MicrocosmosEnv"]
 
 
 def __getattr__(name):
@@ -16,4 +16,7 @@ def __getattr__(name):
     if name in ("simulate", "step", "run"):
         from . import simulate as _s
         return getattr(_s, name)
+    if name == "MicrocosmosEnv":
+        from .env import MicrocosmosEnv
+        return MicrocosmosEnv
     raise AttributeError(name)

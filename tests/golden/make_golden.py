@@ -116,7 +116,7 @@ def save(name, **arrs):
     print("wrote", path, sum(v.nbytes for v in arrs.values()), "bytes")
 
 
-GROUPS = ("base", "cosserat", "synthetic", "gym", "render", "fluidgrid", "worm")
+GROUPS = ("base", "cosserat", "synthetic", "gym", "render", "fluidgrid", "worm", "env")
 
 
 def main(ref_root, groups=GROUPS):
@@ -135,6 +135,32 @@ def main(ref_root, groups=GROUPS):
         fluidgrid_cases(R)
     if "worm" in groups:
         worm_case(R)
+    if "env" in groups:
+        env_cases(R)
+
+
+def env_cases(R):
+    """MicrocosmosEnv (src/microcosmos/env.py): the chain and loop factories, then the
+    env's rollout (PBD_SCHEME, dt 0.05) and one step of the fluid-free preset."""
+    import microcosmos.env as E
+    specs = [("env_chain_32x40", E.MicrocosmosEnv(grid_shape=(32, 40), num_steps=5), "chain", 10, 2.0, "rollout"),
+             ("env_loop_48x48", E.MicrocosmosEnv(grid_shape=(48, 48), num_steps=4), "loop", 16, 1.5, "rollout"),
+             ("env_loop_nofluid_24x24", E.MicrocosmosEnv.no_fluid(grid_shape=(24, 24), num_steps=3), "loop", 9, 2.0,
+              "step")]
+    for name, env, kind, n, spacing, run in specs:
+        nodes, edges = (env.make_chain if kind == "chain" else env.make_loop)(n, spacing=spacing)
+        out = dict(H=np.int32(env.grid_shape[0]), W=np.int32(env.grid_shape[1]), dt=np.float32(env.dt),
+                   num_steps=np.int32(env.num_steps), num_nodes=np.int32(n), spacing=np.float32(spacing),
+                   no_fluid=np.bool_(not env.solver_config.enable_fluid),
+                   in_color_bend=A(nodes.color_bend), **state_arrays("in_", nodes, edges, env.fields))
+        if run == "rollout":
+            nts, fts = env.rollout(nodes, edges)
+            out.update(ts_position=A(nts.position), ts_velocity=A(nts.velocity), ts_steric=A(fts.steric),
+                       ts_fluid_velocity=A(fts.fluid_velocity))
+        else:
+            n1, e1, f1 = env.step(nodes, edges)
+            out.update(**state_arrays("out_", n1, e1, f1))
+        save(name, **out)
 
 
 def base_cases(R):
@@ -512,6 +538,6 @@ def worm_case(R):
 
 
 if __name__ == "__main__":
-    # usage: make_golden.py [reference root] [group,group,...]  (groups: base, cosserat, synthetic)
+    # usage: make_golden.py [reference root] [group,group,...]  (groups: GROUPS)
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     main(root, tuple(sys.argv[2].split(",")) if len(sys.argv) > 2 else GROUPS)
