@@ -4,8 +4,8 @@
 //
 // Scatter-adds are never done with float atomics.  Each contribution k (IB: k = n*K*K + s,
 // CIC: k = corner*N + n — the order in which the reference's scatters apply them) is
-// appended to the bin of its 16x16-cell tile (an integer atomic picks the slot; a full
-// bin spills to an overflow list).  One CTA per tile then counting-sorts the bin by cell,
+// appended to the bin of its 16x16-cell tile with its cell's position in the tile packed
+// above it (an integer atomic picks the slot; a full bin spills to an overflow list).  One CTA per tile then counting-sorts the bin by cell,
 // orders each cell's run by k and sums it sequentially — the reference's in-order
 // scatter-add, bit-reproducibly.  The IB iterations work on the compact list of touched
 // cells ("heads") instead of full (H, W) grids.
@@ -157,8 +157,9 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
     // counting sort by local cell; positions inside a cell come from shared atomics
     // (arbitrary order), so each cell's run is then ordered by k
     for (int i = tid; i < total; i += blockDim.x) {
-      const int k = bin[i];
-      const unsigned lc = local_of(v, v.cell[k]);
+      const unsigned e = (unsigned)bin[i];  // (local cell << 24) | k
+      const unsigned lc = e >> 24;
+      const int k = (int)(e & 0xffffffu);
       const int pos = atomicAdd(cnt + lc, 1);
       lr[i] = (lc << 24) | (unsigned)pos;
       kin[i] = k;
@@ -259,10 +260,7 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
   unsigned* bufA = reinterpret_cast<unsigned*>(v.store) + base;
   unsigned* bufB = bufA + total;
   const int nbin = min(total, v.cap);
-  for (int i = tid; i < nbin; i += blockDim.x) {
-    const int k = bin[i];
-    bufB[i] = (local_of(v, v.cell[k]) << 24) | (unsigned)k;
-  }
+  for (int i = tid; i < nbin; i += blockDim.x) bufB[i] = (unsigned)bin[i];  // already (local << 24) | k
   if (tid == 0) s_fill = nbin;
   __syncthreads();
   if (total > v.cap) {

@@ -206,6 +206,12 @@ __device__ __forceinline__ float2 min_image(float ax, float ay, float bx, float 
   return make_float2(fmod_floor((ax - bx) + hx, W) - hx, fmod_floor((ay - by) + hy, H) - hy);
 }
 
+// A bin entry: contribution index k (< 2^24) with its cell's position inside the 16 x 16
+// bin tile in the top 8 bits, so the tile kernel sorts without looking the cell up.
+__device__ __forceinline__ int bin_entry(int cy, int cx, int k) {
+  return (int)((((unsigned)(cy % kBinTile) * kBinTile + (unsigned)(cx % kBinTile)) << 24) | (unsigned)k);
+}
+
 // Stable-Cosserat pull of an edge angle toward its segment's direction (sx, sy):
 // th + wrap(atan2(sy, sx) - th) * 0.05 (solver/stable_cosserat.py:55-82)
 __device__ __forceinline__ float cos_pull(float th, float sx, float sy) {

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256) k_predict(const RDesc* __restrict__ D, co
     const int g = first[c];
     const int pos = base[g] + rank[g]++;
     if (pos < d.c_cap) {
-      d.c_store[(size_t)tile[c] * d.c_cap + pos] = k;
+      d.c_store[(size_t)tile[c] * d.c_cap + pos] = bin_entry(cy[c], cx[c], k);
     } else {
       d.c_ovf[atomicAdd(d.c_ctl, 1)] = k;
     }
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(256) k_stencil(const RDesc* __restrict__ D, co
             if (pos == 0) d.wl_ib[atomicAdd(d.wl_ctl, 1)] = make_int2(d.ridx, tile);
           }
           if (pos < cap) {
-            d.ib_store[(size_t)tile * cap + pos] = k;
+            d.ib_store[(size_t)tile * cap + pos] = bin_entry(cy[b], cx[a], k);
           } else {
             d.ib_ovf[atomicAdd(d.ib_ctl, 1)] = k;
           }
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(256) k_stencil16(const RDesc* __restrict__ D, 
   base = __shfl_sync(group, base, leader);
   const int pos = base + __popc(group & ((1u << lane) - 1u));
   if (pos < d.ib_cap) {
-    d.ib_store[(size_t)tile * d.ib_cap + pos] = k;
+    d.ib_store[(size_t)tile * d.ib_cap + pos] = bin_entry(cy, cx, k);
   } else {
     d.ib_ovf[atomicAdd(d.ib_ctl, 1)] = k;
   }
