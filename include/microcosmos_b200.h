@@ -177,7 +177,7 @@ mc_status mc_plan_set_bin_threads(mc_plan* plan, int32_t threads);
 int32_t mc_plan_bin_threads(const mc_plan* plan);
 
 /* Contributions a touched tile may hold to be sorted in shared memory (a power of two in
- * 256..8192, capped by the plan's bin capacity; 0 = 1024).  Denser tiles sort in a global
+ * 256..8192, capped by the plan's bin capacity; 0 = 2048).  Denser tiles sort in a global
  * arena.  Smaller capacities keep more CTAs resident.  Results do not depend on it.  Only
  * before mc_plan_bind().  No counterpart in the reference. */
 mc_status mc_plan_set_bin_sort_capacity(mc_plan* plan, int32_t entries);

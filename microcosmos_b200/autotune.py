@@ -27,7 +27,7 @@ from .engine import DeviceState, Plan
 CELLS_PER_LANE = (1, 2, 4)
 ROWS_PER_CTA = (2, 4, 8)
 FFT_VALUES = (4, 8, 16)
-BIN_SHAPES = ((256, 1024), (128, 1024), (128, 512), (256, 512))  # (threads per CTA, shared sort capacity)
+BIN_SHAPES = ((128, 2048), (256, 2048), (128, 1024), (256, 1024), (128, 512))  # (threads per CTA, shared sort capacity)
 
 _cache: dict[str, tuple[dict, dict]] = {}
 
@@ -71,7 +71,7 @@ def _time(scratch, cfgs, dts, actuations, steps, warmup, **shape):
 def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, fft_values=None, use_cache=True):
     """Time ``steps`` graph-replayed steps of the plan for the candidate shapes and return
     ``(best, timings)``: best = {"lbm_shape": (cells_per_lane, rows_per_cta),
-    "fft_values": 4 | 8 | 16, "bin_threads": 128 | 256, "bin_sort_capacity": 512 | 1024},
+    "fft_values": 4 | 8 | 16, "bin_threads": 128 | 256, "bin_sort_capacity": 512 | 1024 | 2048},
     timings = {label: ms per step}.  The caller's states are
     not modified."""
     key = signature(states, cfgs, dts)

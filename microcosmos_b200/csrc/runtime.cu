@@ -37,6 +37,8 @@ mc_status cuda_fail(cudaError_t e, const char* where) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+constexpr int kDefaultSortCap = 2048;  // contributions per tile sorted in shared memory by default
+
 enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16, K_FR12, K_FC12, K_COUNT };
 
 // CTAs of the steric filter kernels for one rollout: the radix-16 register kernels for
@@ -1134,11 +1136,13 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       p->ib_capS = std::max(p->ib_capS, h.ib_cap);
       p->c_capS = std::max(p->c_capS, h.c_cap);
     }
-    // at most 1024 contributions per tile are sorted in shared memory (16 KB per CTA): one
-    // dense rollout of a batch (whose bins are sized for its density) must not cut the
-    // residency of every CTA of the launch; its denser tiles sort in the global arena
-    p->ib_smem = std::min(p->ib_capS, 1024);
-    p->c_smem = std::min(p->c_capS, 1024);
+    // up to 2048 contributions per tile are sorted in shared memory (32 KB per CTA, and only
+    // when some rollout's bins are that deep: sparse plans keep their 1024-entry bins): the
+    // dense rollouts of a batch then rarely take the global-arena sort, while the residency
+    // of the launch's CTAs is not cut further (measured: 2.05 vs 2.10 ms per step of the
+    // 256-rollout batch against 1024, 2.23 ms at 4096)
+    p->ib_smem = std::min(p->ib_capS, kDefaultSortCap);
+    p->c_smem = std::min(p->c_capS, kDefaultSortCap);
   }
   p->ws_bytes = lay.cur;
   // CTA offset tables
@@ -1222,8 +1226,8 @@ mc_status mc_plan_set_bin_sort_capacity(mc_plan* p, int32_t entries) {
   if (!p) return fail(MC_ERR_INVALID, "null plan");
   if (p->bound) return fail(MC_ERR_INVALID, "the tile sort capacity is set before mc_plan_bind()");
   if (entries != 0 && (entries < 256 || entries > 8192 || (entries & (entries - 1))))
-    return fail(MC_ERR_INVALID, "entries must be 0 (default 1024) or a power of two in 256..8192");
-  const int e = entries ? entries : 1024;
+    return fail(MC_ERR_INVALID, "entries must be 0 (default 2048) or a power of two in 256..8192");
+  const int e = entries ? entries : kDefaultSortCap;
   p->ib_smem = std::min(p->ib_capS, e);
   p->c_smem = std::min(p->c_capS, e);
   return MC_OK;

@@ -224,7 +224,7 @@ class Plan:
         FFT), 1 = FFT, 2 = direct convolution.  ``fft_values``: values per thread of the
         power-of-two FFT kernels (4, 8, 16; 0 = the library's choice).  ``bin_threads``:
         threads per CTA of the contribution-sorting tile kernel (64, 128, 256; 0 = 128).
-        ``bin_sort_capacity``: contributions per tile sorted in shared memory (0 = 1024)."""
+        ``bin_sort_capacity``: contributions per tile sorted in shared memory (0 = 2048)."""
         _require_cuda()
         lib = _lib.load()
         n = len(specs)

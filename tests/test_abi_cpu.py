@@ -214,9 +214,14 @@ def test_tile_kernel_threads_setter(lib):
     assert lib.mc_plan_set_bin_threads(h, 96) == _lib.MC_ERR_INVALID
     assert lib.mc_plan_set_fft_values_per_thread(h, 8) == _lib.MC_OK and lib.mc_plan_fft_values_per_thread(h) == 8
     assert lib.mc_plan_set_fft_values_per_thread(h, 5) == _lib.MC_ERR_INVALID
+    # default 2048, capped by the plan's bin capacity (1024 for this sparse rollout)
     assert lib.mc_plan_bin_sort_capacity(h) == 1024
     assert lib.mc_plan_set_bin_sort_capacity(h, 512) == _lib.MC_OK and lib.mc_plan_bin_sort_capacity(h) == 512
     assert lib.mc_plan_set_bin_sort_capacity(h, 300) == _lib.MC_ERR_INVALID
+    lib.mc_plan_destroy(h)
+    dense = scenarios.make_scenario(32, 32, 8, 60, seed=0)  # 480 nodes on 4 tiles: deep bins
+    st, h = _create([(32, 32, dense.N, dense.pairs, dense.bending_pairs, baseline_config(), 0.01)])
+    assert st == _lib.MC_OK and lib.mc_plan_bin_sort_capacity(h) == 2048
     lib.mc_plan_destroy(h)
 
 
