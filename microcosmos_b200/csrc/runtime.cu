@@ -37,6 +37,13 @@ mc_status cuda_fail(cudaError_t e, const char* where) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// CTAs of the tile kernel: they walk the list of touched tiles.  Up to 16 times the CTAs
+// the SMs hold at once (148 SMs x 8 of 256 threads' worth), so that the block scheduler
+// keeps balancing uneven tiles to the end (measured on the 256-rollout batch: 2.025 ms per
+// step with 1x, 2.01 with 2x, 2.00 with 4x, 1.988 with 16x, 2.02 with one CTA per tile).
+long long tile_grid_cap(int threads) { return 148LL * 8 * 16 * (256 / threads); }
+int tile_grid_for(long long tiles, int threads) { return (int)std::max(1LL, std::min(tiles, tile_grid_cap(threads))); }
+
 constexpr int kDefaultSortCap = 2048;  // contributions per tile sorted in shared memory by default
 
 enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16, K_FR12, K_FC12, K_COUNT };
@@ -1131,7 +1138,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     p->r_wl_cic = lay.take((size_t)tiles * sizeof(int2));
     tiles = std::max(tiles, ltiles);
     p->n_tiles = tiles;
-    p->tile_grid = (int)std::max(1LL, std::min(tiles, 148LL * 8 * (256 / p->bin_threads)));
+    p->tile_grid = tile_grid_for(tiles, p->bin_threads);
     for (auto& h : p->R) {
       p->ib_capS = std::max(p->ib_capS, h.ib_cap);
       p->c_capS = std::max(p->c_capS, h.c_cap);
@@ -1215,7 +1222,7 @@ mc_status mc_plan_set_bin_threads(mc_plan* p, int32_t threads) {
   if (threads != 0 && threads != 64 && threads != 128 && threads != 256)
     return fail(MC_ERR_INVALID, "threads must be 0 (default), 64, 128 or 256");
   p->bin_threads = threads ? threads : 128;
-  p->tile_grid = (int)std::max(1LL, std::min(p->n_tiles, 148LL * 8 * (256 / p->bin_threads)));
+  p->tile_grid = tile_grid_for(p->n_tiles, p->bin_threads);
   return MC_OK;
 }
 
