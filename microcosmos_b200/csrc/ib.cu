@@ -774,8 +774,8 @@ cudaError_t tiles_set_smem(size_t bytes) {
   return cudaFuncSetAttribute(k_bin_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(bytes - a.sharedSizeBytes));
 }
-void launch_ib_interp(const Launch& L, int it) { k_ib_interp<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
-void launch_ib_spread(const Launch& L, int it) { k_ib_spread<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, it); }
+void launch_ib_interp(const Launch& L, int it) { k_ib_interp<<<L.grid, kNodeThreads, 0, L.s>>>(L.d, L.off, L.n, it); }
+void launch_ib_spread(const Launch& L, int it) { k_ib_spread<<<L.grid, kHeadThreads, 0, L.s>>>(L.d, L.off, L.n, it); }
 cudaError_t launch_ib_coop(const Launch& L, int parity) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(L.grid);
@@ -794,9 +794,11 @@ cudaError_t ib_coop_blocks_per_sm(int* out) {
 }
 
 void launch_ib_finalize(const Launch& L, int parity) {
-  k_ib_finalize<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, parity);
+  k_ib_finalize<<<L.grid, kHeadThreads, 0, L.s>>>(L.d, L.off, L.n, parity);
 }
-void launch_reaction(const Launch& L, const int* tdev) { k_reaction<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, tdev); }
+void launch_reaction(const Launch& L, const int* tdev) {
+  k_reaction<<<L.grid, kNodeThreads, 0, L.s>>>(L.d, L.off, L.n, tdev);
+}
 void launch_record_fields(const Launch& L, const int* tdev) {
   k_record_fields<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n, tdev);
 }

@@ -1163,14 +1163,14 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     // node kernels cover the IB points too (twice the nodes with synthetic pairs); the
     // node-only kernels return for indices >= N
     const long long npts = (long long)h.dims.N * (c.synthetic_node_width > 0.0f ? 2 : 1);
-    cnt[K_NODES] = div_up(npts, 256);
+    cnt[K_NODES] = div_up(npts, mc::kNodeThreads);
     cnt[K_NODES16] = div_up(16LL * npts, 256);
     // fused IB kernel: one thread per touched-cell candidate / 4 (scaled down at bind if
     // the plan's CTAs would not all be resident)
     cnt[K_IBCOOP] = c.enable_fluid ? std::max(1, div_up(h.M, 1024)) : 0;
     cnt[K_COMP] = h.dims.N > 0 ? (int)h.generic_comp.size() : 0;
     cnt[K_CHAIN] = h.dims.N > 0 ? div_up((long long)h.chain_comp.size(), 4) : 0;
-    cnt[K_IB] = div_up(h.M, 256);  // touched cells: at most M, one thread each
+    cnt[K_IB] = div_up(h.M, mc::kHeadThreads);  // touched cells: at most M, one thread each
     cnt[K_TILES] = h.ntx * h.nty;
     cnt[K_LBM] = c.enable_fluid ? h.lbm_tx * h.lbm_ty : 0;
     cnt[K_CELLS] = std::min(div_up(HW, 256), 1024);
