@@ -164,7 +164,7 @@ extern "C" mc_status mc_steric_potential_noalloc(const float* position, int32_t 
   d.wl_ctl = reinterpret_cast<int*>(P(kOffWlCtl));
 
   // CTA offset tables of the four kernels: deposit (nodes), bin tiles, FFT rows, FFT columns
-  const int cnt[4] = {(N + 255) / 256, d.ntile_x * d.ntile_y, (H + 1) / 2,
+  const int cnt[4] = {(N + mc::kNodeThreads - 1) / mc::kNodeThreads, d.ntile_x * d.ntile_y, (H + 1) / 2,
                       (W + 2 * mc::kFftColsPerCta - 1) / (2 * mc::kFftColsPerCta)};
   const int offs[8] = {0, cnt[0], 0, cnt[1], 0, cnt[2], 0, cnt[3]};
   std::vector<float2> twW, twH;
