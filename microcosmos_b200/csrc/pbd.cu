@@ -723,7 +723,8 @@ __global__ void k_node(const RDesc* __restrict__ D, const int* __restrict__ off,
 void launch_predict(const Launch& L) { k_predict<<<L.grid, kNodeThreads, 0, L.s>>>(L.d, L.off, L.n); }
 void launch_steric(const Launch& L) { k_steric<<<L.grid, kNodeThreads, 0, L.s>>>(L.d, L.off, L.n); }
 void launch_stencil(const Launch& L) { k_stencil<<<L.grid, kNodeThreads, 0, L.s>>>(L.d, L.off, L.n); }
-void launch_stencil16(const Launch& L) { k_stencil16<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }
+// 8 IB points (16 lanes each) per 128-thread CTA (measured 0.5% faster steps than 16 per 256)
+void launch_stencil16(const Launch& L) { k_stencil16<<<L.grid, 128, 0, L.s>>>(L.d, L.off, L.n); }
 void launch_node(const Launch& L, const int* tdev, size_t smem, int bs) {
   k_node<<<L.grid, bs, smem, L.s>>>(L.d, L.off, L.n, tdev);
 }

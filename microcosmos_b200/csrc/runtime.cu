@@ -1164,7 +1164,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     // node-only kernels return for indices >= N
     const long long npts = (long long)h.dims.N * (c.synthetic_node_width > 0.0f ? 2 : 1);
     cnt[K_NODES] = div_up(npts, mc::kNodeThreads);
-    cnt[K_NODES16] = div_up(16LL * npts, 256);
+    cnt[K_NODES16] = div_up(16LL * npts, 128);
     // fused IB kernel: one thread per touched-cell candidate / 4 (scaled down at bind if
     // the plan's CTAs would not all be resident)
     cnt[K_IBCOOP] = c.enable_fluid ? std::max(1, div_up(h.M, 1024)) : 0;
