@@ -20,6 +20,9 @@ constexpr int kBinTile = 16;       // binning tile edge for the deterministic re
 // kernels: 128 spreads the 1024² workload's 16,384 nodes over 128 SMs instead of 64
 // (measured: 0.1733 → 0.1720 ms per step; batch 1.990 → 1.982 ms; 64 is no better)
 constexpr int kNodeThreads = 128;
+// chain rods (one warp each) per CTA of the chain kernel: one spreads the rods over the most
+// SMs (measured per batch step: 1.963 ms with 1, 1.965 with 2, 1.973 with 4)
+constexpr int kChainWarps = 1;
 constexpr int kHeadThreads = 128;
 constexpr int kLbmTileX = 128;     // dense LBM CTA tile: 32 lanes x 4 cells
 constexpr int kLbmTileY = 2;      // default LBM tile height (rows per CTA): 64 threads, the most CTAs to spread

@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, cons
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ci = (blockIdx.x - off[r]) * 4 + warp;
+  const int ci = (blockIdx.x - off[r]) * kChainWarps + warp;
   if (ci >= d.nchain) return;  // the whole warp leaves together
   const int comp = d.chain_comp[ci];
   const int n0 = d.comp_n[comp], nn = d.comp_n[comp + 1] - n0;
@@ -730,10 +730,10 @@ void launch_node(const Launch& L, const int* tdev, size_t smem, int bs) {
 }
 void launch_chain(const Launch& L, const int* tdev, int slots) {
   switch (slots) {
-    case 1: k_chain<1><<<L.grid, 128, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
-    case 2: k_chain<2><<<L.grid, 128, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
-    case 4: k_chain<4><<<L.grid, 128, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
-    default: k_chain<8><<<L.grid, 128, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
+    case 1: k_chain<1><<<L.grid, 32 * kChainWarps, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
+    case 2: k_chain<2><<<L.grid, 32 * kChainWarps, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
+    case 4: k_chain<4><<<L.grid, 32 * kChainWarps, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
+    default: k_chain<8><<<L.grid, 32 * kChainWarps, 0, L.s>>>(L.d, L.off, L.n, tdev); break;
   }
 }
 cudaError_t node_set_smem(size_t bytes) {

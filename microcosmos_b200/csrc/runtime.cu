@@ -1169,7 +1169,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     // the plan's CTAs would not all be resident)
     cnt[K_IBCOOP] = c.enable_fluid ? std::max(1, div_up(h.M, 1024)) : 0;
     cnt[K_COMP] = h.dims.N > 0 ? (int)h.generic_comp.size() : 0;
-    cnt[K_CHAIN] = h.dims.N > 0 ? div_up((long long)h.chain_comp.size(), 4) : 0;
+    cnt[K_CHAIN] = h.dims.N > 0 ? div_up((long long)h.chain_comp.size(), mc::kChainWarps) : 0;
     cnt[K_IB] = div_up(h.M, mc::kHeadThreads);  // touched cells: at most M, one thread each
     cnt[K_TILES] = h.ntx * h.nty;
     cnt[K_LBM] = c.enable_fluid ? h.lbm_tx * h.lbm_ty : 0;
