@@ -6,7 +6,8 @@ same grid, 4-point IB, 20 PBD iterations, curvature actuation amp ~U(0.1,0.3),
 period ~U(100,400), dt = 0.01.  A "step" is one simulate.step of that instance.
 
   value      MLUPS = cells x steps / device time, state resident in HBM, L2 flushed
-             (256 MiB write) between timed steps, each step timed with CUDA events
+             (256 MiB written, then 256 MiB read) between timed steps, each step timed
+             with CUDA events
   e2e        MLUPS through the reference-facing run() API with pinned host inputs and
              host outputs (H2D of the state, the rollout, D2H of the final state)
   roofline   the dense stream+collide kernel: 72 B/cell algorithmic traffic per launch
@@ -63,6 +64,8 @@ def parse():
     ap.add_argument("--gym-envs", type=int, default=256)
     ap.add_argument("--gym-steps", type=int, default=50)
     ap.add_argument("--no-gym", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="steps of the end-to-end run() call (0: the workload's own rollout length)")
     return ap.parse_args()
 
 
@@ -72,10 +75,10 @@ def workload(name, seed):
         return scenarios.config_scale(seed=seed), {
             "workload": "plain method at scale: 1024x1024 periodic D2Q9 TRT fp32, 256 filaments x 64 nodes "
                         "(Poisson-disk, min sep 8), steric FFT 1024^2, 4-pt IB, 20 PBD iterations, dt 0.01",
-            "grid": [1024, 1024], "filaments": 256, "nodes_per_filament": 64}
+            "grid": [1024, 1024], "filaments": 256, "nodes_per_filament": 64, "rollout_steps": 10000}
     return scenarios.config_small(seed=seed), {
         "workload": "plain method small: 128x128 periodic D2Q9 TRT fp32, 4 filaments x 32 nodes, dt 0.01",
-        "grid": [128, 128], "filaments": 4, "nodes_per_filament": 32}
+        "grid": [128, 128], "filaments": 4, "nodes_per_filament": 32, "rollout_steps": 1000}
 
 
 def measured_peaks():
@@ -101,18 +104,48 @@ def committed_traffic(kernel, H, W):
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled DURING a timed region.
+
+    NVML is polled from a thread every ~2 ms (the timed regions here last milliseconds to
+    seconds; nvidia-smi's loop mode samples every 100 ms at best); without NVML it falls
+    back to ``nvidia-smi --query-gpu=... -lms 100``.  Read-only: no clock or GPU setting
+    is changed."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, period_s=0.0002):
         self.gpu = gpu_index
+        self.period = period_s
         self.proc = None
+        self.samples = []  # (sm_mhz, max_mhz, reason bits)
         self.lines = []
+        self._stop = threading.Event()
+        self._nvml = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.gpu)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
 
     def start(self):
+        try:
+            self._nvml = self._handle()
+        except Exception:
+            self._nvml = None
+        if self._nvml is not None:
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -122,11 +155,35 @@ class ClockSampler:
         except (OSError, FileNotFoundError):
             self.proc = None
 
+    def _poll(self):
+        nv, h = self._nvml
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self._stop.is_set():
+            try:
+                t = time.perf_counter()
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), mx,
+                                     int(nv.nvmlDeviceGetCurrentClocksEventReasons(h)), t))
+            except Exception:
+                break
+            time.sleep(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
-    def stop(self):
+    def stop(self, window=None):
+        """Summary of the samples; with window = (t0, t1) (time.perf_counter values) only the
+        samples taken inside it."""
+        self._stop.set()
+        if self._nvml is not None:
+            self.t.join(timeout=5)
+            smp = [x for x in self.samples if window is None or window[0] <= x[3] <= window[1]]
+            sm = [x[0] for x in smp]
+            reasons = sorted({n for x in smp for n, b in self.REASONS if x[2] & b})
+            return {"sm_mhz": float(np.median(sm)) if sm else None,
+                    "sm_max_mhz": self.samples[0][1] if self.samples else None,
+                    "reasons": reasons, "samples": len(sm),
+                    "source": f"NVML, polled every {self.period * 1e3:g} ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -149,7 +206,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi -lms 100"}
 
 
 def cpu_baseline(sc, cfg_steps_budget_s=15.0):
@@ -200,7 +257,7 @@ def batch_section(args, flush):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     torch.cuda.synchronize()
     for i in range(K):
-        flush.zero_()
+        flush()
         ev[i][0].record(stream)
         plan.advance(1, use_graph=True, last=(i == K - 1))
         ev[i][1].record(stream)
@@ -214,7 +271,7 @@ def batch_section(args, flush):
     plan.advance(1, use_graph=False)
     plan.profile_reset()
     for i in range(10):
-        flush.zero_()
+        flush()
         plan.advance(1, use_graph=False, last=(i == 9))
     plan.end()
     torch.cuda.synchronize()
@@ -258,6 +315,7 @@ def batch_section(args, flush):
         "workload": f"{len(scs)} uneven rollouts (side U{{128..512}}, 1-32 filaments x 16-128 nodes), "
                     f"{cells} cells, {nodes} nodes in total; rollouts/s for 2000-step rollouts",
         "steps_timed": K, "ms_per_step": t_batch, "mlups": cells / (t_batch / 1e3) / 1e6,
+        "node_steps_per_s": nodes / (t_batch / 1e3),
         "rollouts_per_s": len(scs) / (t_batch / 1e3 * steps),
         "plain_rollouts_per_s": len(scs) / (t_plain_pop / 1e3 * steps),
         "plain_sample": f"{nplain} rollouts, one plan each, {K} graph-launched steps each",
@@ -273,17 +331,17 @@ def batch_section(args, flush):
         "lbm_frac_of_peak": BYTES_PER_CELL * cells / (lbm_ms / 1e3) / 1e9 / measured_peaks()[0],
         "roofline_frac_mlups": cells / (t_batch / 1e3) / 1e6 / (measured_peaks()[0] * 1e9 / BYTES_PER_CELL / 1e6),
         "flags_nonzero": int(sum(1 for f in flags if f)),
-        "l2": "flushed (256 MiB write) before every timed step"}
+        "l2": "flushed before every timed step (256 MiB written, then 256 MiB read)"}
 
 
 def serve_section(args):
     """Serving configuration: a seeded Poisson stream (mean ``--serve-rate`` requests/s) of
     rollouts with grid side ~U{64..1024} step 64, filaments ~U{1..128}, nodes/filament
     ~U{16..128}, steps ~U{500..5000}, 20% marked as asking for gradients, served by the
-    continuous-batching server (admission by a 180 GB budget, up to 16 rollouts in flight,
-    200-step graph-replayed chunks, one stream per rollout, up to 8 gradient jobs at once;
-    16 slots and 8 gradient workers measured best among 16-64 slots and 2-16 workers).
-    Latency = completion minus
+    continuous-batching server (admission by a 180 GB budget; every admitted forward
+    rollout advances in shared epochs, one ragged plan per epoch of at most 200
+    graph-replayed steps, ending where the nearest rollout finishes; up to 8 gradient
+    jobs at once beside them).  Latency = completion (state back on the host) minus
     arrival, wall clock.  The plain path runs a sample of the same requests one after
     another, one plan each."""
     import torch
@@ -295,7 +353,7 @@ def serve_section(args):
     serve.run_plain(be, serve.poisson_requests(1, 1.0, seed=99, sides=(64,), filaments=(1, 1), nodes=(16, 16),
                                                steps=(8, 8)))
     torch.cuda.synchronize()
-    srv = serve.Server(be, hbm_budget_bytes=180e9, max_active=16, chunk=200, keep_state=False)
+    srv = serve.Server(be, hbm_budget_bytes=180e9, max_active=256, chunk=200, keep_state=False)
     t0 = time.perf_counter()
     res = srv.run(reqs, realtime=True)
     torch.cuda.synchronize()
@@ -328,7 +386,7 @@ def serve_section(args):
                 grad_note="gradient requests: forward with checkpoints + adjoint of the mean centre-of-mass x "
                           "displacement w.r.t. actuation and initial positions, on worker threads",
                 flags_nonzero=int(sum(1 for r in res if r.flags)),
-                peak_active=srv.peak_active, peak_bytes=srv.peak_bytes,
+                peak_active=srv.peak_active, peak_bytes=srv.peak_bytes, epochs=srv.epochs,
                 plain_mlups=cs_all / t_plain_all / 1e6, plain_rollouts_per_s=plain_rps,
                 plain_sample=f"first {k} forward requests ({t_f:.2f} s) and first {kg} gradient requests "
                              f"({t_g:.2f} s), each alone and in turn, scaled by cell-steps to the stream",
@@ -434,6 +492,14 @@ def gym_section(args):
             "speedup_vs_single": (B * K / batch_ms) / (K / single_ms), "mean_reward_last_step": mean_reward}
 
 
+def config_json(cfgj, ws):
+    """The ``config`` object of both arms' JSON lines."""
+    return dict(cfgj, l2="flushed before every timed step (256 MiB written, then 256 MiB read); each step timed "
+                         "alone with CUDA events",
+                parallelism=f"replicas x{ws}", dt=0.01,
+                timed="device-resident: one graph-launched simulate.step per event pair")
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -490,11 +556,16 @@ def run_reference(args):
     sample = (f"{procs} single-threaded replicas x {min(k for k, _, _ in res)}-{max(k for k, _, _ in res)} steps of "
               f"the {sc.H}x{sc.W} workload ({dt:.0f} s; numpy restatement of the reference step: JAX is not "
               f"installed, so the reference itself cannot run)")
+    k_min = min(k for k, _, _ in res)
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus, "steps": k_tot,
-        "warmup": w, "ms_per_step": dt / max(1, k_tot // procs) * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy.random)",
-        "config": cfgj,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
+        # every replica runs the same K steps (up to its time budget); steps and ms_per_step
+        # describe one replica, value sums all replicas' cell updates over the slowest one's time
+        "steps": k_min, "warmup": w, "ms_per_step": dt / k_min * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded numpy.random, the benchmark configurations' shapes)",
+        "config": config_json(cfgj, args.gpus), "replicas": procs, "replica_steps_total": k_tot,
+        "node_steps_per_s": k_tot * sc.N / dt,
         "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": procs, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
@@ -524,10 +595,20 @@ def main():
     st = DeviceState.from_scenario(sc)
     act = Actuation.from_scenario(sc)
     plan = Plan.for_states([st], [cfg], [0.01])
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # L2 flush between timed steps: write a 256 MiB buffer (evicts the rollout's data), then
+    # read another 256 MiB buffer, so that the write's dirty lines are written back here and
+    # not during the next timed step
+    flush_w = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush_r = torch.zeros(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def flush():
+        flush_w.zero_()
+        flush_r.sum()
     stream = torch.cuda.current_stream()
 
     # ---------------- device-resident timed region
+    clocks = ClockSampler(local)
+    clocks.start()
     plan.begin([st], actuations=[act])
     plan.advance(args.warmup, use_graph=True)
     K = args.steps
@@ -535,17 +616,16 @@ def main():
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
     # last_launch_count accumulates over the begin/advance calls of one rollout
     launches0 = plan.last_launch_count()
+    tw0 = time.perf_counter()
     for i in range(K):
-        flush.zero_()
+        flush()
         ev[i][0].record(stream)
         plan.advance(1, use_graph=True, last=(i == K - 1))
         ev[i][1].record(stream)
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    clk = clocks.stop(window=(tw0, time.perf_counter()))
     if ws > 1:
         dist.barrier()
     launches = plan.last_launch_count() - launches0
@@ -564,7 +644,7 @@ def main():
     plan.profile_reset()
     P = args.profile_steps
     for i in range(P):
-        flush.zero_()
+        flush()
         plan.advance(1, use_graph=False, last=(i == P - 1))
     plan.end()
     torch.cuda.synchronize()
@@ -595,8 +675,13 @@ def main():
              ("steric", (H, W)), ("fluid_velocity", (2, H, W)))}
     api_run(hn, he, hf, 0.01, 4, cfg, actuation=actn)  # plan/graph warm-up
     torch.cuda.synchronize()
-    Ke = K
+    # one call of the workload's own rollout length (10,000 steps at scale): the state goes
+    # in from pinned host memory once and the final state comes back once, as a caller of
+    # simulate/run with that rollout pays it
+    Ke = args.e2e_steps or cfgj["rollout_steps"]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks_e = ClockSampler(local, period_s=0.01)
+    clocks_e.start()
     e0.record(stream)
     n_, e_, f_ = api_run(hn, he, hf, 0.01, Ke, cfg, actuation=actn)
     outs["position"].copy_(n_.position)
@@ -607,6 +692,7 @@ def main():
     outs["fluid_velocity"].copy_(f_.fluid_velocity)
     e1.record(stream)
     torch.cuda.synchronize()
+    clk_e = clocks_e.stop()
     te = e0.elapsed_time(e1)
     h2d = sum(int(np.asarray(a).nbytes) for a in (sc.position, sc.velocity, sc.theta, sc.rest_lengths,
                                                    sc.bending_rest_angles, sc.bending_stiffness, sc.f_grid,
@@ -636,16 +722,19 @@ def main():
             "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": ws, "steps": K, "warmup": args.warmup,
             "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded numpy.random, the benchmark configurations' shapes)",
-            "config": dict(cfgj, l2="flushed (256 MiB write) before every timed step; each step timed alone with "
-                                    "CUDA events", parallelism=f"replicas x{ws}", dt=0.01,
-                           timed="device-resident: one graph-launched simulate.step per event pair"),
+            "config": config_json(cfgj, ws),
+            "node_steps_per_s": job_cell_steps / cells * sc.N / (t_ms / 1e3),
             "e2e": {"value": job_cell_steps_e / (te / 1e3) / 1e6, "unit": "MLUPS",
                     "h2d_bytes_per_step": h2d / Ke, "d2h_bytes_per_step": d2h / Ke, "steps_per_call": Ke,
-                    "h2d_bytes_per_call": h2d, "d2h_bytes_per_call": d2h,
-                    "api": "microcosmos_b200.simulate.run (pinned host inputs -> host outputs)"},
+                    "h2d_bytes_per_call": h2d, "d2h_bytes_per_call": d2h, "ms": te,
+                    "node_steps_per_s": job_cell_steps_e / cells * sc.N / (te / 1e3),
+                    "clocks": clk_e,
+                    "api": "microcosmos_b200.simulate.run, one call of the workload's rollout length "
+                           "(pinned host inputs -> host outputs)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_lbm (fused pull stream + TRT/Guo collide, float2 rows)",
+                         "kernel": "k_lbm (fused pull stream + TRT/Guo collide), %d cells per lane x %d rows per CTA"
+                                   % plan.lbm_shape(),
                          "algorithmic_bytes_per_launch": BYTES_PER_CELL * cells,
                          "ms_per_launch": lbm_s * 1e3},
             "cpu_baseline": cpu,

@@ -59,8 +59,9 @@ typedef struct mc_config {
   float stiffness_shear;
   float damping;
   int32_t enable_fluid;
-  float viscosity;
-  float max_fluid_velocity;
+  double viscosity;           /* a Python float: omega+ = 1/(3 viscosity + 0.5) is taken in double */
+  double max_fluid_velocity;  /* a Python float: the velocity caps are max_fluid_velocity times the
+                               * mean grid scale, taken in double and rounded once to float32 */
   int32_t ibm_iterations;
   float synthetic_node_width; /* >= 0; > 0 puts a pair of IB points at +- width along the chain normal */
   int32_t ibm_kernel_size;    /* 1..8 */
@@ -70,7 +71,7 @@ typedef struct mc_config {
   int32_t enable_force_clamp;
   int32_t enable_steric;
   float steric_strength;
-  float steric_sigma;
+  double steric_sigma;        /* a Python float: 2 sigma^2 etc. are taken in double */
   int32_t steric_neighbor_skip;
   float steric_scatter_value;
   int32_t solver_type;        /* MC_SOLVER_PBD or MC_SOLVER_COSSERAT */
@@ -140,9 +141,11 @@ void mc_plan_destroy(mc_plan* plan);
 
 /* Tile shape of the dense stream+collide pass: each CTA covers 32 * cells_per_lane columns
  * (1, 2 or 4 cells per thread, vector loads and stores; it must divide every rollout's
- * lattice width) by rows_per_cta rows (2, 4 or 8); the default is 2 cells per lane (1 for an
- * odd width) by 2 rows.  0 keeps the current value.  Results do not depend on
- * the shape.  Only before mc_plan_bind(); microcosmos_b200.autotune picks it by timing.
+ * lattice width) by rows_per_cta rows (2, 4, 8, 16 or 32; up to 4 warps per CTA, each
+ * looping over rows_per_cta / 4 rows).  The default is 4 cells per lane by 16 rows for plans
+ * of at least 4 M lattice cells and 2 cells per lane by 4 rows below (fewer cells per lane
+ * when a width needs it).  0 keeps the current value.  Results do not depend on the shape.
+ * Only before mc_plan_bind(); microcosmos_b200.autotune picks it by timing.
  * No counterpart in the reference (XLA chooses its own fusion tiling). */
 mc_status mc_plan_set_lbm_shape(mc_plan* plan, int32_t cells_per_lane, int32_t rows_per_cta);
 mc_status mc_plan_get_lbm_shape(const mc_plan* plan, int32_t* cells_per_lane, int32_t* rows_per_cta);
@@ -252,9 +255,13 @@ const char* mc_profile_kernel_names(void);
  * <= 13); larger sizes return MC_ERR_INVALID.  The scratch (about 6.6 MB) is one
  * file-scope __device__ array that every GPU loading this library keeps until the process
  * exits.  The first call made on a device looks up that array's device address (set-up);
- * make that first call before any stream capture.  All calls share the array and each call
- * re-initialises what must start at zero, so calls that overlap on the GPU (different
- * streams, no ordering between them) race and must not be issued. */
+ * make that first call before any stream capture.  The address is kept per device together
+ * with the id of the context it belongs to, so the first call after that context is torn
+ * down (cudaDeviceReset) repeats the set-up.  Each call enqueues one set-up kernel that
+ * receives the call's tables and descriptor as its by-value parameter, writes them into the
+ * array and clears what must start at zero, then the deposit and filter kernels.  All calls
+ * share the array, so calls that overlap on the GPU (different streams, no ordering between
+ * them) race and must not be issued. */
 #define MC_NOALLOC_MAX_GRID 512
 #define MC_NOALLOC_MAX_NODES 16384
 mc_status mc_steric_potential_noalloc(const float* position, int32_t N, int32_t H, int32_t W, float sigma,

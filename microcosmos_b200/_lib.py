@@ -27,8 +27,8 @@ class McConfig(ctypes.Structure):
         ("stiffness_shear", ctypes.c_float),
         ("damping", ctypes.c_float),
         ("enable_fluid", ctypes.c_int32),
-        ("viscosity", ctypes.c_float),
-        ("max_fluid_velocity", ctypes.c_float),
+        ("viscosity", ctypes.c_double),
+        ("max_fluid_velocity", ctypes.c_double),
         ("ibm_iterations", ctypes.c_int32),
         ("synthetic_node_width", ctypes.c_float),
         ("ibm_kernel_size", ctypes.c_int32),
@@ -38,7 +38,7 @@ class McConfig(ctypes.Structure):
         ("enable_force_clamp", ctypes.c_int32),
         ("enable_steric", ctypes.c_int32),
         ("steric_strength", ctypes.c_float),
-        ("steric_sigma", ctypes.c_float),
+        ("steric_sigma", ctypes.c_double),
         ("steric_neighbor_skip", ctypes.c_int32),
         ("steric_scatter_value", ctypes.c_float),
         ("solver_type", ctypes.c_int32),

@@ -2,7 +2,8 @@
 
 Three kernels have a free shape:
   * the dense stream+collide pass: each CTA covers 32 x cells_per_lane columns (1, 2 or 4
-    cells per thread, vector loads/stores) by rows_per_cta rows (2, 4 or 8);
+    cells per thread, vector loads/stores) by rows_per_cta rows (4, 8, 16 or 32 tried;
+    up to 4 warps per CTA, each looping over rows_per_cta / 4 rows);
   * the power-of-two FFT kernels of the steric filter: each thread holds 4, 8 or 16
     values in registers (more values: fewer instructions per value; fewer: more threads);
   * the tile kernel that sorts the IB and cloud-in-cell contributions: 128 or 256 threads
@@ -25,7 +26,7 @@ import torch
 from .engine import DeviceState, Plan
 
 CELLS_PER_LANE = (1, 2, 4)
-ROWS_PER_CTA = (2, 4, 8)
+ROWS_PER_CTA = (4, 8, 16, 32)
 FFT_VALUES = (4, 8, 16)
 BIN_SHAPES = ((128, 2048), (256, 2048), (128, 1024), (256, 1024), (128, 512))  # (threads per CTA, shared sort capacity)
 

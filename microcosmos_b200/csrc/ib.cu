@@ -497,14 +497,10 @@ __device__ __forceinline__ void rollout_barrier(int* ctl, int nb, unsigned* flag
 // iterations, then the finalize of every touched cell.  Same arithmetic and order as
 // k_ib_interp / k_ib_spread / k_ib_finalize; values written in one phase and read in the
 // next are loaded with __ldcg (L2, not the SM's L1).
-__global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
-                                                 int parity) {
-  const int r = find_rollout(off, n, blockIdx.x);
-  const RDesc& d = D[r];
-  const int nb = off[r + 1] - off[r];
-  const int lb = blockIdx.x - off[r];
-  const int stride = nb * blockDim.x;
-  const int t0 = lb * blockDim.x + threadIdx.x;
+// The shared body: threads t0, t0 + stride, ... of one rollout; `sync` is the barrier among
+// all of the rollout's threads.
+template <typename Sync>
+__device__ __forceinline__ void ib_iterations(const RDesc& d, int t0, int stride, Sync sync) {
   const int nheads = __ldcg(d.ib_ctl + 2);
   const int K2 = d.K * d.K;
   for (int it = 0; it < d.ib_iters; ++it) {
@@ -546,7 +542,7 @@ __global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, co
       d.delta[2 * node] = sx * cf;
       d.delta[2 * node + 1] = sy * cf;
     }
-    rollout_barrier(d.ib_ctl, nb, d.flags);
+    sync();
     for (int p = t0; p < nheads; p += stride) {
       const int len = d.h_len[p];
       const int* rn = d.ib_store + d.h_start[p];
@@ -582,10 +578,8 @@ __global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, co
       d.s_ucx[p] = __ldcg(d.s_ucx + p) + dx * inv;
       d.s_ucy[p] = __ldcg(d.s_ucy + p) + dy * inv;
     }
-    rollout_barrier(d.ib_ctl, nb, d.flags);
+    sync();
   }
-  const size_t HW = (size_t)d.lH * d.lW;
-  const int nflag = d.lbm_tx * d.lbm_ty;
   for (int p = t0; p < nheads; p += stride) {
     float ucx = __ldcg(d.s_ucx + p), ucy = __ldcg(d.s_ucy + p);
     const float c2 = clamp_factor(ucx, ucy, d.vmax);
@@ -601,22 +595,51 @@ __global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, co
     }
     d.s_fx[p] = Fx;
     d.s_fy[p] = Fy;
-    const int cell = d.h_cell[p];
-    d.fov[cell] = Fx;
-    d.fov[HW + cell] = Fy;
-    const int y = cell / d.lW, x = cell - y * d.lW;
-    d.lbm_flag[(parity & 1) * nflag + (y / d.lbm_th) * d.lbm_tx + x / d.lbm_tw] = 1;
   }
+  if (t0 == 0) d.ib_ctl[5] = nheads;  // for k_collide_heads
 }
 
-// Post-accumulation clamp and body force F = (u_corrected - u) rho (fluid.py:327-339),
-// published to the dense pass through the force overlay.
+__global__ void __launch_bounds__(256) k_ib_coop(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
+                                                 int parity) {
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int nb = off[r + 1] - off[r];
+  const int lb = blockIdx.x - off[r];
+  ib_iterations(d, lb * blockDim.x + threadIdx.x, nb * blockDim.x,
+                [&] { rollout_barrier(d.ib_ctl, nb, d.flags); });
+}
+
+// The same iterations with one thread-block cluster per rollout (cluster c = rollout c):
+// the hardware cluster barrier (release / acquire at cluster scope) separates the phases,
+// so a rollout's 2 x iterations + 1 dependent steps cost no kernel boundaries and no
+// software barrier.  Every CTA of a cluster reaches every barrier: the early return below
+// is uniform across the cluster.
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kIbClusterThreads) k_ib_cluster(const RDesc* __restrict__ D, int n) {
+  unsigned rank, ncta, cid;
+  asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+  asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncta));
+  asm("mov.u32 %0, %%clusterid.x;" : "=r"(cid));
+  if ((int)cid >= n) return;
+  const RDesc& d = D[cid];
+  if (!d.enable_fluid || d.NI == 0) return;
+  ib_iterations(d, (int)(rank * blockDim.x + threadIdx.x), (int)(ncta * blockDim.x), [] { cluster_sync_all(); });
+}
+
+// Post-accumulation clamp and body force F = (u_corrected - u) rho (fluid.py:327-339) per
+// touched cell, for the node reaction and for k_collide_heads, which collides these cells
+// after the dense pass.  The head count is saved in ib_ctl[5] for k_collide_heads.
 __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
                                                      int parity) {
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
-  if (p >= d.ib_ctl[2]) return;
+  const int nheads = d.ib_ctl[2];
+  if (p == 0) d.ib_ctl[5] = nheads;
+  if (p >= nheads) return;
   float ucx = d.s_ucx[p], ucy = d.s_ucy[p];
   const float c2 = clamp_factor(ucx, ucy, d.vmax);
   ucx = ucx * c2;
@@ -631,12 +654,6 @@ __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D
   }
   d.s_fx[p] = Fx;
   d.s_fy[p] = Fy;
-  const int cell = d.h_cell[p];
-  const size_t HW = (size_t)d.lH * d.lW;
-  d.fov[cell] = Fx;
-  d.fov[HW + cell] = Fy;
-  const int y = cell / d.lW, x = cell - y * d.lW;
-  d.lbm_flag[(parity & 1) * d.lbm_tx * d.lbm_ty + (y / d.lbm_th) * d.lbm_tx + x / d.lbm_tw] = 1;
 }
 
 // Node reaction (fluid.py:364-382), final wrap (simulate.py:97-98), non-finite check and
@@ -788,6 +805,26 @@ cudaError_t launch_ib_coop(const Launch& L, int parity) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, k_ib_coop, L.d, L.off, L.n, parity);
+}
+// One cluster of `ctas` CTAs per rollout (1 <= ctas <= 16; above 8 the non-portable size
+// is allowed on the kernel first).
+cudaError_t launch_ib_cluster(const RDesc* d, int n, int ctas, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(n * ctas));
+  cfg.blockDim = dim3(kIbClusterThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)ctas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_ib_cluster, d, n);
+}
+cudaError_t ib_cluster_allow_16() {
+  return cudaFuncSetAttribute(k_ib_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
 cudaError_t ib_coop_blocks_per_sm(int* out) {
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_ib_coop, 256, 0);

@@ -53,103 +53,149 @@ __device__ __forceinline__ void pull_dir(const float* __restrict__ plane, int H,
   }
 }
 
+// One row of VEC cells per lane: pull, collide, store.  All lanes of the warp call it.
 template <int VEC>
-__global__ void __launch_bounds__(256) k_lbm(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
+__device__ __forceinline__ void lbm_row(const RDesc& d, const float* __restrict__ hin, float* __restrict__ hout,
+                                        int H, int W, size_t HW, int y, int x0, int x0c, bool x_ok, int lane,
+                                        int write_u, float hwp, float hwm, float cp, float cm) {
+  float fin[9][VEC];
+  {
+    const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+    const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+#pragma unroll
+    for (int i = 0; i < 9; ++i) pull_dir<VEC>(hin + i * HW, H, W, y, x0c, lane, ex[i], ey[i], fin[i]);
+  }
+  float out[9][VEC];
+  float usx[VEC], usy[VEC];
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) {
+    float f[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = fin[i][c];
+    // rho = max(sum f, 0.1), u = sum e f / rho (fluid.py:136-142)
+    float rho = f[0];
+#pragma unroll
+    for (int i = 1; i < 9; ++i) rho = rho + f[i];
+    rho = max_nan(rho, 0.1f);
+    const float ux = (((((f[1] - f[3]) + f[5]) - f[6]) - f[7]) + f[8]) / rho;
+    const float uy = (((((f[2] - f[4]) + f[5]) + f[6]) - f[7]) - f[8]) / rho;
+    const float usq = ux * ux + uy * uy;
+    float o[9];
+    if (usq + MC_EPSIL <= d.vmax_q4) {
+      // |u| <= vmax/2: both velocity clamp factors are exactly 1 and F = 0
+      collide_free(f, rho, ux, uy, usq, d.wp, hwp, hwm, o);
+      usx[c] = ux;
+      usy[c] = uy;
+    } else {
+      // the velocity clamps (fluid.py:268-274, 327-339) with the unchanged velocity
+      float r2, vx, vy, Fx, Fy;
+      macroscopic(f, d.vmax, d.vmax_q4, r2, vx, vy);
+      free_cell_force(r2, vx, vy, d.vmax, d.vmax_q4, d.force_clamp, Fx, Fy);
+      collide(f, r2, vx, vy, Fx, Fy, d.wp, d.wm, cp, cm, o, usx[c], usy[c]);
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) out[i][c] = o[i];
+  }
+  if (x_ok) {
+    const size_t base = (size_t)y * W + x0;
+    if (VEC == 4) {
+#pragma unroll
+      for (int i = 0; i < 9; ++i)
+        *reinterpret_cast<float4*>(hout + i * HW + base) = make_float4(out[i][0], out[i][1 % VEC], out[i][2 % VEC],
+                                                                       out[i][3 % VEC]);
+      if (write_u) {
+        *reinterpret_cast<float4*>(d.fluid_vel + base) = make_float4(usx[0], usx[1 % VEC], usx[2 % VEC], usx[3 % VEC]);
+        *reinterpret_cast<float4*>(d.fluid_vel + HW + base) =
+            make_float4(usy[0], usy[1 % VEC], usy[2 % VEC], usy[3 % VEC]);
+      }
+    } else if (VEC == 2) {
+#pragma unroll
+      for (int i = 0; i < 9; ++i)
+        *reinterpret_cast<float2*>(hout + i * HW + base) = make_float2(out[i][0], out[i][1 % VEC]);
+      if (write_u) {
+        *reinterpret_cast<float2*>(d.fluid_vel + base) = make_float2(usx[0], usx[1 % VEC]);
+        *reinterpret_cast<float2*>(d.fluid_vel + HW + base) = make_float2(usy[0], usy[1 % VEC]);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 9; ++i) hout[i * HW + base] = out[i][0];
+      if (write_u) {
+        d.fluid_vel[base] = usx[0];
+        d.fluid_vel[HW + base] = usy[0];
+      }
+    }
+  }
+}
+
+// The dense pass.  Every cell is collided as if no IB point touched it (F = 0, or the
+// force of the velocity clamps alone); the cells the IB touched this step ("heads") are
+// collided again with their body force by k_collide_heads, which runs after this kernel
+// and overwrites them.  The pass therefore reads no force field and has no force branch.
+// CTA tile: 32 * VEC columns x lbm_th rows, blockDim = (32, WY) with WY = min(lbm_th, 4)
+// warps; warp wy takes rows wy, wy + WY, ... of the tile (RPW rows each, lbm_th = WY * RPW),
+// so the per-thread set-up (rollout lookup, tile position, descriptor loads) is paid once
+// for VEC * RPW cells.
+template <int VEC, int RPW>
+__global__ void __launch_bounds__(128) k_lbm(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
                                              int parity, int write_u) {
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int lb = blockIdx.x - off[r];
-  const int tx = lb % d.lbm_tx, ty = lb / d.lbm_tx;
-  const int lane = threadIdx.x;
+  const int ntx = d.lbm_tx;
+  const int tx = lb % ntx, ty = lb / ntx;
+  const int lane = threadIdx.x, wy = threadIdx.y;
   const int H = d.lH, W = d.lW;
-  const int y = ty * d.lbm_th + threadIdx.y;
   const int x0 = tx * (32 * VEC) + lane * VEC;
-  const bool row_ok = y < H;
   const bool x_ok = x0 < W;
   const int x0c = x_ok ? x0 : (W - VEC);
   const size_t HW = (size_t)H * W;
   const float* __restrict__ hin = d.h[parity];
   float* __restrict__ hout = d.h[parity ^ 1];
-  // tile flags are double-buffered by step parity: this step's finalize set flag[parity];
-  // the other set belongs to the previous step and is cleared here for the next one
-  const int nflag = d.lbm_tx * d.lbm_ty;
-  const int flag_idx = ty * d.lbm_tx + tx;
-  const bool has_ov = d.lbm_flag[parity * nflag + flag_idx] != 0;
-  if (threadIdx.x == 0 && threadIdx.y == 0) d.lbm_flag[(parity ^ 1) * nflag + flag_idx] = 0;
+  const float hwp = 0.5f * d.wp, hwm = 0.5f * d.wm;
+  const float cp = 1.0f - 0.5f * d.wp, cm = 1.0f - 0.5f * d.wm;
+  const int y0 = ty * d.lbm_th + wy;
+#pragma unroll 1
+  for (int k = 0; k < RPW; ++k) {
+    const int y = y0 + k * (int)blockDim.y;
+    if (y >= H) break;  // uniform across the warp
+    lbm_row<VEC>(d, hin, hout, H, W, HW, y, x0, x0c, x_ok, lane, write_u, hwp, hwm, cp, cm);
+  }
+}
 
-  if (row_ok) {
-    float fin[9][VEC];
-    const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
-    const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+// The cells touched by IB points this step, one thread each: the TRT + Guo collision with
+// the body force F = (u_corrected - u) rho that k_ib_finalize left per head (fluid.py:327-350),
+// written over the dense pass's force-free result.  The populations are pulled again; the
+// density and clamped velocity are the ones the tile kernel computed from the same values.
+// (Storing the pulled populations per head in the tile kernel instead was measured: the
+// stores cost the tile kernel more than the coalesced reads saved here.)
+// The head count is the copy k_ib_finalize saved in ib_ctl[5] (the next step's node
+// pipeline resets ib_ctl[2] while this kernel may still run).
+__global__ void __launch_bounds__(kHeadThreads) k_collide_heads(const RDesc* __restrict__ D, const int* __restrict__ off,
+                                                       int n, int parity, int write_u) {
+  const int r = find_rollout(off, n, blockIdx.x);
+  const RDesc& d = D[r];
+  const int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
+  if (!d.enable_fluid || p >= __ldcg(d.ib_ctl + 5)) return;
+  const int cell = d.h_cell[p];
+  const int W = d.lW, H = d.lH;
+  const int y = cell / W, x = cell - y * W;
+  const size_t HW = (size_t)H * W;
+  const float* __restrict__ hin = d.h[parity];
+  float* __restrict__ hout = d.h[parity ^ 1];
+  float f[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) pull_dir<VEC>(hin + i * HW, H, W, y, x0c, lane, ex[i], ey[i], fin[i]);
-
-    float ovx[VEC], ovy[VEC];
-    bool ov[VEC];
+  for (int i = 0; i < 9; ++i) {
+    const int ys = imod_floor(y - kEy[i], H), xs = imod_floor(x - kEx[i], W);
+    f[i] = hin[i * HW + (size_t)ys * W + xs];
+  }
+  const float cp = 1.0f - 0.5f * d.wp, cm = 1.0f - 0.5f * d.wm;
+  float o[9], usx, usy;
+  collide(f, d.s_rho[p], d.s_vx[p], d.s_vy[p], d.s_fx[p], d.s_fy[p], d.wp, d.wm, cp, cm, o, usx, usy);
 #pragma unroll
-    for (int c = 0; c < VEC; ++c) ov[c] = false;
-    if (has_ov && x_ok) {
-      const size_t base = (size_t)y * W + x0;
-#pragma unroll
-      for (int c = 0; c < VEC; ++c) {
-        float a = d.fov[base + c], b = d.fov[HW + base + c];
-        ov[c] = !is_sentinel(a);
-        ovx[c] = a;
-        ovy[c] = b;
-        if (ov[c]) {
-          d.fov[base + c] = nan_f();
-          d.fov[HW + base + c] = nan_f();
-        }
-      }
-    }
-    const float cp = 1.0f - 0.5f * d.wp, cm = 1.0f - 0.5f * d.wm;
-    float out[9][VEC];
-    float usx[VEC], usy[VEC];
-#pragma unroll
-    for (int c = 0; c < VEC; ++c) {
-      float f[9];
-#pragma unroll
-      for (int i = 0; i < 9; ++i) f[i] = fin[i][c];
-      float rho, vx, vy, Fx, Fy;
-      macroscopic(f, d.vmax, d.vmax_q4, rho, vx, vy);
-      if (ov[c]) {
-        Fx = ovx[c];
-        Fy = ovy[c];
-      } else {
-        free_cell_force(rho, vx, vy, d.vmax, d.vmax_q4, d.force_clamp, Fx, Fy);
-      }
-      float o[9];
-      collide(f, rho, vx, vy, Fx, Fy, d.wp, d.wm, cp, cm, o, usx[c], usy[c]);
-#pragma unroll
-      for (int i = 0; i < 9; ++i) out[i][c] = o[i];
-    }
-    if (x_ok) {
-      const size_t base = (size_t)y * W + x0;
-      if (VEC == 4) {
-#pragma unroll
-        for (int i = 0; i < 9; ++i)
-          *reinterpret_cast<float4*>(hout + i * HW + base) = make_float4(out[i][0], out[i][1], out[i][2], out[i][3]);
-        if (write_u) {
-          *reinterpret_cast<float4*>(d.fluid_vel + base) = make_float4(usx[0], usx[1], usx[2], usx[3]);
-          *reinterpret_cast<float4*>(d.fluid_vel + HW + base) = make_float4(usy[0], usy[1], usy[2], usy[3]);
-        }
-      } else if (VEC == 2) {
-#pragma unroll
-        for (int i = 0; i < 9; ++i)
-          *reinterpret_cast<float2*>(hout + i * HW + base) = make_float2(out[i][0], out[i][1 % VEC]);
-        if (write_u) {
-          *reinterpret_cast<float2*>(d.fluid_vel + base) = make_float2(usx[0], usx[1 % VEC]);
-          *reinterpret_cast<float2*>(d.fluid_vel + HW + base) = make_float2(usy[0], usy[1 % VEC]);
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < 9; ++i) hout[i * HW + base] = out[i][0];
-        if (write_u) {
-          d.fluid_vel[base] = usx[0];
-          d.fluid_vel[HW + base] = usy[0];
-        }
-      }
-    }
+  for (int i = 0; i < 9; ++i) hout[i * HW + cell] = o[i];
+  if (write_u) {
+    d.fluid_vel[cell] = usx;
+    d.fluid_vel[HW + cell] = usy;
   }
 }
 
@@ -194,21 +240,19 @@ __global__ void k_stream_out(const RDesc* __restrict__ D, const int* __restrict_
   }
 }
 
-// Workspace initialisation: overlay = NaN sentinel, deposit grid = 0, counters = 0.
+// Workspace initialisation: deposit grid = 0, counters = 0.
 __global__ void k_clear_ws(const RDesc* __restrict__ D, const int* __restrict__ off, int n) {
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int lb = blockIdx.x - off[r];
   const size_t stride = (size_t)(off[r + 1] - off[r]) * blockDim.x;
-  const size_t HW = (size_t)d.H * d.W, LHW = (size_t)d.lH * d.lW;
+  const size_t HW = (size_t)d.H * d.W;
   const size_t t0 = (size_t)lb * blockDim.x + threadIdx.x;
-  for (size_t i = t0; i < 2 * LHW; i += stride) d.fov[i] = nan_f();
   if (d.dep)
     for (size_t i = t0; i < HW; i += stride) d.dep[i] = 0.0f;
   const int nt = d.ntile_x * d.ntile_y, lnt = d.lntile_x * d.lntile_y;
   for (size_t i = t0; i < (size_t)lnt; i += stride) d.ib_tcount[i] = 0;
   for (size_t i = t0; i < (size_t)nt; i += stride) d.c_tcount[i] = 0;
-  for (size_t i = t0; i < (size_t)2 * d.lbm_tx * d.lbm_ty; i += stride) d.lbm_flag[i] = 0;
   if (t0 < 8) {
     d.ib_ctl[t0] = 0;
     d.c_ctl[t0] = 0;
@@ -216,14 +260,31 @@ __global__ void k_clear_ws(const RDesc* __restrict__ D, const int* __restrict__ 
   if (t0 == 0) *d.flags = 0u;
 }
 
+template <int VEC>
+void launch_lbm_vec(const Launch& L, int parity, int write_u, int rows) {
+  const int wy = rows < 4 ? rows : 4;
+  dim3 block(32, wy);
+  switch (rows / wy) {
+    case 1: k_lbm<VEC, 1><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u); break;
+    case 2: k_lbm<VEC, 2><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u); break;
+    case 4: k_lbm<VEC, 4><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u); break;
+    default: k_lbm<VEC, 8><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u); break;
+  }
+}
+
+// rows: the tile height (2, 4, 8, 16 or 32); up to 4 warps per CTA, each looping over
+// rows / 4 of them
 void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows) {
-  dim3 block(32, rows);
   if (vec == 4)
-    k_lbm<4><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u);
+    launch_lbm_vec<4>(L, parity, write_u, rows);
   else if (vec == 2)
-    k_lbm<2><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u);
+    launch_lbm_vec<2>(L, parity, write_u, rows);
   else
-    k_lbm<1><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u);
+    launch_lbm_vec<1>(L, parity, write_u, rows);
+}
+
+void launch_collide_heads(const Launch& L, int parity, int write_u) {
+  k_collide_heads<<<L.grid, kHeadThreads, 0, L.s>>>(L.d, L.off, L.n, parity, write_u);
 }
 
 void launch_unstream(const Launch& L) { k_unstream<<<L.grid, 256, 0, L.s>>>(L.d, L.off, L.n); }

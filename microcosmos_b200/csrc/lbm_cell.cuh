@@ -14,6 +14,51 @@ __device__ __constant__ static const int kEy[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1}
 __device__ __forceinline__ float max_prop(float v, float c) { return (v < c) ? c : v; }
 __device__ __forceinline__ float min_prop(float c, float v) { return (v > c) ? c : v; }
 
+// The same maximum in one instruction: max.NaN returns NaN when an operand is NaN and the
+// larger operand otherwise, so for a non-NaN constant c it equals max_prop(v, c).
+__device__ __forceinline__ float max_nan(float v, float c) {
+  float r;
+  asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(v), "f"(c));
+  return r;
+}
+
+// TRT collision of a cell with no body force whose velocity clamp factor is exactly 1, so
+// that u* = u (fluid.py:346 with F = 0) and the Guo source is zero, then the EPSIL floor.
+// usq = ux^2 + uy^2 as the reference rounds it.  hwp = wp/2, hwm = wm/2 (exact halvings).
+//
+// Same bits as collide() with F = 0, with fewer operations, by exact identities:
+//  * for opposite directions (i, o), e_o.u = -(e_i.u) exactly, so 3 e_o.u = -(3 e_i.u),
+//    1 + 3 e_o.u = 1 - 3 e_i.u and (e_o.u)^2 = (e_i.u)^2: each pair shares those terms;
+//  * 0.5 a - 0.5 b = 0.5 (a - b) and wp (0.5 d) = (0.5 wp) d exactly (scaling by a power of
+//    two commutes with rounding away from the subnormal range, which populations >= EPSIL
+//    and their equilibria never reach), so sym = (f_i + f_o) - (feq_i + feq_o) scaled into
+//    hwp, anti likewise into hwm, and the o direction takes the negated antisymmetric term;
+//  * the rest direction: 0.5 (f0 + f0) = f0, its antisymmetric part is 0, so
+//    out0 = f0 - wp (f0 - feq0).
+__device__ __forceinline__ void collide_free(const float f[9], float rho, float ux, float uy, float usq, float wp,
+                                             float hwp, float hwm, float out[9]) {
+  const float s = 1.5f * usq;
+  const float r0 = rho * (4.0f / 9.0f), r1 = rho * (1.0f / 9.0f), r2 = rho * (1.0f / 36.0f);
+  out[0] = max_nan(f[0] - wp * (f[0] - r0 * (1.0f - s)), MC_EPSIL);
+  // pairs (1,3), (2,4), (5,7), (6,8): e_i.u = ux, uy, ux + uy, uy - ux
+  const float e[4] = {ux, uy, ux + uy, uy - ux};
+  const int pi[4] = {1, 2, 5, 6};
+  const int po[4] = {3, 4, 7, 8};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float rw = q < 2 ? r1 : r2;
+    const float t = 3.0f * e[q];
+    const float sq = 4.5f * (e[q] * e[q]);
+    const float feq_i = rw * (((1.0f + t) + sq) - s);
+    const float feq_o = rw * (((1.0f - t) + sq) - s);
+    const float fi = f[pi[q]], fo = f[po[q]];
+    const float a = hwp * ((fi + fo) - (feq_i + feq_o));
+    const float b = hwm * ((fi - fo) - (feq_i - feq_o));
+    out[pi[q]] = max_nan((fi - a) - b, MC_EPSIL);
+    out[po[q]] = max_nan((fo - a) + b, MC_EPSIL);
+  }
+}
+
 // min(1, vmax / (sqrt(x^2 + y^2 + EPSIL) + EPSIL))  (fluid.py:272-273, 300-301, 327-328)
 __device__ __forceinline__ float clamp_factor(float x, float y, float vmax) {
   float mag = sqrtf((x * x + y * y) + MC_EPSIL);

@@ -24,9 +24,8 @@ constexpr int kNodeThreads = 128;
 // SMs (measured per batch step: 1.963 ms with 1, 1.965 with 2, 1.973 with 4)
 constexpr int kChainWarps = 1;
 constexpr int kHeadThreads = 128;
+constexpr int kIbClusterThreads = 256;  // threads per CTA of the cluster IB kernel
 constexpr int kLbmTileX = 128;     // dense LBM CTA tile: 32 lanes x 4 cells
-constexpr int kLbmTileY = 2;      // default LBM tile height (rows per CTA): 64 threads, the most CTAs to spread
-constexpr int kLbmMinTileY = 2;   // smallest tile height a plan may be tuned to
 constexpr int kConvTile = 32;     // steric direct convolution: 32 x 32 outputs per CTA
 constexpr int kConvMaxR = 24;     // largest tap radius of the direct convolution       //                    8 rows
 constexpr int kIbCap = 1024;       // minimum IB bin capacity per 16x16 tile (grown with node density)
@@ -113,8 +112,6 @@ struct RDesc {
   const float* ndeg;   // (N,) max(node degree, 1)
   // workspace
   float* h[2];         // pull-scheme post-collision populations (9,lH,lW)
-  float* fov;          // (2,lH,lW) force overlay, NaN = no IB force at the cell
-  int* lbm_flag;       // (2 * lbm_ty*lbm_tx) tile has overlay entries, one set per step parity
   float* dep;          // (H,W) CIC deposit (kept zero between steps)
   float* tmp;          // (H,W) FFT row-pass output
   float* prev;         // (N,2)
@@ -126,7 +123,8 @@ struct RDesc {
   // store[t * cap + atomic position]; a tile that fills up spills into the overflow list.
   // store[ntiles * cap ...] is an arena for sorting tiles with more than cap entries.
   // ctl[0] = overflow count, ctl[1] = arena use, ctl[2] = touched-cell (head) count,
-  // ctl[3], ctl[4] = arrival count and generation of the fused IB kernel's barrier.
+  // ctl[3], ctl[4] = arrival count and generation of the fused IB kernel's barrier,
+  // ctl[5] = the head count saved by the finalize step for k_collide_heads.
   int ib_cap;
   int* ib_cell;     // (M) cell of contribution k = n*K*K + s
   float* ib_w;      // (M) normalised stencil weight
@@ -257,7 +255,10 @@ void launch_ib_spread(const Launch& L, int it);
 void launch_ib_finalize(const Launch& L, int parity);
 cudaError_t launch_ib_coop(const Launch& L, int parity);
 cudaError_t ib_coop_blocks_per_sm(int* out);
+cudaError_t launch_ib_cluster(const RDesc* d, int n, int ctas, cudaStream_t s);
+cudaError_t ib_cluster_allow_16();
 void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows);
+void launch_collide_heads(const Launch& L, int parity, int write_u);
 void launch_steric_conv(const Launch& L, size_t smem);
 void launch_fftreg_rows(const Launch& L, int values_per_thread);
 void launch_fft12_rows(const Launch& L);

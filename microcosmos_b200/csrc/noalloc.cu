@@ -6,6 +6,7 @@
 // library never calls cudaMalloc/cudaFree here, and the caller passes only the positions
 // and the output field.  The kernels are the same ones a rollout step uses.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstring>
@@ -58,27 +59,97 @@ mc_status na_fail(mc_status s, const std::string& m) {
   return s;
 }
 
-// Per-device set-up: the scratch's device address.  Done on the first call made with that
-// device current.  (The FFT kernels need at most 23 KB of dynamic shared memory at the
-// 512 x 512 limit, under the default 48 KB, so no kernel attribute is changed.)
+// Per-device set-up: the scratch's device address, looked up with cudaGetSymbolAddress on
+// the first call made with that device current.  The address belongs to the context that
+// loaded the module, so it is cached with that context's unique id: after a context is torn
+// down (cudaDeviceReset) and a new one created, the next call looks the address up again.
+// (The FFT kernels need at most 23 KB of dynamic shared memory at the 512 x 512 limit,
+// under the default 48 KB, so no kernel attribute is changed.)
+struct NaDevice {
+  unsigned long long ctx_id = 0;
+  unsigned char* ptr = nullptr;
+};
 std::mutex g_na_mutex;
-std::vector<unsigned char*> g_na_ptr;
+std::vector<NaDevice> g_na_dev;
+PFN_cuCtxGetCurrent_v4000 g_ctx_current = nullptr;
+PFN_cuCtxGetId_v12000 g_ctx_id = nullptr;
+
+// id of the calling thread's current context (0 if none is current)
+unsigned long long current_ctx_id() {
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (g_ctx_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 mc_status na_setup(unsigned char** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return na_fail(MC_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   std::lock_guard<std::mutex> lock(g_na_mutex);
-  if ((int)g_na_ptr.size() <= dev) g_na_ptr.resize(dev + 1, nullptr);
-  if (!g_na_ptr[dev]) {
+  if (!g_ctx_current || !g_ctx_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess)
+      return na_fail(MC_ERR_CUDA, "driver entry points cuCtxGetCurrent / cuCtxGetId not found");
+    g_ctx_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f1);
+    g_ctx_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f2);
+  }
+  if ((int)g_na_dev.size() <= dev) g_na_dev.resize(dev + 1);
+  NaDevice& nd = g_na_dev[dev];
+  const unsigned long long id = current_ctx_id();
+  if (!nd.ptr || id == 0 || id != nd.ctx_id) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_na_scratch);
     if (e != cudaSuccess)
       return na_fail(MC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_na_ptr[dev] = static_cast<unsigned char*>(p);
+    nd.ptr = static_cast<unsigned char*>(p);
+    nd.ctx_id = current_ctx_id();  // the lookup above makes the device's context current
   }
-  *out = g_na_ptr[dev];
+  *out = nd.ptr;
   return MC_OK;
+}
+
+// Everything a call writes into the scratch before its kernels run, passed by value as the
+// set-up kernel's parameter (about 14 KB, under the 32 KB kernel-parameter limit), so the
+// call stages nothing through host memory that outlives it.
+struct NaSetup {
+  mc::RDesc d;
+  int offs[8];
+  int N, ntiles;
+  size_t HW;
+  float2 twW[kNaMaxGrid], twH[kNaMaxGrid];
+  float gW[kNaMaxGrid], gH[kNaMaxGrid];
+};
+static_assert(sizeof(NaSetup) <= 32000, "set-up parameter block must fit the kernel parameter limit");
+static_assert(sizeof(mc::RDesc) % 4 == 0, "descriptor is copied as 4-byte words");
+
+// Writes the descriptor, the CTA offset tables and the FFT tables, and clears every
+// region the kernels expect at zero (the scratch keeps the previous call's contents).
+__global__ void k_na_setup(const __grid_constant__ NaSetup p, unsigned char* __restrict__ base) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const int* dw = reinterpret_cast<const int*>(&p.d);
+  int* desc = reinterpret_cast<int*>(base + kOffDesc);
+  for (size_t i = t0; i < sizeof(mc::RDesc) / 4; i += stride) desc[i] = dw[i];
+  if (t0 < 8) reinterpret_cast<int*>(base + kOffOff)[t0] = p.offs[t0];
+  for (size_t i = t0; i < (size_t)p.d.W; i += stride) {
+    reinterpret_cast<float2*>(base + kOffTwW)[i] = p.twW[i];
+    reinterpret_cast<float*>(base + kOffGW)[i] = p.gW[i];
+  }
+  for (size_t i = t0; i < (size_t)p.d.H; i += stride) {
+    reinterpret_cast<float2*>(base + kOffTwH)[i] = p.twH[i];
+    reinterpret_cast<float*>(base + kOffGH)[i] = p.gH[i];
+  }
+  for (size_t i = t0; i < 2 * (size_t)p.N; i += stride) reinterpret_cast<float*>(base + kOffVel)[i] = 0.0f;
+  for (size_t i = t0; i < (size_t)p.ntiles; i += stride) reinterpret_cast<int*>(base + kOffTcount)[i] = 0;
+  if (t0 < 16) reinterpret_cast<int*>(base + kOffCtl)[t0] = 0;
+  if (t0 < 4) reinterpret_cast<int*>(base + kOffWlCtl)[t0] = 0;
+  for (size_t i = t0; i < p.HW; i += stride) reinterpret_cast<float*>(base + kOffDep)[i] = 0.0f;
 }
 
 bool na_factorize(int N, int* f, int* nf) {
@@ -93,9 +164,7 @@ bool na_factorize(int N, int* f, int* nf) {
 
 // roots of unity exp(-2 pi i k / N) and the spectral Gaussian exp(-2 pi^2 sigma^2 f_k^2) / N
 // at numpy.fft.fftfreq abscissae, in float64 rounded to float32
-void na_tables(int N, double sigma, std::vector<float2>& tw, std::vector<float>& g) {
-  tw.resize(N);
-  g.resize(N);
+void na_tables(int N, double sigma, float2* tw, float* g) {
   for (int k = 0; k < N; ++k) {
     const double a = -2.0 * M_PI * (double)k / (double)N;
     tw[k] = make_float2((float)std::cos(a), (float)std::sin(a));
@@ -116,8 +185,11 @@ extern "C" mc_status mc_steric_potential_noalloc(const float* position, int32_t 
     return na_fail(MC_ERR_INVALID, "H and W must be in [4, " + std::to_string(kNaMaxGrid) +
                                        "] for the no-allocation entry point");
   if (!(sigma > 0.0f)) return na_fail(MC_ERR_INVALID, "sigma must be > 0");
-  mc::RDesc d;
-  std::memset(&d, 0, sizeof(d));
+  // the set-up block (about 14 KB) lives on this call's stack: no host heap either
+  NaSetup setup;
+  std::memset(&setup, 0, sizeof(NaSetup));
+  NaSetup* su = &setup;
+  mc::RDesc& d = su->d;
   if (!na_factorize(W, d.fftW_f, &d.fftW_nf) || !na_factorize(H, d.fftH_f, &d.fftH_nf))
     return na_fail(MC_ERR_UNSUPPORTED, "H and W need prime factors <= 13");
   unsigned char* base = nullptr;
@@ -167,32 +239,15 @@ extern "C" mc_status mc_steric_potential_noalloc(const float* position, int32_t 
   const int cnt[4] = {(N + mc::kNodeThreads - 1) / mc::kNodeThreads, d.ntile_x * d.ntile_y, (H + 1) / 2,
                       (W + 2 * mc::kFftColsPerCta - 1) / (2 * mc::kFftColsPerCta)};
   const int offs[8] = {0, cnt[0], 0, cnt[1], 0, cnt[2], 0, cnt[3]};
-  std::vector<float2> twW, twH;
-  std::vector<float> gW, gH;
-  na_tables(W, sigma, twW, gW);
-  na_tables(H, sigma, twH, gH);
-
-  // every value the kernels expect at zero is cleared here: the scratch keeps the
-  // previous call's contents
-  const size_t HW = (size_t)H * W;
-  cudaError_t e = cudaSuccess;
-  auto chk = [&](cudaError_t x) {
-    if (e == cudaSuccess) e = x;
-  };
-  chk(cudaMemcpyAsync(P(kOffDesc), &d, sizeof(d), cudaMemcpyHostToDevice, s));
-  chk(cudaMemcpyAsync(P(kOffOff), offs, sizeof(offs), cudaMemcpyHostToDevice, s));
-  chk(cudaMemcpyAsync(P(kOffTwW), twW.data(), W * sizeof(float2), cudaMemcpyHostToDevice, s));
-  chk(cudaMemcpyAsync(P(kOffTwH), twH.data(), H * sizeof(float2), cudaMemcpyHostToDevice, s));
-  chk(cudaMemcpyAsync(P(kOffGW), gW.data(), W * sizeof(float), cudaMemcpyHostToDevice, s));
-  chk(cudaMemcpyAsync(P(kOffGH), gH.data(), H * sizeof(float), cudaMemcpyHostToDevice, s));
-  chk(cudaMemsetAsync(P(kOffVel), 0, 2 * (size_t)N * 4, s));
-  chk(cudaMemsetAsync(P(kOffTcount), 0, (size_t)d.ntile_x * d.ntile_y * 4, s));
-  chk(cudaMemsetAsync(P(kOffCtl), 0, 16 * 4, s));
-  chk(cudaMemsetAsync(P(kOffDep), 0, HW * 4, s));
-  chk(cudaMemsetAsync(P(kOffWlCtl), 0, 4 * sizeof(int), s));
-  if (e != cudaSuccess) return na_fail(MC_ERR_CUDA, std::string("scratch set-up copy: ") + cudaGetErrorString(e));
-  // cudaMemcpyAsync from pageable host memory returns after the source has been staged,
-  // so the host arrays above may go out of scope
+  std::memcpy(su->offs, offs, sizeof(offs));
+  su->N = N;
+  su->ntiles = d.ntile_x * d.ntile_y;
+  su->HW = (size_t)H * W;
+  na_tables(W, sigma, su->twW, su->gW);
+  na_tables(H, sigma, su->twH, su->gH);
+  k_na_setup<<<128, 256, 0, s>>>(setup, base);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return na_fail(MC_ERR_CUDA, std::string("scratch set-up kernel: ") + cudaGetErrorString(e));
   const mc::RDesc* dd = reinterpret_cast<const mc::RDesc*>(P(kOffDesc));
   const int* off = reinterpret_cast<const int*>(P(kOffOff));
   mc::Launch l{dd, off, 1, cnt[0], s};

@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -84,14 +86,14 @@ struct HostRollout {
   int cRW = 0, cRH = 0;
   bool fft_ok = false, conv_ok = false, use_conv = false;
   Region r_cgW, r_cgH;
-  int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4, lbm_th = mc::kLbmTileY;
+  int M = 0, ntx = 0, nty = 0, lbm_tx = 0, lbm_ty = 0, vec = 4, lbm_th = 4;
   int lH = 0, lW = 0;      // the fluid lattice (= dims.H, dims.W unless dims.fluid_H/W are set)
   int lntx = 0, lnty = 0;  // bin tiles of the lattice (IB); ntx, nty: of the domain grid (CIC)
   int ib_cap = 0, c_cap = 0;  // bin capacities (powers of two)
   int logW = -1, logH = -1;   // log2 of power-of-two grid sides (-1: mixed radix path)
   int T_r = 0, P_r = 0, T_c = 0, P_c = 0;
   // workspace regions (offsets relative to the workspace base)
-  Region r_h0, r_h1, r_fov, r_lflag, r_dep, r_tmp, r_prev, r_pred, r_predw, r_nvl, r_delta;
+  Region r_h0, r_h1, r_dep, r_tmp, r_prev, r_pred, r_predw, r_nvl, r_delta;
   Region r_ibcell, r_ibw, r_ibstore, r_ibstorew, r_ibtc, r_ibovf, r_ibctl, r_ibslot, r_hcell, r_hstart, r_hlen, r_srho, r_svx,
       r_svy, r_sinv, r_sucx, r_sucy, r_sfx, r_sfy;
   Region r_ccell, r_cw, r_cstore, r_ctc, r_covf, r_cctl, r_chain, r_generic;
@@ -133,6 +135,8 @@ struct mc_plan {
   int64_t graph_kernels[2][2][3][2][2] = {};
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t lbm_stream = nullptr;                  // the dense pass, beside the IB chain
+  cudaEvent_t ev_lfork = nullptr, ev_ljoin = nullptr;
   bool pending_next = false;  // the next step's pipeline has already been launched
   int64_t last_launches = 0;
   // rollout in progress (mc_rollout_begin .. mc_rollout_end)
@@ -170,14 +174,18 @@ bool factorize(int N, std::vector<int>& f) {
 // |g| first drops below 1e-10 g[0], if that is smaller) and the taps for offsets -R..R.
 // Dropping the tail changes the filtered field by ~1e-6 relative (1.4e-6 rel-L2 measured
 // for sigma = 1.5 at R = 12, 6e-7 at R = 24).
-int conv_taps(int N, double sigma, std::vector<float>& taps) {
-  std::vector<double> g(N / 2 + 1);
-  for (int k = 0; k <= N / 2; ++k) {
+int conv_taps_compute(int N, double sigma, std::vector<float>& taps) {
+  // only offsets up to kConvMaxR + 1 decide R and are kept; the spectrum is evaluated once
+  const int kmax = std::min(N / 2, mc::kConvMaxR + 1);
+  std::vector<double> spec(N);
+  for (int j = 0; j < N; ++j) {
+    const double f = (j < (N + 1) / 2 ? (double)j : (double)(j - N)) / (double)N;
+    spec[j] = std::exp(-2.0 * M_PI * M_PI * sigma * sigma * f * f);
+  }
+  std::vector<double> g(kmax + 1);
+  for (int k = 0; k <= kmax; ++k) {
     double s = 0.0;
-    for (int j = 0; j < N; ++j) {
-      const double f = (j < (N + 1) / 2 ? (double)j : (double)(j - N)) / (double)N;
-      s += std::exp(-2.0 * M_PI * M_PI * sigma * sigma * f * f) * std::cos(2.0 * M_PI * (double)j * k / N);
-    }
+    for (int j = 0; j < N; ++j) s += spec[j] * std::cos(2.0 * M_PI * (double)j * k / N);
     g[k] = s / N;
   }
   int R = 0;
@@ -187,7 +195,45 @@ int conv_taps(int N, double sigma, std::vector<float>& taps) {
   return R;
 }
 
+// The steric tables depend only on (N, sigma): computed once per pair for the process and
+// copied into each plan (a serving or batching loop builds many plans over the same sides).
+struct StericTables {
+  int R = 0;
+  std::vector<float> taps;
+  std::vector<float2> tw;
+  std::vector<float> g;
+};
+std::mutex g_tables_mutex;
+std::map<std::pair<int, double>, StericTables> g_tables;
+
+void fft_tables_compute(int N, double sigma, std::vector<float2>& tw, std::vector<float>& g);
+
+const StericTables& steric_tables(int N, double sigma) {
+  std::lock_guard<std::mutex> lock(g_tables_mutex);
+  auto key = std::make_pair(N, sigma);
+  auto it = g_tables.find(key);
+  if (it == g_tables.end()) {
+    StericTables t;
+    t.R = conv_taps_compute(N, sigma, t.taps);
+    fft_tables_compute(N, sigma, t.tw, t.g);
+    it = g_tables.emplace(key, std::move(t)).first;
+  }
+  return it->second;
+}
+
+int conv_taps(int N, double sigma, std::vector<float>& taps) {
+  const StericTables& t = steric_tables(N, sigma);
+  taps = t.taps;
+  return t.R;
+}
+
 void fft_tables(int N, double sigma, std::vector<float2>& tw, std::vector<float>& g) {
+  const StericTables& t = steric_tables(N, sigma);
+  tw = t.tw;
+  g = t.g;
+}
+
+void fft_tables_compute(int N, double sigma, std::vector<float2>& tw, std::vector<float>& g) {
   tw.resize(N);
   g.resize(N);
   for (int k = 0; k < N; ++k) {
@@ -211,38 +257,49 @@ mc_status build_topology(HostRollout& h) {
     for (int j = 0; j < 2; ++j)
       if (h.bpairs[2 * b + j] < 0 || h.bpairs[2 * b + j] >= E)
         return fail(MC_ERR_INVALID, "bending pair " + std::to_string(b) + " references an edge outside [0, E)");
-  // edge -> bending pairs: all pairs where it is e_in (ascending), then all where it is e_out
-  std::vector<std::vector<int>> ein(E), eout(E);
-  for (int b = 0; b < B; ++b) {
-    ein[h.bpairs[2 * b]].push_back(b);
-    eout[h.bpairs[2 * b + 1]].push_back(b);
+  // edge -> bending pairs: all pairs where it is e_in (ascending), then all where it is
+  // e_out; node -> edges: edges where it is src (ascending), then edges where it is tgt.
+  // Both are built as CSR lists by counting, then filling in index order.
+  {
+    std::vector<int> cin(E, 0), cout(E, 0);
+    for (int b = 0; b < B; ++b) {
+      cin[h.bpairs[2 * b]]++;
+      cout[h.bpairs[2 * b + 1]]++;
+    }
+    h.ep_off.assign(E + 1, 0);
+    h.edeg.assign(E, 1.f);
+    for (int e = 0; e < E; ++e) {
+      h.ep_off[e + 1] = h.ep_off[e] + cin[e] + cout[e];
+      h.edeg[e] = (float)std::max(cin[e] + cout[e], 1);
+    }
+    h.ep_idx.assign(h.ep_off[E], 0);
+    std::vector<int> fin(E, 0), fout(E, 0);
+    for (int b = 0; b < B; ++b) {
+      const int ei = h.bpairs[2 * b], eo = h.bpairs[2 * b + 1];
+      h.ep_idx[h.ep_off[ei] + fin[ei]++] = b << 1;
+      h.ep_idx[h.ep_off[eo] + cin[eo] + fout[eo]++] = (b << 1) | 1;
+    }
   }
-  h.ep_off.assign(E + 1, 0);
-  h.ep_idx.clear();
-  h.edeg.assign(E, 1.f);
-  for (int e = 0; e < E; ++e) {
-    h.ep_off[e] = (int)h.ep_idx.size();
-    for (int b : ein[e]) h.ep_idx.push_back(b << 1);
-    for (int b : eout[e]) h.ep_idx.push_back((b << 1) | 1);
-    h.edeg[e] = (float)std::max<size_t>(ein[e].size() + eout[e].size(), 1);
+  {
+    std::vector<int> csrc(N, 0), ctgt(N, 0);
+    for (int e = 0; e < E; ++e) {
+      csrc[h.pairs[2 * e]]++;
+      ctgt[h.pairs[2 * e + 1]]++;
+    }
+    h.ne_off.assign(N + 1, 0);
+    h.ndeg.assign(N, 1.f);
+    for (int v = 0; v < N; ++v) {
+      h.ne_off[v + 1] = h.ne_off[v] + csrc[v] + ctgt[v];
+      h.ndeg[v] = (float)std::max(csrc[v] + ctgt[v], 1);
+    }
+    h.ne_idx.assign(h.ne_off[N], 0);
+    std::vector<int> fs(N, 0), ft(N, 0);
+    for (int e = 0; e < E; ++e) {
+      const int a = h.pairs[2 * e], b = h.pairs[2 * e + 1];
+      h.ne_idx[h.ne_off[a] + fs[a]++] = e << 1;
+      h.ne_idx[h.ne_off[b] + csrc[b] + ft[b]++] = (e << 1) | 1;
+    }
   }
-  h.ep_off[E] = (int)h.ep_idx.size();
-  // node -> edges: edges where it is src (ascending), then edges where it is tgt
-  std::vector<std::vector<int>> nsrc(N), ntgt(N);
-  for (int e = 0; e < E; ++e) {
-    nsrc[h.pairs[2 * e]].push_back(e);
-    ntgt[h.pairs[2 * e + 1]].push_back(e);
-  }
-  h.ne_off.assign(N + 1, 0);
-  h.ne_idx.clear();
-  h.ndeg.assign(N, 1.f);
-  for (int v = 0; v < N; ++v) {
-    h.ne_off[v] = (int)h.ne_idx.size();
-    for (int e : nsrc[v]) h.ne_idx.push_back(e << 1);
-    for (int e : ntgt[v]) h.ne_idx.push_back((e << 1) | 1);
-    h.ndeg[v] = (float)std::max<size_t>(nsrc[v].size() + ntgt[v].size(), 1);
-  }
-  h.ne_off[N] = (int)h.ne_idx.size();
   // connected components (union-find over edges)
   std::vector<int> par(N);
   for (int i = 0; i < N; ++i) par[i] = i;
@@ -499,8 +556,6 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   d.ndeg = at<float>(b, h.r_ndeg);
   d.h[0] = at<float>(b, h.r_h0);
   d.h[1] = at<float>(b, h.r_h1);
-  d.fov = at<float>(b, h.r_fov);
-  d.lbm_flag = at<int>(b, h.r_lflag);
   d.dep = at<float>(b, h.r_dep);
   d.tmp = at<float>(b, h.r_tmp);
   d.prev = at<float>(b, h.r_prev);
@@ -560,7 +615,7 @@ mc::Launch L(mc_plan* p, Kind k, cudaStream_t s) {
 const char* const kProfNames[] = {"predict", "cic_bins",  "fft_rows",    "fft_cols", "chain",
                                    "node",    "ib_bins",   "ib_interp",   "ib_spread", "ib_finalize",
                                    "lbm",     "reaction",  "record_fields", "tick",    "steric",
-                                   "stencil", "ib_fused", "steric_conv"};
+                                   "stencil", "ib_fused", "steric_conv", "collide_heads"};
 constexpr int kNumProf = sizeof(kProfNames) / sizeof(kProfNames[0]);
 
 cudaEvent_t take_event(mc_plan* p) {
@@ -753,6 +808,13 @@ int64_t enqueue_lbm(mc_plan* p, int parity, int write_u, cudaStream_t s, bool ca
   return 1;
 }
 
+// The IB-touched cells collided with their body force over the dense pass's result.
+int64_t enqueue_heads(mc_plan* p, int parity, int write_u, cudaStream_t s, bool capture) {
+  if (!p->any_fluid || !p->grid[K_NODES] || !p->grid[K_IB]) return 0;
+  timed(p, 18, s, capture, [&] { mc::launch_collide_heads(L(p, K_IB, s), parity, write_u); });
+  return 1;
+}
+
 int64_t enqueue_tail(mc_plan* p, int rec_fields, cudaStream_t s, bool capture) {
   int* tdev = at<int>(p->ws, p->r_tdev);
   int64_t k = 0;
@@ -769,29 +831,43 @@ int64_t enqueue_tail(mc_plan* p, int rec_fields, cudaStream_t s, bool capture) {
 }
 
 // Everything of step t after its pipeline, plus pipeline(t+1) when has_next.
+//   lbm stream: the dense pass lbm(t) (reads h[parity], writes h[parity^1]) from the start
+//               of the body, concurrently with the IB chain, which reads h[parity] only;
+//   main:       ib(t) (bins, iterations, body force per touched cell), then, once lbm(t)
+//               is done, the touched cells' collision over its result;
+//   side:       after ib(t): tail(t) (node reaction) and pipeline(t+1).
+// The next body starts when all three have finished.
 int64_t enqueue_body(mc_plan* p, int parity, int write_u, int rec_fields, bool has_next, cudaStream_t s,
                      bool capture, mc_status* err) {
-  int64_t k = enqueue_ib(p, parity, s, capture);
   if (rec_fields || p->profiling) {
     // sequential: field recording needs this order; profiling times kernels one at a time
+    int64_t k = enqueue_ib(p, parity, s, capture);
     k += enqueue_lbm(p, parity, write_u, s, capture);
+    k += enqueue_heads(p, parity, write_u, s, capture);
     k += enqueue_tail(p, rec_fields, s, capture);
     if (has_next) k += enqueue_pipeline(p, s, capture);
     return k;
   }
-  cudaStream_t s2 = p->side_stream;
-  cudaError_t e = cudaEventRecord(p->ev_fork, s);
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, p->ev_fork, 0);
-  if (e != cudaSuccess) {
-    *err = cuda_fail(e, "fork to the side stream");
-    return k;
+  auto fork = [&](cudaEvent_t ev, cudaStream_t from, cudaStream_t to, const char* what) {
+    cudaError_t e = cudaEventRecord(ev, from);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(to, ev, 0);
+    if (e != cudaSuccess && *err == MC_OK) *err = cuda_fail(e, what);
+  };
+  int64_t k = 0;
+  cudaStream_t s2 = p->side_stream, s3 = p->lbm_stream;
+  if (p->any_fluid) {
+    fork(p->ev_lfork, s, s3, "fork to the dense-pass stream");
+    k += enqueue_lbm(p, parity, write_u, s3, capture);
   }
+  k += enqueue_ib(p, parity, s, capture);
+  fork(p->ev_fork, s, s2, "fork to the side stream");
   k += enqueue_tail(p, 0, s2, capture);
   if (has_next) k += enqueue_pipeline(p, s2, capture);
-  k += enqueue_lbm(p, parity, write_u, s, capture);
-  e = cudaEventRecord(p->ev_join, s2);
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, p->ev_join, 0);
-  if (e != cudaSuccess) *err = cuda_fail(e, "join from the side stream");
+  if (p->any_fluid) {
+    fork(p->ev_ljoin, s3, s, "join from the dense-pass stream");
+    k += enqueue_heads(p, parity, write_u, s, capture);
+  }
+  fork(p->ev_join, s2, s, "join from the side stream");
   return k;
 }
 
@@ -1039,7 +1115,7 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       h.T_c = threads_for(D.H, 512);
       h.P_c = 512 / h.T_c;
     }
-    h.vec = (h.lW % 2 == 0) ? 2 : 1;
+    h.vec = (h.lW % 4 == 0) ? 4 : (h.lW % 2 == 0) ? 2 : 1;
     if (vec_all == -1) vec_all = h.vec;
     if (vec_all != h.vec) vec_all = 1;
     h.ntx = div_up(D.W, mc::kBinTile);
@@ -1050,7 +1126,6 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     const size_t N = D.N, E = D.E, B = D.B, nt = (size_t)h.ntx * h.nty, lnt = (size_t)h.lntx * h.lnty;
     h.r_h0 = lay.take(9 * LHW * 4);
     h.r_h1 = lay.take(9 * LHW * 4);
-    h.r_fov = lay.take(2 * LHW * 4);
     h.r_dep = lay.take(HW * 4);
     h.r_tmp = lay.take(HW * 4);
     h.r_prev = lay.take(2 * N * 4);
@@ -1119,14 +1194,19 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     p->max_iters = std::max(p->max_iters, c.enable_fluid ? c.ibm_iterations : 0);
     p->max_k = std::max(p->max_k, c.ibm_kernel_size);
   }
+  // default dense-pass tile: 4 cells per lane x 16 rows for plans of >= 4 M lattice cells
+  // (measured best at 2048^2 and on the 25 M-cell batch: 0.78 / 0.91 of HBM), 2 x 4 below
+  // (best at 1024^2: 20.8 us vs 22.9 us for 4 x 16); narrower when the widths need it
+  long long plan_cells = 0;
+  for (const auto& h : p->R) plan_cells += (long long)h.lH * h.lW;
+  const bool big_plan = plan_cells >= (4LL << 20);
+  if (!big_plan && vec_all == 4) vec_all = 2;
   for (int i = 0; i < n; ++i) {
     HostRollout& h = p->R[i];
     h.vec = vec_all;
-    h.lbm_th = mc::kLbmTileY;
+    h.lbm_th = big_plan ? 16 : 4;
     h.lbm_tx = div_up(h.lW, 32 * h.vec);
     h.lbm_ty = div_up(h.lH, h.lbm_th);
-    // sized for the smallest tiles a plan can be tuned to (mc_plan_set_lbm_shape)
-    h.r_lflag = lay.take((size_t)2 * div_up(h.lW, 32) * div_up(h.lH, mc::kLbmMinTileY) * 4);
   }
   {
     long long tiles = 0, ltiles = 0;
@@ -1288,7 +1368,8 @@ mc_status mc_plan_set_lbm_shape(mc_plan* p, int32_t cells_per_lane, int32_t rows
   int vec = cells_per_lane > 0 ? cells_per_lane : p->R[0].vec;
   int rows = rows_per_cta > 0 ? rows_per_cta : p->R[0].lbm_th;
   if (vec != 1 && vec != 2 && vec != 4) return fail(MC_ERR_INVALID, "cells_per_lane must be 1, 2 or 4");
-  if (rows != 2 && rows != 4 && rows != 8) return fail(MC_ERR_INVALID, "rows_per_cta must be 2, 4 or 8");
+  if (rows != 2 && rows != 4 && rows != 8 && rows != 16 && rows != 32)
+    return fail(MC_ERR_INVALID, "rows_per_cta must be 2, 4, 8, 16 or 32");
   for (auto& h : p->R)
     if (h.lW % vec != 0 || h.lW < vec)
       return fail(MC_ERR_UNSUPPORTED, "cells_per_lane must divide every rollout's lattice width");
@@ -1326,6 +1407,9 @@ void mc_plan_destroy(mc_plan* p) {
   if (p->side_stream) cudaStreamDestroy(p->side_stream);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   if (p->ev_join) cudaEventDestroy(p->ev_join);
+  if (p->lbm_stream) cudaStreamDestroy(p->lbm_stream);
+  if (p->ev_lfork) cudaEventDestroy(p->ev_lfork);
+  if (p->ev_ljoin) cudaEventDestroy(p->ev_ljoin);
   delete p;
 }
 
@@ -1391,6 +1475,7 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
   destroy_graphs(p);
   if (!p->cap_stream) MC_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
   if (!p->side_stream) MC_CUDA(cudaStreamCreateWithFlags(&p->side_stream, cudaStreamNonBlocking));
+  if (!p->lbm_stream) MC_CUDA(cudaStreamCreateWithFlags(&p->lbm_stream, cudaStreamNonBlocking));
   {
     // the fused IB kernel needs every CTA resident at once (cooperative launch)
     int dev = 0, sms = 0, per_sm = 0, coop = 0;
@@ -1403,6 +1488,8 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
   }
   if (!p->ev_fork) MC_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
   if (!p->ev_join) MC_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
+  if (!p->ev_lfork) MC_CUDA(cudaEventCreateWithFlags(&p->ev_lfork, cudaEventDisableTiming));
+  if (!p->ev_ljoin) MC_CUDA(cudaEventCreateWithFlags(&p->ev_ljoin, cudaEventDisableTiming));
   p->bound = true;
   return MC_OK;
 }

@@ -2,28 +2,31 @@
 
 Requests (a rollout of any grid and filament size, a step count) arrive over time.  The
 server admits a request as soon as a slot is free and its device memory fits in the HBM
-budget, keeps its lattice and rod state resident on the device, and advances every
-admitted rollout in chunks of steps (CUDA-graph replays) on its own CUDA stream, so the
-work of rollouts that arrive while others run overlaps with theirs on the device.  A
-finished rollout's state is copied back, its memory returns to the budget, and waiting
-requests take its place.
+budget and keeps its lattice and rod state resident on the device.  All admitted forward
+rollouts then advance TOGETHER: the server runs "epochs", each one ragged plan over the
+current set of rollouts (every kernel launched once per step for the whole set, the steps
+replayed from CUDA graphs), for as many steps as the set's nearest finish allows (at most
+``chunk``).  At every epoch boundary finished rollouts leave (their state is copied back and
+their memory returns to the budget) and newly admitted ones join, so requests that arrive
+while others run share the device's launches with them.  Up to ``depth`` epochs are queued
+on the serving stream, so the device does not wait for the host between epochs.
 
-Each rollout owns its plan, workspace and stream, and every kernel is deterministic (no
-float atomics), so a rollout's result is bit-for-bit the same whatever else is in flight.
-
-More hardware queues than CUDA's default of 8 let more rollouts overlap: set
-``CUDA_DEVICE_MAX_CONNECTIONS`` (e.g. 32) before the process first touches the GPU.
+Every kernel is deterministic (no float atomics), a rollout's result does not depend on
+the other rollouts of a plan, and splitting a rollout into epochs (begin / advance / end
+with the actuation clock continued) gives the same bits as one call, so a rollout's result
+is bit-for-bit the same alone and in the mix.
 
 Requests that ask for gradients get the gradient of the mean centre-of-mass x
 displacement of their final state with respect to the actuation (c, amplitude, phase of
 every bending pair) and the initial positions: the forward rollout with checkpoints and
 the adjoint run as one job on a worker thread (own stream, own gradient plan, see
-``microcosmos_b200.autodiff``), overlapping with the chunked forward rollouts.
+``microcosmos_b200.autodiff``), overlapping with the batched forward epochs.
 
-The scheduler is written against a small backend interface (``bytes_needed``, ``start``,
-``advance``, ``inflight``, ``finish``) so that its admission and ordering logic is tested
-without a GPU; ``CudaBackend`` is the device implementation over
-``microcosmos_b200.engine`` and ``microcosmos_b200.autodiff``.
+The scheduler is written against a small backend interface (``bytes_needed``, ``load``,
+``launch_epoch``, ``epoch_done``, ``collect``, ``release_epoch``, ``start_grad``,
+``grad_done``, ``grad_result``) so that its admission and ordering logic is tested without
+a GPU; ``CudaBackend`` is the device implementation over ``microcosmos_b200.engine`` and
+``microcosmos_b200.autodiff``.
 """
 from __future__ import annotations
 
@@ -63,21 +66,29 @@ class Result:
 
 
 class CudaBackend:
-    """Device backend: one bound plan + workspace + CUDA stream per admitted rollout;
-    gradient requests run as one job each on a thread pool.  A gradient job's reverse steps
-    are chains of small dependent kernels that leave most of the GPU idle, so several jobs
-    in flight overlap well: on the serving workload 8 workers finished the stream in 32 s
-    against 45 s with 2 (4: 34 s, 16: 35 s)."""
+    """Device backend.  Forward rollouts: device-resident state per request, one ragged
+    plan per epoch over the epoch's rollouts, all on one serving stream.  Gradient requests
+    run as one job each on a thread pool (own stream, own gradient plan): a gradient job's
+    reverse steps are chains of small dependent kernels that leave most of the GPU idle, so
+    several jobs in flight overlap well (8 workers measured best among 2-16)."""
 
     def __init__(self, cfg, dt=0.01, device="cuda", grad_workers=8):
+        import torch
         self.cfg = cfg
         self.dt = float(dt)
         self.device = device
         self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=max(1, int(grad_workers)))
+        self.stream = torch.cuda.Stream(device=device)       # epochs
+        self.copy_stream = torch.cuda.Stream(device=device)  # results back to the host
+
+    # a forward rollout's workspace exists once per epoch plan alive at a time: up to two
+    # queued (Server.depth) and one completed but not yet released
+    EPOCH_PLANS = 3
 
     def bytes_needed(self, req: Request) -> int:
-        """Device bytes of the rollout: its plan workspace (mc_plan_workspace_bytes, or
-        mc_grad_plan_workspace_bytes for a gradient request) plus state."""
+        """Device bytes of the rollout: its state plus its plan workspace
+        (mc_plan_workspace_bytes, counted EPOCH_PLANS times for a forward rollout; or
+        mc_grad_plan_workspace_bytes for a gradient request)."""
         from . import _lib
         from .engine import mc_config
         sc = req.scenario
@@ -108,8 +119,62 @@ class CudaBackend:
                 lib.mc_plan_destroy(h)
         N = sc.position.shape[0]
         state = 4 * (11 * fh * fw + sc.H * sc.W + 8 * N + 4 * bp.shape[0]) + 256
-        return ws + state
+        return (ws if req.want_grad else self.EPOCH_PLANS * ws) + state
 
+    # ---------------------------------------------------------------- forward rollouts
+    def load(self, req: Request):
+        """Upload the request's state; it stays resident until collected."""
+        import torch
+        from .engine import Actuation, DeviceState
+        with torch.cuda.stream(self.stream):
+            st = DeviceState.from_scenario(req.scenario, device=self.device)
+            sc = req.scenario
+            act = Actuation.from_scenario(sc, device=self.device)
+        return {"state": st, "act": act, "flags": 0}
+
+    def launch_epoch(self, handles, steps: int, t0s):
+        """Enqueue `steps` steps of every rollout in `handles` as one plan (rollout i continues
+        its actuation clock at t0s[i]) on the serving stream; returns the epoch handle."""
+        import torch
+        from .engine import Actuation, Plan
+        stream = self.stream
+        with torch.cuda.stream(stream):
+            sts = [h["state"] for h in handles]
+            acts = [None if h["act"] is None else dataclasses.replace(h["act"], t0=int(t)) for h, t in zip(handles, t0s)]
+            plan = Plan.for_states(sts, [self.cfg] * len(sts), [self.dt] * len(sts), device=self.device)
+            plan.begin(sts, actuations=acts, stream=stream.cuda_stream)
+            plan.advance(int(steps), use_graph=True, last=True, stream=stream.cuda_stream)
+            plan.end(stream=stream.cuda_stream)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        return {"plan": plan, "event": ev, "handles": handles, "flags_read": False}
+
+    def epoch_done(self, e) -> bool:
+        return e["event"].query()
+
+    def _read_epoch_flags(self, e):
+        if not e["flags_read"]:
+            import torch
+            with torch.cuda.stream(self.copy_stream):
+                fl = e["plan"].read_flags()
+            for h, f in zip(e["handles"], fl):
+                h["flags"] |= int(f)
+            e["flags_read"] = True
+
+    def collect(self, h, e=None):
+        """State and flags of a finished rollout (after its last epoch `e` completed)."""
+        import torch
+        if e is not None:
+            self._read_epoch_flags(e)
+        with torch.cuda.stream(self.copy_stream):
+            state = h["state"].host()
+        return state, h["flags"]
+
+    def release_epoch(self, e):
+        self._read_epoch_flags(e)
+        e["plan"].close()
+
+    # ---------------------------------------------------------------- gradient requests
     def _grad_job(self, req: Request):
         import torch
         from .autodiff import GradPlan
@@ -132,58 +197,29 @@ class CudaBackend:
             plan.close()
         return state, 0
 
-    def start(self, req: Request):
-        import torch
-        from .engine import Actuation, DeviceState, Plan
-        if req.want_grad:
-            return {"future": self.pool.submit(self._grad_job, req)}
-        stream = torch.cuda.Stream(device=self.device)
-        with torch.cuda.stream(stream):
-            st = DeviceState.from_scenario(req.scenario, device=self.device)
-            act = Actuation.from_scenario(req.scenario, device=self.device)
-            plan = Plan.for_states([st], [self.cfg], [self.dt], device=self.device)
-            plan.begin([st], actuations=[act], stream=stream.cuda_stream)
-        return {"stream": stream, "state": st, "act": act, "plan": plan, "events": collections.deque()}
+    def start_grad(self, req: Request):
+        return self.pool.submit(self._grad_job, req)
 
-    def advance(self, h, steps: int, last: bool):
-        import torch
-        if "future" in h:
-            return  # the gradient job runs all its steps at once
-        h["plan"].advance(steps, use_graph=True, last=last, stream=h["stream"].cuda_stream)
-        ev = torch.cuda.Event()
-        ev.record(h["stream"])
-        h["events"].append(ev)
+    def grad_done(self, h) -> bool:
+        return h.done()
 
-    def inflight(self, h) -> int:
-        """Chunks issued and not finished yet."""
-        if "future" in h:
-            return 0 if h["future"].done() else 1
-        q = h["events"]
-        while q and q[0].query():
-            q.popleft()
-        return len(q)
+    def grad_result(self, h):
+        return h.result()
 
-    def finish(self, h):
-        import torch
-        if "future" in h:
-            return h["future"].result()
-        with torch.cuda.stream(h["stream"]):
-            h["plan"].end(stream=h["stream"].cuda_stream)
-            flags = h["plan"].read_flags()[0]
-            state = h["state"].host()
-        h["stream"].synchronize()
-        h["plan"].close()
-        return state, flags
+
+@dataclasses.dataclass
+class _Epoch:
+    handle: Any
+    members: list
+    finishing: list
 
 
 class Server:
-    """Admission by memory budget and slot count, chunked stepping, overlap across rollouts.
+    """Admission by memory budget and slot count; forward rollouts advance together in
+    epochs (one ragged plan each), at most ``chunk`` steps per epoch and ``depth`` epochs
+    queued; gradient requests run beside them."""
 
-    ``depth`` chunks per rollout are kept queued on its stream, so a stream never drains
-    while the host services the others.
-    """
-
-    def __init__(self, backend, hbm_budget_bytes: float = 180e9, max_active: int = 16, chunk: int = 200,
+    def __init__(self, backend, hbm_budget_bytes: float = 180e9, max_active: int = 256, chunk: int = 200,
                  depth: int = 2, clock: Callable[[], float] | None = None, sleep: Callable[[float], None] | None = None,
                  keep_state: bool = True):
         if chunk < 1 or depth < 1 or max_active < 1:
@@ -198,11 +234,13 @@ class Server:
         self.keep_state = keep_state
         self.peak_active = 0
         self.peak_bytes = 0
+        self.epochs = 0
 
     def run(self, requests: list[Request], realtime: bool = True) -> list[Result]:
         """Serve ``requests``: arrival times are seconds from the call when ``realtime``,
         otherwise every request is present at the start.  Returns results ordered by id."""
-        need = {r.rid: int(self.backend.bytes_needed(r)) for r in requests}
+        be = self.backend
+        need = {r.rid: int(be.bytes_needed(r)) for r in requests}
         for r in requests:
             if need[r.rid] > self.budget:
                 raise ValueError(f"request {r.rid} needs {need[r.rid]} bytes of device memory, more than the "
@@ -210,7 +248,9 @@ class Server:
             if r.steps < 0:
                 raise ValueError(f"request {r.rid} asks for a negative step count")
         pending = collections.deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
-        active = {}   # rid -> [request, handle, steps issued, admitted at]
+        fwd = {}      # rid -> [request, handle, steps issued, admitted at]
+        grads = {}    # rid -> [request, job, admitted at]
+        queued = collections.deque()  # epochs in flight, oldest first
         used = 0
         results = []
         t0 = self.clock()
@@ -218,56 +258,87 @@ class Server:
         def now():
             return self.clock() - t0
 
-        while pending or active:
+        def done(r, adm, state, flags):
+            nonlocal used
+            used -= need[r.rid]
+            results.append(Result(rid=r.rid, arrival=r.arrival, admitted=adm, done=now(), steps=r.steps,
+                                  cells=r.scenario.H * r.scenario.W,
+                                  state=state if self.keep_state else None, flags=flags))
+
+        while pending or fwd or grads or queued:
             # admit, in arrival order, every request that has arrived and fits
             while pending and (not realtime or pending[0].arrival <= now()):
                 r = pending[0]
-                if len(active) >= self.max_active or used + need[r.rid] > self.budget:
+                if len(fwd) + len(grads) >= self.max_active or used + need[r.rid] > self.budget:
                     break
                 pending.popleft()
                 used += need[r.rid]
-                active[r.rid] = [r, self.backend.start(r), 0, now()]
-                self.peak_active = max(self.peak_active, len(active))
+                if r.want_grad:
+                    grads[r.rid] = [r, be.start_grad(r), now()]
+                else:
+                    fwd[r.rid] = [r, be.load(r), 0, now()]
+                    if r.steps == 0:
+                        state, flags = be.collect(fwd[r.rid][1])
+                        done(r, fwd[r.rid][3], state, flags)
+                        del fwd[r.rid]
+                self.peak_active = max(self.peak_active, len(fwd) + len(grads))
                 self.peak_bytes = max(self.peak_bytes, used)
-            busy = False
-            for rid in list(active):
-                r, h, issued, adm = active[rid]
-                q = self.backend.inflight(h)
-                if issued >= r.steps:
-                    if q:
-                        busy = True
-                        continue
-                    state, flags = self.backend.finish(h)
-                    used -= need[rid]
-                    results.append(Result(rid=rid, arrival=r.arrival, admitted=adm, done=now(), steps=r.steps,
-                                          cells=r.scenario.H * r.scenario.W,
-                                          state=state if self.keep_state else None, flags=flags))
-                    del active[rid]
-                    continue
-                busy = busy or q > 0
-                while q < self.depth and issued < r.steps:
-                    n = min(self.chunk, r.steps - issued)
-                    issued += n
-                    self.backend.advance(h, n, last=issued >= r.steps)
-                    q += 1
-                active[rid][2] = issued
-            if not active and pending and realtime:
+            progressed = False
+            # retire completed epochs, oldest first: their finished rollouts leave
+            while queued and be.epoch_done(queued[0].handle):
+                e = queued.popleft()
+                for rid in e.finishing:
+                    r, h, _, adm = fwd.pop(rid)
+                    state, flags = be.collect(h, e.handle)
+                    done(r, adm, state, flags)
+                be.release_epoch(e.handle)
+                progressed = True
+            for rid in list(grads):
+                r, job, adm = grads[rid]
+                if be.grad_done(job):
+                    state, flags = be.grad_result(job)
+                    done(r, adm, state, flags)
+                    del grads[rid]
+                    progressed = True
+            # queue the next epoch over every admitted rollout with steps left
+            if len(queued) < self.depth:
+                members = [rid for rid, (r, h, issued, _) in fwd.items() if issued < r.steps]
+                if members:
+                    n = min([self.chunk] + [fwd[rid][0].steps - fwd[rid][2] for rid in members])
+                    eh = be.launch_epoch([fwd[rid][1] for rid in members], n, [fwd[rid][2] for rid in members])
+                    for rid in members:
+                        fwd[rid][2] += n
+                    finishing = [rid for rid in members if fwd[rid][2] >= fwd[rid][0].steps]
+                    queued.append(_Epoch(eh, members, finishing))
+                    self.epochs += 1
+                    progressed = True
+            if progressed:
+                continue
+            if not fwd and not grads and not queued and pending and realtime:
                 wait = pending[0].arrival - now()
                 if wait > 0:
                     self.sleep(min(wait, 1e-3))
-            elif busy:
+            else:
                 self.sleep(0)
         return sorted(results, key=lambda x: x.rid)
 
 
 def run_plain(backend, requests: list[Request]):
-    """The plain path for comparison: each request alone, one after another, on one stream."""
+    """The plain path for comparison: each request alone, one after another (a forward
+    request as one single-rollout epoch, a gradient request as its gradient job)."""
     out = []
     for r in requests:
-        h = backend.start(r)
-        if r.steps:
-            backend.advance(h, r.steps, last=True)
-        state, flags = backend.finish(h)
+        if r.want_grad:
+            state, flags = backend.grad_result(backend.start_grad(r))
+        else:
+            h = backend.load(r)
+            e = backend.launch_epoch([h], r.steps, [0]) if r.steps else None
+            if e is not None:
+                while not backend.epoch_done(e):
+                    time.sleep(0)
+            state, flags = backend.collect(h, e)
+            if e is not None:
+                backend.release_epoch(e)
         out.append((r.rid, state, flags))
     return out
 

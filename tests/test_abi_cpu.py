@@ -178,12 +178,13 @@ def test_lbm_shape_setter_validates_and_reports(lib):
     assert st == _lib.MC_OK
     a, b = ctypes.c_int32(), ctypes.c_int32()
     assert lib.mc_plan_get_lbm_shape(h, ctypes.byref(a), ctypes.byref(b)) == _lib.MC_OK
-    assert (a.value, b.value) == (2, 2)  # the library's default
-    assert lib.mc_plan_set_lbm_shape(h, 4, 2) == _lib.MC_OK
+    assert (a.value, b.value) == (2, 4)  # the library's default for a small plan
+    assert lib.mc_plan_set_lbm_shape(h, 2, 32) == _lib.MC_OK
     lib.mc_plan_get_lbm_shape(h, ctypes.byref(a), ctypes.byref(b))
-    assert (a.value, b.value) == (4, 2)
+    assert (a.value, b.value) == (2, 32)
     assert lib.mc_plan_set_lbm_shape(h, 3, 0) == _lib.MC_ERR_INVALID
-    assert lib.mc_plan_set_lbm_shape(h, 0, 16) == _lib.MC_ERR_INVALID
+    assert lib.mc_plan_set_lbm_shape(h, 0, 12) == _lib.MC_ERR_INVALID
+    assert lib.mc_plan_set_lbm_shape(h, 0, 64) == _lib.MC_ERR_INVALID
     lib.mc_plan_destroy(h)
     # 4 cells per lane must divide W
     sc2 = scenarios.make_scenario(64, 66, 1, 10, seed=0)
@@ -200,9 +201,9 @@ def test_autotune_candidates_respect_widths():
         def __init__(self, W):
             self.W = W
 
-    assert autotune.candidates([S(64), S(128)]) == [(v, r) for v in (1, 2, 4) for r in (2, 4, 8)]
-    assert autotune.candidates([S(64), S(66)]) == [(v, r) for v in (1, 2) for r in (2, 4, 8)]
-    assert autotune.candidates([S(63)]) == [(1, r) for r in (2, 4, 8)]
+    assert autotune.candidates([S(64), S(128)]) == [(v, r) for v in (1, 2, 4) for r in (4, 8, 16, 32)]
+    assert autotune.candidates([S(64), S(66)]) == [(v, r) for v in (1, 2) for r in (4, 8, 16, 32)]
+    assert autotune.candidates([S(63)]) == [(1, r) for r in (4, 8, 16, 32)]
 
 
 def test_tile_kernel_threads_setter(lib):

@@ -240,3 +240,105 @@ def test_torch_autograd_binding_matches_the_plan():
     out = rollout(pos, vel, th, f, L0, kb, ra, sc.pairs, sc.bending_pairs, cfg_of(oc), 0.01, 2,
                   actuation=(c, amp, np.asarray(sc.act_omega), ph))
     out[0].sum().backward()
+
+
+def _diff_config():
+    """The differentiation workload: 256^2, 8 filaments x 48 nodes, amplitude 0.2, period 200
+    steps; loss = mean centre-of-mass x displacement of the final positions."""
+    sc = scenarios.make_scenario(256, 256, 8, 48, seed=0, amp=0.2, period=200.0)
+    cot = {k: np.zeros_like(getattr(sc, k)) for k in STATE}
+    cot["position"][:, 0] = 1.0 / sc.position.shape[0]
+    return sc, cot
+
+
+@pytest.mark.parametrize("steps", [5, 20])
+def test_differentiation_configuration_against_the_gradient_oracle(steps, parity_log):
+    """The differentiation workload's own size (256^2, 8 x 48 nodes, the mean centre-of-mass
+    x displacement) over 5 and 20 steps.  At 5 steps every gradient array is within 1e-4
+    (rel-L2) of the float32 oracle.  Over 20 steps float32 arithmetic itself no longer
+    resolves the gradient to 1e-4: the float32 and float64 oracles differ by ~1.5e-3 (the
+    cloud-in-cell and bilinear weights have kinks at cell edges and the adjoint chains 20 x 20
+    rod iterations), so the bar there is the float32 oracle's own distance from float64: the
+    device gradient's distance from the float64 oracle is at most twice it."""
+    oc = O.Config()
+    sc, cot = _diff_config()
+    _, g = gpu_grads(sc, oc, steps, cot)
+    _, g32 = oracle_grads(sc, oc, steps, cot, np.float32)
+    _, g64 = oracle_grads(sc, oc, steps, cot, np.float64)
+    for k in ("act_c", "act_amp", "act_phase", "position", "velocity", "theta", "f_grid"):
+        e32, e64, eref = O.rel_l2(g[k], g32[k]), O.rel_l2(g[k], g64[k]), O.rel_l2(g32[k], g64[k])
+        parity_log(f"grad_256_8x48_{steps}_steps_d{k}", vs_f32=e32, vs_f64=e64, oracle32_vs_f64=eref)
+        assert np.isfinite(g[k]).all()
+        if steps <= 5:
+            assert e32 <= GRAD_TOL, (k, e32)
+        else:
+            assert e64 <= max(2.0 * eref, GRAD_TOL), (k, e64, eref)
+
+
+def test_differentiation_configuration_against_central_differences(parity_log):
+    """16 random directional derivatives of the device gradient (20 steps, the workload's
+    size) against float64 central differences (h = 1e-3) of the oracle with the IB stencil
+    positions held at the unperturbed trajectory's (the reference's stop_gradient).  The
+    bar is relative to the float32 oracle gradient's own agreement with the same
+    differences: the device's error is at most twice it plus 1e-4 of the summed
+    contributions."""
+    oc = O.Config()
+    steps = 20
+    sc, cot = _diff_config()
+    _, g = gpu_grads(sc, oc, steps, cot)
+    _, g32 = oracle_grads(sc, oc, steps, cot, np.float32)
+    s0 = O.state_from_scenario(sc, np.float64)
+    acts = tuple(np.asarray(x, np.float64) for x in (sc.act_c, sc.act_amp, sc.act_omega, sc.act_phase))
+    _, tapes = A.rollout(s0, oc, 0.01, steps, acts)
+    ibp = A.ib_positions_of(tapes)
+    names = ["position", "act_c", "act_amp", "act_phase"]
+    rng = np.random.default_rng(1)
+    worst = 0.0
+    for j in range(16):
+        d = {k: rng.normal(size=g[k].shape) for k in names}
+
+        def run(eps):
+            s = s0.copy()
+            s.position = s0.position + eps * d["position"]
+            a = (acts[0] + eps * d["act_c"], acts[1] + eps * d["act_amp"], acts[2], acts[3] + eps * d["act_phase"])
+            out, _ = A.rollout(s, oc, 0.01, steps, a, ib_positions=ibp)
+            return float(np.sum(out.position * cot["position"]))
+
+        h = 1e-3
+        fd = (run(h) - run(-h)) / (2 * h)
+        terms = [float(np.sum(g[k].astype(np.float64) * d[k])) for k in names]
+        t32 = sum(float(np.sum(g32[k].astype(np.float64) * d[k])) for k in names)
+        ad = sum(terms)
+        scale = sum(abs(t) for t in terms)
+        parity_log(f"grad_256_8x48_20_steps_fd_dir{j}", fd=fd, device=ad, oracle32=t32,
+                   device_err_rel=abs(fd - ad) / scale, oracle32_err_rel=abs(fd - t32) / scale)
+        worst = max(worst, abs(fd - ad) / scale)
+        assert abs(fd - ad) <= 2.0 * abs(fd - t32) + GRAD_TOL * scale, (j, fd, ad, t32)
+    parity_log("grad_256_8x48_20_steps_fd_worst", device_err_rel=worst)
+
+
+def test_differentiation_length_without_fluid_2000_steps(parity_log):
+    """The differentiation workload over its full 2000 steps with the fluid off (rods +
+    steric field; the fluid adjoint is covered at 20 steps above).  Over 2000 steps float32
+    arithmetic itself does not determine the gradient: the loss is piecewise smooth (kinks
+    where nodes cross cell edges of the cloud-in-cell and bilinear weights) and float32
+    trajectories cross different kinks than the float64 one, so the float32 gradient oracle
+    is ~18% from the float64 one along a random direction (the float64 gradient agrees with
+    float64 central differences at h = 1e-5 to ~1e-3).  The device's directional derivative
+    must lie within twice the float32 oracle's distance from the float64 gradient."""
+    oc = O.Config(enable_fluid=False)
+    steps = 2000
+    sc, cot = _diff_config()
+    _, g = gpu_grads(sc, oc, steps, cot)
+    _, g32 = oracle_grads(sc, oc, steps, cot, np.float32)
+    _, g64 = oracle_grads(sc, oc, steps, cot, np.float64)
+    rng = np.random.default_rng(0)
+    d = {k: rng.normal(size=g[k].shape) for k in ("act_c", "act_amp", "act_phase", "position")}
+    dd = {name: sum(float(np.sum(np.asarray(gr[k], np.float64) * d[k])) for k in d)
+          for name, gr in (("device", g), ("oracle32", g32), ("oracle64", g64))}
+    e_dev = abs(dd["device"] - dd["oracle64"]) / abs(dd["oracle64"])
+    e_32 = abs(dd["oracle32"] - dd["oracle64"]) / abs(dd["oracle64"])
+    parity_log("grad_256_8x48_2000_steps_fluid_off", device_rel=e_dev, oracle32_rel=e_32, **dd)
+    for k in ("act_c", "act_amp", "act_phase", "position"):
+        assert np.isfinite(g[k]).all()
+    assert e_dev <= max(2.0 * e_32, GRAD_TOL), (dd, e_dev, e_32)

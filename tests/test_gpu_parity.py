@@ -120,26 +120,42 @@ def test_oracle_parity_small_grids(H, W, F, n):
     assert rel(out["fluid_velocity"], ref.fluid_velocity) < 1e-4
 
 
-def test_small_config_100_steps():
+def _errors_vs_oracles(out, sc, steps):
+    """rel-L2 of every output vs the float32 and the float64 oracle, and of the float32
+    oracle vs the float64 one (the distance float32 arithmetic alone accounts for)."""
+    r32 = _oracle_run(sc, steps)
+    s64, _ = O.simulate(O.state_from_scenario(sc, np.float64), O.Config(), 0.01, steps,
+                        act=(sc.act_c, sc.act_amp, sc.act_omega, sc.act_phase))
+    e = {}
+    for k in ("position", "f_grid", "theta", "velocity", "steric", "fluid_velocity"):
+        e[f"{k}_vs_f32"] = rel(out[k], getattr(r32, k))
+        e[f"{k}_vs_f64"] = rel(out[k], getattr(s64, k))
+        e[f"{k}_oracle32_vs_f64"] = rel(getattr(r32, k), getattr(s64, k))
+    return e
+
+
+def test_small_config_100_steps(parity_log):
     """Plain method, small: 128x128, 4 filaments x 32 nodes, 100 steps: rel-L2 <= 1e-5."""
     sc = scenarios.config_small(seed=0)
     out = _gpu_run(sc, 100)
-    ref = _oracle_run(sc, 100)
+    e = _errors_vs_oracles(out, sc, 100)
+    parity_log("small_128_4x32_100_steps", **e)
     for k in ("position", "f_grid", "theta"):
-        assert rel(out[k], getattr(ref, k)) < TOL, k
-    assert rel(out["velocity"], ref.velocity) < VEL_TOL
+        assert e[f"{k}_vs_f32"] < TOL, k
+    assert e["velocity_vs_f32"] < VEL_TOL
     # the steric field is a sigma = 1.5 Gaussian sum around positions ~1e2: a position
     # difference of rel-L2 1e-6 (~1e-4 absolute) moves it by ~1e-4 relative
-    assert rel(out["steric"], ref.steric) < 1e-3
+    assert e["steric_vs_f32"] < 1e-3
 
 
-def test_small_config_1000_steps():
+def test_small_config_1000_steps(parity_log):
     """Same configuration, 1000 steps: rel-L2 <= 1e-3 (positions and populations)."""
     sc = scenarios.config_small(seed=0)
     out = _gpu_run(sc, 1000)
-    ref = _oracle_run(sc, 1000)
+    e = _errors_vs_oracles(out, sc, 1000)
+    parity_log("small_128_4x32_1000_steps", **e)
     for k in ("position", "f_grid"):
-        assert rel(out[k], getattr(ref, k)) < 1e-3, k
+        assert e[f"{k}_vs_f32"] < 1e-3, k
 
 
 def test_graph_and_direct_launches_agree():

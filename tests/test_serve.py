@@ -7,35 +7,68 @@ from microcosmos_b200 import serve
 
 
 class FakeBackend:
-    """Chunks complete a fixed number of polls after they are issued; memory = cells."""
+    """Epochs complete a fixed number of polls after they are queued; memory = cells.
+    Checks the scheduler's invariants as it goes: an epoch never runs a rollout past its
+    step count, every rollout's actuation clock continues where its last epoch stopped,
+    and epochs complete in the order they were queued."""
 
-    def __init__(self, polls_per_chunk=2):
-        self.polls = polls_per_chunk
+    def __init__(self, polls_per_epoch=2, grad_polls=3):
+        self.polls = polls_per_epoch
+        self.grad_polls = grad_polls
         self.live = set()
         self.log = []
+        self.epochs = []
+        self.queue = []
 
     def bytes_needed(self, r):
         return r.scenario.H * r.scenario.W
 
-    def start(self, r):
+    def load(self, r):
         self.live.add(r.rid)
         self.log.append(("start", r.rid))
-        return {"rid": r.rid, "q": [], "steps": 0, "last": False}
+        return {"rid": r.rid, "target": r.steps, "steps": 0}
 
-    def advance(self, h, n, last):
-        h["q"].append(self.polls)
-        h["steps"] += n
-        h["last"] = last
+    def launch_epoch(self, handles, n, t0s):
+        assert n >= 1
+        for h, t in zip(handles, t0s):
+            assert t == h["steps"]
+            h["steps"] += n
+            assert h["steps"] <= h["target"]
+        e = {"polls": self.polls, "rids": [h["rid"] for h in handles], "n": n}
+        self.epochs.append(e)
+        self.queue.append(e)
+        return e
 
-    def inflight(self, h):
-        h["q"] = [p - 1 for p in h["q"] if p - 1 > 0]
-        return len(h["q"])
+    def epoch_done(self, e):
+        assert e is self.queue[0]  # retired oldest first
+        e["polls"] -= 1
+        if e["polls"] <= 0:
+            self.queue.pop(0)
+            return True
+        return False
 
-    def finish(self, h):
-        assert h["last"] or h["steps"] == 0
+    def collect(self, h, e=None):
+        assert h["steps"] == h["target"]
         self.live.discard(h["rid"])
         self.log.append(("finish", h["rid"]))
         return {"steps": h["steps"]}, 0
+
+    def release_epoch(self, e):
+        pass
+
+    def start_grad(self, r):
+        self.live.add(r.rid)
+        self.log.append(("start", r.rid))
+        return {"rid": r.rid, "polls": self.grad_polls, "steps": r.steps}
+
+    def grad_done(self, h):
+        h["polls"] -= 1
+        return h["polls"] <= 0
+
+    def grad_result(self, h):
+        self.live.discard(h["rid"])
+        self.log.append(("finish", h["rid"]))
+        return {"steps": h["steps"], "grad": True}, 0
 
 
 class _Sc:
@@ -55,10 +88,11 @@ class ManualClock:
         self.t += max(s, 1e-4)
 
 
-def _reqs(sides, steps, arrivals=None):
+def _reqs(sides, steps, arrivals=None, grads=None):
     arrivals = arrivals or [0.0] * len(sides)
-    return [serve.Request(rid=i, arrival=a, scenario=_Sc(s), steps=n)
-            for i, (s, n, a) in enumerate(zip(sides, steps, arrivals))]
+    grads = grads or [False] * len(sides)
+    return [serve.Request(rid=i, arrival=a, scenario=_Sc(s), steps=n, want_grad=g)
+            for i, (s, n, a, g) in enumerate(zip(sides, steps, arrivals, grads))]
 
 
 def test_every_request_completes_with_its_step_count():
@@ -76,8 +110,8 @@ def test_budget_and_slots_are_never_exceeded():
     budget = 2000
 
     class Checking(FakeBackend):
-        def start(self, r):
-            h = super().start(r)
+        def load(self, r):
+            h = super().load(r)
             live_bytes = sum(s * s for i, s in enumerate(sides) if i in self.live)
             assert live_bytes <= budget
             assert len(self.live) <= 3
@@ -92,7 +126,7 @@ def test_budget_and_slots_are_never_exceeded():
 
 
 def test_admission_follows_arrival_and_overlaps_running_work():
-    be = FakeBackend(polls_per_chunk=50)
+    be = FakeBackend(polls_per_epoch=50)
     clock = ManualClock()
     reqs = _reqs([8, 8, 8], [400, 400, 400], arrivals=[0.0, 0.001, 0.002])
     res = serve.Server(be, hbm_budget_bytes=1e6, chunk=100, clock=clock, sleep=clock.sleep).run(reqs)
@@ -106,6 +140,33 @@ def test_admission_follows_arrival_and_overlaps_running_work():
 def test_request_larger_than_budget_is_rejected():
     with pytest.raises(ValueError, match="budget"):
         serve.Server(FakeBackend(), hbm_budget_bytes=100).run(_reqs([11], [10]))
+
+
+def test_rollouts_advance_together_in_epochs():
+    """All admitted forward rollouts share each epoch; an epoch ends at the nearest finish
+    (or after `chunk` steps), the finished rollouts leave and the others go on."""
+    be = FakeBackend()
+    clock = ManualClock()
+    reqs = _reqs([8, 8, 8, 8], [30, 100, 100, 250])
+    srv = serve.Server(be, hbm_budget_bytes=1e6, chunk=80, clock=clock, sleep=clock.sleep)
+    res = srv.run(reqs, realtime=False)
+    assert [r.state["steps"] for r in res] == [30, 100, 100, 250]
+    ep = [(e["rids"], e["n"]) for e in be.epochs]
+    assert ep[0] == ([0, 1, 2, 3], 30)       # ends where rollout 0 finishes
+    assert ep[1] == ([1, 2, 3], 70)          # rollouts 1 and 2 finish together
+    assert ep[2] == ([3], 80) and ep[3] == ([3], 70)
+    assert srv.epochs == 4
+
+
+def test_gradient_requests_run_beside_the_epochs():
+    be = FakeBackend(grad_polls=5)
+    clock = ManualClock()
+    reqs = _reqs([8, 16, 8], [40, 60, 10], grads=[False, True, False])
+    res = serve.Server(be, hbm_budget_bytes=1e6, chunk=25, clock=clock, sleep=clock.sleep).run(reqs, realtime=False)
+    assert [r.state["steps"] for r in res] == [40, 60, 10]
+    assert res[1].state.get("grad") is True
+    assert all(1 not in e["rids"] for e in be.epochs)
+    assert not be.live
 
 
 def test_summary_percentiles():

@@ -46,10 +46,11 @@ def steric_noalloc(pos, H, W, cfg):
 
 def test_noalloc_steric_matches_rollout_twice():
     cfg = baseline_config()
-    cases = [scenarios.make_scenario(96, 128, 5, 30, seed=41), scenarios.make_scenario(64, 64, 3, 20, seed=42)]
+    cases = [scenarios.make_scenario(96, 128, 5, 30, seed=41), scenarios.make_scenario(64, 64, 3, 20, seed=42),
+             scenarios.make_scenario(60, 90, 3, 16, seed=43)]  # 60 x 90: the mixed-radix FFT path
     refs = [steric_via_rollout(sc, cfg) for sc in cases]
-    # two calls in a row on the shared scratch (different sizes, so leftovers would show)
-    for sc, ref in zip(cases, refs):
+    # calls in a row on the shared scratch (different sizes, so leftovers would show)
+    for sc, ref in zip(cases + cases[:1], refs + refs[:1]):
         pos = torch.as_tensor(sc.position, device="cuda").contiguous()
         got = steric_noalloc(pos, sc.H, sc.W, cfg)
         assert np.isfinite(got).all()
@@ -57,6 +58,29 @@ def test_noalloc_steric_matches_rollout_twice():
         # and against the oracle's update_steric_potential of the same positions
         oref = O.update_steric_potential(sc.H, sc.W, sc.position, cfg.steric_sigma, cfg.steric_scatter_value)
         assert O.rel_l2(got, oref) <= TOL
+
+
+def _crowded_positions(H, W, N, crowd, seed):
+    """N positions on an H x W grid, `crowd` of them inside one 16 x 16 tile (more than the
+    per-tile bin holds, so that tile spills into the overflow list and the arena)."""
+    rng = np.random.default_rng(seed)
+    pos = np.stack([rng.uniform(0, W, N), rng.uniform(0, H, N)], axis=1).astype(np.float32)
+    pos[:crowd] = np.stack([rng.uniform(32, 48, crowd), rng.uniform(48, 64, crowd)], axis=1).astype(np.float32)
+    return pos
+
+
+def test_noalloc_at_its_limits_and_after_smaller_calls():
+    """512 x 512 with 16,384 nodes (the limits), 600 of them in one tile (2,400 deposit
+    entries against a bin of 512); then a small call, then the large one again, and the
+    small one first in a fresh order: each matches the oracle."""
+    cfg = baseline_config()
+    big = (512, 512, _crowded_positions(512, 512, 16384, 600, seed=7))
+    small = (64, 96, _crowded_positions(64, 96, 300, 200, seed=8))
+    for H, W, p in (small, big, small, big, big):
+        got = steric_noalloc(torch.as_tensor(p, device="cuda").contiguous(), H, W, cfg)
+        oref = O.update_steric_potential(H, W, p, cfg.steric_sigma, cfg.steric_scatter_value)
+        assert np.isfinite(got).all()
+        assert O.rel_l2(got, oref) <= TOL, (H, W)
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit():
