@@ -249,7 +249,7 @@ def batch_section(args, flush):
     shape = tuned["lbm_shape"]
     plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs), lbm_shape=shape,
                            fft_values=tuned["fft_values"], bin_threads=tuned["bin_threads"],
-                           bin_sort_capacity=tuned["bin_sort_capacity"])
+                           bin_sort_capacity=tuned["bin_sort_capacity"], ib_cluster=tuned["ib_cluster"])
     stream = torch.cuda.current_stream()
     plan.begin(sts, actuations=acts)
     plan.advance(6, use_graph=True)
@@ -324,7 +324,7 @@ def batch_section(args, flush):
                                  "note": "opt-in steric_method=2, no L2 flush between steps"},
         "autotune": {"dense_pass_shape": {"cells_per_lane": shape[0], "rows_per_cta": shape[1]},
                      "fft_values_per_thread": tuned["fft_values"], "bin_threads": tuned["bin_threads"],
-                     "bin_sort_capacity": tuned["bin_sort_capacity"],
+                     "bin_sort_capacity": tuned["bin_sort_capacity"], "ib_cluster_ctas": tuned["ib_cluster"],
                      "ms_per_step_by_candidate": tune_ms},
         "lbm_ms_per_launch": lbm_ms,
         "kernels_ms_per_step": {k: ms / 10 for k, (ms, n) in prof.items() if n},
@@ -340,7 +340,7 @@ def serve_section(args):
     ~U{16..128}, steps ~U{500..5000}, 20% marked as asking for gradients, served by the
     continuous-batching server (admission by a 180 GB budget; every admitted forward
     rollout advances in shared epochs, one ragged plan per epoch of at most 200
-    graph-replayed steps, ending where the nearest rollout finishes; up to 8 gradient
+    graph-replayed steps, ending where the nearest rollout finishes; up to 16 gradient
     jobs at once beside them).  Latency = completion (state back on the host) minus
     arrival, wall clock.  The plain path runs a sample of the same requests one after
     another, one plan each."""
@@ -348,7 +348,7 @@ def serve_section(args):
     from microcosmos_b200 import baseline_config, serve
     cfg = baseline_config()
     reqs = serve.poisson_requests(args.serve_requests, args.serve_rate, seed=0)
-    be = serve.CudaBackend(cfg, dt=0.01, grad_workers=8)
+    be = serve.CudaBackend(cfg, dt=0.01, grad_workers=16)
     # warm the allocator and the module (one tiny request); not part of the measurement
     serve.run_plain(be, serve.poisson_requests(1, 1.0, seed=99, sides=(64,), filaments=(1, 1), nodes=(16, 16),
                                                steps=(8, 8)))

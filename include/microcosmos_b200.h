@@ -232,6 +232,18 @@ int64_t mc_plan_last_launch_count(const mc_plan* plan);
 mc_status mc_plan_set_fused_ib(mc_plan* plan, int32_t enable);
 int32_t mc_plan_uses_fused_ib(const mc_plan* plan);
 
+/* The multi-direct forcing iterations and the body force of each rollout in one
+ * thread-block cluster of `ctas` CTAs (1..16; 0 = separate launches, the default), phases
+ * separated by the hardware cluster barrier instead of kernel boundaries.  Same arithmetic
+ * and order, identical results.  Pays off when a plan holds many rollouts with few IB
+ * points each (their iterations then run side by side with no launch per phase); a single
+ * large rollout keeps more threads in flight with the separate launches.  Call after
+ * mc_plan_bind, outside a rollout; microcosmos_b200.autotune picks it by timing.
+ * No counterpart in the reference (its iterations are a lax.scan of dense grid ops,
+ * solver/fluid.py:292-316). */
+mc_status mc_plan_set_ib_cluster(mc_plan* plan, int32_t ctas);
+int32_t mc_plan_ib_cluster(const mc_plan* plan);
+
 /* Per-kernel CUDA-event timing.  While enabled, steps are launched directly (no graph)
  * and each kernel launch is bracketed by two events; mc_plan_profile_read() returns the
  * accumulated milliseconds and launch count of one kernel (names from

@@ -133,6 +133,8 @@ SIGNATURES = {
     "mc_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(McState), ctypes.c_void_p]),
     "mc_plan_set_fused_ib": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "mc_plan_uses_fused_ib": (ctypes.c_int32, [ctypes.c_void_p]),
+    "mc_plan_set_ib_cluster": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "mc_plan_ib_cluster": (ctypes.c_int32, [ctypes.c_void_p]),
     "mc_plan_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "mc_plan_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_int64)]),

@@ -7,12 +7,14 @@ Three kernels have a free shape:
   * the power-of-two FFT kernels of the steric filter: each thread holds 4, 8 or 16
     values in registers (more values: fewer instructions per value; fewer: more threads);
   * the tile kernel that sorts the IB and cloud-in-cell contributions: 128 or 256 threads
-    per CTA, and 512 or 1024 contributions per tile sorted in shared memory.
+    per CTA, and 512 or 1024 contributions per tile sorted in shared memory;
+  * the IB iterations: separate launches per phase, or (when asked for) one thread-block
+    cluster of CTAs per rollout with hardware cluster barriers between the phases.
 Which shape is fastest depends on the rollout sizes of a plan (grid widths, how many CTAs
 a step launches, how many tiles carry IB forcing), so the tuner times whole
 graph-replayed steps of the actual plan on scratch copies of the states: first the FFT
 shape, then the dense-pass shapes with the chosen FFT shape, then the tile-kernel CTA
-size with both.  Results are cached per plan signature (sizes, configs, dt) for the life of the
+size with both, then the IB iteration layout.  Results are cached per plan signature (sizes, configs, dt) for the life of the
 process.  The dense-pass shape changes no result; the FFT shape changes the float32
 rounding of the transform only.
 """
@@ -29,6 +31,10 @@ CELLS_PER_LANE = (1, 2, 4)
 ROWS_PER_CTA = (4, 8, 16, 32)
 FFT_VALUES = (4, 8, 16)
 BIN_SHAPES = ((128, 2048), (256, 2048), (128, 1024), (256, 1024), (128, 512))  # (threads per CTA, shared sort capacity)
+# CTAs per rollout cluster of the IB iterations tried besides the separate launches: none by
+# default (measured slower everywhere: 1.886 vs 1.852 ms per 256-rollout batch step with 8
+# CTAs, 0.228 vs 0.168 ms per 1024^2 step with 16); tune(ib_cluster=(...)) tries some
+IB_CLUSTER = ()
 
 _cache: dict[str, tuple[dict, dict]] = {}
 
@@ -69,7 +75,8 @@ def _time(scratch, cfgs, dts, actuations, steps, warmup, **shape):
     return a.elapsed_time(b) / steps
 
 
-def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, fft_values=None, use_cache=True):
+def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, fft_values=None, use_cache=True,
+         ib_cluster=IB_CLUSTER):
     """Time ``steps`` graph-replayed steps of the plan for the candidate shapes and return
     ``(best, timings)``: best = {"lbm_shape": (cells_per_lane, rows_per_cta),
     "fft_values": 4 | 8 | 16, "bin_threads": 128 | 256, "bin_sort_capacity": 512 | 1024 | 2048},
@@ -101,7 +108,15 @@ def tune(states, cfgs, dts, actuations=None, steps=10, warmup=4, shapes=None, ff
                                  fft_values=fft_best, bin_threads=t, bin_sort_capacity=cap)
         timings[f"bins{t}x{cap}"] = bt[(t, cap)]
     bins_best = min(bt, key=bt.get)
-    best = {"lbm_shape": lbm_best, "fft_values": fft_best, "bin_threads": bins_best[0],
+    # the IB iterations: separate launches, or one cluster of CTAs per rollout
+    ct = {0: bt[bins_best]}
+    if any(getattr(c, "enable_fluid", True) for c in cfgs):
+        for c in ib_cluster:
+            ct[c] = _time(scratch, cfgs, dts, actuations, steps, warmup, lbm_shape=lbm_best, fft_values=fft_best,
+                          bin_threads=bins_best[0], bin_sort_capacity=bins_best[1], ib_cluster=c)
+            timings[f"ib_cluster{c}"] = ct[c]
+    cl_best = min(ct, key=ct.get)
+    best = {"lbm_shape": lbm_best, "fft_values": fft_best, "bin_threads": bins_best[0], "ib_cluster": cl_best,
             "bin_sort_capacity": bins_best[1]}
     _cache[key] = (best, timings)
     return best, timings
@@ -111,4 +126,5 @@ def tuned_plan(states, cfgs, dts, actuations=None, **kw) -> Plan:
     """A plan for these rollouts with the autotuned launch shapes."""
     best, _ = tune(states, cfgs, dts, actuations=actuations, **kw)
     return Plan.for_states(states, cfgs, dts, lbm_shape=best["lbm_shape"], fft_values=best["fft_values"],
-                           bin_threads=best["bin_threads"], bin_sort_capacity=best["bin_sort_capacity"])
+                           bin_threads=best["bin_threads"], bin_sort_capacity=best["bin_sort_capacity"],
+                           ib_cluster=best["ib_cluster"])

@@ -1576,9 +1576,10 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   p->ws = (unsigned char*)workspace;
   mc_status st = mc_plan_bind(p->fwd, p->ws + p->r_fwd.off, p->fwd_bytes, stream);
   if (st != MC_OK) return st;
+  std::vector<mc::Upload> ups;
   auto up = [&](const mc_grad_plan::R& r, const void* src, size_t n) -> cudaError_t {
-    if (n == 0) return cudaSuccess;
-    return cudaMemcpyAsync(p->ws + r.off, src, n, cudaMemcpyHostToDevice, s);
+    if (n) ups.push_back({p->ws + r.off, src, n});
+    return cudaSuccess;
   };
   GC(up(p->r_pairs, p->pairs.data(), p->pairs.size() * 4));
   GC(up(p->r_bpairs, p->bpairs.data(), p->bpairs.size() * 4));
@@ -1594,6 +1595,7 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   GC(up(p->r_ce, p->c_edges.data(), p->c_edges.size() * 4));
   GC(up(p->r_cbs, p->c_bstart.data(), p->c_bstart.size() * 4));
   GC(up(p->r_cb, p->c_bps.data(), p->c_bps.size() * 4));
+  GC(mc::stage_uploads(ups.data(), (int)ups.size(), s));
   if (p->rev_graph) {
     cudaGraphExecDestroy(p->rev_graph);
     p->rev_graph = nullptr;
@@ -1601,7 +1603,6 @@ mc_status mc_grad_plan_bind(mc_grad_plan* p, void* workspace, size_t bytes, void
   p->filter_ready = false;
   if (!p->cap_stream) GC(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
   GC(cudaMemsetAsync(p->ws + p->r_cnt.off, 0, p->r_cnt.bytes, s));
-  GC(cudaStreamSynchronize(s));  // the host tables above are temporaries of this call's scope
   const mc_config& c = p->cfg;
   const mc_dims& D = p->dims;
   AD& d = p->ad;
@@ -1872,10 +1873,14 @@ mc_status mc_grad_backward(mc_grad_plan* p, const mc_state_cot* final_cot, mc_st
       a.lf_out = at<float>(w, lfcur ? p->r_lf0 : p->r_lf1);
       if (d.fluid) lfcur ^= 1;
     }
-    GC(cudaMemcpyAsync(w + p->r_sargs.off, p->sargs.data(), len * sizeof(StepArgs), cudaMemcpyHostToDevice, s));
     const int jlast = len - 1;
-    GC(cudaMemcpyAsync(w + p->r_jp.off, &jlast, sizeof(int), cudaMemcpyHostToDevice, s));
-    GC(cudaStreamSynchronize(s));  // the host copies above are sources of asynchronous copies
+    {
+      // staged: the host arrays may change once the call returns, and the host does not
+      // wait here for the stream to reach these copies
+      const mc::Upload u[2] = {{w + p->r_sargs.off, p->sargs.data(), len * sizeof(StepArgs)},
+                               {w + p->r_jp.off, &jlast, sizeof(int)}};
+      GC(mc::stage_uploads(u, 2, s));
+    }
     if (!p->rev_graph || p->rev_graph_act != d.has_act) {
       if (p->rev_graph) {
         cudaGraphExecDestroy(p->rev_graph);

@@ -132,8 +132,8 @@ mc_status mc_env_table_upload(const mc_env* envs, int32_t n, void* table, void* 
     if (e.num_segments > 1 && !e.segment_offsets)
       return env_fail(MC_ERR_INVALID, "mc_env_table_upload: several segments need segment_offsets");
   }
-  cudaError_t err = cudaMemcpyAsync(table, envs, (size_t)n * sizeof(mc_env), cudaMemcpyHostToDevice,
-                                    static_cast<cudaStream_t>(stream));
+  const mc::Upload u{table, envs, (size_t)n * sizeof(mc_env)};
+  cudaError_t err = mc::stage_uploads(&u, 1, static_cast<cudaStream_t>(stream));
   return err == cudaSuccess ? MC_OK : env_fail(MC_ERR_CUDA, cudaGetErrorString(err));
 }
 

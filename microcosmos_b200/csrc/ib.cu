@@ -618,7 +618,8 @@ __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
-__global__ void __launch_bounds__(kIbClusterThreads) k_ib_cluster(const RDesc* __restrict__ D, int n) {
+template <int T>
+__global__ void __launch_bounds__(T) k_ib_cluster(const RDesc* __restrict__ D, int n) {
   unsigned rank, ncta, cid;
   asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
   asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(ncta));
@@ -806,12 +807,12 @@ cudaError_t launch_ib_coop(const Launch& L, int parity) {
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, k_ib_coop, L.d, L.off, L.n, parity);
 }
-// One cluster of `ctas` CTAs per rollout (1 <= ctas <= 16; above 8 the non-portable size
-// is allowed on the kernel first).
-cudaError_t launch_ib_cluster(const RDesc* d, int n, int ctas, cudaStream_t s) {
+// One cluster of `ctas` CTAs of `threads` (256 or 1024) threads per rollout (1 <= ctas <=
+// 16; above 8 the non-portable size is allowed on the kernel first).
+cudaError_t launch_ib_cluster(const RDesc* d, int n, int ctas, int threads, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(n * ctas));
-  cfg.blockDim = dim3(kIbClusterThreads);
+  cfg.blockDim = dim3(threads);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
@@ -821,10 +822,13 @@ cudaError_t launch_ib_cluster(const RDesc* d, int n, int ctas, cudaStream_t s) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_ib_cluster, d, n);
+  if (threads == 1024) return cudaLaunchKernelEx(&cfg, k_ib_cluster<1024>, d, n);
+  return cudaLaunchKernelEx(&cfg, k_ib_cluster<256>, d, n);
 }
 cudaError_t ib_cluster_allow_16() {
-  return cudaFuncSetAttribute(k_ib_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaError_t e = cudaFuncSetAttribute(k_ib_cluster<256>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_ib_cluster<1024>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
 cudaError_t ib_coop_blocks_per_sm(int* out) {
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_ib_coop, 256, 0);

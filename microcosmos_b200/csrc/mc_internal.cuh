@@ -24,7 +24,6 @@ constexpr int kNodeThreads = 128;
 // SMs (measured per batch step: 1.963 ms with 1, 1.965 with 2, 1.973 with 4)
 constexpr int kChainWarps = 1;
 constexpr int kHeadThreads = 128;
-constexpr int kIbClusterThreads = 256;  // threads per CTA of the cluster IB kernel
 constexpr int kLbmTileX = 128;     // dense LBM CTA tile: 32 lanes x 4 cells
 constexpr int kConvTile = 32;     // steric direct convolution: 32 x 32 outputs per CTA
 constexpr int kConvMaxR = 24;     // largest tap radius of the direct convolution       //                    8 rows
@@ -255,7 +254,7 @@ void launch_ib_spread(const Launch& L, int it);
 void launch_ib_finalize(const Launch& L, int parity);
 cudaError_t launch_ib_coop(const Launch& L, int parity);
 cudaError_t ib_coop_blocks_per_sm(int* out);
-cudaError_t launch_ib_cluster(const RDesc* d, int n, int ctas, cudaStream_t s);
+cudaError_t launch_ib_cluster(const RDesc* d, int n, int ctas, int threads, cudaStream_t s);
 cudaError_t ib_cluster_allow_16();
 void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows);
 void launch_collide_heads(const Launch& L, int parity, int write_u);
@@ -275,6 +274,17 @@ void launch_fft_rows_p2(const Launch& L, size_t smem);
 void launch_fft_cols_p2(const Launch& L, size_t smem);
 cudaError_t fft_p2_set_smem(size_t bytes);
 void set_last_error(const char* msg);  // text returned by mc_last_error() on this thread
+
+// Host -> device copies staged through pinned host memory.  A cudaMemcpyAsync from
+// pageable memory first waits for all earlier work of its stream, which would make plan
+// construction and rollout set-up wait for the rollouts already running on that stream;
+// staged copies are enqueued without waiting.  The source may be released on return.
+struct Upload {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+cudaError_t stage_uploads(const Upload* items, int count, cudaStream_t s);
 
 }  // namespace mc
 

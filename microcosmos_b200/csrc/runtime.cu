@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <string>
@@ -126,6 +127,7 @@ struct mc_plan {
   int fft_e = 4;  // values per thread of the register-radix FFT kernels
   bool use_coop = false, coop_cap_checked = false;
   bool fused_ib = false;  // mc_plan_set_fused_ib (separate launches measured faster)
+  int ib_cluster = 0;     // mc_plan_set_ib_cluster: CTAs per rollout cluster (0: separate launches)
   bool coop_possible = false;
   cudaError_t coop_err = cudaSuccess;
   std::vector<RDesc> desc;
@@ -615,7 +617,7 @@ mc::Launch L(mc_plan* p, Kind k, cudaStream_t s) {
 const char* const kProfNames[] = {"predict", "cic_bins",  "fft_rows",    "fft_cols", "chain",
                                    "node",    "ib_bins",   "ib_interp",   "ib_spread", "ib_finalize",
                                    "lbm",     "reaction",  "record_fields", "tick",    "steric",
-                                   "stencil", "ib_fused", "steric_conv", "collide_heads"};
+                                   "stencil", "ib_fused", "steric_conv", "collide_heads", "ib_cluster"};
 constexpr int kNumProf = sizeof(kProfNames) / sizeof(kProfNames[0]);
 
 cudaEvent_t take_event(mc_plan* p) {
@@ -787,6 +789,13 @@ int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
                          p->bin_threads);
   });
   ++k;
+  if (p->ib_cluster > 0 && p->grid[K_NODES]) {
+    timed(p, 19, s, capture, [&] {
+      // a lone rollout needs all the threads a cluster can hold; a batch many small clusters
+      p->coop_err = mc::launch_ib_cluster(at<RDesc>(p->ws, p->r_desc), p->n, p->ib_cluster, p->n == 1 ? 1024 : 256, s);
+    });
+    return k + 1;
+  }
   if (p->use_coop && p->grid[K_NODES]) {
     timed(p, 16, s, capture, [&] { p->coop_err = mc::launch_ib_coop(L(p, K_IBCOOP, s), parity); });
     return k + 1;
@@ -940,6 +949,83 @@ void destroy_graphs(mc_plan* p) {
 namespace mc {
 void set_last_error(const char* msg) { g_err = msg; }
 
+namespace {
+// One process-wide ring of pinned host memory (allocated on first use, kept until the
+// process exits, so that no copy can outlive it).  Each batch of uploads reserves the next
+// span of the ring, copies its sources there and enqueues the device copies, then records
+// an event; a span is reused only after its event has completed (spans are handed out in
+// ring order, so the spans in the way are always the oldest live ones).
+struct StageRing {
+  std::mutex m;
+  char* buf = nullptr;
+  bool failed = false;
+  size_t head = 0;
+  struct Span {
+    size_t lo, hi;
+    cudaEvent_t ev;
+  };
+  std::deque<Span> live;
+  std::vector<cudaEvent_t> pool;
+};
+StageRing g_ring;
+constexpr size_t kRingBytes = size_t(64) << 20;
+}  // namespace
+
+cudaError_t stage_uploads(const Upload* items, int count, cudaStream_t s) {
+  size_t total = 0;
+  for (int i = 0; i < count; ++i) total += (items[i].bytes + 15) & ~size_t(15);
+  if (total == 0) return cudaSuccess;
+  std::lock_guard<std::mutex> lock(g_ring.m);
+  if (!g_ring.buf && !g_ring.failed) {
+    void* b = nullptr;
+    if (cudaHostAlloc(&b, kRingBytes, cudaHostAllocDefault) == cudaSuccess) {
+      g_ring.buf = static_cast<char*>(b);
+    } else {
+      cudaGetLastError();
+      g_ring.failed = true;
+    }
+  }
+  if (!g_ring.buf || total > kRingBytes) {
+    // no staging memory: plain copies (correct, but they wait for the stream)
+    for (int i = 0; i < count; ++i) {
+      if (!items[i].bytes) continue;
+      cudaError_t e = cudaMemcpyAsync(items[i].dst, items[i].src, items[i].bytes, cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  size_t lo = g_ring.head;
+  if (lo + total > kRingBytes) lo = 0;
+  const size_t hi = lo + total;
+  while (!g_ring.live.empty() && g_ring.live.front().lo < hi && lo < g_ring.live.front().hi) {
+    cudaError_t e = cudaEventSynchronize(g_ring.live.front().ev);
+    if (e != cudaSuccess) return e;
+    g_ring.pool.push_back(g_ring.live.front().ev);
+    g_ring.live.pop_front();
+  }
+  size_t off = lo;
+  for (int i = 0; i < count; ++i) {
+    if (!items[i].bytes) continue;
+    std::memcpy(g_ring.buf + off, items[i].src, items[i].bytes);
+    cudaError_t e = cudaMemcpyAsync(items[i].dst, g_ring.buf + off, items[i].bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    off += (items[i].bytes + 15) & ~size_t(15);
+  }
+  cudaEvent_t ev = nullptr;
+  if (!g_ring.pool.empty()) {
+    ev = g_ring.pool.back();
+    g_ring.pool.pop_back();
+  } else {
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+  }
+  cudaError_t e = cudaEventRecord(ev, s);
+  if (e != cudaSuccess) return e;
+  g_ring.live.push_back({lo, hi, ev});
+  g_ring.head = hi;
+  return cudaSuccess;
+}
+
 // Inside a rollout (between mc_rollout_begin and mc_rollout_end) of a one-rollout plan:
 // write the current populations in fields.f_grid layout into dst, leaving the rollout as
 // it is (the gradient plan's segment recompute snapshots every step's input this way).
@@ -967,7 +1053,8 @@ cudaError_t filter_prepare(mc_plan* p, void* dev, const float* in, float* tmp, f
     const int off[2] = {0, cnt[k]};
     std::memcpy(host.data() + align_up(sizeof(RDesc), 256) + 256 * k, off, sizeof(off));
   }
-  cudaError_t e = cudaMemcpyAsync(dev, host.data(), host.size(), cudaMemcpyHostToDevice, s);
+  const Upload u{dev, host.data(), host.size()};
+  cudaError_t e = stage_uploads(&u, 1, s);
   if (e != cudaSuccess) return e;
   return cudaStreamSynchronize(s);  // `host` is a temporary
 }
@@ -1422,9 +1509,10 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
   if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return fail(MC_ERR_WORKSPACE, "workspace must be 256-byte aligned");
   cudaStream_t s = (cudaStream_t)stream;
   p->ws = (char*)workspace;
+  std::vector<mc::Upload> ups;
   auto up = [&](const Region& r, const void* src, size_t n) -> cudaError_t {
-    if (n == 0) return cudaSuccess;
-    return cudaMemcpyAsync(p->ws + r.off, src, n, cudaMemcpyHostToDevice, s);
+    if (n) ups.push_back({p->ws + r.off, src, n});
+    return cudaSuccess;
   };
   for (int i = 0; i < p->n; ++i) {
     HostRollout& h = p->R[i];
@@ -1451,6 +1539,7 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
   }
   for (int k = 0; k < K_COUNT; ++k) MC_CUDA(up(p->r_off[k], p->off[k].data(), p->off[k].size() * 4));
   MC_CUDA(up(p->r_desc, p->desc.data(), p->desc.size() * sizeof(RDesc)));
+  MC_CUDA(mc::stage_uploads(ups.data(), (int)ups.size(), s));
   // zero the binning counters of every tile before the first clear kernel runs
   {
     // The dynamic shared memory limit is a per-kernel attribute shared by every plan of the
@@ -1521,8 +1610,10 @@ mc_status mc_rollout_begin(mc_plan* p, const mc_state* states, const mc_actuatio
     }
     fill_desc(p, i, &st, a, r);
   }
-  MC_CUDA(cudaMemcpyAsync(p->ws + p->r_desc.off, p->desc.data(), p->desc.size() * sizeof(RDesc),
-                          cudaMemcpyHostToDevice, s));
+  {
+    const mc::Upload u{p->ws + p->r_desc.off, p->desc.data(), p->desc.size() * sizeof(RDesc)};
+    MC_CUDA(mc::stage_uploads(&u, 1, s));
+  }
   MC_CUDA(cudaMemsetAsync(at<int>(p->ws, p->r_tdev), 0, sizeof(int), s));
   p->rec_fields = rec_fields;
   p->rec_fluid = rec_fluid;
@@ -1597,6 +1688,22 @@ mc_status mc_plan_set_fused_ib(mc_plan* p, int32_t enable) {
 }
 
 int32_t mc_plan_uses_fused_ib(const mc_plan* p) { return p && p->use_coop ? 1 : 0; }
+
+mc_status mc_plan_set_ib_cluster(mc_plan* p, int32_t ctas) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (p->active) return fail(MC_ERR_INVALID, "cannot change the IB kernel layout inside a rollout");
+  if (ctas < 0 || ctas > 16) return fail(MC_ERR_INVALID, "CTAs per cluster must be in [0, 16]");
+  if (ctas > 8) {
+    cudaError_t e = mc::ib_cluster_allow_16();
+    if (e != cudaSuccess) return cuda_fail(e, "allowing clusters of more than 8 CTAs");
+  }
+  p->ib_cluster = ctas;
+  destroy_graphs(p);
+  return MC_OK;
+}
+
+int32_t mc_plan_ib_cluster(const mc_plan* p) { return p ? p->ib_cluster : 0; }
 
 mc_status mc_plan_profile(mc_plan* p, int32_t enable) {
   if (!p) return fail(MC_ERR_INVALID, "null plan");

@@ -216,7 +216,7 @@ class Plan:
     """A bound plan for a list of rollouts (dims + config + dt + topology each)."""
 
     def __init__(self, specs, device="cuda", lbm_shape=None, steric_method=0, fft_values=0, bin_threads=0,
-                 bin_sort_capacity=0):
+                 bin_sort_capacity=0, ib_cluster=0):
         """specs: list of (H, W, N, pairs(E,2) int32, bending_pairs(B,2) int32, cfg, dt[, (fluid_H, fluid_W)]).
         ``lbm_shape`` = (cells_per_lane, rows_per_cta) of the dense pass (default: the
         library's choice; ``microcosmos_b200.autotune`` picks one by timing).
@@ -224,7 +224,8 @@ class Plan:
         FFT), 1 = FFT, 2 = direct convolution.  ``fft_values``: values per thread of the
         power-of-two FFT kernels (4, 8, 16; 0 = the library's choice).  ``bin_threads``:
         threads per CTA of the contribution-sorting tile kernel (64, 128, 256; 0 = 128).
-        ``bin_sort_capacity``: contributions per tile sorted in shared memory (0 = 2048)."""
+        ``bin_sort_capacity``: contributions per tile sorted in shared memory (0 = 2048).
+        ``ib_cluster``: CTAs per rollout cluster for the IB iterations (0 = separate launches)."""
         _require_cuda()
         lib = _lib.load()
         n = len(specs)
@@ -267,13 +268,15 @@ class Plan:
         self.workspace_bytes = nbytes
         stream = torch.cuda.current_stream().cuda_stream
         _lib.check(lib.mc_plan_bind(h, ctypes.c_void_p(self._ws_ptr), nbytes, ctypes.c_void_p(stream)))
+        if ib_cluster:
+            _lib.check(lib.mc_plan_set_ib_cluster(h, int(ib_cluster)))
 
     @classmethod
     def for_states(cls, states, cfgs, dts, device="cuda", lbm_shape=None, steric_method=0, fft_values=0,
-                   bin_threads=0, bin_sort_capacity=0):
+                   bin_threads=0, bin_sort_capacity=0, ib_cluster=0):
         specs = [(s.H, s.W, s.N, s.pairs, s.bending_pairs, c, d, (s.lH, s.lW)) for s, c, d in zip(states, cfgs, dts)]
         return cls(specs, device=device, lbm_shape=lbm_shape, steric_method=steric_method, fft_values=fft_values,
-                   bin_threads=bin_threads, bin_sort_capacity=bin_sort_capacity)
+                   bin_threads=bin_threads, bin_sort_capacity=bin_sort_capacity, ib_cluster=ib_cluster)
 
     def bin_threads(self):
         return int(_lib.load().mc_plan_bin_threads(self._h))
@@ -340,6 +343,13 @@ class Plan:
 
     def uses_fused_ib(self):
         return bool(_lib.load().mc_plan_uses_fused_ib(self._h))
+
+    def set_ib_cluster(self, ctas):
+        """Run each rollout's IB iterations in one cluster of `ctas` CTAs (0: separate launches)."""
+        _lib.check(_lib.load().mc_plan_set_ib_cluster(self._h, int(ctas)))
+
+    def ib_cluster(self):
+        return int(_lib.load().mc_plan_ib_cluster(self._h))
 
     def profile(self, enable=True):
         _lib.check(_lib.load().mc_plan_profile(self._h, int(bool(enable))))

@@ -44,12 +44,12 @@ def test_autotuner_picks_a_timed_candidate():
     best, timings = autotune.tune(sts, [cfg] * 3, [0.01] * 3, steps=4, warmup=2, use_cache=False)
     assert f"lbm{best['lbm_shape'][0]}x{best['lbm_shape'][1]}" in timings
     assert f"fft{best['fft_values']}" in timings
-    assert len(timings) == len(autotune.candidates(sts)) + 3 + len(autotune.BIN_SHAPES)
+    assert len(timings) == len(autotune.candidates(sts)) + 3 + len(autotune.BIN_SHAPES) + len(autotune.IB_CLUSTER)
     assert all(t > 0 for t in timings.values())
     assert all(torch.equal(a, b.f_grid) for a, b in zip(before, sts))  # caller's states untouched
     plan = autotune.tuned_plan(sts, [cfg] * 3, [0.01] * 3)
     assert plan.lbm_shape() == best["lbm_shape"] and plan.fft_values() == best["fft_values"]
-    assert plan.bin_threads() == best["bin_threads"]
+    assert plan.bin_threads() == best["bin_threads"] and plan.ib_cluster() == best["ib_cluster"]
 
 
 def test_fft_values_per_thread_agree():

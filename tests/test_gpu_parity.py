@@ -288,3 +288,36 @@ def test_plans_of_different_sizes_coexist():
     torch.cuda.synchronize()
     ref = _oracle_run(big, 3)
     assert rel(st_big.position, ref.position) < TOL
+
+
+@pytest.mark.parametrize("ctas", [1, 3, 8, 16])
+def test_cluster_and_separate_ib_kernels_agree(ctas):
+    """The IB iterations in one thread-block cluster per rollout (hardware cluster barriers
+    between the phases) give the same bits as the separate launches, for a batch of rollouts
+    of different sizes (one without nodes) and for a single 1024^2 rollout."""
+    scs = [scenarios.make_scenario(128, 128, 6, 40, seed=31), scenarios.make_scenario(64, 96, 2, 20, seed=32),
+           scenarios.make_scenario(48, 48, 0, 0, seed=33), scenarios.make_scenario(256, 192, 12, 64, seed=34)]
+    cfg = baseline_config()
+    results = []
+    for cl in (0, ctas):
+        sts = [DeviceState.from_scenario(s) for s in scs]
+        plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs), ib_cluster=cl)
+        assert plan.ib_cluster() == cl
+        plan.rollout(sts, 13, actuations=[Actuation.from_scenario(s) for s in scs])
+        torch.cuda.synchronize()
+        assert plan.read_flags() == [0] * len(scs)
+        results.append([st.host() for st in sts])
+    for a, b in zip(*results):
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k])
+    if ctas == 16:
+        sc = scenarios.config_scale(seed=1)
+        outs = []
+        for cl in (0, 16):
+            st = DeviceState.from_scenario(sc)
+            plan = Plan.for_states([st], [cfg], [0.01], ib_cluster=cl)
+            plan.rollout([st], 4, actuations=[Actuation.from_scenario(sc)])
+            torch.cuda.synchronize()
+            outs.append(st.host())
+        for k in outs[0]:
+            np.testing.assert_array_equal(outs[0][k], outs[1][k])
