@@ -128,12 +128,16 @@ __device__ __forceinline__ void head_work(const RDesc& d, const BinView& v, int 
 // touched cell's run.  Tiles of at most capS contributions are sorted in shared memory;
 // larger ones take the global-arena path.  skeys: dynamic shared memory of 4 * capS words, capS <= the
 // bin capacity of every rollout of the launch (a power of two).
+__device__ __forceinline__ int pc(int c) { return c + (c >> 3); }
+
 __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned* skeys, int capS) {
   const int kCapS = capS;
   const int kChunk = 4 * capS;  // keys per shared-memory chunk sort on the spill path
-  __shared__ int cnt[kBinTile * kBinTile];
-  __shared__ int cpos[kBinTile * kBinTile];
-  __shared__ int hpos[kBinTile * kBinTile];  // rank of a touched cell among the tile's touched cells
+  // per-cell counters at padded slots pc(c) = c + c / 8: the scan below gives each lane 8
+  // consecutive cells, and the padding puts the lanes' slots on distinct banks
+  __shared__ int cnt[kBinTile * kBinTile + kBinTile * kBinTile / 8];
+  __shared__ int cpos[kBinTile * kBinTile + kBinTile * kBinTile / 8];
+  __shared__ int hpos[kBinTile * kBinTile + kBinTile * kBinTile / 8];  // rank of a touched cell among the tile's
   __shared__ int tlist[kBinTile * kBinTile];  // the touched cells, by rank
   __shared__ int s_spill, s_heads, s_base, s_fill;
   const BinView v = bin_view(d, which);
@@ -151,7 +155,7 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
     int* kin = reinterpret_cast<int*>(skeys + kCapS);
     int* kout = reinterpret_cast<int*>(skeys + 2 * kCapS);
     float* wout = reinterpret_cast<float*>(skeys + 3 * kCapS);
-    for (int c = tid; c < kBinTile * kBinTile; c += blockDim.x) cnt[c] = 0;
+    for (int c = tid; c < kBinTile * kBinTile; c += blockDim.x) cnt[pc(c)] = 0;
     if (tid == 0) s_heads = 0;
     __syncthreads();
     // counting sort by local cell; positions inside a cell come from shared atomics
@@ -160,7 +164,7 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
       const unsigned e = (unsigned)bin[i];  // (local cell << 24) | k
       const unsigned lc = e >> 24;
       const int k = (int)(e & 0xffffffu);
-      const int pos = atomicAdd(cnt + lc, 1);
+      const int pos = atomicAdd(cnt + pc(lc), 1);
       lr[i] = (lc << 24) | (unsigned)pos;
       kin[i] = k;
     }
@@ -171,7 +175,7 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
       int sum = 0, nz = 0;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        loc[q] = cnt[tid * 8 + q];
+        loc[q] = cnt[tid * 9 + q];  // pc(tid * 8 + q)
         sum += loc[q];
         nz += loc[q] > 0;
       }
@@ -188,8 +192,8 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
       int run = incl - sum, hrun = inz - nz;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        cpos[tid * 8 + q] = run;
-        hpos[tid * 8 + q] = hrun;
+        cpos[tid * 9 + q] = run;
+        hpos[tid * 9 + q] = hrun;
         run += loc[q];
         hrun += loc[q] > 0;
       }
@@ -199,22 +203,22 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
     // one slot range per tile for its touched cells (IB); the touched cells listed by rank
     if (which == 0 && tid == 0) s_base = atomicAdd(v.ctl + 2, s_heads);
     for (int c = tid; c < kBinTile * kBinTile; c += blockDim.x)
-      if (cnt[c] > 0) tlist[hpos[c]] = c;
+      if (cnt[pc(c)] > 0) tlist[hpos[pc(c)]] = c;
     for (int i = tid; i < total; i += blockDim.x) {
       const unsigned key = lr[i];
       const int lc = (int)(key >> 24), pos = (int)(key & 0xffffffu);
       const int k = kin[i];
-      kout[cpos[lc] + pos] = k;
-      wout[cpos[lc] + pos] = v.w[k];
+      kout[cpos[pc(lc)] + pos] = k;
+      wout[cpos[pc(lc)] + pos] = v.w[k];
     }
     __syncthreads();
     // one thread per touched cell: order its run by k (runs are short), then reduce it
     const int nheads = s_heads;
     for (int hi = tid; hi < nheads; hi += blockDim.x) {
       const int c = tlist[hi];
-      const int len = cnt[c];
-      int* rk = kout + cpos[c];
-      float* rw = wout + cpos[c];
+      const int len = cnt[pc(c)];
+      int* rk = kout + cpos[pc(c)];
+      float* rw = wout + cpos[pc(c)];
       for (int a = 1; a < len; ++a) {
         const int key = rk[a];
         const float kw = rw[a];
@@ -233,9 +237,9 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
       if (which == 1) {
         d.dep[cell] = acc;
       } else {
-        const int slot = s_base + hpos[c];
+        const int slot = s_base + hpos[pc(c)];
         for (int j = 0; j < len; ++j) d.ib_slot[rk[j]] = slot;
-        ib_head(d, parity, cell, acc, slot, len, t * v.cap + cpos[c]);
+        ib_head(d, parity, cell, acc, slot, len, t * v.cap + cpos[pc(c)]);
       }
     }
     __syncthreads();
@@ -331,16 +335,23 @@ __device__ void tile_work(const RDesc& d, int which, int parity, int t, unsigned
 }
 
 // The bin tiles that received contributions this step, listed by the producers as
-// (rollout, tile) pairs; a fixed grid of CTAs walks the list (most tiles of a large or
-// batched grid are empty and are never visited).
+// (rollout, tile) pairs (most tiles of a large or batched grid are empty and never
+// listed).  A grid of as many CTAs as the GPU holds at once takes the listed tiles one at
+// a time from a cursor (wl_count[2], reset with the list), so that no CTA is launched only
+// to find nothing to do and uneven tiles balance across the CTAs.
 __global__ void __launch_bounds__(256) k_bin_tiles(const RDesc* __restrict__ D, const int2* __restrict__ wl,
-                                                   const int* __restrict__ wl_count, int which, int parity, int capS) {
+                                                   int* __restrict__ wl_count, int which, int parity, int capS) {
   extern __shared__ unsigned dyn[];
+  __shared__ int s_item;
   const int count = *wl_count;
-  for (int i = blockIdx.x; i < count; i += gridDim.x) {
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(wl_count + 2, 1);
+    __syncthreads();
+    const int i = s_item;
+    if (i >= count) break;  // uniform across the CTA
     const int2 item = wl[i];
     tile_work(D[item.x], which, parity, item.y, dyn, capS);
-    __syncthreads();  // the shared arrays are reused by the next item
+    __syncthreads();  // the shared arrays and s_item are reused by the next item
   }
 }
 
@@ -669,7 +680,10 @@ __global__ void __launch_bounds__(256) k_reaction(const RDesc* __restrict__ D, c
     d.c_ctl[0] = 0;
     d.c_ctl[1] = 0;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) d.wl_ctl[1] = 0;  // the plan's CIC tile list
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    d.wl_ctl[1] = 0;  // the plan's CIC tile list and its cursor
+    d.wl_ctl[3] = 0;
+  }
   if (node >= d.N) return;
   float vx = d.vel[2 * node], vy = d.vel[2 * node + 1];
   if (d.enable_fluid) {
@@ -780,7 +794,10 @@ __global__ void k_record_fields(const RDesc* __restrict__ D, const int* __restri
 
 __global__ void k_tick(int* tdev) { *tdev += 1; }
 
-void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity, int capS,
+cudaError_t tiles_blocks_per_sm(int threads, int capS, int* out) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_bin_tiles, threads, (size_t)4 * capS * sizeof(unsigned));
+}
+void launch_bin_tiles(const Launch& L, const int2* wl, int* wl_count, int which, int parity, int capS,
                       int threads) {
   k_bin_tiles<<<L.grid, threads, (size_t)4 * capS * sizeof(unsigned), L.s>>>(L.d, wl, wl_count, which, parity, capS);
 }

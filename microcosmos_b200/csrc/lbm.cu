@@ -12,58 +12,68 @@
 
 namespace mc {
 
-// Load the 4 (VEC=4) or 1 (VEC=1) populations of direction (cx, cy) pulled to cells
-// x0..x0+VEC-1 of row y.  All lanes of the warp must call this together.
+// Load the VEC populations of direction (cx, cy) pulled to cells x0c..x0c+VEC-1 of a row:
+// `rb` is the element index of the source row (y - cy) in this direction's plane, `xl` / `xr`
+// the wrapped columns left of the lane's first cell and right of its last one.  Aligned
+// vector loads; the +-1 column shifts come from the neighbouring lane by warp shuffle, the
+// warp's edge lanes (and a lane at the lattice's right edge) load their halo value.  All
+// lanes of the warp must call this together.  Indices are 32-bit (9 h w < 2^31 is checked
+// when a plan is built).
 template <int VEC>
-__device__ __forceinline__ void pull_dir(const float* __restrict__ plane, int H, int W, int y, int x0c, int lane,
-                                         int cx, int cy, float v[VEC]) {
-  int ys = y - cy;
-  ys = ys < 0 ? ys + H : (ys >= H ? ys - H : ys);
-  const float* row = plane + (size_t)ys * W;
+__device__ __forceinline__ void pull_dir(const float* __restrict__ h, int rb, int x0c, int xl, int xr, bool edge_l,
+                                         bool edge_r, int cx, float v[VEC]) {
   if (VEC == 4) {
-    float4 a = __ldg(reinterpret_cast<const float4*>(row + x0c));
+    const float4 a = __ldg(reinterpret_cast<const float4*>(h + (rb + x0c)));
     if (cx == 0) {
-      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+      v[0] = a.x; v[1 % VEC] = a.y; v[2 % VEC] = a.z; v[3 % VEC] = a.w;
     } else if (cx == 1) {
       float up = __shfl_up_sync(0xffffffffu, a.w, 1);
-      if (lane == 0) up = __ldg(row + (x0c == 0 ? W - 1 : x0c - 1));
-      v[0] = up; v[1] = a.x; v[2] = a.y; v[3] = a.z;
+      if (edge_l) up = __ldg(h + (rb + xl));
+      v[0] = up; v[1 % VEC] = a.x; v[2 % VEC] = a.y; v[3 % VEC] = a.z;
     } else {
       float dn = __shfl_down_sync(0xffffffffu, a.x, 1);
-      if (lane == 31 || x0c + 4 >= W) dn = __ldg(row + (x0c + 4 >= W ? x0c + 4 - W : x0c + 4));
-      v[0] = a.y; v[1] = a.z; v[2] = a.w; v[3] = dn;
+      if (edge_r) dn = __ldg(h + (rb + xr));
+      v[0] = a.y; v[1 % VEC] = a.z; v[2 % VEC] = a.w; v[3 % VEC] = dn;
     }
   } else if (VEC == 2) {
-    float2 a = __ldg(reinterpret_cast<const float2*>(row + x0c));
+    const float2 a = __ldg(reinterpret_cast<const float2*>(h + (rb + x0c)));
     if (cx == 0) {
       v[0] = a.x; v[1 % VEC] = a.y;
     } else if (cx == 1) {
       float up = __shfl_up_sync(0xffffffffu, a.y, 1);
-      if (lane == 0) up = __ldg(row + (x0c == 0 ? W - 1 : x0c - 1));
+      if (edge_l) up = __ldg(h + (rb + xl));
       v[0] = up; v[1 % VEC] = a.x;
     } else {
       float dn = __shfl_down_sync(0xffffffffu, a.x, 1);
-      if (lane == 31 || x0c + 2 >= W) dn = __ldg(row + (x0c + 2 >= W ? x0c + 2 - W : x0c + 2));
+      if (edge_r) dn = __ldg(h + (rb + xr));
       v[0] = a.y; v[1 % VEC] = dn;
     }
   } else {
-    int xs = x0c - cx;
-    xs = xs < 0 ? xs + W : (xs >= W ? xs - W : xs);
-    v[0] = __ldg(row + xs);
+    v[0] = __ldg(h + (rb + (cx == 0 ? x0c : cx == 1 ? xl : xr)));
   }
 }
 
 // One row of VEC cells per lane: pull, collide, store.  All lanes of the warp call it.
 template <int VEC>
 __device__ __forceinline__ void lbm_row(const RDesc& d, const float* __restrict__ hin, float* __restrict__ hout,
-                                        int H, int W, size_t HW, int y, int x0, int x0c, bool x_ok, int lane,
+                                        int H, int W, int HW, int y, int x0, int x0c, bool x_ok, int lane,
                                         int write_u, float hwp, float hwm, float cp, float cm) {
   float fin[9][VEC];
   {
     const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
     const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+    // element index of row y - cy, for cy = -1, 0, +1 (periodic)
+    const int ym = y == 0 ? H - 1 : y - 1, yp = y == H - 1 ? 0 : y + 1;
+    const int r_cm = yp * W, r_c0 = y * W, r_cp = ym * W;
+    // wrapped halo columns (VEC = 1: the left and right neighbours themselves)
+    const int xl = x0c == 0 ? W - 1 : x0c - 1;
+    const int xr = x0c + VEC >= W ? x0c + VEC - W : x0c + VEC;
+    const bool edge_l = lane == 0, edge_r = lane == 31 || x0c + VEC >= W;
 #pragma unroll
-    for (int i = 0; i < 9; ++i) pull_dir<VEC>(hin + i * HW, H, W, y, x0c, lane, ex[i], ey[i], fin[i]);
+    for (int i = 0; i < 9; ++i) {
+      const int rb = i * HW + (ey[i] == 1 ? r_cp : ey[i] == -1 ? r_cm : r_c0);
+      pull_dir<VEC>(hin, rb, x0c, xl, xr, edge_l, edge_r, ex[i], fin[i]);
+    }
   }
   float out[9][VEC];
   float usx[VEC], usy[VEC];
@@ -97,24 +107,24 @@ __device__ __forceinline__ void lbm_row(const RDesc& d, const float* __restrict_
     for (int i = 0; i < 9; ++i) out[i][c] = o[i];
   }
   if (x_ok) {
-    const size_t base = (size_t)y * W + x0;
+    const int base = y * W + x0;
     if (VEC == 4) {
 #pragma unroll
       for (int i = 0; i < 9; ++i)
-        *reinterpret_cast<float4*>(hout + i * HW + base) = make_float4(out[i][0], out[i][1 % VEC], out[i][2 % VEC],
+        *reinterpret_cast<float4*>(hout + (i * HW + base)) = make_float4(out[i][0], out[i][1 % VEC], out[i][2 % VEC],
                                                                        out[i][3 % VEC]);
       if (write_u) {
         *reinterpret_cast<float4*>(d.fluid_vel + base) = make_float4(usx[0], usx[1 % VEC], usx[2 % VEC], usx[3 % VEC]);
-        *reinterpret_cast<float4*>(d.fluid_vel + HW + base) =
+        *reinterpret_cast<float4*>(d.fluid_vel + (HW + base)) =
             make_float4(usy[0], usy[1 % VEC], usy[2 % VEC], usy[3 % VEC]);
       }
     } else if (VEC == 2) {
 #pragma unroll
       for (int i = 0; i < 9; ++i)
-        *reinterpret_cast<float2*>(hout + i * HW + base) = make_float2(out[i][0], out[i][1 % VEC]);
+        *reinterpret_cast<float2*>(hout + (i * HW + base)) = make_float2(out[i][0], out[i][1 % VEC]);
       if (write_u) {
         *reinterpret_cast<float2*>(d.fluid_vel + base) = make_float2(usx[0], usx[1 % VEC]);
-        *reinterpret_cast<float2*>(d.fluid_vel + HW + base) = make_float2(usy[0], usy[1 % VEC]);
+        *reinterpret_cast<float2*>(d.fluid_vel + (HW + base)) = make_float2(usy[0], usy[1 % VEC]);
       }
     } else {
 #pragma unroll
@@ -148,7 +158,7 @@ __global__ void __launch_bounds__(128) k_lbm(const RDesc* __restrict__ D, const 
   const int x0 = tx * (32 * VEC) + lane * VEC;
   const bool x_ok = x0 < W;
   const int x0c = x_ok ? x0 : (W - VEC);
-  const size_t HW = (size_t)H * W;
+  const int HW = H * W;
   const float* __restrict__ hin = d.h[parity];
   float* __restrict__ hout = d.h[parity ^ 1];
   const float hwp = 0.5f * d.wp, hwm = 0.5f * d.wm;

@@ -68,6 +68,8 @@ struct RDesc {
   int fftW_f[kFftMaxFactors], fftH_f[kFftMaxFactors];
   const float2* twW;  // W roots exp(-2 pi i k / W)
   const float2* twH;
+  const float2* ptW;  // the register-radix passes' twiddles of length W, per pass (pass_twiddles)
+  const float2* ptH;
   const float* gW;    // separable spectral Gaussian / W
   const float* gH;    // ... / H
   // direct-convolution form of the same filter: the periodic kernel of the spectral
@@ -157,7 +159,7 @@ struct RDesc {
   int ridx;            // this rollout's index in the plan
   int2* wl_ib;
   int2* wl_cic;
-  int* wl_ctl;         // [0] IB list length, [1] CIC list length
+  int* wl_ctl;         // [0] IB list length, [1] CIC list length, [2] / [3] their cursors
   // rod components: chains (warp kernel) and general graphs (CTA kernel)
   int nchain, ngeneric;
   const int* chain_comp;    // (nchain) component index
@@ -239,8 +241,11 @@ struct Launch {
 };
 
 void launch_predict(const Launch& L);
-void launch_bin_tiles(const Launch& L, const int2* wl, const int* wl_count, int which, int parity, int capS,
+// wl_count: the list length; wl_count[2] is the cursor the CTAs take tiles from (reset to 0
+// with the list)
+void launch_bin_tiles(const Launch& L, const int2* wl, int* wl_count, int which, int parity, int capS,
                       int threads = 256);
+cudaError_t tiles_blocks_per_sm(int threads, int capS, int* out);
 cudaError_t tiles_set_smem(size_t bytes);
 void launch_fft_rows(const Launch& L, size_t smem);
 void launch_fft_cols(const Launch& L, size_t smem);

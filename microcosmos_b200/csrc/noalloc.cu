@@ -254,8 +254,8 @@ extern "C" mc_status mc_steric_potential_noalloc(const float* position, int32_t 
   mc::launch_predict(l);
   l.off = off + 2;
   l.grid = cnt[1] < 1184 ? cnt[1] : 1184;
-  mc::launch_bin_tiles(l, reinterpret_cast<const int2*>(P(kOffWl)), reinterpret_cast<const int*>(P(kOffWlCtl)) + 1, 1,
-                       0, mc::kCicCap);
+  mc::launch_bin_tiles(l, reinterpret_cast<const int2*>(P(kOffWl)), reinterpret_cast<int*>(P(kOffWlCtl)) + 1, 1, 0,
+                       mc::kCicCap);
   l.off = off + 4;
   l.grid = cnt[2];
   mc::launch_fft_rows(l, (size_t)3 * W * sizeof(float2) + W * sizeof(float));

@@ -26,7 +26,10 @@ __global__ void __launch_bounds__(256) k_predict(const RDesc* __restrict__ D, co
     d.ib_ctl[1] = 0;
     d.ib_ctl[2] = 0;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) d.wl_ctl[0] = 0;  // the plan's IB tile list
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    d.wl_ctl[0] = 0;  // the plan's IB tile list and its cursor
+    d.wl_ctl[2] = 0;
+  }
   if (node >= d.N) return;
   const float px = d.pos[2 * node], py = d.pos[2 * node + 1];
   const float vx = d.vel[2 * node] * d.damping, vy = d.vel[2 * node + 1] * d.damping;

@@ -40,12 +40,6 @@ mc_status cuda_fail(cudaError_t e, const char* where) {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// CTAs of the tile kernel: they walk the list of touched tiles.  Up to 16 times the CTAs
-// the SMs hold at once (148 SMs x 8 of 256 threads' worth), so that the block scheduler
-// keeps balancing uneven tiles to the end (measured on the 256-rollout batch: 2.025 ms per
-// step with 1x, 2.01 with 2x, 2.00 with 4x, 1.988 with 16x, 2.02 with one CTA per tile).
-long long tile_grid_cap(int threads) { return 148LL * 8 * 16 * (256 / threads); }
-int tile_grid_for(long long tiles, int threads) { return (int)std::max(1LL, std::min(tiles, tile_grid_cap(threads))); }
 
 constexpr int kDefaultSortCap = 2048;  // contributions per tile sorted in shared memory by default
 
@@ -82,6 +76,7 @@ struct HostRollout {
   int max_chain = 0;                          // longest chain (nodes)
   std::vector<int> fW, fH;
   std::vector<float2> twW, twH;
+  std::vector<float2> ptW, ptH;  // the register-radix FFT's twiddles laid out per pass (bind time)
   std::vector<float> gW, gH;
   std::vector<float> cgW, cgH;  // direct-convolution taps of the steric filter
   int cRW = 0, cRH = 0;
@@ -99,7 +94,7 @@ struct HostRollout {
       r_svy, r_sinv, r_sucx, r_sucy, r_sfx, r_sfy;
   Region r_ccell, r_cw, r_cstore, r_ctc, r_covf, r_cctl, r_chain, r_generic;
   Region r_pairs, r_bpairs, r_compn, r_compe, r_compb, r_epo, r_epi, r_neo, r_nei, r_edeg, r_ndeg;
-  Region r_twW, r_twH, r_gW, r_gH, r_flags;
+  Region r_twW, r_twH, r_ptW, r_ptH, r_gW, r_gH, r_flags;
 };
 
 }  // namespace
@@ -109,7 +104,8 @@ struct mc_plan {
   std::vector<HostRollout> R;
   size_t ws_bytes = 0;
   Region r_desc, r_tdev, r_wl_ib, r_wl_cic, r_wl_ctl;
-  int tile_grid = 1;  // CTAs walking the tile lists
+  int tile_grid = 1;     // CTAs walking the tile lists (set at bind: as many as the GPU holds)
+  int tile_grid_c = 1;   // the same for the cloud-in-cell tiles (their shared sort capacity differs)
   long long n_tiles = 0;  // bin tiles of all rollouts
   int bin_threads = 128;  // threads per CTA of the tile kernel
   int ib_capS = 0, c_capS = 0;  // largest bin capacity of the plan
@@ -244,6 +240,29 @@ void fft_tables_compute(int N, double sigma, std::vector<float2>& tw, std::vecto
     // numpy.fft.fftfreq abscissa
     const double f = (k < (N + 1) / 2 ? (double)k : (double)(k - N)) / (double)N;
     g[k] = (float)(std::exp(-2.0 * M_PI * M_PI * sigma * sigma * f * f) / (double)N);
+  }
+}
+
+// The twiddles of the register-radix Stockham passes (steric.cu, pass_reg) for a
+// power-of-two length N and E values per thread, laid out per pass: the pass with Ns
+// (the product of the earlier radices) and radix R keeps, for each k < Ns, the R - 1
+// factors tw[(m k) << (log N - log Ns - log R)], m = 1..R-1, at (Ns - 1) + k (R - 1) + m - 1
+// (the passes' tables fill [0, N - 1) exactly).  The same values as the root table, so
+// the transform's results are unchanged; a thread reads its factors from one base address.
+void pass_twiddles(const std::vector<float2>& tw, int E, std::vector<float2>& pt) {
+  const int N = (int)tw.size();
+  pt.assign(N, make_float2(0.f, 0.f));
+  if (N < 2 || (N & (N - 1))) return;
+  int logN = 0;
+  while ((1 << logN) < N) ++logN;
+  const int LE = E == 4 ? 2 : E == 8 ? 3 : 4;
+  int logNs = 0;
+  while (logNs < logN) {
+    const int LR = logNs + LE <= logN ? LE : logN - logNs;
+    const int R = 1 << LR, Ns = 1 << logNs, tsh = logN - logNs - LR;
+    for (int k = 0; k < Ns; ++k)
+      for (int m = 1; m < R; ++m) pt[(Ns - 1) + k * (R - 1) + (m - 1)] = tw[(m * k) << tsh];
+    logNs += LR;
   }
 }
 
@@ -502,6 +521,8 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   for (size_t k = 0; k < h.fH.size(); ++k) d.fftH_f[k] = h.fH[k];
   d.twW = at<float2>(b, h.r_twW);
   d.twH = at<float2>(b, h.r_twH);
+  d.ptW = at<float2>(b, h.r_ptW);
+  d.ptH = at<float2>(b, h.r_ptH);
   d.gW = at<float>(b, h.r_gW);
   d.gH = at<float>(b, h.r_gH);
   d.conv_gW = at<float>(b, h.r_cgW);
@@ -715,7 +736,7 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
   if (p->any_steric) {
     timed(p, 1, s, capture, [&] {
       mc::Launch l = L(p, K_TILES, s);
-      l.grid = p->tile_grid;
+      l.grid = p->tile_grid_c;
       mc::launch_bin_tiles(l, at<int2>(p->ws, p->r_wl_cic), at<int>(p->ws, p->r_wl_ctl) + 1, 1, 0, p->c_smem,
                            p->bin_threads);
     });
@@ -1143,6 +1164,14 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
       delete p;
       return fail(MC_ERR_INVALID, "dt must be > 0");
     }
+    // the dense pass indexes the populations (9, h, w) with 32-bit integers
+    {
+      const long long lh = D.fluid_H > 0 ? D.fluid_H : D.H, lw = D.fluid_W > 0 ? D.fluid_W : D.W;
+      if (9LL * lh * lw >= (1LL << 31)) {
+        delete p;
+        return fail(MC_ERR_UNSUPPORTED, "fluid lattice too large: 9 * h * w must be below 2^31");
+      }
+    }
     // IB points: the nodes, or a synthetic pair per node (fluid.py:244-263)
     const long long NI = (long long)D.N * (c.synthetic_node_width > 0.0f ? 2 : 1);
     const long long M = c.enable_fluid ? NI * c.ibm_kernel_size * c.ibm_kernel_size : 0;
@@ -1271,6 +1300,8 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     h.r_ndeg = lay.take(N * 4);
     h.r_twW = lay.take(h.twW.size() * 8);
     h.r_twH = lay.take(h.twH.size() * 8);
+    h.r_ptW = lay.take(h.twW.size() * 8);
+    h.r_ptH = lay.take(h.twH.size() * 8);
     h.r_gW = lay.take(h.gW.size() * 4);
     h.r_gH = lay.take(h.gH.size() * 4);
     h.r_cgW = lay.take(h.cgW.size() * 4);
@@ -1305,7 +1336,6 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     p->r_wl_cic = lay.take((size_t)tiles * sizeof(int2));
     tiles = std::max(tiles, ltiles);
     p->n_tiles = tiles;
-    p->tile_grid = tile_grid_for(tiles, p->bin_threads);
     for (auto& h : p->R) {
       p->ib_capS = std::max(p->ib_capS, h.ib_cap);
       p->c_capS = std::max(p->c_capS, h.c_cap);
@@ -1389,7 +1419,6 @@ mc_status mc_plan_set_bin_threads(mc_plan* p, int32_t threads) {
   if (threads != 0 && threads != 64 && threads != 128 && threads != 256)
     return fail(MC_ERR_INVALID, "threads must be 0 (default), 64, 128 or 256");
   p->bin_threads = threads ? threads : 128;
-  p->tile_grid = tile_grid_for(p->n_tiles, p->bin_threads);
   return MC_OK;
 }
 
@@ -1531,6 +1560,10 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
     MC_CUDA(up(h.r_generic, h.generic_comp.data(), h.generic_comp.size() * 4));
     MC_CUDA(up(h.r_twW, h.twW.data(), h.twW.size() * 8));
     MC_CUDA(up(h.r_twH, h.twH.data(), h.twH.size() * 8));
+    pass_twiddles(h.twW, p->fft_e, h.ptW);
+    pass_twiddles(h.twH, p->fft_e, h.ptH);
+    MC_CUDA(up(h.r_ptW, h.ptW.data(), h.ptW.size() * 8));
+    MC_CUDA(up(h.r_ptH, h.ptH.data(), h.ptH.size() * 8));
     MC_CUDA(up(h.r_gW, h.gW.data(), h.gW.size() * 4));
     MC_CUDA(up(h.r_gH, h.gH.data(), h.gH.size() * 4));
     MC_CUDA(up(h.r_cgW, h.cgW.data(), h.cgW.size() * 4));
@@ -1559,6 +1592,16 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
     }
   }
   MC_CUDA(cudaMemsetAsync(p->ws + p->r_wl_ctl.off, 0, 4 * sizeof(int), s));
+  {
+    // the tile kernels take listed tiles from a cursor: launch as many CTAs as fit at once
+    int dev = 0, sms = 0, nib = 0, nc = 0;
+    MC_CUDA(cudaGetDevice(&dev));
+    MC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MC_CUDA(mc::tiles_blocks_per_sm(p->bin_threads, std::max(p->ib_smem, 1), &nib));
+    MC_CUDA(mc::tiles_blocks_per_sm(p->bin_threads, std::max(p->c_smem, 1), &nc));
+    p->tile_grid = std::max(1, sms * nib);
+    p->tile_grid_c = std::max(1, sms * nc);
+  }
   mc::launch_clear_ws(L(p, K_CELLS, s));
   MC_CUDA(cudaGetLastError());
   destroy_graphs(p);

@@ -502,7 +502,8 @@ void launch_steric_conv(const Launch& L, size_t smem) {
 // Fewer values per thread give more threads for small problems; more give fewer
 // instructions per value for large batches.  Shared-memory addresses are padded by one
 // element every 16 (a -> a + a / 16) so the strided stores of the first pass spread over
-// the banks.  Twiddles are read from the float64-derived root table.
+// the banks.  Twiddles are the float64-derived roots, read from a table laid out per pass
+// (the host's pass_twiddles) so that a butterfly's R - 1 factors sit at one base address.
 
 __device__ __forceinline__ int pad16(int a) { return a + (a >> 4); }
 
@@ -600,24 +601,26 @@ __device__ __forceinline__ constexpr int dft_slot(int k) {
 
 // One in-place Stockham pass of radix R over a padded buffer of N = 2^logN values,
 // G = N / E threads (local index lt) holding E values each, Ns = 2^logNs.
+// `pt`: this length's per-pass twiddle table (pass_twiddles on the host): the R - 1 factors of
+// butterfly k of the pass with Ns = 2^logNs start at pt[(Ns - 1) + k (R - 1)].
 template <int E, int R>
-__device__ __forceinline__ void pass_reg(float2* buf, int logN, int logNs, int lt, const float2* __restrict__ tw) {
+__device__ __forceinline__ void pass_reg(float2* buf, int logN, int logNs, int lt, const float2* __restrict__ pt) {
   constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
   constexpr int LE = E == 4 ? 2 : E == 8 ? 3 : 4;
   constexpr int C = E / R;  // butterflies per thread
   const int G = 1 << (logN - LE);
   const int S = 1 << (logN - LR);  // butterflies in the pass
   const int Ns = 1 << logNs;
-  const int tsh = logN - logNs - LR;  // twiddle index step as a shift
   float2 v[E];
 #pragma unroll
   for (int c = 0; c < C; ++c) {
     const int j = lt + c * G;
     const int k = j & (Ns - 1);
+    const float2* __restrict__ tk = pt + (Ns - 1) + k * (R - 1) - 1;  // tk[m], m = 1..R-1
 #pragma unroll
     for (int m = 0; m < R; ++m) {
       float2 a = buf[pad16(j + m * S)];
-      if (m > 0 && k > 0) a = cmul(a, __ldg(tw + ((m * k) << tsh)));
+      if (m > 0 && k > 0) a = cmul(a, __ldg(tk + m));
       v[c * R + m] = a;
     }
     dft_reg<R>(v + c * R);
@@ -637,36 +640,36 @@ __device__ __forceinline__ void pass_reg(float2* buf, int logN, int logNs, int l
 
 // Forward transform in place (natural order in and out), N = 2^logN >= E.
 template <int E>
-__device__ __forceinline__ void fft_reg(float2* buf, int logN, int lt, const float2* __restrict__ tw) {
+__device__ __forceinline__ void fft_reg(float2* buf, int logN, int lt, const float2* __restrict__ pt) {
   constexpr int LE = E == 4 ? 2 : E == 8 ? 3 : 4;
   int logNs = 0;
   while (logNs + LE <= logN) {
-    pass_reg<E, E>(buf, logN, logNs, lt, tw);
+    pass_reg<E, E>(buf, logN, logNs, lt, pt);
     logNs += LE;
   }
   const int rem = logN - logNs;
-  if (rem == 1) pass_reg<E, 2>(buf, logN, logNs, lt, tw);
+  if (rem == 1) pass_reg<E, 2>(buf, logN, logNs, lt, pt);
   if constexpr (E >= 8) {
-    if (rem == 2) pass_reg<E, 4>(buf, logN, logNs, lt, tw);
+    if (rem == 2) pass_reg<E, 4>(buf, logN, logNs, lt, pt);
   }
   if constexpr (E >= 16) {
-    if (rem == 3) pass_reg<E, 8>(buf, logN, logNs, lt, tw);
+    if (rem == 3) pass_reg<E, 8>(buf, logN, logNs, lt, pt);
   }
 }
 
 // x -> IFFT(G * FFT(x)) with 1/N folded into g: conj(FFT(conj(G * FFT(x)))).
 template <int E>
-__device__ __forceinline__ void filter_reg(float2* buf, int logN, int lt, const float2* __restrict__ tw,
+__device__ __forceinline__ void filter_reg(float2* buf, int logN, int lt, const float2* __restrict__ pt,
                                            const float* __restrict__ g) {
   const int N = 1 << logN, G = N / E;
-  fft_reg<E>(buf, logN, lt, tw);
+  fft_reg<E>(buf, logN, lt, pt);
   for (int i = lt; i < N; i += G) {
     const float gk = __ldg(g + i);
     const float2 v = buf[pad16(i)];
     buf[pad16(i)] = make_float2(v.x * gk, -(v.y * gk));
   }
   __syncthreads();
-  fft_reg<E>(buf, logN, lt, tw);
+  fft_reg<E>(buf, logN, lt, pt);
 }
 
 // Row pass: 256 / G row pairs per CTA (one packed transform each), G = W / E.
@@ -686,7 +689,7 @@ __global__ void __launch_bounds__(256) k_fftreg_rows(const RDesc* __restrict__ D
   const float* r1 = d.dep + (size_t)(act1 ? y1 : 0) * W;
   for (int x = lt; x < W; x += G) buf[pad16(x)] = make_float2(act0 ? r0[x] : 0.0f, act1 ? r1[x] : 0.0f);
   __syncthreads();
-  filter_reg<E>(buf, logN, lt, d.twW, d.gW);
+  filter_reg<E>(buf, logN, lt, d.ptW, d.gW);
   if (act0) {
     float* o = d.tmp + (size_t)y0 * W;
     for (int x = lt; x < W; x += G) o[x] = buf[pad16(x)].x;
@@ -719,7 +722,7 @@ __global__ void __launch_bounds__(4096 / E) k_fftreg_cols(const RDesc* __restric
   }
   __syncthreads();
   const int tr = threadIdx.x / G, lt = threadIdx.x - tr * G;
-  filter_reg<E>(smr + (size_t)tr * S, logN, lt, d.twH, d.gH);
+  filter_reg<E>(smr + (size_t)tr * S, logN, lt, d.ptH, d.gH);
   for (int idx = threadIdx.x; idx < P * H; idx += blockDim.x) {
     const int y = idx / P, t = idx - y * P;
     const int xr = xbase + 2 * t, xi = xr + 1;
