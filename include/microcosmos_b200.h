@@ -150,6 +150,17 @@ void mc_plan_destroy(mc_plan* plan);
 mc_status mc_plan_set_lbm_shape(mc_plan* plan, int32_t cells_per_lane, int32_t rows_per_cta);
 mc_status mc_plan_get_lbm_shape(const mc_plan* plan, int32_t* cells_per_lane, int32_t* rows_per_cta);
 
+/* Staged dense pass: stages = 2..6 runs the stream+collide pass as a persistent kernel whose
+ * CTAs copy bands of whole lattice rows (about 1024 cells) of the 9 population planes into
+ * shared memory with bulk asynchronous copies, `stages` bands in flight per CTA, and collide
+ * them from there; 0 selects the tiled kernel of mc_plan_set_lbm_shape (which also selects
+ * it).  Needs every fluid lattice width to be a multiple of 4 and at most 1024
+ * (MC_ERR_UNSUPPORTED otherwise).  Results do not depend on the choice.  Only before
+ * mc_plan_bind(); mc_plan_lbm_staging returns the current value (-1 for a null plan).
+ * No counterpart in the reference (XLA chooses its own fusion tiling). */
+mc_status mc_plan_set_lbm_staging(mc_plan* plan, int32_t stages);
+int32_t mc_plan_lbm_staging(const mc_plan* plan);
+
 /* How the steric potential's spectral Gaussian (src/microcosmos/utils.py:35-49) is applied:
  * 1 = FFT along rows, then columns (H, W with prime factors <= 13, at most 4096): the
  *     reference's operator, to float32 rounding;

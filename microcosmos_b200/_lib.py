@@ -119,6 +119,8 @@ SIGNATURES = {
     "mc_plan_bin_sort_capacity": (ctypes.c_int32, [ctypes.c_void_p]),
     "mc_plan_get_lbm_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
                                              ctypes.POINTER(ctypes.c_int32)]),
+    "mc_plan_set_lbm_staging": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "mc_plan_lbm_staging": (ctypes.c_int32, [ctypes.c_void_p]),
     "mc_plan_workspace_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
     "mc_plan_bind": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     "mc_rollout": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(McState), ctypes.c_int32,

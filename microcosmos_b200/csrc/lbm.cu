@@ -53,6 +53,33 @@ __device__ __forceinline__ void pull_dir(const float* __restrict__ h, int rb, in
   }
 }
 
+// One cell of the dense pass: density and velocity of the pulled populations, then the
+// force-free TRT collision (exact fast path when |u| <= vmax / 2, the velocity clamps
+// otherwise) and the EPSIL floor; u* of the cell in (usx, usy).
+__device__ __forceinline__ void dense_cell(const RDesc& d, const float f[9], float hwp, float hwm, float cp,
+                                           float cm, float o[9], float& usx, float& usy) {
+  // rho = max(sum f, 0.1), u = sum e f / rho (fluid.py:136-142)
+  float rho = f[0];
+#pragma unroll
+  for (int i = 1; i < 9; ++i) rho = rho + f[i];
+  rho = max_nan(rho, 0.1f);
+  const float ux = (((((f[1] - f[3]) + f[5]) - f[6]) - f[7]) + f[8]) / rho;
+  const float uy = (((((f[2] - f[4]) + f[5]) + f[6]) - f[7]) - f[8]) / rho;
+  const float usq = ux * ux + uy * uy;
+  if (usq + MC_EPSIL <= d.vmax_q4) {
+    // |u| <= vmax/2: both velocity clamp factors are exactly 1 and F = 0
+    collide_free(f, rho, ux, uy, usq, d.wp, hwp, hwm, o);
+    usx = ux;
+    usy = uy;
+  } else {
+    // the velocity clamps (fluid.py:268-274, 327-339) with the unchanged velocity
+    float r2, vx, vy, Fx, Fy;
+    macroscopic(f, d.vmax, d.vmax_q4, r2, vx, vy);
+    free_cell_force(r2, vx, vy, d.vmax, d.vmax_q4, d.force_clamp, Fx, Fy);
+    collide(f, r2, vx, vy, Fx, Fy, d.wp, d.wm, cp, cm, o, usx, usy);
+  }
+}
+
 // One row of VEC cells per lane: pull, collide, store.  All lanes of the warp call it.
 template <int VEC>
 __device__ __forceinline__ void lbm_row(const RDesc& d, const float* __restrict__ hin, float* __restrict__ hout,
@@ -79,30 +106,10 @@ __device__ __forceinline__ void lbm_row(const RDesc& d, const float* __restrict_
   float usx[VEC], usy[VEC];
 #pragma unroll
   for (int c = 0; c < VEC; ++c) {
-    float f[9];
+    float f[9], o[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) f[i] = fin[i][c];
-    // rho = max(sum f, 0.1), u = sum e f / rho (fluid.py:136-142)
-    float rho = f[0];
-#pragma unroll
-    for (int i = 1; i < 9; ++i) rho = rho + f[i];
-    rho = max_nan(rho, 0.1f);
-    const float ux = (((((f[1] - f[3]) + f[5]) - f[6]) - f[7]) + f[8]) / rho;
-    const float uy = (((((f[2] - f[4]) + f[5]) + f[6]) - f[7]) - f[8]) / rho;
-    const float usq = ux * ux + uy * uy;
-    float o[9];
-    if (usq + MC_EPSIL <= d.vmax_q4) {
-      // |u| <= vmax/2: both velocity clamp factors are exactly 1 and F = 0
-      collide_free(f, rho, ux, uy, usq, d.wp, hwp, hwm, o);
-      usx[c] = ux;
-      usy[c] = uy;
-    } else {
-      // the velocity clamps (fluid.py:268-274, 327-339) with the unchanged velocity
-      float r2, vx, vy, Fx, Fy;
-      macroscopic(f, d.vmax, d.vmax_q4, r2, vx, vy);
-      free_cell_force(r2, vx, vy, d.vmax, d.vmax_q4, d.force_clamp, Fx, Fy);
-      collide(f, r2, vx, vy, Fx, Fy, d.wp, d.wm, cp, cm, o, usx[c], usy[c]);
-    }
+    dense_cell(d, f, hwp, hwm, cp, cm, o, usx[c], usy[c]);
 #pragma unroll
     for (int i = 0; i < 9; ++i) out[i][c] = o[i];
   }
@@ -169,6 +176,178 @@ __global__ void __launch_bounds__(128) k_lbm(const RDesc* __restrict__ D, const 
     const int y = y0 + k * (int)blockDim.y;
     if (y >= H) break;  // uniform across the warp
     lbm_row<VEC>(d, hin, hout, H, W, HW, y, x0, x0c, x_ok, lane, write_u, hwp, hwm, cp, cm);
+  }
+}
+
+// ---------------------------------------------------------------- staged dense pass
+// The same pass with its source rows staged in shared memory by bulk asynchronous copies
+// (cp.async.bulk global -> shared, completion counted in bytes on an mbarrier).  An item is
+// a band of whole lattice rows of one rollout (R = max(1, kStageCells / W) rows, the last
+// band of a rollout shorter); for each of the 9 directions the band's source rows y - cy
+// (periodic, at most two contiguous pieces) are copied into one shared-memory plane, so a
+// population is fetched from HBM once and each bulk copy moves up to 4 KB.  A persistent
+// grid walks the items, each CTA keeping `stages` items in flight: while it collides one
+// band, the next stages - 1 bands are arriving.  Requires lW % 4 == 0 (16-byte rows) and
+// lW <= kStageCells; every cell is collided with exactly the arithmetic of k_lbm.
+// Thread t of an item owns cells 4t .. 4t + 3 of the band (row-major); the +-1 column
+// shifts come from the neighbouring lane by shuffle or, at a warp or row edge, from the
+// row's wrapped column in shared memory.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void bar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void bar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+// bytes: a multiple of 16; both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool bar_test(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for phase `parity` of a stage barrier (about a second at most): false when
+// it gave up.
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, unsigned parity) {
+  for (unsigned it = 0; it < (1u << 24); ++it) {
+    if (bar_test(bar, parity)) return true;
+    if (it >= 32) __nanosleep(64);
+  }
+  return false;
+}
+
+// Thread 0: copy item g's 9 source planes into stage buffer `st`, arming `bar`.
+__device__ __forceinline__ void stage_item(const RDesc* __restrict__ D, const int* __restrict__ off, int n, int g,
+                                           int parity, float* st, uint64_t* bar) {
+  const int r = find_rollout(off, n, g);
+  const RDesc& d = D[r];
+  const int H = d.lH, W = d.lW, R = d.lbm_th;
+  const int y0 = (g - off[r]) * R;
+  const int rows = min(R, H - y0);
+  const int HW = H * W;
+  const float* __restrict__ hin = d.h[parity];
+  const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+  bar_expect_tx(bar, 9u * (unsigned)(rows * W) * 4u);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    int ys = y0 - ey[i];
+    ys = ys < 0 ? ys + H : ys >= H ? ys - H : ys;
+    const int n1 = min(rows, H - ys);
+    float* dst = st + i * kStageCells;
+    bulk_load(dst, hin + (i * HW + ys * W), (unsigned)(n1 * W) * 4u, bar);
+    if (n1 < rows) bulk_load(dst + n1 * W, hin + i * HW, (unsigned)((rows - n1) * W) * 4u, bar);
+  }
+}
+
+__global__ void __launch_bounds__(kStagedThreads, 2)
+    k_lbm_staged(const RDesc* __restrict__ D, const int* __restrict__ off, int n, int nitems, int parity, int write_u,
+                 int stages) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
+  float* buf = reinterpret_cast<float*>(smem_raw + 128);
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (tid == 0) {
+    for (int s = 0; s < stages; ++s) bar_init(bar + s, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int s = 0; s < stages; ++s) {
+      const int g = blockIdx.x + s * gridDim.x;
+      if (g < nitems) stage_item(D, off, n, g, parity, buf + s * 9 * kStageCells, bar + s);
+    }
+  }
+  __syncthreads();
+  for (int j = 0;; ++j) {
+    const int g = blockIdx.x + j * gridDim.x;
+    if (g >= nitems) break;
+    const int s = j % stages;
+    const float* st = buf + s * 9 * kStageCells;
+    const int r = find_rollout(off, n, g);
+    const RDesc& d = D[r];
+    const bool ok = bar_wait(bar + s, (unsigned)(j / stages) & 1u);
+    if (__syncthreads_or(!ok)) {
+      // a copy never completed: flag the rollout, wait (bounded) for this CTA's copies in
+      // flight so that none lands after the CTA has exited, and stop
+      if (tid == 0) {
+        atomicOr(d.flags, 2u);  // MC_FLAG_TIMEOUT
+        for (int k = j; k < j + stages && blockIdx.x + k * gridDim.x < nitems; ++k)
+          bar_wait(bar + k % stages, (unsigned)(k / stages) & 1u);
+      }
+      return;
+    }
+    const int H = d.lH, W = d.lW, R = d.lbm_th;
+    const int y0 = (g - off[r]) * R;
+    const int chunks = min(R, H - y0) * W / 4;
+    const bool active = tid < chunks;
+    const int c = active ? tid : chunks - 1;  // idle lanes shadow the last chunk (shuffles)
+    const int row = (c * 4) / W, x = c * 4 - row * W;
+    const int xl = x == 0 ? W - 1 : x - 1, xr = x + 4 >= W ? x + 4 - W : x + 4;
+    const bool edge_l = lane == 0 || x == 0, edge_r = lane == 31 || x + 4 >= W;
+    const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+    float fin[9][4];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const float* p = st + i * kStageCells + row * W;
+      const float4 a = *reinterpret_cast<const float4*>(p + x);
+      if (ex[i] == 0) {
+        fin[i][0] = a.x; fin[i][1] = a.y; fin[i][2] = a.z; fin[i][3] = a.w;
+      } else if (ex[i] == 1) {
+        float up = __shfl_up_sync(0xffffffffu, a.w, 1);
+        if (edge_l) up = p[xl];
+        fin[i][0] = up; fin[i][1] = a.x; fin[i][2] = a.y; fin[i][3] = a.z;
+      } else {
+        float dn = __shfl_down_sync(0xffffffffu, a.x, 1);
+        if (edge_r) dn = p[xr];
+        fin[i][0] = a.y; fin[i][1] = a.z; fin[i][2] = a.w; fin[i][3] = dn;
+      }
+    }
+    if (active) {
+      const float hwp = 0.5f * d.wp, hwm = 0.5f * d.wm;
+      const float cp = 1.0f - 0.5f * d.wp, cm = 1.0f - 0.5f * d.wm;
+      float out[9][4], usx[4], usy[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float f[9], o[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) f[i] = fin[i][q];
+        dense_cell(d, f, hwp, hwm, cp, cm, o, usx[q], usy[q]);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) out[i][q] = o[i];
+      }
+      const int HW = H * W, base = (y0 + row) * W + x;
+      float* __restrict__ hout = d.h[parity ^ 1];
+#pragma unroll
+      for (int i = 0; i < 9; ++i)
+        *reinterpret_cast<float4*>(hout + (i * HW + base)) = make_float4(out[i][0], out[i][1], out[i][2], out[i][3]);
+      if (write_u) {
+        *reinterpret_cast<float4*>(d.fluid_vel + base) = make_float4(usx[0], usx[1], usx[2], usx[3]);
+        *reinterpret_cast<float4*>(d.fluid_vel + (HW + base)) = make_float4(usy[0], usy[1], usy[2], usy[3]);
+      }
+    }
+    // every thread has read stage s: refill it with the item `stages` ahead
+    __syncthreads();
+    if (tid == 0) {
+      const int gn = g + stages * gridDim.x;
+      if (gn < nitems) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        stage_item(D, off, n, gn, parity, buf + s * 9 * kStageCells, bar + s);
+      }
+    }
   }
 }
 
@@ -280,6 +459,24 @@ void launch_lbm_vec(const Launch& L, int parity, int write_u, int rows) {
     case 4: k_lbm<VEC, 4><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u); break;
     default: k_lbm<VEC, 8><<<L.grid, block, 0, L.s>>>(L.d, L.off, L.n, parity, write_u); break;
   }
+}
+
+size_t lbm_staged_smem(int stages) { return 128 + (size_t)stages * 9 * kStageCells * sizeof(float); }
+
+cudaError_t lbm_staged_set_smem(size_t bytes) {
+  return cudaFuncSetAttribute(k_lbm_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t lbm_staged_blocks_per_sm(int stages, int* out) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_lbm_staged, kStagedThreads, lbm_staged_smem(stages));
+}
+
+// L.grid: the number of items (bands) of the plan; ctas: the persistent grid
+void launch_lbm_staged(const Launch& L, int parity, int write_u, int stages, int ctas) {
+  const int grid = ctas < L.grid ? ctas : L.grid;
+  if (grid <= 0) return;
+  k_lbm_staged<<<grid, kStagedThreads, lbm_staged_smem(stages), L.s>>>(L.d, L.off, L.n, L.grid, parity, write_u,
+                                                                       stages);
 }
 
 // rows: the tile height (2, 4, 8, 16 or 32); up to 4 warps per CTA, each looping over

@@ -25,6 +25,8 @@ constexpr int kNodeThreads = 128;
 constexpr int kChainWarps = 1;
 constexpr int kHeadThreads = 128;
 constexpr int kLbmTileX = 128;     // dense LBM CTA tile: 32 lanes x 4 cells
+constexpr int kStageCells = 1024;  // staged dense pass: lattice cells per item (a band of whole rows)
+constexpr int kStagedThreads = 256;  // ... and threads per CTA (4 cells each)
 constexpr int kConvTile = 32;     // steric direct convolution: 32 x 32 outputs per CTA
 constexpr int kConvMaxR = 24;     // largest tap radius of the direct convolution       //                    8 rows
 constexpr int kIbCap = 1024;       // minimum IB bin capacity per 16x16 tile (grown with node density)
@@ -262,6 +264,10 @@ cudaError_t ib_coop_blocks_per_sm(int* out);
 cudaError_t launch_ib_cluster(const RDesc* d, int n, int ctas, int threads, cudaStream_t s);
 cudaError_t ib_cluster_allow_16();
 void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows);
+void launch_lbm_staged(const Launch& L, int parity, int write_u, int stages, int ctas);
+size_t lbm_staged_smem(int stages);
+cudaError_t lbm_staged_set_smem(size_t bytes);
+cudaError_t lbm_staged_blocks_per_sm(int stages, int* out);
 void launch_collide_heads(const Launch& L, int parity, int write_u);
 void launch_steric_conv(const Launch& L, size_t smem);
 void launch_fftreg_rows(const Launch& L, int values_per_thread);

@@ -108,6 +108,9 @@ struct mc_plan {
   int tile_grid_c = 1;   // the same for the cloud-in-cell tiles (their shared sort capacity differs)
   long long n_tiles = 0;  // bin tiles of all rollouts
   int bin_threads = 128;  // threads per CTA of the tile kernel
+  int lbm_vec = 2, lbm_rows = 4;  // tile of the direct dense-pass kernel: cells per lane, rows per CTA
+  int lbm_stages = 0;       // > 0: the staged dense-pass kernel, with that many bands in flight per CTA
+  int lbm_staged_ctas = 0;  // its persistent grid (set at bind: as many CTAs as the GPU holds)
   int ib_capS = 0, c_capS = 0;  // largest bin capacity of the plan
   int ib_smem = 0, c_smem = 0;  // contributions a tile may hold to be sorted in shared memory
   Region r_off[K_COUNT];
@@ -625,6 +628,41 @@ void fill_desc(mc_plan* p, int i, const mc_state* st, const mc_actuation* act, c
   p->desc[i] = d;
 }
 
+// The staged dense pass copies whole 16-byte aligned rows of at most kStageCells cells.
+bool lbm_staging_fits(const mc_plan* p) {
+  for (const auto& h : p->R)
+    if (h.cfg.enable_fluid && (h.lW % 4 != 0 || h.lW > mc::kStageCells)) return false;
+  return true;
+}
+
+// The dense pass's work table for the plan's current kernel: tiles of lbm_vec * 32 columns x
+// lbm_rows rows (direct kernel) or bands of whole rows of about kStageCells cells (staged
+// kernel), per rollout, and the CTA / item offsets of K_LBM.
+void lbm_tiles(mc_plan* p) {
+  int prev = 0;
+  for (int i = 0; i < p->n; ++i) {
+    HostRollout& h = p->R[i];
+    if (p->lbm_stages > 0) {
+      h.vec = 4;
+      h.lbm_th = std::min(h.lH, std::max(1, mc::kStageCells / h.lW));
+      h.lbm_tx = 1;
+    } else {
+      h.vec = p->lbm_vec;
+      h.lbm_th = p->lbm_rows;
+      h.lbm_tx = div_up(h.lW, 32 * h.vec);
+    }
+    h.lbm_ty = div_up(h.lH, h.lbm_th);
+    if (!p->off[K_LBM].empty()) {
+      p->off[K_LBM][i] = prev;
+      prev += h.cfg.enable_fluid ? h.lbm_tx * h.lbm_ty : 0;
+    }
+  }
+  if (!p->off[K_LBM].empty()) {
+    p->off[K_LBM][p->n] = prev;
+    p->grid[K_LBM] = prev;
+  }
+}
+
 mc::Launch L(mc_plan* p, Kind k, cudaStream_t s) {
   mc::Launch l;
   l.d = at<RDesc>(p->ws, p->r_desc);
@@ -834,7 +872,11 @@ int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
 
 int64_t enqueue_lbm(mc_plan* p, int parity, int write_u, cudaStream_t s, bool capture) {
   if (!p->any_fluid) return 0;
-  timed(p, 10, s, capture, [&] { mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->R[0].vec, p->R[0].lbm_th); });
+  if (p->lbm_stages > 0)
+    timed(p, 10, s, capture,
+          [&] { mc::launch_lbm_staged(L(p, K_LBM, s), parity, write_u, p->lbm_stages, p->lbm_staged_ctas); });
+  else
+    timed(p, 10, s, capture, [&] { mc::launch_lbm(L(p, K_LBM, s), parity, write_u, p->lbm_vec, p->lbm_rows); });
   return 1;
 }
 
@@ -1319,13 +1361,10 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
   for (const auto& h : p->R) plan_cells += (long long)h.lH * h.lW;
   const bool big_plan = plan_cells >= (4LL << 20);
   if (!big_plan && vec_all == 4) vec_all = 2;
-  for (int i = 0; i < n; ++i) {
-    HostRollout& h = p->R[i];
-    h.vec = vec_all;
-    h.lbm_th = big_plan ? 16 : 4;
-    h.lbm_tx = div_up(h.lW, 32 * h.vec);
-    h.lbm_ty = div_up(h.lH, h.lbm_th);
-  }
+  p->lbm_vec = vec_all;
+  p->lbm_rows = big_plan ? 16 : 4;
+  p->lbm_stages = 0;
+  lbm_tiles(p);
   {
     long long tiles = 0, ltiles = 0;
     for (auto& h : p->R) {
@@ -1481,35 +1520,42 @@ mc_status mc_plan_set_lbm_shape(mc_plan* p, int32_t cells_per_lane, int32_t rows
   g_err.clear();
   if (!p) return fail(MC_ERR_INVALID, "null plan");
   if (p->bound) return fail(MC_ERR_INVALID, "the dense-pass tile shape is set before mc_plan_bind()");
-  int vec = cells_per_lane > 0 ? cells_per_lane : p->R[0].vec;
-  int rows = rows_per_cta > 0 ? rows_per_cta : p->R[0].lbm_th;
+  int vec = cells_per_lane > 0 ? cells_per_lane : p->lbm_vec;
+  int rows = rows_per_cta > 0 ? rows_per_cta : p->lbm_rows;
   if (vec != 1 && vec != 2 && vec != 4) return fail(MC_ERR_INVALID, "cells_per_lane must be 1, 2 or 4");
   if (rows != 2 && rows != 4 && rows != 8 && rows != 16 && rows != 32)
     return fail(MC_ERR_INVALID, "rows_per_cta must be 2, 4, 8, 16 or 32");
   for (auto& h : p->R)
     if (h.lW % vec != 0 || h.lW < vec)
       return fail(MC_ERR_UNSUPPORTED, "cells_per_lane must divide every rollout's lattice width");
-  int prev = 0;
-  for (int i = 0; i < p->n; ++i) {
-    HostRollout& h = p->R[i];
-    h.vec = vec;
-    h.lbm_th = rows;
-    h.lbm_tx = div_up(h.lW, 32 * vec);
-    h.lbm_ty = div_up(h.lH, rows);
-    p->off[K_LBM][i] = prev;
-    prev += h.cfg.enable_fluid ? h.lbm_tx * h.lbm_ty : 0;
-  }
-  p->off[K_LBM][p->n] = prev;
-  p->grid[K_LBM] = prev;
+  p->lbm_vec = vec;
+  p->lbm_rows = rows;
+  p->lbm_stages = 0;
+  lbm_tiles(p);
   return MC_OK;
 }
 
 mc_status mc_plan_get_lbm_shape(const mc_plan* p, int32_t* cells_per_lane, int32_t* rows_per_cta) {
   if (!p || !cells_per_lane || !rows_per_cta) return fail(MC_ERR_INVALID, "null argument");
-  *cells_per_lane = p->R[0].vec;
-  *rows_per_cta = p->R[0].lbm_th;
+  *cells_per_lane = p->lbm_vec;
+  *rows_per_cta = p->lbm_rows;
   return MC_OK;
 }
+
+mc_status mc_plan_set_lbm_staging(mc_plan* p, int32_t stages) {
+  g_err.clear();
+  if (!p) return fail(MC_ERR_INVALID, "null plan");
+  if (p->bound) return fail(MC_ERR_INVALID, "the dense-pass staging is set before mc_plan_bind()");
+  if (stages != 0 && (stages < 2 || stages > 6)) return fail(MC_ERR_INVALID, "stages must be 0 or 2..6");
+  if (stages > 0 && !lbm_staging_fits(p))
+    return fail(MC_ERR_UNSUPPORTED, "the staged dense pass needs lattice widths that are multiples of 4 and at most " +
+                                        std::to_string(mc::kStageCells));
+  p->lbm_stages = stages;
+  lbm_tiles(p);
+  return MC_OK;
+}
+
+int32_t mc_plan_lbm_staging(const mc_plan* p) { return p ? p->lbm_stages : -1; }
 
 void mc_plan_destroy(mc_plan* p) {
   if (!p) return;
@@ -1586,6 +1632,11 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
       return fail(MC_ERR_UNSUPPORTED, "shared memory needed by the plan exceeds the device limit");
     MC_CUDA(mc::node_set_smem((size_t)optin));
     MC_CUDA(mc::tiles_set_smem((size_t)optin));
+    if (p->lbm_stages > 0) {
+      if (mc::lbm_staged_smem(p->lbm_stages) > (size_t)optin)
+        return fail(MC_ERR_UNSUPPORTED, "the staged dense pass's shared memory exceeds the device limit");
+      MC_CUDA(mc::lbm_staged_set_smem((size_t)optin));
+    }
     if (p->any_steric) {
       MC_CUDA(mc::fft_set_smem((size_t)optin, (size_t)optin));
       MC_CUDA(mc::fft_p2_set_smem((size_t)optin));
@@ -1601,6 +1652,12 @@ mc_status mc_plan_bind(mc_plan* p, void* workspace, size_t bytes, void* stream) 
     MC_CUDA(mc::tiles_blocks_per_sm(p->bin_threads, std::max(p->c_smem, 1), &nc));
     p->tile_grid = std::max(1, sms * nib);
     p->tile_grid_c = std::max(1, sms * nc);
+    if (p->lbm_stages > 0) {
+      int nl = 0;
+      MC_CUDA(mc::lbm_staged_blocks_per_sm(p->lbm_stages, &nl));
+      if (nl < 1) return fail(MC_ERR_UNSUPPORTED, "the staged dense pass does not fit on an SM");
+      p->lbm_staged_ctas = sms * nl;
+    }
   }
   mc::launch_clear_ws(L(p, K_CELLS, s));
   MC_CUDA(cudaGetLastError());

@@ -216,7 +216,7 @@ class Plan:
     """A bound plan for a list of rollouts (dims + config + dt + topology each)."""
 
     def __init__(self, specs, device="cuda", lbm_shape=None, steric_method=0, fft_values=0, bin_threads=0,
-                 bin_sort_capacity=0, ib_cluster=0):
+                 bin_sort_capacity=0, ib_cluster=0, lbm_stages=None):
         """specs: list of (H, W, N, pairs(E,2) int32, bending_pairs(B,2) int32, cfg, dt[, (fluid_H, fluid_W)]).
         ``lbm_shape`` = (cells_per_lane, rows_per_cta) of the dense pass (default: the
         library's choice; ``microcosmos_b200.autotune`` picks one by timing).
@@ -225,7 +225,11 @@ class Plan:
         power-of-two FFT kernels (4, 8, 16; 0 = the library's choice).  ``bin_threads``:
         threads per CTA of the contribution-sorting tile kernel (64, 128, 256; 0 = 128).
         ``bin_sort_capacity``: contributions per tile sorted in shared memory (0 = 2048).
-        ``ib_cluster``: CTAs per rollout cluster for the IB iterations (0 = separate launches)."""
+        ``ib_cluster``: CTAs per rollout cluster for the IB iterations (0 = separate launches).
+        ``lbm_stages``: 2..6 runs the staged dense pass (row bands copied into shared
+        memory by bulk copies, that many in flight per CTA), 0 the tiled kernel of
+        ``lbm_shape``; None keeps the library's choice (a given ``lbm_shape`` selects the
+        tiled kernel)."""
         _require_cuda()
         lib = _lib.load()
         n = len(specs)
@@ -253,6 +257,8 @@ class Plan:
         self.specs = specs
         if lbm_shape is not None:
             _lib.check(lib.mc_plan_set_lbm_shape(h, int(lbm_shape[0]), int(lbm_shape[1])))
+        if lbm_stages is not None:
+            _lib.check(lib.mc_plan_set_lbm_staging(h, int(lbm_stages)))
         if steric_method:
             _lib.check(lib.mc_plan_set_steric_method(h, int(steric_method)))
         if fft_values:
@@ -273,10 +279,11 @@ class Plan:
 
     @classmethod
     def for_states(cls, states, cfgs, dts, device="cuda", lbm_shape=None, steric_method=0, fft_values=0,
-                   bin_threads=0, bin_sort_capacity=0, ib_cluster=0):
+                   bin_threads=0, bin_sort_capacity=0, ib_cluster=0, lbm_stages=None):
         specs = [(s.H, s.W, s.N, s.pairs, s.bending_pairs, c, d, (s.lH, s.lW)) for s, c, d in zip(states, cfgs, dts)]
         return cls(specs, device=device, lbm_shape=lbm_shape, steric_method=steric_method, fft_values=fft_values,
-                   bin_threads=bin_threads, bin_sort_capacity=bin_sort_capacity, ib_cluster=ib_cluster)
+                   bin_threads=bin_threads, bin_sort_capacity=bin_sort_capacity, ib_cluster=ib_cluster,
+                   lbm_stages=lbm_stages)
 
     def bin_threads(self):
         return int(_lib.load().mc_plan_bin_threads(self._h))
@@ -289,8 +296,12 @@ class Plan:
         """1: FFT, 2: direct convolution, 3: mixed across rollouts, 0: no steric."""
         return int(_lib.load().mc_plan_steric_method(self._h))
 
+    def lbm_stages(self):
+        """Bands in flight per CTA of the staged dense pass (0: the tiled kernel)."""
+        return int(_lib.load().mc_plan_lbm_staging(self._h))
+
     def lbm_shape(self):
-        """(cells_per_lane, rows_per_cta) of the dense pass."""
+        """(cells_per_lane, rows_per_cta) of the tiled dense-pass kernel."""
         a, b = ctypes.c_int32(), ctypes.c_int32()
         _lib.check(_lib.load().mc_plan_get_lbm_shape(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
