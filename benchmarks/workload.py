@@ -13,7 +13,8 @@ Workloads (seeded synthetic inputs):
   small  one 128x128 lattice, 4 filaments x 32 nodes
   batch  a population of uneven rollouts (side U{128..512}, 1-32 filaments x 16-128 nodes)
          as one plan with the library's default launch shapes
-  grad   the 256x256, 8 x 48 differentiation workload: forward with checkpoints + backward
+  grad   the 256x256, 8 x 48 differentiation workload (--grad-size picks another): forward with
+         checkpoints + backward
   gym    --rollouts LineEnv environments (128x128, 16 nodes) stepped together by BatchedEnv
 Steps are launched directly (no CUDA graph) unless --graph is given, so that every kernel
 launch is visible to a profiler.
@@ -35,6 +36,8 @@ def main(argv=None):
     ap.add_argument("--rollouts", type=int, default=64)
     ap.add_argument("--graph", action="store_true")
     ap.add_argument("--side", type=int, default=1024, help="lattice side of the scale workload")
+    ap.add_argument("--grad-size", type=int, nargs=3, default=(256, 8, 48), metavar=("SIDE", "FILAMENTS", "NODES"),
+                    help="lattice side, filaments and nodes per filament of the grad workload")
     ap.add_argument("--lbm-shape", type=int, nargs=2, default=None, metavar=("CELLS_PER_LANE", "ROWS"),
                     help="dense-pass tile shape (default: the library's)")
     a = ap.parse_args(argv)
@@ -46,7 +49,8 @@ def main(argv=None):
     cfg = baseline_config()
     if a.workload == "grad":
         from microcosmos_b200.autodiff import GradPlan
-        sc = scenarios.make_scenario(256, 256, 8, 48, seed=0, amp=0.2, period=200.0)
+        side, nf, nn = a.grad_size
+        sc = scenarios.make_scenario(side, side, nf, nn, seed=0, amp=0.2, period=200.0)
         st = DeviceState.from_scenario(sc)
         plan = GradPlan(sc.H, sc.W, st.N, sc.pairs, sc.bending_pairs, cfg, 0.01, a.steps)
         plan.forward(st, Actuation.from_scenario(sc))

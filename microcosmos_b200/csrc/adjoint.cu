@@ -234,18 +234,23 @@ __global__ void k_pred(AD d) {
 }
 
 // ------------------------------------------------------------------ tape: PBD iterates (one CTA)
-__device__ __forceinline__ float bend_corr(const AD& d, const float* th, int b) {
-  const int2 bp = d.bpairs[b];
+// bending correction of pair (e_in, e_out) from the angles th_in = theta[e_in], th_out = theta[e_out]
+__device__ __forceinline__ float bend_corr_v(float th_in, float th_out, float rest, float kb) {
   const float pi = (float)M_PI;
-  const float diff = mc::fmod_floor((th[bp.y] - th[bp.x]) + pi, (float)(2.0 * M_PI)) - pi;
-  return ((diff - d.rest[b]) * d.kb[b]) * 0.5f;
+  const float diff = mc::fmod_floor((th_out - th_in) + pi, (float)(2.0 * M_PI)) - pi;
+  return ((diff - rest) * kb) * 0.5f;
 }
 
-__device__ __forceinline__ float2 edge_force(const AD& d, const float2* p, float thn, int e) {
-  const int2 pr = d.pairs[e];
-  const float L0 = d.rest_len[e];
+__device__ __forceinline__ float bend_corr(const AD& d, const float* th, int b) {
+  const int2 bp = d.bpairs[b];
+  return bend_corr_v(th[bp.x], th[bp.y], d.rest[b], d.kb[b]);
+}
+
+// stretch + shear force of an edge from its endpoints a = p[src], b = p[tgt], its new angle
+// and its rest length
+__device__ __forceinline__ float2 edge_force_v(const AD& d, float2 a, float2 b, float thn, float L0) {
   const float tx = cosf(thn) * L0, ty = sinf(thn) * L0;
-  const float2 cur = mc::min_image(p[pr.y].x, p[pr.y].y, p[pr.x].x, p[pr.x].y, (float)d.W, (float)d.H);
+  const float2 cur = mc::min_image(b.x, b.y, a.x, a.y, (float)d.W, (float)d.H);
   const float L = sqrtf(cur.x * cur.x + cur.y * cur.y);
   const float m = mc::max_prop(L, 1e-8f);
   const float sx = (cur.x / m) * (L - L0), sy = (cur.y / m) * (L - L0);
@@ -253,10 +258,139 @@ __device__ __forceinline__ float2 edge_force(const AD& d, const float2* p, float
   return make_float2(((sx + shx * d.kshear) * d.kstretch) * 0.5f, ((sy + shy * d.kshear) * d.kstretch) * 0.5f);
 }
 
+__device__ __forceinline__ float2 edge_force(const AD& d, const float2* p, float thn, int e) {
+  const int2 pr = d.pairs[e];
+  return edge_force_v(d, p[pr.x], p[pr.y], thn, d.rest_len[e]);
+}
+
+// Rod components whose edges, nodes and bending pairs fit one per thread, with at most
+// kPbdGather incidences each (chains: 2), keep their topology in registers for all C
+// iterations: each phase of an iteration then waits for one round of independent loads of
+// the iterates instead of a chain of index loads.  Same operands and summation order as the
+// general loops below, so the same bits.
+constexpr int kPbdGather = 4;
+
+struct PbdEdgeReg {  // an edge and its bending pairs (edge pass of the forward)
+  int e = -1, nb = 0;
+  int2 bp[kPbdGather];
+  float rest[kPbdGather], kb[kPbdGather];
+  bool neg[kPbdGather];
+  float edeg = 1.0f;
+};
+
+struct PbdNodeReg {  // a node and its incident edges
+  int n = -1, ne = 0;
+  int e[kPbdGather];
+  int2 pr[kPbdGather];
+  float L0[kPbdGather];
+  bool neg[kPbdGather];
+  float ndeg = 1.0f;
+};
+
+// loads thread t's edge / node of component c; false when a list is too long for registers
+__device__ __forceinline__ bool pbd_load_edge(const AD& d, int ie, int eb, PbdEdgeReg& r) {
+  if (ie >= eb) return true;
+  r.e = d.c_edges[ie];
+  const int qa = d.e_start[r.e], qb = d.e_start[r.e + 1];
+  r.nb = qb - qa;
+  if (r.nb > kPbdGather) return false;
+#pragma unroll
+  for (int q = 0; q < kPbdGather; ++q)
+    if (q < r.nb) {
+      const int en = d.e_list[qa + q];
+      r.bp[q] = d.bpairs[en >> 1];
+      r.rest[q] = d.rest[en >> 1];
+      r.kb[q] = d.kb[en >> 1];
+      r.neg[q] = en & 1;
+    }
+  r.edeg = d.edeg[r.e];
+  return true;
+}
+
+__device__ __forceinline__ bool pbd_load_node(const AD& d, int in, int nb, PbdNodeReg& r) {
+  if (in >= nb) return true;
+  r.n = d.c_nodes[in];
+  const int qa = d.n_start[r.n], qb = d.n_start[r.n + 1];
+  r.ne = qb - qa;
+  if (r.ne > kPbdGather) return false;
+#pragma unroll
+  for (int q = 0; q < kPbdGather; ++q)
+    if (q < r.ne) {
+      const int en = d.n_list[qa + q];
+      r.e[q] = en >> 1;
+      r.pr[q] = d.pairs[en >> 1];
+      r.L0[q] = d.rest_len[en >> 1];
+      r.neg[q] = en & 1;
+    }
+  r.ndeg = d.ndeg[r.n];
+  return true;
+}
+
 // one CTA per rod component: the components never interact in the PBD passes
 __global__ void __launch_bounds__(kPbdThreads) k_pbd_fwd(AD d) {
   const int c = blockIdx.x;
   const int ea = d.c_estart[c], eb = d.c_estart[c + 1], na = d.c_nstart[c], nb = d.c_nstart[c + 1];
+  {
+    PbdEdgeReg re;
+    PbdNodeReg rn;
+    bool ok = eb - ea <= (int)blockDim.x && nb - na <= (int)blockDim.x;
+    if (ok) ok = pbd_load_edge(d, ea + threadIdx.x, eb, re) && pbd_load_node(d, na + threadIdx.x, nb, rn);
+    if (__syncthreads_and(ok)) {
+      for (int k = 0; k < d.C; ++k) {
+        const float* th = d.tt + (size_t)k * d.E;
+        float* thn = d.tt + (size_t)(k + 1) * d.E;
+        if (re.e >= 0) {
+          float tin[kPbdGather], tout[kPbdGather];
+#pragma unroll
+          for (int q = 0; q < kPbdGather; ++q)
+            if (q < re.nb) {
+              tin[q] = th[re.bp[q].x];
+              tout[q] = th[re.bp[q].y];
+            }
+          const float th_e = th[re.e];
+          float acc = 0.0f;
+#pragma unroll
+          for (int q = 0; q < kPbdGather; ++q)
+            if (q < re.nb) {
+              const float cr = bend_corr_v(tin[q], tout[q], re.rest[q], re.kb[q]);
+              acc = acc + (re.neg[q] ? -cr : cr);
+            }
+          thn[re.e] = th_e + (acc / re.edeg) * 1.8f;
+        }
+        __syncthreads();
+        const float2* p = d.pp + (size_t)k * d.N;
+        float2* pn = d.pp + (size_t)(k + 1) * d.N;
+        if (rn.n >= 0) {
+          float2 pa[kPbdGather], pb[kPbdGather];
+          float tq[kPbdGather];
+#pragma unroll
+          for (int q = 0; q < kPbdGather; ++q)
+            if (q < rn.ne) {
+              pa[q] = p[rn.pr[q].x];
+              pb[q] = p[rn.pr[q].y];
+              tq[q] = thn[rn.e[q]];
+            }
+          const float2 self = p[rn.n];
+          float ax = 0.0f, ay = 0.0f;
+#pragma unroll
+          for (int q = 0; q < kPbdGather; ++q)
+            if (q < rn.ne) {
+              const float2 f = edge_force_v(d, pa[q], pb[q], tq[q], rn.L0[q]);
+              if (rn.neg[q]) {
+                ax = ax + (-f.x);
+                ay = ay + (-f.y);
+              } else {
+                ax = ax + f.x;
+                ay = ay + f.y;
+              }
+            }
+          pn[rn.n] = make_float2(self.x + ax / rn.ndeg, self.y + ay / rn.ndeg);
+        }
+        __syncthreads();
+      }
+      return;
+    }
+  }
   for (int k = 0; k < d.C; ++k) {
     const float* th = d.tt + (size_t)k * d.E;
     float* thn = d.tt + (size_t)(k + 1) * d.E;
@@ -732,6 +866,136 @@ __global__ void k_node_adj(AD d) {
 }
 
 // ------------------------------------------------------------------ adjoint: PBD iterations (one CTA per rod component)
+// The reverse iterations of a component whose edges, nodes and bending pairs fit one per
+// thread (kPbdGather incidences at most): topology in registers, the accumulated cotangents
+// of the owned edge / pair (d_len, rest_acc, d_kb) in registers and written once.  Same
+// arithmetic and order as the general loops of k_pbd_rev.  All threads of the CTA call it;
+// false (nothing done) when the component does not fit.
+__device__ __forceinline__ bool pbd_rev_fast(const AD& d, int ea, int eb, int na, int nb, int ba, int bb, float ks,
+                                             float kst) {
+  const int tid = threadIdx.x;
+  PbdNodeReg rn;
+  int e = -1, ne3 = 0, b = -1;
+  int2 pr = make_int2(0, 0), bp = make_int2(0, 0);
+  float ns = 1.0f, nt = 1.0f, L0 = 0.0f, ed_x = 1.0f, ed_y = 1.0f, kbb = 0.0f, rst = 0.0f;
+  int bq[kPbdGather];
+  bool negq[kPbdGather];
+  bool ok = eb - ea <= (int)blockDim.x && nb - na <= (int)blockDim.x && bb - ba <= (int)blockDim.x;
+  if (ok) ok = pbd_load_node(d, na + tid, nb, rn);
+  if (ok && ea + tid < eb) {
+    e = d.c_edges[ea + tid];
+    pr = d.pairs[e];
+    ns = d.ndeg[pr.x];
+    nt = d.ndeg[pr.y];
+    L0 = d.rest_len[e];
+    const int qa = d.e_start[e];
+    ne3 = d.e_start[e + 1] - qa;
+    if (ne3 > kPbdGather) ok = false;
+#pragma unroll
+    for (int q = 0; q < kPbdGather; ++q)
+      if (q < ne3) {
+        const int en = d.e_list[qa + q];
+        bq[q] = en >> 1;
+        negq[q] = en & 1;
+      }
+  }
+  if (ok && ba + tid < bb) {
+    b = d.c_bps[ba + tid];
+    bp = d.bpairs[b];
+    ed_x = d.edeg[bp.x];
+    ed_y = d.edeg[bp.y];
+    kbb = d.kb[b];
+    rst = d.rest[b];
+  }
+  if (!__syncthreads_and(ok)) return false;
+  float acc_len = e >= 0 ? d.d_len[e] : 0.0f;
+  float acc_rest = b >= 0 ? d.rest_acc[b] : 0.0f;
+  float acc_kb = b >= 0 ? d.d_kb[b] : 0.0f;
+  int cur = 0;
+  for (int k = d.C - 1; k >= 0; --k) {
+    const float2* p = d.pp + (size_t)k * d.N;
+    const float* th = d.tt + (size_t)k * d.E;
+    const float* thn = d.tt + (size_t)(k + 1) * d.E;
+    const float2* lpi = d.lp[cur];
+    float2* lpo = d.lp[cur ^ 1];
+    const float* lti = d.lt[cur];
+    float* lto = d.lt[cur ^ 1];
+    // position pass
+    if (e >= 0) {
+      const float2 la = lpi[pr.x], lb = lpi[pr.y], pa = p[pr.x], pb = p[pr.y];
+      const float th_n = thn[e], lt_e = lti[e];
+      const float hx = ((la.x / ns - lb.x / nt) * kst) * 0.5f;
+      const float hy = ((la.y / ns - lb.y / nt) * kst) * 0.5f;
+      const float2 cur_v = mc::min_image(pb.x, pb.y, pa.x, pa.y, (float)d.W, (float)d.H);
+      const float L = sqrtf(cur_v.x * cur_v.x + cur_v.y * cur_v.y);
+      const float m = mc::max_prop(L, 1e-8f);
+      const float a = (L - L0) / m;
+      const float da = (1.0f / m - (L - L0) * dmaxf(L, 1e-8f) / (m * m)) / L;
+      const float lsx = (1.0f - ks) * hx, lsy = (1.0f - ks) * hy;
+      const float sdot = cur_v.x * lsx + cur_v.y * lsy;
+      const float lcx = ks * hx + a * lsx + (sdot * da) * cur_v.x;
+      const float lcy = ks * hy + a * lsy + (sdot * da) * cur_v.y;
+      const float ltx = -ks * hx, lty = -ks * hy;
+      float cs, sn;
+      sincosf(th_n, &sn, &cs);
+      acc_len += -sdot / m + (cs * ltx + sn * lty);
+      d.lthn[e] = lt_e + L0 * (-sn * ltx + cs * lty);
+      d.lcur[e] = make_float2(lcx, lcy);
+    }
+    __syncthreads();
+    if (rn.n >= 0) {
+      float2 lc[kPbdGather];
+#pragma unroll
+      for (int q = 0; q < kPbdGather; ++q)
+        if (q < rn.ne) lc[q] = d.lcur[rn.e[q]];
+      float ax = lpi[rn.n].x, ay = lpi[rn.n].y;
+#pragma unroll
+      for (int q = 0; q < kPbdGather; ++q)
+        if (q < rn.ne) {
+          if (rn.neg[q]) {
+            ax += lc[q].x;
+            ay += lc[q].y;
+          } else {
+            ax -= lc[q].x;
+            ay -= lc[q].y;
+          }
+        }
+      lpo[rn.n] = make_float2(ax, ay);
+    }
+    if (b >= 0) {
+      const float lx = d.lthn[bp.x], ly = d.lthn[bp.y], tx = th[bp.x], ty = th[bp.y];
+      const float lcorr = 1.8f * (lx / ed_x - ly / ed_y);
+      const float g = lcorr * kbb * 0.5f;
+      d.gb[b] = g;
+      acc_rest -= g;
+      const float pi = (float)M_PI;
+      const float diff = mc::fmod_floor((ty - tx) + pi, (float)(2.0 * M_PI)) - pi;
+      acc_kb += lcorr * (diff - rst) * 0.5f;
+    }
+    __syncthreads();
+    if (e >= 0) {
+      float gq[kPbdGather];
+#pragma unroll
+      for (int q = 0; q < kPbdGather; ++q)
+        if (q < ne3) gq[q] = d.gb[bq[q]];
+      float a = d.lthn[e];
+#pragma unroll
+      for (int q = 0; q < kPbdGather; ++q)
+        if (q < ne3) a += negq[q] ? gq[q] : -gq[q];
+      lto[e] = a;
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  if (e >= 0) d.d_len[e] = acc_len;
+  if (b >= 0) {
+    d.rest_acc[b] = acc_rest;
+    d.d_kb[b] = acc_kb;
+  }
+  __syncthreads();
+  return true;
+}
+
 __global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d) {
   const int t = d.sa[*d.jp].t;
   const int c = blockIdx.x;
@@ -739,6 +1003,9 @@ __global__ void __launch_bounds__(kPbdThreads) k_pbd_rev(AD d) {
   const int ba = d.c_bstart[c], bb = d.c_bstart[c + 1];
   int cur = 0;
   const float ks = d.kshear, kst = d.kstretch;
+  if (pbd_rev_fast(d, ea, eb, na, nb, ba, bb, ks, kst))
+    cur = d.C & 1;
+  else
   for (int k = d.C - 1; k >= 0; --k) {
     const float2* p = d.pp + (size_t)k * d.N;
     const float* th = d.tt + (size_t)k * d.E;
