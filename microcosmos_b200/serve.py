@@ -225,9 +225,16 @@ class Server:
 
     def __init__(self, backend, hbm_budget_bytes: float = 180e9, max_active: int = 256, chunk: int = 200,
                  depth: int = 2, clock: Callable[[], float] | None = None, sleep: Callable[[float], None] | None = None,
-                 keep_state: bool = True):
+                 keep_state: bool = True, epoch_cells: int | None = None):
+        """``epoch_cells``: None advances every admitted forward rollout in each epoch; a
+        number makes each epoch take the rollouts with the least remaining work (remaining
+        steps x lattice cells) first, up to that many lattice cells in total (at least one
+        rollout), so that short requests finish early while long ones wait for room."""
         if chunk < 1 or depth < 1 or max_active < 1:
             raise ValueError("chunk, depth and max_active must be >= 1")
+        if epoch_cells is not None and epoch_cells < 1:
+            raise ValueError("epoch_cells must be >= 1")
+        self.epoch_cells = epoch_cells
         self.backend = backend
         self.budget = float(hbm_budget_bytes)
         self.max_active = int(max_active)
@@ -306,7 +313,7 @@ class Server:
                     progressed = True
             # queue the next epoch over every admitted rollout with steps left
             if len(queued) < self.depth:
-                members = [rid for rid, (r, h, issued, _) in fwd.items() if issued < r.steps]
+                members = self._epoch_members(fwd)
                 if members:
                     n = min([self.chunk] + [fwd[rid][0].steps - fwd[rid][2] for rid in members])
                     eh = be.launch_epoch([fwd[rid][1] for rid in members], n, [fwd[rid][2] for rid in members])
@@ -325,6 +332,26 @@ class Server:
             else:
                 self.sleep(0)
         return sorted(results, key=lambda x: x.rid)
+
+
+    def _epoch_members(self, fwd):
+        """The admitted forward rollouts with steps left that the next epoch advances."""
+        cand = [rid for rid, (r, h, issued, _) in fwd.items() if issued < r.steps]
+        if self.epoch_cells is None:
+            return cand
+
+        def cells(rid):
+            sc = fwd[rid][0].scenario
+            return sc.H * sc.W
+
+        cand.sort(key=lambda rid: ((fwd[rid][0].steps - fwd[rid][2]) * cells(rid), rid))
+        members, total = [], 0
+        for rid in cand:
+            if members and total + cells(rid) > self.epoch_cells:
+                continue
+            members.append(rid)
+            total += cells(rid)
+        return members
 
 
 def run_plain(backend, requests: list[Request]):

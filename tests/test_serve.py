@@ -158,6 +158,28 @@ def test_rollouts_advance_together_in_epochs():
     assert srv.epochs == 4
 
 
+def test_least_remaining_work_epochs():
+    """With a cell budget per epoch, each epoch takes the rollouts with the least remaining
+    work (steps left x cells) up to the budget: the short requests finish first, every
+    request still completes with its step count, and no epoch exceeds the budget unless it
+    holds a single rollout."""
+    be = FakeBackend()
+    clock = ManualClock()
+    # cells: 64, 64, 256, 1024; remaining work 64*300, 64*40, 256*40, 1024*20
+    reqs = _reqs([8, 8, 16, 32], [300, 40, 40, 20])
+    srv = serve.Server(be, hbm_budget_bytes=1e6, chunk=50, clock=clock, sleep=clock.sleep, epoch_cells=400)
+    res = srv.run(reqs, realtime=False)
+    assert [r.state["steps"] for r in res] == [300, 40, 40, 20]
+    cells = {0: 64, 1: 64, 2: 256, 3: 1024}
+    for e in be.epochs:
+        assert len(e["rids"]) == 1 or sum(cells[r] for r in e["rids"]) <= 400
+    assert be.epochs[0]["rids"] == [1, 2, 0]  # 2,560 < 10,240 < 19,200; rollout 3 (20,480) waits
+    done = [rid for kind, rid in be.log if kind == "finish"]
+    assert done.index(1) < done.index(3) and done.index(2) < done.index(3)
+    with pytest.raises(ValueError):
+        serve.Server(be, epoch_cells=0)
+
+
 def test_gradient_requests_run_beside_the_epochs():
     be = FakeBackend(grad_polls=5)
     clock = ManualClock()
