@@ -1013,14 +1013,19 @@ namespace mc {
 void set_last_error(const char* msg) { g_err = msg; }
 
 namespace {
-// One process-wide ring of pinned host memory (allocated on first use, kept until the
-// process exits, so that no copy can outlive it).  Each batch of uploads reserves the next
-// span of the ring, copies its sources there and enqueues the device copies, then records
-// an event; a span is reused only after its event has completed (spans are handed out in
-// ring order, so the spans in the way are always the oldest live ones).
+// Rings of pinned host memory, one per host thread that uploads (a thread's ring goes back to
+// a free list when the thread exits, for the next new thread; rings are never freed, so that
+// no copy can outlive its source).  Each batch of uploads reserves the next span of the
+// calling thread's ring, copies its sources there and enqueues the device copies, then
+// records an event; a span is reused only after its event has completed (spans are handed
+// out in ring order, so the spans in the way are always the oldest live ones).  A thread
+// therefore only ever waits for its own earlier uploads: a ring shared by all threads made a
+// thread wait for another thread's stream (a serving loop's next epoch behind a gradient
+// job's queued reverse steps).  A ring grows (after its live spans complete) when one batch
+// does not fit.
 struct StageRing {
-  std::mutex m;
   char* buf = nullptr;
+  size_t cap = 0;
   bool failed = false;
   size_t head = 0;
   struct Span {
@@ -1030,25 +1035,71 @@ struct StageRing {
   std::deque<Span> live;
   std::vector<cudaEvent_t> pool;
 };
-StageRing g_ring;
-constexpr size_t kRingBytes = size_t(64) << 20;
+constexpr size_t kRingBytes = size_t(16) << 20;  // initial size of a thread's ring
+std::mutex g_rings_m;
+std::vector<StageRing*> g_free_rings;
+struct RingHolder {
+  StageRing* r = nullptr;
+  ~RingHolder() {
+    if (!r) return;
+    std::lock_guard<std::mutex> lock(g_rings_m);
+    g_free_rings.push_back(r);
+  }
+};
+thread_local RingHolder t_ring;
+
+StageRing& my_ring() {
+  if (!t_ring.r) {
+    std::lock_guard<std::mutex> lock(g_rings_m);
+    if (!g_free_rings.empty()) {
+      t_ring.r = g_free_rings.back();
+      g_free_rings.pop_back();
+    } else {
+      t_ring.r = new StageRing;
+    }
+  }
+  return *t_ring.r;
+}
+
+// Wait for the ring's oldest live span; false on a CUDA error (returned in *err).
+bool retire_oldest(StageRing& g, cudaError_t* err) {
+  const cudaError_t e = cudaEventSynchronize(g.live.front().ev);
+  if (e != cudaSuccess) {
+    *err = e;
+    return false;
+  }
+  g.pool.push_back(g.live.front().ev);
+  g.live.pop_front();
+  return true;
+}
 }  // namespace
 
 cudaError_t stage_uploads(const Upload* items, int count, cudaStream_t s) {
   size_t total = 0;
   for (int i = 0; i < count; ++i) total += (items[i].bytes + 15) & ~size_t(15);
   if (total == 0) return cudaSuccess;
-  std::lock_guard<std::mutex> lock(g_ring.m);
-  if (!g_ring.buf && !g_ring.failed) {
+  StageRing& g = my_ring();
+  cudaError_t err = cudaSuccess;
+  if (!g.failed && (!g.buf || total > g.cap)) {
+    // first use, or a batch larger than the ring: (re)allocate once nothing is in flight
+    while (!g.live.empty())
+      if (!retire_oldest(g, &err)) return err;
+    size_t want = g.cap ? g.cap : kRingBytes;
+    while (want < total) want *= 2;
+    if (g.buf) cudaFreeHost(g.buf);
+    g.buf = nullptr;
+    g.cap = 0;
+    g.head = 0;
     void* b = nullptr;
-    if (cudaHostAlloc(&b, kRingBytes, cudaHostAllocDefault) == cudaSuccess) {
-      g_ring.buf = static_cast<char*>(b);
+    if (cudaHostAlloc(&b, want, cudaHostAllocDefault) == cudaSuccess) {
+      g.buf = static_cast<char*>(b);
+      g.cap = want;
     } else {
       cudaGetLastError();
-      g_ring.failed = true;
+      g.failed = true;
     }
   }
-  if (!g_ring.buf || total > kRingBytes) {
+  if (!g.buf) {
     // no staging memory: plain copies (correct, but they wait for the stream)
     for (int i = 0; i < count; ++i) {
       if (!items[i].bytes) continue;
@@ -1057,35 +1108,31 @@ cudaError_t stage_uploads(const Upload* items, int count, cudaStream_t s) {
     }
     return cudaSuccess;
   }
-  size_t lo = g_ring.head;
-  if (lo + total > kRingBytes) lo = 0;
+  size_t lo = g.head;
+  if (lo + total > g.cap) lo = 0;
   const size_t hi = lo + total;
-  while (!g_ring.live.empty() && g_ring.live.front().lo < hi && lo < g_ring.live.front().hi) {
-    cudaError_t e = cudaEventSynchronize(g_ring.live.front().ev);
-    if (e != cudaSuccess) return e;
-    g_ring.pool.push_back(g_ring.live.front().ev);
-    g_ring.live.pop_front();
-  }
+  while (!g.live.empty() && g.live.front().lo < hi && lo < g.live.front().hi)
+    if (!retire_oldest(g, &err)) return err;
   size_t off = lo;
   for (int i = 0; i < count; ++i) {
     if (!items[i].bytes) continue;
-    std::memcpy(g_ring.buf + off, items[i].src, items[i].bytes);
-    cudaError_t e = cudaMemcpyAsync(items[i].dst, g_ring.buf + off, items[i].bytes, cudaMemcpyHostToDevice, s);
+    std::memcpy(g.buf + off, items[i].src, items[i].bytes);
+    cudaError_t e = cudaMemcpyAsync(items[i].dst, g.buf + off, items[i].bytes, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return e;
     off += (items[i].bytes + 15) & ~size_t(15);
   }
   cudaEvent_t ev = nullptr;
-  if (!g_ring.pool.empty()) {
-    ev = g_ring.pool.back();
-    g_ring.pool.pop_back();
+  if (!g.pool.empty()) {
+    ev = g.pool.back();
+    g.pool.pop_back();
   } else {
     cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     if (e != cudaSuccess) return e;
   }
   cudaError_t e = cudaEventRecord(ev, s);
   if (e != cudaSuccess) return e;
-  g_ring.live.push_back({lo, hi, ev});
-  g_ring.head = hi;
+  g.live.push_back({lo, hi, ev});
+  g.head = hi;
   return cudaSuccess;
 }
 
