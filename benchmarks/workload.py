@@ -40,6 +40,8 @@ def main(argv=None):
                     help="lattice side, filaments and nodes per filament of the grad workload")
     ap.add_argument("--lbm-shape", type=int, nargs=2, default=None, metavar=("CELLS_PER_LANE", "ROWS"),
                     help="dense-pass tile shape (default: the library's)")
+    ap.add_argument("--lbm-stages", type=int, default=None,
+                    help="staged dense pass with this many row bands in flight per CTA (0: tiled)")
     a = ap.parse_args(argv)
     import numpy as np
     import torch
@@ -85,7 +87,7 @@ def main(argv=None):
     sts = [DeviceState.from_scenario(s) for s in scs]
     acts = [Actuation.from_scenario(s) for s in scs]
     plan = Plan.for_states(sts, [cfg] * len(scs), [0.01] * len(scs),
-                           lbm_shape=tuple(a.lbm_shape) if a.lbm_shape else None)
+                           lbm_shape=tuple(a.lbm_shape) if a.lbm_shape else None, lbm_stages=a.lbm_stages)
     plan.begin(sts, actuations=acts)
     plan.advance(a.warmup, use_graph=a.graph)
     plan.advance(a.steps, use_graph=a.graph, last=True)
