@@ -41,6 +41,7 @@ sys.path.insert(0, HERE)
 
 METRIC = "lattice MLUPS & rollouts/s batched vs plain on 1 B200; p50/p99 latency"
 BYTES_PER_CELL = 72  # 9 fp32 populations read + 9 written per cell per step
+QUEUE_SPIN_CYCLES = 1_000_000  # device spin after each L2 flush (about 0.5 ms at 1.965 GHz)
 
 
 def parse():
@@ -602,13 +603,17 @@ def main():
     plan = Plan.for_states([st], [cfg], [0.01])
     # L2 flush between timed steps: write a 256 MiB buffer (evicts the rollout's data), then
     # read another 256 MiB buffer, so that the write's dirty lines are written back here and
-    # not during the next timed step
+    # not during the next timed step.  Then a spin kernel that touches no memory holds the
+    # stream for about 0.5 ms while the host enqueues the step behind it, so the step's
+    # events and kernels run back to back on the device instead of each waiting for the
+    # host's launch call (which otherwise lands inside the per-kernel event pairs).
     flush_w = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     flush_r = torch.zeros(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def flush():
         flush_w.zero_()
         flush_r.sum()
+        torch.cuda._sleep(QUEUE_SPIN_CYCLES)
     stream = torch.cuda.current_stream()
 
     # ---------------- device-resident timed region

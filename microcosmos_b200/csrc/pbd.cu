@@ -533,7 +533,26 @@ __global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, cons
     }
     return;
   }
+  // descriptor values the iterations use, held in registers for the whole loop
+  const float Wf = (float)d.W, Hf = (float)d.H, ksh = d.k_shear, kst = d.k_stretch;
   for (int it = 0; it < cycles; ++it) {
+    // The part of each edge force that depends only on the positions (min-image segment,
+    // length, stretch term: edge_force's first half) is taken before the bending pass, whose
+    // chain of shuffles and angle updates it then overlaps; the angle-dependent half follows
+    // it.  Same expressions as edge_force, so the same bits.
+    float xn[P], yn[P], sgx[P], sgy[P], stx[P], sty[P];
+    shift_next<P>(x, xn);
+    shift_next<P>(y, yn);
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      const float2 cur = min_image(xn[q], yn[q], x[q], y[q], Wf, Hf);
+      const float L = sqrtf(cur.x * cur.x + cur.y * cur.y);
+      const float Lc = max_prop(L, 1e-8f);
+      sgx[q] = cur.x;
+      sgy[q] = cur.y;
+      stx[q] = (cur.x / Lc) * (L - l0[q]);
+      sty[q] = (cur.y / Lc) * (L - l0[q]);
+    }
     float nx[P], pv[P], c[P];
     shift_next<P>(th, nx);
 #pragma unroll
@@ -549,16 +568,17 @@ __global__ void __launch_bounds__(128) k_chain(const RDesc* __restrict__ D, cons
         th[q] = th[q] + (acc * edg[q]) * 1.8f;
       }
     }
-    float xn[P], yn[P], fx[P], fy[P], fxp[P], fyp[P];
-    shift_next<P>(x, xn);
-    shift_next<P>(y, yn);
+    float fx[P], fy[P], fxp[P], fyp[P];
 #pragma unroll
     for (int q = 0; q < P; ++q) {
       fx[q] = fy[q] = 0.0f;
       if (lane * P + q < ne) {
-        const float2 f = edge_force(d, th[q], l0[q], x[q], y[q], xn[q], yn[q]);
-        fx[q] = f.x;
-        fy[q] = f.y;
+        float sn, cs;
+        sincosf(th[q], &sn, &cs);
+        const float tx = cs * l0[q], ty = sn * l0[q];
+        const float shx = (sgx[q] - tx) - stx[q], shy = (sgy[q] - ty) - sty[q];
+        fx[q] = ((stx[q] + shx * ksh) * kst) * 0.5f;
+        fy[q] = ((sty[q] + shy * ksh) * kst) * 0.5f;
       }
     }
     shift_prev<P>(fx, fxp);
