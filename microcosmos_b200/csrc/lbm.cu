@@ -490,6 +490,18 @@ void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows) {
     launch_lbm_vec<1>(L, parity, write_u, rows);
 }
 
+// Whether f is one of the dense-pass kernels (tiled shapes or the staged form).
+bool is_dense_pass_kernel(const void* f) {
+  const void* ks[] = {(const void*)k_lbm<1, 1>, (const void*)k_lbm<1, 2>, (const void*)k_lbm<1, 4>,
+                      (const void*)k_lbm<1, 8>, (const void*)k_lbm<2, 1>, (const void*)k_lbm<2, 2>,
+                      (const void*)k_lbm<2, 4>, (const void*)k_lbm<2, 8>, (const void*)k_lbm<4, 1>,
+                      (const void*)k_lbm<4, 2>, (const void*)k_lbm<4, 4>, (const void*)k_lbm<4, 8>,
+                      (const void*)k_lbm_staged};
+  for (const void* k : ks)
+    if (k == f) return true;
+  return false;
+}
+
 void launch_collide_heads(const Launch& L, int parity, int write_u) {
   k_collide_heads<<<L.grid, kHeadThreads, 0, L.s>>>(L.d, L.off, L.n, parity, write_u);
 }

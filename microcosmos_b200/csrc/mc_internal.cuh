@@ -188,17 +188,14 @@ __device__ __forceinline__ int find_rollout(const int* __restrict__ off, int n, 
 // For |x| < 2y, fmodf(x, y) is x or x -/+ y, and both subtractions are exact (Sterbenz),
 // so the shortcut below returns the same bits as the fmodf route.
 __device__ __forceinline__ float fmod_floor(float x, float y) {
-  float r;
   if (fabsf(x) < 2.0f * y) {
-    if (x >= 0.0f) {
-      r = (x >= y) ? x - y : x;
-    } else {
-      r = (x <= -y) ? x + y : x;
-      if (r < 0.0f) r += y;
-    }
-    return r;
+    // both signs' results are formed and one is selected (no divergent branch)
+    const float rp = (x >= y) ? x - y : x;
+    float rn = (x <= -y) ? x + y : x;
+    rn = (rn < 0.0f) ? rn + y : rn;
+    return (x >= 0.0f) ? rp : rn;
   }
-  r = fmodf(x, y);
+  float r = fmodf(x, y);
   if (r != 0.0f && ((r < 0.0f) != (y < 0.0f))) r += y;
   return r;
 }
@@ -264,6 +261,7 @@ cudaError_t ib_coop_blocks_per_sm(int* out);
 cudaError_t launch_ib_cluster(const RDesc* d, int n, int ctas, int threads, cudaStream_t s);
 cudaError_t ib_cluster_allow_16();
 void launch_lbm(const Launch& L, int parity, int write_u, int vec, int rows);
+bool is_dense_pass_kernel(const void* f);
 void launch_lbm_staged(const Launch& L, int parity, int write_u, int stages, int ctas);
 size_t lbm_staged_smem(int stages);
 cudaError_t lbm_staged_set_smem(size_t bytes);
@@ -273,7 +271,7 @@ void launch_steric_conv(const Launch& L, size_t smem);
 void launch_fftreg_rows(const Launch& L, int values_per_thread);
 void launch_fft12_rows(const Launch& L);
 void launch_fft12_cols(const Launch& L);
-void launch_fftreg_cols(const Launch& L, int values_per_thread);
+void launch_fftreg_cols(const Launch& L, int values_per_thread, int values_per_cta);
 void launch_reaction(const Launch& L, const int* tdev);
 void launch_record_fields(const Launch& L, const int* tdev);
 void launch_unstream(const Launch& L);

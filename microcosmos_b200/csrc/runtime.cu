@@ -124,6 +124,7 @@ struct mc_plan {
   int max_chain = 0, chain_slots = 1;
   int max_k = 0;  // largest IB kernel size of the plan
   int fft_e = 4;  // values per thread of the register-radix FFT kernels
+  int fft_tv = 4096;  // values per CTA of the register-radix column pass (4096 or 2048)
   bool use_coop = false, coop_cap_checked = false;
   bool fused_ib = false;  // mc_plan_set_fused_ib (separate launches measured faster)
   int ib_cluster = 0;     // mc_plan_set_ib_cluster: CTAs per rollout cluster (0: separate launches)
@@ -717,8 +718,8 @@ void timed(mc_plan* p, int kind, cudaStream_t s, bool capture, F&& launch) {
 // lbm(t); ib(t+1) joins both.  Per-step field recording needs lbm(t) before tail(t)'s
 // field copy and before pipeline(t+1) rewrites the steric field, so it runs sequentially.
 // e: values per thread of the register-radix kernels (4, 8 or 16); a side of length N takes
-// them when it is a power of two with E <= N <= 256 E
-StericCtas steric_ctas(const HostRollout& h, int e) {
+// them when it is a power of two with E <= N <= 256 E.  tv: values per column-pass CTA.
+StericCtas steric_ctas(const HostRollout& h, int e, int tv) {
   StericCtas c;
   if (!h.cfg.enable_steric) return c;
   if (h.use_conv) {
@@ -729,7 +730,7 @@ StericCtas steric_ctas(const HostRollout& h, int e) {
   if (h.logW >= 4 && W >= e && W <= 256 * e) c.fr16 = div_up(div_up(H, 2), 256 * e / W);
   else if (three_pow2(W)) c.fr12 = div_up(div_up(H, 2), 256 / (W / 12));
   else c.fftr2 = div_up(div_up(H, 2), h.P_r);
-  if (h.logH >= 4 && H >= e && H <= 256 * e) c.fc16 = div_up(div_up(W, 2), 4096 / H);
+  if (h.logH >= 4 && H >= e && H <= 256 * e) c.fc16 = div_up(div_up(W, 2), tv / H);
   else if (three_pow2(H)) c.fc12 = div_up(div_up(W, 2), 384 / (H / 12));
   else c.fftc2 = div_up(W, 2 * h.P_c);
   return c;
@@ -747,12 +748,28 @@ int default_fft_values(const std::vector<HostRollout>& R) {
   return 4;
 }
 
+// Values per CTA of the register-radix column pass: 4096, or 2048 when that many would give
+// the plan fewer than two column CTAs per SM (148 SMs) and every such side fits 2048.
+int default_fft_cols_tv(const std::vector<HostRollout>& R, int e) {
+  long long ctas = 0;
+  int maxH = 0;
+  for (auto& h : R) {
+    const StericCtas c = steric_ctas(h, e, 4096);
+    if (c.fc16) {
+      ctas += c.fc16;
+      maxH = std::max(maxH, h.dims.H);
+    }
+  }
+  return (ctas > 0 && ctas < 2 * 148 && maxH <= 2048) ? 2048 : 4096;
+}
+
 void recount_steric(mc_plan* p);
 
 void recount_steric(mc_plan* p) {
+  p->fft_tv = default_fft_cols_tv(p->R, p->fft_e);
   for (int k : {K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16, K_FR12, K_FC12}) p->off[k][0] = 0;
   for (int i = 0; i < p->n; ++i) {
-    const StericCtas c = steric_ctas(p->R[i], p->fft_e);
+    const StericCtas c = steric_ctas(p->R[i], p->fft_e, p->fft_tv);
     p->off[K_FFTR2][i + 1] = p->off[K_FFTR2][i] + c.fftr2;
     p->off[K_FFTC2][i + 1] = p->off[K_FFTC2][i] + c.fftc2;
     p->off[K_SCONV][i + 1] = p->off[K_SCONV][i] + c.sconv;
@@ -796,7 +813,7 @@ int64_t enqueue_pipeline(mc_plan* p, cudaStream_t s, bool capture) {
       ++k;
     }
     if (p->grid[K_FC16]) {
-      timed(p, 3, s, capture, [&] { mc::launch_fftreg_cols(L(p, K_FC16, s), p->fft_e); });
+      timed(p, 3, s, capture, [&] { mc::launch_fftreg_cols(L(p, K_FC16, s), p->fft_e, p->fft_tv); });
       ++k;
     }
     if (p->grid[K_FC12]) {
@@ -943,6 +960,38 @@ int64_t enqueue_body(mc_plan* p, int parity, int write_u, int rec_fields, bool h
   return k;
 }
 
+// Kernel-node priorities of a captured step graph: the dense pass (off the step's critical
+// path: only the touched-cell collision waits for it) gets the device's lowest priority and
+// every other kernel (the IB chain, the node pipeline) the highest, so that whenever CTAs of
+// both are waiting, the block scheduler starts the critical path's first.  The graph is
+// instantiated with cudaGraphInstantiateFlagUseNodePriority; priorities change no result.
+cudaError_t prioritise_graph(cudaGraph_t graph) {
+  int least = 0, greatest = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (e != cudaSuccess) return e;
+  size_t n = 0;
+  e = cudaGraphGetNodes(graph, nullptr, &n);
+  if (e != cudaSuccess || n == 0) return e;
+  std::vector<cudaGraphNode_t> nodes(n);
+  e = cudaGraphGetNodes(graph, nodes.data(), &n);
+  if (e != cudaSuccess) return e;
+  for (size_t i = 0; i < n; ++i) {
+    cudaGraphNodeType t;
+    e = cudaGraphNodeGetType(nodes[i], &t);
+    if (e != cudaSuccess) return e;
+    if (t != cudaGraphNodeTypeKernel) continue;
+    cudaKernelNodeParams kp;
+    e = cudaGraphKernelNodeGetParams(nodes[i], &kp);
+    if (e != cudaSuccess) return e;
+    cudaKernelNodeAttrValue v;
+    std::memset(&v, 0, sizeof(v));
+    v.priority = mc::is_dense_pass_kernel(kp.func) ? least : greatest;
+    e = cudaGraphKernelNodeSetAttribute(nodes[i], cudaKernelNodeAttributePriority, &v);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 mc_status run_steps(mc_plan* p, int num, int use_graph, int last, cudaStream_t s, int64_t& launches) {
   const int recv = p->rec_fields ? (p->rec_fluid ? 2 : 1) : 0;
   // the first step of this call needs its node pipeline unless the previous call left it
@@ -971,7 +1020,8 @@ mc_status run_steps(mc_plan* p, int num, int use_graph, int last, cudaStream_t s
         cudaError_t e = cudaStreamEndCapture(p->cap_stream, &graph);
         if (err != MC_OK) return err;
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-        e = cudaGraphInstantiate(&g, graph, 0);
+        e = prioritise_graph(graph);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&g, graph, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) {
           g = nullptr;
@@ -1155,7 +1205,7 @@ cudaError_t filter_prepare(mc_plan* p, void* dev, const float* in, float* tmp, f
   d.dep = const_cast<float*>(in);
   d.tmp = tmp;
   d.steric = out;
-  const StericCtas c = steric_ctas(p->R[0], p->fft_e);
+  const StericCtas c = steric_ctas(p->R[0], p->fft_e, p->fft_tv);
   const int cnt[7] = {c.fr16, c.fftr2, c.sconv, c.fc16, c.fftc2, c.fr12, c.fc12};
   std::vector<unsigned char> host(filter_desc_bytes(), 0);
   std::memcpy(host.data(), &d, sizeof(RDesc));
@@ -1171,7 +1221,7 @@ cudaError_t filter_prepare(mc_plan* p, void* dev, const float* in, float* tmp, f
 
 void filter_launch(mc_plan* p, const void* dev, cudaStream_t s) {
   const unsigned char* b = static_cast<const unsigned char*>(dev);
-  const StericCtas c = steric_ctas(p->R[0], p->fft_e);
+  const StericCtas c = steric_ctas(p->R[0], p->fft_e, p->fft_tv);
   const int cnt[7] = {c.fr16, c.fftr2, c.sconv, c.fc16, c.fftc2, c.fr12, c.fc12};
   auto launch = [&](int k) {
     Launch l;
@@ -1186,7 +1236,7 @@ void filter_launch(mc_plan* p, const void* dev, cudaStream_t s) {
   if (cnt[5]) launch_fft12_rows(launch(5));
   if (cnt[1]) launch_fft_rows_p2(launch(1), p->fftr2_smem);
   if (cnt[2]) launch_steric_conv(launch(2), p->sconv_smem);
-  if (cnt[3]) launch_fftreg_cols(launch(3), p->fft_e);
+  if (cnt[3]) launch_fftreg_cols(launch(3), p->fft_e, p->fft_tv);
   if (cnt[6]) launch_fft12_cols(launch(6));
   if (cnt[4]) launch_fft_cols_p2(launch(4), p->fftc2_smem);
 }

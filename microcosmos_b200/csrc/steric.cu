@@ -700,11 +700,14 @@ __global__ void __launch_bounds__(256) k_fftreg_rows(const RDesc* __restrict__ D
   }
 }
 
-// Column pass: 4096 / H column pairs per CTA of 4096 / E threads (G = H / E per pair),
-// staged from the row-pass output: at H = 1024 a CTA reads 32-byte row segments.
-template <int E>
-__global__ void __launch_bounds__(4096 / E) k_fftreg_cols(const RDesc* __restrict__ D, const int* __restrict__ off,
-                                                          int n) {
+// Column pass: TV / H column pairs per CTA of TV / E threads (G = H / E per pair), TV = 4096
+// values per CTA, or 2048 when a plan has too few columns to give every SM two CTAs (a single
+// 1024^2 lattice: 256 CTAs instead of 128); staged from the row-pass output: at H = 1024 a
+// CTA reads 32-byte (TV = 4096) or 16-byte row segments.  Every column pair is transformed
+// by the same code whatever TV is, so both give the same bits.
+template <int E, int TV>
+__global__ void __launch_bounds__(TV / E) k_fftreg_cols(const RDesc* __restrict__ D, const int* __restrict__ off,
+                                                        int n) {
   extern __shared__ float2 smr[];
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
@@ -858,19 +861,26 @@ void launch_fft12_rows(const Launch& L) { k_fft12_rows<<<L.grid, 256, kFft12Rows
 void launch_fft12_cols(const Launch& L) { k_fft12_cols<<<L.grid, 384, kFft12ColsSmem, L.s>>>(L.d, L.off, L.n); }
 
 // shared memory of a CTA: (row pass, 256 threads) 256 E / N transforms or (column pass,
-// 4096 / E threads) 4096 / N transforms, of N + N / 16 values each
+// TV / E threads) TV / N transforms, of N + N / 16 values each (+1 per column pair)
 size_t fftreg_smem(int e) { return (size_t)256 * e * 17 / 16 * sizeof(float2); }
-constexpr size_t kFftColsSmem = ((size_t)4096 * 17 / 16 + 256) * sizeof(float2);
+size_t fftreg_cols_smem(int tv) { return ((size_t)tv * 17 / 16 + 256) * sizeof(float2); }
 
 void launch_fftreg_rows(const Launch& L, int e) {
   if (e == 16) k_fftreg_rows<16><<<L.grid, 256, fftreg_smem(16), L.s>>>(L.d, L.off, L.n);
   else if (e == 8) k_fftreg_rows<8><<<L.grid, 256, fftreg_smem(8), L.s>>>(L.d, L.off, L.n);
   else k_fftreg_rows<4><<<L.grid, 256, fftreg_smem(4), L.s>>>(L.d, L.off, L.n);
 }
-void launch_fftreg_cols(const Launch& L, int e) {
-  if (e == 16) k_fftreg_cols<16><<<L.grid, 256, kFftColsSmem, L.s>>>(L.d, L.off, L.n);
-  else if (e == 8) k_fftreg_cols<8><<<L.grid, 512, kFftColsSmem, L.s>>>(L.d, L.off, L.n);
-  else k_fftreg_cols<4><<<L.grid, 1024, kFftColsSmem, L.s>>>(L.d, L.off, L.n);
+void launch_fftreg_cols(const Launch& L, int e, int tv) {
+  const size_t sm = fftreg_cols_smem(tv);
+  if (tv == 2048) {
+    if (e == 16) k_fftreg_cols<16, 2048><<<L.grid, 128, sm, L.s>>>(L.d, L.off, L.n);
+    else if (e == 8) k_fftreg_cols<8, 2048><<<L.grid, 256, sm, L.s>>>(L.d, L.off, L.n);
+    else k_fftreg_cols<4, 2048><<<L.grid, 512, sm, L.s>>>(L.d, L.off, L.n);
+    return;
+  }
+  if (e == 16) k_fftreg_cols<16, 4096><<<L.grid, 256, sm, L.s>>>(L.d, L.off, L.n);
+  else if (e == 8) k_fftreg_cols<8, 4096><<<L.grid, 512, sm, L.s>>>(L.d, L.off, L.n);
+  else k_fftreg_cols<4, 4096><<<L.grid, 1024, sm, L.s>>>(L.d, L.off, L.n);
 }
 
 
