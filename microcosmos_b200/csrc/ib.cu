@@ -415,6 +415,25 @@ __device__ __forceinline__ void stencil_sum_any(const RDesc& d, int node, const 
   sy = y;
 }
 
+// Body force of touched cell p from its corrected velocity after the last multi-direct
+// forcing round (fluid.py:327-339): post clamp of u_corrected, F = (u_c - u) rho, optional
+// force clamp.
+__device__ __forceinline__ void head_force(const RDesc& d, int p, float ucx, float ucy) {
+  const float c2 = clamp_factor(ucx, ucy, d.vmax);
+  ucx = ucx * c2;
+  ucy = ucy * c2;
+  const float rho = d.s_rho[p];
+  float Fx = (ucx - d.s_vx[p]) * rho;
+  float Fy = (ucy - d.s_vy[p]) * rho;
+  if (d.force_clamp) {
+    const float c3 = clamp_factor(Fx, Fy, d.vmax);
+    Fx = Fx * c3;
+    Fy = Fy * c3;
+  }
+  d.s_fx[p] = Fx;
+  d.s_fy[p] = Fy;
+}
+
 // Multi-direct forcing, interpolation half (fluid.py:292-302): per IB point, u at the point
 // = sum_s w_s u_corrected(cell_s); correction = (U_point - u) * relaxation, clamped.
 __global__ void __launch_bounds__(256) k_ib_interp(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
@@ -436,10 +455,14 @@ __global__ void __launch_bounds__(256) k_ib_interp(const RDesc* __restrict__ D, 
 // of correction * weight over its contributions, times 1/max(coverage, 1), added to
 // u_corrected.
 __global__ void __launch_bounds__(256) k_ib_spread(const RDesc* __restrict__ D, const int* __restrict__ off, int n,
-                                                   int it) {
+                                                   int it, int fuse_finalize) {
   const int r = find_rollout(off, n, blockIdx.x);
   const RDesc& d = D[r];
   const int p = (blockIdx.x - off[r]) * blockDim.x + threadIdx.x;
+  // the plan's last round also computes each touched cell's body force (k_ib_finalize's
+  // work for the same cell) when every rollout of the plan runs the same number of rounds
+  const bool fin = fuse_finalize && it == d.ib_iters - 1;
+  if (fin && p == 0) d.ib_ctl[5] = d.ib_ctl[2];
   if (it >= d.ib_iters || p >= d.ib_ctl[2]) return;
   const int len = d.h_len[p];
   const int* rn = d.ib_store + d.h_start[p];      // contributing nodes, in k order
@@ -471,8 +494,10 @@ __global__ void __launch_bounds__(256) k_ib_spread(const RDesc* __restrict__ D, 
     }
   }
   const float inv = d.s_inv[p];
-  d.s_ucx[p] = d.s_ucx[p] + dx * inv;
-  d.s_ucy[p] = d.s_ucy[p] + dy * inv;
+  const float ucx = d.s_ucx[p] + dx * inv, ucy = d.s_ucy[p] + dy * inv;
+  d.s_ucx[p] = ucx;
+  d.s_ucy[p] = ucy;
+  if (fin) head_force(d, p, ucx, ucy);
 }
 
 // ---------------------------------------------------------------- fused IB iterations
@@ -652,20 +677,7 @@ __global__ void __launch_bounds__(256) k_ib_finalize(const RDesc* __restrict__ D
   const int nheads = d.ib_ctl[2];
   if (p == 0) d.ib_ctl[5] = nheads;
   if (p >= nheads) return;
-  float ucx = d.s_ucx[p], ucy = d.s_ucy[p];
-  const float c2 = clamp_factor(ucx, ucy, d.vmax);
-  ucx = ucx * c2;
-  ucy = ucy * c2;
-  const float rho = d.s_rho[p];
-  float Fx = (ucx - d.s_vx[p]) * rho;
-  float Fy = (ucy - d.s_vy[p]) * rho;
-  if (d.force_clamp) {
-    const float c3 = clamp_factor(Fx, Fy, d.vmax);
-    Fx = Fx * c3;
-    Fy = Fy * c3;
-  }
-  d.s_fx[p] = Fx;
-  d.s_fy[p] = Fy;
+  head_force(d, p, d.s_ucx[p], d.s_ucy[p]);
 }
 
 // Node reaction (fluid.py:364-382), final wrap (simulate.py:97-98), non-finite check and
@@ -810,7 +822,9 @@ cudaError_t tiles_set_smem(size_t bytes) {
                               (int)(bytes - a.sharedSizeBytes));
 }
 void launch_ib_interp(const Launch& L, int it) { k_ib_interp<<<L.grid, kNodeThreads, 0, L.s>>>(L.d, L.off, L.n, it); }
-void launch_ib_spread(const Launch& L, int it) { k_ib_spread<<<L.grid, kHeadThreads, 0, L.s>>>(L.d, L.off, L.n, it); }
+void launch_ib_spread(const Launch& L, int it, int fuse_finalize) {
+  k_ib_spread<<<L.grid, kHeadThreads, 0, L.s>>>(L.d, L.off, L.n, it, fuse_finalize);
+}
 cudaError_t launch_ib_coop(const Launch& L, int parity) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(L.grid);

@@ -254,7 +254,7 @@ void launch_steric(const Launch& L);
 void launch_stencil(const Launch& L);
 void launch_stencil16(const Launch& L);
 void launch_ib_interp(const Launch& L, int it);
-void launch_ib_spread(const Launch& L, int it);
+void launch_ib_spread(const Launch& L, int it, int fuse_finalize);
 void launch_ib_finalize(const Launch& L, int parity);
 cudaError_t launch_ib_coop(const Launch& L, int parity);
 cudaError_t ib_coop_blocks_per_sm(int* out);

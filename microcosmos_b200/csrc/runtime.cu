@@ -42,6 +42,8 @@ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 
 constexpr int kDefaultSortCap = 2048;  // contributions per tile sorted in shared memory by default
+// largest plan (IB points over all rollouts) whose body force is computed by the last IB round
+constexpr long long kFuseFinalizeMaxPoints = 65536;
 
 enum Kind { K_NODES = 0, K_COMP, K_CHAIN, K_IB, K_TILES, K_LBM, K_CELLS, K_FFTR, K_FFTC, K_NODES16, K_IBCOOP, K_FFTR2, K_FFTC2, K_SCONV, K_FR16, K_FC16, K_FR12, K_FC12, K_COUNT };
 
@@ -124,6 +126,7 @@ struct mc_plan {
   int max_chain = 0, chain_slots = 1;
   int max_k = 0;  // largest IB kernel size of the plan
   int fft_e = 4;  // values per thread of the register-radix FFT kernels
+  bool fuse_finalize = false;  // body force computed by the last IB spread round
   int fft_tv = 4096;  // values per CTA of the register-radix column pass (4096 or 2048)
   bool use_coop = false, coop_cap_checked = false;
   bool fused_ib = false;  // mc_plan_set_fused_ib (separate launches measured faster)
@@ -878,11 +881,14 @@ int64_t enqueue_ib(mc_plan* p, int parity, cudaStream_t s, bool capture) {
   }
   // rollouts without nodes have no IB points: nothing to launch when no rollout has any
   if (!p->grid[K_NODES] || !p->grid[K_IB]) return k;
+  // when every rollout runs max_iters rounds, the last spread also computes the body force
+  const int fuse = p->fuse_finalize ? 1 : 0;
   for (int it = 0; it < p->max_iters; ++it) {
     timed(p, 7, s, capture, [&] { mc::launch_ib_interp(L(p, K_NODES, s), it); });
-    timed(p, 8, s, capture, [&] { mc::launch_ib_spread(L(p, K_IB, s), it); });
+    timed(p, 8, s, capture, [&] { mc::launch_ib_spread(L(p, K_IB, s), it, fuse); });
     k += 2;
   }
+  if (fuse) return k;
   timed(p, 9, s, capture, [&] { mc::launch_ib_finalize(L(p, K_IB, s), parity); });
   return k + 1;
 }
@@ -1451,6 +1457,18 @@ mc_status mc_plan_create(int32_t n, const mc_dims* dims, const mc_config* cfg, c
     p->max_iters = std::max(p->max_iters, c.enable_fluid ? c.ibm_iterations : 0);
     p->max_k = std::max(p->max_k, c.ibm_kernel_size);
   }
+  // The body force rides on the last multi-direct forcing round when every rollout with a
+  // fluid runs the same number of rounds (at least one) and the plan has at most
+  // kFuseFinalizeMaxPoints IB points.  Measured (L2 flushed before each step, same bits): one
+  // 1024^2 lattice with 16,384 points 0.1674 -> 0.1634 ms per step (one dependent launch
+  // less); the 256-rollout batch with 296 k points 1.864 -> 1.892 ms (there the separate
+  // pass over the touched cells is faster than the longer last round).
+  long long ib_points = 0;
+  for (const auto& h : p->R)
+    if (h.cfg.enable_fluid) ib_points += (long long)h.dims.N * (h.cfg.synthetic_node_width > 0.0f ? 2 : 1);
+  p->fuse_finalize = p->max_iters > 0 && ib_points <= kFuseFinalizeMaxPoints;
+  for (const auto& h : p->R)
+    if (h.cfg.enable_fluid && h.cfg.ibm_iterations != p->max_iters) p->fuse_finalize = false;
   // default dense-pass tile: 4 cells per lane x 16 rows for plans of >= 4 M lattice cells
   // (measured best at 2048^2 and on the 25 M-cell batch: 0.78 / 0.91 of HBM), 2 x 4 below
   // (best at 1024^2: 20.8 us vs 22.9 us for 4 x 16); narrower when the widths need it

@@ -190,6 +190,29 @@ def test_batch_equals_single_rollouts():
             np.testing.assert_array_equal(both[k], alone[k])
 
 
+def test_batch_with_different_ib_rounds_equals_single_rollouts():
+    """A plan whose rollouts run different numbers of multi-direct forcing rounds computes the
+    body force in its own pass after the rounds; a rollout alone computes it in its last
+    round.  Both give the same bits."""
+    scs = [scenarios.make_scenario(64, 64, 2, 16, seed=11), scenarios.make_scenario(48, 80, 3, 12, seed=12),
+           scenarios.make_scenario(64, 48, 2, 20, seed=13)]
+    cfgs = [baseline_config(ibm_iterations=5), baseline_config(ibm_iterations=2),
+            baseline_config(ibm_iterations=1)]
+    sts = [DeviceState.from_scenario(s) for s in scs]
+    acts = [Actuation.from_scenario(s) for s in scs]
+    plan = Plan.for_states(sts, cfgs, [0.01] * 3)
+    plan.rollout(sts, 10, actuations=acts)
+    torch.cuda.synchronize()
+    for sc, cfg, st, act in zip(scs, cfgs, sts, acts):
+        one = DeviceState.from_scenario(sc)
+        p1 = Plan.for_states([one], [cfg], [0.01])
+        p1.rollout([one], 10, actuations=[act])
+        torch.cuda.synchronize()
+        alone, both = one.host(), st.host()
+        for k in alone:
+            np.testing.assert_array_equal(both[k], alone[k])
+
+
 def test_recording_matches_final_state():
     sc = scenarios.make_scenario(32, 48, 2, 10, seed=4)
     cfg = baseline_config()
