@@ -605,8 +605,8 @@ def main():
     # read another 256 MiB buffer, so that the write's dirty lines are written back here and
     # not during the next timed step.  Then a spin kernel that touches no memory holds the
     # stream for about 0.5 ms while the host enqueues the step behind it, so the step's
-    # events and kernels run back to back on the device instead of each waiting for the
-    # host's launch call (which otherwise lands inside the per-kernel event pairs).
+    # events and kernels run back to back on the device instead of waiting for the host's
+    # launch calls.
     flush_w = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     flush_r = torch.zeros(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
